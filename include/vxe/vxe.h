@@ -1,0 +1,353 @@
+/*
+ * vxe.h -- C ABI of the B200-native primary / godray / composite passes.
+ *
+ * Drop-in boundary for voxel-engine-v0's compute frame.  Every struct below is
+ * byte-identical to the Rust `#[repr(C)]` POD that the reference uploads with
+ * `queue.write_buffer`, so a Rust host can pass its existing slices straight
+ * through `extern "C"`.  Every entry point cites the reference method it
+ * replaces (paths relative to the reference project root).
+ *
+ * Conventions
+ *  - All calls return vxe_status; vxe_last_error(ctx) gives a message.
+ *  - A vxe_ctx is externally synchronised (one host thread at a time), the
+ *    same contract as the reference `Renderer` (render/state/mod.rs:34-709).
+ *  - Host pointers are borrowed for the duration of the call only.
+ *  - Device pointers returned in vxe_frame_out stay valid until the next
+ *    vxe_render_frame / vxe_resize / vxe_destroy on the same ctx.
+ */
+#ifndef VXE_VXE_H
+#define VXE_VXE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+typedef enum vxe_status {
+  VXE_OK = 0,
+  VXE_ERR_INVALID_ARG = 1,
+  VXE_ERR_CAPACITY = 2,   /* upload exceeds an arena (reference skips silently) */
+  VXE_ERR_OOM = 3,        /* device allocation failed                          */
+  VXE_ERR_TIMEOUT = 4,    /* a bounded device wait gave up                      */
+  VXE_ERR_DEVICE = 5,     /* CUDA runtime error                                 */
+  VXE_ERR_BOUNDS = 6,     /* device-side bounds check tripped (error word set)  */
+  VXE_ERR_NO_DEVICE = 7   /* no CUDA device / extension unusable                */
+} vxe_status;
+
+/* ------------------------------------------------------------------------ */
+/* Constants (common.wgsl:16-19, 416-420; app/config.rs:5-51)                */
+/* ------------------------------------------------------------------------ */
+#define VXE_INVALID_U32 0xFFFFFFFFu
+#define VXE_LEAF_U32 0xFFFFFFFFu
+#define VXE_MACRO_WORDS_PER_CHUNK 16u
+#define VXE_COLINFO_WORDS_PER_CHUNK 2048u
+#define VXE_CHUNK_SIZE 64u
+#define VXE_CLIP_LEVELS_MAX 16u
+#define VXE_TILE_SIZE 8u
+#define VXE_MAX_TILE_CHUNKS 192u
+#define VXE_PRIMARY_MAX_TILE_CHUNKS 24u
+
+enum {
+  VXE_MAT_AIR = 0, VXE_MAT_GRASS = 1, VXE_MAT_DIRT = 2, VXE_MAT_STONE = 3,
+  VXE_MAT_WOOD = 4, VXE_MAT_LEAF = 5, VXE_MAT_LIGHT = 6
+};
+
+/* ------------------------------------------------------------------------ */
+/* GPU records (render/gpu_types.rs)                                         */
+/* ------------------------------------------------------------------------ */
+
+/* NodeGpu (render/gpu_types.rs:13-20, common.wgsl:338-343): 16 B. */
+typedef struct vxe_node {
+  uint32_t child_base; /* local index of first packed child, or VXE_LEAF_U32 */
+  uint32_t child_mask; /* bit ci = x | y<<1 | z<<2                           */
+  uint32_t material;
+  uint32_t key;        /* x | y<<6 | z<<12 | level<<18 (svo/builder_svo.rs:22-35) */
+} vxe_node;
+
+/* NodeRopesGpu (render/gpu_types.rs:22-33): 32 B, local neighbour indices. */
+typedef struct vxe_node_ropes {
+  uint32_t px, nx, py, ny, pz, nz, _pad0, _pad1;
+} vxe_node_ropes;
+
+/* ChunkMetaGpu (render/gpu_types.rs:36-48): 48 B. */
+typedef struct vxe_chunk_meta {
+  int32_t origin[4];     /* chunk origin in voxels, w = 0 */
+  uint32_t node_base;    /* global arena index of the chunk's root */
+  uint32_t node_count;
+  uint32_t macro_base;   /* slot * 16 */
+  uint32_t colinfo_base; /* slot * 2048 */
+  uint32_t macro_empty;  /* 1 when all 512 macro bits are 0 */
+  uint32_t _pad0, _pad1, _pad2;
+} vxe_chunk_meta;
+
+/* CameraGpu (render/gpu_types.rs:50-86): 464 B, matrices column-major. */
+typedef struct vxe_camera_gpu {
+  float view_inv[4][4];
+  float proj_inv[4][4];
+  float view_proj[4][4];
+  float prev_view_proj[4][4];
+  float cam_pos[4];
+  float ray00[4];
+  float ray_dx[4];
+  float ray_dy[4];
+  uint32_t chunk_size;
+  uint32_t chunk_count;
+  uint32_t max_steps;
+  uint32_t frame_index;
+  float voxel_params[4];      /* [voxel_size, time_s, wind_strength, fog_density] */
+  int32_t grid_origin_chunk[4];
+  uint32_t grid_dims[4];
+  uint32_t render_present_px[4]; /* internal w,h ; present w,h */
+  uint32_t profile_flags;
+  uint32_t _pad_profile[3];
+  uint32_t _pad0[4];
+  uint32_t _pad1[4];
+  uint32_t _pad2[4];
+} vxe_camera_gpu;
+
+/* ClipmapGpu (render/gpu_types.rs:103-138): 528 B. */
+typedef struct vxe_clipmap_gpu {
+  uint32_t levels;
+  uint32_t res;
+  float base_cell_m;
+  float _pad0;
+  float level[VXE_CLIP_LEVELS_MAX][4];     /* origin_x_m, origin_z_m, cell_m, 0 */
+  uint32_t offset[VXE_CLIP_LEVELS_MAX][4]; /* off_x, off_z, 0, 0 (texels)      */
+} vxe_clipmap_gpu;
+
+/* ClipmapUpload (clipmap.rs:35-42): a sub-rectangle of one level layer. */
+typedef struct vxe_clip_patch {
+  uint32_t level, x, y, w, h;
+  const float* data; /* w*h floats, row-major */
+} vxe_clip_patch;
+
+/* ChunkUpload (streaming/types.rs:87-103). */
+typedef struct vxe_chunk_upload {
+  uint32_t slot;
+  vxe_chunk_meta meta;
+  uint32_t node_base;
+  uint32_t node_count;
+  const vxe_node* nodes;          /* node_count records */
+  const vxe_node_ropes* ropes;    /* node_count records */
+  const uint32_t* macro_words;    /* 16 words            */
+  const uint32_t* colinfo_words;  /* 2048 words          */
+} vxe_chunk_upload;
+
+/* ------------------------------------------------------------------------ */
+/* Context                                                                   */
+/* ------------------------------------------------------------------------ */
+typedef struct vxe_ctx vxe_ctx;
+
+enum {
+  /* The reference binds the scene group for main_godray with macro_occ at
+   * binding 8 while the shader reads binding 9 (render/state/bindgroups.rs:
+   * 116-156 vs shaders/common.wgsl:407-409), so godray shadow marches read
+   * rope words as macro bits.  Set = reproduce that aliasing (default). */
+  VXE_FLAG_GODRAY_MACRO_ALIAS = 1u << 0,
+  /* Reference render/state/mod.rs:538-565 silently skips uploads that do not
+   * fit; set to keep that behaviour, clear to get VXE_ERR_CAPACITY. */
+  VXE_FLAG_SILENT_CAPACITY_SKIP = 1u << 1,
+  /* Write per-pixel hit records (t, node, voxel, face, mat) from the primary
+   * pass (the reference has no such output; see vxe_hit). */
+  VXE_FLAG_HIT_RECORDS = 1u << 2,
+  /* Keep the intermediate images (local_img, output_pre_taa) that the fused
+   * kernels otherwise never materialise; used by parity tests. */
+  VXE_FLAG_DEBUG_INTERMEDIATES = 1u << 3,
+  /* Device-side bounds checks on every arena index (sets the error word). */
+  VXE_FLAG_CHECKED = 1u << 4
+};
+
+typedef struct vxe_config {
+  uint32_t node_capacity;    /* NodeGpu records in the arena (ropes: same)   */
+  uint32_t chunk_capacity;   /* ChunkMetaGpu slots                           */
+  uint32_t grid_capacity;    /* chunk_grid cells                             */
+  uint32_t clip_levels;      /* clipmap layers allocated (<= 16)             */
+  uint32_t clip_res;         /* clipmap texture side                         */
+  uint32_t flags;            /* VXE_FLAG_*                                    */
+  int32_t device;            /* CUDA ordinal                                 */
+  uint32_t _reserved;
+} vxe_config;
+
+/* Renderer::new (render/state/mod.rs:147-267). */
+vxe_status vxe_create(const vxe_config* cfg, vxe_ctx** out);
+void vxe_destroy(vxe_ctx* ctx);
+const char* vxe_last_error(const vxe_ctx* ctx);
+uint32_t vxe_get_flags(const vxe_ctx* ctx);
+vxe_status vxe_set_flags(vxe_ctx* ctx, uint32_t flags);
+
+/* Renderer::resize_output (render/state/mod.rs:297-308): recreates the images
+ * (internal = round(present*render_scale)) and resets histories + ping. */
+vxe_status vxe_resize(vxe_ctx* ctx, uint32_t present_w, uint32_t present_h, float render_scale);
+vxe_status vxe_get_internal_dims(const vxe_ctx* ctx, uint32_t* w, uint32_t* h);
+
+/* Renderer::apply_chunk_uploads (render/state/mod.rs:514-582).  Copies are
+ * issued on the upload stream and ordered before the next frame by an event. */
+vxe_status vxe_upload_chunks(vxe_ctx* ctx, const vxe_chunk_upload* ups, uint32_t n);
+/* Meta-only rewrite of slots [first, first+n) (render/state/mod.rs:104-144). */
+vxe_status vxe_write_meta(vxe_ctx* ctx, uint32_t first_slot, const vxe_chunk_meta* metas, uint32_t n);
+/* Renderer::write_chunk_grid (render/state/mod.rs:310-317). */
+vxe_status vxe_write_grid(vxe_ctx* ctx, const uint32_t* grid, uint32_t n);
+/* Renderer::write_camera (render/state/mod.rs:319-322). */
+vxe_status vxe_write_camera(vxe_ctx* ctx, const vxe_camera_gpu* cam);
+/* Renderer::write_clipmap_updates (render/state/mod.rs:586-634): patches
+ * first, then the uniform, both ordered before the next frame. */
+vxe_status vxe_write_clipmap(vxe_ctx* ctx, const vxe_clipmap_gpu* params,
+                             const vxe_clip_patch* patches, uint32_t n);
+
+/* Outputs of one frame (device pointers, ctx-owned). */
+typedef struct vxe_frame_out {
+  float* color;        /* internal w*h RGBA32F  (color_img)      */
+  float* depth;        /* internal w*h R32F     (depth_img)      */
+  float* godray;       /* internal w*h RGBA32F  (godray[pong])   */
+  float* output;       /* present  w*h RGBA32F  (output_tex)     */
+  uint32_t internal_w, internal_h, present_w, present_h;
+} vxe_frame_out;
+
+/* Renderer::encode_compute (render/state/mod.rs:329-446): primary, local
+ * TAA, godray, composite, composite TAA with the reference ping-pong; plain
+ * launches on the ctx compute stream.  Synchronous unless `async` != 0. */
+vxe_status vxe_render_frame(vxe_ctx* ctx, vxe_frame_out* out);
+vxe_status vxe_render_frame_async(vxe_ctx* ctx, vxe_frame_out* out);
+/* Same frame replayed from a CUDA graph captured on first use (per size). */
+vxe_status vxe_render_frame_graph(vxe_ctx* ctx, vxe_frame_out* out);
+vxe_status vxe_synchronize(vxe_ctx* ctx);
+
+/* Hit record (no reference counterpart; defined by this project):
+ *   node  = global arena index of the leaf that produced the hit, or
+ *           VXE_INVALID_U32 for implicit-air grass hits and heightfield hits
+ *   voxel = world voxel containing the hit point, clamped to the leaf cube
+ *   face  = 0..5 (+X,-X,+Y,-Y,+Z,-Z) of the dominant normal axis, 255 = miss
+ *   mat   = HitGeom.mat (chunk_trace.wgsl:15-32); 0 on miss               */
+typedef struct vxe_hit {
+  float t;
+  uint32_t node;
+  int32_t voxel[3];
+  uint32_t face;
+  uint32_t mat;
+  uint32_t _pad;
+} vxe_hit;
+
+/* Ray queries (picking / physics): per-ray chunk-grid DDA over the resident
+ * world, voxel geometry only, first hit within [0, tmax].  Host arrays of
+ * n*3 floats; result written to host `out`.  The reference does this on the
+ * CPU (app/app.rs:847-961). */
+vxe_status vxe_trace_rays(vxe_ctx* ctx, const float* origins, const float* dirs, uint32_t n,
+                          float tmax, vxe_hit* out);
+/* Same, device pointers in and out, launched on the compute stream. */
+vxe_status vxe_trace_rays_device(vxe_ctx* ctx, const float* d_origins, const float* d_dirs,
+                                 uint32_t n, float tmax, vxe_hit* d_out);
+
+/* GpuTimingsMs (render/state/mod.rs:22-31) minus blit; CUDA events of the last
+ * frame.  local_taa and composite_taa are fused into primary / composite and
+ * report 0. */
+typedef struct vxe_timings {
+  double primary, local_taa, godray, composite, composite_taa, tiles, total;
+} vxe_timings;
+vxe_status vxe_get_timings(vxe_ctx* ctx, vxe_timings* out);
+
+/* Images that can be read / written for teacher-forced parity runs. */
+typedef enum vxe_image {
+  VXE_IMG_COLOR = 0, VXE_IMG_DEPTH = 1, VXE_IMG_LOCAL = 2,
+  VXE_IMG_PRIMARY_HIST_IN = 3, VXE_IMG_PRIMARY_HIST_OUT = 4,
+  VXE_IMG_SHADOW_IN = 5, VXE_IMG_SHADOW_OUT = 6,
+  VXE_IMG_LOCAL_HIST_IN = 7, VXE_IMG_LOCAL_HIST_OUT = 8,
+  VXE_IMG_GODRAY_IN = 9, VXE_IMG_GODRAY_OUT = 10,
+  VXE_IMG_OUTPUT_PRE_TAA = 11, VXE_IMG_OUTPUT = 12,
+  VXE_IMG_OUTPUT_HIST_IN = 13, VXE_IMG_OUTPUT_HIST_OUT = 14,
+  VXE_IMG_HITS = 15,
+  VXE_IMG_COUNT = 16
+} vxe_image;
+/* "IN" = the history the next frame reads, "OUT" = the one it writes. */
+vxe_status vxe_image_size(const vxe_ctx* ctx, vxe_image img, size_t* bytes);
+vxe_status vxe_read_image(vxe_ctx* ctx, vxe_image img, void* host, size_t bytes);
+vxe_status vxe_write_image(vxe_ctx* ctx, vxe_image img, const void* host, size_t bytes);
+
+/* Device error word (bounds checks / bounded waits); cleared on read. */
+vxe_status vxe_read_error_word(vxe_ctx* ctx, uint32_t* word);
+
+/* Diagnostic (no reference counterpart): evaluates the deterministic math
+ * of detmath.h on the device for n host inputs; which = 0 sin, 1 cos, 2 exp,
+ * 3 pow(x, y), 4 min(x, y), 5 max(x, y).  Used to prove host/device bit
+ * equality of the functions every pass depends on. */
+vxe_status vxe_debug_detmath(int which, const float* x, const float* y, float* out, uint32_t n);
+
+/* ------------------------------------------------------------------------ */
+/* Producer side (C++ port of src/svo, streaming meta, clipmap, camera)      */
+/* ------------------------------------------------------------------------ */
+
+/* Seeded synthetic world used for every benchmark configuration (the
+ * reference's Perlin worldgen is replaced by project value noise). */
+typedef struct vxe_world_params {
+  uint32_t seed;
+  int32_t height_min;       /* surface voxel y range [min, max] */
+  int32_t height_max;
+  int32_t dirt_depth;       /* dirt voxels below grass; also builder dirt_depth */
+  uint32_t carve_mod;       /* solid voxel -> air when hash3 % carve_mod == 0 (0 = off) */
+  float cave_threshold;     /* 3D value noise > threshold -> air (>= 1 = off) */
+  float height_scale_vox;   /* lattice spacing of the height noise octave 0 */
+  uint32_t features;        /* bit0 trees (wood+leaf), bit1 light voxels */
+} vxe_world_params;
+
+typedef struct vxe_built_chunk {
+  vxe_node* nodes;
+  vxe_node_ropes* ropes;
+  uint32_t node_count;
+  uint32_t macro_words[VXE_MACRO_WORDS_PER_CHUNK];
+  uint32_t colinfo_words[VXE_COLINFO_WORDS_PER_CHUNK];
+  uint32_t solid_voxels;
+} vxe_built_chunk;
+
+/* build_chunk_svo_sparse_cancelable_with_scratch (svo/builder.rs:846-986). */
+vxe_status vxe_build_chunk(const vxe_world_params* wp, int32_t cx, int32_t cy, int32_t cz,
+                           vxe_built_chunk* out);
+void vxe_free_chunk(vxe_built_chunk* c);
+/* Dense material grid (layout y*64*64 + z*64 + x, svo/builder.rs:528-668). */
+vxe_status vxe_chunk_materials(const vxe_world_params* wp, int32_t cx, int32_t cy, int32_t cz,
+                               uint8_t* out_64cubed);
+/* Ground height (surface voxel y) at a world voxel column. */
+int32_t vxe_ground_height(const vxe_world_params* wp, int32_t wx, int32_t wz);
+
+/* Build the SVO + ropes + macro + colinfo from a caller material grid. */
+vxe_status vxe_build_from_materials(const uint8_t* material_64cubed, int32_t chunk_oy,
+                                    const int32_t* ground_64x64, int32_t dirt_depth,
+                                    vxe_built_chunk* out);
+
+/* Camera packing (app/app.rs:411-511, app/camera.rs:95-111), double math
+ * rounded to f32. */
+typedef struct vxe_camera_params {
+  float pos[3];
+  float yaw, pitch;
+  float fovy_rad, z_near, z_far;
+  uint32_t present_w, present_h, internal_w, internal_h;
+  uint32_t frame_index;
+  uint32_t jitter;            /* 1 = halton(frame+1)-0.5 sub-pixel jitter */
+  float time_s;
+  uint32_t chunk_count;
+  int32_t grid_origin_chunk[3];
+  uint32_t grid_dims[3];
+  uint32_t has_prev;          /* 0 -> prev_view_proj = view_proj */
+  float prev_view_proj[4][4];
+} vxe_camera_params;
+vxe_status vxe_build_camera(const vxe_camera_params* p, vxe_camera_gpu* out);
+
+/* Toroidal clipmap (clipmap.rs:182-577).  State lives in an opaque handle. */
+typedef struct vxe_clipmap_state vxe_clipmap_state;
+vxe_clipmap_state* vxe_clipmap_new(const vxe_world_params* wp, uint32_t levels, uint32_t res,
+                                   float base_cell_m);
+void vxe_clipmap_free(vxe_clipmap_state* s);
+/* Computes the new params and patches for camera (x,z).  Patch data pointers
+ * stay valid until the next update / free. */
+vxe_status vxe_clipmap_update(vxe_clipmap_state* s, float cam_x, float cam_z,
+                              vxe_clipmap_gpu* params, const vxe_clip_patch** patches,
+                              uint32_t* n_patches);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* VXE_VXE_H */

@@ -1,0 +1,726 @@
+// frame_kernels.cuh -- the frame passes as sm_100a kernels.
+//
+//   k_tiles      per 8x8 logical tile: two probe-ray chunk-grid DDAs, dedup,
+//                partial selection sort (ray_main.wgsl:179-197,
+//                chunk_trace.wgsl:1007-1175).  Runs as its own launch so the
+//                primary launch shape is free of the 8x8 workgroup.
+//   k_primary    main_primary (ray_main.wgsl:163-517) with main_local_taa
+//                (taa.wgsl:26-69) fused into the epilogue: local TAA reads only
+//                the same pixel, so local_img never round-trips through HBM.
+//   k_godray     main_godray (ray_main.wgsl:520-535, godrays.wgsl:241-356).
+//   k_composite  main_composite (ray_main.wgsl:537-573, composite.wgsl) with
+//                main_composite_taa (taa.wgsl:82-110) fused: it reads only the
+//                composite output of the same pixel.
+//   k_query      ray queries: per-ray chunk DDA, voxel geometry only.
+#pragma once
+
+#include "device_trace.cuh"
+
+namespace vxe {
+namespace dev {
+
+struct FrameArgs {
+  vxe_camera_gpu cam;
+  vxe_clipmap_gpu clip;
+  const uint4* nodes;
+  uint64_t nodes_n;
+  const uint32_t* ropes;
+  uint64_t ropes_n;
+  const uint4* metas;
+  uint64_t metas_n;
+  const uint32_t* grid;
+  uint64_t grid_n;
+  const uint32_t* macro;
+  uint64_t macro_n;
+  const uint32_t* colinfo;
+  uint64_t colinfo_n;
+  const float* clip_tex;
+  uint32_t clip_layers, clip_res;
+  uint32_t* err;
+  uint32_t godray_alias;
+  uint32_t iw, ih, pw, ph;
+  uint32_t* tile_count;  // tiles
+  uint32_t* tile_slots;  // tiles * 24
+  const uint4* hist_in;
+  uint4* hist_out;
+  const float* shadow_in;
+  float* shadow_out;
+  const float4* local_hist_in;
+  float4* local_hist_out;
+  float4* color;
+  float* depth;
+  float4* local;  // optional (debug intermediates)
+  const float4* god_in;
+  float4* god_out;
+  float4* pre_taa;  // optional (debug intermediates)
+  float4* output;
+  const float4* out_hist_in;
+  float4* out_hist_out;
+  uint4* hits;  // optional, 2 x uint4 per pixel (vxe_hit)
+};
+
+__device__ __forceinline__ Scene make_scene(const FrameArgs& A, bool godray) {
+  Scene s;
+  s.cam = &A.cam;
+  s.clip = &A.clip;
+  s.nodes = A.nodes;
+  s.nodes_n = A.nodes_n;
+  s.ropes = A.ropes;
+  s.ropes_n = A.ropes_n;
+  s.metas = A.metas;
+  s.metas_n = A.metas_n;
+  s.grid = A.grid;
+  s.grid_n = A.grid_n;
+  if (godray && A.godray_alias) {
+    // Reference binding mismatch: main_godray's macro_occ reads the rope buffer.
+    s.macro = A.ropes;
+    s.macro_n = A.ropes_n * 8u;
+  } else {
+    s.macro = A.macro;
+    s.macro_n = A.macro_n;
+  }
+  s.colinfo = A.colinfo;
+  s.colinfo_n = A.colinfo_n;
+  s.clip_tex = A.clip_tex;
+  s.clip_layers = A.clip_layers;
+  s.clip_res = A.clip_res;
+  s.err = A.err;
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// Tile candidate lists
+// ---------------------------------------------------------------------------
+constexpr int TILE_THREADS = 32;
+
+__global__ void __launch_bounds__(TILE_THREADS) k_tiles(const __grid_constant__ FrameArgs A) {
+  __shared__ uint32_t sl[MAX_TILE_CHUNKS][TILE_THREADS];
+  __shared__ float en[MAX_TILE_CHUNKS][TILE_THREADS];
+  const uint32_t lane = threadIdx.x;
+  const uint32_t tiles_x = (A.iw + 7u) / 8u, tiles_y = (A.ih + 7u) / 8u;
+  const uint32_t tile = blockIdx.x * TILE_THREADS + lane;
+  if (tile >= tiles_x * tiles_y) return;
+  const Scene s = make_scene(A, false);
+  const uint32_t tx = tile % tiles_x, ty = tile / tiles_x;
+  uint32_t count = 0;
+  if (s.cam->chunk_count != 0u) {
+    const v2 base = V2((float)(tx * TILE_SIZE), (float)(ty * TILE_SIZE));
+    const v3 ro = cam_pos(s);
+    auto add = [&](uint32_t slot, float te) -> bool {
+      // tile_add_candidate (chunk_trace.wgsl:1007-1026)
+      if (slot < s.cam->chunk_count && meta_empty(s, slot) != 0u) return false;
+      for (uint32_t i = 0; i < count && i < MAX_TILE_CHUNKS; ++i) {
+        if (sl[i][lane] == slot) {
+          en[i][lane] = fminf(en[i][lane], te);
+          return false;
+        }
+      }
+      const uint32_t idx = count++;
+      if (idx < MAX_TILE_CHUNKS) {
+        sl[idx][lane] = slot;
+        en[idx][lane] = te;
+      }
+      return false;
+    };
+    chunk_grid_dda(s, ro, ray_dir_from_pixel(s, base + V2(4.5f, 4.5f)), 0.0f, FOG_MAX_DIST, add);
+    chunk_grid_dda(s, ro, ray_dir_from_pixel(s, base + V2(1.5f, 1.5f)), 0.0f, FOG_MAX_DIST, add);
+  }
+  const uint32_t raw = min(count, MAX_TILE_CHUNKS);
+  const uint32_t limit = min(raw, TILE_CANDS);
+  // tile_sort_candidates_by_enter (chunk_trace.wgsl:1153-1175): selection sort of the first 24.
+  if (raw > 1u && limit > 1u) {
+    for (uint32_t i = 0; i + 1u < limit; ++i) {
+      uint32_t mi = i;
+      float mt = en[i][lane];
+      for (uint32_t j = i + 1u; j < limit; ++j) {
+        const float e = en[j][lane];
+        if (e < mt) { mt = e; mi = j; }
+      }
+      if (mi != i) {
+        const uint32_t ts = sl[i][lane];
+        const float tt = en[i][lane];
+        sl[i][lane] = sl[mi][lane];
+        en[i][lane] = en[mi][lane];
+        sl[mi][lane] = ts;
+        en[mi][lane] = tt;
+      }
+    }
+  }
+  A.tile_count[tile] = limit;
+  for (uint32_t i = 0; i < TILE_CANDS; ++i) A.tile_slots[(size_t)tile * TILE_CANDS + i] = i < limit ? sl[i][lane] : INVALID;
+}
+
+// trace_scene_voxels_candidates (chunk_trace.wgsl:1177-1265) over a tile list
+// staged in shared memory (slots + their ChunkMeta records).
+__device__ VoxTraceResult trace_candidates(const Scene& s, const uint32_t* cslot, const Meta* cmeta, v3 ro, v3 rd,
+                                           float t_min, float t_max, bool anchor_valid_in, i3 anchor_chunk_in,
+                                           uint32_t anchor_key_in, uint32_t cand_count) {
+  VoxTraceResult none{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
+  if (s.cam->chunk_count == 0u) return none;
+  const float vsz = vs_(s);
+  const float cs = (float)s.cam->chunk_size * vsz;
+  const int32_t* go = s.cam->grid_origin_chunk;
+  const uint32_t* gd = s.cam->grid_dims;
+  const v3 gb0 = V3((float)go[0], (float)go[1], (float)go[2]) * cs;
+  const v3 gb1 = gb0 + V3((float)gd[0], (float)gd[1], (float)gd[2]) * cs;
+  const v2 rtg = intersect_aabb(ro, rd, gb0, gb1);
+  const float t_enter = fmax_(fmax_(rtg.x, 0.0f), t_min);
+  const float t_exit = fmin_(fmin_(rtg.y, FOG_MAX_DIST), t_max);
+  if (t_exit < t_enter) return none;
+  HitGeom best = miss_hitgeom();
+  bool bav = false;
+  uint32_t bak = INVALID;
+  i3 bac{0, 0, 0};
+  const v3 inv = safe_inv3(rd);
+  const float rs = (float)s.cam->chunk_size * vsz;
+  const uint32_t maxc = min(cand_count, MAX_TILE_CHUNKS);
+  const TraceOpts opt{false};
+  for (uint32_t i = 0; i < maxc; ++i) {
+    const uint32_t slot = cslot[i];
+    if (slot == INVALID || slot >= s.cam->chunk_count) continue;
+    const Meta ch = cmeta[i];
+    if (ch.macro_empty != 0u) continue;
+    const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vsz;
+    const v2 rt = intersect_aabb(ro, rd, rb, rb + V3s(rs));
+    const float ce = fmax_(rt.x, t_enter), cx = fmin_(rt.y, t_exit);
+    if (cx < ce) continue;
+    if (best.hit != 0u && ce >= best.t) continue;
+    if (chunk_heightfield_early_skip(s, ro, rd, ce, cx, ch, vsz)) continue;
+    const int32_t csz = (int32_t)s.cam->chunk_size;
+    const i3 cc{ch.ox / csz, ch.oy / csz, ch.oz / csz};
+    const bool ua = anchor_valid_in && chunk_coords_neighbor(cc, anchor_chunk_in);
+    const uint32_t aku = ua ? anchor_key_in : INVALID;
+    const ChunkTraceResult h = trace_chunk_interval_stream_macro(s, ro, rd, inv, ch, ce, cx, ua, aku, opt);
+    if (h.hit.hit != 0u && h.hit.t < best.t) {
+      best = h.hit;
+      bav = h.anchor_valid;
+      bak = h.anchor_key;
+      bac = cc;
+    }
+  }
+  return VoxTraceResult{true, best, t_exit, bav, bak, bac};
+}
+
+// ---------------------------------------------------------------------------
+// Hit records
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t face_from_n(v3 n) {
+  const float ax = fabsf(n.x), ay = fabsf(n.y), az = fabsf(n.z);
+  if (ax >= ay && ax >= az) return n.x > 0.0f ? 0u : 1u;
+  if (ay >= az) return n.y > 0.0f ? 2u : 3u;
+  return n.z > 0.0f ? 4u : 5u;
+}
+
+struct HitRec {
+  float t;
+  uint32_t node;
+  int32_t vx, vy, vz;
+  uint32_t face, mat;
+};
+
+__device__ __forceinline__ HitRec miss_rec() { return HitRec{BIG, INVALID, 0, 0, 0, 255u, 0u}; }
+
+__device__ HitRec make_rec(const HitGeom& g, v3 ro, v3 rd, float vs, bool voxel_hit) {
+  HitRec h;
+  h.t = g.t;
+  h.node = g.node;
+  h.mat = g.mat;
+  h.face = face_from_n(g.n);
+  const v3 p = ro + rd * g.t;
+  if (voxel_hit) {
+    const v3 lr = (p - g.root_bmin) / vs;
+    const v3 lmin = (g.leaf_bmin - g.root_bmin) / vs;
+    const int32_t l0x = to_i32(floorf(lmin.x + 0.5f)), l0y = to_i32(floorf(lmin.y + 0.5f)),
+                  l0z = to_i32(floorf(lmin.z + 0.5f));
+    const int32_t ls = to_i32(floorf(g.leaf_size / vs + 0.5f));
+    const int32_t ox = to_i32(floorf(g.root_bmin.x / vs + 0.5f)), oy = to_i32(floorf(g.root_bmin.y / vs + 0.5f)),
+                  oz = to_i32(floorf(g.root_bmin.z / vs + 0.5f));
+    h.vx = ox + clampi(to_i32(floorf(lr.x)), l0x, l0x + ls - 1);
+    h.vy = oy + clampi(to_i32(floorf(lr.y)), l0y, l0y + ls - 1);
+    h.vz = oz + clampi(to_i32(floorf(lr.z)), l0z, l0z + ls - 1);
+  } else {
+    h.vx = to_i32(floorf(p.x / vs));
+    h.vy = to_i32(floorf(p.y / vs));
+    h.vz = to_i32(floorf(p.z / vs));
+  }
+  return h;
+}
+
+__device__ __forceinline__ void store_rec(uint4* dst, const HitRec& h) {
+  dst[0] = make_uint4(__float_as_uint(h.t), h.node, (uint32_t)h.vx, (uint32_t)h.vy);
+  dst[1] = make_uint4((uint32_t)h.vz, h.face, h.mat, 0u);
+}
+
+__device__ __forceinline__ uint32_t pack_i16x2(int32_t a, int32_t b) {
+  return ((uint32_t)a & 0xFFFFu) | (((uint32_t)b & 0xFFFFu) << 16);
+}
+__device__ __forceinline__ int32_t unpack_i16(uint32_t v) {
+  const int32_t s = (int32_t)(v & 0xFFFFu);
+  return (v & 0x8000u) != 0u ? s - 0x10000 : s;
+}
+__device__ __forceinline__ int32_t nearest_idx(float u, uint32_t n) {
+  return clampi(to_i32(floorf(u * (float)n)), 0, (int32_t)n - 1);
+}
+__device__ __forceinline__ v3 xyz(float4 v) { return V3(v.x, v.y, v.z); }
+
+// ---------------------------------------------------------------------------
+// Primary pass (+ fused local TAA)
+// ---------------------------------------------------------------------------
+constexpr int PRIMARY_THREADS = 128;  // two 8x8 logical tiles per block
+
+__global__ void __launch_bounds__(PRIMARY_THREADS) k_primary(const __grid_constant__ FrameArgs A) {
+  __shared__ uint32_t cslot[2][TILE_CANDS];
+  __shared__ Meta cmeta[2][TILE_CANDS];
+  __shared__ uint32_t ccount[2];
+  const Scene s = make_scene(A, false);
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+  const uint32_t tiles_x = (A.iw + 7u) / 8u;
+  const uint32_t ty = blockIdx.y;
+  if (tid < 2u * TILE_CANDS) {
+    const uint32_t t = tid / TILE_CANDS, i = tid % TILE_CANDS;
+    const uint32_t tx = blockIdx.x * 2u + t;
+    uint32_t n = 0u, slot = INVALID;
+    if (tx < tiles_x) {
+      const size_t tile = (size_t)ty * tiles_x + tx;
+      n = A.tile_count[tile];
+      slot = A.tile_slots[tile * TILE_CANDS + i];
+    }
+    if (i == 0u) ccount[t] = n;
+    cslot[t][i] = slot;
+    if (i < n && slot != INVALID && slot < s.cam->chunk_count) cmeta[t][i] = meta_at(s, slot);
+  }
+  __syncthreads();
+  const uint32_t t = warp >> 1;
+  const uint32_t tx = blockIdx.x * 2u + t;
+  const uint32_t gx = tx * 8u + (lane & 7u);
+  const uint32_t gy = ty * 8u + (warp & 1u) * 4u + (lane >> 3);
+  if (tx >= tiles_x || gx >= A.iw || gy >= A.ih) return;
+  const uint32_t W = A.iw, H = A.ih;
+  const size_t pix = (size_t)gy * W + gx;
+  const uint32_t tile_count = ccount[t];
+  const v3 sky_up = sky_bg(V3(0.0f, 1.0f, 0.0f));
+  const v2 res = V2((float)W, (float)H);
+  const v2 px = V2((float)gx + 0.5f, (float)gy + 0.5f);
+  const uint32_t seed = (gx * 1973u) ^ (gy * 9277u) ^ (s.cam->frame_index * 26699u);
+  const v3 ro = cam_pos(s);
+  const v3 rd = ray_dir_from_pixel(s, px);
+  const float vs = vs_(s);
+  v3 local_out = V3s(0.0f);
+  float local_w = 0.0f;
+  float t_store = 0.0f;
+  float shadow_out = 1.0f;
+  HitRec rec = miss_rec();
+  v3 col;
+  float depth;
+  uint4 hist;
+
+  bool shade_hf = true;
+  if (s.cam->chunk_count != 0u) {
+    float t_hist = 0.0f;
+    bool hist_valid = false;
+    uint32_t hak = INVALID;
+    i3 hac{0, 0, 0};
+    const bool has_tc = tile_count != 0u;
+    const v2 uv = px / res;
+    if (has_tc) {
+      const float t_guess = __uint_as_float(A.hist_in[pix].x);
+      if (t_guess > 1e-3f) {
+        const v3 p_ws = ro + rd * t_guess;
+        const v2 uvp = prev_uv_from_world(s, p_ws);
+        if (in_unit_square(uvp)) {
+          const int32_t sx = nearest_idx(uvp.x, W), sy = nearest_idx(uvp.y, H);
+          const uint4 hp = A.hist_in[(size_t)sy * W + (uint32_t)sx];
+          const float t_prev = __uint_as_float(hp.x);
+          const float rel = fabsf(t_prev - t_guess) / fmax_(t_guess, 1e-3f);
+          const float depth_ok = 1.0f - smooth(PRIMARY_HIT_DEPTH_REL0, PRIMARY_HIT_DEPTH_REL1, rel);
+          const float vel = length((uvp - uv) * res);
+          const float motion_ok = 1.0f - smooth(PRIMARY_HIT_MOTION_PX0, PRIMARY_HIT_MOTION_PX1, vel);
+          if (t_prev > 1e-3f && depth_ok > 0.5f && motion_ok > 0.5f) {
+            t_hist = t_prev;
+            hist_valid = true;
+            if ((hp.w & 0x80000000u) != 0u) {
+              hak = hp.y;
+              hac = i3{unpack_i16(hp.z), unpack_i16(hp.z >> 16), unpack_i16(hp.w)};
+            }
+          }
+        }
+      }
+    }
+    const float t_start = fmax_(t_hist - PRIMARY_HIT_MARGIN, 0.0f);
+    const float t_end = fmin_(t_hist + PRIMARY_HIT_WINDOW, FOG_MAX_DIST);
+    VoxTraceResult vt{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
+    if (has_tc) {
+      bool done = false;
+      if (hist_valid) {
+        const VoxTraceResult h =
+            trace_candidates(s, cslot[t], cmeta[t], ro, rd, t_start, t_end, hak != INVALID, hac, hak, tile_count);
+        if (h.best.hit != 0u) { vt = h; done = true; }
+      }
+      if (!done)
+        vt = trace_candidates(s, cslot[t], cmeta[t], ro, rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID,
+                              tile_count);
+    }
+    if (vt.in_grid && vt.best.hit != 0u) {
+      shade_hf = false;
+      HitGeom best = vt.best;
+      if (best.mat == MAT_GRASS) {
+        const int32_t csv = (int32_t)s.cam->chunk_size;
+        const i3 ov{to_i32(floorf(best.root_bmin.x / vs + 0.5f)), to_i32(floorf(best.root_bmin.y / vs + 0.5f)),
+                    to_i32(floorf(best.root_bmin.z / vs + 0.5f))};
+        const v3 hp = ro + rd * best.t;
+        const GrassCell cell = pick_grass_cell_in_chunk_with_bias(hp, rd, best.root_bmin, ov, vs, csv);
+        const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, best.t, cell.bmin_m, cell.id_vox, vs,
+                                               s.cam->voxel_params[1], s.cam->voxel_params[2]);
+        if (gh.hit) { best.t = gh.t; best.n = gh.n; }
+      }
+      const v3 hp = ro + rd * best.t;
+      const v3 hps = hp + best.n * (0.75f * vs);
+      if ((seed & SHADOW_SUBSAMPLE_MASK) == 0u) {
+        float sh = A.shadow_in[pix];
+        const v2 uvp = prev_uv_from_world(s, hp);
+        if (in_unit_square(uvp)) {
+          const int32_t ppx = clampi(to_i32(uvp.x * (float)W), 0, (int32_t)W - 1);
+          const int32_t ppy = clampi(to_i32(uvp.y * (float)H), 0, (int32_t)H - 1);
+          sh = A.shadow_in[(size_t)ppy * W + (uint32_t)ppx];
+        }
+        sh = clampf(sh, 0.0f, 1.0f);
+        const float cur = sun_transmittance_geom_only(s, hps, SUN_DIR);
+        shadow_out = mixf(sh, cur, SHADOW_TAA_ALPHA);
+      } else {
+        shadow_out = clampf(A.shadow_in[pix], 0.0f, 1.0f);
+      }
+      const v3 base_hdr = shade_hit(s, ro, rd, best, sky_up, shadow_out);
+      if (best.hit != 0u && best.mat != MAT_LIGHT && best.t <= LOCAL_LIGHT_MAX_DIST) {
+        const v3 hpl = ro + rd * best.t;
+        const v3 alb = base_albedo(best.mat, hpl, best.t);
+        local_out = gather_voxel_lights(s, hpl, best.n, best.root_bmin) * alb;
+        local_w = 1.0f;
+      }
+      const float t_scene = fmin_(best.t, FOG_MAX_DIST);
+      col = apply_fog(s, base_hdr, ro, rd, t_scene, sky_bg(rd));
+      depth = t_scene;
+      t_store = t_scene;
+      uint32_t pxy = 0u, pz = 0u, ak = 0u;
+      if (vt.anchor_valid) {
+        pxy = pack_i16x2(vt.anchor_chunk.x, vt.anchor_chunk.y);
+        pz = pack_i16x2(vt.anchor_chunk.z, 0) | 0x80000000u;
+        ak = vt.anchor_key;
+      }
+      hist = make_uint4(__float_as_uint(t_store), ak, pxy, pz);
+      rec = make_rec(best, ro, rd, vs, true);
+    }
+  }
+  if (shade_hf) {
+    // Heightfield, then sky (ray_main.wgsl:224-269 / 327-372 / 473-516).
+    ClipHit hf = clip_trace_heightfield(s, ro, rd, 0.0f, FOG_MAX_DIST);
+    if (hf.hit) {
+      if (hf.mat == MAT_GRASS) {
+        const v3 hp = ro + rd * hf.t;
+        const GrassCell cell = grass_cell_from_world_global(hp, rd, vs);
+        const v3 gb = V3(cell.bmin_m.x, hp.y - vs, cell.bmin_m.z);
+        const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, hf.t, gb, cell.id_vox, vs, s.cam->voxel_params[1],
+                                               s.cam->voxel_params[2]);
+        if (gh.hit) { hf.t = gh.t; hf.n = gh.n; }
+      }
+      const v3 surface = shade_clip_hit(s, ro, rd, hf, sky_up);
+      const float t_scene = fmin_(hf.t, FOG_MAX_DIST);
+      col = apply_fog(s, surface, ro, rd, t_scene, sky_bg(rd));
+      depth = t_scene;
+      t_store = t_scene;
+      HitGeom g = miss_hitgeom();
+      g.hit = 1u;
+      g.t = hf.t;
+      g.n = hf.n;
+      g.mat = hf.mat;
+      rec = make_rec(g, ro, rd, vs, false);
+    } else {
+      col = sky_color(s, rd);
+      depth = FOG_MAX_DIST;
+    }
+    hist = make_uint4(__float_as_uint(t_store), 0u, 0u, 0u);
+  }
+  A.color[pix] = make_float4(col.x, col.y, col.z, 1.0f);
+  A.depth[pix] = depth;
+  A.hist_out[pix] = hist;
+  A.shadow_out[pix] = shadow_out;
+  if (A.local) A.local[pix] = make_float4(local_out.x, local_out.y, local_out.z, local_w);
+  if (A.hits) store_rec(A.hits + pix * 2u, rec);
+  // main_local_taa (taa.wgsl:26-69) for this pixel.
+  const float4 h4 = A.local_hist_in[pix];
+  const v3 cur = local_out;
+  const bool hist_ok = !is_bad(xyz(h4));
+  const v3 hl = hist_ok ? xyz(h4) : V3s(0.0f);
+  const float conf0 = hist_ok ? h4.w : 0.0f;
+  const bool has_sample = local_w > 0.0f && !is_bad(cur);
+  const float k = has_sample ? LOCAL_TAA_ALPHA * clampf(local_w, 0.0f, 1.0f) : 0.0f;
+  const v3 ol = vmix(hl, cur, k);
+  const float conf1 = has_sample ? fmin_(1.0f, conf0 + k) : conf0;
+  A.local_hist_out[pix] = make_float4(ol.x, ol.y, ol.z, conf1);
+}
+
+// ---------------------------------------------------------------------------
+// Godray pass
+// ---------------------------------------------------------------------------
+constexpr int POST_THREADS_X = 32, POST_THREADS_Y = 4;
+
+__global__ void __launch_bounds__(POST_THREADS_X* POST_THREADS_Y) k_godray(const __grid_constant__ FrameArgs A) {
+  const uint32_t gx = blockIdx.x * POST_THREADS_X + threadIdx.x;
+  const uint32_t gy = blockIdx.y * POST_THREADS_Y + threadIdx.y;
+  if (gx >= A.iw || gy >= A.ih) return;
+  const Scene s = make_scene(A, true);
+  const uint32_t W = A.iw, H = A.ih;
+  const int32_t Wi = (int32_t)W, Hi = (int32_t)H;
+  const v3 ro = cam_pos(s);
+  const int32_t x = (int32_t)gx, y = (int32_t)gy;
+  const v2 qpx = V2((float)gx, (float)gy);
+  const float fi = (float)(s.cam->frame_index & 1023u);
+  const v2 fj = V2(fi, fi * 1.371f);
+  const float* D = A.depth;
+  const float t_c = D[(size_t)y * W + x];
+  const float t_l = D[(size_t)y * W + clampi(x - 1, 0, Wi - 1)], t_r = D[(size_t)y * W + clampi(x + 1, 0, Wi - 1)];
+  const float t_u = D[(size_t)clampi(y - 1, 0, Hi - 1) * W + x], t_d = D[(size_t)clampi(y + 1, 0, Hi - 1) * W + x];
+  const float dmin = fmin_(t_c, fmin_(fmin_(t_l, t_r), fmin_(t_u, t_d)));
+  const float dmax = fmax_(t_c, fmax_(fmax_(t_l, t_r), fmax_(t_u, t_d)));
+  const float span = (dmax - dmin) / fmax_(dmin, 1e-3f);
+  const float stable = 1.0f - smooth(0.06f, 0.30f, span);
+  const float t_hist = dmin;
+  const float j4 = 0.20f * (hash12(qpx * J0_SCALE + fj) - 0.5f);
+  const float j_phase = hash12(qpx * 0.91f + fj * 0.73f + V2(31.7f, 12.3f)) - 0.5f;
+  const float qstep = 0.03f;
+  const float dq = (hash12(qpx * 1.37f + fj * 1.19f + V2(9.2f, 1.1f)) - 0.5f) * qstep;
+  const v2 j_rd = V2(hash12(qpx + fj + V2(1.7f, 9.2f)) - 0.5f, hash12(qpx + fj * 1.13f + V2(8.3f, 2.1f)) - 0.5f);
+  const float t_end = fmin_(floorf((t_c + dq) / qstep) * qstep, GODRAY_MAX_DIST);
+  const bool fog_ok = fog_density_godray(s) > 0.0f;
+  const v2 pxc = V2((float)gx + 0.5f, (float)gy + 0.5f) + j_rd * 0.35f;
+  const v3 rd = ray_dir_from_pixel(s, pxc);
+  v3 cur = V3s(0.0f);
+  if (fog_ok && t_end > 0.0f) cur = godray_integrate_1(s, ro, rd, t_end, j4, j_phase);
+  const v3 p_ws = ro + rd * t_hist;
+  const v2 uvp = prev_uv_from_world(s, p_ws);
+  v3 hl = cur;
+  float hv = 0.0f;
+  const v2 hdf = V2((float)W, (float)H);
+  const v2 uvc = V2((float)gx + 0.5f, (float)gy + 0.5f) / hdf;
+  if (in_unit_square(uvp)) {
+    const float4 h = A.god_in[(size_t)nearest_idx(uvp.y, H) * W + (uint32_t)nearest_idx(uvp.x, W)];
+    const float hd = h.w;
+    hl = godray_decompress(xyz(h));
+    const float rel = fabsf(hd - t_hist) / fmax_(t_hist, 1e-3f);
+    const float dok = 1.0f - smooth(0.08f, 0.20f, rel);
+    const float dsane = hd > 1e-3f ? 1.0f : 0.0f;
+    const float vel = length((uvp - uvc) * hdf);
+    const float mok = 1.0f - smooth(0.75f, 2.50f, vel);
+    hv = dok * dsane * mok;
+  }
+  const float delta = length(cur - hl);
+  const float energy = fmax_(length(cur), 1e-3f);
+  const float drel = delta / (0.05f + energy);
+  const float react = smooth(0.10f, 0.45f, drel);
+  const float cs = mixf(0.55f, 0.18f, stable);
+  const v3 cw = vmax(cur * cs, V3s(0.015f));
+  const v3 hc = vclamp(hl, cur - cw, cur + cw);
+  const float hwb = mixf(0.25f, 0.92f, stable);
+  const float hw = mixf(hwb, 0.03f, react) * hv;
+  const v3 ol = vmix(cur, hc, hw);
+  const v3 oc = godray_compress(vmax(ol, V3s(0.0f)));
+  A.god_out[(size_t)gy * W + gx] = make_float4(oc.x, oc.y, oc.z, t_hist);
+}
+
+// ---------------------------------------------------------------------------
+// Composite pass (+ fused composite TAA)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(POST_THREADS_X* POST_THREADS_Y) k_composite(const __grid_constant__ FrameArgs A) {
+  const uint32_t gx = blockIdx.x * POST_THREADS_X + threadIdx.x;
+  const uint32_t gy = blockIdx.y * POST_THREADS_Y + threadIdx.y;
+  if (gx >= A.pw || gy >= A.ph) return;
+  const Scene s = make_scene(A, false);
+  const uint32_t RW = A.iw, RH = A.ih, PW = A.pw, PH = A.ph;
+  const v2 pp = V2((float)gx + 0.5f, (float)gy + 0.5f);
+  const v2 rdim = V2((float)s.cam->render_present_px[0], (float)s.cam->render_present_px[1]);
+  const v2 pdim = V2((float)s.cam->render_present_px[2], (float)s.cam->render_present_px[3]);
+  const v2 px_render = (pp / pdim) * rdim;
+  const int32_t ipr_x = clampi(to_i32(floorf(px_render.x)), 0, to_i32(rdim.x) - 1);
+  const int32_t ipr_y = clampi(to_i32(floorf(px_render.y)), 0, to_i32(rdim.y) - 1);
+  const int32_t rwi = (int32_t)RW, rhi = (int32_t)RH;
+  const v2 rdf = V2((float)RW, (float)RH);
+  const int32_t irx = clampi(ipr_x, 0, rwi - 1), iry = clampi(ipr_y, 0, rhi - 1);
+  auto C4 = [&](int32_t xx, int32_t yy) { return A.color[(size_t)yy * RW + (uint32_t)xx]; };
+  auto DEP = [&](int32_t xx, int32_t yy) { return A.depth[(size_t)yy * RW + (uint32_t)xx]; };
+  const v3 base = xyz(C4(irx, iry));
+  const v2 fdf = rdf;
+  const v2 px_full = px_render * (fdf / rdf);
+  const int32_t ifx = clampi(to_i32(floorf(px_full.x)), 0, rwi - 1);
+  const int32_t ify = clampi(to_i32(floorf(px_full.y)), 0, rhi - 1);
+  const v2 uv_full = (px_full + V2(0.5f, 0.5f)) / fdf;
+  const float d0 = DEP(ifx, ify);
+  const v2 gdf = V2((float)RW, (float)RH);
+  const v2 du = V2(1.0f / gdf.x, 0.0f), dv = V2(0.0f, 1.0f / gdf.y);
+  auto G = [&](v2 uv) {
+    const float4 c = A.god_out[(size_t)nearest_idx(uv.y, RH) * RW + (uint32_t)nearest_idx(uv.x, RW)];
+    return godray_decompress(xyz(c));
+  };
+  const v3 gC = G(uv_full), gE = G(uv_full + du), gW = G(uv_full - du), gN = G(uv_full + dv), gS = G(uv_full - dv);
+  const float dE = DEP(min(ifx + 1, rwi - 1), ify), dW = DEP(max(ifx - 1, 0), ify);
+  const float dN = DEP(ifx, min(ify + 1, rhi - 1)), dS = DEP(ifx, max(ify - 1, 0));
+  const float tol = 0.02f + 0.06f * smooth(10.0f, 80.0f, d0);
+  const float wE = 1.0f - smooth(0.0f, tol, fabsf(dE - d0));
+  const float wW = 1.0f - smooth(0.0f, tol, fabsf(dW - d0));
+  const float wN = 1.0f - smooth(0.0f, tol, fabsf(dN - d0));
+  const float wS = 1.0f - smooth(0.0f, tol, fabsf(dS - d0));
+  const float wsum = fmax_(wE + wW + wN + wS, 1e-4f);
+  const v3 blur = (gE * wE + gW * wW + gN * wN + gS * wS) / wsum;
+  v3 god = vmax(gC + (gC - blur) * COMPOSITE_SHARPEN, V3s(0.0f));
+  god = vmax(god - V3s(GODRAY_BLACK_LEVEL), V3s(0.0f));
+  god = god / (god + V3s(GODRAY_KNEE_COMPOSITE));
+  const float god_far = smooth(GODRAY_FADE_NEAR, GODRAY_FADE_FAR, d0);
+  const float god_scale = GODRAY_COMPOSITE_SCALE * mixf(1.0f, 0.25f, god_far);
+  const v3 lum_w = V3(0.2126f, 0.7152f, 0.0722f);
+  const v3 sun_hue = normalize(vmax(SUN_COLOR, V3s(1e-4f)));
+  const float g_lum = fmax_(dot(god, lum_w), 0.0f);
+  const v3 god_sun = sun_hue * g_lum;
+  god = vmix(god, god_sun, 0.55f * god_far);
+  god = god * vmix(V3s(1.0f), V3(1.08f, 1.03f, 0.92f), god_far);
+  v3 hdr = vmax(base + god * god_scale, V3s(0.0f));
+  {
+    const float bt = 1.4f;
+    const float bk = 0.12f * mixf(1.0f, 0.0f, god_far);
+    const v3 b0 = bright_extract_hue(hdr, bt);
+    const v3 hx1 = vmax(xyz(C4(clampi(irx + 2, 0, rwi - 1), iry)), V3s(0.0f));
+    const v3 hx0 = vmax(xyz(C4(clampi(irx - 2, 0, rwi - 1), iry)), V3s(0.0f));
+    const v3 hy1 = vmax(xyz(C4(irx, clampi(iry + 2, 0, rhi - 1))), V3s(0.0f));
+    const v3 hy0 = vmax(xyz(C4(irx, clampi(iry - 2, 0, rhi - 1))), V3s(0.0f));
+    const v3 bloom = (b0 + bright_extract_hue(hx1, bt) + bright_extract_hue(hx0, bt) + bright_extract_hue(hy1, bt) +
+                      bright_extract_hue(hy0, bt)) /
+                     5.0f;
+    const v3 bmx = vmax(hdr, V3s(0.0f)) * 0.35f;
+    hdr = hdr + vmin(bloom, bmx) * bk;
+  }
+  const float l_hdr = fmax_(dot(hdr, lum_w), 1e-6f);
+  const float t_sat = smooth(30.0f, 100.0f, d0);
+  float sat = 1.00f + 0.55f * t_sat;
+  const float hi = smooth(1.6f, 6.0f, l_hdr);
+  sat = mixf(sat, 1.0f, 0.55f * hi);
+  hdr = vmix(V3s(l_hdr), hdr, sat);
+  hdr = hdr * 1.10f;
+  hdr = hdr * V3(1.0f + 0.03f, 1.0f, 1.0f - 0.03f);
+  hdr = (hdr - V3s(0.18f)) * 1.05f + V3s(0.18f);
+  hdr = vmax(hdr, V3s(0.0f));
+  v3 c = tonemap_white(hdr * POST_EXPOSURE, 6.0f);
+  c = vclamp(c, V3s(0.0f), V3s(1.0f));
+  c = V3(powf_(c.x, 0.98f), powf_(c.y, 0.98f), powf_(c.z, 0.98f));
+  const float fi = (float)(s.cam->frame_index & 255u);
+  const float n0 = hash12(px_render + V2(fi, 0.0f)) - 0.5f;
+  const float n1 = hash12(px_render * 0.73f + V2(0.0f, fi)) - 0.5f;
+  const float n = 0.6f * n0 + 0.4f * n1;
+  c = c + V3s(n / 1536.0f);
+  const v3 cc = vclamp(c, V3s(0.0f), V3s(1.0f));
+  const float ge = 1.0f / 2.2f;
+  const v3 ldr = V3(powf_(cc.x, ge), powf_(cc.y, ge), powf_(cc.z, ge));
+  const v2 uv_r = px_render * V2(1.0f / (float)RW, 1.0f / (float)RH);
+  const float4 lh = A.local_hist_out[(size_t)nearest_idx(uv_r.y, RH) * RW + (uint32_t)nearest_idx(uv_r.x, RW)];
+  const v3 fin = ldr + xyz(lh);
+  const size_t opix = (size_t)gy * PW + gx;
+  if (A.pre_taa) A.pre_taa[opix] = make_float4(fin.x, fin.y, fin.z, 1.0f);
+  v3 taa = fin;
+  if (s.cam->frame_index > 1u) {
+    const float dd = DEP(ipr_x, ipr_y);
+    const v3 rdv = ray_dir_from_pixel(s, px_render);
+    const v3 p_ws = cam_pos(s) + rdv * dd;
+    const v2 uvp = prev_uv_from_world(s, p_ws);
+    if (in_unit_square(uvp)) {
+      const float4 h = A.out_hist_in[(size_t)nearest_idx(uvp.y, PH) * PW + (uint32_t)nearest_idx(uvp.x, PW)];
+      taa = vmix(xyz(h), taa, COMPOSITE_TAA_ALPHA);
+    }
+  }
+  const float4 o = make_float4(taa.x, taa.y, taa.z, 1.0f);
+  A.output[opix] = o;
+  A.out_hist_out[opix] = o;
+}
+
+// ---------------------------------------------------------------------------
+// Ray queries
+// ---------------------------------------------------------------------------
+struct QueryArgs {
+  vxe_camera_gpu cam;  // only chunk_size, chunk_count, voxel_params, grid fields are read
+  vxe_clipmap_gpu clip;
+  const uint4* nodes;
+  uint64_t nodes_n;
+  const uint32_t* ropes;
+  uint64_t ropes_n;
+  const uint4* metas;
+  uint64_t metas_n;
+  const uint32_t* grid;
+  uint64_t grid_n;
+  const uint32_t* macro;
+  uint64_t macro_n;
+  const uint32_t* colinfo;
+  uint64_t colinfo_n;
+  uint32_t* err;
+  const float* origins;
+  const float* dirs;
+  uint32_t n;
+  float tmax;
+  uint4* out;  // 2 x uint4 per ray
+};
+
+__device__ __forceinline__ Scene make_query_scene(const QueryArgs& Q) {
+  Scene s;
+  s.cam = &Q.cam;
+  s.clip = &Q.clip;
+  s.nodes = Q.nodes;
+  s.nodes_n = Q.nodes_n;
+  s.ropes = Q.ropes;
+  s.ropes_n = Q.ropes_n;
+  s.metas = Q.metas;
+  s.metas_n = Q.metas_n;
+  s.grid = Q.grid;
+  s.grid_n = Q.grid_n;
+  s.macro = Q.macro;
+  s.macro_n = Q.macro_n;
+  s.colinfo = Q.colinfo;
+  s.colinfo_n = Q.colinfo_n;
+  s.clip_tex = nullptr;
+  s.clip_layers = 0;
+  s.clip_res = 0;
+  s.err = Q.err;
+  return s;
+}
+
+// One ray: chunk DDA front to back, first hit wins (cells are disjoint in t).
+__device__ __forceinline__ HitRec trace_query_ray(const Scene& s, v3 ro, v3 rd, float tmax) {
+  const v3 inv = safe_inv3(rd);
+  HitGeom best = miss_hitgeom();
+  const float vs = vs_(s);
+  const float rs = (float)s.cam->chunk_size * vs;
+  const TraceOpts opt{true};
+  chunk_grid_dda(s, ro, rd, 0.0f, tmax, [&](uint32_t slot, float) -> bool {
+    const Meta ch = meta_at(s, slot);
+    if (ch.macro_empty != 0u) return false;
+    const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vs;
+    const v2 rt = intersect_aabb(ro, rd, rb, rb + V3s(rs));
+    const float ce = fmax_(rt.x, 0.0f), cx = fmin_(rt.y, fmin_(tmax, FOG_MAX_DIST));
+    if (cx < ce) return false;
+    const ChunkTraceResult h = trace_chunk_interval_stream_macro(s, ro, rd, inv, ch, ce, cx, false, INVALID, opt);
+    if (h.hit.hit != 0u) {
+      best = h.hit;
+      return true;
+    }
+    return false;
+  });
+  if (best.hit) return make_rec(best, ro, rd, vs, true);
+  return miss_rec();
+}
+
+constexpr int QUERY_THREADS = 128;
+
+__global__ void __launch_bounds__(QUERY_THREADS) k_query(const __grid_constant__ QueryArgs Q) {
+  const uint32_t i = blockIdx.x * QUERY_THREADS + threadIdx.x;
+  if (i >= Q.n) return;
+  const Scene s = make_query_scene(Q);
+  const v3 ro = V3(Q.origins[3 * i], Q.origins[3 * i + 1], Q.origins[3 * i + 2]);
+  const v3 rd = V3(Q.dirs[3 * i], Q.dirs[3 * i + 1], Q.dirs[3 * i + 2]);
+  store_rec(Q.out + (size_t)i * 2u, trace_query_ray(s, ro, rd, Q.tmax));
+}
+
+}  // namespace dev
+}  // namespace vxe

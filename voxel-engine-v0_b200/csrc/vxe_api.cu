@@ -1,0 +1,645 @@
+// vxe_api.cu -- C ABI of the B200 passes (declared in include/vxe/vxe.h).
+//
+// A vxe_ctx owns every device resource of one renderer instance, like the
+// reference `Renderer` (render/state/mod.rs:34-709):
+//   arenas   nodes (16 B), ropes (32 B), ChunkMeta slots (48 B), macro words,
+//            colinfo words, chunk grid, clipmap layers;
+//   images   internal-size color / depth / histories, present-size output and
+//            output history, per-tile candidate lists;
+//   streams  a compute stream for the passes and an upload stream whose copies
+//            are ordered before the next frame by an event.
+// The ping-pong wiring mirrors Renderer::encode_compute (render/state/mod.rs:
+// 329-446): the primary pass reads hist[ping] and writes hist[pong]; godray
+// reads godray[ping] and writes godray[pong]; composite reads godray[pong] and
+// local_hist[pong]; composite TAA reads out_hist[ping] and writes
+// out_hist[pong]; then ping = pong.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "kernels/frame_kernels.cuh"
+#include "vxe/vxe.h"
+
+using vxe::dev::FrameArgs;
+using vxe::dev::QueryArgs;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+enum Img {
+  IMG_COLOR, IMG_DEPTH, IMG_LOCAL, IMG_HIST0, IMG_HIST1, IMG_SHADOW0, IMG_SHADOW1, IMG_LHIST0, IMG_LHIST1,
+  IMG_GOD0, IMG_GOD1, IMG_PRE_TAA, IMG_OUTPUT, IMG_OHIST0, IMG_OHIST1, IMG_HITS, IMG_TILE_COUNT, IMG_TILE_SLOTS,
+  IMG_N
+};
+
+}  // namespace
+
+struct vxe_ctx {
+  vxe_config cfg{};
+  uint32_t flags = 0;
+  std::string err;
+  int device = 0;
+  cudaStream_t compute = nullptr, upload = nullptr;
+  cudaEvent_t upload_done = nullptr;
+  bool upload_pending = false;
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool timed = false;
+  // arenas
+  DevBuf nodes, ropes, metas, macro, colinfo, grid, clip_tex, errword;
+  // images
+  DevBuf img[IMG_N];
+  uint32_t iw = 0, ih = 0, pw = 0, ph = 0;
+  int ping = 0;
+  vxe_camera_gpu cam{};
+  vxe_clipmap_gpu clip{};
+  // query scratch
+  DevBuf q_in, q_out;
+};
+
+namespace {
+
+vxe_status fail(vxe_ctx* c, vxe_status st, const char* fmt, ...) {
+  if (c) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    c->err = buf;
+  }
+  return st;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return fail(c, e_ == cudaErrorMemoryAllocation ? VXE_ERR_OOM : VXE_ERR_DEVICE, "%s: %s", #call, \
+                  cudaGetErrorString(e_));                                                    \
+  } while (0)
+
+vxe_status alloc(vxe_ctx* c, DevBuf& b, size_t bytes) {
+  if (b.p) {
+    cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+  }
+  if (bytes == 0) return VXE_OK;
+  CK(cudaMalloc(&b.p, bytes));
+  b.bytes = bytes;
+  CK(cudaMemset(b.p, 0, bytes));
+  return VXE_OK;
+}
+
+void release(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+}
+
+size_t img_bytes(const vxe_ctx* c, int i) {
+  const size_t in = (size_t)c->iw * c->ih, pn = (size_t)c->pw * c->ph;
+  const size_t tiles = (size_t)((c->iw + 7) / 8) * ((c->ih + 7) / 8);
+  switch (i) {
+    case IMG_COLOR: case IMG_LOCAL: case IMG_LHIST0: case IMG_LHIST1: case IMG_GOD0: case IMG_GOD1:
+    case IMG_HIST0: case IMG_HIST1:
+      return in * 16;
+    case IMG_DEPTH: case IMG_SHADOW0: case IMG_SHADOW1:
+      return in * 4;
+    case IMG_PRE_TAA: case IMG_OUTPUT: case IMG_OHIST0: case IMG_OHIST1:
+      return pn * 16;
+    case IMG_HITS:
+      return in * 32;
+    case IMG_TILE_COUNT:
+      return tiles * 4;
+    case IMG_TILE_SLOTS:
+      return tiles * 4 * VXE_PRIMARY_MAX_TILE_CHUNKS;
+    default:
+      return 0;
+  }
+}
+
+bool img_enabled(const vxe_ctx* c, int i) {
+  if (i == IMG_LOCAL || i == IMG_PRE_TAA) return (c->flags & VXE_FLAG_DEBUG_INTERMEDIATES) != 0;
+  if (i == IMG_HITS) return (c->flags & VXE_FLAG_HIT_RECORDS) != 0;
+  return true;
+}
+
+vxe_status alloc_images(vxe_ctx* c) {
+  for (int i = 0; i < IMG_N; ++i) {
+    const size_t b = img_enabled(c, i) ? img_bytes(c, i) : 0;
+    if (b != c->img[i].bytes || (b != 0) != (c->img[i].p != nullptr)) {
+      vxe_status st = alloc(c, c->img[i], b);
+      if (st != VXE_OK) return st;
+    } else if (c->img[i].p) {
+      if (cudaMemset(c->img[i].p, 0, b) != cudaSuccess) return fail(c, VXE_ERR_DEVICE, "memset failed");
+    }
+  }
+  c->ping = 0;
+  return VXE_OK;
+}
+
+// Maps the public image id to the buffer index under the current ping.
+int map_image(const vxe_ctx* c, vxe_image im) {
+  const int p = c->ping, q = 1 - c->ping;
+  switch (im) {
+    case VXE_IMG_COLOR: return IMG_COLOR;
+    case VXE_IMG_DEPTH: return IMG_DEPTH;
+    case VXE_IMG_LOCAL: return IMG_LOCAL;
+    case VXE_IMG_PRIMARY_HIST_IN: return IMG_HIST0 + p;
+    case VXE_IMG_PRIMARY_HIST_OUT: return IMG_HIST0 + q;
+    case VXE_IMG_SHADOW_IN: return IMG_SHADOW0 + p;
+    case VXE_IMG_SHADOW_OUT: return IMG_SHADOW0 + q;
+    case VXE_IMG_LOCAL_HIST_IN: return IMG_LHIST0 + p;
+    case VXE_IMG_LOCAL_HIST_OUT: return IMG_LHIST0 + q;
+    case VXE_IMG_GODRAY_IN: return IMG_GOD0 + p;
+    case VXE_IMG_GODRAY_OUT: return IMG_GOD0 + q;
+    case VXE_IMG_OUTPUT_PRE_TAA: return IMG_PRE_TAA;
+    case VXE_IMG_OUTPUT: return IMG_OUTPUT;
+    case VXE_IMG_OUTPUT_HIST_IN: return IMG_OHIST0 + p;
+    case VXE_IMG_OUTPUT_HIST_OUT: return IMG_OHIST0 + q;
+    case VXE_IMG_HITS: return IMG_HITS;
+    default: return -1;
+  }
+}
+
+void fill_scene_args(const vxe_ctx* c, FrameArgs& A) {
+  std::memset(&A, 0, sizeof A);
+  A.cam = c->cam;
+  A.clip = c->clip;
+  A.nodes = (const uint4*)c->nodes.p;
+  A.nodes_n = c->cfg.node_capacity;
+  A.ropes = (const uint32_t*)c->ropes.p;
+  A.ropes_n = c->cfg.node_capacity;
+  A.metas = (const uint4*)c->metas.p;
+  A.metas_n = c->cfg.chunk_capacity;
+  A.grid = (const uint32_t*)c->grid.p;
+  A.grid_n = c->cfg.grid_capacity;
+  A.macro = (const uint32_t*)c->macro.p;
+  A.macro_n = (uint64_t)c->cfg.chunk_capacity * VXE_MACRO_WORDS_PER_CHUNK;
+  A.colinfo = (const uint32_t*)c->colinfo.p;
+  A.colinfo_n = (uint64_t)c->cfg.chunk_capacity * VXE_COLINFO_WORDS_PER_CHUNK;
+  A.clip_tex = (const float*)c->clip_tex.p;
+  A.clip_layers = c->cfg.clip_levels;
+  A.clip_res = c->cfg.clip_res;
+  A.err = (uint32_t*)c->errword.p;
+  A.godray_alias = (c->flags & VXE_FLAG_GODRAY_MACRO_ALIAS) ? 1u : 0u;
+}
+
+vxe_status launch_frame(vxe_ctx* c, bool timed) {
+  if (c->iw == 0 || c->pw == 0) return fail(c, VXE_ERR_INVALID_ARG, "vxe_resize must be called before rendering");
+  if (c->cam.render_present_px[0] != c->iw || c->cam.render_present_px[1] != c->ih ||
+      c->cam.render_present_px[2] != c->pw || c->cam.render_present_px[3] != c->ph)
+    return fail(c, VXE_ERR_INVALID_ARG, "camera render_present_px (%u,%u,%u,%u) does not match images (%u,%u,%u,%u)",
+                c->cam.render_present_px[0], c->cam.render_present_px[1], c->cam.render_present_px[2],
+                c->cam.render_present_px[3], c->iw, c->ih, c->pw, c->ph);
+  if (c->cam.chunk_size != 64u) return fail(c, VXE_ERR_INVALID_ARG, "chunk_size must be 64 (colinfo layout)");
+  if ((uint64_t)c->cam.grid_dims[0] * c->cam.grid_dims[1] * c->cam.grid_dims[2] > c->cfg.grid_capacity)
+    return fail(c, VXE_ERR_CAPACITY, "grid_dims exceed grid capacity");
+  if (c->cam.chunk_count > c->cfg.chunk_capacity) return fail(c, VXE_ERR_CAPACITY, "chunk_count exceeds capacity");
+  if (c->clip.levels > c->cfg.clip_levels && c->clip.levels != 0)
+    return fail(c, VXE_ERR_CAPACITY, "clipmap levels exceed allocated layers");
+  if (c->clip.levels != 0 && c->clip.res != c->cfg.clip_res)
+    return fail(c, VXE_ERR_INVALID_ARG, "clipmap res %u != allocated %u", c->clip.res, c->cfg.clip_res);
+  if (c->upload_pending) {
+    CK(cudaStreamWaitEvent(c->compute, c->upload_done, 0));
+    c->upload_pending = false;
+  }
+  FrameArgs A;
+  fill_scene_args(c, A);
+  const int p = c->ping, q = 1 - c->ping;
+  A.iw = c->iw;
+  A.ih = c->ih;
+  A.pw = c->pw;
+  A.ph = c->ph;
+  A.tile_count = (uint32_t*)c->img[IMG_TILE_COUNT].p;
+  A.tile_slots = (uint32_t*)c->img[IMG_TILE_SLOTS].p;
+  A.hist_in = (const uint4*)c->img[IMG_HIST0 + p].p;
+  A.hist_out = (uint4*)c->img[IMG_HIST0 + q].p;
+  A.shadow_in = (const float*)c->img[IMG_SHADOW0 + p].p;
+  A.shadow_out = (float*)c->img[IMG_SHADOW0 + q].p;
+  A.local_hist_in = (const float4*)c->img[IMG_LHIST0 + p].p;
+  A.local_hist_out = (float4*)c->img[IMG_LHIST0 + q].p;
+  A.color = (float4*)c->img[IMG_COLOR].p;
+  A.depth = (float*)c->img[IMG_DEPTH].p;
+  A.local = (float4*)c->img[IMG_LOCAL].p;
+  A.god_in = (const float4*)c->img[IMG_GOD0 + p].p;
+  A.god_out = (float4*)c->img[IMG_GOD0 + q].p;
+  A.pre_taa = (float4*)c->img[IMG_PRE_TAA].p;
+  A.output = (float4*)c->img[IMG_OUTPUT].p;
+  A.out_hist_in = (const float4*)c->img[IMG_OHIST0 + p].p;
+  A.out_hist_out = (float4*)c->img[IMG_OHIST0 + q].p;
+  A.hits = (uint4*)c->img[IMG_HITS].p;
+  const uint32_t tiles_x = (c->iw + 7) / 8, tiles_y = (c->ih + 7) / 8;
+  const uint32_t tiles = tiles_x * tiles_y;
+  using namespace vxe::dev;
+  if (timed) CK(cudaEventRecord(c->ev[0], c->compute));
+  k_tiles<<<(tiles + TILE_THREADS - 1) / TILE_THREADS, TILE_THREADS, 0, c->compute>>>(A);
+  if (timed) CK(cudaEventRecord(c->ev[1], c->compute));
+  k_primary<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, c->compute>>>(A);
+  if (timed) CK(cudaEventRecord(c->ev[2], c->compute));
+  k_godray<<<dim3((c->iw + POST_THREADS_X - 1) / POST_THREADS_X, (c->ih + POST_THREADS_Y - 1) / POST_THREADS_Y),
+             dim3(POST_THREADS_X, POST_THREADS_Y), 0, c->compute>>>(A);
+  if (timed) CK(cudaEventRecord(c->ev[3], c->compute));
+  k_composite<<<dim3((c->pw + POST_THREADS_X - 1) / POST_THREADS_X, (c->ph + POST_THREADS_Y - 1) / POST_THREADS_Y),
+                dim3(POST_THREADS_X, POST_THREADS_Y), 0, c->compute>>>(A);
+  if (timed) CK(cudaEventRecord(c->ev[4], c->compute));
+  CK(cudaGetLastError());
+  c->timed = timed;
+  c->ping = q;
+  return VXE_OK;
+}
+
+void frame_out(vxe_ctx* c, vxe_frame_out* out) {
+  if (!out) return;
+  out->color = (float*)c->img[IMG_COLOR].p;
+  out->depth = (float*)c->img[IMG_DEPTH].p;
+  out->godray = (float*)c->img[IMG_GOD0 + c->ping].p;  // written this frame (ping already flipped)
+  out->output = (float*)c->img[IMG_OUTPUT].p;
+  out->internal_w = c->iw;
+  out->internal_h = c->ih;
+  out->present_w = c->pw;
+  out->present_h = c->ph;
+}
+
+}  // namespace
+
+extern "C" {
+
+vxe_status vxe_create(const vxe_config* cfg, vxe_ctx** out) {
+  if (!cfg || !out) return VXE_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (cfg->node_capacity == 0 || cfg->chunk_capacity == 0 || cfg->grid_capacity == 0 ||
+      cfg->clip_levels > VXE_CLIP_LEVELS_MAX)
+    return VXE_ERR_INVALID_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device || cfg->device < 0) return VXE_ERR_NO_DEVICE;
+  auto* c = new (std::nothrow) vxe_ctx();
+  if (!c) return VXE_ERR_OOM;
+  c->cfg = *cfg;
+  c->flags = cfg->flags;
+  c->device = cfg->device;
+  vxe_status st = VXE_OK;
+  auto bail = [&](vxe_status s) {
+    vxe_destroy(c);
+    return s;
+  };
+  if (cudaSetDevice(c->device) != cudaSuccess) return bail(VXE_ERR_DEVICE);
+  if (cudaStreamCreateWithFlags(&c->compute, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->upload, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->upload_done, cudaEventDisableTiming) != cudaSuccess)
+    return bail(VXE_ERR_DEVICE);
+  for (auto& e : c->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return bail(VXE_ERR_DEVICE);
+  const uint64_t nc = cfg->node_capacity, cc = cfg->chunk_capacity;
+  if ((st = alloc(c, c->nodes, nc * 16)) != VXE_OK) return bail(st);
+  if ((st = alloc(c, c->ropes, nc * 32)) != VXE_OK) return bail(st);
+  if ((st = alloc(c, c->metas, cc * 48)) != VXE_OK) return bail(st);
+  if ((st = alloc(c, c->macro, cc * VXE_MACRO_WORDS_PER_CHUNK * 4)) != VXE_OK) return bail(st);
+  if ((st = alloc(c, c->colinfo, cc * VXE_COLINFO_WORDS_PER_CHUNK * 4)) != VXE_OK) return bail(st);
+  if ((st = alloc(c, c->grid, (uint64_t)cfg->grid_capacity * 4)) != VXE_OK) return bail(st);
+  if (cudaMemset(c->grid.p, 0xFF, c->grid.bytes) != cudaSuccess) return bail(VXE_ERR_DEVICE);
+  const uint64_t clip_bytes = (uint64_t)cfg->clip_levels * cfg->clip_res * cfg->clip_res * 4;
+  if ((st = alloc(c, c->clip_tex, clip_bytes)) != VXE_OK) return bail(st);
+  if ((st = alloc(c, c->errword, 4)) != VXE_OK) return bail(st);
+  c->cam.chunk_size = 64u;
+  *out = c;
+  return VXE_OK;
+}
+
+void vxe_destroy(vxe_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->compute) cudaStreamSynchronize(c->compute);
+  if (c->upload) cudaStreamSynchronize(c->upload);
+  for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword,
+                  &c->q_in, &c->q_out})
+    release(*b);
+  for (auto& b : c->img) release(b);
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->upload_done) cudaEventDestroy(c->upload_done);
+  if (c->compute) cudaStreamDestroy(c->compute);
+  if (c->upload) cudaStreamDestroy(c->upload);
+  delete c;
+}
+
+const char* vxe_last_error(const vxe_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+uint32_t vxe_get_flags(const vxe_ctx* c) { return c ? c->flags : 0u; }
+
+vxe_status vxe_set_flags(vxe_ctx* c, uint32_t flags) {
+  if (!c) return VXE_ERR_INVALID_ARG;
+  const uint32_t img_bits = VXE_FLAG_DEBUG_INTERMEDIATES | VXE_FLAG_HIT_RECORDS;
+  const bool realloc = ((flags ^ c->flags) & img_bits) != 0;
+  c->flags = flags;
+  if (realloc && c->iw != 0) {
+    cudaSetDevice(c->device);
+    // Only (de)allocate the optional images; histories are kept.
+    for (int i : {IMG_LOCAL, IMG_PRE_TAA, IMG_HITS}) {
+      const size_t b = img_enabled(c, i) ? img_bytes(c, i) : 0;
+      if (b != c->img[i].bytes) {
+        vxe_status st = alloc(c, c->img[i], b);
+        if (st != VXE_OK) return st;
+      }
+    }
+  }
+  return VXE_OK;
+}
+
+vxe_status vxe_resize(vxe_ctx* c, uint32_t present_w, uint32_t present_h, float render_scale) {
+  if (!c || present_w == 0 || present_h == 0 || !(render_scale > 0.0f) || render_scale > 4.0f)
+    return fail(c, VXE_ERR_INVALID_ARG, "bad resize arguments");
+  cudaSetDevice(c->device);
+  CK(cudaStreamSynchronize(c->compute));
+  // internal = round(present * scale).max(1) (render/state/mod.rs:239-241)
+  const float fw = (float)present_w * render_scale, fh = (float)present_h * render_scale;
+  // f32::round rounds half away from zero, like std::round.
+  c->iw = (uint32_t)std::max(1.0f, std::round(fw));
+  c->ih = (uint32_t)std::max(1.0f, std::round(fh));
+  c->pw = present_w;
+  c->ph = present_h;
+  return alloc_images(c);
+}
+
+vxe_status vxe_get_internal_dims(const vxe_ctx* c, uint32_t* w, uint32_t* h) {
+  if (!c || !w || !h) return VXE_ERR_INVALID_ARG;
+  *w = c->iw;
+  *h = c->ih;
+  return VXE_OK;
+}
+
+vxe_status vxe_upload_chunks(vxe_ctx* c, const vxe_chunk_upload* ups, uint32_t n) {
+  if (!c || (n && !ups)) return fail(c, VXE_ERR_INVALID_ARG, "null uploads");
+  cudaSetDevice(c->device);
+  const bool silent = (c->flags & VXE_FLAG_SILENT_CAPACITY_SKIP) != 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const vxe_chunk_upload& u = ups[i];
+    const uint64_t mb = (uint64_t)u.meta.macro_base, cb = (uint64_t)u.meta.colinfo_base;
+    const bool fits = u.slot < c->cfg.chunk_capacity && (uint64_t)u.node_base + u.node_count <= c->cfg.node_capacity &&
+                      mb + VXE_MACRO_WORDS_PER_CHUNK <= (uint64_t)c->cfg.chunk_capacity * VXE_MACRO_WORDS_PER_CHUNK &&
+                      cb + VXE_COLINFO_WORDS_PER_CHUNK <= (uint64_t)c->cfg.chunk_capacity * VXE_COLINFO_WORDS_PER_CHUNK &&
+                      u.meta.node_base == u.node_base;
+    if (!fits) {
+      if (silent) continue;
+      return fail(c, VXE_ERR_CAPACITY, "upload %u (slot %u, node_base %u, count %u) exceeds capacity", i, u.slot,
+                  u.node_base, u.node_count);
+    }
+    if (u.node_count && (!u.nodes || !u.ropes)) return fail(c, VXE_ERR_INVALID_ARG, "upload %u has no node data", i);
+    CK(cudaMemcpyAsync((char*)c->metas.p + (size_t)u.slot * 48, &u.meta, 48, cudaMemcpyHostToDevice, c->upload));
+    if (u.node_count) {
+      CK(cudaMemcpyAsync((char*)c->nodes.p + (size_t)u.node_base * 16, u.nodes, (size_t)u.node_count * 16,
+                         cudaMemcpyHostToDevice, c->upload));
+      CK(cudaMemcpyAsync((char*)c->ropes.p + (size_t)u.node_base * 32, u.ropes, (size_t)u.node_count * 32,
+                         cudaMemcpyHostToDevice, c->upload));
+    }
+    if (u.macro_words)
+      CK(cudaMemcpyAsync((char*)c->macro.p + mb * 4, u.macro_words, VXE_MACRO_WORDS_PER_CHUNK * 4,
+                         cudaMemcpyHostToDevice, c->upload));
+    if (u.colinfo_words)
+      CK(cudaMemcpyAsync((char*)c->colinfo.p + cb * 4, u.colinfo_words, VXE_COLINFO_WORDS_PER_CHUNK * 4,
+                         cudaMemcpyHostToDevice, c->upload));
+  }
+  CK(cudaEventRecord(c->upload_done, c->upload));
+  c->upload_pending = true;
+  return VXE_OK;
+}
+
+vxe_status vxe_write_meta(vxe_ctx* c, uint32_t first, const vxe_chunk_meta* metas, uint32_t n) {
+  if (!c || (n && !metas)) return fail(c, VXE_ERR_INVALID_ARG, "null metas");
+  if ((uint64_t)first + n > c->cfg.chunk_capacity) return fail(c, VXE_ERR_CAPACITY, "meta run exceeds capacity");
+  cudaSetDevice(c->device);
+  if (n) CK(cudaMemcpyAsync((char*)c->metas.p + (size_t)first * 48, metas, (size_t)n * 48, cudaMemcpyHostToDevice, c->upload));
+  CK(cudaEventRecord(c->upload_done, c->upload));
+  c->upload_pending = true;
+  return VXE_OK;
+}
+
+vxe_status vxe_write_grid(vxe_ctx* c, const uint32_t* grid, uint32_t n) {
+  if (!c || (n && !grid)) return fail(c, VXE_ERR_INVALID_ARG, "null grid");
+  if (n > c->cfg.grid_capacity) return fail(c, VXE_ERR_CAPACITY, "grid of %u cells exceeds capacity %u", n, c->cfg.grid_capacity);
+  cudaSetDevice(c->device);
+  if (n) CK(cudaMemcpyAsync(c->grid.p, grid, (size_t)n * 4, cudaMemcpyHostToDevice, c->upload));
+  CK(cudaEventRecord(c->upload_done, c->upload));
+  c->upload_pending = true;
+  return VXE_OK;
+}
+
+vxe_status vxe_write_camera(vxe_ctx* c, const vxe_camera_gpu* cam) {
+  if (!c || !cam) return fail(c, VXE_ERR_INVALID_ARG, "null camera");
+  c->cam = *cam;
+  return VXE_OK;
+}
+
+vxe_status vxe_write_clipmap(vxe_ctx* c, const vxe_clipmap_gpu* params, const vxe_clip_patch* patches, uint32_t n) {
+  if (!c || !params || (n && !patches)) return fail(c, VXE_ERR_INVALID_ARG, "null clipmap arguments");
+  cudaSetDevice(c->device);
+  const uint32_t res = c->cfg.clip_res;
+  for (uint32_t i = 0; i < n; ++i) {
+    const vxe_clip_patch& p = patches[i];
+    if (p.level >= c->cfg.clip_levels || (uint64_t)p.x + p.w > res || (uint64_t)p.y + p.h > res || !p.data)
+      return fail(c, VXE_ERR_CAPACITY, "clip patch %u out of range", i);
+    if (p.w == 0 || p.h == 0) continue;
+    char* dst = (char*)c->clip_tex.p + (((size_t)p.level * res + p.y) * res + p.x) * 4;
+    CK(cudaMemcpy2DAsync(dst, (size_t)res * 4, p.data, (size_t)p.w * 4, (size_t)p.w * 4, p.h, cudaMemcpyHostToDevice,
+                         c->upload));
+  }
+  c->clip = *params;
+  CK(cudaEventRecord(c->upload_done, c->upload));
+  c->upload_pending = true;
+  return VXE_OK;
+}
+
+vxe_status vxe_render_frame_async(vxe_ctx* c, vxe_frame_out* out) {
+  if (!c) return VXE_ERR_INVALID_ARG;
+  cudaSetDevice(c->device);
+  vxe_status st = launch_frame(c, true);
+  if (st != VXE_OK) return st;
+  frame_out(c, out);
+  return VXE_OK;
+}
+
+vxe_status vxe_render_frame(vxe_ctx* c, vxe_frame_out* out) {
+  vxe_status st = vxe_render_frame_async(c, out);
+  if (st != VXE_OK) return st;
+  CK(cudaStreamSynchronize(c->compute));
+  uint32_t word = 0;
+  CK(cudaMemcpy(&word, c->errword.p, 4, cudaMemcpyDeviceToHost));
+  if (word) return fail(c, VXE_ERR_BOUNDS, "device bounds check tripped (error word 0x%x)", word);
+  return VXE_OK;
+}
+
+vxe_status vxe_render_frame_graph(vxe_ctx* c, vxe_frame_out* out) {
+  // Plain launches until the graph path is enabled for this context.
+  return vxe_render_frame(c, out);
+}
+
+vxe_status vxe_synchronize(vxe_ctx* c) {
+  if (!c) return VXE_ERR_INVALID_ARG;
+  cudaSetDevice(c->device);
+  CK(cudaStreamSynchronize(c->compute));
+  CK(cudaStreamSynchronize(c->upload));
+  return VXE_OK;
+}
+
+vxe_status vxe_get_timings(vxe_ctx* c, vxe_timings* t) {
+  if (!c || !t) return VXE_ERR_INVALID_ARG;
+  std::memset(t, 0, sizeof *t);
+  if (!c->timed) return VXE_OK;
+  cudaSetDevice(c->device);
+  CK(cudaEventSynchronize(c->ev[4]));
+  float ms[4];
+  for (int i = 0; i < 4; ++i) CK(cudaEventElapsedTime(&ms[i], c->ev[i], c->ev[i + 1]));
+  t->tiles = ms[0];
+  t->primary = ms[1];
+  t->godray = ms[2];
+  t->composite = ms[3];
+  t->total = (double)ms[0] + ms[1] + ms[2] + ms[3];
+  return VXE_OK;
+}
+
+vxe_status vxe_image_size(const vxe_ctx* c, vxe_image im, size_t* bytes) {
+  if (!c || !bytes) return VXE_ERR_INVALID_ARG;
+  const int i = map_image(c, im);
+  if (i < 0) return VXE_ERR_INVALID_ARG;
+  *bytes = c->img[i].bytes;
+  return VXE_OK;
+}
+
+vxe_status vxe_read_image(vxe_ctx* c, vxe_image im, void* host, size_t bytes) {
+  if (!c || !host) return VXE_ERR_INVALID_ARG;
+  const int i = map_image(c, im);
+  if (i < 0 || !c->img[i].p) return fail(c, VXE_ERR_INVALID_ARG, "image %d not available", (int)im);
+  if (bytes != c->img[i].bytes) return fail(c, VXE_ERR_INVALID_ARG, "image %d is %zu bytes, got %zu", (int)im, c->img[i].bytes, bytes);
+  cudaSetDevice(c->device);
+  CK(cudaStreamSynchronize(c->compute));
+  CK(cudaMemcpy(host, c->img[i].p, bytes, cudaMemcpyDeviceToHost));
+  return VXE_OK;
+}
+
+vxe_status vxe_write_image(vxe_ctx* c, vxe_image im, const void* host, size_t bytes) {
+  if (!c || !host) return VXE_ERR_INVALID_ARG;
+  const int i = map_image(c, im);
+  if (i < 0 || !c->img[i].p) return fail(c, VXE_ERR_INVALID_ARG, "image %d not available", (int)im);
+  if (bytes != c->img[i].bytes) return fail(c, VXE_ERR_INVALID_ARG, "image %d is %zu bytes, got %zu", (int)im, c->img[i].bytes, bytes);
+  cudaSetDevice(c->device);
+  CK(cudaStreamSynchronize(c->compute));
+  CK(cudaMemcpy(c->img[i].p, host, bytes, cudaMemcpyHostToDevice));
+  return VXE_OK;
+}
+
+vxe_status vxe_read_error_word(vxe_ctx* c, uint32_t* word) {
+  if (!c || !word) return VXE_ERR_INVALID_ARG;
+  cudaSetDevice(c->device);
+  CK(cudaStreamSynchronize(c->compute));
+  CK(cudaMemcpy(word, c->errword.p, 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemset(c->errword.p, 0, 4));
+  return VXE_OK;
+}
+
+static void fill_query_args(const vxe_ctx* c, QueryArgs& Q) {
+  std::memset(&Q, 0, sizeof Q);
+  Q.cam = c->cam;
+  Q.clip = c->clip;
+  Q.nodes = (const uint4*)c->nodes.p;
+  Q.nodes_n = c->cfg.node_capacity;
+  Q.ropes = (const uint32_t*)c->ropes.p;
+  Q.ropes_n = c->cfg.node_capacity;
+  Q.metas = (const uint4*)c->metas.p;
+  Q.metas_n = c->cfg.chunk_capacity;
+  Q.grid = (const uint32_t*)c->grid.p;
+  Q.grid_n = c->cfg.grid_capacity;
+  Q.macro = (const uint32_t*)c->macro.p;
+  Q.macro_n = (uint64_t)c->cfg.chunk_capacity * VXE_MACRO_WORDS_PER_CHUNK;
+  Q.colinfo = (const uint32_t*)c->colinfo.p;
+  Q.colinfo_n = (uint64_t)c->cfg.chunk_capacity * VXE_COLINFO_WORDS_PER_CHUNK;
+  Q.err = (uint32_t*)c->errword.p;
+}
+
+vxe_status vxe_trace_rays_device(vxe_ctx* c, const float* d_o, const float* d_d, uint32_t n, float tmax, vxe_hit* d_out) {
+  if (!c || (n && (!d_o || !d_d || !d_out))) return fail(c, VXE_ERR_INVALID_ARG, "null ray buffers");
+  if (n == 0) return VXE_OK;
+  cudaSetDevice(c->device);
+  if (c->upload_pending) {
+    CK(cudaStreamWaitEvent(c->compute, c->upload_done, 0));
+    c->upload_pending = false;
+  }
+  QueryArgs Q;
+  fill_query_args(c, Q);
+  Q.origins = d_o;
+  Q.dirs = d_d;
+  Q.n = n;
+  Q.tmax = tmax;
+  Q.out = (uint4*)d_out;
+  using namespace vxe::dev;
+  k_query<<<(n + QUERY_THREADS - 1) / QUERY_THREADS, QUERY_THREADS, 0, c->compute>>>(Q);
+  CK(cudaGetLastError());
+  return VXE_OK;
+}
+
+vxe_status vxe_trace_rays(vxe_ctx* c, const float* o, const float* d, uint32_t n, float tmax, vxe_hit* out) {
+  if (!c || (n && (!o || !d || !out))) return fail(c, VXE_ERR_INVALID_ARG, "null ray buffers");
+  if (n == 0) return VXE_OK;
+  cudaSetDevice(c->device);
+  const size_t in_bytes = (size_t)n * 24, out_bytes = (size_t)n * sizeof(vxe_hit);
+  vxe_status st;
+  if (c->q_in.bytes < in_bytes && (st = alloc(c, c->q_in, in_bytes)) != VXE_OK) return st;
+  if (c->q_out.bytes < out_bytes && (st = alloc(c, c->q_out, out_bytes)) != VXE_OK) return st;
+  float* din = (float*)c->q_in.p;
+  CK(cudaMemcpyAsync(din, o, (size_t)n * 12, cudaMemcpyHostToDevice, c->compute));
+  CK(cudaMemcpyAsync(din + (size_t)n * 3, d, (size_t)n * 12, cudaMemcpyHostToDevice, c->compute));
+  st = vxe_trace_rays_device(c, din, din + (size_t)n * 3, n, tmax, (vxe_hit*)c->q_out.p);
+  if (st != VXE_OK) return st;
+  CK(cudaMemcpyAsync(out, c->q_out.p, out_bytes, cudaMemcpyDeviceToHost, c->compute));
+  CK(cudaStreamSynchronize(c->compute));
+  return VXE_OK;
+}
+
+}  // extern "C"
+
+namespace {
+__global__ void k_detmath(int which, const float* x, const float* y, float* out, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float r;
+  switch (which) {
+    case 0: r = vxe_sinf(x[i]); break;
+    case 1: r = vxe_cosf(x[i]); break;
+    case 2: r = vxe_expf(x[i]); break;
+    case 3: r = vxe_powf(x[i], y[i]); break;
+    case 4: r = fminf(x[i], y[i]); break;
+    default: r = fmaxf(x[i], y[i]); break;
+  }
+  out[i] = r;
+}
+}  // namespace
+
+extern "C" vxe_status vxe_debug_detmath(int which, const float* x, const float* y, float* out, uint32_t n) {
+  if (!x || !y || !out) return VXE_ERR_INVALID_ARG;
+  if (n == 0) return VXE_OK;
+  float* d = nullptr;
+  if (cudaMalloc(&d, (size_t)n * 12) != cudaSuccess) return VXE_ERR_OOM;
+  vxe_status st = VXE_OK;
+  if (cudaMemcpy(d, x, (size_t)n * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(d + n, y, (size_t)n * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+    st = VXE_ERR_DEVICE;
+  } else {
+    k_detmath<<<(n + 255) / 256, 256>>>(which, d, d + n, d + 2 * (size_t)n, n);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(out, d + 2 * (size_t)n, (size_t)n * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+      st = VXE_ERR_DEVICE;
+  }
+  cudaFree(d);
+  return st;
+}

@@ -1,0 +1,203 @@
+"""ctypes mirror of include/vxe/vxe.h (the C ABI of libvxe.so).
+
+The structs here are byte-identical to the reference's GPU PODs
+(render/gpu_types.rs); ``check_layout`` asserts the sizes the reference
+relies on (NodeGpu 16 B, NodeRopesGpu 32 B, ChunkMetaGpu 48 B, CameraGpu 464 B,
+ClipmapGpu 528 B).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libvxe.so"
+
+VXE_OK = 0
+STATUS_NAMES = {
+    0: "VXE_OK", 1: "VXE_ERR_INVALID_ARG", 2: "VXE_ERR_CAPACITY", 3: "VXE_ERR_OOM", 4: "VXE_ERR_TIMEOUT",
+    5: "VXE_ERR_DEVICE", 6: "VXE_ERR_BOUNDS", 7: "VXE_ERR_NO_DEVICE",
+}
+
+INVALID_U32 = 0xFFFFFFFF
+MACRO_WORDS_PER_CHUNK = 16
+COLINFO_WORDS_PER_CHUNK = 2048
+CHUNK_SIZE = 64
+CLIP_LEVELS_MAX = 16
+
+FLAG_GODRAY_MACRO_ALIAS = 1 << 0
+FLAG_SILENT_CAPACITY_SKIP = 1 << 1
+FLAG_HIT_RECORDS = 1 << 2
+FLAG_DEBUG_INTERMEDIATES = 1 << 3
+FLAG_CHECKED = 1 << 4
+
+(IMG_COLOR, IMG_DEPTH, IMG_LOCAL, IMG_PRIMARY_HIST_IN, IMG_PRIMARY_HIST_OUT, IMG_SHADOW_IN, IMG_SHADOW_OUT,
+ IMG_LOCAL_HIST_IN, IMG_LOCAL_HIST_OUT, IMG_GODRAY_IN, IMG_GODRAY_OUT, IMG_OUTPUT_PRE_TAA, IMG_OUTPUT,
+ IMG_OUTPUT_HIST_IN, IMG_OUTPUT_HIST_OUT, IMG_HITS) = range(16)
+
+NODE_DTYPE = np.dtype([("child_base", "<u4"), ("child_mask", "<u4"), ("material", "<u4"), ("key", "<u4")])
+ROPES_DTYPE = np.dtype([(n, "<u4") for n in ("px", "nx", "py", "ny", "pz", "nz", "_pad0", "_pad1")])
+HIT_DTYPE = np.dtype([("t", "<f4"), ("node", "<u4"), ("voxel", "<i4", (3,)), ("face", "<u4"), ("mat", "<u4"),
+                      ("_pad", "<u4")])
+
+
+class Node(C.Structure):
+    _fields_ = [("child_base", C.c_uint32), ("child_mask", C.c_uint32), ("material", C.c_uint32), ("key", C.c_uint32)]
+
+
+class NodeRopes(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("px", "nx", "py", "ny", "pz", "nz", "_pad0", "_pad1")]
+
+
+class ChunkMeta(C.Structure):
+    _fields_ = [("origin", C.c_int32 * 4), ("node_base", C.c_uint32), ("node_count", C.c_uint32),
+                ("macro_base", C.c_uint32), ("colinfo_base", C.c_uint32), ("macro_empty", C.c_uint32),
+                ("_pad0", C.c_uint32), ("_pad1", C.c_uint32), ("_pad2", C.c_uint32)]
+
+
+Mat4 = (C.c_float * 4) * 4
+
+
+class CameraGpu(C.Structure):
+    _fields_ = [("view_inv", Mat4), ("proj_inv", Mat4), ("view_proj", Mat4), ("prev_view_proj", Mat4),
+                ("cam_pos", C.c_float * 4), ("ray00", C.c_float * 4), ("ray_dx", C.c_float * 4),
+                ("ray_dy", C.c_float * 4), ("chunk_size", C.c_uint32), ("chunk_count", C.c_uint32),
+                ("max_steps", C.c_uint32), ("frame_index", C.c_uint32), ("voxel_params", C.c_float * 4),
+                ("grid_origin_chunk", C.c_int32 * 4), ("grid_dims", C.c_uint32 * 4),
+                ("render_present_px", C.c_uint32 * 4), ("profile_flags", C.c_uint32),
+                ("_pad_profile", C.c_uint32 * 3), ("_pad0", C.c_uint32 * 4), ("_pad1", C.c_uint32 * 4),
+                ("_pad2", C.c_uint32 * 4)]
+
+
+class ClipmapGpu(C.Structure):
+    _fields_ = [("levels", C.c_uint32), ("res", C.c_uint32), ("base_cell_m", C.c_float), ("_pad0", C.c_float),
+                ("level", (C.c_float * 4) * CLIP_LEVELS_MAX), ("offset", (C.c_uint32 * 4) * CLIP_LEVELS_MAX)]
+
+
+class ClipPatch(C.Structure):
+    _fields_ = [("level", C.c_uint32), ("x", C.c_uint32), ("y", C.c_uint32), ("w", C.c_uint32), ("h", C.c_uint32),
+                ("data", C.POINTER(C.c_float))]
+
+
+class ChunkUpload(C.Structure):
+    _fields_ = [("slot", C.c_uint32), ("meta", ChunkMeta), ("node_base", C.c_uint32), ("node_count", C.c_uint32),
+                ("nodes", C.c_void_p), ("ropes", C.c_void_p), ("macro_words", C.c_void_p),
+                ("colinfo_words", C.c_void_p)]
+
+
+class Config(C.Structure):
+    _fields_ = [("node_capacity", C.c_uint32), ("chunk_capacity", C.c_uint32), ("grid_capacity", C.c_uint32),
+                ("clip_levels", C.c_uint32), ("clip_res", C.c_uint32), ("flags", C.c_uint32), ("device", C.c_int32),
+                ("_reserved", C.c_uint32)]
+
+
+class FrameOut(C.Structure):
+    _fields_ = [("color", C.c_void_p), ("depth", C.c_void_p), ("godray", C.c_void_p), ("output", C.c_void_p),
+                ("internal_w", C.c_uint32), ("internal_h", C.c_uint32), ("present_w", C.c_uint32),
+                ("present_h", C.c_uint32)]
+
+
+class Hit(C.Structure):
+    _fields_ = [("t", C.c_float), ("node", C.c_uint32), ("voxel", C.c_int32 * 3), ("face", C.c_uint32),
+                ("mat", C.c_uint32), ("_pad", C.c_uint32)]
+
+
+class Timings(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("primary", "local_taa", "godray", "composite", "composite_taa", "tiles",
+                                           "total")]
+
+
+class WorldParams(C.Structure):
+    _fields_ = [("seed", C.c_uint32), ("height_min", C.c_int32), ("height_max", C.c_int32),
+                ("dirt_depth", C.c_int32), ("carve_mod", C.c_uint32), ("cave_threshold", C.c_float),
+                ("height_scale_vox", C.c_float), ("features", C.c_uint32)]
+
+
+class BuiltChunk(C.Structure):
+    _fields_ = [("nodes", C.POINTER(Node)), ("ropes", C.POINTER(NodeRopes)), ("node_count", C.c_uint32),
+                ("macro_words", C.c_uint32 * MACRO_WORDS_PER_CHUNK),
+                ("colinfo_words", C.c_uint32 * COLINFO_WORDS_PER_CHUNK), ("solid_voxels", C.c_uint32)]
+
+
+class CameraParams(C.Structure):
+    _fields_ = [("pos", C.c_float * 3), ("yaw", C.c_float), ("pitch", C.c_float), ("fovy_rad", C.c_float),
+                ("z_near", C.c_float), ("z_far", C.c_float), ("present_w", C.c_uint32), ("present_h", C.c_uint32),
+                ("internal_w", C.c_uint32), ("internal_h", C.c_uint32), ("frame_index", C.c_uint32),
+                ("jitter", C.c_uint32), ("time_s", C.c_float), ("chunk_count", C.c_uint32),
+                ("grid_origin_chunk", C.c_int32 * 3), ("grid_dims", C.c_uint32 * 3), ("has_prev", C.c_uint32),
+                ("prev_view_proj", Mat4)]
+
+
+# Every symbol include/vxe/vxe.h declares, with (restype, argtypes).
+P = C.POINTER
+SIGNATURES = {
+    "vxe_create": (C.c_int, [P(Config), P(C.c_void_p)]),
+    "vxe_destroy": (None, [C.c_void_p]),
+    "vxe_last_error": (C.c_char_p, [C.c_void_p]),
+    "vxe_get_flags": (C.c_uint32, [C.c_void_p]),
+    "vxe_set_flags": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "vxe_resize": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float]),
+    "vxe_get_internal_dims": (C.c_int, [C.c_void_p, P(C.c_uint32), P(C.c_uint32)]),
+    "vxe_upload_chunks": (C.c_int, [C.c_void_p, P(ChunkUpload), C.c_uint32]),
+    "vxe_write_meta": (C.c_int, [C.c_void_p, C.c_uint32, P(ChunkMeta), C.c_uint32]),
+    "vxe_write_grid": (C.c_int, [C.c_void_p, P(C.c_uint32), C.c_uint32]),
+    "vxe_write_camera": (C.c_int, [C.c_void_p, P(CameraGpu)]),
+    "vxe_write_clipmap": (C.c_int, [C.c_void_p, P(ClipmapGpu), P(ClipPatch), C.c_uint32]),
+    "vxe_render_frame": (C.c_int, [C.c_void_p, P(FrameOut)]),
+    "vxe_render_frame_async": (C.c_int, [C.c_void_p, P(FrameOut)]),
+    "vxe_render_frame_graph": (C.c_int, [C.c_void_p, P(FrameOut)]),
+    "vxe_synchronize": (C.c_int, [C.c_void_p]),
+    "vxe_trace_rays": (C.c_int, [C.c_void_p, P(C.c_float), P(C.c_float), C.c_uint32, C.c_float, C.c_void_p]),
+    "vxe_trace_rays_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_void_p]),
+    "vxe_get_timings": (C.c_int, [C.c_void_p, P(Timings)]),
+    "vxe_image_size": (C.c_int, [C.c_void_p, C.c_int, P(C.c_size_t)]),
+    "vxe_read_image": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
+    "vxe_write_image": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
+    "vxe_read_error_word": (C.c_int, [C.c_void_p, P(C.c_uint32)]),
+    "vxe_debug_detmath": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
+    "vxe_build_chunk": (C.c_int, [P(WorldParams), C.c_int32, C.c_int32, C.c_int32, P(BuiltChunk)]),
+    "vxe_free_chunk": (None, [P(BuiltChunk)]),
+    "vxe_chunk_materials": (C.c_int, [P(WorldParams), C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
+    "vxe_ground_height": (C.c_int32, [P(WorldParams), C.c_int32, C.c_int32]),
+    "vxe_build_from_materials": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, P(BuiltChunk)]),
+    "vxe_build_camera": (C.c_int, [P(CameraParams), P(CameraGpu)]),
+    "vxe_clipmap_new": (C.c_void_p, [P(WorldParams), C.c_uint32, C.c_uint32, C.c_float]),
+    "vxe_clipmap_free": (None, [C.c_void_p]),
+    "vxe_clipmap_update": (C.c_int, [C.c_void_p, C.c_float, C.c_float, P(ClipmapGpu), P(P(ClipPatch)),
+                                     P(C.c_uint32)]),
+}
+
+
+class VxeError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str = ""):
+        self.status = status
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)}" + (f" ({msg})" if msg else ""))
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libvxe.so.  There is no fallback: a missing library is an error."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise FileNotFoundError(f"{LIB_PATH} is missing; run `python voxel-engine-v0_b200/vxe_build.py` first")
+        l = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(l, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = l
+    return _lib
+
+
+def check_layout() -> None:
+    sizes = {Node: 16, NodeRopes: 32, ChunkMeta: 48, CameraGpu: 464, ClipmapGpu: 528, Hit: 32}
+    for t, n in sizes.items():
+        assert C.sizeof(t) == n, f"{t.__name__} is {C.sizeof(t)} bytes, expected {n}"
+    assert NODE_DTYPE.itemsize == 16 and ROPES_DTYPE.itemsize == 32 and HIT_DTYPE.itemsize == 32
+
+
+check_layout()

@@ -1,0 +1,168 @@
+"""Host-side mirror of the reference ``Renderer`` (render/state/mod.rs:34-709).
+
+Same method set and argument meaning as the Rust renderer, forwarding to the
+C ABI of libvxe.so (include/vxe/vxe.h).  Every call raises ``VxeError`` on a
+non-OK status; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi as A
+from .world import Upload, World
+
+
+class Renderer:
+    def __init__(self, width: int, height: int, render_scale: float = 0.5, *, node_capacity: int,
+                 chunk_capacity: int, grid_capacity: int, clip_levels: int = 16, clip_res: int = 256,
+                 flags: int = A.FLAG_GODRAY_MACRO_ALIAS, device: int = 0):
+        self._lib = A.lib()
+        cfg = A.Config(node_capacity, chunk_capacity, grid_capacity, clip_levels, clip_res, flags, device, 0)
+        h = C.c_void_p()
+        st = self._lib.vxe_create(C.byref(cfg), C.byref(h))
+        if st != A.VXE_OK:
+            raise A.VxeError(st, "vxe_create")
+        self._ctx = h
+        self.render_scale = render_scale
+        self.resize_output(width, height)
+
+    # -- lifecycle --------------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_ctx", None):
+            self._lib.vxe_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int, where: str) -> None:
+        if st != A.VXE_OK:
+            msg = self._lib.vxe_last_error(self._ctx)
+            raise A.VxeError(st, where, msg.decode() if msg else "")
+
+    @property
+    def flags(self) -> int:
+        return int(self._lib.vxe_get_flags(self._ctx))
+
+    def set_flags(self, flags: int) -> None:
+        self._check(self._lib.vxe_set_flags(self._ctx, flags), "vxe_set_flags")
+
+    def resize_output(self, width: int, height: int) -> None:
+        self._check(self._lib.vxe_resize(self._ctx, width, height, self.render_scale), "vxe_resize")
+        self.present = (width, height)
+        w, h = C.c_uint32(), C.c_uint32()
+        self._check(self._lib.vxe_get_internal_dims(self._ctx, C.byref(w), C.byref(h)), "vxe_get_internal_dims")
+        self.internal = (w.value, h.value)
+
+    def internal_dims(self):
+        return self.internal
+
+    # -- uploads ----------------------------------------------------------------
+    def apply_chunk_uploads(self, uploads: list[Upload]) -> None:
+        if not uploads:
+            return
+        arr = (A.ChunkUpload * len(uploads))()
+        keep = []
+        for i, u in enumerate(uploads):
+            d = arr[i]
+            d.slot = u.slot
+            C.memmove(C.byref(d.meta), u.meta.ctypes.data, 48)
+            d.node_base = u.node_base
+            if u.data is not None:
+                nodes = np.ascontiguousarray(u.data.nodes)
+                ropes = np.ascontiguousarray(u.data.ropes)
+                macro = np.ascontiguousarray(u.data.macro, dtype=np.uint32)
+                colinfo = np.ascontiguousarray(u.data.colinfo, dtype=np.uint32)
+                keep += [nodes, ropes, macro, colinfo]
+                d.node_count = len(nodes)
+                d.nodes, d.ropes = nodes.ctypes.data, ropes.ctypes.data
+                d.macro_words, d.colinfo_words = macro.ctypes.data, colinfo.ctypes.data
+        self._check(self._lib.vxe_upload_chunks(self._ctx, arr, len(uploads)), "vxe_upload_chunks")
+
+    def upload_world(self, world: World, uploads: list[Upload]) -> None:
+        self.apply_chunk_uploads(uploads)
+        self.write_chunk_grid(world.grid)
+
+    def write_chunk_grid(self, grid: np.ndarray) -> None:
+        g = np.ascontiguousarray(grid, dtype=np.uint32)
+        self._check(self._lib.vxe_write_grid(self._ctx, g.ctypes.data_as(C.POINTER(C.c_uint32)), g.size),
+                    "vxe_write_grid")
+
+    def write_camera(self, cam: A.CameraGpu) -> None:
+        self._check(self._lib.vxe_write_camera(self._ctx, C.byref(cam)), "vxe_write_camera")
+
+    def write_clipmap_updates(self, params: A.ClipmapGpu, patches) -> None:
+        arr = (A.ClipPatch * max(1, len(patches)))()
+        keep = []
+        for i, (lvl, x, y, w, h, data) in enumerate(patches):
+            d = np.ascontiguousarray(data, dtype=np.float32)
+            keep.append(d)
+            arr[i] = A.ClipPatch(lvl, x, y, w, h, d.ctypes.data_as(C.POINTER(C.c_float)))
+        self._check(self._lib.vxe_write_clipmap(self._ctx, C.byref(params), arr, len(patches)), "vxe_write_clipmap")
+
+    # -- frame ------------------------------------------------------------------
+    def encode_compute(self, sync: bool = True) -> A.FrameOut:
+        out = A.FrameOut()
+        fn = self._lib.vxe_render_frame if sync else self._lib.vxe_render_frame_async
+        self._check(fn(self._ctx, C.byref(out)), "vxe_render_frame")
+        return out
+
+    def render_frame_graph(self) -> A.FrameOut:
+        out = A.FrameOut()
+        self._check(self._lib.vxe_render_frame_graph(self._ctx, C.byref(out)), "vxe_render_frame_graph")
+        return out
+
+    def synchronize(self) -> None:
+        self._check(self._lib.vxe_synchronize(self._ctx), "vxe_synchronize")
+
+    def read_gpu_timings_ms_blocking(self) -> dict:
+        t = A.Timings()
+        self._check(self._lib.vxe_get_timings(self._ctx, C.byref(t)), "vxe_get_timings")
+        return {k: getattr(t, k) for k, _ in A.Timings._fields_}
+
+    def read_error_word(self) -> int:
+        w = C.c_uint32()
+        self._check(self._lib.vxe_read_error_word(self._ctx, C.byref(w)), "vxe_read_error_word")
+        return w.value
+
+    # -- images -----------------------------------------------------------------
+    _IMG_SHAPES = {
+        A.IMG_COLOR: ("i", 4, np.float32), A.IMG_DEPTH: ("i", 1, np.float32), A.IMG_LOCAL: ("i", 4, np.float32),
+        A.IMG_PRIMARY_HIST_IN: ("i", 4, np.uint32), A.IMG_PRIMARY_HIST_OUT: ("i", 4, np.uint32),
+        A.IMG_SHADOW_IN: ("i", 1, np.float32), A.IMG_SHADOW_OUT: ("i", 1, np.float32),
+        A.IMG_LOCAL_HIST_IN: ("i", 4, np.float32), A.IMG_LOCAL_HIST_OUT: ("i", 4, np.float32),
+        A.IMG_GODRAY_IN: ("i", 4, np.float32), A.IMG_GODRAY_OUT: ("i", 4, np.float32),
+        A.IMG_OUTPUT_PRE_TAA: ("p", 4, np.float32), A.IMG_OUTPUT: ("p", 4, np.float32),
+        A.IMG_OUTPUT_HIST_IN: ("p", 4, np.float32), A.IMG_OUTPUT_HIST_OUT: ("p", 4, np.float32),
+    }
+
+    def read_image(self, img: int) -> np.ndarray:
+        if img == A.IMG_HITS:
+            w, h = self.internal
+            arr = np.zeros(w * h, dtype=A.HIT_DTYPE)
+        else:
+            which, ch, dt = self._IMG_SHAPES[img]
+            w, h = self.internal if which == "i" else self.present
+            arr = np.zeros((h, w, ch) if ch > 1 else (h, w), dtype=dt)
+        self._check(self._lib.vxe_read_image(self._ctx, img, arr.ctypes.data, arr.nbytes), "vxe_read_image")
+        return arr
+
+    def write_image(self, img: int, arr: np.ndarray) -> None:
+        a = np.ascontiguousarray(arr)
+        self._check(self._lib.vxe_write_image(self._ctx, img, a.ctypes.data, a.nbytes), "vxe_write_image")
+
+    # -- queries ----------------------------------------------------------------
+    def trace_rays(self, origins: np.ndarray, dirs: np.ndarray, tmax: float) -> np.ndarray:
+        o = np.ascontiguousarray(origins, dtype=np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(dirs, dtype=np.float32).reshape(-1, 3)
+        assert o.shape == d.shape
+        out = np.zeros(len(o), dtype=A.HIT_DTYPE)
+        fp = C.POINTER(C.c_float)
+        self._check(self._lib.vxe_trace_rays(self._ctx, o.ctypes.data_as(fp), d.ctypes.data_as(fp), len(o),
+                                             float(tmax), out.ctypes.data), "vxe_trace_rays")
+        return out

@@ -1,0 +1,330 @@
+"""Resident world bookkeeping: chunk builds, slots, node arena, chunk grid.
+
+Mirrors the parts of the reference streaming manager that define the data the
+passes read:
+  * slots are dense in [0, chunk_count) and an unloaded slot is filled by
+    moving the last slot into the hole (streaming/manager/slots.rs:163-766),
+  * ChunkMetaGpu packing: origin = key * 64, macro_base = slot * 16,
+    colinfo_base = slot * 2048, macro_empty = all macro words zero
+    (slots.rs:231-250),
+  * chunk grid index (iz * ny + iy) * nx + ix, INVALID for empty cells
+    (streaming/manager/grid.rs:15-72).
+The node arena is a first-fit free list over [0, node_capacity) (the
+reference's best-fit NodeArena, streaming/node_arena.rs:30-81, is out of the
+hot path).  Host mirrors of every device buffer are kept so a CPU checker can
+read exactly what the device reads.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi as A
+
+
+@dataclass
+class WorldSpec:
+    seed: int = 12345
+    height_min: int = 8
+    height_max: int = 48
+    dirt_depth: int = 3
+    carve_mod: int = 0          # 50 => 2 % of solid voxels carved
+    cave_threshold: float = 2.0  # >= 1 disables caves
+    height_scale_vox: float = 64.0
+    features: int = 0           # bit0 trees, bit1 light voxels
+
+    def params(self) -> A.WorldParams:
+        return A.WorldParams(self.seed, self.height_min, self.height_max, self.dirt_depth, self.carve_mod,
+                             self.cave_threshold, self.height_scale_vox, self.features)
+
+
+@dataclass
+class ChunkData:
+    key: tuple
+    nodes: np.ndarray      # NODE_DTYPE
+    ropes: np.ndarray      # ROPES_DTYPE
+    macro: np.ndarray      # (16,) u32
+    colinfo: np.ndarray    # (2048,) u32
+    solid_voxels: int = 0
+
+    @property
+    def macro_empty(self) -> int:
+        return int(not self.macro.any())
+
+
+def build_chunk(spec: WorldSpec, cx: int, cy: int, cz: int) -> ChunkData:
+    """Runs the C++ port of the reference chunk builder (svo/builder.rs:846-986)."""
+    lib = A.lib()
+    wp = spec.params()
+    out = A.BuiltChunk()
+    st = lib.vxe_build_chunk(C.byref(wp), cx, cy, cz, C.byref(out))
+    if st != A.VXE_OK:
+        raise A.VxeError(st, "vxe_build_chunk")
+    try:
+        n = out.node_count
+        nodes = np.ctypeslib.as_array(C.cast(out.nodes, C.POINTER(C.c_uint32)), shape=(n * 4,)).copy().view(A.NODE_DTYPE)
+        ropes = np.ctypeslib.as_array(C.cast(out.ropes, C.POINTER(C.c_uint32)), shape=(n * 8,)).copy().view(A.ROPES_DTYPE)
+        macro = np.array(out.macro_words, dtype=np.uint32)
+        colinfo = np.array(out.colinfo_words, dtype=np.uint32)
+        return ChunkData((cx, cy, cz), nodes, ropes, macro, colinfo, out.solid_voxels)
+    finally:
+        lib.vxe_free_chunk(C.byref(out))
+
+
+def chunk_materials(spec: WorldSpec, cx: int, cy: int, cz: int) -> np.ndarray:
+    m = np.zeros(64 * 64 * 64, dtype=np.uint8)
+    st = A.lib().vxe_chunk_materials(C.byref(spec.params()), cx, cy, cz, m.ctypes.data)
+    if st != A.VXE_OK:
+        raise A.VxeError(st, "vxe_chunk_materials")
+    return m.reshape(64, 64, 64)  # [y, z, x]
+
+
+def ground_height(spec: WorldSpec, wx: int, wz: int) -> int:
+    return int(A.lib().vxe_ground_height(C.byref(spec.params()), wx, wz))
+
+
+class NodeArena:
+    """First-fit free-list allocator over node indices."""
+
+    def __init__(self, capacity: int):
+        self.capacity = capacity
+        self.free = [(0, capacity)]  # sorted (start, length)
+
+    def alloc(self, n: int):
+        for i, (s, l) in enumerate(self.free):
+            if l >= n:
+                if l == n:
+                    self.free.pop(i)
+                else:
+                    self.free[i] = (s + n, l - n)
+                return s
+        return None
+
+    def release(self, start: int, n: int) -> None:
+        self.free.append((start, n))
+        self.free.sort()
+        merged = []
+        for s, l in self.free:
+            if merged and merged[-1][0] + merged[-1][1] == s:
+                merged[-1] = (merged[-1][0], merged[-1][1] + l)
+            else:
+                merged.append((s, l))
+        self.free = merged
+
+
+@dataclass
+class Upload:
+    slot: int
+    meta: np.ndarray   # (12,) u32 view of one ChunkMetaGpu
+    node_base: int
+    data: ChunkData | None  # None => meta-only rewrite (slot move without new data)
+
+
+class World:
+    """A resident grid of chunks around ``grid_origin`` with host mirrors."""
+
+    def __init__(self, spec: WorldSpec, grid_origin, grid_dims, node_capacity: int, chunk_capacity: int | None = None,
+                 builder=None):
+        self.spec = spec
+        self.grid_origin = tuple(int(v) for v in grid_origin)
+        self.grid_dims = tuple(int(v) for v in grid_dims)
+        nx, ny, nz = self.grid_dims
+        self.chunk_capacity = chunk_capacity or nx * ny * nz
+        self.grid_capacity = nx * ny * nz
+        self.arena = NodeArena(node_capacity)
+        self.node_capacity = node_capacity
+        self.nodes = np.zeros(node_capacity, dtype=A.NODE_DTYPE)
+        self.ropes = np.zeros(node_capacity, dtype=A.ROPES_DTYPE)
+        self.metas = np.zeros((self.chunk_capacity, 12), dtype=np.uint32)
+        self.macro = np.zeros(self.chunk_capacity * A.MACRO_WORDS_PER_CHUNK, dtype=np.uint32)
+        self.colinfo = np.zeros(self.chunk_capacity * A.COLINFO_WORDS_PER_CHUNK, dtype=np.uint32)
+        self.grid = np.full(self.grid_capacity, A.INVALID_U32, dtype=np.uint32)
+        self.slot_to_key: list[tuple] = []
+        self.key_to_slot: dict[tuple, int] = {}
+        self.alloc: dict[tuple, tuple] = {}  # key -> (node_base, node_count)
+        self.cache: dict[tuple, ChunkData] = {}
+        self.builder = builder or (lambda key: build_chunk(self.spec, *key))
+
+    # -- data -----------------------------------------------------------------
+    def chunk(self, key) -> ChunkData:
+        if key not in self.cache:
+            self.cache[key] = self.builder(key)
+        return self.cache[key]
+
+    @property
+    def chunk_count(self) -> int:
+        return len(self.slot_to_key)
+
+    def keys_in_grid(self):
+        ox, oy, oz = self.grid_origin
+        nx, ny, nz = self.grid_dims
+        for iz in range(nz):
+            for iy in range(ny):
+                for ix in range(nx):
+                    yield (ox + ix, oy + iy, oz + iz)
+
+    def _meta_for(self, slot: int, key, node_base: int, data: ChunkData) -> np.ndarray:
+        m = np.zeros(12, dtype=np.uint32)
+        org = np.array([key[0] * 64, key[1] * 64, key[2] * 64, 0], dtype=np.int32)
+        m[0:4] = org.view(np.uint32)
+        m[4] = node_base
+        m[5] = len(data.nodes)
+        m[6] = slot * A.MACRO_WORDS_PER_CHUNK
+        m[7] = slot * A.COLINFO_WORDS_PER_CHUNK
+        m[8] = data.macro_empty
+        return m
+
+    def _write_slot(self, slot: int, key, node_base: int, data: ChunkData) -> np.ndarray:
+        n = len(data.nodes)
+        self.nodes[node_base:node_base + n] = data.nodes
+        self.ropes[node_base:node_base + n] = data.ropes
+        self.macro[slot * 16:(slot + 1) * 16] = data.macro
+        self.colinfo[slot * 2048:(slot + 1) * 2048] = data.colinfo
+        meta = self._meta_for(slot, key, node_base, data)
+        self.metas[slot] = meta
+        return meta
+
+    def add(self, key) -> Upload:
+        """try_make_uploading (slots.rs:163-275): arena alloc + next dense slot."""
+        data = self.chunk(key)
+        n = len(data.nodes)
+        base = self.arena.alloc(n)
+        if base is None:
+            raise MemoryError(f"node arena full adding chunk {key} ({n} nodes)")
+        slot = len(self.slot_to_key)
+        if slot >= self.chunk_capacity:
+            raise MemoryError("chunk slots exhausted")
+        self.slot_to_key.append(key)
+        self.key_to_slot[key] = slot
+        self.alloc[key] = (base, n)
+        meta = self._write_slot(slot, key, base, data)
+        return Upload(slot, meta, base, data)
+
+    def remove(self, key) -> list[Upload]:
+        """Unload: free arena, move the last slot into the hole (keeps slots dense)."""
+        slot = self.key_to_slot.pop(key)
+        base, n = self.alloc.pop(key)
+        self.arena.release(base, n)
+        last = len(self.slot_to_key) - 1
+        ups = []
+        if slot != last:
+            mkey = self.slot_to_key[last]
+            self.slot_to_key[slot] = mkey
+            self.key_to_slot[mkey] = slot
+            mbase, _ = self.alloc[mkey]
+            data = self.chunk(mkey)
+            # macro / colinfo live at slot-derived bases, so they move with the slot.
+            meta = self._write_slot(slot, mkey, mbase, data)
+            ups.append(Upload(slot, meta, mbase, data))
+        self.slot_to_key.pop()
+        self.metas[last] = 0
+        return ups
+
+    def rebuild_grid(self) -> np.ndarray:
+        ox, oy, oz = self.grid_origin
+        nx, ny, nz = self.grid_dims
+        self.grid[:] = A.INVALID_U32
+        for slot, (cx, cy, cz) in enumerate(self.slot_to_key):
+            ix, iy, iz = cx - ox, cy - oy, cz - oz
+            if 0 <= ix < nx and 0 <= iy < ny and 0 <= iz < nz:
+                self.grid[(iz * ny + iy) * nx + ix] = slot
+        return self.grid
+
+    def populate(self) -> list[Upload]:
+        ups = [self.add(k) for k in self.keys_in_grid() if k not in self.key_to_slot]
+        self.rebuild_grid()
+        return ups
+
+    def shift(self, dx: int, dy: int, dz: int) -> list[Upload]:
+        """Moves the grid origin; unloads chunks that left and loads new ones."""
+        self.grid_origin = (self.grid_origin[0] + dx, self.grid_origin[1] + dy, self.grid_origin[2] + dz)
+        want = set(self.keys_in_grid())
+        ups: list[Upload] = []
+        for k in [k for k in self.slot_to_key if k not in want]:
+            ups.extend(self.remove(k))
+        for k in self.keys_in_grid():
+            if k not in self.key_to_slot:
+                ups.append(self.add(k))
+        self.rebuild_grid()
+        # collapse to the last write per slot
+        last = {}
+        for u in ups:
+            last[u.slot] = u
+        return [last[s] for s in sorted(last)]
+
+    @property
+    def nodes_used(self) -> int:
+        return sum(n for _, n in self.alloc.values())
+
+    def world_aabb_m(self):
+        ox, oy, oz = self.grid_origin
+        nx, ny, nz = self.grid_dims
+        lo = np.array([ox, oy, oz], dtype=np.float64) * 6.4
+        return lo, lo + np.array([nx, ny, nz], dtype=np.float64) * 6.4
+
+
+class Clipmap:
+    """Toroidal clipmap state (C++ port of clipmap.rs:182-577)."""
+
+    def __init__(self, spec: WorldSpec, levels: int, res: int = 256, base_cell_m: float = 1.0):
+        self.levels, self.res = levels, res
+        self._h = A.lib().vxe_clipmap_new(C.byref(spec.params()), levels, res, base_cell_m)
+        if not self._h:
+            raise A.VxeError(A.STATUS_NAMES and 1, "vxe_clipmap_new")
+        self.tex = np.zeros((levels, res, res), dtype=np.float32)  # host mirror of the layers
+        self.params = A.ClipmapGpu()
+
+    def update(self, cam_x: float, cam_z: float):
+        """Returns (params, [(level, x, y, w, h, data)]) and applies them to the host mirror."""
+        params = A.ClipmapGpu()
+        pp = C.POINTER(A.ClipPatch)()
+        n = C.c_uint32()
+        st = A.lib().vxe_clipmap_update(self._h, cam_x, cam_z, C.byref(params), C.byref(pp), C.byref(n))
+        if st != A.VXE_OK:
+            raise A.VxeError(st, "vxe_clipmap_update")
+        patches = []
+        for i in range(n.value):
+            p = pp[i]
+            data = np.ctypeslib.as_array(p.data, shape=(p.h * p.w,)).copy().reshape(p.h, p.w)
+            self.tex[p.level, p.y:p.y + p.h, p.x:p.x + p.w] = data
+            patches.append((p.level, p.x, p.y, p.w, p.h, data))
+        self.params = params
+        return params, patches
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                A.lib().vxe_clipmap_free(h)
+            except Exception:
+                pass
+            self._h = None
+
+
+def build_camera(pos, yaw, pitch, present, internal, frame_index, time_s, world: World | None = None,
+                 jitter=True, prev_view_proj=None, fovy_deg: float = 60.0) -> A.CameraGpu:
+    """CameraGpu packing (app/app.rs:411-511)."""
+    p = A.CameraParams()
+    p.pos[:] = [float(v) for v in pos]
+    p.yaw, p.pitch = float(yaw), float(pitch)
+    p.fovy_rad = float(np.deg2rad(fovy_deg))
+    p.z_near, p.z_far = 0.1, 1000.0
+    p.present_w, p.present_h = present
+    p.internal_w, p.internal_h = internal
+    p.frame_index = frame_index
+    p.jitter = 1 if jitter else 0
+    p.time_s = float(time_s)
+    if world is not None:
+        p.chunk_count = world.chunk_count
+        p.grid_origin_chunk[:] = list(world.grid_origin)
+        p.grid_dims[:] = list(world.grid_dims)
+    if prev_view_proj is not None:
+        p.has_prev = 1
+        C.memmove(C.byref(p.prev_view_proj), C.byref(prev_view_proj), C.sizeof(A.Mat4))
+    cam = A.CameraGpu()
+    st = A.lib().vxe_build_camera(C.byref(p), C.byref(cam))
+    if st != A.VXE_OK:
+        raise A.VxeError(st, "vxe_build_camera")
+    return cam

@@ -1,0 +1,110 @@
+"""Builds the in-tree shared libraries.
+
+* ``vxe/libvxe.so`` -- the product: sm_100a CUDA passes + C ABI + C++
+  producers, compiled with ``-fmad=false -prec-div=true -prec-sqrt=true`` so
+  every float operation is a single IEEE binary32 op.
+* ``oracle/liboracle_vxe.so`` -- the CPU restatement used by tests and the
+  CPU baseline (``-ffp-contract=off``, no fast math).
+
+Both are rebuilt only when a source is newer than the library.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+REPO = PKG.parent
+INCLUDE = REPO / "include"
+CSRC = PKG / "csrc"
+LIB = PKG / "vxe" / "libvxe.so"
+ORACLE_SRC = REPO / "oracle" / "vxe_oracle.cpp"
+ORACLE_LIB = REPO / "oracle" / "liboracle_vxe.so"
+BUILD_DIR = PKG / "_build"
+
+ARCH = "-gencode=arch=compute_100a,code=sm_100a"
+NVCC_FLAGS = [
+    "-O3", "-std=c++17", ARCH, "-lineinfo",
+    "-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+    f"-I{INCLUDE}", f"-I{CSRC}",
+]
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall", f"-I{INCLUDE}"]
+
+
+def _nvcc() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(cand).exists():
+        raise RuntimeError("nvcc not found; the CUDA toolkit is required to build libvxe.so")
+    return cand
+
+
+def _sources():
+    cu = sorted(CSRC.glob("*.cu"))
+    cpp = sorted((CSRC / "host").glob("*.cpp"))
+    headers = sorted(CSRC.rglob("*.cuh")) + sorted(INCLUDE.rglob("*.h"))
+    return cu, cpp, headers
+
+
+def _stale(target: Path, deps) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(Path(d).stat().st_mtime > t for d in deps)
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(str(c) for c in cmd), flush=True)
+    r = subprocess.run([str(c) for c in cmd], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"build step failed ({r.returncode}):\n{' '.join(map(str, cmd))}\n{r.stdout}\n{r.stderr}")
+    return r
+
+
+def build_lib(verbose: bool = False, force: bool = False, ptxas_verbose: bool = False) -> Path:
+    cu, cpp, headers = _sources()
+    if not force and not _stale(LIB, cu + cpp + headers + [Path(__file__)]):
+        return LIB
+    BUILD_DIR.mkdir(exist_ok=True)
+    nvcc = _nvcc()
+    objs = []
+    for src in cu:
+        obj = BUILD_DIR / (src.stem + ".o")
+        extra = ["-Xptxas", "-v"] if ptxas_verbose else []
+        r = _run([nvcc, *NVCC_FLAGS, *extra, "-c", src, "-o", obj], verbose)
+        if ptxas_verbose:
+            print(r.stderr)
+        objs.append(obj)
+    for src in cpp:
+        obj = BUILD_DIR / (src.stem + ".o")
+        _run(["g++", *CXX_FLAGS, "-c", src, "-o", obj], verbose)
+        objs.append(obj)
+    tmp = LIB.with_suffix(".so.tmp")
+    _run([nvcc, ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs], verbose)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+def build_oracle(verbose: bool = False, force: bool = False) -> Path:
+    deps = [ORACLE_SRC, INCLUDE / "vxe" / "detmath.h", INCLUDE / "vxe" / "vxe.h"]
+    if not force and not _stale(ORACLE_LIB, deps):
+        return ORACLE_LIB
+    tmp = ORACLE_LIB.with_suffix(".so.tmp")
+    _run(["g++", *CXX_FLAGS, "-shared", "-o", tmp, ORACLE_SRC, "-lpthread"], verbose)
+    os.replace(tmp, ORACLE_LIB)
+    return ORACLE_LIB
+
+
+def build_all(verbose: bool = False, force: bool = False) -> None:
+    build_lib(verbose=verbose, force=force)
+    build_oracle(verbose=verbose, force=force)
+
+
+if __name__ == "__main__":
+    build_all(verbose=True, force="--force" in sys.argv)
+    if "--ptxas" in sys.argv:
+        build_lib(verbose=True, force=True, ptxas_verbose=True)
