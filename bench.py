@@ -1,0 +1,463 @@
+"""Benchmark: the plain CUDA frame (primary -> godray -> composite) on B200.
+
+Workload (N = 1): the full plain pipeline at 1920x1080 present / 960x540
+internal over a streamed world of 16x4x16 chunks with 3D caves, a 5-level
+256^2 toroidal clipmap and a seeded 64-frame Catmull-Rom camera path with a
++1 chunk grid shift every 16 frames.  One step = one frame.
+
+* ``value``  Mrays/s (primary rays = internal pixels) with every input
+  resident in HBM: all chunks the path needs are uploaded before timing and a
+  grid shift is a 4 KiB grid rewrite; per-step device time from CUDA events on
+  the compute stream, L2 flushed (512 MiB memset) between steps.
+* ``e2e``    the same frames through the C ABI with host buffers: camera,
+  clipmap patches, streamed chunk uploads at grid shifts (host -> device) and
+  the RGBA32F present image read back (device -> host) inside the timed region.
+* ``--gpus N``: replicas only -- each rank renders the same workload on its own
+  GPU, no data-path collective; value = all ranks' rays / max-over-ranks time.
+* ``--impl reference``: the reference cannot run here (Rust + WGSL, no
+  graphics stack), so the reference arm is the C++ scalar restatement of its
+  WGSL (oracle/) on all host cores, one full frame per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "voxel-engine-v0_b200"))
+sys.path.insert(0, str(REPO))
+
+METRIC = "Mrays/s + 1080p frame ms on 1×B200, served p50/p99 latency, vs plain CUDA pass"
+UNIT = "Mrays/s"
+WORKLOAD = ("config2 plain pipeline: 16x4x16 chunks (caves > 0.6), 5-level 256^2 clipmap, 1920x1080 present / "
+            "960x540 internal, primary+godray+composite per frame, 64-frame Catmull-Rom path, grid shift every 16 frames")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=24)
+    ap.add_argument("--warmup", type=int, default=4)
+    ap.add_argument("--impl", default="vxe", choices=["vxe", "reference"])
+    ap.add_argument("--present", default="1920x1080")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--profile-steps", type=int, default=0, help="render N steps only (for ncu), no JSON")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks / throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                if out.returncode == 0 and out.stdout.strip():
+                    self.samples.append([s.strip() for s in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 5 + i and
+                          s[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def build_world(present, resident_all: bool):
+    from vxe import scenes
+    from vxe.world import World
+
+    sc = scenes.config2(present=present)
+    # Every chunk the 64-frame path visits: grid origins x = 0..3 -> chunk x 0..18.
+    dims = (sc.grid_dims[0] + 3, sc.grid_dims[1], sc.grid_dims[2]) if resident_all else sc.grid_dims
+    world = World(sc.spec, sc.grid_origin, dims, sc.node_capacity, chunk_capacity=int(np.prod(dims)))
+    return sc, world
+
+
+def grid_window(world, ox: int, dims):
+    """chunk_grid for a 16x4x16 window at origin x = ox over a world holding more slots."""
+    nx, ny, nz = dims
+    g = np.full(nx * ny * nz, 0xFFFFFFFF, dtype=np.uint32)
+    for iz in range(nz):
+        for iy in range(ny):
+            for ix in range(nx):
+                s = world.key_to_slot.get((ox + ix, iy, iz))
+                if s is not None:
+                    g[(iz * ny + iy) * nx + ix] = s
+    return g
+
+
+def camera_for(sc, f, ox, prev_vp, chunk_count):
+    from vxe.world import build_camera
+
+    pos, yaw, pitch = sc.path(f)
+    cam = build_camera(pos, yaw, pitch, sc.present, sc.internal, frame_index=f + 1, time_s=f / 60.0, world=None,
+                       jitter=True, prev_view_proj=prev_vp)
+    cam.chunk_count = chunk_count
+    cam.grid_origin_chunk[0], cam.grid_origin_chunk[1], cam.grid_origin_chunk[2] = ox, 0, 0
+    cam.grid_dims[0], cam.grid_dims[1], cam.grid_dims[2] = sc.grid_dims
+    return cam, pos
+
+
+def run_vxe(args, rank: int, world_size: int):
+    import torch
+
+    from vxe import _abi as A
+    from vxe.renderer import Renderer
+    from vxe.world import Clipmap
+
+    dev = rank if torch.cuda.device_count() > rank else 0
+    torch.cuda.set_device(dev)
+    present = tuple(int(v) for v in args.present.split("x"))
+    sc, world = build_world(present, resident_all=True)
+    ups = world.populate()
+    r = Renderer(sc.present[0], sc.present[1], sc.render_scale, node_capacity=world.node_capacity,
+                 chunk_capacity=world.chunk_capacity, grid_capacity=int(np.prod(sc.grid_dims)),
+                 clip_levels=sc.clip_levels, clip_res=sc.clip_res, flags=A.FLAG_GODRAY_MACRO_ALIAS, device=dev)
+    r.apply_chunk_uploads(ups)
+    clip = Clipmap(sc.spec, sc.clip_levels, sc.clip_res, 1.0)
+    rays_per_frame = sc.internal[0] * sc.internal[1]
+    prev_vp = None
+    last_ox = None
+
+    def frame_inputs(step):
+        nonlocal prev_vp, last_ox
+        f = step % 64
+        ox = f // 16
+        cam, pos = camera_for(sc, f, ox, prev_vp, world.chunk_count)
+        prev_vp = cam.view_proj
+        params, patches = clip.update(float(pos[0]), float(pos[2]))
+        grid = None
+        if ox != last_ox:
+            grid = grid_window(world, ox, sc.grid_dims)
+            last_ox = ox
+        return cam, params, patches, grid
+
+    def submit(step):
+        cam, params, patches, grid = frame_inputs(step)
+        if grid is not None:
+            r.write_chunk_grid(grid)
+        r.write_clipmap_updates(params, patches)
+        r.write_camera(cam)
+        r.encode_compute(sync=False)
+
+    if args.profile_steps:
+        for s in range(args.profile_steps):
+            submit(s)
+        r.synchronize()
+        return None
+
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+    for s in range(args.warmup):
+        submit(s)
+    r.synchronize()
+    # ---- device-resident timing: per-step kernel time from the context's events
+    if world_size > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    step_ms, prim_ms, god_ms, comp_ms, tile_ms = [], [], [], [], []
+    with ClockSampler(dev) as clocks:
+        for s in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            submit(args.warmup + s)
+            t = r.read_gpu_timings_ms_blocking()
+            step_ms.append(t["total"])
+            prim_ms.append(t["primary"])
+            god_ms.append(t["godray"])
+            comp_ms.append(t["composite"])
+            tile_ms.append(t["tiles"])
+    torch.cuda.synchronize()
+    if world_size > 1:
+        torch.distributed.barrier()
+    total_ms = float(sum(step_ms))
+    err = r.read_error_word()
+    r.close()
+    # ---- end to end through the C ABI with host buffers (streaming world)
+    if args.no_e2e:
+        e2e = {"seconds": float("nan"), "rays": 0, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    else:
+        e2e = run_e2e(args, sc, dev, world_size)
+    return {
+        "total_ms": total_ms, "step_ms": step_ms, "primary_ms": prim_ms, "godray_ms": god_ms,
+        "composite_ms": comp_ms, "tiles_ms": tile_ms, "rays_per_frame": rays_per_frame,
+        "internal": list(sc.internal),
+        "clocks": clocks.summary(), "e2e": e2e, "error_word": err, "device": torch.cuda.get_device_name(dev),
+    }
+
+
+def run_e2e(args, sc, dev, world_size):
+    import torch
+
+    from vxe import _abi as A
+    from vxe.renderer import Renderer
+    from vxe.scenes import FrameDriver
+
+    drv = FrameDriver(sc)
+    ups = drv.initial_uploads()
+    # Chunks entering the grid at the shifts are built on the host before timing
+    # (the reference builds them on its worker pool); their upload is timed.
+    for ox in range(1, 4):
+        for iz in range(sc.grid_dims[2]):
+            for iy in range(sc.grid_dims[1]):
+                drv.world.chunk((ox + sc.grid_dims[0] - 1, iy, iz))
+    r = Renderer(sc.present[0], sc.present[1], sc.render_scale, node_capacity=drv.world.node_capacity,
+                 chunk_capacity=drv.world.chunk_capacity, grid_capacity=drv.world.grid_capacity,
+                 clip_levels=sc.clip_levels, clip_res=sc.clip_res, flags=A.FLAG_GODRAY_MACRO_ALIAS, device=dev)
+    r.upload_world(drv.world, ups)
+    pw, ph = sc.present
+    host_out = torch.empty((ph, pw, 4), dtype=torch.float32).pin_memory().numpy()
+    h2d = d2h = 0
+
+    def one():
+        nonlocal h2d, d2h
+        back = []
+        if drv.frame >= 64:
+            # restart the path: the grid returns to its first origin
+            drv.frame = 0
+            back = drv.world.shift(-drv.world.grid_origin[0], 0, 0)
+        uploads, grid_changed, clip, cam = drv.step()
+        if back:
+            uploads, grid_changed = back + uploads, True
+        b = 464
+        if uploads:
+            r.apply_chunk_uploads(uploads)
+            b += sum(48 + (len(u.data.nodes) * 48 + 16 * 4 + 2048 * 4 if u.data is not None else 0) for u in uploads)
+        if grid_changed:
+            r.write_chunk_grid(drv.world.grid)
+            b += drv.world.grid.nbytes
+        params, patches = clip
+        r.write_clipmap_updates(params, patches)
+        b += 528 + sum(p[5].nbytes for p in patches)
+        r.write_camera(cam)
+        r.encode_compute(sync=False)
+        r._check(r._lib.vxe_read_image(r._ctx, A.IMG_OUTPUT, host_out.ctypes.data, host_out.nbytes), "read")
+        h2d += b
+        d2h += host_out.nbytes
+
+    for _ in range(args.warmup):
+        one()
+    r.synchronize()
+    h2d = d2h = 0
+    if world_size > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one()
+    r.synchronize()
+    dt = time.perf_counter() - t0
+    if world_size > 1:
+        torch.distributed.barrier()
+    r.close()
+    rays = sc.internal[0] * sc.internal[1] * args.steps
+    return {"seconds": dt, "rays": rays, "h2d_bytes_per_step": h2d // args.steps,
+            "d2h_bytes_per_step": d2h // args.steps}
+
+
+def cpu_sample(seconds: float, present, threads: int):
+    """Times the oracle (scalar C++ restatement of the WGSL) on full frames."""
+    from oracle import oracle as O
+    from vxe.scenes import FrameDriver, config2
+
+    sc = config2(present=present)
+    drv = FrameDriver(sc)
+    drv.initial_uploads()
+    runner = O.OracleFrameRunner(drv.world, sc.internal, sc.present, drv.clip.tex, sc.clip_res)
+    frames = 0
+    ctr = None
+    t0 = time.perf_counter()
+    elapsed = 0.0
+    while elapsed < seconds or frames == 0:
+        uploads, gc, clip, cam = drv.step()
+        runner.render(cam, clip[0], threads=threads)
+        if ctr is None:
+            ctr = (runner.primary_ctr.as_dict(), runner.godray_ctr.as_dict())
+        frames += 1
+        elapsed = time.perf_counter() - t0
+    rays = frames * sc.internal[0] * sc.internal[1]
+    return {"rays": rays, "seconds": elapsed, "frames": frames, "counters": ctr}
+
+
+def algorithmic_primary_bytes(counters: dict, pixels: int) -> int:
+    """Record bytes the reference algorithm loads (full record sizes) + compulsory image I/O."""
+    c = counters
+    loads = (16 * c["node_loads"] + 32 * c["rope_loads"] + 48 * c["meta_loads"] + 4 * c["grid_loads"] +
+             4 * c["macro_loads"] + 4 * c["colinfo_loads"] + 4 * c["clip_loads"])
+    # outputs: color 16 + depth 4 + hist 16 + shadow 4 + local_hist 16; inputs: hist 16 + shadow 4 + local_hist 16
+    io = pixels * (16 + 4 + 16 + 4 + 16 + 16 + 4 + 16)
+    return int(loads + io)
+
+
+def max_over_ranks(values, device="cpu"):
+    """Element-wise max of per-rank timings (replicas: the job ends with the slowest rank)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def replica_value(rays_per_rank: int, world_size: int, max_seconds: float) -> float:
+    """Whole-job Mrays/s: every rank traces the same workload on its own GPU."""
+    return rays_per_rank * world_size / max_seconds / 1e6
+
+
+def peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        return main_reference(args, rank, world_size)
+    if world_size > 1:
+        import datetime
+
+        import torch
+
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    res = run_vxe(args, rank, world_size)
+    if res is None:
+        return
+    if world_size > 1:
+        import torch
+
+        total_ms, e2e_s = max_over_ranks([res["total_ms"], res["e2e"]["seconds"]], device="cuda")
+        torch.distributed.destroy_process_group()
+    else:
+        total_ms, e2e_s = res["total_ms"], res["e2e"]["seconds"]
+    if rank != 0:
+        return
+    n = max(1, world_size)
+    value = replica_value(res["rays_per_frame"] * args.steps, n, total_ms * 1e-3)
+    e2e_val = replica_value(res["e2e"]["rays"], n, e2e_s)
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": n, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded value-noise world)",
+        "config": {"workload": WORKLOAD, "present": list(map(int, args.present.split("x"))),
+                   "internal": res["internal"],
+                   "parallelism": "replicas" if n > 1 else "single",
+                   "l2": "flushed between steps (512 MiB memset), per-step CUDA events",
+                   "frame_ms": {"tiles": round(statistics.mean(res["tiles_ms"]), 4),
+                                "primary": round(statistics.mean(res["primary_ms"]), 4),
+                                "godray": round(statistics.mean(res["godray_ms"]), 4),
+                                "composite": round(statistics.mean(res["composite_ms"]), 4)}},
+        "e2e": {"value": round(e2e_val, 3), "unit": UNIT, "h2d_bytes_per_step": res["e2e"]["h2d_bytes_per_step"],
+                "d2h_bytes_per_step": res["e2e"]["d2h_bytes_per_step"],
+                "frame_ms": round(e2e_s * 1e3 / args.steps, 3)},
+        "gpu_launches": 4 * args.steps,
+        "clocks": res["clocks"],
+        "device_error_word": res["error_word"],
+    }
+    peak, peak_kind = peaks()
+    prim_s = statistics.mean(res["primary_ms"]) * 1e-3
+    roof = {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None, "traffic": None,
+            "kernel": "k_primary", "peak_kind": peak_kind}
+    if not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        present = tuple(int(v) for v in args.present.split("x"))
+        cs = cpu_sample(args.cpu_seconds, present, threads)
+        line["cpu_baseline"] = {"value": round(cs["rays"] / cs["seconds"] / 1e6, 4), "unit": UNIT, "cores": threads,
+                                "kind": "port",
+                                "sample": f"{cs['frames']} full frames of the same workload (path frames 0..{cs['frames'] - 1})"}
+        ab = algorithmic_primary_bytes(cs["counters"][0], res["rays_per_frame"])
+        achieved = ab / prim_s / 1e9
+        roof.update({"achieved": round(achieved, 2), "frac": round(achieved / peak, 5),
+                     "algorithmic_bytes_per_launch": ab,
+                     "bytes_per_ray": round(ab / res["rays_per_frame"], 2)})
+    traffic = REPO / "profiles" / "k_primary_traffic.json"
+    if traffic.exists():
+        roof["traffic"] = json.loads(traffic.read_text()).get("dram_bytes_per_launch")
+    line["roofline"] = roof
+    print(json.dumps(line))
+
+
+def main_reference(args, rank, world_size):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    present = tuple(int(v) for v in args.present.split("x"))
+    from oracle import oracle as O
+    from vxe.scenes import FrameDriver, config2
+
+    sc = config2(present=present)
+    drv = FrameDriver(sc)
+    drv.initial_uploads()
+    runner = O.OracleFrameRunner(drv.world, sc.internal, sc.present, drv.clip.tex, sc.clip_res)
+
+    def step():
+        if drv.frame >= 64:
+            drv.frame = 0
+        _, _, clip, cam = drv.step()
+        runner.render(cam, clip[0], threads=threads)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    rays = sc.internal[0] * sc.internal[1] * args.steps
+    v = rays / dt / 1e6
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 2),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded value-noise world)",
+        "config": {"workload": WORKLOAD, "present": list(present), "internal": list(sc.internal)},
+        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": "full frames of the same workload, one per step"},
+        "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference is Rust+WGSL; no Rust toolchain or graphics stack here, so this arm runs the C++ "
+                "scalar restatement of its WGSL (oracle/) on the host cores",
+    }))
+
+
+if __name__ == "__main__":
+    main()

@@ -18,8 +18,12 @@
 
 #if defined(__CUDACC__)
 #define VXE_HD __host__ __device__ __forceinline__
+/* Out of line on the device: called from dozens of sites, inlining them all
+ * overflows the instruction cache of the frame kernels. */
+#define VXE_HD_CALL __host__ __device__ __noinline__
 #else
 #define VXE_HD static inline
+#define VXE_HD_CALL static inline
 #include <string.h>
 #endif
 
@@ -161,7 +165,7 @@ VXE_HD double vxe_reduce_pio2(double x, int* q) {
   return ((x - kd * VXE_PIO2_1) - kd * VXE_PIO2_2) - kd * VXE_PIO2_3;
 }
 
-VXE_HD float vxe_sinf(float xf) {
+VXE_HD_CALL float vxe_sinf(float xf) {
   const double x = (double)xf;
   if (x != x || x - x != 0.0) return (float)(x - x); /* NaN for NaN / inf */
   if (x > 1e18 || x < -1e18) return 0.0f;              /* beyond the reduction */
@@ -175,7 +179,7 @@ VXE_HD float vxe_sinf(float xf) {
   return (float)v;
 }
 
-VXE_HD float vxe_cosf(float xf) {
+VXE_HD_CALL float vxe_cosf(float xf) {
   const double x = (double)xf;
   if (x != x || x - x != 0.0) return (float)(x - x);
   if (x > 1e18 || x < -1e18) return 1.0f;
@@ -189,11 +193,11 @@ VXE_HD float vxe_cosf(float xf) {
   return (float)v;
 }
 
-VXE_HD float vxe_expf(float x) { return (float)vxe_exp_d((double)x); }
+VXE_HD_CALL float vxe_expf(float x) { return (float)vxe_exp_d((double)x); }
 
 /* pow for the non-negative bases the passes use: pow(0, y>0) = 0,
  * pow(x, 0) = 1, negative bases give NaN (WGSL leaves them undefined). */
-VXE_HD float vxe_powf(float x, float y) {
+VXE_HD_CALL float vxe_powf(float x, float y) {
   if (y == 0.0f) return 1.0f;
   if (x == 0.0f) return y > 0.0f ? 0.0f : vxe_u2d(0x7FF0000000000000ull);
   if (x == 1.0f) return 1.0f;

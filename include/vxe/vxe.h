@@ -159,7 +159,11 @@ enum {
    * kernels otherwise never materialise; used by parity tests. */
   VXE_FLAG_DEBUG_INTERMEDIATES = 1u << 3,
   /* Device-side bounds checks on every arena index (sets the error word). */
-  VXE_FLAG_CHECKED = 1u << 4
+  VXE_FLAG_CHECKED = 1u << 4,
+  /* Run the primary pass as one kernel per pixel (trace + shading) instead of
+   * the default wavefront (trace kernel -> per-class shading kernels).  Both
+   * produce identical images. */
+  VXE_FLAG_PRIMARY_MEGAKERNEL = 1u << 5
 };
 
 typedef struct vxe_config {

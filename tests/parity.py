@@ -75,11 +75,13 @@ def make_renderer(scene, world, flags=A.FLAG_GODRAY_MACRO_ALIAS | A.FLAG_HIT_REC
                     clip_levels=max(1, scene.clip_levels), clip_res=scene.clip_res, flags=flags)
 
 
-def run_parity(scene, frames: int, threads: int | None = None, godray_alias: bool = True, on_frame=None):
+def run_parity(scene, frames: int, threads: int | None = None, godray_alias: bool = True, on_frame=None,
+               extra_flags: int = 0):
     """Renders `frames` frames on both sides; returns a list of per-frame mismatch dicts."""
     drv = FrameDriver(scene)
     ups = drv.initial_uploads()
     flags = A.FLAG_HIT_RECORDS | A.FLAG_DEBUG_INTERMEDIATES | (A.FLAG_GODRAY_MACRO_ALIAS if godray_alias else 0)
+    flags |= extra_flags
     r = make_renderer(scene, drv.world, flags)
     try:
         r.upload_world(drv.world, ups)

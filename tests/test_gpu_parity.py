@@ -34,6 +34,13 @@ def test_features_scene_all_shading_paths_bit_exact():
     assert all(r == {} for r in res), res
 
 
+def test_features_scene_megakernel_schedule_bit_exact():
+    # The one-kernel-per-pixel schedule must give the same images as the wavefront.
+    sc = scenes.features()
+    res = run_parity(sc, frames=3, extra_flags=A.FLAG_PRIMARY_MEGAKERNEL)
+    assert all(r == {} for r in res), res
+
+
 def test_features_scene_godray_alias_off_bit_exact():
     sc = scenes.features()
     res = run_parity(sc, frames=2, godray_alias=False)

@@ -160,7 +160,7 @@ __device__ __forceinline__ float hash31(v3 p) {
                  iz = (uint32_t)to_i32(floorf(p.z));
   return (float)hash3_u32(ix, iy, iz) * U32_TO_F01;
 }
-__device__ float value_noise(v2 p) {
+__device__ __noinline__ float value_noise(v2 p) {
   const v2 i = vfloor(p), f = vfract(p);
   const float a = hash12(i), b = hash12(i + V2(1.0f, 0.0f)), c = hash12(i + V2(0.0f, 1.0f)),
               d = hash12(i + V2(1.0f, 1.0f));
@@ -168,7 +168,7 @@ __device__ float value_noise(v2 p) {
   const float x1 = mixf(a, b, u.x), x2 = mixf(c, d, u.x);
   return mixf(x1, x2, u.y);
 }
-__device__ float fbm(v2 p) {
+__device__ __noinline__ float fbm(v2 p) {
   v2 x = p;
   float sum = 0.0f, amp = 0.5f;
   for (uint32_t i = 0; i < 5; ++i) {
@@ -252,7 +252,7 @@ __device__ __forceinline__ BoxHit aabb_hit_normal_inv(v3 ro, v3 rd, v3 inv, v3 b
 // ---------------------------------------------------------------------------
 struct LeafQuery { v3 bmin; float size; uint32_t mat; };
 
-__device__ LeafQuery query_leaf_at(const Scene& s, v3 p, v3 root_bmin, float root_size, uint32_t node_base,
+__device__ __noinline__ LeafQuery query_leaf_at(const Scene& s, v3 p, v3 root_bmin, float root_size, uint32_t node_base,
                         uint32_t macro_base) {  // svo_query.wgsl:11-108
   uint32_t idx = node_base;
   v3 bmin = root_bmin;
@@ -287,7 +287,7 @@ __device__ LeafQuery query_leaf_at(const Scene& s, v3 p, v3 root_bmin, float roo
   return LeafQuery{bmin, size, MAT_AIR};
 }
 
-__device__ LeafQuery query_leaf_world(const Scene& s, v3 p) {  // svo_query.wgsl:270-291
+__device__ __noinline__ LeafQuery query_leaf_world(const Scene& s, v3 p) {  // svo_query.wgsl:270-291
   const float vs = vs_(s);
   const float cs = (float)s.cam->chunk_size * vs;
   const i3 c = chunk_coord_from_pos(p, cs);
@@ -303,7 +303,7 @@ __device__ LeafQuery query_leaf_world(const Scene& s, v3 p) {  // svo_query.wgsl
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float hash1(v3 p) { return fract(sinf_(dot(p, V3(127.1f, 311.7f, 74.7f))) * 43758.5453f); }
 
-__device__ v3 wind_field(v3 pos, float t) {  // wind.wgsl:10-36
+__device__ __noinline__ v3 wind_field(v3 pos, float t) {  // wind.wgsl:10-36
   const v3 cell = vfloor(pos * WIND_CELL_FREQ);
   const float ph0 = hash1(cell), ph1 = hash1(cell + V3(19.0f, 7.0f, 11.0f));
   const v2 dir = normalize(V2(0.9f, 0.4f));
@@ -321,7 +321,7 @@ __device__ __forceinline__ v3 clamp_len(v3 v, float max_len) {  // wind.wgsl:38-
   return v * (max_len / sqrtf(l2));
 }
 
-__device__ v3 leaf_cube_offset(const Scene& s, v3 bmin, float size, float time_s, float strength) {  // leaves.wgsl:5-18
+__device__ __noinline__ v3 leaf_cube_offset(const Scene& s, v3 bmin, float size, float time_s, float strength) {  // leaves.wgsl:5-18
   const v3 center = bmin + V3s(0.5f * size);
   const float d = length(center - cam_pos(s));
   const float fade = smooth(LEAF_LOD_DISP_START, LEAF_LOD_DISP_END, d);
@@ -332,7 +332,7 @@ __device__ v3 leaf_cube_offset(const Scene& s, v3 bmin, float size, float time_s
   return clamp_len(w * amp, LEAF_OFFSET_MAX_FRAC * size);
 }
 
-__device__ BoxHit leaf_displaced_cube_hit(const Scene& s, v3 ro, v3 rd, v3 bmin, float size, float time_s, float strength,
+__device__ __noinline__ BoxHit leaf_displaced_cube_hit(const Scene& s, v3 ro, v3 rd, v3 bmin, float size, float time_s, float strength,
                                float tmin, float tmax) {  // leaves.wgsl:26-43
   const v3 off = leaf_cube_offset(s, bmin, size, time_s, strength);
   const v3 b2 = bmin + off;
@@ -403,7 +403,7 @@ __device__ __forceinline__ v2 grass_wind_xz(v3 root, float t, float strength) { 
   return V2(w.x, w.z);
 }
 
-__device__ float grass_sdf_lod(const Scene& s, v3 p, v3 cb, v3 id, float time_s, float strength, uint32_t lod) {
+__device__ __noinline__ float grass_sdf_lod(const Scene& s, v3 p, v3 cb, v3 id, float time_s, float strength, uint32_t lod) {
   // grass.wgsl:192-350
   const float vs = vs_(s);
   const float top_y = cb.y + vs;
@@ -480,7 +480,130 @@ __device__ float grass_sdf_lod(const Scene& s, v3 p, v3 cb, v3 id, float time_s,
   return dmin;
 }
 
-__device__ v3 grass_sdf_normal_lod(const Scene& s, v3 p, v3 cb, v3 id, float time_s, float strength, uint32_t lod) {
+// ---------------------------------------------------------------------------
+// Per-cell grass blade geometry.  grass_sdf_lod derives every blade's root,
+// wind bend, lean, radius, side axis and per-segment taper from the cell id
+// alone (10 sin/cos + 2 wind fields per blade, a pow per segment); only the
+// final box distance depends on the query point.  A march, its 6-tap normal
+// and the self-shadow march evaluate the same cell up to 13 times, so the
+// invariants are computed once per cell, lazily (after the point-dependent
+// rejects pass), with the identical float operation sequence.
+// ---------------------------------------------------------------------------
+struct GrassBladeGeom {
+  v3 root;
+  v2 w_xz, lean_dir;
+  float lean_amt, r0;
+  v3 side_hint;
+};
+
+struct GrassCellGeom {
+  bool built;
+  uint32_t blade_count, segs;
+  float blade_len, inv_segs;
+  GrassBladeGeom blade[3];
+  float taper[6];
+};
+
+__device__ __noinline__ void grass_cell_build(const Scene& s, v3 cb, v3 id, float time_s, float strength, uint32_t lod,
+                                              GrassCellGeom& G) {
+  const float vs = vs_(s);
+  const float top_y = cb.y + vs;
+  const float layer_h = GRASS_LAYER_HEIGHT_VOX * vs;
+  G.blade_len = layer_h * (0.65f + 0.35f * hash31(id + V3(9.1f, 3.7f, 5.2f)));
+  uint32_t blade_count = GRASS_BLADE_COUNT;
+  uint32_t segs = to_u32(fmax_(3.0f, floorf(GRASS_VOXEL_SEGS)));
+  if (lod == 1u) {
+    blade_count = min(blade_count, GRASS_BLADE_COUNT_MID);
+    segs = min(segs, GRASS_SEGS_MID);
+  } else if (lod == 2u) {
+    blade_count = min(blade_count, GRASS_BLADE_COUNT_FAR);
+    segs = min(segs, GRASS_SEGS_FAR);
+  }
+  G.blade_count = blade_count;
+  G.segs = segs;
+  G.inv_segs = 1.0f / fmax_((float)segs, 1.0f);
+  const float clump_r = 0.18f * vs;
+  const float base_r = (GRASS_VOXEL_THICKNESS_VOX * vs) * 0.85f;
+  for (uint32_t i = 0; i < blade_count; ++i) {
+    const v4 uvpw = grass_blade_params(id, i);
+    const float u0 = uvpw.x, v0 = uvpw.y, ph = uvpw.z, wR = uvpw.w;
+    const float cfi = (float)(i % 5u);
+    const float cu = hash31(id + V3(13.7f + cfi, 2.1f, 9.9f));
+    const float cv = hash31(id + V3(4.2f + cfi, 7.3f, 1.4f));
+    const float inset = 0.10f;
+    const float cux = mixf(inset, 1.0f - inset, cu), cvz = mixf(inset, 1.0f - inset, cv);
+    const v2 clump_center = V2(cb.x + cux * vs, cb.z + cvz * vs);
+    const float ang = TAU * u0;
+    const float rr = clump_r * (0.15f + 0.85f * v0);
+    const v2 root_xz = clump_center + V2(cosf_(ang), sinf_(ang)) * rr;
+    GrassBladeGeom& B = G.blade[i];
+    B.root = V3(root_xz.x, top_y, root_xz.y);
+    B.w_xz = 0.35f * grass_wind_xz(B.root + V3(0.0f, ph, 0.0f), time_s, strength);
+    const float lean_ang = TAU * fract(u0 * 1.73f + v0 * 2.11f);
+    B.lean_dir = V2(cosf_(lean_ang), sinf_(lean_ang));
+    B.lean_amt = 0.10f + 0.25f * (v0 * v0);
+    B.r0 = base_r * mixf(0.85f, 1.35f, wR);
+    const float roll = TAU * (0.15f * ph + 0.10f * wR);
+    const v2 roll_dir = V2(cosf_(roll), sinf_(roll));
+    B.side_hint = normalize(V3(B.lean_dir.x * roll_dir.x - B.lean_dir.y * roll_dir.y, 0.12f,
+                               B.lean_dir.x * roll_dir.y + B.lean_dir.y * roll_dir.x));
+  }
+  for (uint32_t sg = 0; sg < segs; ++sg) {
+    const float t01a = (float)sg * G.inv_segs;
+    const float t01b = ((float)sg + 1.0f) * G.inv_segs;
+    const float tmid = 0.5f * (t01a + t01b);
+    const float taper_shape = powf_(clampf(1.0f - tmid, 0.0f, 1.0f), 3.0f);
+    G.taper[sg] = mixf(GRASS_VOXEL_TAPER, 1.0f, taper_shape);
+  }
+  G.built = true;
+}
+
+// grass_sdf_lod (grass.wgsl:192-350) over the cached cell geometry.
+__device__ __noinline__ float grass_sdf_cached(const Scene& s, v3 p, v3 cb, v3 id, float time_s, float strength,
+                                               uint32_t lod, GrassCellGeom& G) {
+  const float vs = vs_(s);
+  const float top_y = cb.y + vs;
+  const float layer_h = GRASS_LAYER_HEIGHT_VOX * vs;
+  const float y01 = (p.y - top_y) / fmax_(layer_h, 1e-6f);
+  if (y01 < 0.0f || y01 > 1.0f) return BIG;
+  const float over = GRASS_OVERHANG_VOX * vs;
+  if (p.x < cb.x - over || p.x > cb.x + vs + over || p.z < cb.z - over || p.z > cb.z + vs + over) return BIG;
+  if (!G.built) grass_cell_build(s, cb, id, time_s, strength, lod, G);
+  const float blade_len = G.blade_len;
+  float dmin = BIG;
+  for (uint32_t i = 0; i < G.blade_count; ++i) {
+    const GrassBladeGeom& B = G.blade[i];
+    for (uint32_t sg = 0; sg < G.segs; ++sg) {
+      const float t01a = (float)sg * G.inv_segs;
+      const float t01b = ((float)sg + 1.0f) * G.inv_segs;
+      const float ya = t01a * blade_len, yb = t01b * blade_len;
+      const float seg_h = yb - ya;
+      const float bend_a = (blade_len * t01a) * (0.55f + 0.45f * t01a);
+      const float bend_b = (blade_len * t01b) * (0.55f + 0.45f * t01b);
+      const v2 bva = B.w_xz * t01a + B.lean_dir * B.lean_amt;
+      const v2 bvb = B.w_xz * t01b + B.lean_dir * B.lean_amt;
+      const v2 offa = bva * bend_a, offb = bvb * bend_b;
+      const v3 pa = B.root + V3(offa.x, ya, offa.y);
+      const v3 pb = B.root + V3(offb.x, yb, offb.y);
+      const v3 T = normalize(pb - pa);
+      v3 S = B.side_hint - T * dot(B.side_hint, T);
+      const float s2 = dot(S, S);
+      if (s2 < 1e-6f) S = ortho_basis_x(T);
+      else S = S * (1.0f / sqrtf(s2));
+      const v3 N = cross(T, S);
+      const v3 mid = 0.5f * (pa + pb);
+      const v3 d = p - mid;
+      const v3 local = V3(dot(d, S), dot(d, T), dot(d, N));
+      const float half_w = B.r0 * G.taper[sg] * 0.7f;
+      const float dbox = sdf_box(local, V3s(0.0f), V3(half_w, 0.5f * seg_h, half_w));
+      dmin = fmin_(dmin, dbox);
+    }
+  }
+  return dmin;
+}
+
+__device__ __noinline__ v3 grass_sdf_normal_lod(const Scene& s, v3 p, v3 cb, v3 id, float time_s, float strength,
+                                                uint32_t lod, GrassCellGeom& G) {
   // grass.wgsl:370-408
   if (lod != 0u) {
     const float vs = vs_(s);
@@ -491,25 +614,27 @@ __device__ v3 grass_sdf_normal_lod(const Scene& s, v3 p, v3 cb, v3 id, float tim
     return normalize(V3(-w.x * tilt, 1.0f, -w.y * tilt));
   }
   const float e = 0.01f * vs_(s);
-  const float dx = grass_sdf_lod(s, p + V3(e, 0.0f, 0.0f), cb, id, time_s, strength, lod) -
-                   grass_sdf_lod(s, p - V3(e, 0.0f, 0.0f), cb, id, time_s, strength, lod);
-  const float dy = grass_sdf_lod(s, p + V3(0.0f, e, 0.0f), cb, id, time_s, strength, lod) -
-                   grass_sdf_lod(s, p - V3(0.0f, e, 0.0f), cb, id, time_s, strength, lod);
-  const float dz = grass_sdf_lod(s, p + V3(0.0f, 0.0f, e), cb, id, time_s, strength, lod) -
-                   grass_sdf_lod(s, p - V3(0.0f, 0.0f, e), cb, id, time_s, strength, lod);
+  const float dx = grass_sdf_cached(s, p + V3(e, 0.0f, 0.0f), cb, id, time_s, strength, lod, G) -
+                   grass_sdf_cached(s, p - V3(e, 0.0f, 0.0f), cb, id, time_s, strength, lod, G);
+  const float dy = grass_sdf_cached(s, p + V3(0.0f, e, 0.0f), cb, id, time_s, strength, lod, G) -
+                   grass_sdf_cached(s, p - V3(0.0f, e, 0.0f), cb, id, time_s, strength, lod, G);
+  const float dz = grass_sdf_cached(s, p + V3(0.0f, 0.0f, e), cb, id, time_s, strength, lod, G) -
+                   grass_sdf_cached(s, p - V3(0.0f, 0.0f, e), cb, id, time_s, strength, lod, G);
   return normalize(V3(dx, dy, dz));
 }
 
-__device__ float grass_self_shadow(const Scene& s, v3 hp, v3 cb, v3 id, float time_s, float strength, uint32_t lod) {
+__device__ __noinline__ float grass_self_shadow(const Scene& s, v3 hp, v3 cb, v3 id, float time_s, float strength, uint32_t lod) {
   // grass.wgsl:410-447
   const float vs = vs_(s);
+  GrassCellGeom G;
+  G.built = false;
   v3 p = hp + SUN_DIR * (0.02f * vs);
   const float max_dist = (0.55f + 0.35f * (float)lod) * vs;
   const uint32_t steps = lod != 0u ? 4u : 6u;
   const float dt = max_dist / (float)steps;
   float occ = 0.0f;
   for (uint32_t i = 0; i < steps; ++i) {
-    const float d = grass_sdf_lod(s, p, cb, id, time_s, strength, lod);
+    const float d = grass_sdf_cached(s, p, cb, id, time_s, strength, lod, G);
     occ += clampf(1.0f - d / (0.05f * vs), 0.0f, 1.0f);
     p = p + SUN_DIR * dt;
   }
@@ -522,9 +647,11 @@ __device__ __forceinline__ uint32_t grass_lod_from_t(float t) {  // grass.wgsl:5
   return 0u;
 }
 
-__device__ GrassHit grass_layer_trace_lod(const Scene& s, v3 ro, v3 rd, float t_start, float t_end, v3 cb, v3 id, float time_s,
+__device__ __noinline__ GrassHit grass_layer_trace_lod(const Scene& s, v3 ro, v3 rd, float t_start, float t_end, v3 cb, v3 id, float time_s,
                                float strength, uint32_t lod) {  // grass.wgsl:456-491
   const float vs = vs_(s);
+  GrassCellGeom G;
+  G.built = false;
   float t = t_start;
   uint32_t steps = GRASS_TRACE_STEPS;
   if (lod == 1u) steps = GRASS_TRACE_STEPS_MID;
@@ -532,16 +659,16 @@ __device__ GrassHit grass_layer_trace_lod(const Scene& s, v3 ro, v3 rd, float t_
   for (uint32_t i = 0; i < steps; ++i) {
     if (t > t_end) break;
     const v3 p = ro + rd * t;
-    const float d = grass_sdf_lod(s, p, cb, id, time_s, strength, lod);
+    const float d = grass_sdf_cached(s, p, cb, id, time_s, strength, lod, G);
     if (d < GRASS_HIT_EPS_VOX * vs) {
-      return GrassHit{true, t, grass_sdf_normal_lod(s, p, cb, id, time_s, strength, lod)};
+      return GrassHit{true, t, grass_sdf_normal_lod(s, p, cb, id, time_s, strength, lod, G)};
     }
     t += fmax_(d, GRASS_STEP_MIN_VOX * vs);
   }
   return GrassHit{false, BIG, V3s(0.0f)};
 }
 
-__device__ GrassHit try_grass_slab_hit(const Scene& s, v3 ro, v3 rd, float t_min, float t_max, v3 cb, v3 id, float vs,
+__device__ __noinline__ GrassHit try_grass_slab_hit(const Scene& s, v3 ro, v3 rd, float t_min, float t_max, v3 cb, v3 id, float vs,
                             float time_s, float strength) {  // grass.wgsl:494-538
   const float layer_h = GRASS_LAYER_HEIGHT_VOX * vs;
   const float over = GRASS_OVERHANG_VOX * vs;
@@ -601,7 +728,7 @@ __device__ __forceinline__ v4 node_cube_from_key(v3 rb, float rs, uint32_t key) 
 
 struct AnchorNode { bool valid; uint32_t idx; v3 bmin; float size; uint32_t key; };
 
-__device__ AnchorNode anchor_from_key(const Scene& s, uint32_t node_base, v3 rb, float rs, uint32_t key) {
+__device__ __noinline__ AnchorNode anchor_from_key(const Scene& s, uint32_t node_base, v3 rb, float rs, uint32_t key) {
   // chunk_trace.wgsl:138-191
   if (key == INVALID) return AnchorNode{false, 0, V3s(0.0f), 0.0f, INVALID};
   const uint32_t lvl = min(node_level(key), chunk_max_depth(s));
@@ -670,7 +797,7 @@ __device__ ExitFaceRes exit_face_from_slab_safe(v3 rd, const CubeSlab& slab) {  
   return ExitFaceRes{rd.z > 0.0f ? 4u : 5u, 0};
 }
 
-__device__ LeafState descend_leaf_sparse(const Scene& s, v3 p, uint32_t node_base, uint32_t start_idx, v3 start_bmin,
+__device__ __noinline__ LeafState descend_leaf_sparse(const Scene& s, v3 p, uint32_t node_base, uint32_t start_idx, v3 start_bmin,
                               float start_size) {  // chunk_trace.wgsl:296-358
   uint32_t idx = start_idx;
   v3 bmin = start_bmin;
@@ -700,7 +827,7 @@ struct MacroDDAState {
   float tMaxX, tMaxY, tMaxZ, tDeltaX, tDeltaY, tDeltaZ, cell;
 };
 
-__device__ MacroDDAState macro_dda_init(v3 ro, v3 rd, v3 inv, float tcur, v3 rb, float rs, uint32_t macro_base) {
+__device__ __noinline__ MacroDDAState macro_dda_init(v3 ro, v3 rd, v3 inv, float tcur, v3 rb, float rs, uint32_t macro_base) {
   // chunk_trace.wgsl:397-475
   MacroDDAState st;
   st.enabled = false;
@@ -782,7 +909,7 @@ __device__ __forceinline__ ColInfo colinfo_decode(uint32_t e) {
   return ColInfo{true, y8, m8};
 }
 
-__device__ GrassHit probe_grass_columns_xz_dda(const Scene& s, v3 ro, v3 rd, v3 inv, float t0_in, float t1_in, v3 rb,
+__device__ __noinline__ GrassHit probe_grass_columns_xz_dda(const Scene& s, v3 ro, v3 rd, v3 inv, float t0_in, float t1_in, v3 rb,
                                     i3 origin_vox, float vs, uint32_t colinfo_base, float time_s,
                                     float strength) {  // chunk_trace.wgsl:1358-1504
   const float t0 = t0_in, t1 = t1_in;
@@ -845,7 +972,7 @@ __device__ __forceinline__ HitGeom make_hit(uint32_t mat, float t, v3 n, v3 rb, 
   return o;
 }
 
-__device__ ChunkTraceResult trace_chunk_rope_interval_nomacro(const Scene& s, v3 ro, v3 rd, v3 inv, const Meta& ch,
+__device__ __noinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(const Scene& s, v3 ro, v3 rd, v3 inv, const Meta& ch,
                                                    float t_enter, float t_exit, bool use_anchor,
                                                    uint32_t anchor_key, const TraceOpts& opt) {
   // chunk_trace.wgsl:669-961
@@ -978,7 +1105,7 @@ __device__ ChunkTraceResult trace_chunk_rope_interval_nomacro(const Scene& s, v3
   return ChunkTraceResult{miss_hitgeom(), an.valid, an.key};
 }
 
-__device__ ChunkTraceResult trace_chunk_interval_stream_macro(const Scene& s, v3 ro, v3 rd, v3 inv, const Meta& ch,
+__device__ __noinline__ ChunkTraceResult trace_chunk_interval_stream_macro(const Scene& s, v3 ro, v3 rd, v3 inv, const Meta& ch,
                                                    float t0_in, float t1_in, bool use_anchor, uint32_t anchor_key_in,
                                                    const TraceOpts& opt) {  // chunk_trace.wgsl:592-667
   const float vs = vs_(s);
@@ -1085,7 +1212,7 @@ __device__ __forceinline__ bool chunk_coords_neighbor(i3 a, i3 b) {  // chunk_tr
   return abs(a.x - b.x) <= 1 && abs(a.y - b.y) <= 1 && abs(a.z - b.z) <= 1;
 }
 
-__device__ bool chunk_heightfield_early_skip(const Scene& s, v3 ro, v3 rd, float t_enter, float t_exit, const Meta& ch,
+__device__ __noinline__ bool chunk_heightfield_early_skip(const Scene& s, v3 ro, v3 rd, float t_enter, float t_exit, const Meta& ch,
                                   float vs) {  // chunk_trace.wgsl:1310-1352
   if (ch.colinfo_base == INVALID) return false;
   if (rd.y >= 0.0f) return false;
@@ -1138,7 +1265,7 @@ __device__ float clip_height_texel(const Scene& s, uint32_t level, int32_t ix, i
   const int32_t sz = imod(iz + (int32_t)s.clip->offset[level][1], res);
   return clip_texel(s, sx, sz, level);
 }
-__device__ float clip_height_at_level(const Scene& s, v2 xz, uint32_t level) {  // clipmap.wgsl:71-108
+__device__ __noinline__ float clip_height_at_level(const Scene& s, v2 xz, uint32_t level) {  // clipmap.wgsl:71-108
   const int32_t res = max((int32_t)s.clip->res, 1);
   const float* p = s.clip->level[level];
   const float cell = fmax_(p[2], 1e-6f);
@@ -1165,7 +1292,7 @@ __device__ float clip_height_at_level_nearest(const Scene& s, v2 xz, uint32_t le
   const int32_t sz = imod(iz + (int32_t)s.clip->offset[level][1], res);
   return clip_texel(s, sx, sz, level);
 }
-__device__ v3 clip_normal_at_level_2tap(const Scene& s, v2 xz, uint32_t level) {  // clipmap.wgsl:132-147
+__device__ __noinline__ v3 clip_normal_at_level_2tap(const Scene& s, v2 xz, uint32_t level) {  // clipmap.wgsl:132-147
   const float cell = s.clip->level[level][2];
   const HSample h0 = clip_height_at_level_ok(s, xz, level);
   const HSample hx = clip_height_at_level_ok(s, xz + V2(cell, 0.0f), level);
@@ -1180,13 +1307,13 @@ __device__ bool clip_level_contains(const Scene& s, v2 xz, uint32_t level, int32
   const int32_t ix0 = to_i32(floorf(st.x)), iz0 = to_i32(floorf(st.y));
   return ix0 >= guard && iz0 >= guard && ix0 + 1 < res - guard && iz0 + 1 < res - guard;
 }
-__device__ uint32_t clip_best_level(const Scene& s, v2 xz, int32_t guard) {  // clipmap.wgsl:295-301
+__device__ __noinline__ uint32_t clip_best_level(const Scene& s, v2 xz, int32_t guard) {  // clipmap.wgsl:295-301
   const uint32_t n = min(s.clip->levels, CLIP_LEVELS_MAX);
   for (uint32_t i = 0; i < n; ++i)
     if (clip_level_contains(s, xz, i, guard)) return i;
   return max(n, 1u) - 1u;
 }
-__device__ uint32_t clip_ensure_contains(const Scene& s, v2 xz, uint32_t lvl_in, int32_t guard) {  // clipmap.wgsl:304-315
+__device__ __noinline__ uint32_t clip_ensure_contains(const Scene& s, v2 xz, uint32_t lvl_in, int32_t guard) {  // clipmap.wgsl:304-315
   const uint32_t n = min(s.clip->levels, CLIP_LEVELS_MAX);
   if (n == 0u) return 0u;
   uint32_t lvl = min(lvl_in, n - 1u);
@@ -1198,7 +1325,7 @@ __device__ uint32_t clip_ensure_contains(const Scene& s, v2 xz, uint32_t lvl_in,
 }
 struct ClipHit { bool hit; float t; v3 n; uint32_t mat; };
 
-__device__ ClipHit clip_trace_heightfield(const Scene& s, v3 ro, v3 rd, float t_min, float t_max) {  // clipmap.wgsl:156-243
+__device__ __noinline__ ClipHit clip_trace_heightfield(const Scene& s, v3 ro, v3 rd, float t_min, float t_max) {  // clipmap.wgsl:156-243
   const ClipHit miss{false, BIG, V3s(0.0f), MAT_AIR};
   if (s.clip->levels == 0u) return miss;
   if (rd.y >= -1e-4f) return miss;
@@ -1247,7 +1374,7 @@ __device__ ClipHit clip_trace_heightfield(const Scene& s, v3 ro, v3 rd, float t_
 __device__ __forceinline__ float material_variation_clip(v3 p, float cell, float strength) {  // clipmap.wgsl:247-250
   return (hash31(vfloor(p / cell)) - 0.5f) * strength;
 }
-__device__ v3 apply_material_variation_clip(v3 base, uint32_t mat, v3 hp) {  // clipmap.wgsl:252-275
+__device__ __noinline__ v3 apply_material_variation_clip(v3 base, uint32_t mat, v3 hp) {  // clipmap.wgsl:252-275
   v3 c = base;
   if (mat == MAT_GRASS) {
     const float v = material_variation_clip(hp, 3.0f, 1.0f) + material_variation_clip(hp, 0.75f, 0.35f);
@@ -1296,14 +1423,14 @@ __device__ float fog_optical_depth_with_base(float base, v3 ro, v3 rd, float t) 
   const float b = expf_(-k * (y0 + dy * t));
   return base * (a - b) / (k * dy);
 }
-__device__ v3 apply_fog(const Scene& s, v3 surface, v3 ro, v3 rd, float t_scene, v3 sky) {  // fog.wgsl:57-71
+__device__ __noinline__ v3 apply_fog(const Scene& s, v3 surface, v3 ro, v3 rd, float t_scene, v3 sky) {  // fog.wgsl:57-71
   const float od = fmax_(fog_optical_depth_with_base(fog_density_primary(s), ro, rd, t_scene), 0.0f);
   const float T = expf_(-od);
   const v3 ins = fog_inscatter(rd, fog_color_from_sky(rd, sky));
   return surface * T + ins * (1.0f - T);
 }
 
-__device__ v3 sky_bg(v3 rd) {  // sky.wgsl:5-25
+__device__ __noinline__ v3 sky_bg(v3 rd) {  // sky.wgsl:5-25
   const float t0 = smooth(-0.10f, 0.85f, rd.y);
   v3 col = vmix(V3(0.05f, 0.08f, 0.12f), V3(0.55f, 0.75f, 0.95f), t0);
   const float th = 1.0f - smooth(-0.20f, 0.18f, fabsf(rd.y));
@@ -1312,7 +1439,7 @@ __device__ v3 sky_bg(v3 rd) {  // sky.wgsl:5-25
   col = col + V3(0.20f, 0.35f, 0.60f) * (0.05f * tz);
   return col * SKY_EXPOSURE;
 }
-__device__ v3 sky_sun(v3 rd) {  // sky.wgsl:27-41
+__device__ __noinline__ v3 sky_sun(v3 rd) {  // sky.wgsl:27-41
   const float mu = clampf(dot(rd, SUN_DIR), -1.0f, 1.0f);
   const float mu_inner = cosf_(0.009f);
   const float mu_outer = cosf_(0.009f + 0.004f);
@@ -1331,7 +1458,7 @@ __device__ __forceinline__ float cloud_coverage_at_xz(v2 xz, float time_s) {  //
   const float field = 0.65f * fbm(uv) + 0.35f * fbm(uv * 2.3f + V2(13.2f, 7.1f));
   return smooth(CLOUD_COVERAGE, CLOUD_COVERAGE + CLOUD_SOFTNESS, field);
 }
-__device__ float cloud_density(v3 p, float time_s) {  // clouds.wgsl:34-65
+__device__ __noinline__ float cloud_density(v3 p, float time_s) {  // clouds.wgsl:34-65
   if (p.y <= CLOUD_BASE_H || p.y >= CLOUD_TOP_H) return 0.0f;
   const float h = cloud_height01(p.y);
   if (h <= 0.0f) return 0.0f;
@@ -1348,7 +1475,7 @@ __device__ float cloud_density(v3 p, float time_s) {  // clouds.wgsl:34-65
   d = d * h;
   return clampf(d, 0.0f, 1.0f);
 }
-__device__ float cloud_light_transmittance(v3 p, float time_s) {  // clouds.wgsl:68-90
+__device__ __noinline__ float cloud_light_transmittance(v3 p, float time_s) {  // clouds.wgsl:68-90
   const float tmax = (CLOUD_TOP_H - p.y) / fmax_(SUN_DIR_Y, 1e-3f);
   if (tmax <= 0.0f) return 1.0f;
   const float dt = tmax / (float)CLOUD_STEPS_LIGHT;
@@ -1359,7 +1486,7 @@ __device__ float cloud_light_transmittance(v3 p, float time_s) {  // clouds.wgsl
   }
   return expf_(-CLOUD_DENSITY * od * CLOUD_SHADOW_ABSORB);
 }
-__device__ float cloud_sun_transmittance_fast(const Scene& s, v3 p, v3 sd) {  // clouds.wgsl:134-165
+__device__ __noinline__ float cloud_sun_transmittance_fast(const Scene& s, v3 p, v3 sd) {  // clouds.wgsl:134-165
   if (sd.y <= 0.01f) return 1.0f;
   const float t0 = (CLOUD_BASE_H - p.y) / sd.y, t1 = (CLOUD_TOP_H - p.y) / sd.y;
   const float ta = fmin_(t0, t1), tb = fmax_(t0, t1);
@@ -1374,7 +1501,7 @@ __device__ float cloud_sun_transmittance_fast(const Scene& s, v3 p, v3 sd) {  //
   }
   return expf_(-CLOUD_DENSITY * od * CLOUD_SHADOW_ABSORB);
 }
-__device__ float cloud_density_godray(v3 p, float time_s) {  // clouds.wgsl:167-182
+__device__ __noinline__ float cloud_density_godray(v3 p, float time_s) {  // clouds.wgsl:167-182
   if (p.y <= CLOUD_BASE_H || p.y >= CLOUD_TOP_H) return 0.0f;
   const float h = cloud_height01(p.y);
   if (h <= 0.0f) return 0.0f;
@@ -1384,7 +1511,7 @@ __device__ float cloud_density_godray(v3 p, float time_s) {  // clouds.wgsl:167-
   const float field = 0.70f * n0 + 0.30f * n1;
   return smooth(CLOUD_COVERAGE, CLOUD_COVERAGE + CLOUD_SOFTNESS, field) * h;
 }
-__device__ float cloud_sun_transmittance_godray(const Scene& s, v3 p, v3 sd) {  // clouds.wgsl:184-214
+__device__ __noinline__ float cloud_sun_transmittance_godray(const Scene& s, v3 p, v3 sd) {  // clouds.wgsl:184-214
   if (sd.y <= 0.01f) return 1.0f;
   const float t0 = (CLOUD_BASE_H - p.y) / sd.y, t1 = (CLOUD_TOP_H - p.y) / sd.y;
   const float ta = fmin_(t0, t1), tb = fmax_(t0, t1);
@@ -1397,7 +1524,7 @@ __device__ float cloud_sun_transmittance_godray(const Scene& s, v3 p, v3 sd) {  
   return expf_(-CLOUD_DENSITY * dens * (te - ts) * CLOUD_SHADOW_ABSORB);
 }
 
-__device__ v3 sky_color(const Scene& s, v3 rd) {  // sky.wgsl:43-137
+__device__ __noinline__ v3 sky_color(const Scene& s, v3 rd) {  // sky.wgsl:43-137
   const v3 bg = sky_bg(rd);
   const v3 sun = sky_sun(rd);
   float T_view = 1.0f;
@@ -1445,7 +1572,7 @@ __device__ v3 sky_color(const Scene& s, v3 rd) {  // sky.wgsl:43-137
 // ---------------------------------------------------------------------------
 // shadows.wgsl
 // ---------------------------------------------------------------------------
-__device__ float trace_chunk_shadow_trans_interval(const Scene& s, v3 ro, v3 rd, const Meta& ch, float t_enter,
+__device__ __noinline__ float trace_chunk_shadow_trans_interval(const Scene& s, v3 ro, v3 rd, const Meta& ch, float t_enter,
                                         float t_exit) {  // shadows.wgsl:4-82
   const float vs = vs_(s);
   const float nudge = 0.20f * vs;
@@ -1488,7 +1615,7 @@ __device__ float trace_chunk_shadow_trans_interval(const Scene& s, v3 ro, v3 rd,
   return trans;
 }
 
-__device__ float sun_transmittance_geom_only(const Scene& s, v3 p, v3 sd) {  // shadows.wgsl:85-186
+__device__ __noinline__ float sun_transmittance_geom_only(const Scene& s, v3 p, v3 sd) {  // shadows.wgsl:85-186
   const float vs = vs_(s);
   const float nudge = 0.18f * vs;
   const float cs = (float)s.cam->chunk_size * vs;
@@ -1566,7 +1693,7 @@ __device__ __forceinline__ v3 sphere_dir_local(uint32_t i, uint32_t count) {  //
   return V3(cosf_(phi) * r, sinf_(phi) * r, y);
 }
 
-__device__ v4 dda_hit_light(const Scene& s, v3 p0, v3 dir, uint32_t max_steps, float vs) {  // light.wgsl:65-121
+__device__ __noinline__ v4 dda_hit_light(const Scene& s, v3 p0, v3 dir, uint32_t max_steps, float vs) {  // light.wgsl:65-121
   const v3 gpos = p0 / fmax_(vs, 1e-6f);
   const v3 fl = vfloor(gpos);
   i3 cell{to_i32(fl.x), to_i32(fl.y), to_i32(fl.z)};
@@ -1599,7 +1726,7 @@ __device__ __forceinline__ v3 material_emission(uint32_t m) {  // shading.wgsl:2
   return V3s(0.0f);
 }
 
-__device__ v3 gather_voxel_lights(const Scene& s, v3 hp, v3 n, v3 rb) {  // light.wgsl:127-211
+__device__ __noinline__ v3 gather_voxel_lights(const Scene& s, v3 hp, v3 n, v3 rb) {  // light.wgsl:127-211
   uint32_t hits = 0;
   const float vs = vs_(s);
   const v3 p0 = hp + n * (0.75f * vs);
@@ -1660,7 +1787,7 @@ __device__ __forceinline__ v3 color_for_material(uint32_t m) {  // shading.wgsl:
 __device__ __forceinline__ v3 hemi_ambient(v3 n, v3 sky_up) {  // shading.wgsl:18-22
   return vmix(FOG_COLOR_GROUND, sky_up, clampf(n.y * 0.5f + 0.5f, 0.0f, 1.0f));
 }
-__device__ v3 apply_material_variation(v3 base, uint32_t mat, v3 hp) {  // shading.wgsl:24-50
+__device__ __noinline__ v3 apply_material_variation(v3 base, uint32_t mat, v3 hp) {  // shading.wgsl:24-50
   v3 c = base;
   const float v = ALBEDO_VAR_GAIN * ((hash31(vfloor(hp / 0.05f)) - 0.5f) * 2.0f);
   if (mat == MAT_GRASS) {
@@ -1680,13 +1807,13 @@ __device__ v3 apply_material_variation(v3 base, uint32_t mat, v3 hp) {  // shadi
   }
   return vclamp(c, V3s(0.0f), V3s(1.5f));
 }
-__device__ v2 grass_wind_dir_xz(v3 p, float time_s) {  // shading.wgsl:52-59
+__device__ __noinline__ v2 grass_wind_dir_xz(v3 p, float time_s) {  // shading.wgsl:52-59
   const v3 w = wind_field(p, time_s);
   v2 dir = V2(w.x, w.z) + V2(0.6f, 0.2f);
   if (dot(dir, dir) < 1e-4f) dir = V2(0.7f, 0.25f);
   return normalize(dir);
 }
-__device__ float grass_blade_slivers(v3 pw, float time_s, float freq, float detail) {  // shading.wgsl:61-88
+__device__ __noinline__ float grass_blade_slivers(v3 pw, float time_s, float freq, float detail) {  // shading.wgsl:61-88
   const v2 dir = grass_wind_dir_xz(pw, time_s);
   const v2 perp = V2(-dir.y, dir.x);
   const v2 pxz = V2(pw.x, pw.z);
@@ -1708,14 +1835,14 @@ __device__ float grass_blade_slivers(v3 pw, float time_s, float freq, float deta
   const float lm = smooth(0.0f, 0.15f, u) * smooth(1.0f, 0.75f, u);
   return sliver * lm;
 }
-__device__ float grass_blade_field(v3 p, float time_s, float t) {  // shading.wgsl:90-98
+__device__ __noinline__ float grass_blade_field(v3 p, float time_s, float t) {  // shading.wgsl:90-98
   const float detail = 1.0f - smooth(18.0f, 55.0f, t);
   const float low = grass_blade_slivers(p, time_s, 9.0f, detail * 0.6f);
   const float high = grass_blade_slivers(p + V3(1.7f, 0.0f, 2.3f), time_s, 18.0f, detail);
   const float blend = mixf(0.15f, 1.0f, detail);
   return mixf(low, 0.5f * (low + high), blend);
 }
-__device__ v3 grass_top_albedo(const Scene& s, v3 base, v3 hp, float t) {  // shading.wgsl:100-122
+__device__ __noinline__ v3 grass_top_albedo(const Scene& s, v3 base, v3 hp, float t) {  // shading.wgsl:100-122
   const float vs = vs_(s);
   const float tip = clampf(fract(hp.y / fmax_(vs, 1e-6f)), 0.0f, 1.0f);
   const float blade = grass_blade_field(hp, s.cam->voxel_params[1], t);
@@ -1748,7 +1875,7 @@ __device__ float macro_occ_at_ws(const Scene& s, v3 p, v3 rb, float rs, uint32_t
   const uint32_t mz = clampu(to_u32(floorf(lp.z / cell)), 0u, 7u);
   return macro_test(s, macro_base, macro_bit_index(mx, my, mz)) ? 1.0f : 0.0f;
 }
-__device__ float voxel_ao_local(const Scene& s, v3 hp, v3 n, v3 rb, float rs, uint32_t macro_base) {  // shading.wgsl:157-184
+__device__ __noinline__ float voxel_ao_local(const Scene& s, v3 hp, v3 n, v3 rb, float rs, uint32_t macro_base) {  // shading.wgsl:157-184
   const float r = 0.75f * vs_(s);
   const v3 up = fabsf(n.y) > 0.9f ? V3(1.0f, 0.0f, 0.0f) : V3(0.0f, 1.0f, 0.0f);
   const v3 t = normalize(cross(up, n));
@@ -1779,7 +1906,7 @@ __device__ __forceinline__ float material_f0(uint32_t m) {
   return 0.02f;
 }
 
-__device__ v3 shade_hit(const Scene& s, v3 ro, v3 rd, const HitGeom& hg, v3 sky_up, float sun_shadow) {  // shading.wgsl:257-362
+__device__ __noinline__ v3 shade_hit(const Scene& s, v3 ro, v3 rd, const HitGeom& hg, v3 sky_up, float sun_shadow) {  // shading.wgsl:257-362
   const v3 hp = ro + rd * hg.t;
   v3 base = base_albedo(hg.mat, hp, hg.t);
   if (hg.mat == MAT_GRASS) {
@@ -1832,7 +1959,7 @@ __device__ v3 shade_hit(const Scene& s, v3 ro, v3 rd, const HitGeom& hg, v3 sky_
   return base * (ambient + direct) + spec_col * 0.20f + material_emission(hg.mat);
 }
 
-__device__ v3 shade_clip_hit(const Scene& s, v3 ro, v3 rd, const ClipHit& ch, v3 sky_up) {  // shading.wgsl:364-434
+__device__ __noinline__ v3 shade_clip_hit(const Scene& s, v3 ro, v3 rd, const ClipHit& ch, v3 sky_up) {  // shading.wgsl:364-434
   const v3 hp = ro + rd * ch.t;
   v3 base = color_for_material(ch.mat);
   if (ch.t <= FAR_SHADING_DIST) base = apply_material_variation_clip(base, ch.mat, hp);
@@ -1888,7 +2015,7 @@ __device__ __forceinline__ uint32_t godray_steps_for_tend(float t_end) {  // god
   return min(sN, GODRAY_STEPS_FAST);
 }
 
-__device__ v3 godray_integrate_1(const Scene& s, v3 ro, v3 rd, float t_end, float j, float j_phase) {  // godrays.wgsl:45-216
+__device__ __noinline__ v3 godray_integrate_1(const Scene& s, v3 ro, v3 rd, float t_end, float j, float j_phase) {  // godrays.wgsl:45-216
   const float base = fog_density_godray(s);
   if (base <= 0.0f || t_end <= 0.0f) return V3s(0.0f);
   const float phase = phase_blended(dot(rd, SUN_DIR));

@@ -57,6 +57,11 @@ struct FrameArgs {
   const float4* out_hist_in;
   float4* out_hist_out;
   uint4* hits;  // optional, 2 x uint4 per pixel (vxe_hit)
+  // wavefront primary: per-pixel trace results + class queues
+  uint4* pix_hit;     // 5 x uint4 per pixel (PixHit), written for voxel hits
+  uint32_t* q_vox;    // pixel ids with a voxel hit
+  uint32_t* q_far;    // pixel ids for heightfield / sky
+  uint32_t* q_count;  // [0] voxel, [1] far
 };
 
 __device__ __forceinline__ Scene make_scene(const FrameArgs& A, bool godray) {
@@ -265,23 +270,207 @@ __device__ __forceinline__ v3 xyz(float4 v) { return V3(v.x, v.y, v.z); }
 
 // ---------------------------------------------------------------------------
 // Primary pass (+ fused local TAA)
+//
+// Two schedules of the same per-pixel function:
+//   k_primary            one thread per pixel does trace + shading (megakernel);
+//   k_primary_trace  ->  k_shade_vox / k_shade_far  (wavefront): the trace
+//       kernel classifies each pixel (voxel hit vs heightfield/sky) into a
+//       queue with warp-aggregated atomics and stores the hit; each shading
+//       kernel then runs over one class only, so sky cloud marches, terrain
+//       marches and voxel shading no longer share warps.  Queue order does not
+//       matter: every pixel's result depends only on its own inputs.
 // ---------------------------------------------------------------------------
 constexpr int PRIMARY_THREADS = 128;  // two 8x8 logical tiles per block
+constexpr int SHADE_THREADS = 128;
 
-__global__ void __launch_bounds__(PRIMARY_THREADS) k_primary(const __grid_constant__ FrameArgs A) {
-  __shared__ uint32_t cslot[2][TILE_CANDS];
-  __shared__ Meta cmeta[2][TILE_CANDS];
-  __shared__ uint32_t ccount[2];
-  const Scene s = make_scene(A, false);
-  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+struct PrimaryCtx {
+  uint32_t gx, gy;
+  size_t pix;
+  v2 px;
+  uint32_t seed;
+  v3 ro, rd;
+};
+
+__device__ __forceinline__ PrimaryCtx primary_ctx(const Scene& s, uint32_t gx, uint32_t gy, uint32_t W) {
+  PrimaryCtx c;
+  c.gx = gx;
+  c.gy = gy;
+  c.pix = (size_t)gy * W + gx;
+  c.px = V2((float)gx + 0.5f, (float)gy + 0.5f);
+  c.seed = (gx * 1973u) ^ (gy * 9277u) ^ (s.cam->frame_index * 26699u);
+  c.ro = cam_pos(s);
+  c.rd = ray_dir_from_pixel(s, c.px);
+  return c;
+}
+
+// History hint + voxel trace (ray_main.wgsl:274-325 and trace_primary_voxels :116-161).
+__device__ __noinline__ VoxTraceResult primary_trace(const Scene& s, const FrameArgs& A, const PrimaryCtx& c,
+                                                     const uint32_t* cslot, const Meta* cmeta, uint32_t tile_count) {
+  VoxTraceResult vt{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
+  if (s.cam->chunk_count == 0u || tile_count == 0u) return vt;
+  const uint32_t W = A.iw, H = A.ih;
+  const v2 res = V2((float)W, (float)H);
+  float t_hist = 0.0f;
+  bool hist_valid = false;
+  uint32_t hak = INVALID;
+  i3 hac{0, 0, 0};
+  const v2 uv = c.px / res;
+  const float t_guess = __uint_as_float(A.hist_in[c.pix].x);
+  if (t_guess > 1e-3f) {
+    const v3 p_ws = c.ro + c.rd * t_guess;
+    const v2 uvp = prev_uv_from_world(s, p_ws);
+    if (in_unit_square(uvp)) {
+      const int32_t sx = nearest_idx(uvp.x, W), sy = nearest_idx(uvp.y, H);
+      const uint4 hp = A.hist_in[(size_t)sy * W + (uint32_t)sx];
+      const float t_prev = __uint_as_float(hp.x);
+      const float rel = fabsf(t_prev - t_guess) / fmax_(t_guess, 1e-3f);
+      const float depth_ok = 1.0f - smooth(PRIMARY_HIT_DEPTH_REL0, PRIMARY_HIT_DEPTH_REL1, rel);
+      const float vel = length((uvp - uv) * res);
+      const float motion_ok = 1.0f - smooth(PRIMARY_HIT_MOTION_PX0, PRIMARY_HIT_MOTION_PX1, vel);
+      if (t_prev > 1e-3f && depth_ok > 0.5f && motion_ok > 0.5f) {
+        t_hist = t_prev;
+        hist_valid = true;
+        if ((hp.w & 0x80000000u) != 0u) {
+          hak = hp.y;
+          hac = i3{unpack_i16(hp.z), unpack_i16(hp.z >> 16), unpack_i16(hp.w)};
+        }
+      }
+    }
+  }
+  const float t_start = fmax_(t_hist - PRIMARY_HIT_MARGIN, 0.0f);
+  const float t_end = fmin_(t_hist + PRIMARY_HIT_WINDOW, FOG_MAX_DIST);
+  if (hist_valid) {
+    const VoxTraceResult h = trace_candidates(s, cslot, cmeta, c.ro, c.rd, t_start, t_end, hak != INVALID, hac, hak,
+                                              tile_count);
+    if (h.best.hit != 0u) return h;
+  }
+  return trace_candidates(s, cslot, cmeta, c.ro, c.rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID, tile_count);
+}
+
+// main_local_taa (taa.wgsl:26-69) for one pixel, fused after its shading.
+__device__ __forceinline__ void local_taa_store(const FrameArgs& A, size_t pix, v3 local_out, float local_w) {
+  if (A.local) A.local[pix] = make_float4(local_out.x, local_out.y, local_out.z, local_w);
+  const float4 h4 = A.local_hist_in[pix];
+  const bool hist_ok = !is_bad(xyz(h4));
+  const v3 hl = hist_ok ? xyz(h4) : V3s(0.0f);
+  const float conf0 = hist_ok ? h4.w : 0.0f;
+  const bool has_sample = local_w > 0.0f && !is_bad(local_out);
+  const float k = has_sample ? LOCAL_TAA_ALPHA * clampf(local_w, 0.0f, 1.0f) : 0.0f;
+  const v3 ol = vmix(hl, local_out, k);
+  const float conf1 = has_sample ? fmin_(1.0f, conf0 + k) : conf0;
+  A.local_hist_out[pix] = make_float4(ol.x, ol.y, ol.z, conf1);
+}
+
+// Voxel-hit shading (ray_main.wgsl:374-471) + outputs.
+__device__ __noinline__ void shade_voxel_pixel(const Scene& s, const FrameArgs& A, const PrimaryCtx& c, HitGeom best,
+                                               bool anchor_valid, uint32_t anchor_key, i3 anchor_chunk) {
+  const float vs = vs_(s);
+  const v3 ro = c.ro, rd = c.rd;
+  const uint32_t W = A.iw, H = A.ih;
+  const v3 sky_up = sky_bg(V3(0.0f, 1.0f, 0.0f));
+  if (best.mat == MAT_GRASS) {
+    const int32_t csv = (int32_t)s.cam->chunk_size;
+    const i3 ov{to_i32(floorf(best.root_bmin.x / vs + 0.5f)), to_i32(floorf(best.root_bmin.y / vs + 0.5f)),
+                to_i32(floorf(best.root_bmin.z / vs + 0.5f))};
+    const v3 hp = ro + rd * best.t;
+    const GrassCell cell = pick_grass_cell_in_chunk_with_bias(hp, rd, best.root_bmin, ov, vs, csv);
+    const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, best.t, cell.bmin_m, cell.id_vox, vs,
+                                           s.cam->voxel_params[1], s.cam->voxel_params[2]);
+    if (gh.hit) { best.t = gh.t; best.n = gh.n; }
+  }
+  const v3 hp = ro + rd * best.t;
+  const v3 hps = hp + best.n * (0.75f * vs);
+  float shadow_out;
+  if ((c.seed & SHADOW_SUBSAMPLE_MASK) == 0u) {
+    float sh = A.shadow_in[c.pix];
+    const v2 uvp = prev_uv_from_world(s, hp);
+    if (in_unit_square(uvp)) {
+      const int32_t ppx = clampi(to_i32(uvp.x * (float)W), 0, (int32_t)W - 1);
+      const int32_t ppy = clampi(to_i32(uvp.y * (float)H), 0, (int32_t)H - 1);
+      sh = A.shadow_in[(size_t)ppy * W + (uint32_t)ppx];
+    }
+    sh = clampf(sh, 0.0f, 1.0f);
+    const float cur = sun_transmittance_geom_only(s, hps, SUN_DIR);
+    shadow_out = mixf(sh, cur, SHADOW_TAA_ALPHA);
+  } else {
+    shadow_out = clampf(A.shadow_in[c.pix], 0.0f, 1.0f);
+  }
+  const v3 base_hdr = shade_hit(s, ro, rd, best, sky_up, shadow_out);
+  v3 local_out = V3s(0.0f);
+  float local_w = 0.0f;
+  if (best.hit != 0u && best.mat != MAT_LIGHT && best.t <= LOCAL_LIGHT_MAX_DIST) {
+    const v3 hpl = ro + rd * best.t;
+    const v3 alb = base_albedo(best.mat, hpl, best.t);
+    local_out = gather_voxel_lights(s, hpl, best.n, best.root_bmin) * alb;
+    local_w = 1.0f;
+  }
+  const float t_scene = fmin_(best.t, FOG_MAX_DIST);
+  const v3 col = apply_fog(s, base_hdr, ro, rd, t_scene, sky_bg(rd));
+  uint32_t pxy = 0u, pz = 0u, ak = 0u;
+  if (anchor_valid) {
+    pxy = pack_i16x2(anchor_chunk.x, anchor_chunk.y);
+    pz = pack_i16x2(anchor_chunk.z, 0) | 0x80000000u;
+    ak = anchor_key;
+  }
+  A.color[c.pix] = make_float4(col.x, col.y, col.z, 1.0f);
+  A.depth[c.pix] = t_scene;
+  A.hist_out[c.pix] = make_uint4(__float_as_uint(t_scene), ak, pxy, pz);
+  A.shadow_out[c.pix] = shadow_out;
+  if (A.hits) store_rec(A.hits + c.pix * 2u, make_rec(best, ro, rd, vs, true));
+  local_taa_store(A, c.pix, local_out, local_w);
+}
+
+// Heightfield then sky (ray_main.wgsl:224-269 / 327-372 / 473-516) + outputs.
+__device__ __noinline__ void shade_far_pixel(const Scene& s, const FrameArgs& A, const PrimaryCtx& c) {
+  const float vs = vs_(s);
+  const v3 ro = c.ro, rd = c.rd;
+  HitRec rec = miss_rec();
+  v3 col;
+  float depth, t_store = 0.0f;
+  ClipHit hf = clip_trace_heightfield(s, ro, rd, 0.0f, FOG_MAX_DIST);
+  if (hf.hit) {
+    if (hf.mat == MAT_GRASS) {
+      const v3 hp = ro + rd * hf.t;
+      const GrassCell cell = grass_cell_from_world_global(hp, rd, vs);
+      const v3 gb = V3(cell.bmin_m.x, hp.y - vs, cell.bmin_m.z);
+      const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, hf.t, gb, cell.id_vox, vs, s.cam->voxel_params[1],
+                                             s.cam->voxel_params[2]);
+      if (gh.hit) { hf.t = gh.t; hf.n = gh.n; }
+    }
+    const v3 surface = shade_clip_hit(s, ro, rd, hf, sky_bg(V3(0.0f, 1.0f, 0.0f)));
+    const float t_scene = fmin_(hf.t, FOG_MAX_DIST);
+    col = apply_fog(s, surface, ro, rd, t_scene, sky_bg(rd));
+    depth = t_scene;
+    t_store = t_scene;
+    HitGeom g = miss_hitgeom();
+    g.hit = 1u;
+    g.t = hf.t;
+    g.n = hf.n;
+    g.mat = hf.mat;
+    rec = make_rec(g, ro, rd, vs, false);
+  } else {
+    col = sky_color(s, rd);
+    depth = FOG_MAX_DIST;
+  }
+  A.color[c.pix] = make_float4(col.x, col.y, col.z, 1.0f);
+  A.depth[c.pix] = depth;
+  A.hist_out[c.pix] = make_uint4(__float_as_uint(t_store), 0u, 0u, 0u);
+  A.shadow_out[c.pix] = 1.0f;
+  if (A.hits) store_rec(A.hits + c.pix * 2u, rec);
+  local_taa_store(A, c.pix, V3s(0.0f), 0.0f);
+}
+
+// Stages a block's two tile candidate lists (slots + ChunkMeta) in shared memory.
+__device__ __forceinline__ void stage_tiles(const Scene& s, const FrameArgs& A, uint32_t (*cslot)[TILE_CANDS],
+                                            Meta (*cmeta)[TILE_CANDS], uint32_t* ccount) {
+  const uint32_t tid = threadIdx.x;
   const uint32_t tiles_x = (A.iw + 7u) / 8u;
-  const uint32_t ty = blockIdx.y;
   if (tid < 2u * TILE_CANDS) {
     const uint32_t t = tid / TILE_CANDS, i = tid % TILE_CANDS;
     const uint32_t tx = blockIdx.x * 2u + t;
     uint32_t n = 0u, slot = INVALID;
     if (tx < tiles_x) {
-      const size_t tile = (size_t)ty * tiles_x + tx;
+      const size_t tile = (size_t)blockIdx.y * tiles_x + tx;
       n = A.tile_count[tile];
       slot = A.tile_slots[tile * TILE_CANDS + i];
     }
@@ -290,172 +479,107 @@ __global__ void __launch_bounds__(PRIMARY_THREADS) k_primary(const __grid_consta
     if (i < n && slot != INVALID && slot < s.cam->chunk_count) cmeta[t][i] = meta_at(s, slot);
   }
   __syncthreads();
-  const uint32_t t = warp >> 1;
-  const uint32_t tx = blockIdx.x * 2u + t;
-  const uint32_t gx = tx * 8u + (lane & 7u);
-  const uint32_t gy = ty * 8u + (warp & 1u) * 4u + (lane >> 3);
-  if (tx >= tiles_x || gx >= A.iw || gy >= A.ih) return;
-  const uint32_t W = A.iw, H = A.ih;
-  const size_t pix = (size_t)gy * W + gx;
-  const uint32_t tile_count = ccount[t];
-  const v3 sky_up = sky_bg(V3(0.0f, 1.0f, 0.0f));
-  const v2 res = V2((float)W, (float)H);
-  const v2 px = V2((float)gx + 0.5f, (float)gy + 0.5f);
-  const uint32_t seed = (gx * 1973u) ^ (gy * 9277u) ^ (s.cam->frame_index * 26699u);
-  const v3 ro = cam_pos(s);
-  const v3 rd = ray_dir_from_pixel(s, px);
-  const float vs = vs_(s);
-  v3 local_out = V3s(0.0f);
-  float local_w = 0.0f;
-  float t_store = 0.0f;
-  float shadow_out = 1.0f;
-  HitRec rec = miss_rec();
-  v3 col;
-  float depth;
-  uint4 hist;
+}
 
-  bool shade_hf = true;
-  if (s.cam->chunk_count != 0u) {
-    float t_hist = 0.0f;
-    bool hist_valid = false;
-    uint32_t hak = INVALID;
-    i3 hac{0, 0, 0};
-    const bool has_tc = tile_count != 0u;
-    const v2 uv = px / res;
-    if (has_tc) {
-      const float t_guess = __uint_as_float(A.hist_in[pix].x);
-      if (t_guess > 1e-3f) {
-        const v3 p_ws = ro + rd * t_guess;
-        const v2 uvp = prev_uv_from_world(s, p_ws);
-        if (in_unit_square(uvp)) {
-          const int32_t sx = nearest_idx(uvp.x, W), sy = nearest_idx(uvp.y, H);
-          const uint4 hp = A.hist_in[(size_t)sy * W + (uint32_t)sx];
-          const float t_prev = __uint_as_float(hp.x);
-          const float rel = fabsf(t_prev - t_guess) / fmax_(t_guess, 1e-3f);
-          const float depth_ok = 1.0f - smooth(PRIMARY_HIT_DEPTH_REL0, PRIMARY_HIT_DEPTH_REL1, rel);
-          const float vel = length((uvp - uv) * res);
-          const float motion_ok = 1.0f - smooth(PRIMARY_HIT_MOTION_PX0, PRIMARY_HIT_MOTION_PX1, vel);
-          if (t_prev > 1e-3f && depth_ok > 0.5f && motion_ok > 0.5f) {
-            t_hist = t_prev;
-            hist_valid = true;
-            if ((hp.w & 0x80000000u) != 0u) {
-              hak = hp.y;
-              hac = i3{unpack_i16(hp.z), unpack_i16(hp.z >> 16), unpack_i16(hp.w)};
-            }
-          }
-        }
-      }
-    }
-    const float t_start = fmax_(t_hist - PRIMARY_HIT_MARGIN, 0.0f);
-    const float t_end = fmin_(t_hist + PRIMARY_HIT_WINDOW, FOG_MAX_DIST);
-    VoxTraceResult vt{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
-    if (has_tc) {
-      bool done = false;
-      if (hist_valid) {
-        const VoxTraceResult h =
-            trace_candidates(s, cslot[t], cmeta[t], ro, rd, t_start, t_end, hak != INVALID, hac, hak, tile_count);
-        if (h.best.hit != 0u) { vt = h; done = true; }
-      }
-      if (!done)
-        vt = trace_candidates(s, cslot[t], cmeta[t], ro, rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID,
-                              tile_count);
-    }
-    if (vt.in_grid && vt.best.hit != 0u) {
-      shade_hf = false;
-      HitGeom best = vt.best;
-      if (best.mat == MAT_GRASS) {
-        const int32_t csv = (int32_t)s.cam->chunk_size;
-        const i3 ov{to_i32(floorf(best.root_bmin.x / vs + 0.5f)), to_i32(floorf(best.root_bmin.y / vs + 0.5f)),
-                    to_i32(floorf(best.root_bmin.z / vs + 0.5f))};
-        const v3 hp = ro + rd * best.t;
-        const GrassCell cell = pick_grass_cell_in_chunk_with_bias(hp, rd, best.root_bmin, ov, vs, csv);
-        const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, best.t, cell.bmin_m, cell.id_vox, vs,
-                                               s.cam->voxel_params[1], s.cam->voxel_params[2]);
-        if (gh.hit) { best.t = gh.t; best.n = gh.n; }
-      }
-      const v3 hp = ro + rd * best.t;
-      const v3 hps = hp + best.n * (0.75f * vs);
-      if ((seed & SHADOW_SUBSAMPLE_MASK) == 0u) {
-        float sh = A.shadow_in[pix];
-        const v2 uvp = prev_uv_from_world(s, hp);
-        if (in_unit_square(uvp)) {
-          const int32_t ppx = clampi(to_i32(uvp.x * (float)W), 0, (int32_t)W - 1);
-          const int32_t ppy = clampi(to_i32(uvp.y * (float)H), 0, (int32_t)H - 1);
-          sh = A.shadow_in[(size_t)ppy * W + (uint32_t)ppx];
-        }
-        sh = clampf(sh, 0.0f, 1.0f);
-        const float cur = sun_transmittance_geom_only(s, hps, SUN_DIR);
-        shadow_out = mixf(sh, cur, SHADOW_TAA_ALPHA);
-      } else {
-        shadow_out = clampf(A.shadow_in[pix], 0.0f, 1.0f);
-      }
-      const v3 base_hdr = shade_hit(s, ro, rd, best, sky_up, shadow_out);
-      if (best.hit != 0u && best.mat != MAT_LIGHT && best.t <= LOCAL_LIGHT_MAX_DIST) {
-        const v3 hpl = ro + rd * best.t;
-        const v3 alb = base_albedo(best.mat, hpl, best.t);
-        local_out = gather_voxel_lights(s, hpl, best.n, best.root_bmin) * alb;
-        local_w = 1.0f;
-      }
-      const float t_scene = fmin_(best.t, FOG_MAX_DIST);
-      col = apply_fog(s, base_hdr, ro, rd, t_scene, sky_bg(rd));
-      depth = t_scene;
-      t_store = t_scene;
-      uint32_t pxy = 0u, pz = 0u, ak = 0u;
-      if (vt.anchor_valid) {
-        pxy = pack_i16x2(vt.anchor_chunk.x, vt.anchor_chunk.y);
-        pz = pack_i16x2(vt.anchor_chunk.z, 0) | 0x80000000u;
-        ak = vt.anchor_key;
-      }
-      hist = make_uint4(__float_as_uint(t_store), ak, pxy, pz);
-      rec = make_rec(best, ro, rd, vs, true);
-    }
+// Pixel of this thread in the two-tile block layout (warps of 8x4 pixels).
+__device__ __forceinline__ bool block_pixel(const FrameArgs& A, uint32_t* t, uint32_t* gx, uint32_t* gy) {
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t tiles_x = (A.iw + 7u) / 8u;
+  *t = warp >> 1;
+  const uint32_t tx = blockIdx.x * 2u + *t;
+  *gx = tx * 8u + (lane & 7u);
+  *gy = blockIdx.y * 8u + (warp & 1u) * 4u + (lane >> 3);
+  return tx < tiles_x && *gx < A.iw && *gy < A.ih;
+}
+
+__global__ void __launch_bounds__(PRIMARY_THREADS) k_primary(const __grid_constant__ FrameArgs A) {
+  __shared__ uint32_t cslot[2][TILE_CANDS];
+  __shared__ Meta cmeta[2][TILE_CANDS];
+  __shared__ uint32_t ccount[2];
+  const Scene s = make_scene(A, false);
+  stage_tiles(s, A, cslot, cmeta, ccount);
+  uint32_t t, gx, gy;
+  if (!block_pixel(A, &t, &gx, &gy)) return;
+  const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
+  const VoxTraceResult vt = primary_trace(s, A, c, cslot[t], cmeta[t], ccount[t]);
+  if (vt.in_grid && vt.best.hit != 0u) shade_voxel_pixel(s, A, c, vt.best, vt.anchor_valid, vt.anchor_key, vt.anchor_chunk);
+  else shade_far_pixel(s, A, c);
+}
+
+// PixHit: the fields of HitGeom + anchor the shading kernel needs (5 x uint4).
+__device__ __forceinline__ void store_pixhit(uint4* dst, const HitGeom& g, const VoxTraceResult& vt) {
+  dst[0] = make_uint4(__float_as_uint(g.t), __float_as_uint(g.n.x), __float_as_uint(g.n.y), __float_as_uint(g.n.z));
+  dst[1] = make_uint4(__float_as_uint(g.root_bmin.x), __float_as_uint(g.root_bmin.y), __float_as_uint(g.root_bmin.z),
+                      g.mat);
+  dst[2] = make_uint4(g.node_base, g.macro_base, g.node, __float_as_uint(g.leaf_size));
+  dst[3] = make_uint4(__float_as_uint(g.leaf_bmin.x), __float_as_uint(g.leaf_bmin.y), __float_as_uint(g.leaf_bmin.z),
+                      vt.anchor_valid ? 1u : 0u);
+  dst[4] = make_uint4(vt.anchor_key, (uint32_t)vt.anchor_chunk.x, (uint32_t)vt.anchor_chunk.y,
+                      (uint32_t)vt.anchor_chunk.z);
+}
+
+__device__ __forceinline__ void enqueue(uint32_t* q, uint32_t* counter, bool mine, uint32_t value) {
+  const uint32_t mask = __ballot_sync(0xFFFFFFFFu, mine);
+  if (!mine) return;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t leader = __ffs(mask) - 1u;
+  uint32_t base = 0u;
+  if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  q[base + __popc(mask & ((1u << lane) - 1u))] = value;
+}
+
+__global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace(const __grid_constant__ FrameArgs A) {
+  __shared__ uint32_t cslot[2][TILE_CANDS];
+  __shared__ Meta cmeta[2][TILE_CANDS];
+  __shared__ uint32_t ccount[2];
+  const Scene s = make_scene(A, false);
+  stage_tiles(s, A, cslot, cmeta, ccount);
+  uint32_t t, gx, gy;
+  const bool active = block_pixel(A, &t, &gx, &gy);
+  bool vox = false;
+  uint32_t pix = 0u;
+  if (active) {
+    const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
+    pix = (uint32_t)c.pix;
+    const VoxTraceResult vt = primary_trace(s, A, c, cslot[t], cmeta[t], ccount[t]);
+    vox = vt.in_grid && vt.best.hit != 0u;
+    if (vox) store_pixhit(A.pix_hit + (size_t)pix * 5u, vt.best, vt);
   }
-  if (shade_hf) {
-    // Heightfield, then sky (ray_main.wgsl:224-269 / 327-372 / 473-516).
-    ClipHit hf = clip_trace_heightfield(s, ro, rd, 0.0f, FOG_MAX_DIST);
-    if (hf.hit) {
-      if (hf.mat == MAT_GRASS) {
-        const v3 hp = ro + rd * hf.t;
-        const GrassCell cell = grass_cell_from_world_global(hp, rd, vs);
-        const v3 gb = V3(cell.bmin_m.x, hp.y - vs, cell.bmin_m.z);
-        const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, hf.t, gb, cell.id_vox, vs, s.cam->voxel_params[1],
-                                               s.cam->voxel_params[2]);
-        if (gh.hit) { hf.t = gh.t; hf.n = gh.n; }
-      }
-      const v3 surface = shade_clip_hit(s, ro, rd, hf, sky_up);
-      const float t_scene = fmin_(hf.t, FOG_MAX_DIST);
-      col = apply_fog(s, surface, ro, rd, t_scene, sky_bg(rd));
-      depth = t_scene;
-      t_store = t_scene;
-      HitGeom g = miss_hitgeom();
-      g.hit = 1u;
-      g.t = hf.t;
-      g.n = hf.n;
-      g.mat = hf.mat;
-      rec = make_rec(g, ro, rd, vs, false);
-    } else {
-      col = sky_color(s, rd);
-      depth = FOG_MAX_DIST;
-    }
-    hist = make_uint4(__float_as_uint(t_store), 0u, 0u, 0u);
-  }
-  A.color[pix] = make_float4(col.x, col.y, col.z, 1.0f);
-  A.depth[pix] = depth;
-  A.hist_out[pix] = hist;
-  A.shadow_out[pix] = shadow_out;
-  if (A.local) A.local[pix] = make_float4(local_out.x, local_out.y, local_out.z, local_w);
-  if (A.hits) store_rec(A.hits + pix * 2u, rec);
-  // main_local_taa (taa.wgsl:26-69) for this pixel.
-  const float4 h4 = A.local_hist_in[pix];
-  const v3 cur = local_out;
-  const bool hist_ok = !is_bad(xyz(h4));
-  const v3 hl = hist_ok ? xyz(h4) : V3s(0.0f);
-  const float conf0 = hist_ok ? h4.w : 0.0f;
-  const bool has_sample = local_w > 0.0f && !is_bad(cur);
-  const float k = has_sample ? LOCAL_TAA_ALPHA * clampf(local_w, 0.0f, 1.0f) : 0.0f;
-  const v3 ol = vmix(hl, cur, k);
-  const float conf1 = has_sample ? fmin_(1.0f, conf0 + k) : conf0;
-  A.local_hist_out[pix] = make_float4(ol.x, ol.y, ol.z, conf1);
+  enqueue(A.q_vox, &A.q_count[0], active && vox, pix);
+  enqueue(A.q_far, &A.q_count[1], active && !vox, pix);
+}
+
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_vox(const __grid_constant__ FrameArgs A) {
+  const uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x;
+  if (i >= A.q_count[0]) return;
+  const Scene s = make_scene(A, false);
+  const uint32_t pix = A.q_vox[i];
+  const PrimaryCtx c = primary_ctx(s, pix % A.iw, pix / A.iw, A.iw);
+  const uint4* src = A.pix_hit + (size_t)pix * 5u;
+  const uint4 a = src[0], b = src[1], d = src[2], e = src[3], f = src[4];
+  HitGeom g = miss_hitgeom();
+  g.hit = 1u;
+  g.t = __uint_as_float(a.x);
+  g.n = V3(__uint_as_float(a.y), __uint_as_float(a.z), __uint_as_float(a.w));
+  g.root_bmin = V3(__uint_as_float(b.x), __uint_as_float(b.y), __uint_as_float(b.z));
+  g.mat = b.w;
+  g.root_size = (float)s.cam->chunk_size * vs_(s);
+  g.node_base = d.x;
+  g.macro_base = d.y;
+  g.node = d.z;
+  g.leaf_size = __uint_as_float(d.w);
+  g.leaf_bmin = V3(__uint_as_float(e.x), __uint_as_float(e.y), __uint_as_float(e.z));
+  shade_voxel_pixel(s, A, c, g, e.w != 0u, f.x, i3{(int32_t)f.y, (int32_t)f.z, (int32_t)f.w});
+}
+
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_far(const __grid_constant__ FrameArgs A) {
+  const uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x;
+  if (i >= A.q_count[1]) return;
+  const Scene s = make_scene(A, false);
+  const uint32_t pix = A.q_far[i];
+  const PrimaryCtx c = primary_ctx(s, pix % A.iw, pix / A.iw, A.iw);
+  shade_far_pixel(s, A, c);
 }
 
 // ---------------------------------------------------------------------------

@@ -40,6 +40,7 @@ struct DevBuf {
 enum Img {
   IMG_COLOR, IMG_DEPTH, IMG_LOCAL, IMG_HIST0, IMG_HIST1, IMG_SHADOW0, IMG_SHADOW1, IMG_LHIST0, IMG_LHIST1,
   IMG_GOD0, IMG_GOD1, IMG_PRE_TAA, IMG_OUTPUT, IMG_OHIST0, IMG_OHIST1, IMG_HITS, IMG_TILE_COUNT, IMG_TILE_SLOTS,
+  IMG_PIXHIT, IMG_QVOX, IMG_QFAR, IMG_QCOUNT,
   IMG_N
 };
 
@@ -125,6 +126,12 @@ size_t img_bytes(const vxe_ctx* c, int i) {
       return tiles * 4;
     case IMG_TILE_SLOTS:
       return tiles * 4 * VXE_PRIMARY_MAX_TILE_CHUNKS;
+    case IMG_PIXHIT:
+      return in * 80;
+    case IMG_QVOX: case IMG_QFAR:
+      return in * 4;
+    case IMG_QCOUNT:
+      return 16;
     default:
       return 0;
   }
@@ -241,13 +248,27 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
   A.out_hist_in = (const float4*)c->img[IMG_OHIST0 + p].p;
   A.out_hist_out = (float4*)c->img[IMG_OHIST0 + q].p;
   A.hits = (uint4*)c->img[IMG_HITS].p;
+  A.pix_hit = (uint4*)c->img[IMG_PIXHIT].p;
+  A.q_vox = (uint32_t*)c->img[IMG_QVOX].p;
+  A.q_far = (uint32_t*)c->img[IMG_QFAR].p;
+  A.q_count = (uint32_t*)c->img[IMG_QCOUNT].p;
   const uint32_t tiles_x = (c->iw + 7) / 8, tiles_y = (c->ih + 7) / 8;
   const uint32_t tiles = tiles_x * tiles_y;
+  const uint32_t npix = c->iw * c->ih;
   using namespace vxe::dev;
   if (timed) CK(cudaEventRecord(c->ev[0], c->compute));
   k_tiles<<<(tiles + TILE_THREADS - 1) / TILE_THREADS, TILE_THREADS, 0, c->compute>>>(A);
   if (timed) CK(cudaEventRecord(c->ev[1], c->compute));
-  k_primary<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, c->compute>>>(A);
+  if (c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL) {
+    k_primary<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, c->compute>>>(A);
+  } else {
+    CK(cudaMemsetAsync(A.q_count, 0, 16, c->compute));
+    k_primary_trace<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, c->compute>>>(A);
+    // Queue lengths stay on the device: the shading grids cover every pixel
+    // and threads past the class count exit at once.
+    k_shade_vox<<<(npix + SHADE_THREADS - 1) / SHADE_THREADS, SHADE_THREADS, 0, c->compute>>>(A);
+    k_shade_far<<<(npix + SHADE_THREADS - 1) / SHADE_THREADS, SHADE_THREADS, 0, c->compute>>>(A);
+  }
   if (timed) CK(cudaEventRecord(c->ev[2], c->compute));
   k_godray<<<dim3((c->iw + POST_THREADS_X - 1) / POST_THREADS_X, (c->ih + POST_THREADS_Y - 1) / POST_THREADS_Y),
              dim3(POST_THREADS_X, POST_THREADS_Y), 0, c->compute>>>(A);

@@ -102,7 +102,7 @@ def config2(seed: int = 12345, frames: int = 64, present=(1920, 1080), render_sc
         return pos, yaw, -0.12
 
     return Scene("config2", spec, (0, 0, 0), (16, 4, 16), present, render_scale, 5, 256, frames,
-                 node_capacity=48 << 20, shift_every=16, path=at)
+                 node_capacity=12 << 20, shift_every=16, path=at)
 
 
 def features(seed: int = 777, present=(128, 80)) -> Scene:
