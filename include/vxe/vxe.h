@@ -274,6 +274,45 @@ vxe_status vxe_write_image(vxe_ctx* ctx, vxe_image img, const void* host, size_t
 /* Device error word (bounds checks / bounded waits); cleared on read. */
 vxe_status vxe_read_error_word(vxe_ctx* ctx, uint32_t* word);
 
+/* Scene buffers the caller already holds on the device, in the layouts of the
+ * structs above (used by vxe_trace_primary_hits_noalloc). */
+typedef struct vxe_scene_view {
+  const vxe_node* nodes;          /* node_count NodeGpu records                 */
+  const vxe_node_ropes* ropes;    /* node_count NodeRopesGpu records            */
+  uint64_t node_count;
+  const vxe_chunk_meta* metas;    /* chunk_capacity slots                       */
+  const uint32_t* macro_words;    /* chunk_capacity * 16                        */
+  const uint32_t* colinfo_words;  /* chunk_capacity * 2048                      */
+  uint32_t chunk_capacity;
+  uint32_t grid_cells;            /* cells of `grid`                            */
+  const uint32_t* grid;
+  const float* clip_tex;          /* clip_layers * clip_res^2 R32F, or NULL     */
+  uint32_t clip_layers, clip_res;
+} vxe_scene_view;
+
+/* No reference counterpart.  Primary hit records of one cold frame (no history
+ * hint), identical to the records vxe_render_frame writes with
+ * VXE_FLAG_HIT_RECORDS on the first frame after vxe_resize, for callers that
+ * must not allocate device memory: hosts whose frame loop runs under an
+ * allocation-free policy, and engines whose device memory all comes from their
+ * own allocator (for example buffers shared with a graphics API), where a
+ * cudaMalloc from inside a plugin is not allowed.  It allocates nothing: its
+ * scratch (per-tile candidate lists and a device error word) is a fixed
+ * file-scope device array of VXE_NOALLOC_MAX_TILES tiles, which every GPU that
+ * loads the library holds until exit.  Internal sizes whose tile count
+ * (ceil(w/8) * ceil(h/8)) exceeds the maximum return VXE_ERR_CAPACITY.
+ *   scene / cam / clip: host structs; the buffers inside `scene` and `d_hits`
+ *     (w*h records, w,h = cam->render_present_px[0..1]) are device pointers.
+ *   stream: a cudaStream_t (NULL = legacy default stream).  The call returns
+ *     after the work on `stream` has finished.
+ * The first call on a device resolves the scratch address on that device and
+ * should come before any stream capture.  Calls share the one scratch array,
+ * so calls that overlap on the GPU (different streams, threads or devices
+ * sharing a context) race; serialise them. */
+#define VXE_NOALLOC_MAX_TILES 36864u
+vxe_status vxe_trace_primary_hits_noalloc(const vxe_scene_view* scene, const vxe_camera_gpu* cam,
+                                          const vxe_clipmap_gpu* clip, vxe_hit* d_hits, void* stream);
+
 /* Diagnostic (no reference counterpart): evaluates the deterministic math
  * of detmath.h on the device for n host inputs; which = 0 sin, 1 cos, 2 exp,
  * 3 pow(x, y), 4 min(x, y), 5 max(x, y).  Used to prove host/device bit

@@ -664,3 +664,148 @@ extern "C" vxe_status vxe_debug_detmath(int which, const float* x, const float* 
   cudaFree(d);
   return st;
 }
+
+// ===========================================================================
+// Allocation-free primary hit records (vxe_trace_primary_hits_noalloc)
+// ===========================================================================
+#include <mutex>
+
+namespace {
+
+// Scratch of the allocation-free entry point: word 0 is the device error
+// word, the per-tile candidate counts start at word 64 (256 B), the 24-slot
+// lists follow.  Sized for VXE_NOALLOC_MAX_TILES tiles (3.7 MB); every device
+// that loads the library holds it until the process exits.
+constexpr size_t kNoallocCountOff = 64;
+constexpr size_t kNoallocSlotOff = kNoallocCountOff + VXE_NOALLOC_MAX_TILES;
+constexpr size_t kNoallocWords = kNoallocSlotOff + (size_t)VXE_NOALLOC_MAX_TILES * VXE_PRIMARY_MAX_TILE_CHUNKS;
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoallocWords];
+
+// In host code g_noalloc_scratch is only a stand-in symbol, not a device
+// address; the address is resolved per device with that device current.
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+uint32_t* g_noalloc_addr[kMaxDevices] = {};
+
+vxe_status noalloc_scratch(int dev, uint32_t** out) {
+  if (dev < 0 || dev >= kMaxDevices) return VXE_ERR_NO_DEVICE;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return VXE_ERR_DEVICE;
+    g_noalloc_addr[dev] = (uint32_t*)p;
+  }
+  *out = g_noalloc_addr[dev];
+  return VXE_OK;
+}
+
+// Per-pixel hit record of a cold frame: the primary trace without history,
+// then the grass refinement / heightfield fallback of main_primary
+// (ray_main.wgsl:224-269, 327-411, 473-498), as the frame pass records them.
+__global__ void __launch_bounds__(vxe::dev::PRIMARY_THREADS) k_hits_noalloc(const __grid_constant__ FrameArgs A) {
+  using namespace vxe::dev;
+  __shared__ uint32_t cslot[2][TILE_CANDS];
+  __shared__ Meta cmeta[2][TILE_CANDS];
+  __shared__ uint32_t ccount[2];
+  const Scene s = make_scene(A, false);
+  stage_tiles(s, A, cslot, cmeta, ccount);
+  uint32_t t, gx, gy;
+  if (!block_pixel(A, &t, &gx, &gy)) return;
+  const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
+  const float vs = vs_(s);
+  const v3 ro = c.ro, rd = c.rd;
+  VoxTraceResult vt{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
+  if (s.cam->chunk_count != 0u && ccount[t] != 0u)
+    vt = trace_candidates(s, cslot[t], cmeta[t], ro, rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID, ccount[t]);
+  HitRec rec = miss_rec();
+  if (vt.in_grid && vt.best.hit != 0u) {
+    HitGeom best = vt.best;
+    if (best.mat == MAT_GRASS) {
+      const i3 ov{to_i32(floorf(best.root_bmin.x / vs + 0.5f)), to_i32(floorf(best.root_bmin.y / vs + 0.5f)),
+                  to_i32(floorf(best.root_bmin.z / vs + 0.5f))};
+      const v3 hp = ro + rd * best.t;
+      const GrassCell cell = pick_grass_cell_in_chunk_with_bias(hp, rd, best.root_bmin, ov, vs, (int32_t)s.cam->chunk_size);
+      const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, best.t, cell.bmin_m, cell.id_vox, vs,
+                                             s.cam->voxel_params[1], s.cam->voxel_params[2]);
+      if (gh.hit) { best.t = gh.t; best.n = gh.n; }
+    }
+    rec = make_rec(best, ro, rd, vs, true);
+  } else {
+    ClipHit hf = clip_trace_heightfield(s, ro, rd, 0.0f, FOG_MAX_DIST);
+    if (hf.hit) {
+      if (hf.mat == MAT_GRASS) {
+        const v3 hp = ro + rd * hf.t;
+        const GrassCell cell = grass_cell_from_world_global(hp, rd, vs);
+        const v3 gb = V3(cell.bmin_m.x, hp.y - vs, cell.bmin_m.z);
+        const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, hf.t, gb, cell.id_vox, vs, s.cam->voxel_params[1],
+                                               s.cam->voxel_params[2]);
+        if (gh.hit) { hf.t = gh.t; hf.n = gh.n; }
+      }
+      HitGeom g = miss_hitgeom();
+      g.hit = 1u;
+      g.t = hf.t;
+      g.n = hf.n;
+      g.mat = hf.mat;
+      rec = make_rec(g, ro, rd, vs, false);
+    }
+  }
+  store_rec(A.hits + c.pix * 2u, rec);
+}
+
+}  // namespace
+
+extern "C" vxe_status vxe_trace_primary_hits_noalloc(const vxe_scene_view* sv, const vxe_camera_gpu* cam,
+                                                     const vxe_clipmap_gpu* clip, vxe_hit* d_hits, void* stream) {
+  using namespace vxe::dev;
+  if (!sv || !cam || !clip || !d_hits || !sv->nodes || !sv->ropes || !sv->metas || !sv->macro_words ||
+      !sv->colinfo_words || !sv->grid || sv->node_count == 0 || sv->chunk_capacity == 0 || sv->grid_cells == 0)
+    return VXE_ERR_INVALID_ARG;
+  const uint32_t iw = cam->render_present_px[0], ih = cam->render_present_px[1];
+  if (iw == 0 || ih == 0 || cam->chunk_size != 64u) return VXE_ERR_INVALID_ARG;
+  const uint64_t tiles_x = (iw + 7) / 8, tiles_y = (ih + 7) / 8;
+  if (tiles_x * tiles_y > VXE_NOALLOC_MAX_TILES) return VXE_ERR_CAPACITY;
+  if ((uint64_t)cam->grid_dims[0] * cam->grid_dims[1] * cam->grid_dims[2] > sv->grid_cells) return VXE_ERR_CAPACITY;
+  if (cam->chunk_count > sv->chunk_capacity) return VXE_ERR_CAPACITY;
+  if (clip->levels != 0 && (!sv->clip_tex || clip->levels > sv->clip_layers || clip->res != sv->clip_res))
+    return VXE_ERR_INVALID_ARG;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return VXE_ERR_NO_DEVICE;
+  uint32_t* scratch = nullptr;
+  vxe_status st = noalloc_scratch(dev, &scratch);
+  if (st != VXE_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  FrameArgs A;
+  std::memset(&A, 0, sizeof A);
+  A.cam = *cam;
+  A.clip = *clip;
+  A.nodes = (const uint4*)sv->nodes;
+  A.nodes_n = sv->node_count;
+  A.ropes = (const uint32_t*)sv->ropes;
+  A.ropes_n = sv->node_count;
+  A.metas = (const uint4*)sv->metas;
+  A.metas_n = sv->chunk_capacity;
+  A.grid = sv->grid;
+  A.grid_n = sv->grid_cells;
+  A.macro = sv->macro_words;
+  A.macro_n = (uint64_t)sv->chunk_capacity * VXE_MACRO_WORDS_PER_CHUNK;
+  A.colinfo = sv->colinfo_words;
+  A.colinfo_n = (uint64_t)sv->chunk_capacity * VXE_COLINFO_WORDS_PER_CHUNK;
+  A.clip_tex = sv->clip_tex;
+  A.clip_layers = sv->clip_tex ? sv->clip_layers : 0u;
+  A.clip_res = sv->clip_res;
+  A.err = scratch;  // word 0, cleared below: it must start at zero
+  A.iw = iw;
+  A.ih = ih;
+  A.tile_count = scratch + kNoallocCountOff;  // fully rewritten by k_tiles every call
+  A.tile_slots = scratch + kNoallocSlotOff;
+  A.hits = (uint4*)d_hits;
+  if (cudaMemsetAsync(scratch, 0, 4, s) != cudaSuccess) return VXE_ERR_DEVICE;
+  const uint32_t tiles = (uint32_t)(tiles_x * tiles_y);
+  k_tiles<<<(tiles + TILE_THREADS - 1) / TILE_THREADS, TILE_THREADS, 0, s>>>(A);
+  k_hits_noalloc<<<dim3((uint32_t)(tiles_x + 1) / 2, (uint32_t)tiles_y), PRIMARY_THREADS, 0, s>>>(A);
+  if (cudaGetLastError() != cudaSuccess) return VXE_ERR_DEVICE;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return VXE_ERR_DEVICE;
+  uint32_t word = 0;
+  if (cudaMemcpy(&word, scratch, 4, cudaMemcpyDeviceToHost) != cudaSuccess) return VXE_ERR_DEVICE;
+  return word ? VXE_ERR_BOUNDS : VXE_OK;
+}

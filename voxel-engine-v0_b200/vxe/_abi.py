@@ -130,6 +130,16 @@ class CameraParams(C.Structure):
                 ("prev_view_proj", Mat4)]
 
 
+class SceneView(C.Structure):
+    _fields_ = [("nodes", C.c_void_p), ("ropes", C.c_void_p), ("node_count", C.c_uint64), ("metas", C.c_void_p),
+                ("macro_words", C.c_void_p), ("colinfo_words", C.c_void_p), ("chunk_capacity", C.c_uint32),
+                ("grid_cells", C.c_uint32), ("grid", C.c_void_p), ("clip_tex", C.c_void_p),
+                ("clip_layers", C.c_uint32), ("clip_res", C.c_uint32)]
+
+
+NOALLOC_MAX_TILES = 36864
+
+
 # Every symbol include/vxe/vxe.h declares, with (restype, argtypes).
 P = C.POINTER
 SIGNATURES = {
@@ -157,6 +167,8 @@ SIGNATURES = {
     "vxe_write_image": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
     "vxe_read_error_word": (C.c_int, [C.c_void_p, P(C.c_uint32)]),
     "vxe_debug_detmath": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
+    "vxe_trace_primary_hits_noalloc": (C.c_int, [P(SceneView), P(CameraGpu), P(ClipmapGpu), C.c_void_p,
+                                                  C.c_void_p]),
     "vxe_build_chunk": (C.c_int, [P(WorldParams), C.c_int32, C.c_int32, C.c_int32, P(BuiltChunk)]),
     "vxe_free_chunk": (None, [P(BuiltChunk)]),
     "vxe_chunk_materials": (C.c_int, [P(WorldParams), C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),
