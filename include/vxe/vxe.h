@@ -36,7 +36,8 @@ typedef enum vxe_status {
   VXE_ERR_TIMEOUT = 4,    /* a bounded device wait gave up                      */
   VXE_ERR_DEVICE = 5,     /* CUDA runtime error                                 */
   VXE_ERR_BOUNDS = 6,     /* device-side bounds check tripped (error word set)  */
-  VXE_ERR_NO_DEVICE = 7   /* no CUDA device / extension unusable                */
+  VXE_ERR_NO_DEVICE = 7,  /* no CUDA device / extension unusable                */
+  VXE_NOT_READY = 8       /* asynchronous work still running (not an error)     */
 } vxe_status;
 
 /* ------------------------------------------------------------------------ */
@@ -245,6 +246,56 @@ vxe_status vxe_trace_rays(vxe_ctx* ctx, const float* origins, const float* dirs,
 /* Same, device pointers in and out, launched on the compute stream. */
 vxe_status vxe_trace_rays_device(vxe_ctx* ctx, const float* d_origins, const float* d_dirs,
                                  uint32_t n, float tmax, vxe_hit* d_out);
+
+/* Batched requests (no reference counterpart; the reference renders one
+ * viewport per frame and answers picking queries on the CPU).  A viewport
+ * request yields the primary hit records of a cold frame (the records
+ * vxe_render_frame writes with VXE_FLAG_HIT_RECORDS on its first frame after
+ * vxe_resize); a query request yields vxe_trace_rays records.  The world
+ * (chunk_count, grid) is the context's: write it with vxe_write_camera first. */
+enum { VXE_REQ_VIEWPORT = 0, VXE_REQ_QUERY = 1 };
+typedef struct vxe_request {
+  uint32_t kind;
+  uint32_t width, height;      /* viewport: internal size = camera.render_present_px[0..1] */
+  uint32_t ray_count;          /* query */
+  vxe_camera_gpu camera;       /* viewport pose / projection */
+  const float* d_origins;      /* query: device, 3 floats per ray */
+  const float* d_dirs;         /* query: device, 3 floats per ray */
+  float tmax;                  /* query */
+  uint32_t _pad;
+  vxe_hit* d_out;              /* device: width*height or ray_count records */
+} vxe_request;
+
+enum {
+  VXE_BATCH_PERSISTENT = 0,    /* one persistent kernel over an atomic work queue */
+  VXE_BATCH_PLAIN = 1,         /* one launch (or two) per request, back to back */
+  VXE_BATCH_GRAPH = 2          /* the persistent launch replayed from a CUDA graph */
+};
+typedef struct vxe_batch_options {
+  uint32_t tile_w, tile_h;     /* viewport work item: (tile_w * rays_per_thread) x tile_h pixels */
+  uint32_t rays_per_thread;    /* 1..4; query work item = 128 * rays_per_thread rays */
+  uint32_t mode;               /* VXE_BATCH_* */
+} vxe_batch_options;
+
+typedef struct vxe_batch_stats {
+  double ms;                   /* device time of the batch (CUDA events) */
+  uint64_t rays;               /* viewport pixels + query rays */
+  uint32_t items, tiles;
+} vxe_batch_stats;
+
+#define VXE_MAX_BATCH_REQUESTS 256u
+#define VXE_BATCH_LANES 4u
+/* Traces n (<= VXE_MAX_BATCH_REQUESTS) requests; returns when they are done
+ * (lane 0). */
+vxe_status vxe_submit_batch(vxe_ctx* ctx, const vxe_request* reqs, uint32_t n, const vxe_batch_options* opt,
+                            vxe_batch_stats* stats);
+/* Asynchronous form: each of the VXE_BATCH_LANES lanes owns a stream, staging
+ * and scratch, so up to that many batches are in flight and overlap on the
+ * device.  vxe_batch_wait(block = 0) returns VXE_NOT_READY while the lane's
+ * batch runs; after it returns VXE_OK the lane takes a new batch. */
+vxe_status vxe_submit_batch_async(vxe_ctx* ctx, uint32_t lane, const vxe_request* reqs, uint32_t n,
+                                  const vxe_batch_options* opt);
+vxe_status vxe_batch_wait(vxe_ctx* ctx, uint32_t lane, int block, vxe_batch_stats* stats);
 
 /* GpuTimingsMs (render/state/mod.rs:22-31) minus blit; CUDA events of the last
  * frame.  local_taa and composite_taa are fused into primary / composite and

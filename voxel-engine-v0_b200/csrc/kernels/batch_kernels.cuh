@@ -1,0 +1,244 @@
+// batch_kernels.cuh -- many uneven requests traced by one persistent kernel.
+//
+// A batch mixes viewport requests (primary hit records of a cold frame, the
+// records vxe_render_frame writes on its first frame after vxe_resize) and
+// ray-query batches (voxel geometry only, as vxe_trace_rays).  Work is cut
+// into items:
+//   viewport  a rect of (tile_w * rays_per_thread) x tile_h pixels,
+//   query     128 * rays_per_thread rays,
+// numbered in request order.  Every warp of a grid sized to fill the GPU pops
+// items from one atomic counter until the batch is drained, so small and large
+// requests share the machine with no per-request launch and no tail between
+// requests.  Logical 8x8 candidate tiles stay per viewport pixel (x/8, y/8),
+// independent of the item shape, so results do not depend on the tuning.
+// The batch sizes live in a device-side header: one captured CUDA graph
+// serves every batch that fits the allocated capacities.
+#pragma once
+
+#include "frame_kernels.cuh"
+
+namespace vxe {
+namespace dev {
+
+struct BatchReq {  // 64 B
+  uint32_t kind;        // 0 viewport, 1 query
+  uint32_t w, h;        // viewport size; w = ray count for queries
+  uint32_t tiles_x;     // viewport: logical 8x8 tiles per row
+  uint32_t tile_base;   // viewport: first tile in the batch tile arrays
+  uint32_t item_begin;  // first work item of this request
+  uint32_t items_x;     // viewport: items per row
+  uint32_t cam;         // index into the camera array
+  const float* o;       // query origins (3 floats per ray)
+  const float* d;       // query directions
+  uint4* out;           // 2 x uint4 per record
+  float tmax;
+  uint32_t _pad;
+};
+
+struct BatchHeader {
+  uint32_t n_reqs, total_tiles, n_items, tile_w, tile_h, rpt, tile_reqs, _pad;
+};
+
+struct BatchArgs {
+  vxe_clipmap_gpu clip;
+  const uint4* nodes;
+  uint64_t nodes_n;
+  const uint32_t* ropes;
+  uint64_t ropes_n;
+  const uint4* metas;
+  uint64_t metas_n;
+  const uint32_t* grid;
+  uint64_t grid_n;
+  const uint32_t* macro;
+  uint64_t macro_n;
+  const uint32_t* colinfo;
+  uint64_t colinfo_n;
+  const float* clip_tex;
+  uint32_t clip_layers, clip_res;
+  uint32_t* err;
+  const BatchHeader* hdr;
+  const BatchReq* reqs;
+  const vxe_camera_gpu* cams;
+  uint32_t* tile_count;
+  uint32_t* tile_slots;
+  uint32_t* head;       // [0] item counter, [1] tile counter
+  uint32_t req_first;   // plain mode: the one request a launch serves
+  uint32_t plain;       // 1: item = blockIdx-derived, no queue
+};
+
+constexpr int BATCH_THREADS = 128;
+constexpr int MAX_BATCH_REQS = 1024;
+
+__device__ __forceinline__ Scene batch_scene(const BatchArgs& B, const vxe_camera_gpu* cam) {
+  Scene s;
+  s.cam = cam;
+  s.clip = &B.clip;
+  s.nodes = B.nodes;
+  s.nodes_n = B.nodes_n;
+  s.ropes = B.ropes;
+  s.ropes_n = B.ropes_n;
+  s.metas = B.metas;
+  s.metas_n = B.metas_n;
+  s.grid = B.grid;
+  s.grid_n = B.grid_n;
+  s.macro = B.macro;
+  s.macro_n = B.macro_n;
+  s.colinfo = B.colinfo;
+  s.colinfo_n = B.colinfo_n;
+  s.clip_tex = B.clip_tex;
+  s.clip_layers = B.clip_layers;
+  s.clip_res = B.clip_res;
+  s.err = B.err;
+  return s;
+}
+
+// Last request whose first element (item or tile, via `key`) is <= x.
+template <class K>
+__device__ __forceinline__ uint32_t find_req(const BatchReq* reqs, uint32_t n, uint32_t x, K key) {
+  uint32_t lo = 0, hi = n;  // invariant: key(reqs[lo]) <= x
+  while (hi - lo > 1u) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (key(reqs[mid]) <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Cold-frame primary hit record of one viewport pixel: voxel trace without a
+// history hint, then main_primary's grass refinement or heightfield fallback.
+__device__ __noinline__ HitRec viewport_pixel_hit(const Scene& s, const uint32_t* tile_count,
+                                                  const uint32_t* tile_slots, uint32_t tiles_x, uint32_t gx,
+                                                  uint32_t gy) {
+  const float vs = vs_(s);
+  const v3 ro = cam_pos(s);
+  const v3 rd = ray_dir_from_pixel(s, V2((float)gx + 0.5f, (float)gy + 0.5f));
+  const size_t tile = (size_t)(gy >> 3) * tiles_x + (gx >> 3);
+  const uint32_t cnt = tile_count[tile];
+  VoxTraceResult vt{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
+  if (s.cam->chunk_count != 0u && cnt != 0u)
+    vt = trace_candidates(s, tile_slots + tile * TILE_CANDS, nullptr, ro, rd, 0.0f, FOG_MAX_DIST, false,
+                          i3{0, 0, 0}, INVALID, cnt);
+  if (vt.in_grid && vt.best.hit != 0u) {
+    HitGeom best = vt.best;
+    if (best.mat == MAT_GRASS) {
+      const i3 ov{to_i32(floorf(best.root_bmin.x / vs + 0.5f)), to_i32(floorf(best.root_bmin.y / vs + 0.5f)),
+                  to_i32(floorf(best.root_bmin.z / vs + 0.5f))};
+      const v3 hp = ro + rd * best.t;
+      const GrassCell cell =
+          pick_grass_cell_in_chunk_with_bias(hp, rd, best.root_bmin, ov, vs, (int32_t)s.cam->chunk_size);
+      const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, best.t, cell.bmin_m, cell.id_vox, vs,
+                                             s.cam->voxel_params[1], s.cam->voxel_params[2]);
+      if (gh.hit) { best.t = gh.t; best.n = gh.n; }
+    }
+    return make_rec(best, ro, rd, vs, true);
+  }
+  ClipHit hf = clip_trace_heightfield(s, ro, rd, 0.0f, FOG_MAX_DIST);
+  if (!hf.hit) return miss_rec();
+  if (hf.mat == MAT_GRASS) {
+    const v3 hp = ro + rd * hf.t;
+    const GrassCell cell = grass_cell_from_world_global(hp, rd, vs);
+    const v3 gb = V3(cell.bmin_m.x, hp.y - vs, cell.bmin_m.z);
+    const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, hf.t, gb, cell.id_vox, vs, s.cam->voxel_params[1],
+                                           s.cam->voxel_params[2]);
+    if (gh.hit) { hf.t = gh.t; hf.n = gh.n; }
+  }
+  HitGeom g = miss_hitgeom();
+  g.hit = 1u;
+  g.t = hf.t;
+  g.n = hf.n;
+  g.mat = hf.mat;
+  return make_rec(g, ro, rd, vs, false);
+}
+
+// Persistent candidate-tile builder over every viewport tile of the batch.
+__global__ void __launch_bounds__(TILE_THREADS) k_batch_tiles(const __grid_constant__ BatchArgs B) {
+  __shared__ uint32_t sl[MAX_TILE_CHUNKS][TILE_THREADS];
+  __shared__ float en[MAX_TILE_CHUNKS][TILE_THREADS];
+  const BatchHeader H = *B.hdr;
+  const uint32_t lane = threadIdx.x;
+  const uint32_t first = B.plain ? B.req_first : 0u;
+  const uint32_t nreq = B.plain ? 1u : H.tile_reqs;
+  const uint32_t total = B.plain ? B.reqs[first].tiles_x * ((B.reqs[first].h + 7u) / 8u) : H.total_tiles;
+  for (uint32_t t = blockIdx.x * TILE_THREADS + lane; t < total; t += gridDim.x * TILE_THREADS) {
+    const uint32_t gt = B.plain ? B.reqs[first].tile_base + t : t;
+    const uint32_t r = B.plain ? first : find_req(B.reqs, nreq, gt, [](const BatchReq& q) { return q.tile_base; });
+    const BatchReq q = B.reqs[r];
+    const Scene s = batch_scene(B, &B.cams[q.cam]);
+    const uint32_t local = gt - q.tile_base;
+    build_tile_list(s, local % q.tiles_x, local / q.tiles_x, lane, sl, en, &B.tile_count[gt],
+                    &B.tile_slots[(size_t)gt * TILE_CANDS]);
+  }
+}
+
+__device__ __forceinline__ void store_rec_at(uint4* out, size_t i, const HitRec& h) { store_rec(out + i * 2u, h); }
+
+// Processes one work item with the calling warp.
+__device__ __forceinline__ void batch_item(const BatchArgs& B, const BatchHeader& H, const BatchReq& q,
+                                           const Scene& s, uint32_t local, uint32_t lane) {
+  if (q.kind == 0u) {
+    const uint32_t rw = H.tile_w * H.rpt, rh = H.tile_h;
+    const uint32_t x0 = (local % q.items_x) * rw, y0 = (local / q.items_x) * rh;
+    for (uint32_t k = lane; k < rw * rh; k += 32u) {
+      const uint32_t gx = x0 + k % rw, gy = y0 + k / rw;
+      if (gx >= q.w || gy >= q.h) continue;
+      const HitRec h = viewport_pixel_hit(s, B.tile_count + q.tile_base, B.tile_slots + (size_t)q.tile_base * TILE_CANDS,
+                                          q.tiles_x, gx, gy);
+      store_rec_at(q.out, (size_t)gy * q.w + gx, h);
+    }
+  } else {
+    const uint32_t per = 128u * H.rpt;
+    const uint32_t r0 = local * per;
+    for (uint32_t k = lane; k < per; k += 32u) {
+      const uint32_t i = r0 + k;
+      if (i >= q.w) break;
+      const v3 ro = V3(q.o[3 * (size_t)i], q.o[3 * (size_t)i + 1], q.o[3 * (size_t)i + 2]);
+      const v3 rd = V3(q.d[3 * (size_t)i], q.d[3 * (size_t)i + 1], q.d[3 * (size_t)i + 2]);
+      store_rec_at(q.out, i, trace_query_ray(s, ro, rd, q.tmax));
+    }
+  }
+}
+
+// The persistent work-queue kernel (plain = 0) or one request per launch
+// with one warp per item (plain = 1, the per-request baseline).
+__global__ void __launch_bounds__(BATCH_THREADS) k_batch_trace(const __grid_constant__ BatchArgs B) {
+  __shared__ vxe_camera_gpu wcam[BATCH_THREADS / 32];
+  __shared__ uint32_t wcam_id[BATCH_THREADS / 32];
+  const BatchHeader H = *B.hdr;
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  if (lane == 0) wcam_id[warp] = 0xFFFFFFFFu;
+  __syncwarp();
+  auto load_cam = [&](uint32_t cam) {
+    if (wcam_id[warp] != cam) {
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(&B.cams[cam]);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(&wcam[warp]);
+      for (uint32_t k = lane; k < sizeof(vxe_camera_gpu) / 4u; k += 32u) dst[k] = src[k];
+      __syncwarp();
+      if (lane == 0) wcam_id[warp] = cam;
+      __syncwarp();
+    }
+  };
+  if (B.plain) {
+    const BatchReq q = B.reqs[B.req_first];
+    const uint32_t local = blockIdx.x * (BATCH_THREADS / 32) + warp;
+    const uint32_t n_local = (B.req_first + 1 < H.n_reqs ? B.reqs[B.req_first + 1].item_begin : H.n_items) - q.item_begin;
+    if (local >= n_local) return;
+    load_cam(q.cam);
+    const Scene s = batch_scene(B, &wcam[warp]);
+    batch_item(B, H, q, s, local, lane);
+    return;
+  }
+  for (;;) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(&B.head[0], 1u);
+    item = __shfl_sync(0xFFFFFFFFu, item, 0);
+    if (item >= H.n_items) break;
+    const uint32_t r = find_req(B.reqs, H.n_reqs, item, [](const BatchReq& q) { return q.item_begin; });
+    const BatchReq q = B.reqs[r];
+    load_cam(q.cam);
+    const Scene s = batch_scene(B, &wcam[warp]);
+    batch_item(B, H, q, s, item - q.item_begin, lane);
+  }
+}
+
+}  // namespace dev
+}  // namespace vxe

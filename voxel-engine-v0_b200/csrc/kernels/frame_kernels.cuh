@@ -97,16 +97,14 @@ __device__ __forceinline__ Scene make_scene(const FrameArgs& A, bool godray) {
 // Tile candidate lists
 // ---------------------------------------------------------------------------
 constexpr int TILE_THREADS = 32;
+#define TILE_THREADS_DECL 32
 
-__global__ void __launch_bounds__(TILE_THREADS) k_tiles(const __grid_constant__ FrameArgs A) {
-  __shared__ uint32_t sl[MAX_TILE_CHUNKS][TILE_THREADS];
-  __shared__ float en[MAX_TILE_CHUNKS][TILE_THREADS];
-  const uint32_t lane = threadIdx.x;
-  const uint32_t tiles_x = (A.iw + 7u) / 8u, tiles_y = (A.ih + 7u) / 8u;
-  const uint32_t tile = blockIdx.x * TILE_THREADS + lane;
-  if (tile >= tiles_x * tiles_y) return;
-  const Scene s = make_scene(A, false);
-  const uint32_t tx = tile % tiles_x, ty = tile / tiles_x;
+// Candidate list of logical tile (tx, ty) for this lane; `sl` / `en` are the
+// block's [MAX_TILE_CHUNKS][TILE_THREADS] shared scratch.  Writes the clamped
+// count and 24 slots (INVALID-padded) to out_count / out_slots.
+__device__ __noinline__ void build_tile_list(const Scene& s, uint32_t tx, uint32_t ty, uint32_t lane,
+                                             uint32_t (*sl)[TILE_THREADS_DECL], float (*en)[TILE_THREADS_DECL],
+                                             uint32_t* out_count, uint32_t* out_slots) {
   uint32_t count = 0;
   if (s.cam->chunk_count != 0u) {
     const v2 base = V2((float)(tx * TILE_SIZE), (float)(ty * TILE_SIZE));
@@ -151,8 +149,20 @@ __global__ void __launch_bounds__(TILE_THREADS) k_tiles(const __grid_constant__ 
       }
     }
   }
-  A.tile_count[tile] = limit;
-  for (uint32_t i = 0; i < TILE_CANDS; ++i) A.tile_slots[(size_t)tile * TILE_CANDS + i] = i < limit ? sl[i][lane] : INVALID;
+  *out_count = limit;
+  for (uint32_t i = 0; i < TILE_CANDS; ++i) out_slots[i] = i < limit ? sl[i][lane] : INVALID;
+}
+
+__global__ void __launch_bounds__(TILE_THREADS) k_tiles(const __grid_constant__ FrameArgs A) {
+  __shared__ uint32_t sl[MAX_TILE_CHUNKS][TILE_THREADS];
+  __shared__ float en[MAX_TILE_CHUNKS][TILE_THREADS];
+  const uint32_t lane = threadIdx.x;
+  const uint32_t tiles_x = (A.iw + 7u) / 8u, tiles_y = (A.ih + 7u) / 8u;
+  const uint32_t tile = blockIdx.x * TILE_THREADS + lane;
+  if (tile >= tiles_x * tiles_y) return;
+  const Scene s = make_scene(A, false);
+  build_tile_list(s, tile % tiles_x, tile / tiles_x, lane, sl, en, &A.tile_count[tile],
+                  &A.tile_slots[(size_t)tile * TILE_CANDS]);
 }
 
 // trace_scene_voxels_candidates (chunk_trace.wgsl:1177-1265) over a tile list
@@ -183,7 +193,7 @@ __device__ VoxTraceResult trace_candidates(const Scene& s, const uint32_t* cslot
   for (uint32_t i = 0; i < maxc; ++i) {
     const uint32_t slot = cslot[i];
     if (slot == INVALID || slot >= s.cam->chunk_count) continue;
-    const Meta ch = cmeta[i];
+    const Meta ch = cmeta ? cmeta[i] : meta_at(s, slot);  // staged in shared memory, or read through L1
     if (ch.macro_empty != 0u) continue;
     const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vsz;
     const v2 rt = intersect_aabb(ro, rd, rb, rb + V3s(rs));

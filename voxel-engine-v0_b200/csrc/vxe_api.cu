@@ -24,6 +24,7 @@
 #include <string>
 #include <vector>
 
+#include "kernels/batch_kernels.cuh"
 #include "kernels/frame_kernels.cuh"
 #include "vxe/vxe.h"
 
@@ -42,6 +43,19 @@ enum Img {
   IMG_GOD0, IMG_GOD1, IMG_PRE_TAA, IMG_OUTPUT, IMG_OHIST0, IMG_OHIST1, IMG_HITS, IMG_TILE_COUNT, IMG_TILE_SLOTS,
   IMG_PIXHIT, IMG_QVOX, IMG_QFAR, IMG_QCOUNT,
   IMG_N
+};
+
+struct BatchLane {
+  cudaStream_t stream = nullptr;
+  DevBuf hdr, reqs, cams, tile_count, tile_slots, head;
+  void* stage = nullptr;  // pinned: header | requests | cameras
+  cudaGraphExec_t graph = nullptr;
+  uint32_t graph_key[6] = {0, 0, 0, 0, 0, 0};
+  vxe_clipmap_gpu graph_clip{};  // clipmap uniform baked into the captured launches
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  bool busy = false;
+  uint64_t rays = 0;
+  uint32_t items = 0, tiles = 0;
 };
 
 }  // namespace
@@ -66,6 +80,11 @@ struct vxe_ctx {
   vxe_clipmap_gpu clip{};
   // query scratch
   DevBuf q_in, q_out;
+  // batches: independent lanes (stream, pinned staging, descriptors, tile
+  // lists, queue heads, captured graph) so several batches can be in flight
+  BatchLane lanes[VXE_BATCH_LANES];
+  int b_trace_grid = 0, b_tile_grid = 0;
+  bool upload_recorded = false;
 };
 
 namespace {
@@ -219,10 +238,7 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
     return fail(c, VXE_ERR_CAPACITY, "clipmap levels exceed allocated layers");
   if (c->clip.levels != 0 && c->clip.res != c->cfg.clip_res)
     return fail(c, VXE_ERR_INVALID_ARG, "clipmap res %u != allocated %u", c->clip.res, c->cfg.clip_res);
-  if (c->upload_pending) {
-    CK(cudaStreamWaitEvent(c->compute, c->upload_done, 0));
-    c->upload_pending = false;
-  }
+  if (c->upload_recorded) CK(cudaStreamWaitEvent(c->compute, c->upload_done, 0));
   FrameArgs A;
   fill_scene_args(c, A);
   const int p = c->ping, q = 1 - c->ping;
@@ -347,6 +363,15 @@ void vxe_destroy(vxe_ctx* c) {
   for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword,
                   &c->q_in, &c->q_out})
     release(*b);
+  for (auto& L : c->lanes) {
+    if (L.stream) cudaStreamSynchronize(L.stream);
+    for (auto* b : {&L.hdr, &L.reqs, &L.cams, &L.tile_count, &L.tile_slots, &L.head}) release(*b);
+    if (L.graph) cudaGraphExecDestroy(L.graph);
+    if (L.stage) cudaFreeHost(L.stage);
+    for (auto& e : L.ev)
+      if (e) cudaEventDestroy(e);
+    if (L.stream) cudaStreamDestroy(L.stream);
+  }
   for (auto& b : c->img) release(b);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
@@ -434,6 +459,7 @@ vxe_status vxe_upload_chunks(vxe_ctx* c, const vxe_chunk_upload* ups, uint32_t n
   }
   CK(cudaEventRecord(c->upload_done, c->upload));
   c->upload_pending = true;
+  c->upload_recorded = true;
   return VXE_OK;
 }
 
@@ -444,6 +470,7 @@ vxe_status vxe_write_meta(vxe_ctx* c, uint32_t first, const vxe_chunk_meta* meta
   if (n) CK(cudaMemcpyAsync((char*)c->metas.p + (size_t)first * 48, metas, (size_t)n * 48, cudaMemcpyHostToDevice, c->upload));
   CK(cudaEventRecord(c->upload_done, c->upload));
   c->upload_pending = true;
+  c->upload_recorded = true;
   return VXE_OK;
 }
 
@@ -454,6 +481,7 @@ vxe_status vxe_write_grid(vxe_ctx* c, const uint32_t* grid, uint32_t n) {
   if (n) CK(cudaMemcpyAsync(c->grid.p, grid, (size_t)n * 4, cudaMemcpyHostToDevice, c->upload));
   CK(cudaEventRecord(c->upload_done, c->upload));
   c->upload_pending = true;
+  c->upload_recorded = true;
   return VXE_OK;
 }
 
@@ -479,6 +507,7 @@ vxe_status vxe_write_clipmap(vxe_ctx* c, const vxe_clipmap_gpu* params, const vx
   c->clip = *params;
   CK(cudaEventRecord(c->upload_done, c->upload));
   c->upload_pending = true;
+  c->upload_recorded = true;
   return VXE_OK;
 }
 
@@ -592,10 +621,7 @@ vxe_status vxe_trace_rays_device(vxe_ctx* c, const float* d_o, const float* d_d,
   if (!c || (n && (!d_o || !d_d || !d_out))) return fail(c, VXE_ERR_INVALID_ARG, "null ray buffers");
   if (n == 0) return VXE_OK;
   cudaSetDevice(c->device);
-  if (c->upload_pending) {
-    CK(cudaStreamWaitEvent(c->compute, c->upload_done, 0));
-    c->upload_pending = false;
-  }
+  if (c->upload_recorded) CK(cudaStreamWaitEvent(c->compute, c->upload_done, 0));
   QueryArgs Q;
   fill_query_args(c, Q);
   Q.origins = d_o;
@@ -626,6 +652,257 @@ vxe_status vxe_trace_rays(vxe_ctx* c, const float* o, const float* d, uint32_t n
   CK(cudaStreamSynchronize(c->compute));
   return VXE_OK;
 }
+
+}  // extern "C"
+
+namespace {
+
+using vxe::dev::BatchArgs;
+using vxe::dev::BatchHeader;
+using vxe::dev::BatchReq;
+
+constexpr size_t kStageHdr = 0, kStageReqs = 64,
+                 kStageCams = kStageReqs + (size_t)VXE_MAX_BATCH_REQUESTS * sizeof(BatchReq),
+                 kStageBytes = kStageCams + (size_t)(VXE_MAX_BATCH_REQUESTS + 1) * sizeof(vxe_camera_gpu);
+
+vxe_status lane_resources(vxe_ctx* c, BatchLane& L, uint32_t tiles) {
+  vxe_status st;
+  if (!L.stage) {
+    if (cudaMallocHost(&L.stage, kStageBytes) != cudaSuccess) return fail(c, VXE_ERR_OOM, "pinned staging");
+    CK(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
+    if ((st = alloc(c, L.hdr, sizeof(BatchHeader))) != VXE_OK) return st;
+    if ((st = alloc(c, L.reqs, (size_t)VXE_MAX_BATCH_REQUESTS * sizeof(BatchReq))) != VXE_OK) return st;
+    if ((st = alloc(c, L.cams, (size_t)(VXE_MAX_BATCH_REQUESTS + 1) * sizeof(vxe_camera_gpu))) != VXE_OK) return st;
+    if ((st = alloc(c, L.head, 16)) != VXE_OK) return st;
+    for (auto& e : L.ev) CK(cudaEventCreate(&e));
+  }
+  if (c->b_trace_grid == 0) {
+    // Persistent grids: every SM filled to the kernels' occupancy limit.
+    int sms = 0, tb = 0, lb = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tb, vxe::dev::k_batch_trace, vxe::dev::BATCH_THREADS, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lb, vxe::dev::k_batch_tiles, vxe::dev::TILE_THREADS, 0));
+    c->b_trace_grid = sms * std::max(tb, 1);
+    c->b_tile_grid = sms * std::max(lb, 1);
+  }
+  if ((size_t)tiles * 4 > L.tile_count.bytes) {
+    // grow by 1.5x so a stream of slightly larger batches does not reallocate every time
+    const size_t cap = std::max<size_t>((size_t)tiles + tiles / 2, 4096);
+    if ((st = alloc(c, L.tile_count, cap * 4)) != VXE_OK) return st;
+    if ((st = alloc(c, L.tile_slots, cap * 4 * VXE_PRIMARY_MAX_TILE_CHUNKS)) != VXE_OK) return st;
+    if (L.graph) {
+      cudaGraphExecDestroy(L.graph);
+      L.graph = nullptr;
+    }
+  }
+  return VXE_OK;
+}
+
+BatchArgs batch_args(const vxe_ctx* c, const BatchLane& L) {
+  BatchArgs B;
+  std::memset(&B, 0, sizeof B);
+  B.clip = c->clip;
+  B.nodes = (const uint4*)c->nodes.p;
+  B.nodes_n = c->cfg.node_capacity;
+  B.ropes = (const uint32_t*)c->ropes.p;
+  B.ropes_n = c->cfg.node_capacity;
+  B.metas = (const uint4*)c->metas.p;
+  B.metas_n = c->cfg.chunk_capacity;
+  B.grid = (const uint32_t*)c->grid.p;
+  B.grid_n = c->cfg.grid_capacity;
+  B.macro = (const uint32_t*)c->macro.p;
+  B.macro_n = (uint64_t)c->cfg.chunk_capacity * VXE_MACRO_WORDS_PER_CHUNK;
+  B.colinfo = (const uint32_t*)c->colinfo.p;
+  B.colinfo_n = (uint64_t)c->cfg.chunk_capacity * VXE_COLINFO_WORDS_PER_CHUNK;
+  B.clip_tex = (const float*)c->clip_tex.p;
+  B.clip_layers = c->cfg.clip_levels;
+  B.clip_res = c->cfg.clip_res;
+  B.err = (uint32_t*)c->errword.p;
+  B.hdr = (const BatchHeader*)L.hdr.p;
+  B.reqs = (const BatchReq*)L.reqs.p;
+  B.cams = (const vxe_camera_gpu*)L.cams.p;
+  B.tile_count = (uint32_t*)L.tile_count.p;
+  B.tile_slots = (uint32_t*)L.tile_slots.p;
+  B.head = (uint32_t*)L.head.p;
+  return B;
+}
+
+vxe_status launch_persistent(vxe_ctx* c, BatchLane& L, const BatchArgs& B) {
+  using namespace vxe::dev;
+  CK(cudaMemcpyAsync(L.hdr.p, (char*)L.stage + kStageHdr, sizeof(BatchHeader), cudaMemcpyHostToDevice, L.stream));
+  CK(cudaMemcpyAsync(L.reqs.p, (char*)L.stage + kStageReqs, kStageCams - kStageReqs, cudaMemcpyHostToDevice,
+                     L.stream));
+  CK(cudaMemcpyAsync(L.cams.p, (char*)L.stage + kStageCams, kStageBytes - kStageCams, cudaMemcpyHostToDevice,
+                     L.stream));
+  CK(cudaMemsetAsync(L.head.p, 0, 16, L.stream));
+  k_batch_tiles<<<c->b_tile_grid, TILE_THREADS, 0, L.stream>>>(B);
+  k_batch_trace<<<c->b_trace_grid, BATCH_THREADS, 0, L.stream>>>(B);
+  CK(cudaGetLastError());
+  return VXE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* reqs, uint32_t n,
+                                  const vxe_batch_options* opt) {
+  using namespace vxe::dev;
+  if (!c || (n && !reqs) || !opt) return fail(c, VXE_ERR_INVALID_ARG, "null batch arguments");
+  if (lane >= VXE_BATCH_LANES) return fail(c, VXE_ERR_INVALID_ARG, "lane %u >= %u", lane, VXE_BATCH_LANES);
+  BatchLane& L = c->lanes[lane];
+  if (L.busy) return fail(c, VXE_ERR_INVALID_ARG, "lane %u still has a batch in flight", lane);
+  if (n > VXE_MAX_BATCH_REQUESTS) return fail(c, VXE_ERR_CAPACITY, "batch of %u requests > %u", n, VXE_MAX_BATCH_REQUESTS);
+  const uint32_t tw = opt->tile_w, th = opt->tile_h, rpt = opt->rays_per_thread;
+  if (tw == 0 || th == 0 || rpt == 0 || rpt > 8 || tw * th * rpt > 4096 || opt->mode > VXE_BATCH_GRAPH)
+    return fail(c, VXE_ERR_INVALID_ARG, "bad batch options");
+  cudaSetDevice(c->device);
+  // Host-side descriptors (requests keep their order; tiles and items are
+  // numbered in request order so the device finds a request by binary search).
+  uint32_t tiles = 0, items = 0;
+  uint64_t rays = 0;
+  std::vector<BatchReq> R(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    const vxe_request& q = reqs[i];
+    BatchReq& r = R[i];
+    std::memset(&r, 0, sizeof r);
+    r.kind = q.kind;
+    r.out = (uint4*)q.d_out;
+    r.tile_base = tiles;
+    r.item_begin = items;
+    if (!q.d_out) return fail(c, VXE_ERR_INVALID_ARG, "request %u has no output", i);
+    if (q.kind == VXE_REQ_VIEWPORT) {
+      if (q.width == 0 || q.height == 0 || q.camera.render_present_px[0] != q.width ||
+          q.camera.render_present_px[1] != q.height)
+        return fail(c, VXE_ERR_INVALID_ARG, "viewport %u size / camera mismatch", i);
+      r.w = q.width;
+      r.h = q.height;
+      r.tiles_x = (q.width + 7) / 8;
+      r.items_x = (q.width + tw * rpt - 1) / (tw * rpt);
+      r.cam = i + 1;
+      tiles += r.tiles_x * ((q.height + 7) / 8);
+      items += r.items_x * ((q.height + th - 1) / th);
+      rays += (uint64_t)q.width * q.height;
+    } else if (q.kind == VXE_REQ_QUERY) {
+      if (q.ray_count == 0 || !q.d_origins || !q.d_dirs) return fail(c, VXE_ERR_INVALID_ARG, "query %u empty", i);
+      r.w = q.ray_count;
+      r.o = q.d_origins;
+      r.d = q.d_dirs;
+      r.tmax = q.tmax;
+      r.cam = 0;
+      items += (q.ray_count + 128 * rpt - 1) / (128 * rpt);
+      rays += q.ray_count;
+    } else {
+      return fail(c, VXE_ERR_INVALID_ARG, "request %u kind %u", i, q.kind);
+    }
+  }
+  vxe_status st = lane_resources(c, L, tiles);
+  if (st != VXE_OK) return st;
+  if (c->upload_recorded) CK(cudaStreamWaitEvent(L.stream, c->upload_done, 0));
+  BatchHeader H{n, tiles, items, tw, th, rpt, n, 0};
+  std::memcpy((char*)L.stage + kStageHdr, &H, sizeof H);
+  if (n) std::memcpy((char*)L.stage + kStageReqs, R.data(), n * sizeof(BatchReq));
+  auto* cams = (vxe_camera_gpu*)((char*)L.stage + kStageCams);
+  cams[0] = c->cam;  // world camera for queries
+  for (uint32_t i = 0; i < n; ++i) {
+    if (reqs[i].kind != VXE_REQ_VIEWPORT) continue;
+    vxe_camera_gpu v = reqs[i].camera;
+    // the world is the context's
+    v.chunk_size = c->cam.chunk_size;
+    v.chunk_count = c->cam.chunk_count;
+    for (int k = 0; k < 4; ++k) {
+      v.grid_origin_chunk[k] = c->cam.grid_origin_chunk[k];
+      v.grid_dims[k] = c->cam.grid_dims[k];
+    }
+    cams[i + 1] = v;
+  }
+  BatchArgs B = batch_args(c, L);
+  CK(cudaEventRecord(L.ev[0], L.stream));
+  if (opt->mode == VXE_BATCH_PLAIN) {
+    CK(cudaMemcpyAsync(L.hdr.p, (char*)L.stage + kStageHdr, sizeof H, cudaMemcpyHostToDevice, L.stream));
+    CK(cudaMemcpyAsync(L.reqs.p, (char*)L.stage + kStageReqs, n * sizeof(BatchReq), cudaMemcpyHostToDevice, L.stream));
+    CK(cudaMemcpyAsync(L.cams.p, cams, (n + 1) * sizeof(vxe_camera_gpu), cudaMemcpyHostToDevice, L.stream));
+    B.plain = 1;
+    for (uint32_t i = 0; i < n; ++i) {
+      B.req_first = i;
+      const uint32_t n_items = (i + 1 < n ? R[i + 1].item_begin : items) - R[i].item_begin;
+      if (R[i].kind == VXE_REQ_VIEWPORT) {
+        const uint32_t t = R[i].tiles_x * ((R[i].h + 7) / 8);
+        k_batch_tiles<<<(t + TILE_THREADS - 1) / TILE_THREADS, TILE_THREADS, 0, L.stream>>>(B);
+      }
+      k_batch_trace<<<(n_items + BATCH_THREADS / 32 - 1) / (BATCH_THREADS / 32), BATCH_THREADS, 0, L.stream>>>(B);
+    }
+    CK(cudaGetLastError());
+  } else if (opt->mode == VXE_BATCH_PERSISTENT) {
+    if ((st = launch_persistent(c, L, B)) != VXE_OK) return st;
+  } else {
+    // Captured once per tile-buffer allocation and clipmap uniform; later
+    // batches only rewrite the pinned staging the graph's copies read.
+    const uint32_t key[6] = {(uint32_t)(uintptr_t)L.tile_count.p, (uint32_t)((uintptr_t)L.tile_count.p >> 32),
+                             (uint32_t)c->cfg.clip_levels, c->clip.levels, c->clip.res, 1u};
+    const bool same = L.graph != nullptr && std::memcmp(key, L.graph_key, sizeof key) == 0 &&
+                      std::memcmp(&L.graph_clip, &B.clip, sizeof B.clip) == 0;
+    if (!same) {
+      if (L.graph) {
+        cudaGraphExecDestroy(L.graph);
+        L.graph = nullptr;
+      }
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(L.stream, cudaStreamCaptureModeThreadLocal));
+      st = launch_persistent(c, L, B);
+      cudaError_t e = cudaStreamEndCapture(L.stream, &g);
+      if (st != VXE_OK) return st;
+      if (e != cudaSuccess) return fail(c, VXE_ERR_DEVICE, "graph capture: %s", cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&L.graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return fail(c, VXE_ERR_DEVICE, "graph instantiate: %s", cudaGetErrorString(e));
+      std::memcpy(L.graph_key, key, sizeof key);
+      L.graph_clip = B.clip;
+    }
+    CK(cudaGraphLaunch(L.graph, L.stream));
+  }
+  CK(cudaEventRecord(L.ev[1], L.stream));
+  L.busy = true;
+  L.rays = rays;
+  L.items = items;
+  L.tiles = tiles;
+  return VXE_OK;
+}
+
+vxe_status vxe_batch_wait(vxe_ctx* c, uint32_t lane, int block, vxe_batch_stats* stats) {
+  if (!c || lane >= VXE_BATCH_LANES) return fail(c, VXE_ERR_INVALID_ARG, "bad lane");
+  BatchLane& L = c->lanes[lane];
+  if (!L.busy) return fail(c, VXE_ERR_INVALID_ARG, "lane %u has no batch", lane);
+  cudaSetDevice(c->device);
+  if (!block) {
+    const cudaError_t q = cudaEventQuery(L.ev[1]);
+    if (q == cudaErrorNotReady) return VXE_NOT_READY;
+    if (q != cudaSuccess) return fail(c, VXE_ERR_DEVICE, "batch: %s", cudaGetErrorString(q));
+  } else {
+    CK(cudaEventSynchronize(L.ev[1]));
+  }
+  L.busy = false;
+  float ms = 0.0f;
+  CK(cudaEventElapsedTime(&ms, L.ev[0], L.ev[1]));
+  if (stats) {
+    stats->ms = ms;
+    stats->rays = L.rays;
+    stats->items = L.items;
+    stats->tiles = L.tiles;
+  }
+  uint32_t word = 0;
+  CK(cudaMemcpy(&word, c->errword.p, 4, cudaMemcpyDeviceToHost));
+  if (word) return fail(c, VXE_ERR_BOUNDS, "device bounds check tripped (error word 0x%x)", word);
+  return VXE_OK;
+}
+
+vxe_status vxe_submit_batch(vxe_ctx* c, const vxe_request* reqs, uint32_t n, const vxe_batch_options* opt,
+                            vxe_batch_stats* stats) {
+  vxe_status st = vxe_submit_batch_async(c, 0, reqs, n, opt);
+  if (st != VXE_OK) return st;
+  return vxe_batch_wait(c, 0, 1, stats);
+}
+
 
 }  // extern "C"
 

@@ -17,8 +17,10 @@ LIB_PATH = Path(__file__).resolve().parent / "libvxe.so"
 VXE_OK = 0
 STATUS_NAMES = {
     0: "VXE_OK", 1: "VXE_ERR_INVALID_ARG", 2: "VXE_ERR_CAPACITY", 3: "VXE_ERR_OOM", 4: "VXE_ERR_TIMEOUT",
-    5: "VXE_ERR_DEVICE", 6: "VXE_ERR_BOUNDS", 7: "VXE_ERR_NO_DEVICE",
+    5: "VXE_ERR_DEVICE", 6: "VXE_ERR_BOUNDS", 7: "VXE_ERR_NO_DEVICE", 8: "VXE_NOT_READY",
 }
+VXE_NOT_READY = 8
+BATCH_LANES = 4
 
 INVALID_U32 = 0xFFFFFFFF
 MACRO_WORDS_PER_CHUNK = 16
@@ -139,6 +141,25 @@ class SceneView(C.Structure):
 
 NOALLOC_MAX_TILES = 36864
 
+REQ_VIEWPORT, REQ_QUERY = 0, 1
+BATCH_PERSISTENT, BATCH_PLAIN, BATCH_GRAPH = 0, 1, 2
+MAX_BATCH_REQUESTS = 256
+
+
+class Request(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32), ("ray_count", C.c_uint32),
+                ("camera", CameraGpu), ("d_origins", C.c_void_p), ("d_dirs", C.c_void_p), ("tmax", C.c_float),
+                ("_pad", C.c_uint32), ("d_out", C.c_void_p)]
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("tile_w", C.c_uint32), ("tile_h", C.c_uint32), ("rays_per_thread", C.c_uint32),
+                ("mode", C.c_uint32)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("ms", C.c_double), ("rays", C.c_uint64), ("items", C.c_uint32), ("tiles", C.c_uint32)]
+
 
 # Every symbol include/vxe/vxe.h declares, with (restype, argtypes).
 P = C.POINTER
@@ -169,6 +190,9 @@ SIGNATURES = {
     "vxe_debug_detmath": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
     "vxe_trace_primary_hits_noalloc": (C.c_int, [P(SceneView), P(CameraGpu), P(ClipmapGpu), C.c_void_p,
                                                   C.c_void_p]),
+    "vxe_submit_batch": (C.c_int, [C.c_void_p, P(Request), C.c_uint32, P(BatchOptions), P(BatchStats)]),
+    "vxe_submit_batch_async": (C.c_int, [C.c_void_p, C.c_uint32, P(Request), C.c_uint32, P(BatchOptions)]),
+    "vxe_batch_wait": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, P(BatchStats)]),
     "vxe_build_chunk": (C.c_int, [P(WorldParams), C.c_int32, C.c_int32, C.c_int32, P(BuiltChunk)]),
     "vxe_free_chunk": (None, [P(BuiltChunk)]),
     "vxe_chunk_materials": (C.c_int, [P(WorldParams), C.c_int32, C.c_int32, C.c_int32, C.c_void_p]),

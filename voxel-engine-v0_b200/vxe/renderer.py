@@ -156,6 +156,31 @@ class Renderer:
         a = np.ascontiguousarray(arr)
         self._check(self._lib.vxe_write_image(self._ctx, img, a.ctypes.data, a.nbytes), "vxe_write_image")
 
+    # -- batches ----------------------------------------------------------------
+    def submit_batch(self, requests, tile=(8, 8), rays_per_thread=1, mode=A.BATCH_PERSISTENT) -> A.BatchStats:
+        """Traces A.Request records (device outputs) in one batch; returns device timings."""
+        n = len(requests)
+        arr = (A.Request * max(n, 1))(*requests)
+        opt = A.BatchOptions(tile[0], tile[1], rays_per_thread, mode)
+        st = A.BatchStats()
+        self._check(self._lib.vxe_submit_batch(self._ctx, arr, n, C.byref(opt), C.byref(st)), "vxe_submit_batch")
+        return st
+
+    def submit_batch_async(self, lane, requests, tile=(8, 8), rays_per_thread=1, mode=A.BATCH_PERSISTENT) -> None:
+        n = len(requests)
+        arr = (A.Request * max(n, 1))(*requests)
+        opt = A.BatchOptions(tile[0], tile[1], rays_per_thread, mode)
+        self._check(self._lib.vxe_submit_batch_async(self._ctx, lane, arr, n, C.byref(opt)), "vxe_submit_batch_async")
+
+    def batch_wait(self, lane, block=True):
+        """Returns BatchStats when the lane's batch is done, None while it still runs."""
+        st = A.BatchStats()
+        rc = self._lib.vxe_batch_wait(self._ctx, lane, 1 if block else 0, C.byref(st))
+        if rc == A.VXE_NOT_READY:
+            return None
+        self._check(rc, "vxe_batch_wait")
+        return st
+
     # -- queries ----------------------------------------------------------------
     def trace_rays(self, origins: np.ndarray, dirs: np.ndarray, tmax: float) -> np.ndarray:
         o = np.ascontiguousarray(origins, dtype=np.float32).reshape(-1, 3)

@@ -232,7 +232,23 @@ class World:
                 self.grid[(iz * ny + iy) * nx + ix] = slot
         return self.grid
 
+    def prebuild(self, keys, threads: int | None = None) -> None:
+        """Builds missing chunks on a thread pool (the C++ builder releases the GIL),
+        like the reference's rayon build pool (streaming/build_pool.rs:19-25)."""
+        import os
+        from concurrent.futures import ThreadPoolExecutor
+
+        todo = [k for k in keys if k not in self.cache]
+        if len(todo) < 4:
+            for k in todo:
+                self.chunk(k)
+            return
+        with ThreadPoolExecutor(max_workers=threads or min(32, os.cpu_count() or 1)) as ex:
+            for k, data in zip(todo, ex.map(self.builder, todo)):
+                self.cache[k] = data
+
     def populate(self) -> list[Upload]:
+        self.prebuild(list(self.keys_in_grid()))
         ups = [self.add(k) for k in self.keys_in_grid() if k not in self.key_to_slot]
         self.rebuild_grid()
         return ups
