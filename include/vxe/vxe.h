@@ -164,7 +164,13 @@ enum {
   /* Run the primary pass as one kernel per pixel (trace + shading) instead of
    * the default wavefront (trace kernel -> per-class shading kernels).  Both
    * produce identical images. */
-  VXE_FLAG_PRIMARY_MEGAKERNEL = 1u << 5
+  VXE_FLAG_PRIMARY_MEGAKERNEL = 1u << 5,
+  /* Do not keep the per-frame grass cell table (blade roots, wind bend,
+   * lean, radius and side axis of every grass column top, 160 B per column of
+   * every chunk slot).  Without it each grass march derives its cell's blades
+   * itself, as the reference shader does; images are identical either way.
+   * Read at vxe_create (the table is allocated there) and per frame. */
+  VXE_FLAG_NO_GRASS_TABLE = 1u << 6
 };
 
 typedef struct vxe_config {

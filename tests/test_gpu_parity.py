@@ -41,6 +41,14 @@ def test_features_scene_megakernel_schedule_bit_exact():
     assert all(r == {} for r in res), res
 
 
+def test_features_scene_without_grass_table_bit_exact():
+    # Every grass march derives its blades itself (no per-frame cell table):
+    # the same images as the table path and the oracle.
+    sc = scenes.features()
+    res = run_parity(sc, frames=2, extra_flags=A.FLAG_NO_GRASS_TABLE)
+    assert all(r == {} for r in res), res
+
+
 def test_features_scene_godray_alias_off_bit_exact():
     sc = scenes.features()
     res = run_parity(sc, frames=2, godray_alias=False)

@@ -64,6 +64,11 @@ struct BatchArgs {
   uint32_t* head;       // [0] item counter, [1] tile counter
   uint32_t req_first;   // plain mode: the one request a launch serves
   uint32_t plain;       // 1: item = blockIdx-derived, no queue
+  // grass cell table, valid for cameras with this wind time / strength
+  const float4* grass_rec;
+  uint64_t grass_rec_n;
+  const float* grass_taper;
+  uint32_t grass_time_bits, grass_strength_bits;
 };
 
 constexpr int BATCH_THREADS = 128;
@@ -89,6 +94,11 @@ __device__ __forceinline__ Scene batch_scene(const BatchArgs& B, const vxe_camer
   s.clip_layers = B.clip_layers;
   s.clip_res = B.clip_res;
   s.err = B.err;
+  const bool table = B.grass_rec != nullptr && __float_as_uint(cam->voxel_params[1]) == B.grass_time_bits &&
+                     __float_as_uint(cam->voxel_params[2]) == B.grass_strength_bits;
+  s.grass_rec = table ? B.grass_rec : nullptr;
+  s.grass_rec_n = table ? B.grass_rec_n : 0;
+  s.grass_taper = table ? B.grass_taper : nullptr;
   return s;
 }
 

@@ -130,6 +130,11 @@ struct Scene {
   const float* __restrict__ clip_tex;
   uint32_t clip_layers, clip_res;
   uint32_t* err;
+  // Per-frame grass cell table (10 x float4 per column, slot * 4096 + column)
+  // and blade taper per LOD (3 x 6); null when the pass has none.
+  const float4* __restrict__ grass_rec;
+  uint64_t grass_rec_n;
+  const float* __restrict__ grass_taper;
 };
 
 struct Node { uint32_t child_base, child_mask, material, key; };

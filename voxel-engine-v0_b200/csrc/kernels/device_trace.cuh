@@ -504,56 +504,135 @@ struct GrassCellGeom {
   float taper[6];
 };
 
-__device__ __noinline__ void grass_cell_build(const Scene& s, v3 cb, v3 id, float time_s, float strength, uint32_t lod,
-                                              GrassCellGeom& G) {
+// Blade length of cell `id` (grass.wgsl:216).
+__device__ __forceinline__ float grass_blade_len(const Scene& s, v3 id) {
+  const float layer_h = GRASS_LAYER_HEIGHT_VOX * vs_(s);
+  return layer_h * (0.65f + 0.35f * hash31(id + V3(9.1f, 3.7f, 5.2f)));
+}
+
+// The point-independent part of blade i of cell (cb, id) (grass.wgsl:243-298).
+__device__ __noinline__ void grass_blade_geom(const Scene& s, v3 cb, v3 id, float time_s, float strength, uint32_t i,
+                                              GrassBladeGeom& B) {
   const float vs = vs_(s);
   const float top_y = cb.y + vs;
-  const float layer_h = GRASS_LAYER_HEIGHT_VOX * vs;
-  G.blade_len = layer_h * (0.65f + 0.35f * hash31(id + V3(9.1f, 3.7f, 5.2f)));
-  uint32_t blade_count = GRASS_BLADE_COUNT;
+  const float clump_r = 0.18f * vs;
+  const float base_r = (GRASS_VOXEL_THICKNESS_VOX * vs) * 0.85f;
+  const v4 uvpw = grass_blade_params(id, i);
+  const float u0 = uvpw.x, v0 = uvpw.y, ph = uvpw.z, wR = uvpw.w;
+  const float cfi = (float)(i % 5u);
+  const float cu = hash31(id + V3(13.7f + cfi, 2.1f, 9.9f));
+  const float cv = hash31(id + V3(4.2f + cfi, 7.3f, 1.4f));
+  const float inset = 0.10f;
+  const float cux = mixf(inset, 1.0f - inset, cu), cvz = mixf(inset, 1.0f - inset, cv);
+  const v2 clump_center = V2(cb.x + cux * vs, cb.z + cvz * vs);
+  const float ang = TAU * u0;
+  const float rr = clump_r * (0.15f + 0.85f * v0);
+  const v2 root_xz = clump_center + V2(cosf_(ang), sinf_(ang)) * rr;
+  B.root = V3(root_xz.x, top_y, root_xz.y);
+  B.w_xz = 0.35f * grass_wind_xz(B.root + V3(0.0f, ph, 0.0f), time_s, strength);
+  const float lean_ang = TAU * fract(u0 * 1.73f + v0 * 2.11f);
+  B.lean_dir = V2(cosf_(lean_ang), sinf_(lean_ang));
+  B.lean_amt = 0.10f + 0.25f * (v0 * v0);
+  B.r0 = base_r * mixf(0.85f, 1.35f, wR);
+  const float roll = TAU * (0.15f * ph + 0.10f * wR);
+  const v2 roll_dir = V2(cosf_(roll), sinf_(roll));
+  B.side_hint = normalize(V3(B.lean_dir.x * roll_dir.x - B.lean_dir.y * roll_dir.y, 0.12f,
+                             B.lean_dir.x * roll_dir.y + B.lean_dir.y * roll_dir.x));
+}
+
+// Segment taper of a blade with `segs` segments (grass.wgsl:335-339).
+__device__ __forceinline__ float grass_taper_value(float inv_segs, uint32_t sg) {
+  const float t01a = (float)sg * inv_segs;
+  const float t01b = ((float)sg + 1.0f) * inv_segs;
+  const float tmid = 0.5f * (t01a + t01b);
+  const float taper_shape = powf_(clampf(1.0f - tmid, 0.0f, 1.0f), 3.0f);
+  return mixf(GRASS_VOXEL_TAPER, 1.0f, taper_shape);
+}
+
+__device__ __forceinline__ uint32_t grass_lod_segs(uint32_t lod) {
   uint32_t segs = to_u32(fmax_(3.0f, floorf(GRASS_VOXEL_SEGS)));
-  if (lod == 1u) {
-    blade_count = min(blade_count, GRASS_BLADE_COUNT_MID);
-    segs = min(segs, GRASS_SEGS_MID);
-  } else if (lod == 2u) {
-    blade_count = min(blade_count, GRASS_BLADE_COUNT_FAR);
-    segs = min(segs, GRASS_SEGS_FAR);
+  if (lod == 1u) segs = min(segs, GRASS_SEGS_MID);
+  else if (lod == 2u) segs = min(segs, GRASS_SEGS_FAR);
+  return segs;
+}
+
+// Per-frame grass cell table: one record of GRASS_REC_F4 float4 per column
+// (slot * 4096 + lz * 64 + lx) of every resident chunk, written each frame by
+// k_grass_cells for the column's top cell when that cell is grass:
+//   [0]            blade_len, cell id (x, y, z)      (id NaN: no grass top)
+//   [1 + 3b .. 3b + 3]  blade b: root.xyz, w_xz.x | w_xz.y, lean_dir.xy,
+//                       lean_amt | r0, side_hint.xyz
+// Values are produced by the same functions as the in-march build, so a
+// record and a fresh build are bit-identical.
+constexpr uint32_t GRASS_REC_F4 = 10u;
+constexpr uint32_t GRASS_TAPER_N = 18u;
+
+__device__ __forceinline__ void grass_rec_store(float4* r, float blade_len, v3 id, const GrassBladeGeom* B) {
+  r[0] = make_float4(blade_len, id.x, id.y, id.z);
+  for (uint32_t b = 0; b < GRASS_BLADE_COUNT; ++b) {
+    r[1 + 3 * b] = make_float4(B[b].root.x, B[b].root.y, B[b].root.z, B[b].w_xz.x);
+    r[2 + 3 * b] = make_float4(B[b].w_xz.y, B[b].lean_dir.x, B[b].lean_dir.y, B[b].lean_amt);
+    r[3 + 3 * b] = make_float4(B[b].r0, B[b].side_hint.x, B[b].side_hint.y, B[b].side_hint.z);
   }
+}
+
+// Loads cell (cb, id) from the table when the pass has one, the column's
+// record is this cell and cb is the id * vs the record was built from (some
+// callers derive cb from the chunk origin instead, which may differ in the
+// last bit); false means "derive it".
+__device__ __noinline__ bool grass_table_load(const Scene& s, v3 cb, v3 id, GrassCellGeom& G) {
+  if (s.grass_rec == nullptr) return false;
+  const v3 cb_rec = id * vs_(s);
+  if (__float_as_uint(cb_rec.x) != __float_as_uint(cb.x) || __float_as_uint(cb_rec.y) != __float_as_uint(cb.y) ||
+      __float_as_uint(cb_rec.z) != __float_as_uint(cb.z))
+    return false;
+  const int32_t cs = (int32_t)s.cam->chunk_size;
+  if (cs <= 0) return false;
+  const int32_t wx = __float2int_rz(id.x), wy = __float2int_rz(id.y), wz = __float2int_rz(id.z);
+  auto fdiv = [cs](int32_t a) { return a >= 0 ? a / cs : -((-a + cs - 1) / cs); };
+  const uint32_t slot = grid_lookup_slot(s, fdiv(wx), fdiv(wy), fdiv(wz));
+  if (slot == INVALID || slot >= s.cam->chunk_count) return false;
+  const Meta m = meta_at(s, slot);
+  const int32_t lx = wx - m.ox, lz = wz - m.oz;
+  if (lx < 0 || lx > 63 || lz < 0 || lz > 63) return false;
+  const uint64_t e = (uint64_t)slot * 4096u + (uint64_t)(lz * 64 + lx);
+  if (e >= s.grass_rec_n) return false;
+  const float4* r = s.grass_rec + e * GRASS_REC_F4;
+  const float4 h = r[0];
+  if (__float_as_uint(h.y) != __float_as_uint(id.x) || __float_as_uint(h.z) != __float_as_uint(id.y) ||
+      __float_as_uint(h.w) != __float_as_uint(id.z))
+    return false;
+  G.blade_len = h.x;
+  for (uint32_t b = 0; b < G.blade_count; ++b) {
+    const float4 a = r[1 + 3 * b], c = r[2 + 3 * b], d = r[3 + 3 * b];
+    GrassBladeGeom& B = G.blade[b];
+    B.root = V3(a.x, a.y, a.z);
+    B.w_xz = V2(a.w, c.x);
+    B.lean_dir = V2(c.y, c.z);
+    B.lean_amt = c.w;
+    B.r0 = d.x;
+    B.side_hint = V3(d.y, d.z, d.w);
+  }
+  return true;
+}
+
+__device__ __noinline__ void grass_cell_build(const Scene& s, v3 cb, v3 id, float time_s, float strength, uint32_t lod,
+                                              GrassCellGeom& G) {
+  uint32_t blade_count = GRASS_BLADE_COUNT;
+  if (lod == 1u) blade_count = min(blade_count, GRASS_BLADE_COUNT_MID);
+  else if (lod == 2u) blade_count = min(blade_count, GRASS_BLADE_COUNT_FAR);
+  const uint32_t segs = grass_lod_segs(lod);
   G.blade_count = blade_count;
   G.segs = segs;
   G.inv_segs = 1.0f / fmax_((float)segs, 1.0f);
-  const float clump_r = 0.18f * vs;
-  const float base_r = (GRASS_VOXEL_THICKNESS_VOX * vs) * 0.85f;
-  for (uint32_t i = 0; i < blade_count; ++i) {
-    const v4 uvpw = grass_blade_params(id, i);
-    const float u0 = uvpw.x, v0 = uvpw.y, ph = uvpw.z, wR = uvpw.w;
-    const float cfi = (float)(i % 5u);
-    const float cu = hash31(id + V3(13.7f + cfi, 2.1f, 9.9f));
-    const float cv = hash31(id + V3(4.2f + cfi, 7.3f, 1.4f));
-    const float inset = 0.10f;
-    const float cux = mixf(inset, 1.0f - inset, cu), cvz = mixf(inset, 1.0f - inset, cv);
-    const v2 clump_center = V2(cb.x + cux * vs, cb.z + cvz * vs);
-    const float ang = TAU * u0;
-    const float rr = clump_r * (0.15f + 0.85f * v0);
-    const v2 root_xz = clump_center + V2(cosf_(ang), sinf_(ang)) * rr;
-    GrassBladeGeom& B = G.blade[i];
-    B.root = V3(root_xz.x, top_y, root_xz.y);
-    B.w_xz = 0.35f * grass_wind_xz(B.root + V3(0.0f, ph, 0.0f), time_s, strength);
-    const float lean_ang = TAU * fract(u0 * 1.73f + v0 * 2.11f);
-    B.lean_dir = V2(cosf_(lean_ang), sinf_(lean_ang));
-    B.lean_amt = 0.10f + 0.25f * (v0 * v0);
-    B.r0 = base_r * mixf(0.85f, 1.35f, wR);
-    const float roll = TAU * (0.15f * ph + 0.10f * wR);
-    const v2 roll_dir = V2(cosf_(roll), sinf_(roll));
-    B.side_hint = normalize(V3(B.lean_dir.x * roll_dir.x - B.lean_dir.y * roll_dir.y, 0.12f,
-                               B.lean_dir.x * roll_dir.y + B.lean_dir.y * roll_dir.x));
+  if (s.grass_taper != nullptr && lod < 3u) {
+    for (uint32_t sg = 0; sg < segs; ++sg) G.taper[sg] = s.grass_taper[lod * 6u + sg];
+  } else {
+    for (uint32_t sg = 0; sg < segs; ++sg) G.taper[sg] = grass_taper_value(G.inv_segs, sg);
   }
-  for (uint32_t sg = 0; sg < segs; ++sg) {
-    const float t01a = (float)sg * G.inv_segs;
-    const float t01b = ((float)sg + 1.0f) * G.inv_segs;
-    const float tmid = 0.5f * (t01a + t01b);
-    const float taper_shape = powf_(clampf(1.0f - tmid, 0.0f, 1.0f), 3.0f);
-    G.taper[sg] = mixf(GRASS_VOXEL_TAPER, 1.0f, taper_shape);
+  if (!grass_table_load(s, cb, id, G)) {
+    G.blade_len = grass_blade_len(s, id);
+    for (uint32_t i = 0; i < blade_count; ++i) grass_blade_geom(s, cb, id, time_s, strength, i, G.blade[i]);
   }
   G.built = true;
 }

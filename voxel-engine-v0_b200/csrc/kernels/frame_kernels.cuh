@@ -62,6 +62,11 @@ struct FrameArgs {
   uint32_t* q_vox;    // pixel ids with a voxel hit
   uint32_t* q_far;    // pixel ids for heightfield / sky
   uint32_t* q_count;  // [0] voxel, [1] far
+  // per-frame grass cell table: written by k_grass_cells, read by the rest
+  float4* grass_rec;
+  uint64_t grass_rec_n;  // records (slots * 4096)
+  float* grass_taper;    // 3 LODs x 6 segments
+  uint32_t grass_slot0;  // k_grass_cells: first slot of the launch
 };
 
 __device__ __forceinline__ Scene make_scene(const FrameArgs& A, bool godray) {
@@ -90,7 +95,54 @@ __device__ __forceinline__ Scene make_scene(const FrameArgs& A, bool godray) {
   s.clip_layers = A.clip_layers;
   s.clip_res = A.clip_res;
   s.err = A.err;
+  s.grass_rec = A.grass_rec;
+  s.grass_rec_n = A.grass_rec_n;
+  s.grass_taper = A.grass_taper;
   return s;
+}
+
+// ---------------------------------------------------------------------------
+// Per-frame grass cell table (see GRASS_REC_F4): one thread per column of
+// every resident chunk; grass column tops get their blade geometry for this
+// frame's wind, every other column a NaN id so no stale record can match.
+// Thread 0 also writes the per-LOD blade taper.
+// ---------------------------------------------------------------------------
+constexpr int GRASS_CELL_THREADS = 128;
+
+__global__ void __launch_bounds__(GRASS_CELL_THREADS) k_grass_cells(const __grid_constant__ FrameArgs A) {
+  const uint64_t g = (uint64_t)A.grass_slot0 * 4096u + (uint64_t)blockIdx.x * GRASS_CELL_THREADS + threadIdx.x;
+  const Scene s = make_scene(A, false);
+  if (g == 0u) {
+    for (uint32_t lod = 0; lod < 3u; ++lod) {
+      const uint32_t segs = grass_lod_segs(lod);
+      const float inv_segs = 1.0f / fmax_((float)segs, 1.0f);
+      for (uint32_t sg = 0; sg < 6u; ++sg) A.grass_taper[lod * 6u + sg] = sg < segs ? grass_taper_value(inv_segs, sg) : 0.0f;
+    }
+  }
+  const uint32_t slot = (uint32_t)(g >> 12), col = (uint32_t)(g & 4095u);
+  if (slot >= A.cam.chunk_count || (uint64_t)slot * 4096u >= A.grass_rec_n) return;
+  float4* r = A.grass_rec + g * GRASS_REC_F4;
+  const Meta m = meta_at(s, slot);
+  const float nan = __uint_as_float(0x7FC00000u);
+  if (m.colinfo_base == INVALID) {
+    r[0] = make_float4(0.0f, nan, nan, nan);
+    return;
+  }
+  const uint32_t lx = col & 63u, lz = col >> 6;
+  const ColInfo ci = colinfo_decode(colinfo_entry_u16(s, m.colinfo_base, lx, lz));
+  if (!(ci.valid && ci.mat == MAT_GRASS)) {
+    r[0] = make_float4(0.0f, nan, nan, nan);
+    return;
+  }
+  // The cell the column probe and the grass-voxel hit derive
+  // (chunk_trace.wgsl:1434-1445).
+  const float vs = vs_(s);
+  const v3 id = V3((float)(m.ox + (int32_t)lx), (float)(m.oy + (int32_t)ci.y_vox), (float)(m.oz + (int32_t)lz));
+  const v3 cb = id * vs;
+  const float time_s = A.cam.voxel_params[1], strength = A.cam.voxel_params[2];
+  GrassBladeGeom B[GRASS_BLADE_COUNT];
+  for (uint32_t i = 0; i < GRASS_BLADE_COUNT; ++i) grass_blade_geom(s, cb, id, time_s, strength, i, B[i]);
+  grass_rec_store(r, grass_blade_len(s, id), id, B);
 }
 
 // ---------------------------------------------------------------------------
@@ -817,6 +869,9 @@ __device__ __forceinline__ Scene make_query_scene(const QueryArgs& Q) {
   s.clip_layers = 0;
   s.clip_res = 0;
   s.err = Q.err;
+  s.grass_rec = nullptr;
+  s.grass_rec_n = 0;
+  s.grass_taper = nullptr;
   return s;
 }
 

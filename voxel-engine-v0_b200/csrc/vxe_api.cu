@@ -45,12 +45,32 @@ enum Img {
   IMG_N
 };
 
+// The per-frame grass cell table, shared by the frame stream and the batch
+// lanes.  Its contents depend on the chunk records and on the camera's wind
+// time, wind strength, voxel size and chunk count (the tag).  A pass whose
+// camera matches the tag reads it as is; otherwise its stream rebuilds it
+// after every earlier reader on every stream has finished, so no pass sees a
+// table change under it.  Chunk uploads refresh the records of the uploaded
+// slots on the upload stream, with the same ordering as the chunk data.
+constexpr int kGrassReaders = 1 + VXE_BATCH_LANES;  // compute stream, lanes
+
+struct GrassTable {
+  DevBuf rec, taper;
+  bool valid = false;
+  uint32_t time_bits = 0, strength_bits = 0, vs_bits = 0, chunk_count = 0;
+  vxe_camera_gpu cam{};  // camera of the last full build (for slot refreshes)
+  cudaEvent_t built = nullptr;
+  bool built_recorded = false;
+  cudaEvent_t reader[kGrassReaders] = {};
+  bool reader_used[kGrassReaders] = {};
+};
+
 struct BatchLane {
   cudaStream_t stream = nullptr;
   DevBuf hdr, reqs, cams, tile_count, tile_slots, head;
   void* stage = nullptr;  // pinned: header | requests | cameras
   cudaGraphExec_t graph = nullptr;
-  uint32_t graph_key[6] = {0, 0, 0, 0, 0, 0};
+  uint32_t graph_key[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   vxe_clipmap_gpu graph_clip{};  // clipmap uniform baked into the captured launches
   cudaEvent_t ev[2] = {nullptr, nullptr};
   bool busy = false;
@@ -72,6 +92,7 @@ struct vxe_ctx {
   bool timed = false;
   // arenas
   DevBuf nodes, ropes, metas, macro, colinfo, grid, clip_tex, errword;
+  GrassTable gt;
   // images
   DevBuf img[IMG_N];
   uint32_t iw = 0, ih = 0, pw = 0, ph = 0;
@@ -223,6 +244,94 @@ void fill_scene_args(const vxe_ctx* c, FrameArgs& A) {
   A.godray_alias = (c->flags & VXE_FLAG_GODRAY_MACRO_ALIAS) ? 1u : 0u;
 }
 
+uint32_t fbits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+
+void grass_table_args(const vxe_ctx* c, FrameArgs& A) {
+  A.grass_rec = (float4*)c->gt.rec.p;
+  A.grass_rec_n = (uint64_t)c->cfg.chunk_capacity * 4096u;
+  A.grass_taper = (float*)c->gt.taper.p;
+}
+
+// Records of slots [slot0, slot0 + n) for camera `cam` on stream `st`.
+vxe_status grass_table_fill(vxe_ctx* c, cudaStream_t st, const vxe_camera_gpu& cam, uint32_t slot0, uint32_t n) {
+  using namespace vxe::dev;
+  if (n == 0) return VXE_OK;
+  FrameArgs A;
+  fill_scene_args(c, A);
+  A.cam = cam;
+  grass_table_args(c, A);
+  A.grass_slot0 = slot0;
+  const uint64_t threads = (uint64_t)n * 4096u;
+  k_grass_cells<<<(unsigned)((threads + GRASS_CELL_THREADS - 1) / GRASS_CELL_THREADS), GRASS_CELL_THREADS, 0, st>>>(A);
+  CK(cudaGetLastError());
+  return VXE_OK;
+}
+
+// Makes the table valid on stream `st` for `cam`; *use tells whether the
+// pass may read it.  `reader` is the stream's index (0 compute, 1+ lanes).
+vxe_status grass_table_acquire(vxe_ctx* c, cudaStream_t st, int reader, const vxe_camera_gpu& cam, bool* use) {
+  *use = false;
+  GrassTable& T = c->gt;
+  if (!T.rec.p || (c->flags & VXE_FLAG_NO_GRASS_TABLE) || cam.chunk_count == 0 ||
+      cam.chunk_count > c->cfg.chunk_capacity)
+    return VXE_OK;
+  const uint32_t tb = fbits(cam.voxel_params[1]), sb = fbits(cam.voxel_params[2]), vb = fbits(cam.voxel_params[0]);
+  const bool same = T.valid && T.time_bits == tb && T.strength_bits == sb && T.vs_bits == vb &&
+                    T.chunk_count == cam.chunk_count;
+  if (!same) {
+    for (int i = 0; i < kGrassReaders; ++i)
+      if (T.reader_used[i]) CK(cudaStreamWaitEvent(st, T.reader[i], 0));
+    if (T.built_recorded) CK(cudaStreamWaitEvent(st, T.built, 0));
+    vxe_status s2 = grass_table_fill(c, st, cam, 0u, cam.chunk_count);
+    if (s2 != VXE_OK) return s2;
+    T.valid = true;
+    T.time_bits = tb;
+    T.strength_bits = sb;
+    T.vs_bits = vb;
+    T.chunk_count = cam.chunk_count;
+    T.cam = cam;
+  } else if (T.built_recorded) {
+    CK(cudaStreamWaitEvent(st, T.built, 0));
+  }
+  CK(cudaEventRecord(T.built, st));
+  T.built_recorded = true;
+  *use = true;
+  return VXE_OK;
+}
+
+// After chunk uploads: rebuild the records of the uploaded slots on the
+// upload stream, ordered after the copies (and after the last full build).
+vxe_status grass_table_refresh(vxe_ctx* c, const vxe_chunk_upload* ups, uint32_t n) {
+  GrassTable& T = c->gt;
+  if (!T.valid || n == 0) return VXE_OK;
+  if (T.built_recorded) CK(cudaStreamWaitEvent(c->upload, T.built, 0));
+  std::vector<uint32_t> slots;
+  slots.reserve(n);
+  for (uint32_t i = 0; i < n; ++i)
+    if (ups[i].slot < T.chunk_count) slots.push_back(ups[i].slot);
+  std::sort(slots.begin(), slots.end());
+  slots.erase(std::unique(slots.begin(), slots.end()), slots.end());
+  for (size_t i = 0; i < slots.size();) {  // one launch per run of consecutive slots
+    size_t j = i + 1;
+    while (j < slots.size() && slots[j] == slots[j - 1] + 1) ++j;
+    vxe_status st = grass_table_fill(c, c->upload, T.cam, slots[i], (uint32_t)(j - i));
+    if (st != VXE_OK) return st;
+    i = j;
+  }
+  return VXE_OK;
+}
+
+// Marks the end of a pass that read the table on stream `st`.
+vxe_status grass_table_release(vxe_ctx* c, cudaStream_t st, int reader) {
+  CK(cudaEventRecord(c->gt.reader[reader], st));
+  c->gt.reader_used[reader] = true;
+  return VXE_OK;
+}
+
 vxe_status launch_frame(vxe_ctx* c, bool timed) {
   if (c->iw == 0 || c->pw == 0) return fail(c, VXE_ERR_INVALID_ARG, "vxe_resize must be called before rendering");
   if (c->cam.render_present_px[0] != c->iw || c->cam.render_present_px[1] != c->ih ||
@@ -273,6 +382,10 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
   const uint32_t npix = c->iw * c->ih;
   using namespace vxe::dev;
   if (timed) CK(cudaEventRecord(c->ev[0], c->compute));
+  bool use_grass = false;
+  vxe_status gst = grass_table_acquire(c, c->compute, 0, c->cam, &use_grass);
+  if (gst != VXE_OK) return gst;
+  if (use_grass) grass_table_args(c, A);
   k_tiles<<<(tiles + TILE_THREADS - 1) / TILE_THREADS, TILE_THREADS, 0, c->compute>>>(A);
   if (timed) CK(cudaEventRecord(c->ev[1], c->compute));
   if (c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL) {
@@ -293,6 +406,7 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
                 dim3(POST_THREADS_X, POST_THREADS_Y), 0, c->compute>>>(A);
   if (timed) CK(cudaEventRecord(c->ev[4], c->compute));
   CK(cudaGetLastError());
+  if (use_grass && (gst = grass_table_release(c, c->compute, 0)) != VXE_OK) return gst;
   c->timed = timed;
   c->ping = q;
   return VXE_OK;
@@ -350,6 +464,13 @@ vxe_status vxe_create(const vxe_config* cfg, vxe_ctx** out) {
   const uint64_t clip_bytes = (uint64_t)cfg->clip_levels * cfg->clip_res * cfg->clip_res * 4;
   if ((st = alloc(c, c->clip_tex, clip_bytes)) != VXE_OK) return bail(st);
   if ((st = alloc(c, c->errword, 4)) != VXE_OK) return bail(st);
+  if (!(cfg->flags & VXE_FLAG_NO_GRASS_TABLE)) {
+    if ((st = alloc(c, c->gt.rec, cc * 4096u * vxe::dev::GRASS_REC_F4 * 16u)) != VXE_OK) return bail(st);
+    if ((st = alloc(c, c->gt.taper, vxe::dev::GRASS_TAPER_N * 4u)) != VXE_OK) return bail(st);
+  }
+  if (cudaEventCreateWithFlags(&c->gt.built, cudaEventDisableTiming) != cudaSuccess) return bail(VXE_ERR_DEVICE);
+  for (auto& e : c->gt.reader)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return bail(VXE_ERR_DEVICE);
   c->cam.chunk_size = 64u;
   *out = c;
   return VXE_OK;
@@ -360,8 +481,10 @@ void vxe_destroy(vxe_ctx* c) {
   cudaSetDevice(c->device);
   if (c->compute) cudaStreamSynchronize(c->compute);
   if (c->upload) cudaStreamSynchronize(c->upload);
+  for (auto& L : c->lanes)  // lanes read the arenas: drain them before freeing
+    if (L.stream) cudaStreamSynchronize(L.stream);
   for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword,
-                  &c->q_in, &c->q_out})
+                  &c->q_in, &c->q_out, &c->gt.rec, &c->gt.taper})
     release(*b);
   for (auto& L : c->lanes) {
     if (L.stream) cudaStreamSynchronize(L.stream);
@@ -374,6 +497,9 @@ void vxe_destroy(vxe_ctx* c) {
   }
   for (auto& b : c->img) release(b);
   for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->gt.built) cudaEventDestroy(c->gt.built);
+  for (auto& e : c->gt.reader)
     if (e) cudaEventDestroy(e);
   if (c->upload_done) cudaEventDestroy(c->upload_done);
   if (c->compute) cudaStreamDestroy(c->compute);
@@ -457,6 +583,8 @@ vxe_status vxe_upload_chunks(vxe_ctx* c, const vxe_chunk_upload* ups, uint32_t n
       CK(cudaMemcpyAsync((char*)c->colinfo.p + cb * 4, u.colinfo_words, VXE_COLINFO_WORDS_PER_CHUNK * 4,
                          cudaMemcpyHostToDevice, c->upload));
   }
+  vxe_status gst = grass_table_refresh(c, ups, n);
+  if (gst != VXE_OK) return gst;
   CK(cudaEventRecord(c->upload_done, c->upload));
   c->upload_pending = true;
   c->upload_recorded = true;
@@ -468,6 +596,15 @@ vxe_status vxe_write_meta(vxe_ctx* c, uint32_t first, const vxe_chunk_meta* meta
   if ((uint64_t)first + n > c->cfg.chunk_capacity) return fail(c, VXE_ERR_CAPACITY, "meta run exceeds capacity");
   cudaSetDevice(c->device);
   if (n) CK(cudaMemcpyAsync((char*)c->metas.p + (size_t)first * 48, metas, (size_t)n * 48, cudaMemcpyHostToDevice, c->upload));
+  // a slot's records follow its meta (origin, colinfo base)
+  if (n && c->gt.valid) {
+    if (c->gt.built_recorded) CK(cudaStreamWaitEvent(c->upload, c->gt.built, 0));
+    const uint32_t hi = std::min(first + n, c->gt.chunk_count);
+    if (hi > first) {
+      vxe_status gst = grass_table_fill(c, c->upload, c->gt.cam, first, hi - first);
+      if (gst != VXE_OK) return gst;
+    }
+  }
   CK(cudaEventRecord(c->upload_done, c->upload));
   c->upload_pending = true;
   c->upload_recorded = true;
@@ -818,6 +955,23 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
   }
   BatchArgs B = batch_args(c, L);
   CK(cudaEventRecord(L.ev[0], L.stream));
+  // Grass cell table for the wind of the first viewport's camera (requests
+  // with another wind time / strength derive their cells in the march).
+  const vxe_camera_gpu* gcam = &cams[0];
+  for (uint32_t i = 0; i < n; ++i)
+    if (reqs[i].kind == VXE_REQ_VIEWPORT) {
+      gcam = &cams[i + 1];
+      break;
+    }
+  bool use_grass = false;
+  if ((st = grass_table_acquire(c, L.stream, 1 + (int)lane, *gcam, &use_grass)) != VXE_OK) return st;
+  if (use_grass) {
+    B.grass_rec = (const float4*)c->gt.rec.p;
+    B.grass_rec_n = (uint64_t)c->cfg.chunk_capacity * 4096u;
+    B.grass_taper = (const float*)c->gt.taper.p;
+    B.grass_time_bits = fbits(gcam->voxel_params[1]);
+    B.grass_strength_bits = fbits(gcam->voxel_params[2]);
+  }
   if (opt->mode == VXE_BATCH_PLAIN) {
     CK(cudaMemcpyAsync(L.hdr.p, (char*)L.stage + kStageHdr, sizeof H, cudaMemcpyHostToDevice, L.stream));
     CK(cudaMemcpyAsync(L.reqs.p, (char*)L.stage + kStageReqs, n * sizeof(BatchReq), cudaMemcpyHostToDevice, L.stream));
@@ -838,8 +992,9 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
   } else {
     // Captured once per tile-buffer allocation and clipmap uniform; later
     // batches only rewrite the pinned staging the graph's copies read.
-    const uint32_t key[6] = {(uint32_t)(uintptr_t)L.tile_count.p, (uint32_t)((uintptr_t)L.tile_count.p >> 32),
-                             (uint32_t)c->cfg.clip_levels, c->clip.levels, c->clip.res, 1u};
+    const uint32_t key[9] = {(uint32_t)(uintptr_t)L.tile_count.p, (uint32_t)((uintptr_t)L.tile_count.p >> 32),
+                             (uint32_t)c->cfg.clip_levels, c->clip.levels, c->clip.res, 1u,
+                             use_grass ? 1u : 0u, B.grass_time_bits, B.grass_strength_bits};
     const bool same = L.graph != nullptr && std::memcmp(key, L.graph_key, sizeof key) == 0 &&
                       std::memcmp(&L.graph_clip, &B.clip, sizeof B.clip) == 0;
     if (!same) {
@@ -861,6 +1016,7 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
     }
     CK(cudaGraphLaunch(L.graph, L.stream));
   }
+  if (use_grass && (st = grass_table_release(c, L.stream, 1 + (int)lane)) != VXE_OK) return st;
   CK(cudaEventRecord(L.ev[1], L.stream));
   L.busy = true;
   L.rays = rays;
