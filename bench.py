@@ -193,7 +193,7 @@ def run_vxe(args, rank: int, world_size: int):
     if world_size > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    step_ms, prim_ms, god_ms, comp_ms, tile_ms = [], [], [], [], []
+    step_ms, prim_ms, god_ms, comp_ms, tile_ms, trace_ms, grass_ms = [], [], [], [], [], [], []
     with ClockSampler(dev) as clocks:
         for s in range(args.steps):
             flush.zero_()
@@ -205,6 +205,8 @@ def run_vxe(args, rank: int, world_size: int):
             god_ms.append(t["godray"])
             comp_ms.append(t["composite"])
             tile_ms.append(t["tiles"])
+            trace_ms.append(t["primary_trace"])
+            grass_ms.append(t["grass_cells"])
     torch.cuda.synchronize()
     if world_size > 1:
         torch.distributed.barrier()
@@ -218,7 +220,8 @@ def run_vxe(args, rank: int, world_size: int):
         e2e = run_e2e(args, sc, dev, world_size)
     return {
         "total_ms": total_ms, "step_ms": step_ms, "primary_ms": prim_ms, "godray_ms": god_ms,
-        "composite_ms": comp_ms, "tiles_ms": tile_ms, "rays_per_frame": rays_per_frame,
+        "composite_ms": comp_ms, "tiles_ms": tile_ms, "trace_ms": trace_ms, "grass_ms": grass_ms,
+        "rays_per_frame": rays_per_frame,
         "internal": list(sc.internal),
         "clocks": clocks.summary(), "e2e": e2e, "error_word": err, "device": torch.cuda.get_device_name(dev),
     }
@@ -309,21 +312,31 @@ def cpu_sample(seconds: float, present, threads: int):
         uploads, gc, clip, cam = drv.step()
         runner.render(cam, clip[0], threads=threads)
         if ctr is None:
-            ctr = (runner.primary_ctr.as_dict(), runner.godray_ctr.as_dict())
+            ctr = (runner.primary_ctr.as_dict(), runner.godray_ctr.as_dict(), runner.trace_ctr.as_dict())
         frames += 1
         elapsed = time.perf_counter() - t0
     rays = frames * sc.internal[0] * sc.internal[1]
     return {"rays": rays, "seconds": elapsed, "frames": frames, "counters": ctr}
 
 
+def record_bytes(c: dict) -> int:
+    """Full record sizes of the loads the oracle counted: node 16, rope 32, meta 48, grid / macro / colinfo
+    words and clip texels 4."""
+    return int(16 * c["node_loads"] + 32 * c["rope_loads"] + 48 * c["meta_loads"] + 4 * c["grid_loads"] +
+               4 * c["macro_loads"] + 4 * c["colinfo_loads"] + 4 * c["clip_loads"])
+
+
 def algorithmic_primary_bytes(counters: dict, pixels: int) -> int:
-    """Record bytes the reference algorithm loads (full record sizes) + compulsory image I/O."""
-    c = counters
-    loads = (16 * c["node_loads"] + 32 * c["rope_loads"] + 48 * c["meta_loads"] + 4 * c["grid_loads"] +
-             4 * c["macro_loads"] + 4 * c["colinfo_loads"] + 4 * c["clip_loads"])
+    """Primary pass: record bytes the reference algorithm loads + compulsory image I/O."""
     # outputs: color 16 + depth 4 + hist 16 + shadow 4 + local_hist 16; inputs: hist 16 + shadow 4 + local_hist 16
     io = pixels * (16 + 4 + 16 + 4 + 16 + 16 + 4 + 16)
-    return int(loads + io)
+    return record_bytes(counters) + int(io)
+
+
+def algorithmic_trace_bytes(trace_counters: dict, pixels: int) -> int:
+    """Voxel trace phase (k_primary_trace): its record loads + the two history texels the hit-distance
+    hint reads per pixel (own + reprojected, 16 B each)."""
+    return record_bytes(trace_counters) + 32 * int(pixels)
 
 
 def max_over_ranks(values, device="cpu"):
@@ -386,19 +399,25 @@ def main():
                    "l2": "flushed between steps (512 MiB memset), per-step CUDA events",
                    "frame_ms": {"tiles": round(statistics.mean(res["tiles_ms"]), 4),
                                 "primary": round(statistics.mean(res["primary_ms"]), 4),
+                                "primary_trace": round(statistics.mean(res["trace_ms"]), 4),
+                                "grass_cells": round(statistics.mean(res["grass_ms"]), 4),
                                 "godray": round(statistics.mean(res["godray_ms"]), 4),
                                 "composite": round(statistics.mean(res["composite_ms"]), 4)}},
         "e2e": {"value": round(e2e_val, 3), "unit": UNIT, "h2d_bytes_per_step": res["e2e"]["h2d_bytes_per_step"],
                 "d2h_bytes_per_step": res["e2e"]["d2h_bytes_per_step"],
                 "frame_ms": round(e2e_s * 1e3 / args.steps, 3)},
-        "gpu_launches": 4 * args.steps,
+        # per frame: k_grass_cells, k_tiles, k_primary_trace, k_shade_prep, k_shade_shadow, k_shade_lights,
+        # k_shade_vox, k_shade_far, k_godray, k_composite
+        "gpu_launches": 10 * args.steps,
         "clocks": res["clocks"],
         "device_error_word": res["error_word"],
     }
     peak, peak_kind = peaks()
     prim_s = statistics.mean(res["primary_ms"]) * 1e-3
+    trace_s = statistics.mean(res["trace_ms"]) * 1e-3
     roof = {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None, "traffic": None,
-            "kernel": "k_primary", "peak_kind": peak_kind}
+            "kernel": "k_primary_trace", "peak_kind": peak_kind,
+            "launch_ms": round(trace_s * 1e3, 4)}
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         present = tuple(int(v) for v in args.present.split("x"))
@@ -406,14 +425,24 @@ def main():
         line["cpu_baseline"] = {"value": round(cs["rays"] / cs["seconds"] / 1e6, 4), "unit": UNIT, "cores": threads,
                                 "kind": "port",
                                 "sample": f"{cs['frames']} full frames of the same workload (path frames 0..{cs['frames'] - 1})"}
-        ab = algorithmic_primary_bytes(cs["counters"][0], res["rays_per_frame"])
-        achieved = ab / prim_s / 1e9
+        tb = algorithmic_trace_bytes(cs["counters"][2], res["rays_per_frame"])
+        achieved = tb / trace_s / 1e9
         roof.update({"achieved": round(achieved, 2), "frac": round(achieved / peak, 5),
-                     "algorithmic_bytes_per_launch": ab,
-                     "bytes_per_ray": round(ab / res["rays_per_frame"], 2)})
-    traffic = REPO / "profiles" / "k_primary_traffic.json"
+                     "algorithmic_bytes_per_launch": tb,
+                     "bytes_per_ray": round(tb / res["rays_per_frame"], 2)})
+        ab = algorithmic_primary_bytes(cs["counters"][0], res["rays_per_frame"])
+        pa = ab / prim_s / 1e9
+        roof["primary_pass"] = {"kernels": "k_primary_trace + k_shade_vox + k_shade_far",
+                                "achieved": round(pa, 2), "frac": round(pa / peak, 5),
+                                "algorithmic_bytes_per_frame": ab, "ms": round(prim_s * 1e3, 4)}
+    # DRAM bytes per launch of the trace kernel from the committed ncu summary
+    traffic = REPO / "profiles" / "k_primary_trace_config2.md"
     if traffic.exists():
-        roof["traffic"] = json.loads(traffic.read_text()).get("dram_bytes_per_launch")
+        import re
+
+        m = re.search(r"dram_bytes_per_launch_1080p:\s*([0-9]+)", traffic.read_text())
+        if m:
+            roof["traffic"] = int(m.group(1))
     line["roofline"] = roof
     print(json.dumps(line))
 

@@ -305,9 +305,12 @@ vxe_status vxe_batch_wait(vxe_ctx* ctx, uint32_t lane, int block, vxe_batch_stat
 
 /* GpuTimingsMs (render/state/mod.rs:22-31) minus blit; CUDA events of the last
  * frame.  local_taa and composite_taa are fused into primary / composite and
- * report 0. */
+ * report 0.  Extra fields (no reference counterpart): primary_trace is the
+ * trace kernel inside `primary` (the rest of `primary` is shading) and
+ * grass_cells the per-frame grass cell table, which `tiles` includes. */
 typedef struct vxe_timings {
   double primary, local_taa, godray, composite, composite_taa, tiles, total;
+  double primary_trace, grass_cells;
 } vxe_timings;
 vxe_status vxe_get_timings(vxe_ctx* ctx, vxe_timings* out);
 

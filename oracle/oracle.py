@@ -60,7 +60,7 @@ def lib():
         l = C.CDLL(str(LIB_PATH))
         l.ora_render_frame.restype = C.c_int
         l.ora_render_frame.argtypes = [C.POINTER(OraScene), C.POINTER(FrameIO), C.c_int, C.POINTER(OraCounters),
-                                       C.POINTER(OraCounters)]
+                                       C.POINTER(OraCounters), C.POINTER(OraCounters)]
         l.ora_primary_rows.restype = C.c_int
         l.ora_primary_rows.argtypes = [C.POINTER(OraScene), C.POINTER(FrameIO), C.c_uint32, C.c_uint32, C.c_int,
                                        C.POINTER(OraCounters)]
@@ -142,8 +142,9 @@ class OracleFrameRunner:
         sc = self.scene(cam, clip_params)
         self.primary_ctr = OraCounters()
         self.godray_ctr = OraCounters()
+        self.trace_ctr = OraCounters()  # the voxel trace phase of the primary pass
         rc = lib().ora_render_frame(C.byref(sc), C.byref(io), threads or default_threads(),
-                                    C.byref(self.primary_ctr), C.byref(self.godray_ctr))
+                                    C.byref(self.primary_ctr), C.byref(self.godray_ctr), C.byref(self.trace_ctr))
         assert rc == 0
         self.ping = q
 

@@ -209,6 +209,7 @@ struct Scene {
   const float* clip_tex;  // layers * res * res
   uint32_t clip_layers, clip_res;
   Counters* ctr;
+  Counters* trace_ctr = nullptr;  // primary pass: loads of the voxel trace phase only
 };
 
 struct Node { uint32_t child_base, child_mask, material, key; };
@@ -2359,6 +2360,7 @@ void primary_pixel(const Scene& s, const FrameIO& io, const TileList& tl, uint32
     }
     const float t_start = fmax_(t_hist - PRIMARY_HIT_MARGIN, 0.0f);
     const float t_end = fmin_(t_hist + PRIMARY_HIT_WINDOW, FOG_MAX_DIST);
+    const Counters c_before = *s.ctr;
     // trace_primary_voxels (ray_main.wgsl:116-161)
     VoxTraceResult vt{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
     if (has_tc) {
@@ -2370,6 +2372,18 @@ void primary_pixel(const Scene& s, const FrameIO& io, const TileList& tl, uint32
       }
       if (!done)
         vt = trace_scene_voxels_candidates(s, tl, ro, rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID, tile_count);
+    }
+    if (s.trace_ctr) {
+      Counters& t = *s.trace_ctr;
+      const Counters& c = *s.ctr;
+      t.node_loads += c.node_loads - c_before.node_loads;
+      t.rope_loads += c.rope_loads - c_before.rope_loads;
+      t.meta_loads += c.meta_loads - c_before.meta_loads;
+      t.grid_loads += c.grid_loads - c_before.grid_loads;
+      t.macro_loads += c.macro_loads - c_before.macro_loads;
+      t.colinfo_loads += c.colinfo_loads - c_before.colinfo_loads;
+      t.clip_loads += c.clip_loads - c_before.clip_loads;
+      t.oob += c.oob - c_before.oob;
     }
     if (!vt.in_grid || vt.best.hit == 0u) {
       heightfield_or_sky();
@@ -2802,15 +2816,16 @@ static void add_ctr(ora_counters* out, const Counters& c) {
 // One full frame: primary (+local TAA), godray, composite (+composite TAA).
 // `io` arrays follow the layout documented in FrameIO.
 int ora_render_frame(const ora_scene* sc, FrameIO* io, int threads, ora_counters* primary_ctr,
-                     ora_counters* godray_ctr) {
+                     ora_counters* godray_ctr, ora_counters* trace_ctr) {
   if (!sc || !io) return 1;
   const int nt = threads < 1 ? 1 : threads;
   const uint32_t tiles_x = (io->iw + 7) / 8, tiles_y = (io->ih + 7) / 8;
   // primary: per tile row (tile lists are per 8x8 workgroup)
   std::vector<Counters> pc((size_t)nt);
-  std::vector<float> local_tmp;
+  std::vector<Counters> tc((size_t)nt);
   parallel_rows(tiles_y, nt, [&](uint32_t r0, uint32_t r1, int t) {
-    const Scene s = make_scene(sc, &pc[(size_t)t], false);
+    Scene s = make_scene(sc, &pc[(size_t)t], false);
+    s.trace_ctr = &tc[(size_t)t];
     TileList tl;
     for (uint32_t ty = r0; ty < r1; ++ty)
       for (uint32_t tx = 0; tx < tiles_x; ++tx) {
@@ -2820,6 +2835,7 @@ int ora_render_frame(const ora_scene* sc, FrameIO* io, int threads, ora_counters
       }
   });
   for (auto& c : pc) add_ctr(primary_ctr, c);
+  for (auto& c : tc) add_ctr(trace_ctr, c);
   std::vector<Counters> gc((size_t)nt);
   parallel_rows(io->ih, nt, [&](uint32_t r0, uint32_t r1, int t) {
     const Scene s = make_scene(sc, &gc[(size_t)t], true);

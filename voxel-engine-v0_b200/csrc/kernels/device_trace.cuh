@@ -1805,49 +1805,76 @@ __device__ __forceinline__ v3 material_emission(uint32_t m) {  // shading.wgsl:2
   return V3s(0.0f);
 }
 
-__device__ __noinline__ v3 gather_voxel_lights(const Scene& s, v3 hp, v3 n, v3 rb) {  // light.wgsl:127-211
-  uint32_t hits = 0;
+// gather_voxel_lights (light.wgsl:127-211) in three parts so that its eight
+// rays can also run on eight lanes: the per-pixel frame, one ray's direction,
+// and the in-order accumulation (ray results do not depend on each other;
+// only the accumulation stops early, after LIGHT_EARLY_HITS hits).
+struct LightFrame {
+  v3 p0, tt, bb;
+  float rot;
+};
+
+__device__ __forceinline__ LightFrame light_frame(const Scene& s, v3 hp, v3 n, v3 rb) {  // light.wgsl:127-151
   const float vs = vs_(s);
-  const v3 p0 = hp + n * (0.75f * vs);
+  LightFrame F;
+  F.p0 = hp + n * (0.75f * vs);
   // make_tbn (light.wgsl:25-30): columns t, b, n
   const v3 up = fabsf(n.y) > 0.9f ? V3(1.0f, 0.0f, 0.0f) : V3(0.0f, 1.0f, 0.0f);
-  const v3 tt = normalize(cross(up, n));
-  const v3 bb = normalize(cross(n, tt));
+  F.tt = normalize(cross(up, n));
+  F.bb = normalize(cross(n, F.tt));
   const v3 sv = vfloor((hp - rb) / fmax_(vs, 1e-6f));
   const uint32_t h0 = hash3_i32(i3{to_i32(sv.x), to_i32(sv.y), to_i32(sv.z)});
   const uint32_t h1 = hash_u32(h0);
   const uint32_t h2 = hash_u32(h1 ^ (s.cam->frame_index * 747796405u));
-  const float rot = 6.28318530718f * ((float)(h2 & 1023u) / 1024.0f);
+  F.rot = 6.28318530718f * ((float)(h2 & 1023u) / 1024.0f);
+  return F;
+}
+
+__device__ __forceinline__ v3 light_ray_dir(const LightFrame& F, v3 n, uint32_t i) {  // light.wgsl:167-169
+  const v3 sl = normalize(sphere_dir_local(i, LIGHT_RAYS));
+  const v3 ldir = normalize(F.tt * sl.x + F.bb * sl.y + n * sl.z);
+  return normalize(rot_about_axis(ldir, n, F.rot));
+}
+
+// Adds ray result `hit` (dda_hit_light) to `sum`; true when the gather stops.
+__device__ __forceinline__ bool light_accum(const Scene& s, v3 hp, v3 n, v4 hit, uint32_t& hits, v3& sum) {
+  if (!(hit.w > 0.5f)) return false;  // light.wgsl:172-205
+  const float vs = vs_(s);
   const float soft_r = LIGHT_SOFT_RADIUS_VOX * vs, soft_r2 = soft_r * soft_r;
   const float min_r = LIGHT_NEAR_CLAMP_VOX * vs, min_r2 = min_r * min_r;
   const float range_m = LIGHT_RANGE_VOX * vs, range2 = range_m * range_m;
   const v3 Le = material_emission(MAT_LIGHT);
-  v3 sum = V3s(0.0f);
-  for (uint32_t i = 0; i < LIGHT_RAYS; ++i) {
-    const v3 sl = normalize(sphere_dir_local(i, LIGHT_RAYS));
-    v3 ldir = normalize(tt * sl.x + bb * sl.y + n * sl.z);
-    ldir = normalize(rot_about_axis(ldir, n, rot));
-    const v4 hit = dda_hit_light(s, p0, ldir, LIGHT_MAX_DIST_VOX, vs);
-    if (hit.w > 0.5f) {
-      hits += 1u;
-      const v3 L = V3(hit.x, hit.y, hit.z) - hp;
-      const float r2 = fmax_(dot(L, L), min_r2);
-      const float r = sqrtf(r2);
-      const v3 lw = L / r;
-      const float ndl = clampf((dot(n, lw) + LIGHT_WRAP) / (1.0f + LIGHT_WRAP), 0.0f, 1.0f);
-      float att = clampf(1.0f - (r2 / fmax_(range2, 1e-6f)), 0.0f, 1.0f);
-      att = att * att;
-      const float falloff = 1.0f / (r2 + soft_r2);
-      sum = sum + Le * (LIGHT_DIRECT_GAIN * ndl * falloff * att);
-      if (r2 < 0.35f * range2) {
-        const float bounce = LIGHT_INDIRECT_GAIN * falloff * att;
-        sum = sum + Le * (0.25f * bounce);
-      }
-      if (hits >= LIGHT_EARLY_HITS) break;
-    }
+  hits += 1u;
+  const v3 L = V3(hit.x, hit.y, hit.z) - hp;
+  const float r2 = fmax_(dot(L, L), min_r2);
+  const float r = sqrtf(r2);
+  const v3 lw = L / r;
+  const float ndl = clampf((dot(n, lw) + LIGHT_WRAP) / (1.0f + LIGHT_WRAP), 0.0f, 1.0f);
+  float att = clampf(1.0f - (r2 / fmax_(range2, 1e-6f)), 0.0f, 1.0f);
+  att = att * att;
+  const float falloff = 1.0f / (r2 + soft_r2);
+  sum = sum + Le * (LIGHT_DIRECT_GAIN * ndl * falloff * att);
+  if (r2 < 0.35f * range2) {
+    const float bounce = LIGHT_INDIRECT_GAIN * falloff * att;
+    sum = sum + Le * (0.25f * bounce);
   }
+  return hits >= LIGHT_EARLY_HITS;
+}
+
+__device__ __forceinline__ v3 light_finish(v3 sum) {  // light.wgsl:207-210
   const float denom = fmax_(1.0f, (float)LIGHT_RAYS);
   return sum * (1.0f / denom);
+}
+
+__device__ __noinline__ v3 gather_voxel_lights(const Scene& s, v3 hp, v3 n, v3 rb) {  // light.wgsl:127-211
+  const LightFrame F = light_frame(s, hp, n, rb);
+  uint32_t hits = 0;
+  v3 sum = V3s(0.0f);
+  for (uint32_t i = 0; i < LIGHT_RAYS; ++i) {
+    const v4 hit = dda_hit_light(s, F.p0, light_ray_dir(F, n, i), LIGHT_MAX_DIST_VOX, vs_(s));
+    if (light_accum(s, hp, n, hit, hits, sum)) break;
+  }
+  return light_finish(sum);
 }
 
 // ---------------------------------------------------------------------------

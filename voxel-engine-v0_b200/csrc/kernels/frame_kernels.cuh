@@ -61,7 +61,11 @@ struct FrameArgs {
   uint4* pix_hit;     // 5 x uint4 per pixel (PixHit), written for voxel hits
   uint32_t* q_vox;    // pixel ids with a voxel hit
   uint32_t* q_far;    // pixel ids for heightfield / sky
-  uint32_t* q_count;  // [0] voxel, [1] far
+  uint32_t* q_count;  // [0] voxel, [1] far, [2] fresh shadow, [3] light gather
+  uint32_t* q_shadow;  // voxel pixels that trace a fresh sun shadow this frame
+  uint32_t* q_light;   // voxel pixels that gather local lights
+  float* px_shadow;    // fresh sun transmittance per pixel (q_shadow pixels)
+  float4* px_light;    // light gather result per pixel (q_light pixels)
   // per-frame grass cell table: written by k_grass_cells, read by the rest
   float4* grass_rec;
   uint64_t grass_rec_n;  // records (slots * 4096)
@@ -423,47 +427,62 @@ __device__ __forceinline__ void local_taa_store(const FrameArgs& A, size_t pix, 
   A.local_hist_out[pix] = make_float4(ol.x, ol.y, ol.z, conf1);
 }
 
-// Voxel-hit shading (ray_main.wgsl:374-471) + outputs.
-__device__ __noinline__ void shade_voxel_pixel(const Scene& s, const FrameArgs& A, const PrimaryCtx& c, HitGeom best,
-                                               bool anchor_valid, uint32_t anchor_key, i3 anchor_chunk) {
+// Voxel-hit shading (ray_main.wgsl:374-471) + outputs, in the parts the
+// wavefront schedule runs as separate kernels:
+//   grass_refine         grass-on-voxel slab march (may move t and n)
+//   shadow_blend         1/8 of the pixels per frame: reprojected shadow
+//                        history mixed with a fresh sun transmittance
+//   gather_voxel_lights  local light gather (8 rays)
+//   shade_voxel_final    surface shading, fog, outputs, fused local TAA.
+__device__ __forceinline__ void grass_refine(const Scene& s, const PrimaryCtx& c, HitGeom& best) {
+  if (best.mat != MAT_GRASS) return;
+  const float vs = vs_(s);
+  const int32_t csv = (int32_t)s.cam->chunk_size;
+  const i3 ov{to_i32(floorf(best.root_bmin.x / vs + 0.5f)), to_i32(floorf(best.root_bmin.y / vs + 0.5f)),
+              to_i32(floorf(best.root_bmin.z / vs + 0.5f))};
+  const v3 hp = c.ro + c.rd * best.t;
+  const GrassCell cell = pick_grass_cell_in_chunk_with_bias(hp, c.rd, best.root_bmin, ov, vs, csv);
+  const GrassHit gh = try_grass_slab_hit(s, c.ro, c.rd, 0.0f, best.t, cell.bmin_m, cell.id_vox, vs,
+                                         s.cam->voxel_params[1], s.cam->voxel_params[2]);
+  if (gh.hit) { best.t = gh.t; best.n = gh.n; }
+}
+
+__device__ __forceinline__ bool shadow_fresh(const PrimaryCtx& c) { return (c.seed & SHADOW_SUBSAMPLE_MASK) == 0u; }
+__device__ __forceinline__ bool lights_wanted(const HitGeom& best) {
+  return best.hit != 0u && best.mat != MAT_LIGHT && best.t <= LOCAL_LIGHT_MAX_DIST;
+}
+__device__ __forceinline__ v3 shadow_origin(const Scene& s, const PrimaryCtx& c, const HitGeom& best) {
+  return (c.ro + c.rd * best.t) + best.n * (0.75f * vs_(s));
+}
+
+// Shadow for a pixel whose fresh transmittance is `cur` (shadow_fresh).
+__device__ __forceinline__ float shadow_blend(const Scene& s, const FrameArgs& A, const PrimaryCtx& c, v3 hp, float cur) {
+  const uint32_t W = A.iw, H = A.ih;
+  float sh = A.shadow_in[c.pix];
+  const v2 uvp = prev_uv_from_world(s, hp);
+  if (in_unit_square(uvp)) {
+    const int32_t ppx = clampi(to_i32(uvp.x * (float)W), 0, (int32_t)W - 1);
+    const int32_t ppy = clampi(to_i32(uvp.y * (float)H), 0, (int32_t)H - 1);
+    sh = A.shadow_in[(size_t)ppy * W + (uint32_t)ppx];
+  }
+  sh = clampf(sh, 0.0f, 1.0f);
+  return mixf(sh, cur, SHADOW_TAA_ALPHA);
+}
+
+// `light` is gather_voxel_lights' result when lights_wanted(best).
+__device__ __noinline__ void shade_voxel_final(const Scene& s, const FrameArgs& A, const PrimaryCtx& c,
+                                               const HitGeom& best, float shadow_out, v3 light, bool anchor_valid,
+                                               uint32_t anchor_key, i3 anchor_chunk) {
   const float vs = vs_(s);
   const v3 ro = c.ro, rd = c.rd;
-  const uint32_t W = A.iw, H = A.ih;
   const v3 sky_up = sky_bg(V3(0.0f, 1.0f, 0.0f));
-  if (best.mat == MAT_GRASS) {
-    const int32_t csv = (int32_t)s.cam->chunk_size;
-    const i3 ov{to_i32(floorf(best.root_bmin.x / vs + 0.5f)), to_i32(floorf(best.root_bmin.y / vs + 0.5f)),
-                to_i32(floorf(best.root_bmin.z / vs + 0.5f))};
-    const v3 hp = ro + rd * best.t;
-    const GrassCell cell = pick_grass_cell_in_chunk_with_bias(hp, rd, best.root_bmin, ov, vs, csv);
-    const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, best.t, cell.bmin_m, cell.id_vox, vs,
-                                           s.cam->voxel_params[1], s.cam->voxel_params[2]);
-    if (gh.hit) { best.t = gh.t; best.n = gh.n; }
-  }
-  const v3 hp = ro + rd * best.t;
-  const v3 hps = hp + best.n * (0.75f * vs);
-  float shadow_out;
-  if ((c.seed & SHADOW_SUBSAMPLE_MASK) == 0u) {
-    float sh = A.shadow_in[c.pix];
-    const v2 uvp = prev_uv_from_world(s, hp);
-    if (in_unit_square(uvp)) {
-      const int32_t ppx = clampi(to_i32(uvp.x * (float)W), 0, (int32_t)W - 1);
-      const int32_t ppy = clampi(to_i32(uvp.y * (float)H), 0, (int32_t)H - 1);
-      sh = A.shadow_in[(size_t)ppy * W + (uint32_t)ppx];
-    }
-    sh = clampf(sh, 0.0f, 1.0f);
-    const float cur = sun_transmittance_geom_only(s, hps, SUN_DIR);
-    shadow_out = mixf(sh, cur, SHADOW_TAA_ALPHA);
-  } else {
-    shadow_out = clampf(A.shadow_in[c.pix], 0.0f, 1.0f);
-  }
   const v3 base_hdr = shade_hit(s, ro, rd, best, sky_up, shadow_out);
   v3 local_out = V3s(0.0f);
   float local_w = 0.0f;
-  if (best.hit != 0u && best.mat != MAT_LIGHT && best.t <= LOCAL_LIGHT_MAX_DIST) {
+  if (lights_wanted(best)) {
     const v3 hpl = ro + rd * best.t;
     const v3 alb = base_albedo(best.mat, hpl, best.t);
-    local_out = gather_voxel_lights(s, hpl, best.n, best.root_bmin) * alb;
+    local_out = light * alb;
     local_w = 1.0f;
   }
   const float t_scene = fmin_(best.t, FOG_MAX_DIST);
@@ -480,6 +499,22 @@ __device__ __noinline__ void shade_voxel_pixel(const Scene& s, const FrameArgs& 
   A.shadow_out[c.pix] = shadow_out;
   if (A.hits) store_rec(A.hits + c.pix * 2u, make_rec(best, ro, rd, vs, true));
   local_taa_store(A, c.pix, local_out, local_w);
+}
+
+// The whole voxel-hit shading of one pixel (megakernel schedule).
+__device__ __noinline__ void shade_voxel_pixel(const Scene& s, const FrameArgs& A, const PrimaryCtx& c, HitGeom best,
+                                               bool anchor_valid, uint32_t anchor_key, i3 anchor_chunk) {
+  grass_refine(s, c, best);
+  float shadow_out;
+  if (shadow_fresh(c)) {
+    const float cur = sun_transmittance_geom_only(s, shadow_origin(s, c, best), SUN_DIR);
+    shadow_out = shadow_blend(s, A, c, c.ro + c.rd * best.t, cur);
+  } else {
+    shadow_out = clampf(A.shadow_in[c.pix], 0.0f, 1.0f);
+  }
+  v3 light = V3s(0.0f);
+  if (lights_wanted(best)) light = gather_voxel_lights(s, c.ro + c.rd * best.t, best.n, best.root_bmin);
+  shade_voxel_final(s, A, c, best, shadow_out, light, anchor_valid, anchor_key, anchor_chunk);
 }
 
 // Heightfield then sky (ray_main.wgsl:224-269 / 327-372 / 473-516) + outputs.
@@ -612,14 +647,8 @@ __global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace(const __grid_
   enqueue(A.q_far, &A.q_count[1], active && !vox, pix);
 }
 
-__global__ void __launch_bounds__(SHADE_THREADS) k_shade_vox(const __grid_constant__ FrameArgs A) {
-  const uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x;
-  if (i >= A.q_count[0]) return;
-  const Scene s = make_scene(A, false);
-  const uint32_t pix = A.q_vox[i];
-  const PrimaryCtx c = primary_ctx(s, pix % A.iw, pix / A.iw, A.iw);
-  const uint4* src = A.pix_hit + (size_t)pix * 5u;
-  const uint4 a = src[0], b = src[1], d = src[2], e = src[3], f = src[4];
+__device__ __forceinline__ HitGeom load_pixhit(const Scene& s, const uint4* src) {
+  const uint4 a = src[0], b = src[1], d = src[2], e = src[3];
   HitGeom g = miss_hitgeom();
   g.hit = 1u;
   g.t = __uint_as_float(a.x);
@@ -632,16 +661,116 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_shade_vox(const __grid_consta
   g.node = d.z;
   g.leaf_size = __uint_as_float(d.w);
   g.leaf_bmin = V3(__uint_as_float(e.x), __uint_as_float(e.y), __uint_as_float(e.z));
-  shade_voxel_pixel(s, A, c, g, e.w != 0u, f.x, i3{(int32_t)f.y, (int32_t)f.z, (int32_t)f.w});
+  return g;
+}
+
+// Voxel-hit shading, wavefront schedule: prep (grass refine + classify) ->
+// fresh shadows | light gathers -> final.  Each kernel walks its queue with
+// a grid-stride loop whose trip count is uniform per warp (queues are read on
+// the device), so the warp-wide enqueue and shuffles see every lane.
+__device__ __forceinline__ uint32_t warp_uniform_end(uint32_t n) { return (n + 31u) & ~31u; }
+
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_prep(const __grid_constant__ FrameArgs A) {
+  const Scene s = make_scene(A, false);
+  const uint32_t n = A.q_count[0], end = warp_uniform_end(n);
+  for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < end; i += gridDim.x * SHADE_THREADS) {
+    bool fresh = false, light = false;
+    uint32_t pix = 0u;
+    if (i < n) {
+      pix = A.q_vox[i];
+      const PrimaryCtx c = primary_ctx(s, pix % A.iw, pix / A.iw, A.iw);
+      uint4* src = A.pix_hit + (size_t)pix * 5u;
+      HitGeom g = load_pixhit(s, src);
+      if (g.mat == MAT_GRASS) {
+        grass_refine(s, c, g);
+        src[0] = make_uint4(__float_as_uint(g.t), __float_as_uint(g.n.x), __float_as_uint(g.n.y),
+                            __float_as_uint(g.n.z));
+      }
+      fresh = shadow_fresh(c);
+      light = lights_wanted(g);
+    }
+    enqueue(A.q_shadow, &A.q_count[2], fresh, pix);
+    enqueue(A.q_light, &A.q_count[3], light, pix);
+  }
+}
+
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_shadow(const __grid_constant__ FrameArgs A) {
+  const Scene s = make_scene(A, false);
+  const uint32_t n = A.q_count[2];
+  for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < n; i += gridDim.x * SHADE_THREADS) {
+    const uint32_t pix = A.q_shadow[i];
+    const PrimaryCtx c = primary_ctx(s, pix % A.iw, pix / A.iw, A.iw);
+    const HitGeom g = load_pixhit(s, A.pix_hit + (size_t)pix * 5u);
+    A.px_shadow[pix] = sun_transmittance_geom_only(s, shadow_origin(s, c, g), SUN_DIR);
+  }
+}
+
+// Eight lanes per pixel, one light ray each; the group's first lane adds the
+// eight results in ray order (the reference loop's order and early stop).
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_lights(const __grid_constant__ FrameArgs A) {
+  const Scene s = make_scene(A, false);
+  const uint32_t lane = threadIdx.x & 31u, ray = lane & 7u, group0 = lane & ~7u;
+  const uint32_t n = A.q_count[3], groups = n * 8u, end = warp_uniform_end(groups);
+  for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < end; i += gridDim.x * SHADE_THREADS) {
+    const bool active = i < groups;
+    uint32_t pix = 0u;
+    v3 hp = V3s(0.0f), nrm = V3(0.0f, 1.0f, 0.0f);
+    v4 hit = v4{0.0f, 0.0f, 0.0f, 0.0f};
+    if (active) {
+      pix = A.q_light[i >> 3];
+      const PrimaryCtx c = primary_ctx(s, pix % A.iw, pix / A.iw, A.iw);
+      const HitGeom g = load_pixhit(s, A.pix_hit + (size_t)pix * 5u);
+      hp = c.ro + c.rd * g.t;
+      nrm = g.n;
+      const LightFrame F = light_frame(s, hp, nrm, g.root_bmin);
+      hit = dda_hit_light(s, F.p0, light_ray_dir(F, nrm, ray), LIGHT_MAX_DIST_VOX, vs_(s));
+    }
+    v4 h[LIGHT_RAYS];
+    for (uint32_t k = 0; k < LIGHT_RAYS; ++k) {
+      h[k].x = __shfl_sync(0xFFFFFFFFu, hit.x, group0 + k);
+      h[k].y = __shfl_sync(0xFFFFFFFFu, hit.y, group0 + k);
+      h[k].z = __shfl_sync(0xFFFFFFFFu, hit.z, group0 + k);
+      h[k].w = __shfl_sync(0xFFFFFFFFu, hit.w, group0 + k);
+    }
+    if (active && ray == 0u) {
+      uint32_t hits = 0u;
+      v3 sum = V3s(0.0f);
+      for (uint32_t k = 0; k < LIGHT_RAYS; ++k)
+        if (light_accum(s, hp, nrm, h[k], hits, sum)) break;
+      const v3 r = light_finish(sum);
+      A.px_light[pix] = make_float4(r.x, r.y, r.z, 0.0f);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_vox(const __grid_constant__ FrameArgs A) {
+  const Scene s = make_scene(A, false);
+  const uint32_t n = A.q_count[0];
+  for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < n; i += gridDim.x * SHADE_THREADS) {
+    const uint32_t pix = A.q_vox[i];
+    const PrimaryCtx c = primary_ctx(s, pix % A.iw, pix / A.iw, A.iw);
+    const uint4* src = A.pix_hit + (size_t)pix * 5u;
+    const HitGeom g = load_pixhit(s, src);  // t and n as refined by k_shade_prep
+    const uint4 e = src[3], f = src[4];
+    const float shadow_out = shadow_fresh(c) ? shadow_blend(s, A, c, c.ro + c.rd * g.t, A.px_shadow[pix])
+                                             : clampf(A.shadow_in[c.pix], 0.0f, 1.0f);
+    v3 light = V3s(0.0f);
+    if (lights_wanted(g)) {
+      const float4 l = A.px_light[pix];
+      light = V3(l.x, l.y, l.z);
+    }
+    shade_voxel_final(s, A, c, g, shadow_out, light, e.w != 0u, f.x, i3{(int32_t)f.y, (int32_t)f.z, (int32_t)f.w});
+  }
 }
 
 __global__ void __launch_bounds__(SHADE_THREADS) k_shade_far(const __grid_constant__ FrameArgs A) {
-  const uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x;
-  if (i >= A.q_count[1]) return;
   const Scene s = make_scene(A, false);
-  const uint32_t pix = A.q_far[i];
-  const PrimaryCtx c = primary_ctx(s, pix % A.iw, pix / A.iw, A.iw);
-  shade_far_pixel(s, A, c);
+  const uint32_t n = A.q_count[1];
+  for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < n; i += gridDim.x * SHADE_THREADS) {
+    const uint32_t pix = A.q_far[i];
+    const PrimaryCtx c = primary_ctx(s, pix % A.iw, pix / A.iw, A.iw);
+    shade_far_pixel(s, A, c);
+  }
 }
 
 // ---------------------------------------------------------------------------

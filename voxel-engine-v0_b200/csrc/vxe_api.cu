@@ -41,7 +41,7 @@ struct DevBuf {
 enum Img {
   IMG_COLOR, IMG_DEPTH, IMG_LOCAL, IMG_HIST0, IMG_HIST1, IMG_SHADOW0, IMG_SHADOW1, IMG_LHIST0, IMG_LHIST1,
   IMG_GOD0, IMG_GOD1, IMG_PRE_TAA, IMG_OUTPUT, IMG_OHIST0, IMG_OHIST1, IMG_HITS, IMG_TILE_COUNT, IMG_TILE_SLOTS,
-  IMG_PIXHIT, IMG_QVOX, IMG_QFAR, IMG_QCOUNT,
+  IMG_PIXHIT, IMG_QVOX, IMG_QFAR, IMG_QCOUNT, IMG_QSHADOW, IMG_QLIGHT, IMG_PXSHADOW, IMG_PXLIGHT,
   IMG_N
 };
 
@@ -88,8 +88,9 @@ struct vxe_ctx {
   cudaStream_t compute = nullptr, upload = nullptr;
   cudaEvent_t upload_done = nullptr;
   bool upload_pending = false;
-  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
-  bool timed = false;
+  // frame events: start, grass table, tiles, trace, shading, godray, composite
+  cudaEvent_t ev[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool timed = false, timed_trace = false;
   // arenas
   DevBuf nodes, ropes, metas, macro, colinfo, grid, clip_tex, errword;
   GrassTable gt;
@@ -105,6 +106,7 @@ struct vxe_ctx {
   // lists, queue heads, captured graph) so several batches can be in flight
   BatchLane lanes[VXE_BATCH_LANES];
   int b_trace_grid = 0, b_tile_grid = 0;
+  int shade_wave = 148 * 16;  // blocks of the grid-stride shading kernels
   bool upload_recorded = false;
 };
 
@@ -168,8 +170,10 @@ size_t img_bytes(const vxe_ctx* c, int i) {
       return tiles * 4 * VXE_PRIMARY_MAX_TILE_CHUNKS;
     case IMG_PIXHIT:
       return in * 80;
-    case IMG_QVOX: case IMG_QFAR:
+    case IMG_QVOX: case IMG_QFAR: case IMG_QSHADOW: case IMG_QLIGHT: case IMG_PXSHADOW:
       return in * 4;
+    case IMG_PXLIGHT:
+      return in * 16;
     case IMG_QCOUNT:
       return 16;
     default:
@@ -377,6 +381,10 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
   A.q_vox = (uint32_t*)c->img[IMG_QVOX].p;
   A.q_far = (uint32_t*)c->img[IMG_QFAR].p;
   A.q_count = (uint32_t*)c->img[IMG_QCOUNT].p;
+  A.q_shadow = (uint32_t*)c->img[IMG_QSHADOW].p;
+  A.q_light = (uint32_t*)c->img[IMG_QLIGHT].p;
+  A.px_shadow = (float*)c->img[IMG_PXSHADOW].p;
+  A.px_light = (float4*)c->img[IMG_PXLIGHT].p;
   const uint32_t tiles_x = (c->iw + 7) / 8, tiles_y = (c->ih + 7) / 8;
   const uint32_t tiles = tiles_x * tiles_y;
   const uint32_t npix = c->iw * c->ih;
@@ -386,28 +394,39 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
   vxe_status gst = grass_table_acquire(c, c->compute, 0, c->cam, &use_grass);
   if (gst != VXE_OK) return gst;
   if (use_grass) grass_table_args(c, A);
-  k_tiles<<<(tiles + TILE_THREADS - 1) / TILE_THREADS, TILE_THREADS, 0, c->compute>>>(A);
   if (timed) CK(cudaEventRecord(c->ev[1], c->compute));
+  k_tiles<<<(tiles + TILE_THREADS - 1) / TILE_THREADS, TILE_THREADS, 0, c->compute>>>(A);
+  if (timed) CK(cudaEventRecord(c->ev[2], c->compute));
   if (c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL) {
     k_primary<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, c->compute>>>(A);
+    if (timed) CK(cudaEventRecord(c->ev[3], c->compute));
   } else {
     CK(cudaMemsetAsync(A.q_count, 0, 16, c->compute));
     k_primary_trace<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, c->compute>>>(A);
-    // Queue lengths stay on the device: the shading grids cover every pixel
-    // and threads past the class count exit at once.
-    k_shade_vox<<<(npix + SHADE_THREADS - 1) / SHADE_THREADS, SHADE_THREADS, 0, c->compute>>>(A);
-    k_shade_far<<<(npix + SHADE_THREADS - 1) / SHADE_THREADS, SHADE_THREADS, 0, c->compute>>>(A);
+    if (timed) CK(cudaEventRecord(c->ev[3], c->compute));
+    // Queue lengths stay on the device: each shading kernel walks its queue
+    // with a grid-stride loop over at most a full wave of blocks.
+    auto grid = [&](uint64_t threads) {
+      return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((threads + SHADE_THREADS - 1) / SHADE_THREADS,
+                                                                (uint64_t)c->shade_wave));
+    };
+    k_shade_prep<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
+    k_shade_shadow<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
+    k_shade_lights<<<grid((uint64_t)npix * 8u), SHADE_THREADS, 0, c->compute>>>(A);
+    k_shade_vox<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
+    k_shade_far<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
   }
-  if (timed) CK(cudaEventRecord(c->ev[2], c->compute));
+  if (timed) CK(cudaEventRecord(c->ev[4], c->compute));
   k_godray<<<dim3((c->iw + POST_THREADS_X - 1) / POST_THREADS_X, (c->ih + POST_THREADS_Y - 1) / POST_THREADS_Y),
              dim3(POST_THREADS_X, POST_THREADS_Y), 0, c->compute>>>(A);
-  if (timed) CK(cudaEventRecord(c->ev[3], c->compute));
+  if (timed) CK(cudaEventRecord(c->ev[5], c->compute));
   k_composite<<<dim3((c->pw + POST_THREADS_X - 1) / POST_THREADS_X, (c->ph + POST_THREADS_Y - 1) / POST_THREADS_Y),
                 dim3(POST_THREADS_X, POST_THREADS_Y), 0, c->compute>>>(A);
-  if (timed) CK(cudaEventRecord(c->ev[4], c->compute));
+  if (timed) CK(cudaEventRecord(c->ev[6], c->compute));
   CK(cudaGetLastError());
   if (use_grass && (gst = grass_table_release(c, c->compute, 0)) != VXE_OK) return gst;
   c->timed = timed;
+  c->timed_trace = timed && !(c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL);
   c->ping = q;
   return VXE_OK;
 }
@@ -472,6 +491,11 @@ vxe_status vxe_create(const vxe_config* cfg, vxe_ctx** out) {
   for (auto& e : c->gt.reader)
     if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return bail(VXE_ERR_DEVICE);
   c->cam.chunk_size = 64u;
+  {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device) == cudaSuccess && sms > 0)
+      c->shade_wave = sms * 16;
+  }
   *out = c;
   return VXE_OK;
 }
@@ -685,14 +709,16 @@ vxe_status vxe_get_timings(vxe_ctx* c, vxe_timings* t) {
   std::memset(t, 0, sizeof *t);
   if (!c->timed) return VXE_OK;
   cudaSetDevice(c->device);
-  CK(cudaEventSynchronize(c->ev[4]));
-  float ms[4];
-  for (int i = 0; i < 4; ++i) CK(cudaEventElapsedTime(&ms[i], c->ev[i], c->ev[i + 1]));
-  t->tiles = ms[0];
-  t->primary = ms[1];
-  t->godray = ms[2];
-  t->composite = ms[3];
-  t->total = (double)ms[0] + ms[1] + ms[2] + ms[3];
+  CK(cudaEventSynchronize(c->ev[6]));
+  float ms[6];
+  for (int i = 0; i < 6; ++i) CK(cudaEventElapsedTime(&ms[i], c->ev[i], c->ev[i + 1]));
+  t->grass_cells = ms[0];
+  t->tiles = (double)ms[0] + ms[1];
+  t->primary_trace = c->timed_trace ? ms[2] : 0.0;
+  t->primary = (double)ms[2] + ms[3];
+  t->godray = ms[4];
+  t->composite = ms[5];
+  t->total = (double)ms[0] + ms[1] + ms[2] + ms[3] + ms[4] + ms[5];
   return VXE_OK;
 }
 

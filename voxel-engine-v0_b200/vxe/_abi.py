@@ -109,7 +109,7 @@ class Hit(C.Structure):
 
 class Timings(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("primary", "local_taa", "godray", "composite", "composite_taa", "tiles",
-                                           "total")]
+                                           "total", "primary_trace", "grass_cells")]
 
 
 class WorldParams(C.Structure):
