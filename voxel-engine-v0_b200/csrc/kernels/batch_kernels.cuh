@@ -125,9 +125,10 @@ __device__ __noinline__ HitRec viewport_pixel_hit(const Scene& s, const uint32_t
   const size_t tile = (size_t)(gy >> 3) * tiles_x + (gx >> 3);
   const uint32_t cnt = tile_count[tile];
   VoxTraceResult vt{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
+  ProbeHook ph = probe_hook_inline();
   if (s.cam->chunk_count != 0u && cnt != 0u)
     vt = trace_candidates(s, tile_slots + tile * TILE_CANDS, nullptr, ro, rd, 0.0f, FOG_MAX_DIST, false,
-                          i3{0, 0, 0}, INVALID, cnt);
+                          i3{0, 0, 0}, INVALID, cnt, ph);
   if (vt.in_grid && vt.best.hit != 0u) {
     HitGeom best = vt.best;
     if (best.mat == MAT_GRASS) {

@@ -988,11 +988,15 @@ __device__ __forceinline__ ColInfo colinfo_decode(uint32_t e) {
   return ColInfo{true, y8, m8};
 }
 
-__device__ __noinline__ GrassHit probe_grass_columns_xz_dda(const Scene& s, v3 ro, v3 rd, v3 inv, float t0_in, float t1_in, v3 rb,
-                                    i3 origin_vox, float vs, uint32_t colinfo_base, float time_s,
-                                    float strength) {  // chunk_trace.wgsl:1358-1504
+// The column DDA of probe_grass_columns_xz_dda (chunk_trace.wgsl:1358-1504):
+// calls visit(it, t, tNext, id) for every grass column (in DDA order, `it`
+// the iteration) whose grass slab the ray segment [t, tNext] overlaps in y;
+// stops when visit returns true.
+template <class F>
+__device__ __forceinline__ void grass_columns_dda(const Scene& s, v3 ro, v3 rd, v3 inv, float t0_in, float t1_in,
+                                                  v3 rb, i3 origin_vox, float vs, uint32_t colinfo_base, F&& visit) {
   const float t0 = t0_in, t1 = t1_in;
-  if (t1 <= t0) return GrassHit{false, BIG, V3s(0.0f)};
+  if (t1 <= t0) return;
   const float eps = 1e-4f * vs;
   float t = t0 + eps;
   if (t > t1) t = t0;
@@ -1025,8 +1029,7 @@ __device__ __noinline__ GrassHit probe_grass_columns_xz_dda(const Scene& s, v3 r
       const float yA = ro.y + rd.y * t, yB = ro.y + rd.y * tNext;
       const float seg0 = fmin_(yA, yB), seg1 = fmax_(yA, yB);
       if (!(seg1 < sy0 || seg0 > sy1)) {
-        const GrassHit gh = try_grass_slab_hit(s, ro, rd, t, tNext, cb, id, vs, time_s, strength);
-        if (gh.hit) return gh;
+        if (visit(it, t, tNext, id)) return;
       }
     }
     if (tNext >= t1) break;
@@ -1038,7 +1041,19 @@ __device__ __noinline__ GrassHit probe_grass_columns_xz_dda(const Scene& s, v3 r
     if (lx < 0 || lx > 63 || lz < 0 || lz > 63) break;
     p = ro + rd * t;
   }
-  return GrassHit{false, BIG, V3s(0.0f)};
+}
+
+__device__ __noinline__ GrassHit probe_grass_columns_xz_dda(const Scene& s, v3 ro, v3 rd, v3 inv, float t0_in, float t1_in, v3 rb,
+                                    i3 origin_vox, float vs, uint32_t colinfo_base, float time_s,
+                                    float strength) {  // chunk_trace.wgsl:1358-1504
+  GrassHit out{false, BIG, V3s(0.0f)};
+  grass_columns_dda(s, ro, rd, inv, t0_in, t1_in, rb, origin_vox, vs, colinfo_base,
+                    [&](uint32_t, float t, float tNext, v3 id) {
+                      const GrassHit gh = try_grass_slab_hit(s, ro, rd, t, tNext, id * vs, id, vs, time_s, strength);
+                      if (gh.hit) out = gh;
+                      return gh.hit;
+                    });
+  return out;
 }
 
 struct TraceOpts { bool geom_only; };
@@ -1051,9 +1066,80 @@ __device__ __forceinline__ HitGeom make_hit(uint32_t mat, float t, v3 n, v3 rb, 
   return o;
 }
 
+// ---------------------------------------------------------------------------
+// Grass column probes of the leaf walk.
+//
+// The walk (chunk_trace.wgsl:669-961) probes the grass columns of every small
+// air leaf it crosses and ends the chunk at the first probe that hits.  The
+// probes are most of the primary trace's work and are reached by single lanes
+// deep inside divergent walks, so the wavefront schedule runs them apart:
+//   PROBE_RECORD  the walk stores each probe (pixel, order, chunk slot,
+//                 interval) and goes on as if it missed: the voxel-only walk;
+//   (k_probe_dda runs each stored probe's column DDA, one lane each, and
+//                 stores one task per grass slab it meets; k_slab_eval marches
+//                 the slabs, one lane each, and keeps per pixel the first hit
+//                 in walk order);
+//   PROBE_REPLAY  pixels that had a hit (or more probes than were stored) walk
+//                 again: probes before the first hit are known misses, the
+//                 first hit returns the stored result, later ones run inline.
+// The walk up to the first hit is the same in both passes, so every pixel's
+// result is the reference's, operation for operation.  PROBE_INLINE is the
+// reference order (megakernel, batches, queries).
+// ---------------------------------------------------------------------------
+enum : uint32_t { PROBE_INLINE = 0u, PROBE_RECORD = 1u, PROBE_REPLAY = 2u };
+
+struct ProbeRec {
+  uint32_t pixel, seq, slot;
+  float t0, t1;
+};
+
+struct ProbeHook {
+  uint32_t mode;
+  uint32_t seq;       // probes met so far, in walk order
+  uint32_t slot;      // chunk slot of the walk in progress
+  uint32_t pixel;
+  uint32_t recorded;  // record: probes stored; replay: probes the record pass stored
+  ProbeRec* recs;
+  uint32_t* rec_count;
+  uint32_t rec_cap;
+  uint32_t hit_seq;   // replay: first probe that hit (INVALID: none)
+  GrassHit hit;
+};
+
+__device__ __forceinline__ ProbeHook probe_hook_inline() {
+  ProbeHook h;
+  h.mode = PROBE_INLINE;
+  h.seq = 0u;
+  h.slot = INVALID;
+  h.pixel = 0u;
+  h.recorded = 0u;
+  h.recs = nullptr;
+  h.rec_count = nullptr;
+  h.rec_cap = 0u;
+  h.hit_seq = INVALID;
+  h.hit = GrassHit{false, BIG, V3s(0.0f)};
+  return h;
+}
+
+// Stores probe `seq` of this lane's pixel; lanes that reach the store together
+// share one atomic.  Stored probes of a pixel are always a prefix of its
+// sequence (the counter only grows).
+__device__ __forceinline__ void probe_record(ProbeHook& ph, float t0, float t1) {
+  const uint32_t mask = __activemask();
+  const uint32_t lane = threadIdx.x & 31u, leader = __ffs(mask) - 1u;
+  uint32_t base = 0u;
+  if (lane == leader) base = atomicAdd(ph.rec_count, (uint32_t)__popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  const uint32_t idx = base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+  if (idx < ph.rec_cap && ph.recorded == ph.seq) {
+    ph.recs[idx] = ProbeRec{ph.pixel, ph.seq, ph.slot, t0, t1};
+    ++ph.recorded;
+  }
+}
+
 __device__ __noinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(const Scene& s, v3 ro, v3 rd, v3 inv, const Meta& ch,
                                                    float t_enter, float t_exit, bool use_anchor,
-                                                   uint32_t anchor_key, const TraceOpts& opt) {
+                                                   uint32_t anchor_key, const TraceOpts& opt, ProbeHook& ph) {
   // chunk_trace.wgsl:669-961
   const float vs = vs_(s);
   const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vs;
@@ -1093,8 +1179,17 @@ __device__ __noinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(const
           const float t0p = fmax_(t_enter, tcur - eps_step);
           const float t1p = fmin_(t_leave, t_exit);
           if (t1p >= t0p) {
-            const GrassHit gh = probe_grass_columns_xz_dda(s, ro, rd, inv, t0p, t1p, rb, ov, vs, ch.colinfo_base,
-                                                           time_s, strength);
+            GrassHit gh{false, BIG, V3s(0.0f)};
+            if (ph.mode == PROBE_RECORD) {
+              probe_record(ph, t0p, t1p);
+            } else if (ph.mode == PROBE_REPLAY && ph.seq < ph.recorded && ph.seq < ph.hit_seq) {
+              // known miss
+            } else if (ph.mode == PROBE_REPLAY && ph.seq == ph.hit_seq) {
+              gh = ph.hit;
+            } else {
+              gh = probe_grass_columns_xz_dda(s, ro, rd, inv, t0p, t1p, rb, ov, vs, ch.colinfo_base, time_s, strength);
+            }
+            ++ph.seq;
             if (gh.hit) {
               const uint32_t nd = leaf.has_node ? ch.node_base + leaf.idx_local : INVALID;
               return ChunkTraceResult{make_hit(MAT_GRASS, gh.t, gh.n, rb, rs, ch, nd, leaf.bmin, leaf.size),
@@ -1186,7 +1281,7 @@ __device__ __noinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(const
 
 __device__ __noinline__ ChunkTraceResult trace_chunk_interval_stream_macro(const Scene& s, v3 ro, v3 rd, v3 inv, const Meta& ch,
                                                    float t0_in, float t1_in, bool use_anchor, uint32_t anchor_key_in,
-                                                   const TraceOpts& opt) {  // chunk_trace.wgsl:592-667
+                                                   const TraceOpts& opt, ProbeHook& ph) {  // chunk_trace.wgsl:592-667
   const float vs = vs_(s);
   const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vs;
   const float rs = (float)s.cam->chunk_size * vs;
@@ -1196,10 +1291,10 @@ __device__ __noinline__ ChunkTraceResult trace_chunk_interval_stream_macro(const
   uint32_t anchor_key = anchor_key_in;
   bool anchor_valid = use_anchor;
   if (ch.macro_base == INVALID)
-    return trace_chunk_rope_interval_nomacro(s, ro, rd, inv, ch, tcur, t_end, anchor_valid, anchor_key, opt);
+    return trace_chunk_rope_interval_nomacro(s, ro, rd, inv, ch, tcur, t_end, anchor_valid, anchor_key, opt, ph);
   MacroDDAState ms = macro_dda_init(ro, rd, inv, tcur, rb, rs, ch.macro_base);
   if (!ms.enabled)
-    return trace_chunk_rope_interval_nomacro(s, ro, rd, inv, ch, tcur, t_end, anchor_valid, anchor_key, opt);
+    return trace_chunk_rope_interval_nomacro(s, ro, rd, inv, ch, tcur, t_end, anchor_valid, anchor_key, opt, ph);
   for (uint32_t i = 0; i < 128u; ++i) {
     if (tcur >= t_end) break;
     macro_dda_sync(ms, tcur);
@@ -1212,7 +1307,7 @@ __device__ __noinline__ ChunkTraceResult trace_chunk_interval_stream_macro(const
       continue;
     }
     const ChunkTraceResult h =
-        trace_chunk_rope_interval_nomacro(s, ro, rd, inv, ch, tcur, t_cell_exit, anchor_valid, anchor_key, opt);
+        trace_chunk_rope_interval_nomacro(s, ro, rd, inv, ch, tcur, t_cell_exit, anchor_valid, anchor_key, opt, ph);
     if (h.hit.hit != 0u) return h;
     anchor_valid = h.anchor_valid;
     anchor_key = h.anchor_key;

@@ -61,11 +61,22 @@ struct FrameArgs {
   uint4* pix_hit;     // 5 x uint4 per pixel (PixHit), written for voxel hits
   uint32_t* q_vox;    // pixel ids with a voxel hit
   uint32_t* q_far;    // pixel ids for heightfield / sky
-  uint32_t* q_count;  // [0] voxel, [1] far, [2] fresh shadow, [3] light gather
+  uint32_t* q_count;  // [0] voxel, [1] far, [2] fresh shadow, [3] light gather, [4] probes, [5] pending,
+                      // [6] slab tasks
   uint32_t* q_shadow;  // voxel pixels that trace a fresh sun shadow this frame
   uint32_t* q_light;   // voxel pixels that gather local lights
   float* px_shadow;    // fresh sun transmittance per pixel (q_shadow pixels)
   float4* px_light;    // light gather result per pixel (q_light pixels)
+  // deferred grass column probes (PROBE_RECORD -> k_probe_dda -> k_slab_eval
+  // -> PROBE_REPLAY)
+  ProbeRec* probe_recs;           // stored probes, q_count[4] of them (capped)
+  uint32_t probe_cap;
+  uint4* slab_tasks;              // 2 x uint4 per grass column slab to march, q_count[6] of them
+  float4* slab_res;               // per slab task: hit t, normal (written on hits)
+  uint32_t slab_cap;
+  unsigned long long* px_first;   // per pixel: first hit (seq << 38 | column << 32 | task), ~0 = none
+  uint2* px_probe;                // per pixel: probes met | voxel-hit bit 31, probes fully evaluated
+  uint32_t* q_pending;            // pixels whose walk met probes, q_count[5] of them
   // per-frame grass cell table: written by k_grass_cells, read by the rest
   float4* grass_rec;
   uint64_t grass_rec_n;  // records (slots * 4096)
@@ -225,7 +236,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_tiles(const __grid_constant__ 
 // staged in shared memory (slots + their ChunkMeta records).
 __device__ VoxTraceResult trace_candidates(const Scene& s, const uint32_t* cslot, const Meta* cmeta, v3 ro, v3 rd,
                                            float t_min, float t_max, bool anchor_valid_in, i3 anchor_chunk_in,
-                                           uint32_t anchor_key_in, uint32_t cand_count) {
+                                           uint32_t anchor_key_in, uint32_t cand_count, ProbeHook& ph) {
   VoxTraceResult none{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
   if (s.cam->chunk_count == 0u) return none;
   const float vsz = vs_(s);
@@ -261,7 +272,8 @@ __device__ VoxTraceResult trace_candidates(const Scene& s, const uint32_t* cslot
     const i3 cc{ch.ox / csz, ch.oy / csz, ch.oz / csz};
     const bool ua = anchor_valid_in && chunk_coords_neighbor(cc, anchor_chunk_in);
     const uint32_t aku = ua ? anchor_key_in : INVALID;
-    const ChunkTraceResult h = trace_chunk_interval_stream_macro(s, ro, rd, inv, ch, ce, cx, ua, aku, opt);
+    ph.slot = slot;
+    const ChunkTraceResult h = trace_chunk_interval_stream_macro(s, ro, rd, inv, ch, ce, cx, ua, aku, opt, ph);
     if (h.hit.hit != 0u && h.hit.t < best.t) {
       best = h.hit;
       bav = h.anchor_valid;
@@ -371,7 +383,8 @@ __device__ __forceinline__ PrimaryCtx primary_ctx(const Scene& s, uint32_t gx, u
 
 // History hint + voxel trace (ray_main.wgsl:274-325 and trace_primary_voxels :116-161).
 __device__ __noinline__ VoxTraceResult primary_trace(const Scene& s, const FrameArgs& A, const PrimaryCtx& c,
-                                                     const uint32_t* cslot, const Meta* cmeta, uint32_t tile_count) {
+                                                     const uint32_t* cslot, const Meta* cmeta, uint32_t tile_count,
+                                                     ProbeHook& ph) {
   VoxTraceResult vt{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
   if (s.cam->chunk_count == 0u || tile_count == 0u) return vt;
   const uint32_t W = A.iw, H = A.ih;
@@ -407,10 +420,11 @@ __device__ __noinline__ VoxTraceResult primary_trace(const Scene& s, const Frame
   const float t_end = fmin_(t_hist + PRIMARY_HIT_WINDOW, FOG_MAX_DIST);
   if (hist_valid) {
     const VoxTraceResult h = trace_candidates(s, cslot, cmeta, c.ro, c.rd, t_start, t_end, hak != INVALID, hac, hak,
-                                              tile_count);
+                                              tile_count, ph);
     if (h.best.hit != 0u) return h;
   }
-  return trace_candidates(s, cslot, cmeta, c.ro, c.rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID, tile_count);
+  return trace_candidates(s, cslot, cmeta, c.ro, c.rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID, tile_count,
+                          ph);
 }
 
 // main_local_taa (taa.wgsl:26-69) for one pixel, fused after its shading.
@@ -598,7 +612,8 @@ __global__ void __launch_bounds__(PRIMARY_THREADS) k_primary(const __grid_consta
   uint32_t t, gx, gy;
   if (!block_pixel(A, &t, &gx, &gy)) return;
   const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
-  const VoxTraceResult vt = primary_trace(s, A, c, cslot[t], cmeta[t], ccount[t]);
+  ProbeHook ph = probe_hook_inline();
+  const VoxTraceResult vt = primary_trace(s, A, c, cslot[t], cmeta[t], ccount[t], ph);
   if (vt.in_grid && vt.best.hit != 0u) shade_voxel_pixel(s, A, c, vt.best, vt.anchor_valid, vt.anchor_key, vt.anchor_chunk);
   else shade_far_pixel(s, A, c);
 }
@@ -626,6 +641,11 @@ __device__ __forceinline__ void enqueue(uint32_t* q, uint32_t* counter, bool min
   q[base + __popc(mask & ((1u << lane) - 1u))] = value;
 }
 
+__device__ __forceinline__ uint32_t warp_uniform_end(uint32_t n) { return (n + 31u) & ~31u; }
+
+// Voxel walk with the grass column probes stored, not evaluated.  Pixels that
+// met no probe are final here; the rest wait for k_probe_dda, k_slab_eval and
+// k_primary_resolve.
 __global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace(const __grid_constant__ FrameArgs A) {
   __shared__ uint32_t cslot[2][TILE_CANDS];
   __shared__ Meta cmeta[2][TILE_CANDS];
@@ -634,17 +654,122 @@ __global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace(const __grid_
   stage_tiles(s, A, cslot, cmeta, ccount);
   uint32_t t, gx, gy;
   const bool active = block_pixel(A, &t, &gx, &gy);
-  bool vox = false;
+  bool vox = false, pend = false;
   uint32_t pix = 0u;
   if (active) {
     const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
     pix = (uint32_t)c.pix;
-    const VoxTraceResult vt = primary_trace(s, A, c, cslot[t], cmeta[t], ccount[t]);
+    ProbeHook ph = probe_hook_inline();
+    ph.mode = PROBE_RECORD;
+    ph.pixel = pix;
+    ph.recs = A.probe_recs;
+    ph.rec_count = &A.q_count[4];
+    ph.rec_cap = A.probe_cap;
+    const VoxTraceResult vt = primary_trace(s, A, c, cslot[t], cmeta[t], ccount[t], ph);
     vox = vt.in_grid && vt.best.hit != 0u;
     if (vox) store_pixhit(A.pix_hit + (size_t)pix * 5u, vt.best, vt);
+    pend = ph.seq != 0u;
+    if (pend) A.px_probe[pix] = make_uint2(ph.seq | (vox ? 0x80000000u : 0u), ph.recorded);
   }
-  enqueue(A.q_vox, &A.q_count[0], active && vox, pix);
-  enqueue(A.q_far, &A.q_count[1], active && !vox, pix);
+  enqueue(A.q_vox, &A.q_count[0], active && vox && !pend, pix);
+  enqueue(A.q_far, &A.q_count[1], active && !vox && !pend, pix);
+  enqueue(A.q_pending, &A.q_count[5], active && pend, pix);
+}
+
+// One lane per stored probe: the probe's column DDA with the walk's
+// arguments, storing one task per grass slab it would march.  A probe whose
+// tasks do not all fit marks itself (and every later probe of its pixel) as
+// not evaluated, by lowering the pixel's evaluated count to its order.
+__global__ void __launch_bounds__(SHADE_THREADS) k_probe_dda(const __grid_constant__ FrameArgs A) {
+  const Scene s = make_scene(A, false);
+  const uint32_t n = min(A.q_count[4], A.probe_cap);
+  const float vs = vs_(s);
+  for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < n; i += gridDim.x * SHADE_THREADS) {
+    const ProbeRec r = A.probe_recs[i];
+    const PrimaryCtx c = primary_ctx(s, r.pixel % A.iw, r.pixel / A.iw, A.iw);
+    const Meta ch = meta_at(s, r.slot);
+    const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vs;
+    const i3 ov{ch.ox, ch.oy, ch.oz};
+    bool lost = false;
+    grass_columns_dda(s, c.ro, c.rd, safe_inv3(c.rd), r.t0, r.t1, rb, ov, vs, ch.colinfo_base,
+                      [&](uint32_t it, float t, float tNext, v3 id) {
+                        const uint32_t j = atomicAdd(&A.q_count[6], 1u);
+                        if (j < A.slab_cap) {
+                          A.slab_tasks[2u * j] = make_uint4(i, it, __float_as_uint(t), __float_as_uint(tNext));
+                          A.slab_tasks[2u * j + 1u] = make_uint4(__float_as_uint(id.x), __float_as_uint(id.y),
+                                                                 __float_as_uint(id.z), 0u);
+                        } else {
+                          lost = true;
+                        }
+                        return false;
+                      });
+    if (lost) atomicMin(&A.px_probe[r.pixel].y, r.seq);
+  }
+}
+
+// One lane per grass slab: try_grass_slab_hit (the blade march); hits keep,
+// per pixel, the first (probe order, column order) one.
+__global__ void __launch_bounds__(SHADE_THREADS) k_slab_eval(const __grid_constant__ FrameArgs A) {
+  const Scene s = make_scene(A, false);
+  const uint32_t n = min(A.q_count[6], A.slab_cap);
+  const float vs = vs_(s);
+  const float time_s = s.cam->voxel_params[1], strength = s.cam->voxel_params[2];
+  for (uint32_t j = blockIdx.x * SHADE_THREADS + threadIdx.x; j < n; j += gridDim.x * SHADE_THREADS) {
+    const uint4 a = A.slab_tasks[2u * j], b = A.slab_tasks[2u * j + 1u];
+    const ProbeRec r = A.probe_recs[a.x];
+    const PrimaryCtx c = primary_ctx(s, r.pixel % A.iw, r.pixel / A.iw, A.iw);
+    const v3 id = V3(__uint_as_float(b.x), __uint_as_float(b.y), __uint_as_float(b.z));
+    const GrassHit gh = try_grass_slab_hit(s, c.ro, c.rd, __uint_as_float(a.z), __uint_as_float(a.w), id * vs, id, vs,
+                                           time_s, strength);
+    if (gh.hit) {
+      A.slab_res[j] = make_float4(gh.t, gh.n.x, gh.n.y, gh.n.z);
+      atomicMin(&A.px_first[r.pixel],
+                ((unsigned long long)r.seq << 38) | ((unsigned long long)a.y << 32) | (unsigned long long)j);
+    }
+  }
+}
+
+// Pixels that met probes: if every probe was stored and none hit, the voxel
+// walk's result stands; otherwise the walk runs again with the known probe
+// results (PROBE_REPLAY).
+__global__ void __launch_bounds__(SHADE_THREADS) k_primary_resolve(const __grid_constant__ FrameArgs A) {
+  const Scene s = make_scene(A, false);
+  const uint32_t n = A.q_count[5], end = warp_uniform_end(n);
+  const uint32_t tiles_x = (A.iw + 7u) / 8u;
+  for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < end; i += gridDim.x * SHADE_THREADS) {
+    bool active = i < n, vox = false;
+    uint32_t pix = 0u;
+    if (active) {
+      pix = A.q_pending[i];
+      const uint2 pp = A.px_probe[pix];
+      const unsigned long long first = A.px_first[pix];
+      const uint32_t met = pp.x & 0x7FFFFFFFu;
+      // a hit counts only if every probe up to it was evaluated
+      const bool hit_known = first != ~0ull && (uint32_t)(first >> 38) < pp.y;
+      if (first == ~0ull && pp.y == met) {
+        vox = (pp.x >> 31) != 0u;
+      } else {
+        const uint32_t gx = pix % A.iw, gy = pix / A.iw;
+        const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
+        const size_t tile = (size_t)(gy >> 3) * tiles_x + (gx >> 3);
+        ProbeHook ph = probe_hook_inline();
+        ph.mode = PROBE_REPLAY;
+        ph.pixel = pix;
+        ph.recorded = pp.y;
+        if (hit_known) {
+          ph.hit_seq = (uint32_t)(first >> 38);
+          const float4 r = A.slab_res[(uint32_t)(first & 0xFFFFFFFFull)];
+          ph.hit = GrassHit{true, r.x, V3(r.y, r.z, r.w)};
+        }
+        const VoxTraceResult vt = primary_trace(s, A, c, A.tile_slots + tile * TILE_CANDS, nullptr,
+                                                A.tile_count[tile], ph);
+        vox = vt.in_grid && vt.best.hit != 0u;
+        if (vox) store_pixhit(A.pix_hit + (size_t)pix * 5u, vt.best, vt);
+      }
+    }
+    enqueue(A.q_vox, &A.q_count[0], active && vox, pix);
+    enqueue(A.q_far, &A.q_count[1], active && !vox, pix);
+  }
 }
 
 __device__ __forceinline__ HitGeom load_pixhit(const Scene& s, const uint4* src) {
@@ -668,7 +793,6 @@ __device__ __forceinline__ HitGeom load_pixhit(const Scene& s, const uint4* src)
 // fresh shadows | light gathers -> final.  Each kernel walks its queue with
 // a grid-stride loop whose trip count is uniform per warp (queues are read on
 // the device), so the warp-wide enqueue and shuffles see every lane.
-__device__ __forceinline__ uint32_t warp_uniform_end(uint32_t n) { return (n + 31u) & ~31u; }
 
 __global__ void __launch_bounds__(SHADE_THREADS) k_shade_prep(const __grid_constant__ FrameArgs A) {
   const Scene s = make_scene(A, false);
@@ -1018,7 +1142,8 @@ __device__ __forceinline__ HitRec trace_query_ray(const Scene& s, v3 ro, v3 rd, 
     const v2 rt = intersect_aabb(ro, rd, rb, rb + V3s(rs));
     const float ce = fmax_(rt.x, 0.0f), cx = fmin_(rt.y, fmin_(tmax, FOG_MAX_DIST));
     if (cx < ce) return false;
-    const ChunkTraceResult h = trace_chunk_interval_stream_macro(s, ro, rd, inv, ch, ce, cx, false, INVALID, opt);
+    ProbeHook ph = probe_hook_inline();
+    const ChunkTraceResult h = trace_chunk_interval_stream_macro(s, ro, rd, inv, ch, ce, cx, false, INVALID, opt, ph);
     if (h.hit.hit != 0u) {
       best = h.hit;
       return true;

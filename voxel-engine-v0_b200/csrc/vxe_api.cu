@@ -42,6 +42,7 @@ enum Img {
   IMG_COLOR, IMG_DEPTH, IMG_LOCAL, IMG_HIST0, IMG_HIST1, IMG_SHADOW0, IMG_SHADOW1, IMG_LHIST0, IMG_LHIST1,
   IMG_GOD0, IMG_GOD1, IMG_PRE_TAA, IMG_OUTPUT, IMG_OHIST0, IMG_OHIST1, IMG_HITS, IMG_TILE_COUNT, IMG_TILE_SLOTS,
   IMG_PIXHIT, IMG_QVOX, IMG_QFAR, IMG_QCOUNT, IMG_QSHADOW, IMG_QLIGHT, IMG_PXSHADOW, IMG_PXLIGHT,
+  IMG_PROBE_RECS, IMG_SLAB_TASKS, IMG_SLAB_RES, IMG_PXFIRST, IMG_PXPROBE, IMG_QPENDING,
   IMG_N
 };
 
@@ -151,6 +152,12 @@ void release(DevBuf& b) {
   b.bytes = 0;
 }
 
+// Stored grass column probes per internal pixel (the walk meets about four
+// per pixel on grassland; pixels past the cap replay their walk).
+constexpr size_t kProbesPerPixel = 8;
+// Grass slab marches those probes ask for, per internal pixel.
+constexpr size_t kSlabsPerPixel = 4;
+
 size_t img_bytes(const vxe_ctx* c, int i) {
   const size_t in = (size_t)c->iw * c->ih, pn = (size_t)c->pw * c->ph;
   const size_t tiles = (size_t)((c->iw + 7) / 8) * ((c->ih + 7) / 8);
@@ -170,12 +177,20 @@ size_t img_bytes(const vxe_ctx* c, int i) {
       return tiles * 4 * VXE_PRIMARY_MAX_TILE_CHUNKS;
     case IMG_PIXHIT:
       return in * 80;
-    case IMG_QVOX: case IMG_QFAR: case IMG_QSHADOW: case IMG_QLIGHT: case IMG_PXSHADOW:
+    case IMG_QVOX: case IMG_QFAR: case IMG_QSHADOW: case IMG_QLIGHT: case IMG_PXSHADOW: case IMG_QPENDING:
       return in * 4;
+    case IMG_PROBE_RECS:
+      return in * kProbesPerPixel * sizeof(vxe::dev::ProbeRec);
+    case IMG_SLAB_TASKS:
+      return in * kSlabsPerPixel * 32;
+    case IMG_SLAB_RES:
+      return in * kSlabsPerPixel * 16;
+    case IMG_PXFIRST: case IMG_PXPROBE:
+      return in * 8;
     case IMG_PXLIGHT:
       return in * 16;
     case IMG_QCOUNT:
-      return 16;
+      return 32;
     default:
       return 0;
   }
@@ -385,6 +400,14 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
   A.q_light = (uint32_t*)c->img[IMG_QLIGHT].p;
   A.px_shadow = (float*)c->img[IMG_PXSHADOW].p;
   A.px_light = (float4*)c->img[IMG_PXLIGHT].p;
+  A.probe_recs = (vxe::dev::ProbeRec*)c->img[IMG_PROBE_RECS].p;
+  A.probe_cap = (uint32_t)std::min<size_t>(c->img[IMG_PROBE_RECS].bytes / sizeof(vxe::dev::ProbeRec), 0xFFFFFFFFu);
+  A.slab_tasks = (uint4*)c->img[IMG_SLAB_TASKS].p;
+  A.slab_res = (float4*)c->img[IMG_SLAB_RES].p;
+  A.slab_cap = (uint32_t)std::min<size_t>(c->img[IMG_SLAB_TASKS].bytes / 32u, 0xFFFFFFFFu);
+  A.px_first = (unsigned long long*)c->img[IMG_PXFIRST].p;
+  A.px_probe = (uint2*)c->img[IMG_PXPROBE].p;
+  A.q_pending = (uint32_t*)c->img[IMG_QPENDING].p;
   const uint32_t tiles_x = (c->iw + 7) / 8, tiles_y = (c->ih + 7) / 8;
   const uint32_t tiles = tiles_x * tiles_y;
   const uint32_t npix = c->iw * c->ih;
@@ -401,15 +424,19 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
     k_primary<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, c->compute>>>(A);
     if (timed) CK(cudaEventRecord(c->ev[3], c->compute));
   } else {
-    CK(cudaMemsetAsync(A.q_count, 0, 16, c->compute));
-    k_primary_trace<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, c->compute>>>(A);
-    if (timed) CK(cudaEventRecord(c->ev[3], c->compute));
-    // Queue lengths stay on the device: each shading kernel walks its queue
-    // with a grid-stride loop over at most a full wave of blocks.
+    // Queue lengths stay on the device: each kernel after the walk runs over
+    // its queue with a grid-stride loop over at most a full wave of blocks.
     auto grid = [&](uint64_t threads) {
       return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((threads + SHADE_THREADS - 1) / SHADE_THREADS,
                                                                 (uint64_t)c->shade_wave));
     };
+    CK(cudaMemsetAsync(A.q_count, 0, 32, c->compute));
+    CK(cudaMemsetAsync(A.px_first, 0xFF, (size_t)npix * 8u, c->compute));
+    k_primary_trace<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, c->compute>>>(A);
+    k_probe_dda<<<grid((uint64_t)npix * kProbesPerPixel), SHADE_THREADS, 0, c->compute>>>(A);
+    k_slab_eval<<<grid((uint64_t)npix * kSlabsPerPixel), SHADE_THREADS, 0, c->compute>>>(A);
+    k_primary_resolve<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
+    if (timed) CK(cudaEventRecord(c->ev[3], c->compute));
     k_shade_prep<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
     k_shade_shadow<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
     k_shade_lights<<<grid((uint64_t)npix * 8u), SHADE_THREADS, 0, c->compute>>>(A);
@@ -1174,8 +1201,10 @@ __global__ void __launch_bounds__(vxe::dev::PRIMARY_THREADS) k_hits_noalloc(cons
   const float vs = vs_(s);
   const v3 ro = c.ro, rd = c.rd;
   VoxTraceResult vt{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
+  ProbeHook ph = probe_hook_inline();
   if (s.cam->chunk_count != 0u && ccount[t] != 0u)
-    vt = trace_candidates(s, cslot[t], cmeta[t], ro, rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID, ccount[t]);
+    vt = trace_candidates(s, cslot[t], cmeta[t], ro, rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID, ccount[t],
+                          ph);
   HitRec rec = miss_rec();
   if (vt.in_grid && vt.best.hit != 0u) {
     HitGeom best = vt.best;
