@@ -406,9 +406,10 @@ def main():
         "e2e": {"value": round(e2e_val, 3), "unit": UNIT, "h2d_bytes_per_step": res["e2e"]["h2d_bytes_per_step"],
                 "d2h_bytes_per_step": res["e2e"]["d2h_bytes_per_step"],
                 "frame_ms": round(e2e_s * 1e3 / args.steps, 3)},
-        # per frame: k_grass_cells, k_tiles, k_primary_trace, k_probe_dda, k_slab_eval, k_primary_resolve,
-        # k_shade_prep, k_shade_shadow, k_shade_lights, k_shade_vox, k_shade_far, k_godray, k_composite
-        "gpu_launches": 13 * args.steps,
+        # per frame: k_grass_cells, k_tiles, k_primary_trace, k_probe_dda, k_slab_eval, k_slab_pick,
+        # k_primary_resolve, k_shade_prep, k_shade_shadow, k_shade_lights, k_shade_vox, k_shade_far, k_godray,
+        # k_composite
+        "gpu_launches": 14 * args.steps,
         "clocks": res["clocks"],
         "device_error_word": res["error_word"],
     }

@@ -1073,37 +1073,49 @@ __device__ __forceinline__ HitGeom make_hit(uint32_t mat, float t, v3 n, v3 rb, 
 // air leaf it crosses and ends the chunk at the first probe that hits.  The
 // probes are most of the primary trace's work and are reached by single lanes
 // deep inside divergent walks, so the wavefront schedule runs them apart:
-//   PROBE_RECORD  the walk stores each probe (pixel, order, chunk slot,
-//                 interval) and goes on as if it missed: the voxel-only walk;
-//   (k_probe_dda runs each stored probe's column DDA, one lane each, and
-//                 stores one task per grass slab it meets; k_slab_eval marches
-//                 the slabs, one lane each, and keeps per pixel the first hit
-//                 in walk order);
-//   PROBE_REPLAY  pixels that had a hit (or more probes than were stored) walk
-//                 again: probes before the first hit are known misses, the
-//                 first hit returns the stored result, later ones run inline.
-// The walk up to the first hit is the same in both passes, so every pixel's
-// result is the reference's, operation for operation.  PROBE_INLINE is the
-// reference order (megakernel, batches, queries).
+//   PROBE_RECORD  the walk stores each probe (interval, chunk, and the leaf and
+//                 anchor state a hit record needs) and goes on as if it missed;
+//   k_probe_dda   runs each stored probe's column DDA, one lane each, and
+//                 stores one task per grass slab it meets;
+//   k_slab_eval   marches every slab, one lane each;
+//   resolve       rebuilds the candidate loop's answer from the parts.
+// Why the parts suffice: the candidate loop keeps the nearest chunk result
+// (earliest chunk on ties) and a chunk's result is its first probe hit, else
+// its voxel hit.  A chunk walk does not depend on the loop's best so far, so
+// every chunk the reference walks is walked identically here (here fewer
+// chunks are skipped, as probe hits never lower the best).  Along one walk
+// probe intervals follow each other in t, so a chunk's first probe hit is
+// also its nearest; the answer is therefore the nearer of the nearest probe
+// hit over all chunks (key: t, chunk, probe, column) and the walk's voxel
+// answer, unless the voxel answer wins while its own chunk had a probe hit
+// (its grass-slab refinement reached below that hit): such pixels, and pixels
+// whose probes did not all fit the buffers, walk again with inline probes.
+// PROBE_INLINE is the reference order (megakernel, batches, queries, that
+// fallback).
 // ---------------------------------------------------------------------------
-enum : uint32_t { PROBE_INLINE = 0u, PROBE_RECORD = 1u, PROBE_REPLAY = 2u };
+enum : uint32_t { PROBE_INLINE = 0u, PROBE_RECORD = 1u };
 
-struct ProbeRec {
+struct ProbeRec {  // 56 B
   uint32_t pixel, seq, slot;
   float t0, t1;
+  uint32_t cand_phase;  // candidate index | trace phase << 8 (0 hint window, 1 full)
+  uint32_t node;        // hit-record leaf node (INVALID: implicit leaf)
+  float leaf_bmin[3], leaf_size;
+  uint32_t anchor_valid, anchor_key;
 };
 
 struct ProbeHook {
   uint32_t mode;
-  uint32_t seq;       // probes met so far, in walk order
-  uint32_t slot;      // chunk slot of the walk in progress
+  uint32_t seq;        // probes met so far, in walk order
+  uint32_t slot;       // chunk slot of the walk in progress
+  uint32_t cand;       // its index in the candidate list
+  uint32_t phase;      // 0 hint-window trace, 1 full trace
+  uint32_t best_cand;  // candidate index of the trace's current best (INVALID: none)
   uint32_t pixel;
-  uint32_t recorded;  // record: probes stored; replay: probes the record pass stored
+  uint32_t recorded;   // probes stored
   ProbeRec* recs;
   uint32_t* rec_count;
   uint32_t rec_cap;
-  uint32_t hit_seq;   // replay: first probe that hit (INVALID: none)
-  GrassHit hit;
 };
 
 __device__ __forceinline__ ProbeHook probe_hook_inline() {
@@ -1111,28 +1123,43 @@ __device__ __forceinline__ ProbeHook probe_hook_inline() {
   h.mode = PROBE_INLINE;
   h.seq = 0u;
   h.slot = INVALID;
+  h.cand = 0u;
+  h.phase = 1u;
+  h.best_cand = INVALID;
   h.pixel = 0u;
   h.recorded = 0u;
   h.recs = nullptr;
   h.rec_count = nullptr;
   h.rec_cap = 0u;
-  h.hit_seq = INVALID;
-  h.hit = GrassHit{false, BIG, V3s(0.0f)};
   return h;
 }
 
-// Stores probe `seq` of this lane's pixel; lanes that reach the store together
-// share one atomic.  Stored probes of a pixel are always a prefix of its
-// sequence (the counter only grows).
-__device__ __forceinline__ void probe_record(ProbeHook& ph, float t0, float t1) {
+// Stores this lane's probe; lanes that reach the store together share one
+// atomic.
+__device__ __forceinline__ void probe_record(ProbeHook& ph, float t0, float t1, uint32_t node, v3 leaf_bmin,
+                                             float leaf_size, bool anchor_valid, uint32_t anchor_key) {
   const uint32_t mask = __activemask();
   const uint32_t lane = threadIdx.x & 31u, leader = __ffs(mask) - 1u;
   uint32_t base = 0u;
   if (lane == leader) base = atomicAdd(ph.rec_count, (uint32_t)__popc(mask));
   base = __shfl_sync(mask, base, leader);
   const uint32_t idx = base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
-  if (idx < ph.rec_cap && ph.recorded == ph.seq) {
-    ph.recs[idx] = ProbeRec{ph.pixel, ph.seq, ph.slot, t0, t1};
+  if (idx < ph.rec_cap) {
+    ProbeRec r;
+    r.pixel = ph.pixel;
+    r.seq = ph.seq;
+    r.slot = ph.slot;
+    r.t0 = t0;
+    r.t1 = t1;
+    r.cand_phase = ph.cand | (ph.phase << 8);
+    r.node = node;
+    r.leaf_bmin[0] = leaf_bmin.x;
+    r.leaf_bmin[1] = leaf_bmin.y;
+    r.leaf_bmin[2] = leaf_bmin.z;
+    r.leaf_size = leaf_size;
+    r.anchor_valid = anchor_valid ? 1u : 0u;
+    r.anchor_key = anchor_key;
+    ph.recs[idx] = r;
     ++ph.recorded;
   }
 }
@@ -1180,15 +1207,11 @@ __device__ __noinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(const
           const float t1p = fmin_(t_leave, t_exit);
           if (t1p >= t0p) {
             GrassHit gh{false, BIG, V3s(0.0f)};
-            if (ph.mode == PROBE_RECORD) {
-              probe_record(ph, t0p, t1p);
-            } else if (ph.mode == PROBE_REPLAY && ph.seq < ph.recorded && ph.seq < ph.hit_seq) {
-              // known miss
-            } else if (ph.mode == PROBE_REPLAY && ph.seq == ph.hit_seq) {
-              gh = ph.hit;
-            } else {
+            if (ph.mode == PROBE_RECORD)
+              probe_record(ph, t0p, t1p, leaf.has_node ? ch.node_base + leaf.idx_local : INVALID, leaf.bmin,
+                           leaf.size, an.valid, an.key);
+            else
               gh = probe_grass_columns_xz_dda(s, ro, rd, inv, t0p, t1p, rb, ov, vs, ch.colinfo_base, time_s, strength);
-            }
             ++ph.seq;
             if (gh.hit) {
               const uint32_t nd = leaf.has_node ? ch.node_base + leaf.idx_local : INVALID;

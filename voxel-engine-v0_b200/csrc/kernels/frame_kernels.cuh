@@ -62,20 +62,23 @@ struct FrameArgs {
   uint32_t* q_vox;    // pixel ids with a voxel hit
   uint32_t* q_far;    // pixel ids for heightfield / sky
   uint32_t* q_count;  // [0] voxel, [1] far, [2] fresh shadow, [3] light gather, [4] probes, [5] pending,
-                      // [6] slab tasks
+                      // [6] slab tasks, [7] slab hits
   uint32_t* q_shadow;  // voxel pixels that trace a fresh sun shadow this frame
   uint32_t* q_light;   // voxel pixels that gather local lights
   float* px_shadow;    // fresh sun transmittance per pixel (q_shadow pixels)
   float4* px_light;    // light gather result per pixel (q_light pixels)
   // deferred grass column probes (PROBE_RECORD -> k_probe_dda -> k_slab_eval
-  // -> PROBE_REPLAY)
+  // -> k_slab_pick -> k_primary_resolve)
   ProbeRec* probe_recs;           // stored probes, q_count[4] of them (capped)
   uint32_t probe_cap;
   uint4* slab_tasks;              // 2 x uint4 per grass column slab to march, q_count[6] of them
   float4* slab_res;               // per slab task: hit t, normal (written on hits)
+  uint32_t* slab_hits;            // slab tasks that hit, q_count[7] of them
   uint32_t slab_cap;
-  unsigned long long* px_first;   // per pixel: first hit (seq << 38 | column << 32 | task), ~0 = none
-  uint2* px_probe;                // per pixel: probes met | voxel-hit bit 31, probes fully evaluated
+  unsigned long long* px_first;   // per pixel: nearest probe hit key (slab_key), ~0 = none
+  uint32_t* px_task;              // per pixel: the slab task with that key
+  uint2* px_mask;                 // per pixel: candidate chunks with a probe hit, hint / full trace
+  uint2* px_probe;                // per pixel: walk summary (probe_summary) | probes stored
   uint32_t* q_pending;            // pixels whose walk met probes, q_count[5] of them
   // per-frame grass cell table: written by k_grass_cells, read by the rest
   float4* grass_rec;
@@ -238,6 +241,7 @@ __device__ VoxTraceResult trace_candidates(const Scene& s, const uint32_t* cslot
                                            float t_min, float t_max, bool anchor_valid_in, i3 anchor_chunk_in,
                                            uint32_t anchor_key_in, uint32_t cand_count, ProbeHook& ph) {
   VoxTraceResult none{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
+  ph.best_cand = INVALID;
   if (s.cam->chunk_count == 0u) return none;
   const float vsz = vs_(s);
   const float cs = (float)s.cam->chunk_size * vsz;
@@ -273,12 +277,14 @@ __device__ VoxTraceResult trace_candidates(const Scene& s, const uint32_t* cslot
     const bool ua = anchor_valid_in && chunk_coords_neighbor(cc, anchor_chunk_in);
     const uint32_t aku = ua ? anchor_key_in : INVALID;
     ph.slot = slot;
+    ph.cand = i;
     const ChunkTraceResult h = trace_chunk_interval_stream_macro(s, ro, rd, inv, ch, ce, cx, ua, aku, opt, ph);
     if (h.hit.hit != 0u && h.hit.t < best.t) {
       best = h.hit;
       bav = h.anchor_valid;
       bak = h.anchor_key;
       bac = cc;
+      ph.best_cand = i;
     }
   }
   return VoxTraceResult{true, best, t_exit, bav, bak, bac};
@@ -419,10 +425,12 @@ __device__ __noinline__ VoxTraceResult primary_trace(const Scene& s, const Frame
   const float t_start = fmax_(t_hist - PRIMARY_HIT_MARGIN, 0.0f);
   const float t_end = fmin_(t_hist + PRIMARY_HIT_WINDOW, FOG_MAX_DIST);
   if (hist_valid) {
+    ph.phase = 0u;
     const VoxTraceResult h = trace_candidates(s, cslot, cmeta, c.ro, c.rd, t_start, t_end, hak != INVALID, hac, hak,
                                               tile_count, ph);
     if (h.best.hit != 0u) return h;
   }
+  ph.phase = 1u;
   return trace_candidates(s, cslot, cmeta, c.ro, c.rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID, tile_count,
                           ph);
 }
@@ -643,9 +651,24 @@ __device__ __forceinline__ void enqueue(uint32_t* q, uint32_t* counter, bool min
 
 __device__ __forceinline__ uint32_t warp_uniform_end(uint32_t n) { return (n + 31u) & ~31u; }
 
+// Walk summary of a pixel that met probes (px_probe.x): probes met (24 bits),
+// candidate index of the voxel answer, its trace phase, voxel-hit bit.
+__device__ __forceinline__ uint32_t probe_summary(uint32_t met, uint32_t best_cand, uint32_t phase, bool vox) {
+  return min(met, 0xFFFFFFu) | ((best_cand & 31u) << 24) | ((phase & 1u) << 29) | (vox ? 0x80000000u : 0u);
+}
+
+// Order of probe hits: trace phase (hint window first), t, candidate index,
+// probe order, column order.  t >= 0, so its bits order like its value.
+__device__ __forceinline__ unsigned long long slab_key(uint32_t phase, float t, uint32_t cand, uint32_t seq,
+                                                      uint32_t it) {
+  return ((unsigned long long)(phase & 1u) << 62) | ((unsigned long long)__float_as_uint(t) << 31) |
+         ((unsigned long long)(cand & 31u) << 26) | ((unsigned long long)(seq & 0xFFFFFu) << 6) |
+         (unsigned long long)(it & 63u);
+}
+
 // Voxel walk with the grass column probes stored, not evaluated.  Pixels that
-// met no probe are final here; the rest wait for k_probe_dda, k_slab_eval and
-// k_primary_resolve.
+// met no probe are final here; the rest wait for k_probe_dda, k_slab_eval,
+// k_slab_pick and k_primary_resolve.
 __global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace(const __grid_constant__ FrameArgs A) {
   __shared__ uint32_t cslot[2][TILE_CANDS];
   __shared__ Meta cmeta[2][TILE_CANDS];
@@ -669,7 +692,12 @@ __global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace(const __grid_
     vox = vt.in_grid && vt.best.hit != 0u;
     if (vox) store_pixhit(A.pix_hit + (size_t)pix * 5u, vt.best, vt);
     pend = ph.seq != 0u;
-    if (pend) A.px_probe[pix] = make_uint2(ph.seq | (vox ? 0x80000000u : 0u), ph.recorded);
+    if (pend) {
+      // more probes than the summary counts: every stored one is still used,
+      // the pixel just walks again
+      const uint32_t stored = ph.seq > 0xFFFFFFu ? 0u : ph.recorded;
+      A.px_probe[pix] = make_uint2(probe_summary(ph.seq, ph.best_cand, ph.phase, vox), stored);
+    }
   }
   enqueue(A.q_vox, &A.q_count[0], active && vox && !pend, pix);
   enqueue(A.q_far, &A.q_count[1], active && !vox && !pend, pix);
@@ -678,8 +706,7 @@ __global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace(const __grid_
 
 // One lane per stored probe: the probe's column DDA with the walk's
 // arguments, storing one task per grass slab it would march.  A probe whose
-// tasks do not all fit marks itself (and every later probe of its pixel) as
-// not evaluated, by lowering the pixel's evaluated count to its order.
+// tasks do not all fit sends its pixel to the inline walk (stored count 0).
 __global__ void __launch_bounds__(SHADE_THREADS) k_probe_dda(const __grid_constant__ FrameArgs A) {
   const Scene s = make_scene(A, false);
   const uint32_t n = min(A.q_count[4], A.probe_cap);
@@ -690,7 +717,7 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_probe_dda(const __grid_consta
     const Meta ch = meta_at(s, r.slot);
     const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vs;
     const i3 ov{ch.ox, ch.oy, ch.oz};
-    bool lost = false;
+    bool lost = r.seq > 0xFFFFFu;
     grass_columns_dda(s, c.ro, c.rd, safe_inv3(c.rd), r.t0, r.t1, rb, ov, vs, ch.colinfo_base,
                       [&](uint32_t it, float t, float tNext, v3 id) {
                         const uint32_t j = atomicAdd(&A.q_count[6], 1u);
@@ -703,12 +730,12 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_probe_dda(const __grid_consta
                         }
                         return false;
                       });
-    if (lost) atomicMin(&A.px_probe[r.pixel].y, r.seq);
+    if (lost) atomicMin(&A.px_probe[r.pixel].y, 0u);
   }
 }
 
-// One lane per grass slab: try_grass_slab_hit (the blade march); hits keep,
-// per pixel, the first (probe order, column order) one.
+// One lane per grass slab: try_grass_slab_hit (the blade march).  A hit
+// lowers its pixel's nearest-hit key and marks its chunk.
 __global__ void __launch_bounds__(SHADE_THREADS) k_slab_eval(const __grid_constant__ FrameArgs A) {
   const Scene s = make_scene(A, false);
   const uint32_t n = min(A.q_count[6], A.slab_cap);
@@ -722,45 +749,82 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_slab_eval(const __grid_consta
     const GrassHit gh = try_grass_slab_hit(s, c.ro, c.rd, __uint_as_float(a.z), __uint_as_float(a.w), id * vs, id, vs,
                                            time_s, strength);
     if (gh.hit) {
+      if (__float_as_uint(gh.t) & 0x80000000u) {  // not ordered by the key: walk again
+        atomicMin(&A.px_probe[r.pixel].y, 0u);
+        continue;
+      }
+      const uint32_t cand = r.cand_phase & 0xFFu, phase = r.cand_phase >> 8;
       A.slab_res[j] = make_float4(gh.t, gh.n.x, gh.n.y, gh.n.z);
-      atomicMin(&A.px_first[r.pixel],
-                ((unsigned long long)r.seq << 38) | ((unsigned long long)a.y << 32) | (unsigned long long)j);
+      atomicMin(&A.px_first[r.pixel], slab_key(phase, gh.t, cand, r.seq, a.y));
+      atomicOr(phase ? &A.px_mask[r.pixel].y : &A.px_mask[r.pixel].x, 1u << (cand & 31u));
+      A.slab_hits[atomicAdd(&A.q_count[7], 1u)] = j;
     }
   }
 }
 
-// Pixels that met probes: if every probe was stored and none hit, the voxel
-// walk's result stands; otherwise the walk runs again with the known probe
-// results (PROBE_REPLAY).
+// Finds, per pixel, the slab task whose key is the pixel's nearest.
+__global__ void __launch_bounds__(SHADE_THREADS) k_slab_pick(const __grid_constant__ FrameArgs A) {
+  const uint32_t n = min(A.q_count[7], A.slab_cap);
+  for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < n; i += gridDim.x * SHADE_THREADS) {
+    const uint32_t j = A.slab_hits[i];
+    const uint4 a = A.slab_tasks[2u * j];
+    const ProbeRec r = A.probe_recs[a.x];
+    const unsigned long long key =
+        slab_key(r.cand_phase >> 8, A.slab_res[j].x, r.cand_phase & 0xFFu, r.seq, a.y);
+    if (key == A.px_first[r.pixel]) A.px_task[r.pixel] = j;
+  }
+}
+
+// Pixels that met probes: the nearer of the nearest probe hit and the voxel
+// answer (see the comment above ProbeRec), or, when that cannot be decided
+// from the parts, the reference walk with inline probes.
 __global__ void __launch_bounds__(SHADE_THREADS) k_primary_resolve(const __grid_constant__ FrameArgs A) {
   const Scene s = make_scene(A, false);
   const uint32_t n = A.q_count[5], end = warp_uniform_end(n);
   const uint32_t tiles_x = (A.iw + 7u) / 8u;
+  const float vs = vs_(s);
   for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < end; i += gridDim.x * SHADE_THREADS) {
     bool active = i < n, vox = false;
     uint32_t pix = 0u;
     if (active) {
       pix = A.q_pending[i];
       const uint2 pp = A.px_probe[pix];
+      const uint32_t met = pp.x & 0xFFFFFFu, vcand = (pp.x >> 24) & 31u, vphase = (pp.x >> 29) & 1u;
+      vox = (pp.x >> 31) != 0u;
       const unsigned long long first = A.px_first[pix];
-      const uint32_t met = pp.x & 0x7FFFFFFFu;
-      // a hit counts only if every probe up to it was evaluated
-      const bool hit_known = first != ~0ull && (uint32_t)(first >> 38) < pp.y;
-      if (first == ~0ull && pp.y == met) {
-        vox = (pp.x >> 31) != 0u;
-      } else {
+      bool walk = pp.y < met;  // some probes were not evaluated
+      if (!walk && first != ~0ull) {
+        const uint32_t j = A.px_task[pix];
+        const float4 res = A.slab_res[j];
+        const ProbeRec r = A.probe_recs[A.slab_tasks[2u * j].x];
+        const uint32_t pcand = r.cand_phase & 0xFFu, pphase = r.cand_phase >> 8;
+        bool probe_wins = true;
+        if (vox && pphase == vphase) {
+          const float vt = __uint_as_float(A.pix_hit[(size_t)pix * 5u].x);
+          probe_wins = res.x < vt || (res.x == vt && pcand <= vcand);
+        }
+        if (probe_wins) {
+          const Meta ch = meta_at(s, r.slot);
+          const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vs;
+          const float rs = (float)s.cam->chunk_size * vs;
+          const int32_t csz = (int32_t)s.cam->chunk_size;
+          const HitGeom g = make_hit(MAT_GRASS, res.x, V3(res.y, res.z, res.w), rb, rs, ch, r.node,
+                                     V3(r.leaf_bmin[0], r.leaf_bmin[1], r.leaf_bmin[2]), r.leaf_size);
+          const VoxTraceResult vr{true, g, 0.0f, r.anchor_valid != 0u, r.anchor_key,
+                                  i3{ch.ox / csz, ch.oy / csz, ch.oz / csz}};
+          store_pixhit(A.pix_hit + (size_t)pix * 5u, g, vr);
+          vox = true;
+        } else {
+          // the voxel answer's own chunk had a probe hit: undecided here
+          const uint2 pm = A.px_mask[pix];
+          walk = (((vphase ? pm.y : pm.x) >> vcand) & 1u) != 0u;
+        }
+      }
+      if (walk) {
         const uint32_t gx = pix % A.iw, gy = pix / A.iw;
         const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
         const size_t tile = (size_t)(gy >> 3) * tiles_x + (gx >> 3);
         ProbeHook ph = probe_hook_inline();
-        ph.mode = PROBE_REPLAY;
-        ph.pixel = pix;
-        ph.recorded = pp.y;
-        if (hit_known) {
-          ph.hit_seq = (uint32_t)(first >> 38);
-          const float4 r = A.slab_res[(uint32_t)(first & 0xFFFFFFFFull)];
-          ph.hit = GrassHit{true, r.x, V3(r.y, r.z, r.w)};
-        }
         const VoxTraceResult vt = primary_trace(s, A, c, A.tile_slots + tile * TILE_CANDS, nullptr,
                                                 A.tile_count[tile], ph);
         vox = vt.in_grid && vt.best.hit != 0u;

@@ -42,7 +42,8 @@ enum Img {
   IMG_COLOR, IMG_DEPTH, IMG_LOCAL, IMG_HIST0, IMG_HIST1, IMG_SHADOW0, IMG_SHADOW1, IMG_LHIST0, IMG_LHIST1,
   IMG_GOD0, IMG_GOD1, IMG_PRE_TAA, IMG_OUTPUT, IMG_OHIST0, IMG_OHIST1, IMG_HITS, IMG_TILE_COUNT, IMG_TILE_SLOTS,
   IMG_PIXHIT, IMG_QVOX, IMG_QFAR, IMG_QCOUNT, IMG_QSHADOW, IMG_QLIGHT, IMG_PXSHADOW, IMG_PXLIGHT,
-  IMG_PROBE_RECS, IMG_SLAB_TASKS, IMG_SLAB_RES, IMG_PXFIRST, IMG_PXPROBE, IMG_QPENDING,
+  IMG_PROBE_RECS, IMG_SLAB_TASKS, IMG_SLAB_RES, IMG_SLAB_HITS, IMG_PXFIRST, IMG_PXPROBE, IMG_PXMASK, IMG_PXTASK,
+  IMG_QPENDING,
   IMG_N
 };
 
@@ -185,7 +186,11 @@ size_t img_bytes(const vxe_ctx* c, int i) {
       return in * kSlabsPerPixel * 32;
     case IMG_SLAB_RES:
       return in * kSlabsPerPixel * 16;
-    case IMG_PXFIRST: case IMG_PXPROBE:
+    case IMG_SLAB_HITS:
+      return in * kSlabsPerPixel * 4;
+    case IMG_PXTASK:
+      return in * 4;
+    case IMG_PXFIRST: case IMG_PXPROBE: case IMG_PXMASK:
       return in * 8;
     case IMG_PXLIGHT:
       return in * 16;
@@ -407,6 +412,9 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
   A.slab_cap = (uint32_t)std::min<size_t>(c->img[IMG_SLAB_TASKS].bytes / 32u, 0xFFFFFFFFu);
   A.px_first = (unsigned long long*)c->img[IMG_PXFIRST].p;
   A.px_probe = (uint2*)c->img[IMG_PXPROBE].p;
+  A.slab_hits = (uint32_t*)c->img[IMG_SLAB_HITS].p;
+  A.px_task = (uint32_t*)c->img[IMG_PXTASK].p;
+  A.px_mask = (uint2*)c->img[IMG_PXMASK].p;
   A.q_pending = (uint32_t*)c->img[IMG_QPENDING].p;
   const uint32_t tiles_x = (c->iw + 7) / 8, tiles_y = (c->ih + 7) / 8;
   const uint32_t tiles = tiles_x * tiles_y;
@@ -432,9 +440,11 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
     };
     CK(cudaMemsetAsync(A.q_count, 0, 32, c->compute));
     CK(cudaMemsetAsync(A.px_first, 0xFF, (size_t)npix * 8u, c->compute));
+    CK(cudaMemsetAsync(A.px_mask, 0, (size_t)npix * 8u, c->compute));
     k_primary_trace<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, c->compute>>>(A);
     k_probe_dda<<<grid((uint64_t)npix * kProbesPerPixel), SHADE_THREADS, 0, c->compute>>>(A);
     k_slab_eval<<<grid((uint64_t)npix * kSlabsPerPixel), SHADE_THREADS, 0, c->compute>>>(A);
+    k_slab_pick<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
     k_primary_resolve<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
     if (timed) CK(cudaEventRecord(c->ev[3], c->compute));
     k_shade_prep<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
