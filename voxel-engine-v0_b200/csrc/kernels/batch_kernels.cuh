@@ -32,11 +32,11 @@ struct BatchReq {  // 64 B
   const float* d;       // query directions
   uint4* out;           // 2 x uint4 per record
   float tmax;
-  uint32_t _pad;
+  uint32_t ray_base;    // first ray in the batch's viewport ray numbering (queries: the next viewport's)
 };
 
 struct BatchHeader {
-  uint32_t n_reqs, total_tiles, n_items, tile_w, tile_h, rpt, tile_reqs, _pad;
+  uint32_t n_reqs, total_tiles, n_items, tile_w, tile_h, rpt, tile_reqs, vp_rays;
 };
 
 struct BatchArgs {
@@ -69,6 +69,23 @@ struct BatchArgs {
   uint64_t grass_rec_n;
   const float* grass_taper;
   uint32_t grass_time_bits, grass_strength_bits;
+  // deferred grass probes of viewport rays (persistent and graph modes), the
+  // frame's scheme over the batch's viewport ray numbering (BatchReq::ray_base)
+  uint32_t defer;
+  ProbeRec* probe_recs;
+  uint32_t probe_cap;
+  uint4* slab_tasks;
+  float4* slab_res;
+  uint32_t* slab_hits;
+  uint32_t slab_cap;
+  uint32_t ray_cap;               // per-ray arrays' capacity
+  unsigned long long* px_first;
+  uint32_t* px_task;
+  uint2* px_mask;
+  uint2* px_probe;
+  float* px_vt;                   // voxel answer's t of rays that met probes
+  uint32_t* q_pending;
+  uint32_t* dcount;               // [0] probes, [1] pending rays, [2] slab tasks, [3] slab hits
 };
 
 constexpr int BATCH_THREADS = 128;
@@ -116,21 +133,28 @@ __device__ __forceinline__ uint32_t find_req(const BatchReq* reqs, uint32_t n, u
 
 // Cold-frame primary hit record of one viewport pixel: voxel trace without a
 // history hint, then main_primary's grass refinement or heightfield fallback.
-__device__ __noinline__ HitRec viewport_pixel_hit(const Scene& s, const uint32_t* tile_count,
-                                                  const uint32_t* tile_slots, uint32_t tiles_x, uint32_t gx,
-                                                  uint32_t gy) {
-  const float vs = vs_(s);
+__device__ __noinline__ VoxTraceResult viewport_trace(const Scene& s, const uint32_t* tile_count,
+                                                      const uint32_t* tile_slots, uint32_t tiles_x, uint32_t gx,
+                                                      uint32_t gy, ProbeHook& ph) {
   const v3 ro = cam_pos(s);
   const v3 rd = ray_dir_from_pixel(s, V2((float)gx + 0.5f, (float)gy + 0.5f));
   const size_t tile = (size_t)(gy >> 3) * tiles_x + (gx >> 3);
   const uint32_t cnt = tile_count[tile];
   VoxTraceResult vt{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
-  ProbeHook ph = probe_hook_inline();
+  ph.best_cand = INVALID;
   if (s.cam->chunk_count != 0u && cnt != 0u)
     vt = trace_candidates(s, tile_slots + tile * TILE_CANDS, nullptr, ro, rd, 0.0f, FOG_MAX_DIST, false,
                           i3{0, 0, 0}, INVALID, cnt, ph);
-  if (vt.in_grid && vt.best.hit != 0u) {
-    HitGeom best = vt.best;
+  return vt;
+}
+
+// The record of a voxel hit `best` (grass refinement first) or, without
+// one, of the heightfield (main_primary's fallback).
+__device__ __noinline__ HitRec viewport_finish(const Scene& s, uint32_t gx, uint32_t gy, bool voxel, HitGeom best) {
+  const float vs = vs_(s);
+  const v3 ro = cam_pos(s);
+  const v3 rd = ray_dir_from_pixel(s, V2((float)gx + 0.5f, (float)gy + 0.5f));
+  if (voxel) {
     if (best.mat == MAT_GRASS) {
       const i3 ov{to_i32(floorf(best.root_bmin.x / vs + 0.5f)), to_i32(floorf(best.root_bmin.y / vs + 0.5f)),
                   to_i32(floorf(best.root_bmin.z / vs + 0.5f))};
@@ -161,6 +185,15 @@ __device__ __noinline__ HitRec viewport_pixel_hit(const Scene& s, const uint32_t
   return make_rec(g, ro, rd, vs, false);
 }
 
+// Cold-frame primary hit record of one viewport pixel: voxel trace without a
+// history hint, then main_primary's grass refinement or heightfield fallback.
+__device__ __forceinline__ HitRec viewport_pixel_hit(const Scene& s, const uint32_t* tile_count,
+                                                     const uint32_t* tile_slots, uint32_t tiles_x, uint32_t gx,
+                                                     uint32_t gy, ProbeHook& ph) {
+  const VoxTraceResult vt = viewport_trace(s, tile_count, tile_slots, tiles_x, gx, gy, ph);
+  return viewport_finish(s, gx, gy, vt.in_grid && vt.best.hit != 0u, vt.best);
+}
+
 // Persistent candidate-tile builder over every viewport tile of the batch.
 __global__ void __launch_bounds__(TILE_THREADS) k_batch_tiles(const __grid_constant__ BatchArgs B) {
   __shared__ uint32_t sl[MAX_TILE_CHUNKS][TILE_THREADS];
@@ -183,6 +216,16 @@ __global__ void __launch_bounds__(TILE_THREADS) k_batch_tiles(const __grid_const
 
 __device__ __forceinline__ void store_rec_at(uint4* out, size_t i, const HitRec& h) { store_rec(out + i * 2u, h); }
 
+// Appends `value` to queue q; the lanes that arrive together share one atomic.
+__device__ __forceinline__ void enqueue_active(uint32_t* q, uint32_t* counter, uint32_t value) {
+  const uint32_t mask = __activemask();
+  const uint32_t lane = threadIdx.x & 31u, leader = __ffs(mask) - 1u;
+  uint32_t base = 0u;
+  if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  q[base + (uint32_t)__popc(mask & ((1u << lane) - 1u))] = value;
+}
+
 // Processes one work item with the calling warp.
 __device__ __forceinline__ void batch_item(const BatchArgs& B, const BatchHeader& H, const BatchReq& q,
                                            const Scene& s, uint32_t local, uint32_t lane) {
@@ -192,9 +235,27 @@ __device__ __forceinline__ void batch_item(const BatchArgs& B, const BatchHeader
     for (uint32_t k = lane; k < rw * rh; k += 32u) {
       const uint32_t gx = x0 + k % rw, gy = y0 + k / rw;
       if (gx >= q.w || gy >= q.h) continue;
-      const HitRec h = viewport_pixel_hit(s, B.tile_count + q.tile_base, B.tile_slots + (size_t)q.tile_base * TILE_CANDS,
-                                          q.tiles_x, gx, gy);
-      store_rec_at(q.out, (size_t)gy * q.w + gx, h);
+      ProbeHook ph = probe_hook_inline();
+      const uint32_t ray = q.ray_base + gy * q.w + gx;
+      if (B.defer) {
+        ph.mode = PROBE_RECORD;
+        ph.pixel = ray;
+        ph.recs = B.probe_recs;
+        ph.rec_count = &B.dcount[0];
+        ph.rec_cap = B.probe_cap;
+      }
+      const VoxTraceResult vt = viewport_trace(s, B.tile_count + q.tile_base,
+                                               B.tile_slots + (size_t)q.tile_base * TILE_CANDS, q.tiles_x, gx, gy, ph);
+      const bool vox = vt.in_grid && vt.best.hit != 0u;
+      // With deferred probes this is the record of the walk without probe
+      // hits; k_batch_resolve rewrites it for rays a probe hit decides.
+      store_rec_at(q.out, (size_t)gy * q.w + gx, viewport_finish(s, gx, gy, vox, vt.best));
+      if (B.defer && ph.seq != 0u) {  // an inline walk counts its probes too
+        const uint32_t stored = ph.seq > 0xFFFFFFu ? 0u : ph.recorded;
+        B.px_probe[ray] = make_uint2(probe_summary(ph.seq, ph.best_cand, ph.phase, vox), stored);
+        B.px_vt[ray] = vt.best.t;
+        enqueue_active(B.q_pending, &B.dcount[1], ray);
+      }
     }
   } else {
     const uint32_t per = 128u * H.rpt;
@@ -248,6 +309,149 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_trace(const __grid_cons
     load_cam(q.cam);
     const Scene s = batch_scene(B, &wcam[warp]);
     batch_item(B, H, q, s, item - q.item_begin, lane);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Deferred grass probes of viewport rays: the frame's k_probe_dda /
+// k_slab_eval / k_slab_pick / k_primary_resolve over the batch's viewport
+// rays (one trace phase: cold rays have no hint window).
+// ---------------------------------------------------------------------------
+struct BatchRay {
+  const BatchReq* q;
+  uint32_t gx, gy;
+};
+
+__device__ __forceinline__ BatchRay batch_ray(const BatchArgs& B, uint32_t n_reqs, uint32_t ray) {
+  // ray_base never decreases over the requests and a query repeats the next
+  // viewport's base, so the last request whose base is <= ray is a viewport.
+  const uint32_t r = find_req(B.reqs, n_reqs, ray, [](const BatchReq& q) { return q.ray_base; });
+  const BatchReq* q = &B.reqs[r];
+  const uint32_t local = ray - q->ray_base;
+  return BatchRay{q, local % q->w, local / q->w};
+}
+
+__global__ void __launch_bounds__(BATCH_THREADS) k_batch_defer_clear(const __grid_constant__ BatchArgs B) {
+  const uint32_t n = min(B.hdr->vp_rays, B.ray_cap);
+  for (uint32_t i = blockIdx.x * BATCH_THREADS + threadIdx.x; i < n; i += gridDim.x * BATCH_THREADS) {
+    B.px_first[i] = ~0ull;
+    B.px_mask[i] = make_uint2(0u, 0u);
+  }
+}
+
+__global__ void __launch_bounds__(BATCH_THREADS) k_batch_probe_dda(const __grid_constant__ BatchArgs B) {
+  const uint32_t n_reqs = B.hdr->n_reqs;
+  const uint32_t n = min(B.dcount[0], B.probe_cap);
+  for (uint32_t i = blockIdx.x * BATCH_THREADS + threadIdx.x; i < n; i += gridDim.x * BATCH_THREADS) {
+    const ProbeRec r = B.probe_recs[i];
+    const BatchRay br = batch_ray(B, n_reqs, r.pixel);
+    const Scene s = batch_scene(B, &B.cams[br.q->cam]);
+    const float vs = vs_(s);
+    const v3 ro = cam_pos(s);
+    const v3 rd = ray_dir_from_pixel(s, V2((float)br.gx + 0.5f, (float)br.gy + 0.5f));
+    const Meta ch = meta_at(s, r.slot);
+    const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vs;
+    const i3 ov{ch.ox, ch.oy, ch.oz};
+    bool lost = r.seq > 0xFFFFFu;
+    grass_columns_dda(s, ro, rd, safe_inv3(rd), r.t0, r.t1, rb, ov, vs, ch.colinfo_base,
+                      [&](uint32_t it, float t, float tNext, v3 id) {
+                        const uint32_t j = atomicAdd(&B.dcount[2], 1u);
+                        if (j < B.slab_cap) {
+                          B.slab_tasks[2u * j] = make_uint4(i, it, __float_as_uint(t), __float_as_uint(tNext));
+                          B.slab_tasks[2u * j + 1u] = make_uint4(__float_as_uint(id.x), __float_as_uint(id.y),
+                                                                 __float_as_uint(id.z), 0u);
+                        } else {
+                          lost = true;
+                        }
+                        return false;
+                      });
+    if (lost) atomicMin(&B.px_probe[r.pixel].y, 0u);
+  }
+}
+
+__global__ void __launch_bounds__(BATCH_THREADS) k_batch_slab_eval(const __grid_constant__ BatchArgs B) {
+  const uint32_t n_reqs = B.hdr->n_reqs;
+  const uint32_t n = min(B.dcount[2], B.slab_cap);
+  for (uint32_t j = blockIdx.x * BATCH_THREADS + threadIdx.x; j < n; j += gridDim.x * BATCH_THREADS) {
+    const uint4 a = B.slab_tasks[2u * j], b = B.slab_tasks[2u * j + 1u];
+    const ProbeRec r = B.probe_recs[a.x];
+    const BatchRay br = batch_ray(B, n_reqs, r.pixel);
+    const Scene s = batch_scene(B, &B.cams[br.q->cam]);
+    const float vs = vs_(s);
+    const v3 ro = cam_pos(s);
+    const v3 rd = ray_dir_from_pixel(s, V2((float)br.gx + 0.5f, (float)br.gy + 0.5f));
+    const v3 id = V3(__uint_as_float(b.x), __uint_as_float(b.y), __uint_as_float(b.z));
+    const GrassHit gh = try_grass_slab_hit(s, ro, rd, __uint_as_float(a.z), __uint_as_float(a.w), id * vs, id, vs,
+                                           s.cam->voxel_params[1], s.cam->voxel_params[2]);
+    if (gh.hit) {
+      if (__float_as_uint(gh.t) & 0x80000000u) {
+        atomicMin(&B.px_probe[r.pixel].y, 0u);
+        continue;
+      }
+      const uint32_t cand = r.cand_phase & 0xFFu, phase = r.cand_phase >> 8;
+      B.slab_res[j] = make_float4(gh.t, gh.n.x, gh.n.y, gh.n.z);
+      atomicMin(&B.px_first[r.pixel], slab_key(phase, gh.t, cand, r.seq, a.y));
+      atomicOr(phase ? &B.px_mask[r.pixel].y : &B.px_mask[r.pixel].x, 1u << (cand & 31u));
+      B.slab_hits[atomicAdd(&B.dcount[3], 1u)] = j;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(BATCH_THREADS) k_batch_slab_pick(const __grid_constant__ BatchArgs B) {
+  const uint32_t n = min(B.dcount[3], B.slab_cap);
+  for (uint32_t i = blockIdx.x * BATCH_THREADS + threadIdx.x; i < n; i += gridDim.x * BATCH_THREADS) {
+    const uint32_t j = B.slab_hits[i];
+    const uint4 a = B.slab_tasks[2u * j];
+    const ProbeRec r = B.probe_recs[a.x];
+    const unsigned long long key = slab_key(r.cand_phase >> 8, B.slab_res[j].x, r.cand_phase & 0xFFu, r.seq, a.y);
+    if (key == B.px_first[r.pixel]) B.px_task[r.pixel] = j;
+  }
+}
+
+// Rays that met probes: the nearer of the nearest probe hit and the voxel
+// answer, or the reference walk with inline probes when the parts cannot
+// decide; the record written by the trace is rewritten only when it changes.
+__global__ void __launch_bounds__(BATCH_THREADS) k_batch_resolve(const __grid_constant__ BatchArgs B) {
+  const uint32_t n_reqs = B.hdr->n_reqs;
+  const uint32_t n = B.dcount[1];
+  for (uint32_t i = blockIdx.x * BATCH_THREADS + threadIdx.x; i < n; i += gridDim.x * BATCH_THREADS) {
+    const uint32_t ray = B.q_pending[i];
+    const uint2 pp = B.px_probe[ray];
+    const unsigned long long first = B.px_first[ray];
+    const uint32_t met = pp.x & 0xFFFFFFu, vcand = (pp.x >> 24) & 31u, vphase = (pp.x >> 29) & 1u;
+    const bool vox = (pp.x >> 31) != 0u;
+    bool walk = pp.y < met;
+    if (!walk && first == ~0ull) continue;  // no probe hit: the stored record stands
+    const BatchRay br = batch_ray(B, n_reqs, ray);
+    const BatchReq& q = *br.q;
+    const Scene s = batch_scene(B, &B.cams[q.cam]);
+    if (!walk) {
+      const uint32_t j = B.px_task[ray];
+      const float4 res = B.slab_res[j];
+      const ProbeRec r = B.probe_recs[B.slab_tasks[2u * j].x];
+      const uint32_t pcand = r.cand_phase & 0xFFu, pphase = r.cand_phase >> 8;
+      bool probe_wins = true;
+      if (vox && pphase == vphase) {
+        const float vt = B.px_vt[ray];
+        probe_wins = res.x < vt || (res.x == vt && pcand <= vcand);
+      }
+      if (probe_wins) {
+        const float vs = vs_(s);
+        const Meta ch = meta_at(s, r.slot);
+        const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vs;
+        const HitGeom g = make_hit(MAT_GRASS, res.x, V3(res.y, res.z, res.w), rb, (float)s.cam->chunk_size * vs, ch,
+                                   r.node, V3(r.leaf_bmin[0], r.leaf_bmin[1], r.leaf_bmin[2]), r.leaf_size);
+        store_rec_at(q.out, (size_t)br.gy * q.w + br.gx, viewport_finish(s, br.gx, br.gy, true, g));
+        continue;
+      }
+      const uint2 pm = B.px_mask[ray];
+      walk = (((vphase ? pm.y : pm.x) >> vcand) & 1u) != 0u;
+      if (!walk) continue;
+    }
+    ProbeHook ph = probe_hook_inline();
+    const HitRec h = viewport_pixel_hit(s, B.tile_count + q.tile_base, B.tile_slots + (size_t)q.tile_base * TILE_CANDS,
+                                        q.tiles_x, br.gx, br.gy, ph);
+    store_rec_at(q.out, (size_t)br.gy * q.w + br.gx, h);
   }
 }
 

@@ -70,6 +70,10 @@ struct GrassTable {
 struct BatchLane {
   cudaStream_t stream = nullptr;
   DevBuf hdr, reqs, cams, tile_count, tile_slots, head;
+  // deferred grass probes of viewport rays: per-ray arrays for ray_cap rays,
+  // probe records and slab tasks in proportion, counters
+  DevBuf probe_recs, slab_tasks, slab_res, slab_hits, px_first, px_task, px_mask, px_probe, px_vt, q_pending, dcount;
+  uint32_t ray_cap = 0;
   void* stage = nullptr;  // pinned: header | requests | cameras
   cudaGraphExec_t graph = nullptr;
   uint32_t graph_key[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -549,7 +553,10 @@ void vxe_destroy(vxe_ctx* c) {
     release(*b);
   for (auto& L : c->lanes) {
     if (L.stream) cudaStreamSynchronize(L.stream);
-    for (auto* b : {&L.hdr, &L.reqs, &L.cams, &L.tile_count, &L.tile_slots, &L.head}) release(*b);
+    for (auto* b : {&L.hdr, &L.reqs, &L.cams, &L.tile_count, &L.tile_slots, &L.head, &L.probe_recs, &L.slab_tasks,
+                    &L.slab_res, &L.slab_hits, &L.px_first, &L.px_task, &L.px_mask, &L.px_probe, &L.px_vt,
+                    &L.q_pending, &L.dcount})
+      release(*b);
     if (L.graph) cudaGraphExecDestroy(L.graph);
     if (L.stage) cudaFreeHost(L.stage);
     for (auto& e : L.ev)
@@ -865,7 +872,11 @@ constexpr size_t kStageHdr = 0, kStageReqs = 64,
                  kStageCams = kStageReqs + (size_t)VXE_MAX_BATCH_REQUESTS * sizeof(BatchReq),
                  kStageBytes = kStageCams + (size_t)(VXE_MAX_BATCH_REQUESTS + 1) * sizeof(vxe_camera_gpu);
 
-vxe_status lane_resources(vxe_ctx* c, BatchLane& L, uint32_t tiles) {
+// Stored probes and slab tasks per viewport ray of a batch; rays past the
+// budget walk again with inline probes.
+constexpr uint32_t kBatchProbesPerRay = 4, kBatchSlabsPerRay = 2;
+
+vxe_status lane_resources(vxe_ctx* c, BatchLane& L, uint32_t tiles, uint32_t vp_rays) {
   vxe_status st;
   if (!L.stage) {
     if (cudaMallocHost(&L.stage, kStageBytes) != cudaSuccess) return fail(c, VXE_ERR_OOM, "pinned staging");
@@ -884,6 +895,26 @@ vxe_status lane_resources(vxe_ctx* c, BatchLane& L, uint32_t tiles) {
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lb, vxe::dev::k_batch_tiles, vxe::dev::TILE_THREADS, 0));
     c->b_trace_grid = sms * std::max(tb, 1);
     c->b_tile_grid = sms * std::max(lb, 1);
+  }
+  if (vp_rays > L.ray_cap) {
+    const uint64_t cap = std::min<uint64_t>(std::max<uint64_t>((uint64_t)vp_rays + vp_rays / 2, 1u << 16),
+                                            0x3FFFFFFFu / kBatchProbesPerRay);
+    if ((st = alloc(c, L.px_first, cap * 8)) != VXE_OK) return st;
+    if ((st = alloc(c, L.px_mask, cap * 8)) != VXE_OK) return st;
+    if ((st = alloc(c, L.px_probe, cap * 8)) != VXE_OK) return st;
+    if ((st = alloc(c, L.px_task, cap * 4)) != VXE_OK) return st;
+    if ((st = alloc(c, L.px_vt, cap * 4)) != VXE_OK) return st;
+    if ((st = alloc(c, L.q_pending, cap * 4)) != VXE_OK) return st;
+    if ((st = alloc(c, L.probe_recs, cap * kBatchProbesPerRay * sizeof(vxe::dev::ProbeRec))) != VXE_OK) return st;
+    if ((st = alloc(c, L.slab_tasks, cap * kBatchSlabsPerRay * 32)) != VXE_OK) return st;
+    if ((st = alloc(c, L.slab_res, cap * kBatchSlabsPerRay * 16)) != VXE_OK) return st;
+    if ((st = alloc(c, L.slab_hits, cap * kBatchSlabsPerRay * 4)) != VXE_OK) return st;
+    if (!L.dcount.p && (st = alloc(c, L.dcount, 16)) != VXE_OK) return st;
+    L.ray_cap = (uint32_t)cap;
+    if (L.graph) {  // the captured launches hold the old pointers
+      cudaGraphExecDestroy(L.graph);
+      L.graph = nullptr;
+    }
   }
   if ((size_t)tiles * 4 > L.tile_count.bytes) {
     // grow by 1.5x so a stream of slightly larger batches does not reallocate every time
@@ -924,6 +955,20 @@ BatchArgs batch_args(const vxe_ctx* c, const BatchLane& L) {
   B.tile_count = (uint32_t*)L.tile_count.p;
   B.tile_slots = (uint32_t*)L.tile_slots.p;
   B.head = (uint32_t*)L.head.p;
+  B.probe_recs = (vxe::dev::ProbeRec*)L.probe_recs.p;
+  B.probe_cap = L.ray_cap * kBatchProbesPerRay;
+  B.slab_tasks = (uint4*)L.slab_tasks.p;
+  B.slab_res = (float4*)L.slab_res.p;
+  B.slab_hits = (uint32_t*)L.slab_hits.p;
+  B.slab_cap = L.ray_cap * kBatchSlabsPerRay;
+  B.ray_cap = L.ray_cap;
+  B.px_first = (unsigned long long*)L.px_first.p;
+  B.px_task = (uint32_t*)L.px_task.p;
+  B.px_mask = (uint2*)L.px_mask.p;
+  B.px_probe = (uint2*)L.px_probe.p;
+  B.px_vt = (float*)L.px_vt.p;
+  B.q_pending = (uint32_t*)L.q_pending.p;
+  B.dcount = (uint32_t*)L.dcount.p;
   return B;
 }
 
@@ -935,8 +980,18 @@ vxe_status launch_persistent(vxe_ctx* c, BatchLane& L, const BatchArgs& B) {
   CK(cudaMemcpyAsync(L.cams.p, (char*)L.stage + kStageCams, kStageBytes - kStageCams, cudaMemcpyHostToDevice,
                      L.stream));
   CK(cudaMemsetAsync(L.head.p, 0, 16, L.stream));
+  if (B.defer) {
+    CK(cudaMemsetAsync(L.dcount.p, 0, 16, L.stream));
+    k_batch_defer_clear<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
+  }
   k_batch_tiles<<<c->b_tile_grid, TILE_THREADS, 0, L.stream>>>(B);
   k_batch_trace<<<c->b_trace_grid, BATCH_THREADS, 0, L.stream>>>(B);
+  if (B.defer) {
+    k_batch_probe_dda<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
+    k_batch_slab_eval<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
+    k_batch_slab_pick<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
+    k_batch_resolve<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
+  }
   CK(cudaGetLastError());
   return VXE_OK;
 }
@@ -960,7 +1015,7 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
   // Host-side descriptors (requests keep their order; tiles and items are
   // numbered in request order so the device finds a request by binary search).
   uint32_t tiles = 0, items = 0;
-  uint64_t rays = 0;
+  uint64_t rays = 0, vp_rays = 0;
   std::vector<BatchReq> R(n);
   for (uint32_t i = 0; i < n; ++i) {
     const vxe_request& q = reqs[i];
@@ -970,6 +1025,7 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
     r.out = (uint4*)q.d_out;
     r.tile_base = tiles;
     r.item_begin = items;
+    r.ray_base = (uint32_t)vp_rays;  // a query repeats the next viewport's base
     if (!q.d_out) return fail(c, VXE_ERR_INVALID_ARG, "request %u has no output", i);
     if (q.kind == VXE_REQ_VIEWPORT) {
       if (q.width == 0 || q.height == 0 || q.camera.render_present_px[0] != q.width ||
@@ -983,6 +1039,8 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
       tiles += r.tiles_x * ((q.height + 7) / 8);
       items += r.items_x * ((q.height + th - 1) / th);
       rays += (uint64_t)q.width * q.height;
+      vp_rays += (uint64_t)q.width * q.height;
+      if (vp_rays > 0x3FFFFFFFull) return fail(c, VXE_ERR_CAPACITY, "batch of more than 2^30 viewport rays");
     } else if (q.kind == VXE_REQ_QUERY) {
       if (q.ray_count == 0 || !q.d_origins || !q.d_dirs) return fail(c, VXE_ERR_INVALID_ARG, "query %u empty", i);
       r.w = q.ray_count;
@@ -996,10 +1054,14 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
       return fail(c, VXE_ERR_INVALID_ARG, "request %u kind %u", i, q.kind);
     }
   }
-  vxe_status st = lane_resources(c, L, tiles);
+  // Deferred grass probes in the persistent and graph modes; the plain mode
+  // is the per-request single-launch baseline with the reference's inline
+  // probes.
+  const bool defer = opt->mode != VXE_BATCH_PLAIN && vp_rays != 0;
+  vxe_status st = lane_resources(c, L, tiles, defer ? (uint32_t)vp_rays : 0u);
   if (st != VXE_OK) return st;
   if (c->upload_recorded) CK(cudaStreamWaitEvent(L.stream, c->upload_done, 0));
-  BatchHeader H{n, tiles, items, tw, th, rpt, n, 0};
+  BatchHeader H{n, tiles, items, tw, th, rpt, n, (uint32_t)vp_rays};
   std::memcpy((char*)L.stage + kStageHdr, &H, sizeof H);
   if (n) std::memcpy((char*)L.stage + kStageReqs, R.data(), n * sizeof(BatchReq));
   auto* cams = (vxe_camera_gpu*)((char*)L.stage + kStageCams);
@@ -1017,6 +1079,7 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
     cams[i + 1] = v;
   }
   BatchArgs B = batch_args(c, L);
+  B.defer = defer ? 1u : 0u;
   CK(cudaEventRecord(L.ev[0], L.stream));
   // Grass cell table for the wind of the first viewport's camera (requests
   // with another wind time / strength derive their cells in the march).
@@ -1057,7 +1120,7 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
     // batches only rewrite the pinned staging the graph's copies read.
     const uint32_t key[9] = {(uint32_t)(uintptr_t)L.tile_count.p, (uint32_t)((uintptr_t)L.tile_count.p >> 32),
                              (uint32_t)c->cfg.clip_levels, c->clip.levels, c->clip.res, 1u,
-                             use_grass ? 1u : 0u, B.grass_time_bits, B.grass_strength_bits};
+                             (use_grass ? 1u : 0u) | (B.defer ? 2u : 0u), B.grass_time_bits, B.grass_strength_bits};
     const bool same = L.graph != nullptr && std::memcmp(key, L.graph_key, sizeof key) == 0 &&
                       std::memcmp(&L.graph_clip, &B.clip, sizeof B.clip) == 0;
     if (!same) {
