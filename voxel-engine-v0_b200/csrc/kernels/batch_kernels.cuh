@@ -83,9 +83,11 @@ struct BatchArgs {
   uint32_t* px_task;
   uint2* px_mask;
   uint2* px_probe;
-  float* px_vt;                   // voxel answer's t of rays that met probes
+  uint4* px_hit;                  // 4 x uint4 per ray: voxel answer of a ray that met probes or needs refining
   uint32_t* q_pending;
-  uint32_t* dcount;               // [0] probes, [1] pending rays, [2] slab tasks, [3] slab hits
+  uint32_t* q_refine;             // rays whose answer is a grass voxel (grass-slab refinement)
+  uint32_t* q_far;                // rays without a voxel answer (heightfield)
+  uint32_t* dcount;               // [0] probes, [1] pending rays, [2] slab tasks, [3] slab hits, [4] refine, [5] far
 };
 
 constexpr int BATCH_THREADS = 128;
@@ -131,8 +133,7 @@ __device__ __forceinline__ uint32_t find_req(const BatchReq* reqs, uint32_t n, u
   return lo;
 }
 
-// Cold-frame primary hit record of one viewport pixel: voxel trace without a
-// history hint, then main_primary's grass refinement or heightfield fallback.
+// Voxel trace of one cold viewport pixel (no history hint).
 __device__ __noinline__ VoxTraceResult viewport_trace(const Scene& s, const uint32_t* tile_count,
                                                       const uint32_t* tile_slots, uint32_t tiles_x, uint32_t gx,
                                                       uint32_t gy, ProbeHook& ph) {
@@ -148,25 +149,31 @@ __device__ __noinline__ VoxTraceResult viewport_trace(const Scene& s, const uint
   return vt;
 }
 
-// The record of a voxel hit `best` (grass refinement first) or, without
-// one, of the heightfield (main_primary's fallback).
-__device__ __noinline__ HitRec viewport_finish(const Scene& s, uint32_t gx, uint32_t gy, bool voxel, HitGeom best) {
+// Record of voxel hit `best` (grass voxels get main_primary's grass-slab
+// refinement first).
+__device__ __noinline__ HitRec viewport_voxel_rec(const Scene& s, uint32_t gx, uint32_t gy, HitGeom best) {
   const float vs = vs_(s);
   const v3 ro = cam_pos(s);
   const v3 rd = ray_dir_from_pixel(s, V2((float)gx + 0.5f, (float)gy + 0.5f));
-  if (voxel) {
-    if (best.mat == MAT_GRASS) {
-      const i3 ov{to_i32(floorf(best.root_bmin.x / vs + 0.5f)), to_i32(floorf(best.root_bmin.y / vs + 0.5f)),
-                  to_i32(floorf(best.root_bmin.z / vs + 0.5f))};
-      const v3 hp = ro + rd * best.t;
-      const GrassCell cell =
-          pick_grass_cell_in_chunk_with_bias(hp, rd, best.root_bmin, ov, vs, (int32_t)s.cam->chunk_size);
-      const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, best.t, cell.bmin_m, cell.id_vox, vs,
-                                             s.cam->voxel_params[1], s.cam->voxel_params[2]);
-      if (gh.hit) { best.t = gh.t; best.n = gh.n; }
-    }
-    return make_rec(best, ro, rd, vs, true);
+  if (best.mat == MAT_GRASS) {
+    const i3 ov{to_i32(floorf(best.root_bmin.x / vs + 0.5f)), to_i32(floorf(best.root_bmin.y / vs + 0.5f)),
+                to_i32(floorf(best.root_bmin.z / vs + 0.5f))};
+    const v3 hp = ro + rd * best.t;
+    const GrassCell cell =
+        pick_grass_cell_in_chunk_with_bias(hp, rd, best.root_bmin, ov, vs, (int32_t)s.cam->chunk_size);
+    const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, best.t, cell.bmin_m, cell.id_vox, vs,
+                                           s.cam->voxel_params[1], s.cam->voxel_params[2]);
+    if (gh.hit) { best.t = gh.t; best.n = gh.n; }
   }
+  return make_rec(best, ro, rd, vs, true);
+}
+
+// Record of a ray without a voxel hit: the heightfield (main_primary's
+// fallback, with its grass refinement) or a miss.
+__device__ __noinline__ HitRec viewport_far_rec(const Scene& s, uint32_t gx, uint32_t gy) {
+  const float vs = vs_(s);
+  const v3 ro = cam_pos(s);
+  const v3 rd = ray_dir_from_pixel(s, V2((float)gx + 0.5f, (float)gy + 0.5f));
   ClipHit hf = clip_trace_heightfield(s, ro, rd, 0.0f, FOG_MAX_DIST);
   if (!hf.hit) return miss_rec();
   if (hf.mat == MAT_GRASS) {
@@ -183,6 +190,11 @@ __device__ __noinline__ HitRec viewport_finish(const Scene& s, uint32_t gx, uint
   g.n = hf.n;
   g.mat = hf.mat;
   return make_rec(g, ro, rd, vs, false);
+}
+
+__device__ __forceinline__ HitRec viewport_finish(const Scene& s, uint32_t gx, uint32_t gy, bool voxel,
+                                                  const HitGeom& best) {
+  return voxel ? viewport_voxel_rec(s, gx, gy, best) : viewport_far_rec(s, gx, gy);
 }
 
 // Cold-frame primary hit record of one viewport pixel: voxel trace without a
@@ -226,6 +238,30 @@ __device__ __forceinline__ void enqueue_active(uint32_t* q, uint32_t* counter, u
   q[base + (uint32_t)__popc(mask & ((1u << lane) - 1u))] = value;
 }
 
+__device__ __forceinline__ void store_hitgeom(uint4* dst, const HitGeom& g) {
+  dst[0] = make_uint4(__float_as_uint(g.t), __float_as_uint(g.n.x), __float_as_uint(g.n.y), __float_as_uint(g.n.z));
+  dst[1] = make_uint4(__float_as_uint(g.root_bmin.x), __float_as_uint(g.root_bmin.y), __float_as_uint(g.root_bmin.z),
+                      g.mat);
+  dst[2] = make_uint4(g.node_base, g.macro_base, g.node, __float_as_uint(g.leaf_size));
+  dst[3] = make_uint4(__float_as_uint(g.leaf_bmin.x), __float_as_uint(g.leaf_bmin.y), __float_as_uint(g.leaf_bmin.z),
+                      0u);
+}
+
+// Finishes a decided viewport ray (deferred mode): a non-grass voxel hit is
+// written at once, a grass voxel hit waits for k_batch_refine, a ray without
+// a voxel hit for k_batch_far.
+__device__ __forceinline__ void batch_finish(const BatchArgs& B, const Scene& s, const BatchReq& q, uint32_t ray,
+                                             uint32_t gx, uint32_t gy, bool vox, const HitGeom& best) {
+  if (vox && best.mat != MAT_GRASS) {
+    store_rec_at(q.out, (size_t)gy * q.w + gx, viewport_voxel_rec(s, gx, gy, best));
+  } else if (vox) {
+    store_hitgeom(B.px_hit + (size_t)ray * 4u, best);
+    enqueue_active(B.q_refine, &B.dcount[4], ray);
+  } else {
+    enqueue_active(B.q_far, &B.dcount[5], ray);
+  }
+}
+
 // Processes one work item with the calling warp.
 __device__ __forceinline__ void batch_item(const BatchArgs& B, const BatchHeader& H, const BatchReq& q,
                                            const Scene& s, uint32_t local, uint32_t lane) {
@@ -247,14 +283,15 @@ __device__ __forceinline__ void batch_item(const BatchArgs& B, const BatchHeader
       const VoxTraceResult vt = viewport_trace(s, B.tile_count + q.tile_base,
                                                B.tile_slots + (size_t)q.tile_base * TILE_CANDS, q.tiles_x, gx, gy, ph);
       const bool vox = vt.in_grid && vt.best.hit != 0u;
-      // With deferred probes this is the record of the walk without probe
-      // hits; k_batch_resolve rewrites it for rays a probe hit decides.
-      store_rec_at(q.out, (size_t)gy * q.w + gx, viewport_finish(s, gx, gy, vox, vt.best));
-      if (B.defer && ph.seq != 0u) {  // an inline walk counts its probes too
+      if (!B.defer) {
+        store_rec_at(q.out, (size_t)gy * q.w + gx, viewport_finish(s, gx, gy, vox, vt.best));
+      } else if (ph.seq != 0u) {  // met probes: k_batch_resolve decides
+        if (vox) store_hitgeom(B.px_hit + (size_t)ray * 4u, vt.best);
         const uint32_t stored = ph.seq > 0xFFFFFFu ? 0u : ph.recorded;
         B.px_probe[ray] = make_uint2(probe_summary(ph.seq, ph.best_cand, ph.phase, vox), stored);
-        B.px_vt[ray] = vt.best.t;
         enqueue_active(B.q_pending, &B.dcount[1], ray);
+      } else {
+        batch_finish(B, s, q, ray, gx, gy, vox, vt.best);
       }
     }
   } else {
@@ -410,7 +447,7 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_slab_pick(const __grid_
 
 // Rays that met probes: the nearer of the nearest probe hit and the voxel
 // answer, or the reference walk with inline probes when the parts cannot
-// decide; the record written by the trace is rewritten only when it changes.
+// decide.
 __global__ void __launch_bounds__(BATCH_THREADS) k_batch_resolve(const __grid_constant__ BatchArgs B) {
   const uint32_t n_reqs = B.hdr->n_reqs;
   const uint32_t n = B.dcount[1];
@@ -420,19 +457,18 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_resolve(const __grid_co
     const unsigned long long first = B.px_first[ray];
     const uint32_t met = pp.x & 0xFFFFFFu, vcand = (pp.x >> 24) & 31u, vphase = (pp.x >> 29) & 1u;
     const bool vox = (pp.x >> 31) != 0u;
-    bool walk = pp.y < met;
-    if (!walk && first == ~0ull) continue;  // no probe hit: the stored record stands
     const BatchRay br = batch_ray(B, n_reqs, ray);
     const BatchReq& q = *br.q;
     const Scene s = batch_scene(B, &B.cams[q.cam]);
-    if (!walk) {
+    bool walk = pp.y < met;
+    if (!walk && first != ~0ull) {
       const uint32_t j = B.px_task[ray];
       const float4 res = B.slab_res[j];
       const ProbeRec r = B.probe_recs[B.slab_tasks[2u * j].x];
       const uint32_t pcand = r.cand_phase & 0xFFu, pphase = r.cand_phase >> 8;
       bool probe_wins = true;
       if (vox && pphase == vphase) {
-        const float vt = B.px_vt[ray];
+        const float vt = __uint_as_float(B.px_hit[(size_t)ray * 4u].x);
         probe_wins = res.x < vt || (res.x == vt && pcand <= vcand);
       }
       if (probe_wins) {
@@ -441,17 +477,45 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_resolve(const __grid_co
         const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vs;
         const HitGeom g = make_hit(MAT_GRASS, res.x, V3(res.y, res.z, res.w), rb, (float)s.cam->chunk_size * vs, ch,
                                    r.node, V3(r.leaf_bmin[0], r.leaf_bmin[1], r.leaf_bmin[2]), r.leaf_size);
-        store_rec_at(q.out, (size_t)br.gy * q.w + br.gx, viewport_finish(s, br.gx, br.gy, true, g));
+        batch_finish(B, s, q, ray, br.gx, br.gy, true, g);
         continue;
       }
       const uint2 pm = B.px_mask[ray];
       walk = (((vphase ? pm.y : pm.x) >> vcand) & 1u) != 0u;
-      if (!walk) continue;
     }
-    ProbeHook ph = probe_hook_inline();
-    const HitRec h = viewport_pixel_hit(s, B.tile_count + q.tile_base, B.tile_slots + (size_t)q.tile_base * TILE_CANDS,
-                                        q.tiles_x, br.gx, br.gy, ph);
-    store_rec_at(q.out, (size_t)br.gy * q.w + br.gx, h);
+    if (walk) {
+      ProbeHook ph = probe_hook_inline();
+      const HitRec h = viewport_pixel_hit(s, B.tile_count + q.tile_base,
+                                          B.tile_slots + (size_t)q.tile_base * TILE_CANDS, q.tiles_x, br.gx, br.gy, ph);
+      store_rec_at(q.out, (size_t)br.gy * q.w + br.gx, h);
+      continue;
+    }
+    // no probe hit, or the voxel answer is nearer: the walk's answer stands
+    const HitGeom best = vox ? load_pixhit(s, B.px_hit + (size_t)ray * 4u) : miss_hitgeom();
+    batch_finish(B, s, q, ray, br.gx, br.gy, vox, best);
+  }
+}
+
+__global__ void __launch_bounds__(BATCH_THREADS) k_batch_refine(const __grid_constant__ BatchArgs B) {
+  const uint32_t n_reqs = B.hdr->n_reqs;
+  const uint32_t n = B.dcount[4];
+  for (uint32_t i = blockIdx.x * BATCH_THREADS + threadIdx.x; i < n; i += gridDim.x * BATCH_THREADS) {
+    const uint32_t ray = B.q_refine[i];
+    const BatchRay br = batch_ray(B, n_reqs, ray);
+    const Scene s = batch_scene(B, &B.cams[br.q->cam]);
+    const HitGeom best = load_pixhit(s, B.px_hit + (size_t)ray * 4u);
+    store_rec_at(br.q->out, (size_t)br.gy * br.q->w + br.gx, viewport_voxel_rec(s, br.gx, br.gy, best));
+  }
+}
+
+__global__ void __launch_bounds__(BATCH_THREADS) k_batch_far(const __grid_constant__ BatchArgs B) {
+  const uint32_t n_reqs = B.hdr->n_reqs;
+  const uint32_t n = B.dcount[5];
+  for (uint32_t i = blockIdx.x * BATCH_THREADS + threadIdx.x; i < n; i += gridDim.x * BATCH_THREADS) {
+    const uint32_t ray = B.q_far[i];
+    const BatchRay br = batch_ray(B, n_reqs, ray);
+    const Scene s = batch_scene(B, &B.cams[br.q->cam]);
+    store_rec_at(br.q->out, (size_t)br.gy * br.q->w + br.gx, viewport_far_rec(s, br.gx, br.gy));
   }
 }
 

@@ -72,7 +72,8 @@ struct BatchLane {
   DevBuf hdr, reqs, cams, tile_count, tile_slots, head;
   // deferred grass probes of viewport rays: per-ray arrays for ray_cap rays,
   // probe records and slab tasks in proportion, counters
-  DevBuf probe_recs, slab_tasks, slab_res, slab_hits, px_first, px_task, px_mask, px_probe, px_vt, q_pending, dcount;
+  DevBuf probe_recs, slab_tasks, slab_res, slab_hits, px_first, px_task, px_mask, px_probe, px_hit, q_pending,
+      q_refine, q_far, dcount;
   uint32_t ray_cap = 0;
   void* stage = nullptr;  // pinned: header | requests | cameras
   cudaGraphExec_t graph = nullptr;
@@ -554,8 +555,8 @@ void vxe_destroy(vxe_ctx* c) {
   for (auto& L : c->lanes) {
     if (L.stream) cudaStreamSynchronize(L.stream);
     for (auto* b : {&L.hdr, &L.reqs, &L.cams, &L.tile_count, &L.tile_slots, &L.head, &L.probe_recs, &L.slab_tasks,
-                    &L.slab_res, &L.slab_hits, &L.px_first, &L.px_task, &L.px_mask, &L.px_probe, &L.px_vt,
-                    &L.q_pending, &L.dcount})
+                    &L.slab_res, &L.slab_hits, &L.px_first, &L.px_task, &L.px_mask, &L.px_probe, &L.px_hit,
+                    &L.q_pending, &L.q_refine, &L.q_far, &L.dcount})
       release(*b);
     if (L.graph) cudaGraphExecDestroy(L.graph);
     if (L.stage) cudaFreeHost(L.stage);
@@ -903,13 +904,15 @@ vxe_status lane_resources(vxe_ctx* c, BatchLane& L, uint32_t tiles, uint32_t vp_
     if ((st = alloc(c, L.px_mask, cap * 8)) != VXE_OK) return st;
     if ((st = alloc(c, L.px_probe, cap * 8)) != VXE_OK) return st;
     if ((st = alloc(c, L.px_task, cap * 4)) != VXE_OK) return st;
-    if ((st = alloc(c, L.px_vt, cap * 4)) != VXE_OK) return st;
+    if ((st = alloc(c, L.px_hit, cap * 64)) != VXE_OK) return st;
     if ((st = alloc(c, L.q_pending, cap * 4)) != VXE_OK) return st;
+    if ((st = alloc(c, L.q_refine, cap * 4)) != VXE_OK) return st;
+    if ((st = alloc(c, L.q_far, cap * 4)) != VXE_OK) return st;
     if ((st = alloc(c, L.probe_recs, cap * kBatchProbesPerRay * sizeof(vxe::dev::ProbeRec))) != VXE_OK) return st;
     if ((st = alloc(c, L.slab_tasks, cap * kBatchSlabsPerRay * 32)) != VXE_OK) return st;
     if ((st = alloc(c, L.slab_res, cap * kBatchSlabsPerRay * 16)) != VXE_OK) return st;
     if ((st = alloc(c, L.slab_hits, cap * kBatchSlabsPerRay * 4)) != VXE_OK) return st;
-    if (!L.dcount.p && (st = alloc(c, L.dcount, 16)) != VXE_OK) return st;
+    if (!L.dcount.p && (st = alloc(c, L.dcount, 32)) != VXE_OK) return st;
     L.ray_cap = (uint32_t)cap;
     if (L.graph) {  // the captured launches hold the old pointers
       cudaGraphExecDestroy(L.graph);
@@ -966,8 +969,10 @@ BatchArgs batch_args(const vxe_ctx* c, const BatchLane& L) {
   B.px_task = (uint32_t*)L.px_task.p;
   B.px_mask = (uint2*)L.px_mask.p;
   B.px_probe = (uint2*)L.px_probe.p;
-  B.px_vt = (float*)L.px_vt.p;
+  B.px_hit = (uint4*)L.px_hit.p;
   B.q_pending = (uint32_t*)L.q_pending.p;
+  B.q_refine = (uint32_t*)L.q_refine.p;
+  B.q_far = (uint32_t*)L.q_far.p;
   B.dcount = (uint32_t*)L.dcount.p;
   return B;
 }
@@ -981,7 +986,7 @@ vxe_status launch_persistent(vxe_ctx* c, BatchLane& L, const BatchArgs& B) {
                      L.stream));
   CK(cudaMemsetAsync(L.head.p, 0, 16, L.stream));
   if (B.defer) {
-    CK(cudaMemsetAsync(L.dcount.p, 0, 16, L.stream));
+    CK(cudaMemsetAsync(L.dcount.p, 0, 32, L.stream));
     k_batch_defer_clear<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
   }
   k_batch_tiles<<<c->b_tile_grid, TILE_THREADS, 0, L.stream>>>(B);
@@ -991,6 +996,8 @@ vxe_status launch_persistent(vxe_ctx* c, BatchLane& L, const BatchArgs& B) {
     k_batch_slab_eval<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
     k_batch_slab_pick<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
     k_batch_resolve<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
+    k_batch_refine<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
+    k_batch_far<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
   }
   CK(cudaGetLastError());
   return VXE_OK;
