@@ -20,7 +20,7 @@
 namespace vxe {
 namespace dev {
 
-struct BatchReq {  // 64 B
+struct BatchReq {  // 80 B
   uint32_t kind;        // 0 viewport, 1 query
   uint32_t w, h;        // viewport size; w = ray count for queries
   uint32_t tiles_x;     // viewport: logical 8x8 tiles per row
@@ -33,10 +33,14 @@ struct BatchReq {  // 64 B
   uint4* out;           // 2 x uint4 per record
   float tmax;
   uint32_t ray_base;    // first ray in the batch's viewport ray numbering (queries: the next viewport's)
+  uint32_t q_base;      // first ray in the batch's query ray numbering (viewports: the next query's)
+  uint32_t _pad[3];
 };
 
 struct BatchHeader {
   uint32_t n_reqs, total_tiles, n_items, tile_w, tile_h, rpt, tile_reqs, vp_rays;
+  // coherent queries: items >= vp_items take query rays in sorted order
+  uint32_t vp_items, q_rays, nbins, sorted;
 };
 
 struct BatchArgs {
@@ -88,6 +92,10 @@ struct BatchArgs {
   uint32_t* q_refine;             // rays whose answer is a grass voxel (grass-slab refinement)
   uint32_t* q_far;                // rays without a voxel answer (heightfield)
   uint32_t* dcount;               // [0] probes, [1] pending rays, [2] slab tasks, [3] slab hits, [4] refine, [5] far
+  // coherent queries: query rays binned by (origin chunk, direction octant)
+  uint32_t* q_keys;               // bin of each query ray
+  uint32_t* q_perm;               // query rays in bin order
+  uint32_t* bin_count;            // per bin: rays, then (after the scan) the next free position
 };
 
 constexpr int BATCH_THREADS = 128;
@@ -307,6 +315,25 @@ __device__ __forceinline__ void batch_item(const BatchArgs& B, const BatchHeader
   }
 }
 
+// Query rays in bin order (coherent mode): item k takes sorted positions
+// [k * 128 * rpt, ...); each lane finds its ray's request by the query base.
+__device__ __forceinline__ void batch_sorted_queries(const BatchArgs& B, const BatchHeader& H, uint32_t k,
+                                                     uint32_t lane) {
+  const uint32_t per = 128u * H.rpt;
+  for (uint32_t j = lane; j < per; j += 32u) {
+    const uint32_t pos = k * per + j;
+    if (pos >= H.q_rays) break;
+    const uint32_t ray = B.q_perm[pos];
+    const uint32_t r = find_req(B.reqs, H.n_reqs, ray, [](const BatchReq& q) { return q.q_base; });
+    const BatchReq& q = B.reqs[r];
+    const uint32_t i = ray - q.q_base;
+    const Scene s = batch_scene(B, &B.cams[0]);
+    const v3 ro = V3(q.o[3 * (size_t)i], q.o[3 * (size_t)i + 1], q.o[3 * (size_t)i + 2]);
+    const v3 rd = V3(q.d[3 * (size_t)i], q.d[3 * (size_t)i + 1], q.d[3 * (size_t)i + 2]);
+    store_rec_at(q.out, i, trace_query_ray(s, ro, rd, q.tmax));
+  }
+}
+
 // The persistent work-queue kernel (plain = 0) or one request per launch
 // with one warp per item (plain = 1, the per-request baseline).
 __global__ void __launch_bounds__(BATCH_THREADS) k_batch_trace(const __grid_constant__ BatchArgs B) {
@@ -341,6 +368,10 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_trace(const __grid_cons
     if (lane == 0) item = atomicAdd(&B.head[0], 1u);
     item = __shfl_sync(0xFFFFFFFFu, item, 0);
     if (item >= H.n_items) break;
+    if (H.sorted && item >= H.vp_items) {
+      batch_sorted_queries(B, H, item - H.vp_items, lane);
+      continue;
+    }
     const uint32_t r = find_req(B.reqs, H.n_reqs, item, [](const BatchReq& q) { return q.item_begin; });
     const BatchReq q = B.reqs[r];
     load_cam(q.cam);
@@ -517,6 +548,70 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_far(const __grid_consta
     const Scene s = batch_scene(B, &B.cams[br.q->cam]);
     store_rec_at(br.q->out, (size_t)br.gy * br.q->w + br.gx, viewport_far_rec(s, br.gx, br.gy));
   }
+}
+
+// ---------------------------------------------------------------------------
+// Coherent queries: query rays are binned by origin chunk (world grid cell,
+// clamped into the grid) and direction octant, and traced in bin order, so a
+// warp's rays start in the same chunk heading the same way.  Each ray's
+// record is its own; only the order of work changes.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t query_bin(const vxe_camera_gpu& cam, v3 o, v3 d) {
+  const float cs = (float)cam.chunk_size * cam.voxel_params[0];
+  const int32_t c[3] = {__float2int_rd(o.x / cs) - cam.grid_origin_chunk[0],
+                        __float2int_rd(o.y / cs) - cam.grid_origin_chunk[1],
+                        __float2int_rd(o.z / cs) - cam.grid_origin_chunk[2]};
+  uint32_t idx[3];
+  for (int k = 0; k < 3; ++k) idx[k] = (uint32_t)min(max(c[k], 0), (int32_t)max(cam.grid_dims[k], 1u) - 1);
+  const uint32_t cell = (idx[2] * max(cam.grid_dims[1], 1u) + idx[1]) * max(cam.grid_dims[0], 1u) + idx[0];
+  const uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+  return cell * 8u + oct;
+}
+
+__global__ void __launch_bounds__(BATCH_THREADS) k_qsort_count(const __grid_constant__ BatchArgs B) {
+  const BatchHeader& H = *B.hdr;
+  const uint32_t n = H.q_rays, n_reqs = H.n_reqs, nbins = H.nbins;
+  for (uint32_t ray = blockIdx.x * BATCH_THREADS + threadIdx.x; ray < n; ray += gridDim.x * BATCH_THREADS) {
+    const uint32_t r = find_req(B.reqs, n_reqs, ray, [](const BatchReq& q) { return q.q_base; });
+    const BatchReq& q = B.reqs[r];
+    const uint32_t i = ray - q.q_base;
+    const v3 o = V3(q.o[3 * (size_t)i], q.o[3 * (size_t)i + 1], q.o[3 * (size_t)i + 2]);
+    const v3 d = V3(q.d[3 * (size_t)i], q.d[3 * (size_t)i + 1], q.d[3 * (size_t)i + 2]);
+    const uint32_t bin = min(query_bin(B.cams[0], o, d), nbins - 1u);
+    B.q_keys[ray] = bin;
+    atomicAdd(&B.bin_count[bin], 1u);
+  }
+}
+
+// Exclusive scan of the bin counts in place (one block).
+constexpr int QSCAN_THREADS = 1024;
+__global__ void __launch_bounds__(QSCAN_THREADS) k_qsort_scan(const __grid_constant__ BatchArgs B) {
+  __shared__ uint32_t part[QSCAN_THREADS];
+  const uint32_t nbins = B.hdr->nbins;
+  const uint32_t per = (nbins + QSCAN_THREADS - 1) / QSCAN_THREADS;
+  const uint32_t b0 = threadIdx.x * per, b1 = min(b0 + per, nbins);
+  uint32_t sum = 0u;
+  for (uint32_t b = b0; b < b1; ++b) sum += B.bin_count[b];
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (uint32_t off = 1; off < QSCAN_THREADS; off <<= 1) {
+    const uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  uint32_t run = part[threadIdx.x] - sum;  // exclusive prefix of this thread's range
+  for (uint32_t b = b0; b < b1; ++b) {
+    const uint32_t c = B.bin_count[b];
+    B.bin_count[b] = run;
+    run += c;
+  }
+}
+
+__global__ void __launch_bounds__(BATCH_THREADS) k_qsort_scatter(const __grid_constant__ BatchArgs B) {
+  const uint32_t n = B.hdr->q_rays;
+  for (uint32_t ray = blockIdx.x * BATCH_THREADS + threadIdx.x; ray < n; ray += gridDim.x * BATCH_THREADS)
+    B.q_perm[atomicAdd(&B.bin_count[B.q_keys[ray]], 1u)] = ray;
 }
 
 }  // namespace dev

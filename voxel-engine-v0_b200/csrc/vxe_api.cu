@@ -75,6 +75,9 @@ struct BatchLane {
   DevBuf probe_recs, slab_tasks, slab_res, slab_hits, px_first, px_task, px_mask, px_probe, px_hit, q_pending,
       q_refine, q_far, dcount;
   uint32_t ray_cap = 0;
+  // coherent queries: bin of each query ray, rays in bin order, bin counters
+  DevBuf q_keys, q_perm, bin_count;
+  uint32_t q_cap = 0;
   void* stage = nullptr;  // pinned: header | requests | cameras
   cudaGraphExec_t graph = nullptr;
   uint32_t graph_key[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -556,7 +559,7 @@ void vxe_destroy(vxe_ctx* c) {
     if (L.stream) cudaStreamSynchronize(L.stream);
     for (auto* b : {&L.hdr, &L.reqs, &L.cams, &L.tile_count, &L.tile_slots, &L.head, &L.probe_recs, &L.slab_tasks,
                     &L.slab_res, &L.slab_hits, &L.px_first, &L.px_task, &L.px_mask, &L.px_probe, &L.px_hit,
-                    &L.q_pending, &L.q_refine, &L.q_far, &L.dcount})
+                    &L.q_pending, &L.q_refine, &L.q_far, &L.dcount, &L.q_keys, &L.q_perm, &L.bin_count})
       release(*b);
     if (L.graph) cudaGraphExecDestroy(L.graph);
     if (L.stage) cudaFreeHost(L.stage);
@@ -877,7 +880,7 @@ constexpr size_t kStageHdr = 0, kStageReqs = 64,
 // budget walk again with inline probes.
 constexpr uint32_t kBatchProbesPerRay = 4, kBatchSlabsPerRay = 2;
 
-vxe_status lane_resources(vxe_ctx* c, BatchLane& L, uint32_t tiles, uint32_t vp_rays) {
+vxe_status lane_resources(vxe_ctx* c, BatchLane& L, uint32_t tiles, uint32_t vp_rays, uint32_t q_rays) {
   vxe_status st;
   if (!L.stage) {
     if (cudaMallocHost(&L.stage, kStageBytes) != cudaSuccess) return fail(c, VXE_ERR_OOM, "pinned staging");
@@ -915,6 +918,18 @@ vxe_status lane_resources(vxe_ctx* c, BatchLane& L, uint32_t tiles, uint32_t vp_
     if (!L.dcount.p && (st = alloc(c, L.dcount, 32)) != VXE_OK) return st;
     L.ray_cap = (uint32_t)cap;
     if (L.graph) {  // the captured launches hold the old pointers
+      cudaGraphExecDestroy(L.graph);
+      L.graph = nullptr;
+    }
+  }
+  if (q_rays > L.q_cap) {
+    const uint64_t cap = std::max<uint64_t>((uint64_t)q_rays + q_rays / 2, 1u << 16);
+    if ((st = alloc(c, L.q_keys, cap * 4)) != VXE_OK) return st;
+    if ((st = alloc(c, L.q_perm, cap * 4)) != VXE_OK) return st;
+    if (!L.bin_count.p && (st = alloc(c, L.bin_count, (size_t)std::max(c->cfg.grid_capacity, 1u) * 8u * 4u)) != VXE_OK)
+      return st;
+    L.q_cap = (uint32_t)cap;
+    if (L.graph) {
       cudaGraphExecDestroy(L.graph);
       L.graph = nullptr;
     }
@@ -973,11 +988,14 @@ BatchArgs batch_args(const vxe_ctx* c, const BatchLane& L) {
   B.q_pending = (uint32_t*)L.q_pending.p;
   B.q_refine = (uint32_t*)L.q_refine.p;
   B.q_far = (uint32_t*)L.q_far.p;
+  B.q_keys = (uint32_t*)L.q_keys.p;
+  B.q_perm = (uint32_t*)L.q_perm.p;
+  B.bin_count = (uint32_t*)L.bin_count.p;
   B.dcount = (uint32_t*)L.dcount.p;
   return B;
 }
 
-vxe_status launch_persistent(vxe_ctx* c, BatchLane& L, const BatchArgs& B) {
+vxe_status launch_persistent(vxe_ctx* c, BatchLane& L, const BatchArgs& B, bool sorted) {
   using namespace vxe::dev;
   CK(cudaMemcpyAsync(L.hdr.p, (char*)L.stage + kStageHdr, sizeof(BatchHeader), cudaMemcpyHostToDevice, L.stream));
   CK(cudaMemcpyAsync(L.reqs.p, (char*)L.stage + kStageReqs, kStageCams - kStageReqs, cudaMemcpyHostToDevice,
@@ -988,6 +1006,12 @@ vxe_status launch_persistent(vxe_ctx* c, BatchLane& L, const BatchArgs& B) {
   if (B.defer) {
     CK(cudaMemsetAsync(L.dcount.p, 0, 32, L.stream));
     k_batch_defer_clear<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
+  }
+  if (sorted) {
+    CK(cudaMemsetAsync(L.bin_count.p, 0, L.bin_count.bytes, L.stream));
+    k_qsort_count<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
+    k_qsort_scan<<<1, QSCAN_THREADS, 0, L.stream>>>(B);
+    k_qsort_scatter<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
   }
   k_batch_tiles<<<c->b_tile_grid, TILE_THREADS, 0, L.stream>>>(B);
   k_batch_trace<<<c->b_trace_grid, BATCH_THREADS, 0, L.stream>>>(B);
@@ -1022,7 +1046,12 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
   // Host-side descriptors (requests keep their order; tiles and items are
   // numbered in request order so the device finds a request by binary search).
   uint32_t tiles = 0, items = 0;
-  uint64_t rays = 0, vp_rays = 0;
+  uint64_t rays = 0, vp_rays = 0, q_rays = 0;
+  // Coherent queries (persistent and graph modes): query rays are traced in
+  // bin order after every viewport item instead of as per-request items.
+  bool sorted = false;
+  if (opt->mode != VXE_BATCH_PLAIN)
+    for (uint32_t i = 0; i < n; ++i) sorted = sorted || reqs[i].kind == VXE_REQ_QUERY;
   std::vector<BatchReq> R(n);
   for (uint32_t i = 0; i < n; ++i) {
     const vxe_request& q = reqs[i];
@@ -1033,6 +1062,7 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
     r.tile_base = tiles;
     r.item_begin = items;
     r.ray_base = (uint32_t)vp_rays;  // a query repeats the next viewport's base
+    r.q_base = (uint32_t)q_rays;     // a viewport repeats the next query's base
     if (!q.d_out) return fail(c, VXE_ERR_INVALID_ARG, "request %u has no output", i);
     if (q.kind == VXE_REQ_VIEWPORT) {
       if (q.width == 0 || q.height == 0 || q.camera.render_present_px[0] != q.width ||
@@ -1055,8 +1085,10 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
       r.d = q.d_dirs;
       r.tmax = q.tmax;
       r.cam = 0;
-      items += (q.ray_count + 128 * rpt - 1) / (128 * rpt);
+      if (!sorted) items += (q.ray_count + 128 * rpt - 1) / (128 * rpt);
       rays += q.ray_count;
+      q_rays += q.ray_count;
+      if (q_rays > 0x3FFFFFFFull) return fail(c, VXE_ERR_CAPACITY, "batch of more than 2^30 query rays");
     } else {
       return fail(c, VXE_ERR_INVALID_ARG, "request %u kind %u", i, q.kind);
     }
@@ -1065,10 +1097,13 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
   // is the per-request single-launch baseline with the reference's inline
   // probes.
   const bool defer = opt->mode != VXE_BATCH_PLAIN && vp_rays != 0;
-  vxe_status st = lane_resources(c, L, tiles, defer ? (uint32_t)vp_rays : 0u);
+  const uint32_t vp_items = items;
+  if (sorted) items += (uint32_t)((q_rays + 128u * rpt - 1) / (128u * rpt));
+  vxe_status st = lane_resources(c, L, tiles, defer ? (uint32_t)vp_rays : 0u, sorted ? (uint32_t)q_rays : 0u);
   if (st != VXE_OK) return st;
   if (c->upload_recorded) CK(cudaStreamWaitEvent(L.stream, c->upload_done, 0));
-  BatchHeader H{n, tiles, items, tw, th, rpt, n, (uint32_t)vp_rays};
+  const uint32_t nbins = std::max(c->cfg.grid_capacity, 1u) * 8u;
+  BatchHeader H{n, tiles, items, tw, th, rpt, n, (uint32_t)vp_rays, vp_items, (uint32_t)q_rays, nbins, sorted ? 1u : 0u};
   std::memcpy((char*)L.stage + kStageHdr, &H, sizeof H);
   if (n) std::memcpy((char*)L.stage + kStageReqs, R.data(), n * sizeof(BatchReq));
   auto* cams = (vxe_camera_gpu*)((char*)L.stage + kStageCams);
@@ -1121,13 +1156,14 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
     }
     CK(cudaGetLastError());
   } else if (opt->mode == VXE_BATCH_PERSISTENT) {
-    if ((st = launch_persistent(c, L, B)) != VXE_OK) return st;
+    if ((st = launch_persistent(c, L, B, sorted)) != VXE_OK) return st;
   } else {
     // Captured once per tile-buffer allocation and clipmap uniform; later
     // batches only rewrite the pinned staging the graph's copies read.
     const uint32_t key[9] = {(uint32_t)(uintptr_t)L.tile_count.p, (uint32_t)((uintptr_t)L.tile_count.p >> 32),
                              (uint32_t)c->cfg.clip_levels, c->clip.levels, c->clip.res, 1u,
-                             (use_grass ? 1u : 0u) | (B.defer ? 2u : 0u), B.grass_time_bits, B.grass_strength_bits};
+                             (use_grass ? 1u : 0u) | (B.defer ? 2u : 0u) | (sorted ? 4u : 0u), B.grass_time_bits,
+                             B.grass_strength_bits};
     const bool same = L.graph != nullptr && std::memcmp(key, L.graph_key, sizeof key) == 0 &&
                       std::memcmp(&L.graph_clip, &B.clip, sizeof B.clip) == 0;
     if (!same) {
@@ -1137,7 +1173,7 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
       }
       cudaGraph_t g = nullptr;
       CK(cudaStreamBeginCapture(L.stream, cudaStreamCaptureModeThreadLocal));
-      st = launch_persistent(c, L, B);
+      st = launch_persistent(c, L, B, sorted);
       cudaError_t e = cudaStreamEndCapture(L.stream, &g);
       if (st != VXE_OK) return st;
       if (e != cudaSuccess) return fail(c, VXE_ERR_DEVICE, "graph capture: %s", cudaGetErrorString(e));
