@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--present", default="1920x1080")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched / served workloads")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--profile-steps", type=int, default=0, help="render N steps only (for ncu), no JSON")
     return ap.parse_args()
@@ -227,6 +228,58 @@ def run_vxe(args, rank: int, world_size: int):
     }
 
 
+def run_batch_serve(dev):
+    """Batched (north-star item 2) and served (item 5) workloads on the config-2 world.
+
+    batch: the config-3 request mix (24 viewports 128^2-1920x1080, 40 query
+    batches 1e3-1e6 rays, seeded) as one persistent batch vs one plain launch
+    per request (the single-launch pass with the reference's inline grass
+    probes), device time from the lane's CUDA events, best of 3.
+    serve: 120 Poisson requests at 1000 req/s (70 % viewports 256^2-1920x1080,
+    30 % query batches 1k-256k rays), continuous batching over 2 lanes with a
+    4 GiB admission budget and 10 chunk re-uploads per 16 ms tick, vs the plain
+    one-request-at-a-time server; latency = completion - arrival (host clock).
+    """
+    import torch
+
+    from vxe import _abi as A
+    from vxe.batch import make_batch
+    from vxe.renderer import Renderer
+    from vxe.scenes import FrameDriver, config2
+    from vxe.serve import make_arrivals, serve, serve_plain
+
+    sc = config2()
+    drv = FrameDriver(sc)
+    ups = drv.initial_uploads()
+    _, _, clip, cam = drv.step()
+    w = drv.world
+    r = Renderer(sc.present[0], sc.present[1], sc.render_scale, node_capacity=w.node_capacity,
+                 chunk_capacity=w.chunk_capacity, grid_capacity=w.grid_capacity, clip_levels=sc.clip_levels,
+                 clip_res=sc.clip_res, device=dev)
+    try:
+        r.upload_world(w, ups)
+        r.write_clipmap_updates(*clip)
+        r.write_camera(cam)
+        b = make_batch(w, torch, seed=3)
+        out = {}
+        for mode, name in [(A.BATCH_PLAIN, "plain"), (A.BATCH_PERSISTENT, "persistent"), (A.BATCH_GRAPH, "graph")]:
+            ms = min(r.submit_batch(b.requests, (8, 4), 1, mode).ms for _ in range(3))
+            out[name] = {"ms": round(ms, 3), "mrays_per_s": round(b.rays / ms / 1e3, 3)}
+        batch = {"workload": "config-3 mix: 24 viewports + 40 query batches, seed 3", "rays": int(b.rays),
+                 "tile": [8, 4], "rays_per_thread": 1, **out,
+                 "speedup_vs_plain": round(out["plain"]["ms"] / out["persistent"]["ms"], 3)}
+        reqs = make_arrivals(w, 2000.0, 20, seed=1)
+        serve(r, w, reqs, torch, mem_budget=4 << 30, lanes=2)  # warm-up
+        rep = serve(r, w, make_arrivals(w, 1000.0, 120, seed=7), torch, mem_budget=4 << 30, lanes=2, max_batch=32)
+        base = serve_plain(r, w, make_arrivals(w, 1000.0, 120, seed=7), torch)
+        srv = {"workload": "120 Poisson requests at 1000 req/s, 70 % viewports / 30 % query batches",
+               "batched": rep.summary(), "plain": base.summary(),
+               "speedup_vs_plain": round(base.seconds / rep.seconds, 3)}
+        return batch, srv
+    finally:
+        r.close()
+
+
 def run_e2e(args, sc, dev, world_size):
     import torch
 
@@ -377,6 +430,9 @@ def main():
     res = run_vxe(args, rank, world_size)
     if res is None:
         return
+    batch = srv = None
+    if not args.no_batch and world_size == 1:  # one GPU: the workloads north-star items 2 and 5 name
+        batch, srv = run_batch_serve(0)
     if world_size > 1:
         import torch
 
@@ -410,6 +466,8 @@ def main():
         # k_primary_resolve, k_shade_prep, k_shade_shadow, k_shade_lights, k_shade_vox, k_shade_far, k_godray,
         # k_composite
         "gpu_launches": 14 * args.steps,
+        "batch": batch,
+        "serve": srv,
         "clocks": res["clocks"],
         "device_error_word": res["error_word"],
     }
