@@ -76,7 +76,7 @@ def make_renderer(scene, world, flags=A.FLAG_GODRAY_MACRO_ALIAS | A.FLAG_HIT_REC
 
 
 def run_parity(scene, frames: int, threads: int | None = None, godray_alias: bool = True, on_frame=None,
-               extra_flags: int = 0):
+               extra_flags: int = 0, graph: bool = False):
     """Renders `frames` frames on both sides; returns a list of per-frame mismatch dicts."""
     drv = FrameDriver(scene)
     ups = drv.initial_uploads()
@@ -101,7 +101,10 @@ def run_parity(scene, frames: int, threads: int | None = None, godray_alias: boo
                 params = drv.empty_clip()
                 r.write_clipmap_updates(params, [])
             r.write_camera(cam)
-            r.encode_compute()
+            if graph:
+                r.render_frame_graph()
+            else:
+                r.encode_compute()
             ora.render(cam, params, threads=threads)
             g = read_gpu_frame(r)
             o = ora.outputs()

@@ -41,6 +41,16 @@ def test_features_scene_megakernel_schedule_bit_exact():
     assert all(r == {} for r in res), res
 
 
+def test_frames_as_cuda_graph_bit_exact():
+    # vxe_render_frame_graph: captured on the first frame, relaunched with new
+    # arguments afterwards (camera, clipmap, ping-pong images) -- including a
+    # grid shift with chunk uploads between frames.
+    sc = scenes.config2(present=(320, 180))
+    sc.shift_every = 2
+    res = run_parity(sc, frames=4, graph=True)
+    assert all(r == {} for r in res), res
+
+
 def test_features_scene_without_grass_table_bit_exact():
     # Every grass march derives its blades itself (no per-frame cell table):
     # the same images as the table path and the oracle.

@@ -118,6 +118,11 @@ struct vxe_ctx {
   int b_trace_grid = 0, b_tile_grid = 0;
   int shade_wave = 148 * 16;  // blocks of the grid-stride shading kernels
   bool upload_recorded = false;
+  // the frame as a captured CUDA graph (vxe_render_frame_graph)
+  cudaGraph_t fgraph = nullptr;
+  cudaGraphExec_t fgraph_exec = nullptr;
+  std::vector<cudaGraphNode_t> fgraph_nodes;
+  uint64_t fgraph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
 namespace {
@@ -364,7 +369,7 @@ vxe_status grass_table_release(vxe_ctx* c, cudaStream_t st, int reader) {
   return VXE_OK;
 }
 
-vxe_status launch_frame(vxe_ctx* c, bool timed) {
+vxe_status frame_validate(vxe_ctx* c) {
   if (c->iw == 0 || c->pw == 0) return fail(c, VXE_ERR_INVALID_ARG, "vxe_resize must be called before rendering");
   if (c->cam.render_present_px[0] != c->iw || c->cam.render_present_px[1] != c->ih ||
       c->cam.render_present_px[2] != c->pw || c->cam.render_present_px[3] != c->ph)
@@ -379,8 +384,10 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
     return fail(c, VXE_ERR_CAPACITY, "clipmap levels exceed allocated layers");
   if (c->clip.levels != 0 && c->clip.res != c->cfg.clip_res)
     return fail(c, VXE_ERR_INVALID_ARG, "clipmap res %u != allocated %u", c->clip.res, c->cfg.clip_res);
-  if (c->upload_recorded) CK(cudaStreamWaitEvent(c->compute, c->upload_done, 0));
-  FrameArgs A;
+  return VXE_OK;
+}
+
+void frame_fill(vxe_ctx* c, FrameArgs& A) {
   fill_scene_args(c, A);
   const int p = c->ping, q = 1 - c->ping;
   A.iw = c->iw;
@@ -424,15 +431,15 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
   A.px_task = (uint32_t*)c->img[IMG_PXTASK].p;
   A.px_mask = (uint2*)c->img[IMG_PXMASK].p;
   A.q_pending = (uint32_t*)c->img[IMG_QPENDING].p;
+}
+
+// The frame's launches on the compute stream (captured as-is by the graph
+// path; `timed` adds the per-pass events).
+vxe_status frame_enqueue(vxe_ctx* c, const FrameArgs& A, bool timed) {
   const uint32_t tiles_x = (c->iw + 7) / 8, tiles_y = (c->ih + 7) / 8;
   const uint32_t tiles = tiles_x * tiles_y;
   const uint32_t npix = c->iw * c->ih;
   using namespace vxe::dev;
-  if (timed) CK(cudaEventRecord(c->ev[0], c->compute));
-  bool use_grass = false;
-  vxe_status gst = grass_table_acquire(c, c->compute, 0, c->cam, &use_grass);
-  if (gst != VXE_OK) return gst;
-  if (use_grass) grass_table_args(c, A);
   if (timed) CK(cudaEventRecord(c->ev[1], c->compute));
   k_tiles<<<(tiles + TILE_THREADS - 1) / TILE_THREADS, TILE_THREADS, 0, c->compute>>>(A);
   if (timed) CK(cudaEventRecord(c->ev[2], c->compute));
@@ -469,10 +476,87 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
                 dim3(POST_THREADS_X, POST_THREADS_Y), 0, c->compute>>>(A);
   if (timed) CK(cudaEventRecord(c->ev[6], c->compute));
   CK(cudaGetLastError());
-  if (use_grass && (gst = grass_table_release(c, c->compute, 0)) != VXE_OK) return gst;
+  return VXE_OK;
+}
+
+vxe_status launch_frame(vxe_ctx* c, bool timed) {
+  vxe_status st = frame_validate(c);
+  if (st != VXE_OK) return st;
+  if (c->upload_recorded) CK(cudaStreamWaitEvent(c->compute, c->upload_done, 0));
+  FrameArgs A;
+  frame_fill(c, A);
+  if (timed) CK(cudaEventRecord(c->ev[0], c->compute));
+  bool use_grass = false;
+  if ((st = grass_table_acquire(c, c->compute, 0, c->cam, &use_grass)) != VXE_OK) return st;
+  if (use_grass) grass_table_args(c, A);
+  if ((st = frame_enqueue(c, A, timed)) != VXE_OK) return st;
+  if (use_grass && (st = grass_table_release(c, c->compute, 0)) != VXE_OK) return st;
   c->timed = timed;
   c->timed_trace = timed && !(c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL);
-  c->ping = q;
+  c->ping = 1 - c->ping;
+  return VXE_OK;
+}
+
+// The frame as one CUDA graph: captured on first use and again whenever the
+// launch shapes or the buffers of its memset nodes change (resize, schedule,
+// grass table use); every other frame only rewrites the kernel nodes'
+// argument (camera, clipmap uniform, ping-pong images) and relaunches.  The
+// grass cell table's (re)build is launched before the graph, outside it.
+vxe_status launch_frame_graph(vxe_ctx* c) {
+  vxe_status st = frame_validate(c);
+  if (st != VXE_OK) return st;
+  if (c->upload_recorded) CK(cudaStreamWaitEvent(c->compute, c->upload_done, 0));
+  FrameArgs A;
+  frame_fill(c, A);
+  bool use_grass = false;
+  if ((st = grass_table_acquire(c, c->compute, 0, c->cam, &use_grass)) != VXE_OK) return st;
+  if (use_grass) grass_table_args(c, A);
+  const uint64_t key[8] = {c->iw, c->ih, c->pw, c->ph,
+                           (uint64_t)(c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL) | (use_grass ? 2u : 0u),
+                           (uint64_t)c->shade_wave, (uint64_t)(uintptr_t)A.q_count, (uint64_t)(uintptr_t)A.px_first};
+  if (!c->fgraph_exec || std::memcmp(key, c->fgraph_key, sizeof key) != 0) {
+    if (c->fgraph_exec) cudaGraphExecDestroy(c->fgraph_exec);
+    if (c->fgraph) cudaGraphDestroy(c->fgraph);
+    c->fgraph_exec = nullptr;
+    c->fgraph = nullptr;
+    c->fgraph_nodes.clear();
+    CK(cudaStreamBeginCapture(c->compute, cudaStreamCaptureModeThreadLocal));
+    st = frame_enqueue(c, A, false);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->compute, &g);
+    if (st != VXE_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (e != cudaSuccess) return fail(c, VXE_ERR_DEVICE, "frame graph capture: %s", cudaGetErrorString(e));
+    c->fgraph = g;
+    size_t n = 0;
+    CK(cudaGraphGetNodes(g, nullptr, &n));
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (n) CK(cudaGraphGetNodes(g, nodes.data(), &n));
+    for (cudaGraphNode_t nd : nodes) {
+      cudaGraphNodeType t;
+      CK(cudaGraphNodeGetType(nd, &t));
+      if (t == cudaGraphNodeTypeKernel) c->fgraph_nodes.push_back(nd);
+    }
+    CK(cudaGraphInstantiate(&c->fgraph_exec, g, 0));
+    std::memcpy(c->fgraph_key, key, sizeof key);
+  } else {
+    // every frame kernel takes the one FrameArgs
+    void* args[1] = {(void*)&A};
+    for (cudaGraphNode_t nd : c->fgraph_nodes) {
+      cudaKernelNodeParams kp;
+      CK(cudaGraphKernelNodeGetParams(nd, &kp));
+      kp.kernelParams = args;
+      kp.extra = nullptr;
+      CK(cudaGraphExecKernelNodeSetParams(c->fgraph_exec, nd, &kp));
+    }
+  }
+  CK(cudaGraphLaunch(c->fgraph_exec, c->compute));
+  if (use_grass && (st = grass_table_release(c, c->compute, 0)) != VXE_OK) return st;
+  c->timed = false;
+  c->timed_trace = false;
+  c->ping = 1 - c->ping;
   return VXE_OK;
 }
 
@@ -550,6 +634,8 @@ void vxe_destroy(vxe_ctx* c) {
   cudaSetDevice(c->device);
   if (c->compute) cudaStreamSynchronize(c->compute);
   if (c->upload) cudaStreamSynchronize(c->upload);
+  if (c->fgraph_exec) cudaGraphExecDestroy(c->fgraph_exec);
+  if (c->fgraph) cudaGraphDestroy(c->fgraph);
   for (auto& L : c->lanes)  // lanes read the arenas: drain them before freeing
     if (L.stream) cudaStreamSynchronize(L.stream);
   for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword,
@@ -740,8 +826,16 @@ vxe_status vxe_render_frame(vxe_ctx* c, vxe_frame_out* out) {
 }
 
 vxe_status vxe_render_frame_graph(vxe_ctx* c, vxe_frame_out* out) {
-  // Plain launches until the graph path is enabled for this context.
-  return vxe_render_frame(c, out);
+  if (!c) return VXE_ERR_INVALID_ARG;
+  cudaSetDevice(c->device);
+  vxe_status st = launch_frame_graph(c);
+  if (st != VXE_OK) return st;
+  frame_out(c, out);
+  CK(cudaStreamSynchronize(c->compute));
+  uint32_t word = 0;
+  CK(cudaMemcpy(&word, c->errword.p, 4, cudaMemcpyDeviceToHost));
+  if (word) return fail(c, VXE_ERR_BOUNDS, "device bounds check tripped (error word 0x%x)", word);
+  return VXE_OK;
 }
 
 vxe_status vxe_synchronize(vxe_ctx* c) {
