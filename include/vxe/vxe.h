@@ -303,6 +303,31 @@ vxe_status vxe_submit_batch_async(vxe_ctx* ctx, uint32_t lane, const vxe_request
                                   const vxe_batch_options* opt);
 vxe_status vxe_batch_wait(vxe_ctx* ctx, uint32_t lane, int block, vxe_batch_stats* stats);
 
+/* Viewport sessions (serving; no counterpart in the reference, whose
+ * Renderer owns exactly one frame pipeline).  A view owns what one client's
+ * frames carry from frame to frame -- internal and present images, the
+ * primary-hit, shadow, local-light, godray and output histories, their
+ * ping-pong state and a captured frame graph -- and renders from the
+ * context's world (arenas, grid, clipmap, grass table).  Its frames are
+ * exactly the frames vxe_render_frame renders from the same camera sequence
+ * after vxe_resize (render/state/mod.rs:297-308, 329-446).
+ *   vxe_view_bytes          device bytes a view of that size holds (admission)
+ *   vxe_view_create         allocates it (histories start at zero)
+ *   vxe_view_render_async   one frame on a batch lane's stream; it may follow
+ *                           a batch on the same lane, and vxe_batch_wait then
+ *                           waits for both.  The camera's world fields
+ *                           (chunk size and count, grid origin and dims) are
+ *                           taken from the context's camera.
+ *   vxe_view_read_image     waits for the view's last frame, copies an image
+ *   vxe_view_destroy        waits for the view's last frame, frees it. */
+typedef struct vxe_view vxe_view;
+uint64_t vxe_view_bytes(const vxe_ctx* ctx, uint32_t present_w, uint32_t present_h, float render_scale);
+vxe_status vxe_view_create(vxe_ctx* ctx, uint32_t present_w, uint32_t present_h, float render_scale,
+                           vxe_view** out);
+vxe_status vxe_view_render_async(vxe_ctx* ctx, vxe_view* view, uint32_t lane, const vxe_camera_gpu* camera);
+vxe_status vxe_view_read_image(vxe_ctx* ctx, vxe_view* view, int image, void* host, size_t bytes);
+vxe_status vxe_view_destroy(vxe_ctx* ctx, vxe_view* view);
+
 /* GpuTimingsMs (render/state/mod.rs:22-31) minus blit; CUDA events of the last
  * frame.  local_taa and composite_taa are fused into primary / composite and
  * report 0.  Extra fields (no reference counterpart): primary_trace is the

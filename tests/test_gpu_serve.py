@@ -32,10 +32,13 @@ def test_served_results_equal_results_alone():
         assert s["requests"] == 40 and s["batches"] > 1
         assert all(x.done > 0 for x in reqs)
         for q in reqs:
-            mixed = q.out.cpu().numpy().tobytes()
+            mixed = q.out.cpu().numpy().view(A.HIT_DTYPE).copy()
             alone = _to_request(q, torch)
             torch.cuda.synchronize()
             r.submit_batch([alone], (8, 8), 2, A.BATCH_PERSISTENT)
-            assert q.out.cpu().numpy().tobytes() == mixed, q.rid
+            got = q.out.cpu().numpy().view(A.HIT_DTYPE)
+            diff = np.nonzero(got != mixed)[0]
+            assert diff.size == 0, (q.rid, q.kind, q.w, q.h, q.n, diff.size, diff[:4].tolist(),
+                                    str(mixed[diff[0]]), str(got[diff[0]]))
     finally:
         r.close()

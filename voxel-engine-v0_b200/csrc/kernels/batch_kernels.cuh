@@ -472,7 +472,9 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_slab_pick(const __grid_
     const uint4 a = B.slab_tasks[2u * j];
     const ProbeRec r = B.probe_recs[a.x];
     const unsigned long long key = slab_key(r.cand_phase >> 8, B.slab_res[j].x, r.cand_phase & 0xFFu, r.seq, a.y);
-    if (key == B.px_first[r.pixel]) B.px_task[r.pixel] = j;
+    const unsigned long long first = B.px_first[r.pixel];
+    if (key == first) B.px_task[r.pixel] = j;
+    else if (slab_hit_shadows_first(first, key)) atomicMin(&B.px_probe[r.pixel].y, 0u);
   }
 }
 

@@ -1084,10 +1084,11 @@ __device__ __forceinline__ HitGeom make_hit(uint32_t mat, float t, v3 n, v3 rb, 
 // its voxel hit.  A chunk walk does not depend on the loop's best so far, so
 // every chunk the reference walks is walked identically here (here fewer
 // chunks are skipped, as probe hits never lower the best).  Along one walk
-// probe intervals follow each other in t, so a chunk's first probe hit is
-// also its nearest; the answer is therefore the nearer of the nearest probe
-// hit over all chunks (key: t, chunk, probe, column) and the walk's voxel
-// answer, unless the voxel answer wins while its own chunk had a probe hit
+// probe intervals follow each other in t (up to rounding where one leaf's exit
+// meets the next: k_slab_pick sends those rare pixels to the inline walk), so
+// a chunk's first probe hit is also its nearest; the answer is therefore
+// the nearer of the nearest probe hit over all chunks (key: t, chunk, probe,
+// column) and the walk's voxel answer, unless the voxel answer wins while its own chunk had a probe hit
 // (its grass-slab refinement reached below that hit): such pixels, and pixels
 // whose probes did not all fit the buffers, walk again with inline probes.
 // PROBE_INLINE is the reference order (megakernel, batches, queries, that

@@ -762,7 +762,19 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_slab_eval(const __grid_consta
   }
 }
 
-// Finds, per pixel, the slab task whose key is the pixel's nearest.
+// True when hit `key` cannot stand for its chunk: an earlier probe of the
+// same chunk and trace phase also hit.  Successive probe intervals meet at a
+// leaf exit only up to rounding (t_leave + eps - eps), so in that rare case a
+// later probe's hit may be nearer than the chunk's first one, which is the
+// one the reference keeps.
+__device__ __forceinline__ bool slab_hit_shadows_first(unsigned long long first, unsigned long long key) {
+  const unsigned long long chunk_mask = (1ull << 62) | (31ull << 26);  // phase, candidate
+  const unsigned long long seq_mask = 0xFFFFFull << 6;
+  return first != ~0ull && (key & chunk_mask) == (first & chunk_mask) && (key & seq_mask) < (first & seq_mask);
+}
+
+// Finds, per pixel, the slab task whose key is the pixel's nearest; pixels
+// where that hit is not its chunk's first are sent to the inline walk.
 __global__ void __launch_bounds__(SHADE_THREADS) k_slab_pick(const __grid_constant__ FrameArgs A) {
   const uint32_t n = min(A.q_count[7], A.slab_cap);
   for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < n; i += gridDim.x * SHADE_THREADS) {
@@ -771,7 +783,9 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_slab_pick(const __grid_consta
     const ProbeRec r = A.probe_recs[a.x];
     const unsigned long long key =
         slab_key(r.cand_phase >> 8, A.slab_res[j].x, r.cand_phase & 0xFFu, r.seq, a.y);
-    if (key == A.px_first[r.pixel]) A.px_task[r.pixel] = j;
+    const unsigned long long first = A.px_first[r.pixel];
+    if (key == first) A.px_task[r.pixel] = j;
+    else if (slab_hit_shadows_first(first, key)) atomicMin(&A.px_probe[r.pixel].y, 0u);
   }
 }
 

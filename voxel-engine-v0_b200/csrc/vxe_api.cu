@@ -88,6 +88,22 @@ struct BatchLane {
   uint32_t items = 0, tiles = 0;
 };
 
+// One frame pipeline's images, ping-pong state, timing events and captured
+// graph: the context's own frame, and one per viewport session (vxe_view).
+struct FrameState {
+  DevBuf img[IMG_N];
+  uint32_t iw = 0, ih = 0, pw = 0, ph = 0;
+  int ping = 0;
+  // frame events: start, grass table, tiles, trace, shading, godray, composite
+  cudaEvent_t ev[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool timed = false, timed_trace = false;
+  // the frame as a captured CUDA graph
+  cudaGraph_t fgraph = nullptr;
+  cudaGraphExec_t fgraph_exec = nullptr;
+  std::vector<cudaGraphNode_t> fgraph_nodes;
+  uint64_t fgraph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+};
+
 }  // namespace
 
 struct vxe_ctx {
@@ -98,16 +114,10 @@ struct vxe_ctx {
   cudaStream_t compute = nullptr, upload = nullptr;
   cudaEvent_t upload_done = nullptr;
   bool upload_pending = false;
-  // frame events: start, grass table, tiles, trace, shading, godray, composite
-  cudaEvent_t ev[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-  bool timed = false, timed_trace = false;
   // arenas
   DevBuf nodes, ropes, metas, macro, colinfo, grid, clip_tex, errword;
   GrassTable gt;
-  // images
-  DevBuf img[IMG_N];
-  uint32_t iw = 0, ih = 0, pw = 0, ph = 0;
-  int ping = 0;
+  FrameState fr;  // the context's own frame
   vxe_camera_gpu cam{};
   vxe_clipmap_gpu clip{};
   // query scratch
@@ -118,11 +128,12 @@ struct vxe_ctx {
   int b_trace_grid = 0, b_tile_grid = 0;
   int shade_wave = 148 * 16;  // blocks of the grid-stride shading kernels
   bool upload_recorded = false;
-  // the frame as a captured CUDA graph (vxe_render_frame_graph)
-  cudaGraph_t fgraph = nullptr;
-  cudaGraphExec_t fgraph_exec = nullptr;
-  std::vector<cudaGraphNode_t> fgraph_nodes;
-  uint64_t fgraph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+};
+
+struct vxe_view {
+  FrameState fr;
+  cudaStream_t last_stream = nullptr;  // stream of the view's last frame
+  cudaEvent_t done = nullptr;          // orders frames that move between lanes
 };
 
 namespace {
@@ -147,6 +158,16 @@ vxe_status fail(vxe_ctx* c, vxe_status st, const char* fmt, ...) {
                   cudaGetErrorString(e_));                                                    \
   } while (0)
 
+// Fills device memory and waits for it.  A plain cudaMemset runs on the
+// legacy default stream, which the context's non-blocking streams do not wait
+// for: a pass launched right after could write the buffer first and then see
+// its results overwritten.
+cudaError_t fill_sync(void* p, int value, size_t bytes) {
+  cudaError_t e = cudaMemsetAsync(p, value, bytes, cudaStreamLegacy);
+  if (e != cudaSuccess) return e;
+  return cudaStreamSynchronize(cudaStreamLegacy);
+}
+
 vxe_status alloc(vxe_ctx* c, DevBuf& b, size_t bytes) {
   if (b.p) {
     cudaFree(b.p);
@@ -156,7 +177,7 @@ vxe_status alloc(vxe_ctx* c, DevBuf& b, size_t bytes) {
   if (bytes == 0) return VXE_OK;
   CK(cudaMalloc(&b.p, bytes));
   b.bytes = bytes;
-  CK(cudaMemset(b.p, 0, bytes));
+  CK(fill_sync(b.p, 0, bytes));
   return VXE_OK;
 }
 
@@ -172,9 +193,9 @@ constexpr size_t kProbesPerPixel = 8;
 // Grass slab marches those probes ask for, per internal pixel.
 constexpr size_t kSlabsPerPixel = 4;
 
-size_t img_bytes(const vxe_ctx* c, int i) {
-  const size_t in = (size_t)c->iw * c->ih, pn = (size_t)c->pw * c->ph;
-  const size_t tiles = (size_t)((c->iw + 7) / 8) * ((c->ih + 7) / 8);
+size_t img_bytes(const FrameState& F, int i) {
+  const size_t in = (size_t)F.iw * F.ih, pn = (size_t)F.pw * F.ph;
+  const size_t tiles = (size_t)((F.iw + 7) / 8) * ((F.ih + 7) / 8);
   switch (i) {
     case IMG_COLOR: case IMG_LOCAL: case IMG_LHIST0: case IMG_LHIST1: case IMG_GOD0: case IMG_GOD1:
     case IMG_HIST0: case IMG_HIST1:
@@ -220,23 +241,23 @@ bool img_enabled(const vxe_ctx* c, int i) {
   return true;
 }
 
-vxe_status alloc_images(vxe_ctx* c) {
+vxe_status alloc_images(vxe_ctx* c, FrameState& F) {
   for (int i = 0; i < IMG_N; ++i) {
-    const size_t b = img_enabled(c, i) ? img_bytes(c, i) : 0;
-    if (b != c->img[i].bytes || (b != 0) != (c->img[i].p != nullptr)) {
-      vxe_status st = alloc(c, c->img[i], b);
+    const size_t b = img_enabled(c, i) ? img_bytes(F, i) : 0;
+    if (b != F.img[i].bytes || (b != 0) != (F.img[i].p != nullptr)) {
+      vxe_status st = alloc(c, F.img[i], b);
       if (st != VXE_OK) return st;
-    } else if (c->img[i].p) {
-      if (cudaMemset(c->img[i].p, 0, b) != cudaSuccess) return fail(c, VXE_ERR_DEVICE, "memset failed");
+    } else if (F.img[i].p) {
+      if (fill_sync(F.img[i].p, 0, b) != cudaSuccess) return fail(c, VXE_ERR_DEVICE, "memset failed");
     }
   }
-  c->ping = 0;
+  F.ping = 0;
   return VXE_OK;
 }
 
 // Maps the public image id to the buffer index under the current ping.
-int map_image(const vxe_ctx* c, vxe_image im) {
-  const int p = c->ping, q = 1 - c->ping;
+int map_image(const FrameState& F, vxe_image im) {
+  const int p = F.ping, q = 1 - F.ping;
   switch (im) {
     case VXE_IMG_COLOR: return IMG_COLOR;
     case VXE_IMG_DEPTH: return IMG_DEPTH;
@@ -369,17 +390,17 @@ vxe_status grass_table_release(vxe_ctx* c, cudaStream_t st, int reader) {
   return VXE_OK;
 }
 
-vxe_status frame_validate(vxe_ctx* c) {
-  if (c->iw == 0 || c->pw == 0) return fail(c, VXE_ERR_INVALID_ARG, "vxe_resize must be called before rendering");
-  if (c->cam.render_present_px[0] != c->iw || c->cam.render_present_px[1] != c->ih ||
-      c->cam.render_present_px[2] != c->pw || c->cam.render_present_px[3] != c->ph)
+vxe_status frame_validate(vxe_ctx* c, const FrameState& F, const vxe_camera_gpu& cam) {
+  if (F.iw == 0 || F.pw == 0) return fail(c, VXE_ERR_INVALID_ARG, "vxe_resize must be called before rendering");
+  if (cam.render_present_px[0] != F.iw || cam.render_present_px[1] != F.ih ||
+      cam.render_present_px[2] != F.pw || cam.render_present_px[3] != F.ph)
     return fail(c, VXE_ERR_INVALID_ARG, "camera render_present_px (%u,%u,%u,%u) does not match images (%u,%u,%u,%u)",
-                c->cam.render_present_px[0], c->cam.render_present_px[1], c->cam.render_present_px[2],
-                c->cam.render_present_px[3], c->iw, c->ih, c->pw, c->ph);
-  if (c->cam.chunk_size != 64u) return fail(c, VXE_ERR_INVALID_ARG, "chunk_size must be 64 (colinfo layout)");
-  if ((uint64_t)c->cam.grid_dims[0] * c->cam.grid_dims[1] * c->cam.grid_dims[2] > c->cfg.grid_capacity)
+                cam.render_present_px[0], cam.render_present_px[1], cam.render_present_px[2],
+                cam.render_present_px[3], F.iw, F.ih, F.pw, F.ph);
+  if (cam.chunk_size != 64u) return fail(c, VXE_ERR_INVALID_ARG, "chunk_size must be 64 (colinfo layout)");
+  if ((uint64_t)cam.grid_dims[0] * cam.grid_dims[1] * cam.grid_dims[2] > c->cfg.grid_capacity)
     return fail(c, VXE_ERR_CAPACITY, "grid_dims exceed grid capacity");
-  if (c->cam.chunk_count > c->cfg.chunk_capacity) return fail(c, VXE_ERR_CAPACITY, "chunk_count exceeds capacity");
+  if (cam.chunk_count > c->cfg.chunk_capacity) return fail(c, VXE_ERR_CAPACITY, "chunk_count exceeds capacity");
   if (c->clip.levels > c->cfg.clip_levels && c->clip.levels != 0)
     return fail(c, VXE_ERR_CAPACITY, "clipmap levels exceed allocated layers");
   if (c->clip.levels != 0 && c->clip.res != c->cfg.clip_res)
@@ -387,65 +408,66 @@ vxe_status frame_validate(vxe_ctx* c) {
   return VXE_OK;
 }
 
-void frame_fill(vxe_ctx* c, FrameArgs& A) {
+void frame_fill(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& cam, FrameArgs& A) {
   fill_scene_args(c, A);
-  const int p = c->ping, q = 1 - c->ping;
-  A.iw = c->iw;
-  A.ih = c->ih;
-  A.pw = c->pw;
-  A.ph = c->ph;
-  A.tile_count = (uint32_t*)c->img[IMG_TILE_COUNT].p;
-  A.tile_slots = (uint32_t*)c->img[IMG_TILE_SLOTS].p;
-  A.hist_in = (const uint4*)c->img[IMG_HIST0 + p].p;
-  A.hist_out = (uint4*)c->img[IMG_HIST0 + q].p;
-  A.shadow_in = (const float*)c->img[IMG_SHADOW0 + p].p;
-  A.shadow_out = (float*)c->img[IMG_SHADOW0 + q].p;
-  A.local_hist_in = (const float4*)c->img[IMG_LHIST0 + p].p;
-  A.local_hist_out = (float4*)c->img[IMG_LHIST0 + q].p;
-  A.color = (float4*)c->img[IMG_COLOR].p;
-  A.depth = (float*)c->img[IMG_DEPTH].p;
-  A.local = (float4*)c->img[IMG_LOCAL].p;
-  A.god_in = (const float4*)c->img[IMG_GOD0 + p].p;
-  A.god_out = (float4*)c->img[IMG_GOD0 + q].p;
-  A.pre_taa = (float4*)c->img[IMG_PRE_TAA].p;
-  A.output = (float4*)c->img[IMG_OUTPUT].p;
-  A.out_hist_in = (const float4*)c->img[IMG_OHIST0 + p].p;
-  A.out_hist_out = (float4*)c->img[IMG_OHIST0 + q].p;
-  A.hits = (uint4*)c->img[IMG_HITS].p;
-  A.pix_hit = (uint4*)c->img[IMG_PIXHIT].p;
-  A.q_vox = (uint32_t*)c->img[IMG_QVOX].p;
-  A.q_far = (uint32_t*)c->img[IMG_QFAR].p;
-  A.q_count = (uint32_t*)c->img[IMG_QCOUNT].p;
-  A.q_shadow = (uint32_t*)c->img[IMG_QSHADOW].p;
-  A.q_light = (uint32_t*)c->img[IMG_QLIGHT].p;
-  A.px_shadow = (float*)c->img[IMG_PXSHADOW].p;
-  A.px_light = (float4*)c->img[IMG_PXLIGHT].p;
-  A.probe_recs = (vxe::dev::ProbeRec*)c->img[IMG_PROBE_RECS].p;
-  A.probe_cap = (uint32_t)std::min<size_t>(c->img[IMG_PROBE_RECS].bytes / sizeof(vxe::dev::ProbeRec), 0xFFFFFFFFu);
-  A.slab_tasks = (uint4*)c->img[IMG_SLAB_TASKS].p;
-  A.slab_res = (float4*)c->img[IMG_SLAB_RES].p;
-  A.slab_cap = (uint32_t)std::min<size_t>(c->img[IMG_SLAB_TASKS].bytes / 32u, 0xFFFFFFFFu);
-  A.px_first = (unsigned long long*)c->img[IMG_PXFIRST].p;
-  A.px_probe = (uint2*)c->img[IMG_PXPROBE].p;
-  A.slab_hits = (uint32_t*)c->img[IMG_SLAB_HITS].p;
-  A.px_task = (uint32_t*)c->img[IMG_PXTASK].p;
-  A.px_mask = (uint2*)c->img[IMG_PXMASK].p;
-  A.q_pending = (uint32_t*)c->img[IMG_QPENDING].p;
+  A.cam = cam;
+  const int p = F.ping, q = 1 - F.ping;
+  A.iw = F.iw;
+  A.ih = F.ih;
+  A.pw = F.pw;
+  A.ph = F.ph;
+  A.tile_count = (uint32_t*)F.img[IMG_TILE_COUNT].p;
+  A.tile_slots = (uint32_t*)F.img[IMG_TILE_SLOTS].p;
+  A.hist_in = (const uint4*)F.img[IMG_HIST0 + p].p;
+  A.hist_out = (uint4*)F.img[IMG_HIST0 + q].p;
+  A.shadow_in = (const float*)F.img[IMG_SHADOW0 + p].p;
+  A.shadow_out = (float*)F.img[IMG_SHADOW0 + q].p;
+  A.local_hist_in = (const float4*)F.img[IMG_LHIST0 + p].p;
+  A.local_hist_out = (float4*)F.img[IMG_LHIST0 + q].p;
+  A.color = (float4*)F.img[IMG_COLOR].p;
+  A.depth = (float*)F.img[IMG_DEPTH].p;
+  A.local = (float4*)F.img[IMG_LOCAL].p;
+  A.god_in = (const float4*)F.img[IMG_GOD0 + p].p;
+  A.god_out = (float4*)F.img[IMG_GOD0 + q].p;
+  A.pre_taa = (float4*)F.img[IMG_PRE_TAA].p;
+  A.output = (float4*)F.img[IMG_OUTPUT].p;
+  A.out_hist_in = (const float4*)F.img[IMG_OHIST0 + p].p;
+  A.out_hist_out = (float4*)F.img[IMG_OHIST0 + q].p;
+  A.hits = (uint4*)F.img[IMG_HITS].p;
+  A.pix_hit = (uint4*)F.img[IMG_PIXHIT].p;
+  A.q_vox = (uint32_t*)F.img[IMG_QVOX].p;
+  A.q_far = (uint32_t*)F.img[IMG_QFAR].p;
+  A.q_count = (uint32_t*)F.img[IMG_QCOUNT].p;
+  A.q_shadow = (uint32_t*)F.img[IMG_QSHADOW].p;
+  A.q_light = (uint32_t*)F.img[IMG_QLIGHT].p;
+  A.px_shadow = (float*)F.img[IMG_PXSHADOW].p;
+  A.px_light = (float4*)F.img[IMG_PXLIGHT].p;
+  A.probe_recs = (vxe::dev::ProbeRec*)F.img[IMG_PROBE_RECS].p;
+  A.probe_cap = (uint32_t)std::min<size_t>(F.img[IMG_PROBE_RECS].bytes / sizeof(vxe::dev::ProbeRec), 0xFFFFFFFFu);
+  A.slab_tasks = (uint4*)F.img[IMG_SLAB_TASKS].p;
+  A.slab_res = (float4*)F.img[IMG_SLAB_RES].p;
+  A.slab_cap = (uint32_t)std::min<size_t>(F.img[IMG_SLAB_TASKS].bytes / 32u, 0xFFFFFFFFu);
+  A.px_first = (unsigned long long*)F.img[IMG_PXFIRST].p;
+  A.px_probe = (uint2*)F.img[IMG_PXPROBE].p;
+  A.slab_hits = (uint32_t*)F.img[IMG_SLAB_HITS].p;
+  A.px_task = (uint32_t*)F.img[IMG_PXTASK].p;
+  A.px_mask = (uint2*)F.img[IMG_PXMASK].p;
+  A.q_pending = (uint32_t*)F.img[IMG_QPENDING].p;
 }
 
 // The frame's launches on the compute stream (captured as-is by the graph
 // path; `timed` adds the per-pass events).
-vxe_status frame_enqueue(vxe_ctx* c, const FrameArgs& A, bool timed) {
-  const uint32_t tiles_x = (c->iw + 7) / 8, tiles_y = (c->ih + 7) / 8;
+vxe_status frame_enqueue(vxe_ctx* c, FrameState& F, const FrameArgs& A, bool timed, cudaStream_t st) {
+  const uint32_t tiles_x = (F.iw + 7) / 8, tiles_y = (F.ih + 7) / 8;
   const uint32_t tiles = tiles_x * tiles_y;
-  const uint32_t npix = c->iw * c->ih;
+  const uint32_t npix = F.iw * F.ih;
   using namespace vxe::dev;
-  if (timed) CK(cudaEventRecord(c->ev[1], c->compute));
-  k_tiles<<<(tiles + TILE_THREADS - 1) / TILE_THREADS, TILE_THREADS, 0, c->compute>>>(A);
-  if (timed) CK(cudaEventRecord(c->ev[2], c->compute));
+  if (timed) CK(cudaEventRecord(F.ev[1], st));
+  k_tiles<<<(tiles + TILE_THREADS - 1) / TILE_THREADS, TILE_THREADS, 0, st>>>(A);
+  if (timed) CK(cudaEventRecord(F.ev[2], st));
   if (c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL) {
-    k_primary<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, c->compute>>>(A);
-    if (timed) CK(cudaEventRecord(c->ev[3], c->compute));
+    k_primary<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, st>>>(A);
+    if (timed) CK(cudaEventRecord(F.ev[3], st));
   } else {
     // Queue lengths stay on the device: each kernel after the walk runs over
     // its queue with a grid-stride loop over at most a full wave of blocks.
@@ -453,47 +475,47 @@ vxe_status frame_enqueue(vxe_ctx* c, const FrameArgs& A, bool timed) {
       return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((threads + SHADE_THREADS - 1) / SHADE_THREADS,
                                                                 (uint64_t)c->shade_wave));
     };
-    CK(cudaMemsetAsync(A.q_count, 0, 32, c->compute));
-    CK(cudaMemsetAsync(A.px_first, 0xFF, (size_t)npix * 8u, c->compute));
-    CK(cudaMemsetAsync(A.px_mask, 0, (size_t)npix * 8u, c->compute));
-    k_primary_trace<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, c->compute>>>(A);
-    k_probe_dda<<<grid((uint64_t)npix * kProbesPerPixel), SHADE_THREADS, 0, c->compute>>>(A);
-    k_slab_eval<<<grid((uint64_t)npix * kSlabsPerPixel), SHADE_THREADS, 0, c->compute>>>(A);
-    k_slab_pick<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
-    k_primary_resolve<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
-    if (timed) CK(cudaEventRecord(c->ev[3], c->compute));
-    k_shade_prep<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
-    k_shade_shadow<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
-    k_shade_lights<<<grid((uint64_t)npix * 8u), SHADE_THREADS, 0, c->compute>>>(A);
-    k_shade_vox<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
-    k_shade_far<<<grid(npix), SHADE_THREADS, 0, c->compute>>>(A);
+    CK(cudaMemsetAsync(A.q_count, 0, 32, st));
+    CK(cudaMemsetAsync(A.px_first, 0xFF, (size_t)npix * 8u, st));
+    CK(cudaMemsetAsync(A.px_mask, 0, (size_t)npix * 8u, st));
+    k_primary_trace<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, st>>>(A);
+    k_probe_dda<<<grid((uint64_t)npix * kProbesPerPixel), SHADE_THREADS, 0, st>>>(A);
+    k_slab_eval<<<grid((uint64_t)npix * kSlabsPerPixel), SHADE_THREADS, 0, st>>>(A);
+    k_slab_pick<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
+    k_primary_resolve<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
+    if (timed) CK(cudaEventRecord(F.ev[3], st));
+    k_shade_prep<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
+    k_shade_shadow<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
+    k_shade_lights<<<grid((uint64_t)npix * 8u), SHADE_THREADS, 0, st>>>(A);
+    k_shade_vox<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
+    k_shade_far<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
   }
-  if (timed) CK(cudaEventRecord(c->ev[4], c->compute));
-  k_godray<<<dim3((c->iw + POST_THREADS_X - 1) / POST_THREADS_X, (c->ih + POST_THREADS_Y - 1) / POST_THREADS_Y),
-             dim3(POST_THREADS_X, POST_THREADS_Y), 0, c->compute>>>(A);
-  if (timed) CK(cudaEventRecord(c->ev[5], c->compute));
-  k_composite<<<dim3((c->pw + POST_THREADS_X - 1) / POST_THREADS_X, (c->ph + POST_THREADS_Y - 1) / POST_THREADS_Y),
-                dim3(POST_THREADS_X, POST_THREADS_Y), 0, c->compute>>>(A);
-  if (timed) CK(cudaEventRecord(c->ev[6], c->compute));
+  if (timed) CK(cudaEventRecord(F.ev[4], st));
+  k_godray<<<dim3((F.iw + POST_THREADS_X - 1) / POST_THREADS_X, (F.ih + POST_THREADS_Y - 1) / POST_THREADS_Y),
+             dim3(POST_THREADS_X, POST_THREADS_Y), 0, st>>>(A);
+  if (timed) CK(cudaEventRecord(F.ev[5], st));
+  k_composite<<<dim3((F.pw + POST_THREADS_X - 1) / POST_THREADS_X, (F.ph + POST_THREADS_Y - 1) / POST_THREADS_Y),
+                dim3(POST_THREADS_X, POST_THREADS_Y), 0, st>>>(A);
+  if (timed) CK(cudaEventRecord(F.ev[6], st));
   CK(cudaGetLastError());
   return VXE_OK;
 }
 
 vxe_status launch_frame(vxe_ctx* c, bool timed) {
-  vxe_status st = frame_validate(c);
+  vxe_status st = frame_validate(c, c->fr, c->cam);
   if (st != VXE_OK) return st;
   if (c->upload_recorded) CK(cudaStreamWaitEvent(c->compute, c->upload_done, 0));
   FrameArgs A;
-  frame_fill(c, A);
-  if (timed) CK(cudaEventRecord(c->ev[0], c->compute));
+  frame_fill(c, c->fr, c->cam, A);
+  if (timed) CK(cudaEventRecord(c->fr.ev[0], c->compute));
   bool use_grass = false;
   if ((st = grass_table_acquire(c, c->compute, 0, c->cam, &use_grass)) != VXE_OK) return st;
   if (use_grass) grass_table_args(c, A);
-  if ((st = frame_enqueue(c, A, timed)) != VXE_OK) return st;
+  if ((st = frame_enqueue(c, c->fr, A, timed, c->compute)) != VXE_OK) return st;
   if (use_grass && (st = grass_table_release(c, c->compute, 0)) != VXE_OK) return st;
-  c->timed = timed;
-  c->timed_trace = timed && !(c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL);
-  c->ping = 1 - c->ping;
+  c->fr.timed = timed;
+  c->fr.timed_trace = timed && !(c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL);
+  c->fr.ping = 1 - c->fr.ping;
   return VXE_OK;
 }
 
@@ -502,34 +524,34 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
 // grass table use); every other frame only rewrites the kernel nodes'
 // argument (camera, clipmap uniform, ping-pong images) and relaunches.  The
 // grass cell table's (re)build is launched before the graph, outside it.
-vxe_status launch_frame_graph(vxe_ctx* c) {
-  vxe_status st = frame_validate(c);
-  if (st != VXE_OK) return st;
-  if (c->upload_recorded) CK(cudaStreamWaitEvent(c->compute, c->upload_done, 0));
+vxe_status launch_frame_graph(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& cam, cudaStream_t st, int reader) {
+  vxe_status rc = frame_validate(c, F, cam);
+  if (rc != VXE_OK) return rc;
+  if (c->upload_recorded) CK(cudaStreamWaitEvent(st, c->upload_done, 0));
   FrameArgs A;
-  frame_fill(c, A);
+  frame_fill(c, F, cam, A);
   bool use_grass = false;
-  if ((st = grass_table_acquire(c, c->compute, 0, c->cam, &use_grass)) != VXE_OK) return st;
+  if ((rc = grass_table_acquire(c, st, reader, cam, &use_grass)) != VXE_OK) return rc;
   if (use_grass) grass_table_args(c, A);
-  const uint64_t key[8] = {c->iw, c->ih, c->pw, c->ph,
+  const uint64_t key[8] = {F.iw, F.ih, F.pw, F.ph,
                            (uint64_t)(c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL) | (use_grass ? 2u : 0u),
                            (uint64_t)c->shade_wave, (uint64_t)(uintptr_t)A.q_count, (uint64_t)(uintptr_t)A.px_first};
-  if (!c->fgraph_exec || std::memcmp(key, c->fgraph_key, sizeof key) != 0) {
-    if (c->fgraph_exec) cudaGraphExecDestroy(c->fgraph_exec);
-    if (c->fgraph) cudaGraphDestroy(c->fgraph);
-    c->fgraph_exec = nullptr;
-    c->fgraph = nullptr;
-    c->fgraph_nodes.clear();
-    CK(cudaStreamBeginCapture(c->compute, cudaStreamCaptureModeThreadLocal));
-    st = frame_enqueue(c, A, false);
+  if (!F.fgraph_exec || std::memcmp(key, F.fgraph_key, sizeof key) != 0) {
+    if (F.fgraph_exec) cudaGraphExecDestroy(F.fgraph_exec);
+    if (F.fgraph) cudaGraphDestroy(F.fgraph);
+    F.fgraph_exec = nullptr;
+    F.fgraph = nullptr;
+    F.fgraph_nodes.clear();
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    rc = frame_enqueue(c, F, A, false, st);
     cudaGraph_t g = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(c->compute, &g);
-    if (st != VXE_OK) {
+    const cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (rc != VXE_OK) {
       if (g) cudaGraphDestroy(g);
-      return st;
+      return rc;
     }
     if (e != cudaSuccess) return fail(c, VXE_ERR_DEVICE, "frame graph capture: %s", cudaGetErrorString(e));
-    c->fgraph = g;
+    F.fgraph = g;
     size_t n = 0;
     CK(cudaGraphGetNodes(g, nullptr, &n));
     std::vector<cudaGraphNode_t> nodes(n);
@@ -537,39 +559,58 @@ vxe_status launch_frame_graph(vxe_ctx* c) {
     for (cudaGraphNode_t nd : nodes) {
       cudaGraphNodeType t;
       CK(cudaGraphNodeGetType(nd, &t));
-      if (t == cudaGraphNodeTypeKernel) c->fgraph_nodes.push_back(nd);
+      if (t == cudaGraphNodeTypeKernel) F.fgraph_nodes.push_back(nd);
     }
-    CK(cudaGraphInstantiate(&c->fgraph_exec, g, 0));
-    std::memcpy(c->fgraph_key, key, sizeof key);
+    CK(cudaGraphInstantiate(&F.fgraph_exec, g, 0));
+    std::memcpy(F.fgraph_key, key, sizeof key);
   } else {
     // every frame kernel takes the one FrameArgs
     void* args[1] = {(void*)&A};
-    for (cudaGraphNode_t nd : c->fgraph_nodes) {
+    for (cudaGraphNode_t nd : F.fgraph_nodes) {
       cudaKernelNodeParams kp;
       CK(cudaGraphKernelNodeGetParams(nd, &kp));
       kp.kernelParams = args;
       kp.extra = nullptr;
-      CK(cudaGraphExecKernelNodeSetParams(c->fgraph_exec, nd, &kp));
+      CK(cudaGraphExecKernelNodeSetParams(F.fgraph_exec, nd, &kp));
     }
   }
-  CK(cudaGraphLaunch(c->fgraph_exec, c->compute));
-  if (use_grass && (st = grass_table_release(c, c->compute, 0)) != VXE_OK) return st;
-  c->timed = false;
-  c->timed_trace = false;
-  c->ping = 1 - c->ping;
+  CK(cudaGraphLaunch(F.fgraph_exec, st));
+  if (use_grass && (rc = grass_table_release(c, st, reader)) != VXE_OK) return rc;
+  F.timed = false;
+  F.timed_trace = false;
+  F.ping = 1 - F.ping;
   return VXE_OK;
+}
+
+// internal = round(present * scale).max(1) (render/state/mod.rs:239-241);
+// f32::round rounds half away from zero, like std::round.
+void set_dims(FrameState& F, uint32_t present_w, uint32_t present_h, float render_scale) {
+  const float fw = (float)present_w * render_scale, fh = (float)present_h * render_scale;
+  F.iw = (uint32_t)std::max(1.0f, std::round(fw));
+  F.ih = (uint32_t)std::max(1.0f, std::round(fh));
+  F.pw = present_w;
+  F.ph = present_h;
+}
+
+void release_frame_state(FrameState& F) {
+  if (F.fgraph_exec) cudaGraphExecDestroy(F.fgraph_exec);
+  if (F.fgraph) cudaGraphDestroy(F.fgraph);
+  F.fgraph_exec = nullptr;
+  F.fgraph = nullptr;
+  F.fgraph_nodes.clear();
+  for (auto& b : F.img) release(b);
 }
 
 void frame_out(vxe_ctx* c, vxe_frame_out* out) {
   if (!out) return;
-  out->color = (float*)c->img[IMG_COLOR].p;
-  out->depth = (float*)c->img[IMG_DEPTH].p;
-  out->godray = (float*)c->img[IMG_GOD0 + c->ping].p;  // written this frame (ping already flipped)
-  out->output = (float*)c->img[IMG_OUTPUT].p;
-  out->internal_w = c->iw;
-  out->internal_h = c->ih;
-  out->present_w = c->pw;
-  out->present_h = c->ph;
+  out->color = (float*)c->fr.img[IMG_COLOR].p;
+  out->depth = (float*)c->fr.img[IMG_DEPTH].p;
+  out->godray = (float*)c->fr.img[IMG_GOD0 + c->fr.ping].p;  // written this frame (ping already flipped)
+  out->output = (float*)c->fr.img[IMG_OUTPUT].p;
+  out->internal_w = c->fr.iw;
+  out->internal_h = c->fr.ih;
+  out->present_w = c->fr.pw;
+  out->present_h = c->fr.ph;
 }
 
 }  // namespace
@@ -599,7 +640,7 @@ vxe_status vxe_create(const vxe_config* cfg, vxe_ctx** out) {
       cudaStreamCreateWithFlags(&c->upload, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->upload_done, cudaEventDisableTiming) != cudaSuccess)
     return bail(VXE_ERR_DEVICE);
-  for (auto& e : c->ev)
+  for (auto& e : c->fr.ev)
     if (cudaEventCreate(&e) != cudaSuccess) return bail(VXE_ERR_DEVICE);
   const uint64_t nc = cfg->node_capacity, cc = cfg->chunk_capacity;
   if ((st = alloc(c, c->nodes, nc * 16)) != VXE_OK) return bail(st);
@@ -608,7 +649,7 @@ vxe_status vxe_create(const vxe_config* cfg, vxe_ctx** out) {
   if ((st = alloc(c, c->macro, cc * VXE_MACRO_WORDS_PER_CHUNK * 4)) != VXE_OK) return bail(st);
   if ((st = alloc(c, c->colinfo, cc * VXE_COLINFO_WORDS_PER_CHUNK * 4)) != VXE_OK) return bail(st);
   if ((st = alloc(c, c->grid, (uint64_t)cfg->grid_capacity * 4)) != VXE_OK) return bail(st);
-  if (cudaMemset(c->grid.p, 0xFF, c->grid.bytes) != cudaSuccess) return bail(VXE_ERR_DEVICE);
+  if (fill_sync(c->grid.p, 0xFF, c->grid.bytes) != cudaSuccess) return bail(VXE_ERR_DEVICE);
   const uint64_t clip_bytes = (uint64_t)cfg->clip_levels * cfg->clip_res * cfg->clip_res * 4;
   if ((st = alloc(c, c->clip_tex, clip_bytes)) != VXE_OK) return bail(st);
   if ((st = alloc(c, c->errword, 4)) != VXE_OK) return bail(st);
@@ -634,8 +675,8 @@ void vxe_destroy(vxe_ctx* c) {
   cudaSetDevice(c->device);
   if (c->compute) cudaStreamSynchronize(c->compute);
   if (c->upload) cudaStreamSynchronize(c->upload);
-  if (c->fgraph_exec) cudaGraphExecDestroy(c->fgraph_exec);
-  if (c->fgraph) cudaGraphDestroy(c->fgraph);
+  if (c->fr.fgraph_exec) cudaGraphExecDestroy(c->fr.fgraph_exec);
+  if (c->fr.fgraph) cudaGraphDestroy(c->fr.fgraph);
   for (auto& L : c->lanes)  // lanes read the arenas: drain them before freeing
     if (L.stream) cudaStreamSynchronize(L.stream);
   for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword,
@@ -653,8 +694,8 @@ void vxe_destroy(vxe_ctx* c) {
       if (e) cudaEventDestroy(e);
     if (L.stream) cudaStreamDestroy(L.stream);
   }
-  for (auto& b : c->img) release(b);
-  for (auto& e : c->ev)
+  for (auto& b : c->fr.img) release(b);
+  for (auto& e : c->fr.ev)
     if (e) cudaEventDestroy(e);
   if (c->gt.built) cudaEventDestroy(c->gt.built);
   for (auto& e : c->gt.reader)
@@ -674,13 +715,13 @@ vxe_status vxe_set_flags(vxe_ctx* c, uint32_t flags) {
   const uint32_t img_bits = VXE_FLAG_DEBUG_INTERMEDIATES | VXE_FLAG_HIT_RECORDS;
   const bool realloc = ((flags ^ c->flags) & img_bits) != 0;
   c->flags = flags;
-  if (realloc && c->iw != 0) {
+  if (realloc && c->fr.iw != 0) {
     cudaSetDevice(c->device);
     // Only (de)allocate the optional images; histories are kept.
     for (int i : {IMG_LOCAL, IMG_PRE_TAA, IMG_HITS}) {
-      const size_t b = img_enabled(c, i) ? img_bytes(c, i) : 0;
-      if (b != c->img[i].bytes) {
-        vxe_status st = alloc(c, c->img[i], b);
+      const size_t b = img_enabled(c, i) ? img_bytes(c->fr, i) : 0;
+      if (b != c->fr.img[i].bytes) {
+        vxe_status st = alloc(c, c->fr.img[i], b);
         if (st != VXE_OK) return st;
       }
     }
@@ -693,20 +734,14 @@ vxe_status vxe_resize(vxe_ctx* c, uint32_t present_w, uint32_t present_h, float 
     return fail(c, VXE_ERR_INVALID_ARG, "bad resize arguments");
   cudaSetDevice(c->device);
   CK(cudaStreamSynchronize(c->compute));
-  // internal = round(present * scale).max(1) (render/state/mod.rs:239-241)
-  const float fw = (float)present_w * render_scale, fh = (float)present_h * render_scale;
-  // f32::round rounds half away from zero, like std::round.
-  c->iw = (uint32_t)std::max(1.0f, std::round(fw));
-  c->ih = (uint32_t)std::max(1.0f, std::round(fh));
-  c->pw = present_w;
-  c->ph = present_h;
-  return alloc_images(c);
+  set_dims(c->fr, present_w, present_h, render_scale);
+  return alloc_images(c, c->fr);
 }
 
 vxe_status vxe_get_internal_dims(const vxe_ctx* c, uint32_t* w, uint32_t* h) {
   if (!c || !w || !h) return VXE_ERR_INVALID_ARG;
-  *w = c->iw;
-  *h = c->ih;
+  *w = c->fr.iw;
+  *h = c->fr.ih;
   return VXE_OK;
 }
 
@@ -828,7 +863,7 @@ vxe_status vxe_render_frame(vxe_ctx* c, vxe_frame_out* out) {
 vxe_status vxe_render_frame_graph(vxe_ctx* c, vxe_frame_out* out) {
   if (!c) return VXE_ERR_INVALID_ARG;
   cudaSetDevice(c->device);
-  vxe_status st = launch_frame_graph(c);
+  vxe_status st = launch_frame_graph(c, c->fr, c->cam, c->compute, 0);
   if (st != VXE_OK) return st;
   frame_out(c, out);
   CK(cudaStreamSynchronize(c->compute));
@@ -849,14 +884,14 @@ vxe_status vxe_synchronize(vxe_ctx* c) {
 vxe_status vxe_get_timings(vxe_ctx* c, vxe_timings* t) {
   if (!c || !t) return VXE_ERR_INVALID_ARG;
   std::memset(t, 0, sizeof *t);
-  if (!c->timed) return VXE_OK;
+  if (!c->fr.timed) return VXE_OK;
   cudaSetDevice(c->device);
-  CK(cudaEventSynchronize(c->ev[6]));
+  CK(cudaEventSynchronize(c->fr.ev[6]));
   float ms[6];
-  for (int i = 0; i < 6; ++i) CK(cudaEventElapsedTime(&ms[i], c->ev[i], c->ev[i + 1]));
+  for (int i = 0; i < 6; ++i) CK(cudaEventElapsedTime(&ms[i], c->fr.ev[i], c->fr.ev[i + 1]));
   t->grass_cells = ms[0];
   t->tiles = (double)ms[0] + ms[1];
-  t->primary_trace = c->timed_trace ? ms[2] : 0.0;
+  t->primary_trace = c->fr.timed_trace ? ms[2] : 0.0;
   t->primary = (double)ms[2] + ms[3];
   t->godray = ms[4];
   t->composite = ms[5];
@@ -866,31 +901,32 @@ vxe_status vxe_get_timings(vxe_ctx* c, vxe_timings* t) {
 
 vxe_status vxe_image_size(const vxe_ctx* c, vxe_image im, size_t* bytes) {
   if (!c || !bytes) return VXE_ERR_INVALID_ARG;
-  const int i = map_image(c, im);
+  const int i = map_image(c->fr, im);
   if (i < 0) return VXE_ERR_INVALID_ARG;
-  *bytes = c->img[i].bytes;
+  *bytes = c->fr.img[i].bytes;
   return VXE_OK;
 }
 
 vxe_status vxe_read_image(vxe_ctx* c, vxe_image im, void* host, size_t bytes) {
   if (!c || !host) return VXE_ERR_INVALID_ARG;
-  const int i = map_image(c, im);
-  if (i < 0 || !c->img[i].p) return fail(c, VXE_ERR_INVALID_ARG, "image %d not available", (int)im);
-  if (bytes != c->img[i].bytes) return fail(c, VXE_ERR_INVALID_ARG, "image %d is %zu bytes, got %zu", (int)im, c->img[i].bytes, bytes);
+  const int i = map_image(c->fr, im);
+  if (i < 0 || !c->fr.img[i].p) return fail(c, VXE_ERR_INVALID_ARG, "image %d not available", (int)im);
+  if (bytes != c->fr.img[i].bytes) return fail(c, VXE_ERR_INVALID_ARG, "image %d is %zu bytes, got %zu", (int)im, c->fr.img[i].bytes, bytes);
   cudaSetDevice(c->device);
   CK(cudaStreamSynchronize(c->compute));
-  CK(cudaMemcpy(host, c->img[i].p, bytes, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(host, c->fr.img[i].p, bytes, cudaMemcpyDeviceToHost));
   return VXE_OK;
 }
 
 vxe_status vxe_write_image(vxe_ctx* c, vxe_image im, const void* host, size_t bytes) {
   if (!c || !host) return VXE_ERR_INVALID_ARG;
-  const int i = map_image(c, im);
-  if (i < 0 || !c->img[i].p) return fail(c, VXE_ERR_INVALID_ARG, "image %d not available", (int)im);
-  if (bytes != c->img[i].bytes) return fail(c, VXE_ERR_INVALID_ARG, "image %d is %zu bytes, got %zu", (int)im, c->img[i].bytes, bytes);
+  const int i = map_image(c->fr, im);
+  if (i < 0 || !c->fr.img[i].p) return fail(c, VXE_ERR_INVALID_ARG, "image %d not available", (int)im);
+  if (bytes != c->fr.img[i].bytes) return fail(c, VXE_ERR_INVALID_ARG, "image %d is %zu bytes, got %zu", (int)im, c->fr.img[i].bytes, bytes);
   cudaSetDevice(c->device);
   CK(cudaStreamSynchronize(c->compute));
-  CK(cudaMemcpy(c->img[i].p, host, bytes, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->fr.img[i].p, host, bytes, cudaMemcpyHostToDevice));
+  CK(cudaStreamSynchronize(cudaStreamLegacy));  // a pageable copy may still be landing
   return VXE_OK;
 }
 
@@ -899,7 +935,7 @@ vxe_status vxe_read_error_word(vxe_ctx* c, uint32_t* word) {
   cudaSetDevice(c->device);
   CK(cudaStreamSynchronize(c->compute));
   CK(cudaMemcpy(word, c->errword.p, 4, cudaMemcpyDeviceToHost));
-  CK(cudaMemset(c->errword.p, 0, 4));
+  CK(fill_sync(c->errword.p, 0, 4));
   return VXE_OK;
 }
 
@@ -1322,6 +1358,101 @@ vxe_status vxe_submit_batch(vxe_ctx* c, const vxe_request* reqs, uint32_t n, con
   return vxe_batch_wait(c, 0, 1, stats);
 }
 
+
+// ---------------------------------------------------------------------------
+// Viewport sessions
+// ---------------------------------------------------------------------------
+vxe_status lane_ready(vxe_ctx* c, uint32_t lane) {
+  if (lane >= VXE_BATCH_LANES) return fail(c, VXE_ERR_INVALID_ARG, "lane %u >= %u", lane, VXE_BATCH_LANES);
+  return lane_resources(c, c->lanes[lane], 0u, 0u, 0u);
+}
+
+uint64_t vxe_view_bytes(const vxe_ctx* c, uint32_t present_w, uint32_t present_h, float render_scale) {
+  if (!c || present_w == 0 || present_h == 0 || !(render_scale > 0.0f)) return 0;
+  FrameState F;
+  set_dims(F, present_w, present_h, render_scale);
+  uint64_t total = 0;
+  for (int i = 0; i < IMG_N; ++i)
+    if (img_enabled(c, i)) total += img_bytes(F, i);
+  return total;
+}
+
+vxe_status vxe_view_create(vxe_ctx* c, uint32_t present_w, uint32_t present_h, float render_scale, vxe_view** out) {
+  if (!c || !out || present_w == 0 || present_h == 0 || !(render_scale > 0.0f) || render_scale > 4.0f)
+    return fail(c, VXE_ERR_INVALID_ARG, "bad view arguments");
+  *out = nullptr;
+  cudaSetDevice(c->device);
+  auto* v = new (std::nothrow) vxe_view();
+  if (!v) return fail(c, VXE_ERR_OOM, "view");
+  set_dims(v->fr, present_w, present_h, render_scale);
+  if (cudaEventCreateWithFlags(&v->done, cudaEventDisableTiming) != cudaSuccess) {
+    delete v;
+    return fail(c, VXE_ERR_DEVICE, "view event");
+  }
+  vxe_status st = alloc_images(c, v->fr);
+  if (st != VXE_OK) {
+    release_frame_state(v->fr);
+    cudaEventDestroy(v->done);
+    delete v;
+    return st;
+  }
+  *out = v;
+  return VXE_OK;
+}
+
+vxe_status vxe_view_render_async(vxe_ctx* c, vxe_view* v, uint32_t lane, const vxe_camera_gpu* cam) {
+  if (!c || !v || !cam) return fail(c, VXE_ERR_INVALID_ARG, "null view arguments");
+  cudaSetDevice(c->device);
+  vxe_status st = lane_ready(c, lane);
+  if (st != VXE_OK) return st;
+  BatchLane& L = c->lanes[lane];
+  // a view's frames run in order: follow its previous frame's lane
+  if (v->last_stream && v->last_stream != L.stream) {
+    CK(cudaEventRecord(v->done, v->last_stream));
+    CK(cudaStreamWaitEvent(L.stream, v->done, 0));
+  }
+  vxe_camera_gpu vc = *cam;
+  vc.chunk_size = c->cam.chunk_size;
+  vc.chunk_count = c->cam.chunk_count;
+  for (int k = 0; k < 4; ++k) {
+    vc.grid_origin_chunk[k] = c->cam.grid_origin_chunk[k];
+    vc.grid_dims[k] = c->cam.grid_dims[k];
+  }
+  if (!L.busy) CK(cudaEventRecord(L.ev[0], L.stream));
+  if ((st = launch_frame_graph(c, v->fr, vc, L.stream, 1 + (int)lane)) != VXE_OK) return st;
+  CK(cudaEventRecord(L.ev[1], L.stream));
+  if (!L.busy) {
+    L.rays = 0;
+    L.items = 0;
+    L.tiles = 0;
+  }
+  L.busy = true;
+  L.rays += (uint64_t)v->fr.iw * v->fr.ih;
+  v->last_stream = L.stream;
+  return VXE_OK;
+}
+
+vxe_status vxe_view_read_image(vxe_ctx* c, vxe_view* v, int image, void* host, size_t bytes) {
+  if (!c || !v || !host) return fail(c, VXE_ERR_INVALID_ARG, "null view arguments");
+  const int i = map_image(v->fr, (vxe_image)image);
+  if (i < 0 || !v->fr.img[i].p) return fail(c, VXE_ERR_INVALID_ARG, "image %d not available", image);
+  if (bytes != v->fr.img[i].bytes)
+    return fail(c, VXE_ERR_INVALID_ARG, "image %d is %zu bytes, got %zu", image, v->fr.img[i].bytes, bytes);
+  cudaSetDevice(c->device);
+  if (v->last_stream) CK(cudaStreamSynchronize(v->last_stream));
+  CK(cudaMemcpy(host, v->fr.img[i].p, bytes, cudaMemcpyDeviceToHost));
+  return VXE_OK;
+}
+
+vxe_status vxe_view_destroy(vxe_ctx* c, vxe_view* v) {
+  if (!c || !v) return VXE_ERR_INVALID_ARG;
+  cudaSetDevice(c->device);
+  if (v->last_stream) cudaStreamSynchronize(v->last_stream);
+  release_frame_state(v->fr);
+  if (v->done) cudaEventDestroy(v->done);
+  delete v;
+  return VXE_OK;
+}
 
 }  // extern "C"
 

@@ -181,6 +181,13 @@ class Renderer:
         self._check(rc, "vxe_batch_wait")
         return st
 
+    # -- viewport sessions --------------------------------------------------------
+    def view_bytes(self, width: int, height: int, render_scale: float) -> int:
+        return int(self._lib.vxe_view_bytes(self._ctx, width, height, render_scale))
+
+    def view(self, width: int, height: int, render_scale: float) -> "View":
+        return View(self, width, height, render_scale)
+
     # -- queries ----------------------------------------------------------------
     def trace_rays(self, origins: np.ndarray, dirs: np.ndarray, tmax: float) -> np.ndarray:
         o = np.ascontiguousarray(origins, dtype=np.float32).reshape(-1, 3)
@@ -191,3 +198,36 @@ class Renderer:
         self._check(self._lib.vxe_trace_rays(self._ctx, o.ctypes.data_as(fp), d.ctypes.data_as(fp), len(o),
                                              float(tmax), out.ctypes.data), "vxe_trace_rays")
         return out
+
+
+class View:
+    """A viewport session: its own images and histories, rendered from the
+    renderer's world on a batch lane (vxe_view_*)."""
+
+    def __init__(self, renderer: Renderer, width: int, height: int, render_scale: float):
+        self._r = renderer
+        self.present = (width, height)
+        # round(present * scale), halves away from zero, in binary32 (as vxe_resize)
+        self.internal = tuple(max(1, int(np.floor(np.float32(v) * np.float32(render_scale) + np.float32(0.5))))
+                              for v in (width, height))
+        h = C.c_void_p()
+        renderer._check(renderer._lib.vxe_view_create(renderer._ctx, width, height, render_scale, C.byref(h)),
+                        "vxe_view_create")
+        self._h = h
+
+    def render_async(self, lane: int, cam: A.CameraGpu) -> None:
+        self._r._check(self._r._lib.vxe_view_render_async(self._r._ctx, self._h, lane, C.byref(cam)),
+                       "vxe_view_render_async")
+
+    def read_image(self, img: int) -> np.ndarray:
+        which, ch, dt = Renderer._IMG_SHAPES[img]
+        w, h = self.internal if which == "i" else self.present
+        arr = np.zeros((h, w, ch) if ch > 1 else (h, w), dtype=dt)
+        self._r._check(self._r._lib.vxe_view_read_image(self._r._ctx, self._h, img, arr.ctypes.data, arr.nbytes),
+                       "vxe_view_read_image")
+        return arr
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._r._ctx:
+            self._r._lib.vxe_view_destroy(self._r._ctx, self._h)
+        self._h = None
