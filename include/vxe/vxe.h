@@ -306,22 +306,35 @@ vxe_status vxe_batch_wait(vxe_ctx* ctx, uint32_t lane, int block, vxe_batch_stat
 /* Viewport sessions (serving; no counterpart in the reference, whose
  * Renderer owns exactly one frame pipeline).  A view owns what one client's
  * frames carry from frame to frame -- internal and present images, the
- * primary-hit, shadow, local-light, godray and output histories, their
- * ping-pong state and a captured frame graph -- and renders from the
- * context's world (arenas, grid, clipmap, grass table).  Its frames are
+ * primary-hit, shadow, local-light, godray and output histories and their
+ * ping-pong state -- and renders from the context's world (arenas, grid,
+ * clipmap, grass table).  A frame's working buffers (tile lists, shading
+ * queues, grass probe and slab records) belong to the lane it renders on,
+ * sized for the largest view that lane has rendered.  Its frames are
  * exactly the frames vxe_render_frame renders from the same camera sequence
  * after vxe_resize (render/state/mod.rs:297-308, 329-446).
- *   vxe_view_bytes          device bytes a view of that size holds (admission)
+ *   vxe_view_bytes          device bytes a view of that size holds (admission;
+ *                           the lane's working buffers are not included)
+ *   vxe_view_lane_bytes     device bytes of a lane's working buffers for
+ *                           views up to that size
  *   vxe_view_create         allocates it (histories start at zero)
  *   vxe_view_render_async   one frame on a batch lane's stream; it may follow
  *                           a batch on the same lane, and vxe_batch_wait then
- *                           waits for both.  The camera's world fields
+ *                           waits for both.  A view larger than any before on
+ *                           that lane first waits for the lane and grows its
+ *                           working buffers.  The camera's world fields
  *                           (chunk size and count, grid origin and dims) are
  *                           taken from the context's camera.
  *   vxe_view_read_image     waits for the view's last frame, copies an image
- *   vxe_view_destroy        waits for the view's last frame, frees it. */
+ *   vxe_view_destroy        frees it after its last frame (stream-ordered;
+ *                           does not wait)
+ * A view's images and a lane's buffers come from a stream-ordered pool of
+ * the context: creating, growing and freeing them never waits for the
+ * device.  A view rendered after vxe_set_flags changed the image flags
+ * (VXE_FLAG_DEBUG_INTERMEDIATES, VXE_FLAG_HIT_RECORDS) is refused. */
 typedef struct vxe_view vxe_view;
 uint64_t vxe_view_bytes(const vxe_ctx* ctx, uint32_t present_w, uint32_t present_h, float render_scale);
+uint64_t vxe_view_lane_bytes(const vxe_ctx* ctx, uint32_t present_w, uint32_t present_h, float render_scale);
 vxe_status vxe_view_create(vxe_ctx* ctx, uint32_t present_w, uint32_t present_h, float render_scale,
                            vxe_view** out);
 vxe_status vxe_view_render_async(vxe_ctx* ctx, vxe_view* view, uint32_t lane, const vxe_camera_gpu* camera);

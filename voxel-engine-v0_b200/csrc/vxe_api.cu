@@ -36,6 +36,7 @@ namespace {
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  bool pooled = false;  // from the context's stream-ordered pool
 };
 
 enum Img {
@@ -67,6 +68,22 @@ struct GrassTable {
   bool reader_used[kGrassReaders] = {};
 };
 
+// One frame pipeline's images, ping-pong state, timing events and captured
+// graph: the context's own frame, and one per viewport session (vxe_view).
+struct FrameState {
+  DevBuf img[IMG_N];
+  uint32_t iw = 0, ih = 0, pw = 0, ph = 0;
+  int ping = 0;
+  // frame events: start, grass table, tiles, trace, shading, godray, composite
+  cudaEvent_t ev[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool timed = false, timed_trace = false;
+  // the frame as a captured CUDA graph
+  cudaGraph_t fgraph = nullptr;
+  cudaGraphExec_t fgraph_exec = nullptr;
+  std::vector<cudaGraphNode_t> fgraph_nodes;
+  uint64_t fgraph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+};
+
 struct BatchLane {
   cudaStream_t stream = nullptr;
   DevBuf hdr, reqs, cams, tile_count, tile_slots, head;
@@ -86,22 +103,9 @@ struct BatchLane {
   bool busy = false;
   uint64_t rays = 0;
   uint32_t items = 0, tiles = 0;
-};
-
-// One frame pipeline's images, ping-pong state, timing events and captured
-// graph: the context's own frame, and one per viewport session (vxe_view).
-struct FrameState {
-  DevBuf img[IMG_N];
-  uint32_t iw = 0, ih = 0, pw = 0, ph = 0;
-  int ping = 0;
-  // frame events: start, grass table, tiles, trace, shading, godray, composite
-  cudaEvent_t ev[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-  bool timed = false, timed_trace = false;
-  // the frame as a captured CUDA graph
-  cudaGraph_t fgraph = nullptr;
-  cudaGraphExec_t fgraph_exec = nullptr;
-  std::vector<cudaGraphNode_t> fgraph_nodes;
-  uint64_t fgraph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  // per-frame working buffers (tile lists, queues, probe and slab records)
+  // of the viewport sessions rendered on this lane, sized for the largest
+  FrameState scratch;
 };
 
 }  // namespace
@@ -128,6 +132,22 @@ struct vxe_ctx {
   int b_trace_grid = 0, b_tile_grid = 0;
   int shade_wave = 148 * 16;  // blocks of the grid-stride shading kernels
   bool upload_recorded = false;
+  // Stream-ordered pool for lane and view buffers: growing or freeing them
+  // never waits for the device (cudaFree would wait for every stream).
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t aux = nullptr;  // zero-fills new views' images
+  // Pinned staging for world writes: blocks filled in turn; a block is
+  // refilled only after the copies queued from it have run.
+  struct StageBlock {
+    char* p = nullptr;
+    cudaEvent_t ev = nullptr;
+    bool rec = false;
+  };
+  std::vector<StageBlock> ring;
+  size_t ring_off = 0;
+  size_t ring_cur = 0;
+  // where the compute stream and each lane stood at the last world write
+  cudaEvent_t rd_ev[1 + VXE_BATCH_LANES] = {};
 };
 
 struct vxe_view {
@@ -174,6 +194,7 @@ vxe_status alloc(vxe_ctx* c, DevBuf& b, size_t bytes) {
     b.p = nullptr;
     b.bytes = 0;
   }
+  b.pooled = false;
   if (bytes == 0) return VXE_OK;
   CK(cudaMalloc(&b.p, bytes));
   b.bytes = bytes;
@@ -181,10 +202,28 @@ vxe_status alloc(vxe_ctx* c, DevBuf& b, size_t bytes) {
   return VXE_OK;
 }
 
-void release(DevBuf& b) {
-  if (b.p) cudaFree(b.p);
+// Releases a buffer; a pooled one after the work queued on `st` so far.
+void release(DevBuf& b, cudaStream_t st = nullptr) {
+  if (b.p) {
+    if (b.pooled)
+      cudaFreeAsync(b.p, st ? st : cudaStreamLegacy);
+    else
+      cudaFree(b.p);
+  }
   b.p = nullptr;
   b.bytes = 0;
+  b.pooled = false;
+}
+
+// Stream-ordered (re)allocation from the context's pool, zero-filled on `st`.
+vxe_status alloc_on(vxe_ctx* c, DevBuf& b, size_t bytes, cudaStream_t st) {
+  release(b, st);
+  if (bytes == 0) return VXE_OK;
+  CK(cudaMallocFromPoolAsync(&b.p, bytes, c->pool, st));
+  b.bytes = bytes;
+  b.pooled = true;
+  CK(cudaMemsetAsync(b.p, 0, bytes, st));
+  return VXE_OK;
 }
 
 // Stored grass column probes per internal pixel (the walk meets about four
@@ -241,14 +280,31 @@ bool img_enabled(const vxe_ctx* c, int i) {
   return true;
 }
 
-vxe_status alloc_images(vxe_ctx* c, FrameState& F) {
+// Per-frame working buffers of the wavefront (tile lists, queues, probe and
+// slab records): a frame's contents only, nothing carried to the next frame.
+// A view borrows them from the lane it renders on; the rest of a frame state
+// (outputs and histories) is its own.
+bool img_is_scratch(int i) {
+  return i == IMG_TILE_COUNT || i == IMG_TILE_SLOTS || i >= IMG_PIXHIT;
+}
+
+enum ImgSet { IMG_SET_ALL, IMG_SET_OWN, IMG_SET_SCRATCH };
+
+bool img_in_set(int i, ImgSet set) {
+  return set == IMG_SET_ALL || (set == IMG_SET_SCRATCH) == img_is_scratch(i);
+}
+
+// Allocates and zero-fills a frame state's images: synchronously, or with
+// `st`, stream-ordered from the pool.
+vxe_status alloc_images(vxe_ctx* c, FrameState& F, ImgSet set = IMG_SET_ALL, cudaStream_t st = nullptr) {
   for (int i = 0; i < IMG_N; ++i) {
-    const size_t b = img_enabled(c, i) ? img_bytes(F, i) : 0;
+    const size_t b = img_enabled(c, i) && img_in_set(i, set) ? img_bytes(F, i) : 0;
     if (b != F.img[i].bytes || (b != 0) != (F.img[i].p != nullptr)) {
-      vxe_status st = alloc(c, F.img[i], b);
-      if (st != VXE_OK) return st;
+      vxe_status rc = st ? alloc_on(c, F.img[i], b, st) : alloc(c, F.img[i], b);
+      if (rc != VXE_OK) return rc;
     } else if (F.img[i].p) {
-      if (fill_sync(F.img[i].p, 0, b) != cudaSuccess) return fail(c, VXE_ERR_DEVICE, "memset failed");
+      if ((st ? cudaMemsetAsync(F.img[i].p, 0, b, st) : fill_sync(F.img[i].p, 0, b)) != cudaSuccess)
+        return fail(c, VXE_ERR_DEVICE, "memset failed");
     }
   }
   F.ping = 0;
@@ -408,7 +464,9 @@ vxe_status frame_validate(vxe_ctx* c, const FrameState& F, const vxe_camera_gpu&
   return VXE_OK;
 }
 
-void frame_fill(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& cam, FrameArgs& A) {
+// `S` holds the per-frame working buffers (F itself, or a lane's for a view).
+void frame_fill(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& cam, FrameArgs& A, const FrameState* S = nullptr) {
+  if (!S) S = &F;
   fill_scene_args(c, A);
   A.cam = cam;
   const int p = F.ping, q = 1 - F.ping;
@@ -416,8 +474,8 @@ void frame_fill(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& cam, FrameArgs&
   A.ih = F.ih;
   A.pw = F.pw;
   A.ph = F.ph;
-  A.tile_count = (uint32_t*)F.img[IMG_TILE_COUNT].p;
-  A.tile_slots = (uint32_t*)F.img[IMG_TILE_SLOTS].p;
+  A.tile_count = (uint32_t*)S->img[IMG_TILE_COUNT].p;
+  A.tile_slots = (uint32_t*)S->img[IMG_TILE_SLOTS].p;
   A.hist_in = (const uint4*)F.img[IMG_HIST0 + p].p;
   A.hist_out = (uint4*)F.img[IMG_HIST0 + q].p;
   A.shadow_in = (const float*)F.img[IMG_SHADOW0 + p].p;
@@ -434,25 +492,25 @@ void frame_fill(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& cam, FrameArgs&
   A.out_hist_in = (const float4*)F.img[IMG_OHIST0 + p].p;
   A.out_hist_out = (float4*)F.img[IMG_OHIST0 + q].p;
   A.hits = (uint4*)F.img[IMG_HITS].p;
-  A.pix_hit = (uint4*)F.img[IMG_PIXHIT].p;
-  A.q_vox = (uint32_t*)F.img[IMG_QVOX].p;
-  A.q_far = (uint32_t*)F.img[IMG_QFAR].p;
-  A.q_count = (uint32_t*)F.img[IMG_QCOUNT].p;
-  A.q_shadow = (uint32_t*)F.img[IMG_QSHADOW].p;
-  A.q_light = (uint32_t*)F.img[IMG_QLIGHT].p;
-  A.px_shadow = (float*)F.img[IMG_PXSHADOW].p;
-  A.px_light = (float4*)F.img[IMG_PXLIGHT].p;
-  A.probe_recs = (vxe::dev::ProbeRec*)F.img[IMG_PROBE_RECS].p;
-  A.probe_cap = (uint32_t)std::min<size_t>(F.img[IMG_PROBE_RECS].bytes / sizeof(vxe::dev::ProbeRec), 0xFFFFFFFFu);
-  A.slab_tasks = (uint4*)F.img[IMG_SLAB_TASKS].p;
-  A.slab_res = (float4*)F.img[IMG_SLAB_RES].p;
-  A.slab_cap = (uint32_t)std::min<size_t>(F.img[IMG_SLAB_TASKS].bytes / 32u, 0xFFFFFFFFu);
-  A.px_first = (unsigned long long*)F.img[IMG_PXFIRST].p;
-  A.px_probe = (uint2*)F.img[IMG_PXPROBE].p;
-  A.slab_hits = (uint32_t*)F.img[IMG_SLAB_HITS].p;
-  A.px_task = (uint32_t*)F.img[IMG_PXTASK].p;
-  A.px_mask = (uint2*)F.img[IMG_PXMASK].p;
-  A.q_pending = (uint32_t*)F.img[IMG_QPENDING].p;
+  A.pix_hit = (uint4*)S->img[IMG_PIXHIT].p;
+  A.q_vox = (uint32_t*)S->img[IMG_QVOX].p;
+  A.q_far = (uint32_t*)S->img[IMG_QFAR].p;
+  A.q_count = (uint32_t*)S->img[IMG_QCOUNT].p;
+  A.q_shadow = (uint32_t*)S->img[IMG_QSHADOW].p;
+  A.q_light = (uint32_t*)S->img[IMG_QLIGHT].p;
+  A.px_shadow = (float*)S->img[IMG_PXSHADOW].p;
+  A.px_light = (float4*)S->img[IMG_PXLIGHT].p;
+  A.probe_recs = (vxe::dev::ProbeRec*)S->img[IMG_PROBE_RECS].p;
+  A.probe_cap = (uint32_t)std::min<size_t>(S->img[IMG_PROBE_RECS].bytes / sizeof(vxe::dev::ProbeRec), 0xFFFFFFFFu);
+  A.slab_tasks = (uint4*)S->img[IMG_SLAB_TASKS].p;
+  A.slab_res = (float4*)S->img[IMG_SLAB_RES].p;
+  A.slab_cap = (uint32_t)std::min<size_t>(S->img[IMG_SLAB_TASKS].bytes / 32u, 0xFFFFFFFFu);
+  A.px_first = (unsigned long long*)S->img[IMG_PXFIRST].p;
+  A.px_probe = (uint2*)S->img[IMG_PXPROBE].p;
+  A.slab_hits = (uint32_t*)S->img[IMG_SLAB_HITS].p;
+  A.px_task = (uint32_t*)S->img[IMG_PXTASK].p;
+  A.px_mask = (uint2*)S->img[IMG_PXMASK].p;
+  A.q_pending = (uint32_t*)S->img[IMG_QPENDING].p;
 }
 
 // The frame's launches on the compute stream (captured as-is by the graph
@@ -592,13 +650,13 @@ void set_dims(FrameState& F, uint32_t present_w, uint32_t present_h, float rende
   F.ph = present_h;
 }
 
-void release_frame_state(FrameState& F) {
+void release_frame_state(FrameState& F, cudaStream_t st = nullptr) {
   if (F.fgraph_exec) cudaGraphExecDestroy(F.fgraph_exec);
   if (F.fgraph) cudaGraphDestroy(F.fgraph);
   F.fgraph_exec = nullptr;
   F.fgraph = nullptr;
   F.fgraph_nodes.clear();
-  for (auto& b : F.img) release(b);
+  for (auto& b : F.img) release(b, st);
 }
 
 void frame_out(vxe_ctx* c, vxe_frame_out* out) {
@@ -642,6 +700,18 @@ vxe_status vxe_create(const vxe_config* cfg, vxe_ctx** out) {
     return bail(VXE_ERR_DEVICE);
   for (auto& e : c->fr.ev)
     if (cudaEventCreate(&e) != cudaSuccess) return bail(VXE_ERR_DEVICE);
+  {
+    cudaMemPoolProps pp{};
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.handleTypes = cudaMemHandleTypeNone;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = c->device;
+    if (cudaMemPoolCreate(&c->pool, &pp) != cudaSuccess) return bail(VXE_ERR_DEVICE);
+    // keep freed blocks for the next view or lane growth
+    uint64_t keep = ~0ull;
+    if (cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess)
+      return bail(VXE_ERR_DEVICE);
+  }
   const uint64_t nc = cfg->node_capacity, cc = cfg->chunk_capacity;
   if ((st = alloc(c, c->nodes, nc * 16)) != VXE_OK) return bail(st);
   if ((st = alloc(c, c->ropes, nc * 32)) != VXE_OK) return bail(st);
@@ -687,12 +757,26 @@ void vxe_destroy(vxe_ctx* c) {
     for (auto* b : {&L.hdr, &L.reqs, &L.cams, &L.tile_count, &L.tile_slots, &L.head, &L.probe_recs, &L.slab_tasks,
                     &L.slab_res, &L.slab_hits, &L.px_first, &L.px_task, &L.px_mask, &L.px_probe, &L.px_hit,
                     &L.q_pending, &L.q_refine, &L.q_far, &L.dcount, &L.q_keys, &L.q_perm, &L.bin_count})
-      release(*b);
+      release(*b, L.stream);
+    release_frame_state(L.scratch, L.stream);
+    if (L.stream) cudaStreamSynchronize(L.stream);
     if (L.graph) cudaGraphExecDestroy(L.graph);
     if (L.stage) cudaFreeHost(L.stage);
     for (auto& e : L.ev)
       if (e) cudaEventDestroy(e);
     if (L.stream) cudaStreamDestroy(L.stream);
+  }
+  if (c->aux) {
+    cudaStreamSynchronize(c->aux);
+    cudaStreamDestroy(c->aux);
+  }
+  if (c->pool) cudaMemPoolDestroy(c->pool);
+  for (auto& e : c->rd_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->upload) cudaStreamSynchronize(c->upload);
+  for (auto& b : c->ring) {
+    cudaFreeHost(b.p);
+    if (b.ev) cudaEventDestroy(b.ev);
   }
   for (auto& b : c->fr.img) release(b);
   for (auto& e : c->fr.ev)
@@ -745,10 +829,95 @@ vxe_status vxe_get_internal_dims(const vxe_ctx* c, uint32_t* w, uint32_t* h) {
   return VXE_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+constexpr size_t kStageBlock = (size_t)16 << 20;
+constexpr size_t kStageBlocksMax = 16;  // 256 MB of pinned staging at most
+
+vxe_status stage_block_add(vxe_ctx* c) {
+  vxe_ctx::StageBlock b;
+  CK(cudaMallocHost((void**)&b.p, kStageBlock));
+  if (cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming) != cudaSuccess) {
+    cudaFreeHost(b.p);
+    return fail(c, VXE_ERR_DEVICE, "staging event");
+  }
+  c->ring.push_back(b);
+  return VXE_OK;
+}
+
+// Queues a host-to-device copy on the upload stream through the pinned
+// staging blocks: the host returns once the bytes are in pinned memory (a
+// pageable cudaMemcpyAsync would hold the host until the copy has run).
+// World writes wait for the passes in flight, so with a deep queue the next
+// block may still be in use: another block is added rather than waiting,
+// up to the cap.
+vxe_status ring_copy(vxe_ctx* c, void* dst, const void* src, size_t bytes) {
+  vxe_status rs;
+  if (c->ring.empty() && (rs = stage_block_add(c)) != VXE_OK) return rs;
+  char* d = (char*)dst;
+  const char* h = (const char*)src;
+  while (bytes) {
+    if (c->ring_off >= kStageBlock) {  // this block is full: move to a free one
+      vxe_ctx::StageBlock& cur = c->ring[c->ring_cur];
+      CK(cudaEventRecord(cur.ev, c->upload));
+      cur.rec = true;
+      const size_t next = (c->ring_cur + 1) % c->ring.size();
+      vxe_ctx::StageBlock& nb = c->ring[next];
+      const cudaError_t q = nb.rec ? cudaEventQuery(nb.ev) : cudaSuccess;
+      if (q != cudaSuccess && q != cudaErrorNotReady) return fail(c, VXE_ERR_DEVICE, "staging event query");
+      if (q == cudaErrorNotReady && c->ring.size() < kStageBlocksMax) {
+        if ((rs = stage_block_add(c)) != VXE_OK) return rs;
+        // the new block goes after the current one, so blocks stay in fill order
+        std::rotate(c->ring.begin() + c->ring_cur + 1, c->ring.end() - 1, c->ring.end());
+        c->ring_cur = c->ring_cur + 1;
+      } else {
+        if (q == cudaErrorNotReady) CK(cudaEventSynchronize(nb.ev));
+        c->ring_cur = next;
+      }
+      c->ring_off = 0;
+    }
+    const size_t n = std::min(bytes, kStageBlock - c->ring_off);
+    char* stage = c->ring[c->ring_cur].p + c->ring_off;
+    std::memcpy(stage, h, n);
+    CK(cudaMemcpyAsync(d, stage, n, cudaMemcpyHostToDevice, c->upload));
+    c->ring_off = (c->ring_off + n + 15) & ~(size_t)15;
+    d += n;
+    h += n;
+    bytes -= n;
+  }
+  return VXE_OK;
+}
+
+// World writes (chunk data, metas, grid, clipmap texels) are ordered after
+// every pass already enqueued on the compute stream and the lanes, and before
+// every pass enqueued later (which waits for upload_done): a frame in flight
+// reads the world as it was when the frame was enqueued, like a queue write
+// between two submissions in the reference.  Nothing here waits on the host.
+vxe_status upload_after_readers(vxe_ctx* c) {
+  cudaStream_t streams[1 + VXE_BATCH_LANES];
+  streams[0] = c->compute;
+  for (int l = 0; l < VXE_BATCH_LANES; ++l) streams[1 + l] = c->lanes[l].stream;
+  for (int k = 0; k < 1 + VXE_BATCH_LANES; ++k) {
+    if (!streams[k]) continue;
+    if (!c->rd_ev[k]) CK(cudaEventCreateWithFlags(&c->rd_ev[k], cudaEventDisableTiming));
+    CK(cudaEventRecord(c->rd_ev[k], streams[k]));
+    CK(cudaStreamWaitEvent(c->upload, c->rd_ev[k], 0));
+  }
+  return VXE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 vxe_status vxe_upload_chunks(vxe_ctx* c, const vxe_chunk_upload* ups, uint32_t n) {
   if (!c || (n && !ups)) return fail(c, VXE_ERR_INVALID_ARG, "null uploads");
   cudaSetDevice(c->device);
   const bool silent = (c->flags & VXE_FLAG_SILENT_CAPACITY_SKIP) != 0;
+  vxe_status ws = upload_after_readers(c);
+  if (ws != VXE_OK) return ws;
   for (uint32_t i = 0; i < n; ++i) {
     const vxe_chunk_upload& u = ups[i];
     const uint64_t mb = (uint64_t)u.meta.macro_base, cb = (uint64_t)u.meta.colinfo_base;
@@ -762,19 +931,22 @@ vxe_status vxe_upload_chunks(vxe_ctx* c, const vxe_chunk_upload* ups, uint32_t n
                   u.node_base, u.node_count);
     }
     if (u.node_count && (!u.nodes || !u.ropes)) return fail(c, VXE_ERR_INVALID_ARG, "upload %u has no node data", i);
-    CK(cudaMemcpyAsync((char*)c->metas.p + (size_t)u.slot * 48, &u.meta, 48, cudaMemcpyHostToDevice, c->upload));
+    vxe_status rs;
+    if ((rs = ring_copy(c, (char*)c->metas.p + (size_t)u.slot * 48, &u.meta, 48)) != VXE_OK) return rs;
     if (u.node_count) {
-      CK(cudaMemcpyAsync((char*)c->nodes.p + (size_t)u.node_base * 16, u.nodes, (size_t)u.node_count * 16,
-                         cudaMemcpyHostToDevice, c->upload));
-      CK(cudaMemcpyAsync((char*)c->ropes.p + (size_t)u.node_base * 32, u.ropes, (size_t)u.node_count * 32,
-                         cudaMemcpyHostToDevice, c->upload));
+      if ((rs = ring_copy(c, (char*)c->nodes.p + (size_t)u.node_base * 16, u.nodes, (size_t)u.node_count * 16)) !=
+          VXE_OK)
+        return rs;
+      if ((rs = ring_copy(c, (char*)c->ropes.p + (size_t)u.node_base * 32, u.ropes, (size_t)u.node_count * 32)) !=
+          VXE_OK)
+        return rs;
     }
-    if (u.macro_words)
-      CK(cudaMemcpyAsync((char*)c->macro.p + mb * 4, u.macro_words, VXE_MACRO_WORDS_PER_CHUNK * 4,
-                         cudaMemcpyHostToDevice, c->upload));
-    if (u.colinfo_words)
-      CK(cudaMemcpyAsync((char*)c->colinfo.p + cb * 4, u.colinfo_words, VXE_COLINFO_WORDS_PER_CHUNK * 4,
-                         cudaMemcpyHostToDevice, c->upload));
+    if (u.macro_words &&
+        (rs = ring_copy(c, (char*)c->macro.p + mb * 4, u.macro_words, VXE_MACRO_WORDS_PER_CHUNK * 4)) != VXE_OK)
+      return rs;
+    if (u.colinfo_words &&
+        (rs = ring_copy(c, (char*)c->colinfo.p + cb * 4, u.colinfo_words, VXE_COLINFO_WORDS_PER_CHUNK * 4)) != VXE_OK)
+      return rs;
   }
   vxe_status gst = grass_table_refresh(c, ups, n);
   if (gst != VXE_OK) return gst;
@@ -788,7 +960,9 @@ vxe_status vxe_write_meta(vxe_ctx* c, uint32_t first, const vxe_chunk_meta* meta
   if (!c || (n && !metas)) return fail(c, VXE_ERR_INVALID_ARG, "null metas");
   if ((uint64_t)first + n > c->cfg.chunk_capacity) return fail(c, VXE_ERR_CAPACITY, "meta run exceeds capacity");
   cudaSetDevice(c->device);
-  if (n) CK(cudaMemcpyAsync((char*)c->metas.p + (size_t)first * 48, metas, (size_t)n * 48, cudaMemcpyHostToDevice, c->upload));
+  vxe_status ws = upload_after_readers(c);
+  if (ws != VXE_OK) return ws;
+  if (n && (ws = ring_copy(c, (char*)c->metas.p + (size_t)first * 48, metas, (size_t)n * 48)) != VXE_OK) return ws;
   // a slot's records follow its meta (origin, colinfo base)
   if (n && c->gt.valid) {
     if (c->gt.built_recorded) CK(cudaStreamWaitEvent(c->upload, c->gt.built, 0));
@@ -808,7 +982,9 @@ vxe_status vxe_write_grid(vxe_ctx* c, const uint32_t* grid, uint32_t n) {
   if (!c || (n && !grid)) return fail(c, VXE_ERR_INVALID_ARG, "null grid");
   if (n > c->cfg.grid_capacity) return fail(c, VXE_ERR_CAPACITY, "grid of %u cells exceeds capacity %u", n, c->cfg.grid_capacity);
   cudaSetDevice(c->device);
-  if (n) CK(cudaMemcpyAsync(c->grid.p, grid, (size_t)n * 4, cudaMemcpyHostToDevice, c->upload));
+  vxe_status ws = upload_after_readers(c);
+  if (ws != VXE_OK) return ws;
+  if (n && (ws = ring_copy(c, c->grid.p, grid, (size_t)n * 4)) != VXE_OK) return ws;
   CK(cudaEventRecord(c->upload_done, c->upload));
   c->upload_pending = true;
   c->upload_recorded = true;
@@ -829,6 +1005,11 @@ vxe_status vxe_write_clipmap(vxe_ctx* c, const vxe_clipmap_gpu* params, const vx
     const vxe_clip_patch& p = patches[i];
     if (p.level >= c->cfg.clip_levels || (uint64_t)p.x + p.w > res || (uint64_t)p.y + p.h > res || !p.data)
       return fail(c, VXE_ERR_CAPACITY, "clip patch %u out of range", i);
+  }
+  vxe_status ws = upload_after_readers(c);
+  if (ws != VXE_OK) return ws;
+  for (uint32_t i = 0; i < n; ++i) {
+    const vxe_clip_patch& p = patches[i];
     if (p.w == 0 || p.h == 0) continue;
     char* dst = (char*)c->clip_tex.p + (((size_t)p.level * res + p.y) * res + p.x) * 4;
     CK(cudaMemcpy2DAsync(dst, (size_t)res * 4, p.data, (size_t)p.w * 4, (size_t)p.w * 4, p.h, cudaMemcpyHostToDevice,
@@ -1015,10 +1196,10 @@ vxe_status lane_resources(vxe_ctx* c, BatchLane& L, uint32_t tiles, uint32_t vp_
   if (!L.stage) {
     if (cudaMallocHost(&L.stage, kStageBytes) != cudaSuccess) return fail(c, VXE_ERR_OOM, "pinned staging");
     CK(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
-    if ((st = alloc(c, L.hdr, sizeof(BatchHeader))) != VXE_OK) return st;
-    if ((st = alloc(c, L.reqs, (size_t)VXE_MAX_BATCH_REQUESTS * sizeof(BatchReq))) != VXE_OK) return st;
-    if ((st = alloc(c, L.cams, (size_t)(VXE_MAX_BATCH_REQUESTS + 1) * sizeof(vxe_camera_gpu))) != VXE_OK) return st;
-    if ((st = alloc(c, L.head, 16)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.hdr, sizeof(BatchHeader), L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.reqs, (size_t)VXE_MAX_BATCH_REQUESTS * sizeof(BatchReq), L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.cams, (size_t)(VXE_MAX_BATCH_REQUESTS + 1) * sizeof(vxe_camera_gpu), L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.head, 16, L.stream)) != VXE_OK) return st;
     for (auto& e : L.ev) CK(cudaEventCreate(&e));
   }
   if (c->b_trace_grid == 0) {
@@ -1033,19 +1214,19 @@ vxe_status lane_resources(vxe_ctx* c, BatchLane& L, uint32_t tiles, uint32_t vp_
   if (vp_rays > L.ray_cap) {
     const uint64_t cap = std::min<uint64_t>(std::max<uint64_t>((uint64_t)vp_rays + vp_rays / 2, 1u << 16),
                                             0x3FFFFFFFu / kBatchProbesPerRay);
-    if ((st = alloc(c, L.px_first, cap * 8)) != VXE_OK) return st;
-    if ((st = alloc(c, L.px_mask, cap * 8)) != VXE_OK) return st;
-    if ((st = alloc(c, L.px_probe, cap * 8)) != VXE_OK) return st;
-    if ((st = alloc(c, L.px_task, cap * 4)) != VXE_OK) return st;
-    if ((st = alloc(c, L.px_hit, cap * 64)) != VXE_OK) return st;
-    if ((st = alloc(c, L.q_pending, cap * 4)) != VXE_OK) return st;
-    if ((st = alloc(c, L.q_refine, cap * 4)) != VXE_OK) return st;
-    if ((st = alloc(c, L.q_far, cap * 4)) != VXE_OK) return st;
-    if ((st = alloc(c, L.probe_recs, cap * kBatchProbesPerRay * sizeof(vxe::dev::ProbeRec))) != VXE_OK) return st;
-    if ((st = alloc(c, L.slab_tasks, cap * kBatchSlabsPerRay * 32)) != VXE_OK) return st;
-    if ((st = alloc(c, L.slab_res, cap * kBatchSlabsPerRay * 16)) != VXE_OK) return st;
-    if ((st = alloc(c, L.slab_hits, cap * kBatchSlabsPerRay * 4)) != VXE_OK) return st;
-    if (!L.dcount.p && (st = alloc(c, L.dcount, 32)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.px_first, cap * 8, L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.px_mask, cap * 8, L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.px_probe, cap * 8, L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.px_task, cap * 4, L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.px_hit, cap * 64, L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.q_pending, cap * 4, L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.q_refine, cap * 4, L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.q_far, cap * 4, L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.probe_recs, cap * kBatchProbesPerRay * sizeof(vxe::dev::ProbeRec), L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.slab_tasks, cap * kBatchSlabsPerRay * 32, L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.slab_res, cap * kBatchSlabsPerRay * 16, L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.slab_hits, cap * kBatchSlabsPerRay * 4, L.stream)) != VXE_OK) return st;
+    if (!L.dcount.p && (st = alloc_on(c, L.dcount, 32, L.stream)) != VXE_OK) return st;
     L.ray_cap = (uint32_t)cap;
     if (L.graph) {  // the captured launches hold the old pointers
       cudaGraphExecDestroy(L.graph);
@@ -1054,9 +1235,9 @@ vxe_status lane_resources(vxe_ctx* c, BatchLane& L, uint32_t tiles, uint32_t vp_
   }
   if (q_rays > L.q_cap) {
     const uint64_t cap = std::max<uint64_t>((uint64_t)q_rays + q_rays / 2, 1u << 16);
-    if ((st = alloc(c, L.q_keys, cap * 4)) != VXE_OK) return st;
-    if ((st = alloc(c, L.q_perm, cap * 4)) != VXE_OK) return st;
-    if (!L.bin_count.p && (st = alloc(c, L.bin_count, (size_t)std::max(c->cfg.grid_capacity, 1u) * 8u * 4u)) != VXE_OK)
+    if ((st = alloc_on(c, L.q_keys, cap * 4, L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.q_perm, cap * 4, L.stream)) != VXE_OK) return st;
+    if (!L.bin_count.p && (st = alloc_on(c, L.bin_count, (size_t)std::max(c->cfg.grid_capacity, 1u) * 8u * 4u, L.stream)) != VXE_OK)
       return st;
     L.q_cap = (uint32_t)cap;
     if (L.graph) {
@@ -1067,8 +1248,8 @@ vxe_status lane_resources(vxe_ctx* c, BatchLane& L, uint32_t tiles, uint32_t vp_
   if ((size_t)tiles * 4 > L.tile_count.bytes) {
     // grow by 1.5x so a stream of slightly larger batches does not reallocate every time
     const size_t cap = std::max<size_t>((size_t)tiles + tiles / 2, 4096);
-    if ((st = alloc(c, L.tile_count, cap * 4)) != VXE_OK) return st;
-    if ((st = alloc(c, L.tile_slots, cap * 4 * VXE_PRIMARY_MAX_TILE_CHUNKS)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.tile_count, cap * 4, L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.tile_slots, cap * 4 * VXE_PRIMARY_MAX_TILE_CHUNKS, L.stream)) != VXE_OK) return st;
     if (L.graph) {
       cudaGraphExecDestroy(L.graph);
       L.graph = nullptr;
@@ -1367,13 +1548,34 @@ vxe_status lane_ready(vxe_ctx* c, uint32_t lane) {
   return lane_resources(c, c->lanes[lane], 0u, 0u, 0u);
 }
 
+// Grows the lane's per-frame working buffers to cover an iw x ih frame.  The
+// lane's queued frames may still use the old buffers: those are freed after
+// them, in stream order.
+vxe_status lane_scratch(vxe_ctx* c, BatchLane& L, uint32_t iw, uint32_t ih) {
+  FrameState& S = L.scratch;
+  if (S.img[IMG_PIXHIT].p && S.iw >= iw && S.ih >= ih) return VXE_OK;
+  S.iw = S.pw = std::max(S.iw, iw);
+  S.ih = S.ph = std::max(S.ih, ih);
+  return alloc_images(c, S, IMG_SET_SCRATCH, L.stream);  // the old ones are freed in stream order
+}
+
 uint64_t vxe_view_bytes(const vxe_ctx* c, uint32_t present_w, uint32_t present_h, float render_scale) {
   if (!c || present_w == 0 || present_h == 0 || !(render_scale > 0.0f)) return 0;
   FrameState F;
   set_dims(F, present_w, present_h, render_scale);
   uint64_t total = 0;
   for (int i = 0; i < IMG_N; ++i)
-    if (img_enabled(c, i)) total += img_bytes(F, i);
+    if (img_enabled(c, i) && !img_is_scratch(i)) total += img_bytes(F, i);
+  return total;
+}
+
+uint64_t vxe_view_lane_bytes(const vxe_ctx* c, uint32_t present_w, uint32_t present_h, float render_scale) {
+  if (!c || present_w == 0 || present_h == 0 || !(render_scale > 0.0f)) return 0;
+  FrameState F;
+  set_dims(F, present_w, present_h, render_scale);
+  uint64_t total = 0;
+  for (int i = 0; i < IMG_N; ++i)
+    if (img_enabled(c, i) && img_is_scratch(i)) total += img_bytes(F, i);
   return total;
 }
 
@@ -1382,6 +1584,7 @@ vxe_status vxe_view_create(vxe_ctx* c, uint32_t present_w, uint32_t present_h, f
     return fail(c, VXE_ERR_INVALID_ARG, "bad view arguments");
   *out = nullptr;
   cudaSetDevice(c->device);
+  if (!c->aux) CK(cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking));
   auto* v = new (std::nothrow) vxe_view();
   if (!v) return fail(c, VXE_ERR_OOM, "view");
   set_dims(v->fr, present_w, present_h, render_scale);
@@ -1389,13 +1592,16 @@ vxe_status vxe_view_create(vxe_ctx* c, uint32_t present_w, uint32_t present_h, f
     delete v;
     return fail(c, VXE_ERR_DEVICE, "view event");
   }
-  vxe_status st = alloc_images(c, v->fr);
+  // images from the pool, zero-filled on the aux stream; the first frame
+  // waits for the fill like a frame that follows one on another lane
+  vxe_status st = alloc_images(c, v->fr, IMG_SET_OWN, c->aux);
   if (st != VXE_OK) {
-    release_frame_state(v->fr);
+    release_frame_state(v->fr, c->aux);
     cudaEventDestroy(v->done);
     delete v;
     return st;
   }
+  v->last_stream = c->aux;
   *out = v;
   return VXE_OK;
 }
@@ -1418,8 +1624,24 @@ vxe_status vxe_view_render_async(vxe_ctx* c, vxe_view* v, uint32_t lane, const v
     vc.grid_origin_chunk[k] = c->cam.grid_origin_chunk[k];
     vc.grid_dims[k] = c->cam.grid_dims[k];
   }
+  if ((st = frame_validate(c, v->fr, vc)) != VXE_OK) return st;
+  for (int i = 0; i < IMG_N; ++i)
+    if (!img_is_scratch(i) && img_enabled(c, i) != (v->fr.img[i].p != nullptr))
+      return fail(c, VXE_ERR_INVALID_ARG, "view was created under other image flags");
+  if ((st = lane_scratch(c, L, v->fr.iw, v->fr.ih)) != VXE_OK) return st;
   if (!L.busy) CK(cudaEventRecord(L.ev[0], L.stream));
-  if ((st = launch_frame_graph(c, v->fr, vc, L.stream, 1 + (int)lane)) != VXE_OK) return st;
+  if (c->upload_recorded) CK(cudaStreamWaitEvent(L.stream, c->upload_done, 0));
+  // The view's own outputs and histories, the lane's working buffers; plain
+  // launches (a view's graph would be re-captured whenever it changes lanes).
+  FrameArgs A;
+  frame_fill(c, v->fr, vc, A, &L.scratch);
+  bool use_grass = false;
+  const int reader = 1 + (int)lane;
+  if ((st = grass_table_acquire(c, L.stream, reader, vc, &use_grass)) != VXE_OK) return st;
+  if (use_grass) grass_table_args(c, A);
+  if ((st = frame_enqueue(c, v->fr, A, false, L.stream)) != VXE_OK) return st;
+  if (use_grass && (st = grass_table_release(c, L.stream, reader)) != VXE_OK) return st;
+  v->fr.ping = 1 - v->fr.ping;
   CK(cudaEventRecord(L.ev[1], L.stream));
   if (!L.busy) {
     L.rays = 0;
@@ -1447,8 +1669,7 @@ vxe_status vxe_view_read_image(vxe_ctx* c, vxe_view* v, int image, void* host, s
 vxe_status vxe_view_destroy(vxe_ctx* c, vxe_view* v) {
   if (!c || !v) return VXE_ERR_INVALID_ARG;
   cudaSetDevice(c->device);
-  if (v->last_stream) cudaStreamSynchronize(v->last_stream);
-  release_frame_state(v->fr);
+  release_frame_state(v->fr, v->last_stream);  // freed after the view's last frame
   if (v->done) cudaEventDestroy(v->done);
   delete v;
   return VXE_OK;

@@ -195,6 +195,7 @@ SIGNATURES = {
     "vxe_submit_batch_async": (C.c_int, [C.c_void_p, C.c_uint32, P(Request), C.c_uint32, P(BatchOptions)]),
     "vxe_batch_wait": (C.c_int, [C.c_void_p, C.c_uint32, C.c_int, P(BatchStats)]),
     "vxe_view_bytes": (C.c_uint64, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float]),
+    "vxe_view_lane_bytes": (C.c_uint64, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float]),
     "vxe_view_create": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, P(C.c_void_p)]),
     "vxe_view_render_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, P(CameraGpu)]),
     "vxe_view_read_image": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),

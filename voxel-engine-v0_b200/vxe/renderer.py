@@ -185,6 +185,10 @@ class Renderer:
     def view_bytes(self, width: int, height: int, render_scale: float) -> int:
         return int(self._lib.vxe_view_bytes(self._ctx, width, height, render_scale))
 
+    def view_lane_bytes(self, width: int, height: int, render_scale: float) -> int:
+        """Bytes of one lane's per-frame working buffers for views up to this size."""
+        return int(self._lib.vxe_view_lane_bytes(self._ctx, width, height, render_scale))
+
     def view(self, width: int, height: int, render_scale: float) -> "View":
         return View(self, width, height, render_scale)
 
