@@ -239,6 +239,8 @@ def run_batch_serve(dev):
     30 % query batches 1k-256k rays), continuous batching over 2 lanes with a
     4 GiB admission budget and 10 chunk re-uploads per 16 ms tick, vs the plain
     one-request-at-a-time server; latency = completion - arrival (host clock).
+    serve.sessions: the same with session frames (resident histories) at a
+    saturating (1000 req/s) and a light (200 req/s) load.
     """
     import torch
 
@@ -246,7 +248,7 @@ def run_batch_serve(dev):
     from vxe.batch import make_batch
     from vxe.renderer import Renderer
     from vxe.scenes import FrameDriver, config2
-    from vxe.serve import make_arrivals, serve, serve_plain
+    from vxe.serve import make_arrivals, make_sessions, serve, serve_plain
 
     sc = config2()
     drv = FrameDriver(sc)
@@ -275,6 +277,20 @@ def run_batch_serve(dev):
         srv = {"workload": "120 Poisson requests at 1000 req/s, 70 % viewports / 30 % query batches",
                "batched": rep.summary(), "plain": base.summary(),
                "speedup_vs_plain": round(base.seconds / rep.seconds, 3)}
+        # Sessions: frames of 16 clients whose TAA / godray / shadow histories
+        # stay resident between requests (one view each), with query batches.
+        sess = {}
+        for rate in (1000.0, 200.0):
+            ss = make_sessions(w, 16, seed=3)
+            rep = serve(r, w, make_arrivals(w, rate, 160, seed=7, sessions=ss), torch, mem_budget=6 << 30, lanes=2,
+                        max_batch=16, sessions=ss)
+            ss = make_sessions(w, 16, seed=3)
+            base = serve_plain(r, w, make_arrivals(w, rate, 160, seed=7, sessions=ss), torch, sessions=ss)
+            sess[f"{int(rate)}_per_s"] = {"batched": rep.summary(), "plain": base.summary(),
+                                          "speedup_vs_plain": round(base.seconds / rep.seconds, 3)}
+        srv["sessions"] = {"workload": "160 Poisson requests, 70 % frames of 16 sessions (256^2-1920x1080 "
+                                       "present at render scale 0.5, histories resident) / 30 % query batches",
+                           **sess}
         return batch, srv
     finally:
         r.close()

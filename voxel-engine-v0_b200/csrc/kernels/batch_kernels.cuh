@@ -72,6 +72,8 @@ struct BatchArgs {
   const float4* grass_rec;
   uint64_t grass_rec_n;
   const float* grass_taper;
+  uint32_t* grass_state;
+  float4* grass_frames;
   uint32_t grass_time_bits, grass_strength_bits;
   // deferred grass probes of viewport rays (persistent and graph modes), the
   // frame's scheme over the batch's viewport ray numbering (BatchReq::ray_base)
@@ -126,6 +128,8 @@ __device__ __forceinline__ Scene batch_scene(const BatchArgs& B, const vxe_camer
   s.grass_rec = table ? B.grass_rec : nullptr;
   s.grass_rec_n = table ? B.grass_rec_n : 0;
   s.grass_taper = table ? B.grass_taper : nullptr;
+  s.grass_state = table ? B.grass_state : nullptr;
+  s.grass_frames = table ? B.grass_frames : nullptr;
   return s;
 }
 

@@ -135,6 +135,12 @@ struct Scene {
   const float4* __restrict__ grass_rec;
   uint64_t grass_rec_n;
   const float* __restrict__ grass_taper;
+  // Lod-0 blade segment frames of the table's records (GRASS_FRAME_F4 float4
+  // each), filled in by the first march that needs them in a frame, and their
+  // state (0 not built, 1 being built, 2 ready); null when the pass has none.
+  // Written during passes, so never read through the read-only path.
+  uint32_t* grass_state;
+  float4* grass_frames;
 };
 
 struct Node { uint32_t child_base, child_mask, material, key; };

@@ -502,7 +502,49 @@ struct GrassCellGeom {
   float blade_len, inv_segs;
   GrassBladeGeom blade[3];
   float taper[6];
+  uint64_t rec;     // table record the cell was loaded from (~0: derived)
+  uint32_t frames;  // lod-0 segment frames of the record: 0 unknown, 1 ready, 2 none
 };
+
+// One blade segment's box frame (grass.wgsl:300-345): everything of the
+// segment's box SDF that does not depend on the point.
+struct GrassSegFrame {
+  v3 mid, S, T, N;
+  float half_w, half_h;
+};
+
+__device__ __forceinline__ GrassSegFrame grass_seg_frame(const GrassBladeGeom& B, float blade_len, float inv_segs,
+                                                         float taper, uint32_t sg) {
+  const float t01a = (float)sg * inv_segs;
+  const float t01b = ((float)sg + 1.0f) * inv_segs;
+  const float ya = t01a * blade_len, yb = t01b * blade_len;
+  const float seg_h = yb - ya;
+  const float bend_a = (blade_len * t01a) * (0.55f + 0.45f * t01a);
+  const float bend_b = (blade_len * t01b) * (0.55f + 0.45f * t01b);
+  const v2 bva = B.w_xz * t01a + B.lean_dir * B.lean_amt;
+  const v2 bvb = B.w_xz * t01b + B.lean_dir * B.lean_amt;
+  const v2 offa = bva * bend_a, offb = bvb * bend_b;
+  const v3 pa = B.root + V3(offa.x, ya, offa.y);
+  const v3 pb = B.root + V3(offb.x, yb, offb.y);
+  GrassSegFrame f;
+  f.T = normalize(pb - pa);
+  v3 S = B.side_hint - f.T * dot(B.side_hint, f.T);
+  const float s2 = dot(S, S);
+  if (s2 < 1e-6f) S = ortho_basis_x(f.T);
+  else S = S * (1.0f / sqrtf(s2));
+  f.S = S;
+  f.N = cross(f.T, S);
+  f.mid = 0.5f * (pa + pb);
+  f.half_w = B.r0 * taper * 0.7f;
+  f.half_h = 0.5f * seg_h;
+  return f;
+}
+
+__device__ __forceinline__ float grass_seg_sdf(const GrassSegFrame& f, v3 p) {
+  const v3 d = p - f.mid;
+  const v3 local = V3(dot(d, f.S), dot(d, f.T), dot(d, f.N));
+  return sdf_box(local, V3s(0.0f), V3(f.half_w, f.half_h, f.half_w));
+}
 
 // Blade length of cell `id` (grass.wgsl:216).
 __device__ __forceinline__ float grass_blade_len(const Scene& s, v3 id) {
@@ -566,6 +608,10 @@ __device__ __forceinline__ uint32_t grass_lod_segs(uint32_t lod) {
 // record and a fresh build are bit-identical.
 constexpr uint32_t GRASS_REC_F4 = 10u;
 constexpr uint32_t GRASS_TAPER_N = 18u;
+// Lod-0 segment frames of a record (blade-major, 3 blades x 6 segments):
+// (mid, half_w), (S, half_h), (T, 0) per segment; N = cross(T, S).
+constexpr uint32_t GRASS_FRAME_SEGS = 18u;
+constexpr uint32_t GRASS_FRAME_F4 = 3u * GRASS_FRAME_SEGS;
 
 __device__ __forceinline__ void grass_rec_store(float4* r, float blade_len, v3 id, const GrassBladeGeom* B) {
   r[0] = make_float4(blade_len, id.x, id.y, id.z);
@@ -602,6 +648,7 @@ __device__ __noinline__ bool grass_table_load(const Scene& s, v3 cb, v3 id, Gras
   if (__float_as_uint(h.y) != __float_as_uint(id.x) || __float_as_uint(h.z) != __float_as_uint(id.y) ||
       __float_as_uint(h.w) != __float_as_uint(id.z))
     return false;
+  G.rec = e;
   G.blade_len = h.x;
   for (uint32_t b = 0; b < G.blade_count; ++b) {
     const float4 a = r[1 + 3 * b], c = r[2 + 3 * b], d = r[3 + 3 * b];
@@ -625,6 +672,8 @@ __device__ __noinline__ void grass_cell_build(const Scene& s, v3 cb, v3 id, floa
   G.blade_count = blade_count;
   G.segs = segs;
   G.inv_segs = 1.0f / fmax_((float)segs, 1.0f);
+  G.rec = ~0ull;
+  G.frames = 2u;
   if (s.grass_taper != nullptr && lod < 3u) {
     for (uint32_t sg = 0; sg < segs; ++sg) G.taper[sg] = s.grass_taper[lod * 6u + sg];
   } else {
@@ -633,8 +682,46 @@ __device__ __noinline__ void grass_cell_build(const Scene& s, v3 cb, v3 id, floa
   if (!grass_table_load(s, cb, id, G)) {
     G.blade_len = grass_blade_len(s, id);
     for (uint32_t i = 0; i < blade_count; ++i) grass_blade_geom(s, cb, id, time_s, strength, i, G.blade[i]);
+  } else if (lod == 0u && s.grass_state != nullptr && blade_count * segs == GRASS_FRAME_SEGS) {
+    G.frames = 0u;
   }
   G.built = true;
+}
+
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Makes the record's lod-0 segment frames usable: ready already, or built
+// here by the first lane to claim them (the same grass_seg_frame values every
+// march would compute).  A lane that finds another one building them goes on
+// without (false) and asks again at its next evaluation; nothing waits.
+__device__ __noinline__ bool grass_frames_ready(const Scene& s, GrassCellGeom& G) {
+  uint32_t* st = s.grass_state + G.rec;
+  const uint32_t v = ld_acquire_gpu(st);
+  if (v == 2u) {
+    G.frames = 1u;
+    return true;
+  }
+  if (v != 0u || atomicCAS(st, 0u, 1u) != 0u) return false;
+  float4* F = s.grass_frames + G.rec * GRASS_FRAME_F4;
+  for (uint32_t i = 0; i < G.blade_count; ++i)
+    for (uint32_t sg = 0; sg < G.segs; ++sg) {
+      const GrassSegFrame f = grass_seg_frame(G.blade[i], G.blade_len, G.inv_segs, G.taper[sg], sg);
+      float4* o = F + 3u * (i * G.segs + sg);
+      o[0] = make_float4(f.mid.x, f.mid.y, f.mid.z, f.half_w);
+      o[1] = make_float4(f.S.x, f.S.y, f.S.z, f.half_h);
+      o[2] = make_float4(f.T.x, f.T.y, f.T.z, 0.0f);
+    }
+  st_release_gpu(st, 2u);
+  G.frames = 1u;
+  return true;
 }
 
 // grass_sdf_lod (grass.wgsl:192-350) over the cached cell geometry.
@@ -648,36 +735,26 @@ __device__ __noinline__ float grass_sdf_cached(const Scene& s, v3 p, v3 cb, v3 i
   const float over = GRASS_OVERHANG_VOX * vs;
   if (p.x < cb.x - over || p.x > cb.x + vs + over || p.z < cb.z - over || p.z > cb.z + vs + over) return BIG;
   if (!G.built) grass_cell_build(s, cb, id, time_s, strength, lod, G);
-  const float blade_len = G.blade_len;
   float dmin = BIG;
-  for (uint32_t i = 0; i < G.blade_count; ++i) {
-    const GrassBladeGeom& B = G.blade[i];
-    for (uint32_t sg = 0; sg < G.segs; ++sg) {
-      const float t01a = (float)sg * G.inv_segs;
-      const float t01b = ((float)sg + 1.0f) * G.inv_segs;
-      const float ya = t01a * blade_len, yb = t01b * blade_len;
-      const float seg_h = yb - ya;
-      const float bend_a = (blade_len * t01a) * (0.55f + 0.45f * t01a);
-      const float bend_b = (blade_len * t01b) * (0.55f + 0.45f * t01b);
-      const v2 bva = B.w_xz * t01a + B.lean_dir * B.lean_amt;
-      const v2 bvb = B.w_xz * t01b + B.lean_dir * B.lean_amt;
-      const v2 offa = bva * bend_a, offb = bvb * bend_b;
-      const v3 pa = B.root + V3(offa.x, ya, offa.y);
-      const v3 pb = B.root + V3(offb.x, yb, offb.y);
-      const v3 T = normalize(pb - pa);
-      v3 S = B.side_hint - T * dot(B.side_hint, T);
-      const float s2 = dot(S, S);
-      if (s2 < 1e-6f) S = ortho_basis_x(T);
-      else S = S * (1.0f / sqrtf(s2));
-      const v3 N = cross(T, S);
-      const v3 mid = 0.5f * (pa + pb);
-      const v3 d = p - mid;
-      const v3 local = V3(dot(d, S), dot(d, T), dot(d, N));
-      const float half_w = B.r0 * G.taper[sg] * 0.7f;
-      const float dbox = sdf_box(local, V3s(0.0f), V3(half_w, 0.5f * seg_h, half_w));
-      dmin = fmin_(dmin, dbox);
+  if (G.frames == 1u || (G.frames == 0u && grass_frames_ready(s, G))) {
+    const float4* F = s.grass_frames + G.rec * GRASS_FRAME_F4;
+#pragma unroll 6
+    for (uint32_t k = 0; k < GRASS_FRAME_SEGS; ++k) {
+      const float4 a = F[3u * k], b = F[3u * k + 1u], c = F[3u * k + 2u];
+      GrassSegFrame f;
+      f.mid = V3(a.x, a.y, a.z);
+      f.S = V3(b.x, b.y, b.z);
+      f.T = V3(c.x, c.y, c.z);
+      f.N = cross(f.T, f.S);
+      f.half_w = a.w;
+      f.half_h = b.w;
+      dmin = fmin_(dmin, grass_seg_sdf(f, p));
     }
+    return dmin;
   }
+  for (uint32_t i = 0; i < G.blade_count; ++i)
+    for (uint32_t sg = 0; sg < G.segs; ++sg)
+      dmin = fmin_(dmin, grass_seg_sdf(grass_seg_frame(G.blade[i], G.blade_len, G.inv_segs, G.taper[sg], sg), p));
   return dmin;
 }
 
@@ -747,8 +824,9 @@ __device__ __noinline__ GrassHit grass_layer_trace_lod(const Scene& s, v3 ro, v3
   return GrassHit{false, BIG, V3s(0.0f)};
 }
 
-__device__ __noinline__ GrassHit try_grass_slab_hit(const Scene& s, v3 ro, v3 rd, float t_min, float t_max, v3 cb, v3 id, float vs,
-                            float time_s, float strength) {  // grass.wgsl:494-538
+// The part of [t_min, t_max] inside the cell's grass slab and before the
+// cell's own voxel (grass.wgsl:494-535); empty when t1 <= t0.
+__device__ __forceinline__ v2 grass_slab_interval(v3 ro, v3 rd, float t_min, float t_max, v3 cb, float vs) {
   const float layer_h = GRASS_LAYER_HEIGHT_VOX * vs;
   const float over = GRASS_OVERHANG_VOX * vs;
   const v3 sb0 = V3(cb.x - over, cb.y + vs, cb.z - over);
@@ -761,9 +839,16 @@ __device__ __noinline__ GrassHit try_grass_slab_hit(const Scene& s, v3 ro, v3 rd
   if (rv.y > rv.x) {
     if (rv.x > t0) t1 = fmin_(t1, rv.x - clip_eps);
   }
-  if (t1 <= t0) return GrassHit{false, BIG, V3s(0.0f)};
-  return grass_layer_trace_lod(s, ro, rd, t0, t1, cb, id, time_s, strength, grass_lod_from_t(t0));
+  return V2(t0, t1);
 }
+
+__device__ __noinline__ GrassHit try_grass_slab_hit(const Scene& s, v3 ro, v3 rd, float t_min, float t_max, v3 cb, v3 id, float vs,
+                            float time_s, float strength) {  // grass.wgsl:494-538
+  const v2 iv = grass_slab_interval(ro, rd, t_min, t_max, cb, vs);
+  if (iv.y <= iv.x) return GrassHit{false, BIG, V3s(0.0f)};
+  return grass_layer_trace_lod(s, ro, rd, iv.x, iv.y, cb, id, time_s, strength, grass_lod_from_t(iv.x));
+}
+
 
 // ---------------------------------------------------------------------------
 // chunk_trace.wgsl
@@ -876,7 +961,7 @@ __device__ ExitFaceRes exit_face_from_slab_safe(v3 rd, const CubeSlab& slab) {  
   return ExitFaceRes{rd.z > 0.0f ? 4u : 5u, 0};
 }
 
-__device__ __noinline__ LeafState descend_leaf_sparse(const Scene& s, v3 p, uint32_t node_base, uint32_t start_idx, v3 start_bmin,
+__device__ __forceinline__ LeafState descend_leaf_sparse(const Scene& s, v3 p, uint32_t node_base, uint32_t start_idx, v3 start_bmin,
                               float start_size) {  // chunk_trace.wgsl:296-358
   uint32_t idx = start_idx;
   v3 bmin = start_bmin;
@@ -906,7 +991,7 @@ struct MacroDDAState {
   float tMaxX, tMaxY, tMaxZ, tDeltaX, tDeltaY, tDeltaZ, cell;
 };
 
-__device__ __noinline__ MacroDDAState macro_dda_init(v3 ro, v3 rd, v3 inv, float tcur, v3 rb, float rs, uint32_t macro_base) {
+__device__ __forceinline__ MacroDDAState macro_dda_init(v3 ro, v3 rd, v3 inv, float tcur, v3 rb, float rs, uint32_t macro_base) {
   // chunk_trace.wgsl:397-475
   MacroDDAState st;
   st.enabled = false;
@@ -1165,7 +1250,7 @@ __device__ __forceinline__ void probe_record(ProbeHook& ph, float t0, float t1, 
   }
 }
 
-__device__ __noinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(const Scene& s, v3 ro, v3 rd, v3 inv, const Meta& ch,
+__device__ __forceinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(const Scene& s, v3 ro, v3 rd, v3 inv, const Meta& ch,
                                                    float t_enter, float t_exit, bool use_anchor,
                                                    uint32_t anchor_key, const TraceOpts& opt, ProbeHook& ph) {
   // chunk_trace.wgsl:669-961
@@ -1303,7 +1388,7 @@ __device__ __noinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(const
   return ChunkTraceResult{miss_hitgeom(), an.valid, an.key};
 }
 
-__device__ __noinline__ ChunkTraceResult trace_chunk_interval_stream_macro(const Scene& s, v3 ro, v3 rd, v3 inv, const Meta& ch,
+__device__ __forceinline__ ChunkTraceResult trace_chunk_interval_stream_macro(const Scene& s, v3 ro, v3 rd, v3 inv, const Meta& ch,
                                                    float t0_in, float t1_in, bool use_anchor, uint32_t anchor_key_in,
                                                    const TraceOpts& opt, ProbeHook& ph) {  // chunk_trace.wgsl:592-667
   const float vs = vs_(s);
@@ -1314,29 +1399,34 @@ __device__ __noinline__ ChunkTraceResult trace_chunk_interval_stream_macro(const
   const float t_end = t1_in;
   uint32_t anchor_key = anchor_key_in;
   bool anchor_valid = use_anchor;
-  if (ch.macro_base == INVALID)
-    return trace_chunk_rope_interval_nomacro(s, ro, rd, inv, ch, tcur, t_end, anchor_valid, anchor_key, opt, ph);
-  MacroDDAState ms = macro_dda_init(ro, rd, inv, tcur, rb, rs, ch.macro_base);
-  if (!ms.enabled)
-    return trace_chunk_rope_interval_nomacro(s, ro, rd, inv, ch, tcur, t_end, anchor_valid, anchor_key, opt, ph);
+  MacroDDAState ms;
+  ms.enabled = false;
+  if (ch.macro_base != INVALID) ms = macro_dda_init(ro, rd, inv, tcur, rb, rs, ch.macro_base);
+  // Without a usable macro grid the whole interval is one segment.  One call
+  // site for the leaf walk keeps it inlined once.
+  const bool whole = !ms.enabled;
   for (uint32_t i = 0; i < 128u; ++i) {
-    if (tcur >= t_end) break;
-    macro_dda_sync(ms, tcur);
-    const MacroStep st = macro_dda_current(s, ms, ch.macro_base);
-    if (!st.valid) break;
-    const float t_cell_exit = fmin_(st.t_exit, t_end);
-    if (st.empty) {
-      tcur = t_cell_exit + eps_step;
-      if (ms.enabled && tcur >= st.t_exit) macro_dda_step(ms);
-      continue;
+    float seg_end = t_end, cell_exit = t_end;
+    if (!whole) {
+      if (tcur >= t_end) break;
+      macro_dda_sync(ms, tcur);
+      const MacroStep st = macro_dda_current(s, ms, ch.macro_base);
+      if (!st.valid) break;
+      cell_exit = st.t_exit;
+      seg_end = fmin_(st.t_exit, t_end);
+      if (st.empty) {
+        tcur = seg_end + eps_step;
+        if (ms.enabled && tcur >= st.t_exit) macro_dda_step(ms);
+        continue;
+      }
     }
     const ChunkTraceResult h =
-        trace_chunk_rope_interval_nomacro(s, ro, rd, inv, ch, tcur, t_cell_exit, anchor_valid, anchor_key, opt, ph);
-    if (h.hit.hit != 0u) return h;
+        trace_chunk_rope_interval_nomacro(s, ro, rd, inv, ch, tcur, seg_end, anchor_valid, anchor_key, opt, ph);
+    if (whole || h.hit.hit != 0u) return h;
     anchor_valid = h.anchor_valid;
     anchor_key = h.anchor_key;
-    tcur = t_cell_exit + eps_step;
-    if (ms.enabled && tcur >= st.t_exit) macro_dda_step(ms);
+    tcur = seg_end + eps_step;
+    if (ms.enabled && tcur >= cell_exit) macro_dda_step(ms);
   }
   return ChunkTraceResult{miss_hitgeom(), anchor_valid, anchor_key};
 }

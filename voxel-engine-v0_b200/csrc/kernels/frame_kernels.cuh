@@ -84,6 +84,8 @@ struct FrameArgs {
   float4* grass_rec;
   uint64_t grass_rec_n;  // records (slots * 4096)
   float* grass_taper;    // 3 LODs x 6 segments
+  uint32_t* grass_state;  // per record: lod-0 segment frames built?
+  float4* grass_frames;   // per record: the frames
   uint32_t grass_slot0;  // k_grass_cells: first slot of the launch
 };
 
@@ -116,6 +118,8 @@ __device__ __forceinline__ Scene make_scene(const FrameArgs& A, bool godray) {
   s.grass_rec = A.grass_rec;
   s.grass_rec_n = A.grass_rec_n;
   s.grass_taper = A.grass_taper;
+  s.grass_state = A.grass_rec ? A.grass_state : nullptr;
+  s.grass_frames = A.grass_rec ? A.grass_frames : nullptr;
   return s;
 }
 
@@ -140,6 +144,7 @@ __global__ void __launch_bounds__(GRASS_CELL_THREADS) k_grass_cells(const __grid
   const uint32_t slot = (uint32_t)(g >> 12), col = (uint32_t)(g & 4095u);
   if (slot >= A.cam.chunk_count || (uint64_t)slot * 4096u >= A.grass_rec_n) return;
   float4* r = A.grass_rec + g * GRASS_REC_F4;
+  if (A.grass_state) A.grass_state[g] = 0u;  // this frame's segment frames are built on first use
   const Meta m = meta_at(s, slot);
   const float nan = __uint_as_float(0x7FC00000u);
   if (m.colinfo_base == INVALID) {
@@ -1202,6 +1207,8 @@ __device__ __forceinline__ Scene make_query_scene(const QueryArgs& Q) {
   s.err = Q.err;
   s.grass_rec = nullptr;
   s.grass_rec_n = 0;
+  s.grass_state = nullptr;
+  s.grass_frames = nullptr;
   s.grass_taper = nullptr;
   return s;
 }

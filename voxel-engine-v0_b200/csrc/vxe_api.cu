@@ -58,7 +58,7 @@ enum Img {
 constexpr int kGrassReaders = 1 + VXE_BATCH_LANES;  // compute stream, lanes
 
 struct GrassTable {
-  DevBuf rec, taper;
+  DevBuf rec, taper, state, frames;
   bool valid = false;
   uint32_t time_bits = 0, strength_bits = 0, vs_bits = 0, chunk_count = 0;
   vxe_camera_gpu cam{};  // camera of the last full build (for slot refreshes)
@@ -367,6 +367,8 @@ uint32_t fbits(float f) {
 void grass_table_args(const vxe_ctx* c, FrameArgs& A) {
   A.grass_rec = (float4*)c->gt.rec.p;
   A.grass_rec_n = (uint64_t)c->cfg.chunk_capacity * 4096u;
+  A.grass_state = (uint32_t*)c->gt.state.p;
+  A.grass_frames = (float4*)c->gt.frames.p;
   A.grass_taper = (float*)c->gt.taper.p;
 }
 
@@ -726,6 +728,8 @@ vxe_status vxe_create(const vxe_config* cfg, vxe_ctx** out) {
   if (!(cfg->flags & VXE_FLAG_NO_GRASS_TABLE)) {
     if ((st = alloc(c, c->gt.rec, cc * 4096u * vxe::dev::GRASS_REC_F4 * 16u)) != VXE_OK) return bail(st);
     if ((st = alloc(c, c->gt.taper, vxe::dev::GRASS_TAPER_N * 4u)) != VXE_OK) return bail(st);
+    if ((st = alloc(c, c->gt.state, cc * 4096u * 4u)) != VXE_OK) return bail(st);
+    if ((st = alloc(c, c->gt.frames, cc * 4096u * vxe::dev::GRASS_FRAME_F4 * 16u)) != VXE_OK) return bail(st);
   }
   if (cudaEventCreateWithFlags(&c->gt.built, cudaEventDisableTiming) != cudaSuccess) return bail(VXE_ERR_DEVICE);
   for (auto& e : c->gt.reader)
@@ -750,7 +754,7 @@ void vxe_destroy(vxe_ctx* c) {
   for (auto& L : c->lanes)  // lanes read the arenas: drain them before freeing
     if (L.stream) cudaStreamSynchronize(L.stream);
   for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword,
-                  &c->q_in, &c->q_out, &c->gt.rec, &c->gt.taper})
+                  &c->q_in, &c->q_out, &c->gt.rec, &c->gt.taper, &c->gt.state, &c->gt.frames})
     release(*b);
   for (auto& L : c->lanes) {
     if (L.stream) cudaStreamSynchronize(L.stream);
@@ -1447,6 +1451,8 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
   if (use_grass) {
     B.grass_rec = (const float4*)c->gt.rec.p;
     B.grass_rec_n = (uint64_t)c->cfg.chunk_capacity * 4096u;
+    B.grass_state = (uint32_t*)c->gt.state.p;
+    B.grass_frames = (float4*)c->gt.frames.p;
     B.grass_taper = (const float*)c->gt.taper.p;
     B.grass_time_bits = fbits(gcam->voxel_params[1]);
     B.grass_strength_bits = fbits(gcam->voxel_params[2]);
