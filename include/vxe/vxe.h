@@ -169,8 +169,18 @@ enum {
    * lean, radius and side axis of every grass column top, 160 B per column of
    * every chunk slot).  Without it each grass march derives its cell's blades
    * itself, as the reference shader does; images are identical either way.
-   * Read at vxe_create (the table is allocated there) and per frame. */
-  VXE_FLAG_NO_GRASS_TABLE = 1u << 6
+   * Read at vxe_create (the table is allocated there) and per frame.  The
+   * table also caches, per frame, the lod-0 blade segment frames of the
+   * columns that grass marches visit (864 B per column). */
+  VXE_FLAG_NO_GRASS_TABLE = 1u << 6,
+  /* vxe_upload_chunks copies are ordered before every pass enqueued after
+   * the call but not after the passes already in flight (a world write is
+   * otherwise ordered after both, like a queue write between submissions).
+   * For callers whose uploads only write chunk slots and node ranges that no
+   * pass in flight reads -- freshly allocated slots of a streaming loader --
+   * or rewrite them with identical contents.  Grid, meta and clipmap writes
+   * stay ordered. */
+  VXE_FLAG_UPLOADS_UNORDERED = 1u << 7
 };
 
 typedef struct vxe_config {

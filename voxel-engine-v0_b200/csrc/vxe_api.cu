@@ -920,8 +920,10 @@ vxe_status vxe_upload_chunks(vxe_ctx* c, const vxe_chunk_upload* ups, uint32_t n
   if (!c || (n && !ups)) return fail(c, VXE_ERR_INVALID_ARG, "null uploads");
   cudaSetDevice(c->device);
   const bool silent = (c->flags & VXE_FLAG_SILENT_CAPACITY_SKIP) != 0;
-  vxe_status ws = upload_after_readers(c);
-  if (ws != VXE_OK) return ws;
+  if (!(c->flags & VXE_FLAG_UPLOADS_UNORDERED)) {
+    vxe_status ws = upload_after_readers(c);
+    if (ws != VXE_OK) return ws;
+  }
   for (uint32_t i = 0; i < n; ++i) {
     const vxe_chunk_upload& u = ups[i];
     const uint64_t mb = (uint64_t)u.meta.macro_base, cb = (uint64_t)u.meta.colinfo_base;

@@ -35,6 +35,7 @@ FLAG_DEBUG_INTERMEDIATES = 1 << 3
 FLAG_CHECKED = 1 << 4
 FLAG_PRIMARY_MEGAKERNEL = 1 << 5
 FLAG_NO_GRASS_TABLE = 1 << 6
+FLAG_UPLOADS_UNORDERED = 1 << 7
 
 (IMG_COLOR, IMG_DEPTH, IMG_LOCAL, IMG_PRIMARY_HIST_IN, IMG_PRIMARY_HIST_OUT, IMG_SHADOW_IN, IMG_SHADOW_OUT,
  IMG_LOCAL_HIST_IN, IMG_LOCAL_HIST_OUT, IMG_GODRAY_IN, IMG_GODRAY_OUT, IMG_OUTPUT_PRE_TAA, IMG_OUTPUT,

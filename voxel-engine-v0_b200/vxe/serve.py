@@ -233,6 +233,9 @@ class _Views:
 
 
 def _reupload(renderer, world, resident, rng, count):
+    """Re-uploads `count` resident chunks with their own contents: the upload
+    traffic of a streaming loader without changing the world, so the uploads
+    may overlap the passes in flight (FLAG_UPLOADS_UNORDERED)."""
     picks = rng.choice(len(resident), size=min(count, len(resident)), replace=False)
     ups = []
     for i in picks:
@@ -268,6 +271,8 @@ def serve(renderer, world: World, requests, torch, mem_budget: int, lanes: int =
     rng = np.random.default_rng(99)
     resident = [k for k in world.slot_to_key if not world.chunk(k).macro_empty]
     batches = uploads = max_inflight = 0
+    flags0 = renderer.flags
+    renderer.set_flags(flags0 | A.FLAG_UPLOADS_UNORDERED)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     next_tick = 0.0
@@ -333,6 +338,7 @@ def serve(renderer, world: World, requests, torch, mem_budget: int, lanes: int =
         seconds = time.perf_counter() - t0
     finally:
         views.close()
+        renderer.set_flags(flags0)
     lat = [(r.done - r.arrival) * 1e3 for r in reqs]
     extra = ({"views_created": views.created, "view_evictions": views.evictions, "lane_bytes": lane_bytes}
              if sessions else {})
