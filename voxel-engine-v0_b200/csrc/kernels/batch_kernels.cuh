@@ -130,6 +130,7 @@ __device__ __forceinline__ Scene batch_scene(const BatchArgs& B, const vxe_camer
   s.grass_taper = table ? B.grass_taper : nullptr;
   s.grass_state = table ? B.grass_state : nullptr;
   s.grass_frames = table ? B.grass_frames : nullptr;
+  s.slot_lights = nullptr;
   return s;
 }
 

@@ -141,6 +141,9 @@ struct Scene {
   // Written during passes, so never read through the read-only path.
   uint32_t* grass_state;
   float4* grass_frames;
+  // Per chunk slot: 1 when the slot's nodes hold a LIGHT leaf (written with
+  // the slot's uploads and meta writes); null when the pass has none.
+  const uint32_t* __restrict__ slot_lights;
 };
 
 struct Node { uint32_t child_base, child_mask, material, key; };

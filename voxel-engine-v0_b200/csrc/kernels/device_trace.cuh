@@ -2075,10 +2075,34 @@ __device__ __forceinline__ v3 light_finish(v3 sum) {  // light.wgsl:207-210
   return sum * (1.0f / denom);
 }
 
+// False when no chunk within reach of dda_hit_light from p0 (at most
+// LIGHT_MAX_DIST_VOX cells, each step one cell along one axis) holds a LIGHT
+// leaf: every light ray then ends on a solid voxel, in air or outside the
+// grid, and the gather adds nothing.  The cell box gets one cell of margin
+// for the half-cell offset of the query points.
+__device__ __noinline__ bool lights_possible(const Scene& s, v3 p0) {
+  if (s.slot_lights == nullptr) return true;
+  const v3 fl = vfloor(p0 / fmax_(vs_(s), 1e-6f));
+  const int32_t cs = (int32_t)s.cam->chunk_size;
+  if (cs <= 0) return true;
+  const int32_t r = (int32_t)LIGHT_MAX_DIST_VOX + 1;
+  auto fdiv = [cs](int32_t a) { return a >= 0 ? a / cs : -((-a + cs - 1) / cs); };
+  const int32_t cx = to_i32(fl.x), cy = to_i32(fl.y), cz = to_i32(fl.z);
+  for (int32_t z = fdiv(cz - r); z <= fdiv(cz + r); ++z)
+    for (int32_t y = fdiv(cy - r); y <= fdiv(cy + r); ++y)
+      for (int32_t x = fdiv(cx - r); x <= fdiv(cx + r); ++x) {
+        const uint32_t slot = grid_lookup_slot(s, x, y, z);
+        if (slot != INVALID && slot < s.cam->chunk_count && slot < s.metas_n && __ldg(&s.slot_lights[slot]) != 0u)
+          return true;
+      }
+  return false;
+}
+
 __device__ __noinline__ v3 gather_voxel_lights(const Scene& s, v3 hp, v3 n, v3 rb) {  // light.wgsl:127-211
   const LightFrame F = light_frame(s, hp, n, rb);
   uint32_t hits = 0;
   v3 sum = V3s(0.0f);
+  if (!lights_possible(s, F.p0)) return light_finish(sum);
   for (uint32_t i = 0; i < LIGHT_RAYS; ++i) {
     const v4 hit = dda_hit_light(s, F.p0, light_ray_dir(F, n, i), LIGHT_MAX_DIST_VOX, vs_(s));
     if (light_accum(s, hp, n, hit, hits, sum)) break;

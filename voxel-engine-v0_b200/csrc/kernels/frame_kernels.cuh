@@ -86,6 +86,7 @@ struct FrameArgs {
   float* grass_taper;    // 3 LODs x 6 segments
   uint32_t* grass_state;  // per record: lod-0 segment frames built?
   float4* grass_frames;   // per record: the frames
+  const uint32_t* slot_lights;  // per slot: holds a LIGHT leaf
   uint32_t grass_slot0;  // k_grass_cells: first slot of the launch
 };
 
@@ -120,6 +121,7 @@ __device__ __forceinline__ Scene make_scene(const FrameArgs& A, bool godray) {
   s.grass_taper = A.grass_taper;
   s.grass_state = A.grass_rec ? A.grass_state : nullptr;
   s.grass_frames = A.grass_rec ? A.grass_frames : nullptr;
+  s.slot_lights = A.slot_lights;
   return s;
 }
 
@@ -166,6 +168,29 @@ __global__ void __launch_bounds__(GRASS_CELL_THREADS) k_grass_cells(const __grid
   GrassBladeGeom B[GRASS_BLADE_COUNT];
   for (uint32_t i = 0; i < GRASS_BLADE_COUNT; ++i) grass_blade_geom(s, cb, id, time_s, strength, i, B[i]);
   grass_rec_store(r, grass_blade_len(s, id), id, B);
+}
+
+// ---------------------------------------------------------------------------
+// Per-slot light flags: one block per slot of [slot0, slot0 + gridDim.x),
+// over the node records of its meta's range; 1 when one is a LIGHT leaf.
+// ---------------------------------------------------------------------------
+constexpr int SLOT_LIGHT_THREADS = 256;
+
+__global__ void __launch_bounds__(SLOT_LIGHT_THREADS) k_slot_lights(const uint4* metas, uint64_t metas_n,
+                                                                     const uint4* nodes, uint64_t nodes_n,
+                                                                     uint32_t slot0, uint32_t* out) {
+  const uint32_t slot = slot0 + blockIdx.x;
+  if (slot >= metas_n) return;
+  const uint4 b = metas[(size_t)slot * 3u + 1u];  // node_base, node_count, macro_base, colinfo_base
+  int any = 0;
+  for (uint32_t i = threadIdx.x; i < b.y; i += SLOT_LIGHT_THREADS) {
+    const uint64_t gi = (uint64_t)b.x + i;
+    if (gi >= nodes_n) break;
+    const uint4 n = nodes[gi];
+    any |= (n.x == LEAF && n.z == MAT_LIGHT) ? 1 : 0;
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) out[slot] = any ? 1u : 0u;
 }
 
 // ---------------------------------------------------------------------------
@@ -895,6 +920,12 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_shade_prep(const __grid_const
       }
       fresh = shadow_fresh(c);
       light = lights_wanted(g);
+      if (light && !lights_possible(s, (c.ro + c.rd * g.t) + g.n * (0.75f * vs_(s)))) {
+        // no LIGHT voxel within the gather's reach: its exact result, +0
+        const v3 r = light_finish(V3s(0.0f));
+        A.px_light[pix] = make_float4(r.x, r.y, r.z, 0.0f);
+        light = false;
+      }
     }
     enqueue(A.q_shadow, &A.q_count[2], fresh, pix);
     enqueue(A.q_light, &A.q_count[3], light, pix);
@@ -1209,6 +1240,7 @@ __device__ __forceinline__ Scene make_query_scene(const QueryArgs& Q) {
   s.grass_rec_n = 0;
   s.grass_state = nullptr;
   s.grass_frames = nullptr;
+  s.slot_lights = nullptr;
   s.grass_taper = nullptr;
   return s;
 }

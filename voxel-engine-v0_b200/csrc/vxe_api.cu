@@ -120,6 +120,7 @@ struct vxe_ctx {
   bool upload_pending = false;
   // arenas
   DevBuf nodes, ropes, metas, macro, colinfo, grid, clip_tex, errword;
+  DevBuf slot_lights;  // per slot: holds a LIGHT leaf (k_slot_lights)
   GrassTable gt;
   FrameState fr;  // the context's own frame
   vxe_camera_gpu cam{};
@@ -356,6 +357,18 @@ void fill_scene_args(const vxe_ctx* c, FrameArgs& A) {
   A.clip_res = c->cfg.clip_res;
   A.err = (uint32_t*)c->errword.p;
   A.godray_alias = (c->flags & VXE_FLAG_GODRAY_MACRO_ALIAS) ? 1u : 0u;
+  A.slot_lights = (const uint32_t*)c->slot_lights.p;
+}
+
+// Recomputes the light flags of slots [first, first + n) on the upload
+// stream, after the writes queued there.
+vxe_status slot_lights_refresh(vxe_ctx* c, uint32_t first, uint32_t n) {
+  if (n == 0 || !c->slot_lights.p) return VXE_OK;
+  vxe::dev::k_slot_lights<<<n, vxe::dev::SLOT_LIGHT_THREADS, 0, c->upload>>>(
+      (const uint4*)c->metas.p, c->cfg.chunk_capacity, (const uint4*)c->nodes.p, c->cfg.node_capacity, first,
+      (uint32_t*)c->slot_lights.p);
+  CK(cudaGetLastError());
+  return VXE_OK;
 }
 
 uint32_t fbits(float f) {
@@ -725,6 +738,7 @@ vxe_status vxe_create(const vxe_config* cfg, vxe_ctx** out) {
   const uint64_t clip_bytes = (uint64_t)cfg->clip_levels * cfg->clip_res * cfg->clip_res * 4;
   if ((st = alloc(c, c->clip_tex, clip_bytes)) != VXE_OK) return bail(st);
   if ((st = alloc(c, c->errword, 4)) != VXE_OK) return bail(st);
+  if ((st = alloc(c, c->slot_lights, cc * 4)) != VXE_OK) return bail(st);
   if (!(cfg->flags & VXE_FLAG_NO_GRASS_TABLE)) {
     if ((st = alloc(c, c->gt.rec, cc * 4096u * vxe::dev::GRASS_REC_F4 * 16u)) != VXE_OK) return bail(st);
     if ((st = alloc(c, c->gt.taper, vxe::dev::GRASS_TAPER_N * 4u)) != VXE_OK) return bail(st);
@@ -753,7 +767,7 @@ void vxe_destroy(vxe_ctx* c) {
   if (c->fr.fgraph) cudaGraphDestroy(c->fr.fgraph);
   for (auto& L : c->lanes)  // lanes read the arenas: drain them before freeing
     if (L.stream) cudaStreamSynchronize(L.stream);
-  for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword,
+  for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword, &c->slot_lights,
                   &c->q_in, &c->q_out, &c->gt.rec, &c->gt.taper, &c->gt.state, &c->gt.frames})
     release(*b);
   for (auto& L : c->lanes) {
@@ -956,6 +970,20 @@ vxe_status vxe_upload_chunks(vxe_ctx* c, const vxe_chunk_upload* ups, uint32_t n
   }
   vxe_status gst = grass_table_refresh(c, ups, n);
   if (gst != VXE_OK) return gst;
+  {
+    std::vector<uint32_t> slots;
+    slots.reserve(n);
+    for (uint32_t i = 0; i < n; ++i)
+      if (ups[i].slot < c->cfg.chunk_capacity) slots.push_back(ups[i].slot);
+    std::sort(slots.begin(), slots.end());
+    slots.erase(std::unique(slots.begin(), slots.end()), slots.end());
+    for (size_t i = 0; i < slots.size();) {  // one launch per run of consecutive slots
+      size_t j = i + 1;
+      while (j < slots.size() && slots[j] == slots[j - 1] + 1) ++j;
+      if ((gst = slot_lights_refresh(c, slots[i], (uint32_t)(j - i))) != VXE_OK) return gst;
+      i = j;
+    }
+  }
   CK(cudaEventRecord(c->upload_done, c->upload));
   c->upload_pending = true;
   c->upload_recorded = true;
@@ -969,6 +997,7 @@ vxe_status vxe_write_meta(vxe_ctx* c, uint32_t first, const vxe_chunk_meta* meta
   vxe_status ws = upload_after_readers(c);
   if (ws != VXE_OK) return ws;
   if (n && (ws = ring_copy(c, (char*)c->metas.p + (size_t)first * 48, metas, (size_t)n * 48)) != VXE_OK) return ws;
+  if ((ws = slot_lights_refresh(c, first, n)) != VXE_OK) return ws;
   // a slot's records follow its meta (origin, colinfo base)
   if (n && c->gt.valid) {
     if (c->gt.built_recorded) CK(cudaStreamWaitEvent(c->upload, c->gt.built, 0));
