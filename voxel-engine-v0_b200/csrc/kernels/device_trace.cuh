@@ -985,6 +985,11 @@ __device__ __forceinline__ LeafState descend_leaf_sparse(const Scene& s, v3 p, u
   return LeafState{false, INVALID, start_bmin, start_size, MAT_AIR, false, INVALID, V3s(0.0f), 0.0f};
 }
 
+__device__ __noinline__ LeafState descend_leaf_sparse_ool(const Scene& s, v3 p, uint32_t node_base, uint32_t start_idx,
+                                                         v3 start_bmin, float start_size) {
+  return descend_leaf_sparse(s, p, node_base, start_idx, start_bmin, start_size);
+}
+
 struct MacroDDAState {
   bool enabled;
   int32_t mx, my, mz, step_x, step_y, step_z;
@@ -1266,18 +1271,44 @@ __device__ __forceinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(co
   const float time_s = s.cam->voxel_params[1], strength = s.cam->voxel_params[2];
   bool have_leaf = false;
   LeafState leaf{};
+  // A descent chosen at the end of an air step (rope neighbour or anchor) is
+  // made at the top of the next iteration, at the same point, so that the walk
+  // has one descent site.
+  bool pend = false, pend_anchor = false;
+  uint32_t pend_idx = 0u;
+  v3 pend_bmin = V3s(0.0f);
+  float pend_size = 0.0f;
   const uint32_t MAX_ITERS = 128u + s.cam->chunk_size * 2u;
   for (uint32_t it = 0; it < MAX_ITERS; ++it) {
     if (tcur > t_exit) break;
     const v3 p = ro + rd * tcur;
     const v3 pq = p + ray_eps_vec(rd, 1e-4f * vs);
-    if (!have_leaf || !point_in_cube(pq, leaf.bmin, leaf.size)) {
-      if (an.valid && point_in_cube(pq, an.bmin, an.size))
-        leaf = descend_leaf_sparse(s, pq, ch.node_base, an.idx, an.bmin, an.size);
-      else
-        leaf = descend_leaf_sparse(s, pq, ch.node_base, 0u, rb, rs);
-      const AnchorNode na = anchor_from_leaf(s, leaf, ch.node_base);
-      if (na.valid && (!an.valid || na.key != an.key)) an = na;
+    // the pending descent, then (as after any descent) a re-descent from the
+    // anchor or the root when the leaf does not hold the point
+    for (uint32_t pass = 0; pass < 2u; ++pass) {
+      uint32_t si;
+      v3 sb;
+      float ss;
+      bool upd = true;
+      if (pend) {
+        si = pend_idx;
+        sb = pend_bmin;
+        ss = pend_size;
+        upd = pend_anchor;
+        pend = false;
+      } else if (!have_leaf || !point_in_cube(pq, leaf.bmin, leaf.size)) {
+        const bool use_an = an.valid && point_in_cube(pq, an.bmin, an.size);
+        si = use_an ? an.idx : 0u;
+        sb = use_an ? an.bmin : rb;
+        ss = use_an ? an.size : rs;
+      } else {
+        break;
+      }
+      leaf = descend_leaf_sparse(s, pq, ch.node_base, si, sb, ss);
+      if (upd) {
+        const AnchorNode na = anchor_from_leaf(s, leaf, ch.node_base);
+        if (na.valid && (!an.valid || na.key != an.key)) an = na;
+      }
       have_leaf = true;
     }
     const CubeSlab slab = cube_slab_inv(ro, inv, leaf.bmin, leaf.size);
@@ -1312,33 +1343,36 @@ __device__ __forceinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(co
       if (tcur > t_exit) break;
       if (ex.amb != 0u) { have_leaf = false; continue; }
       const uint32_t face = ex.face;
-      const v3 pn = ro + rd * tcur;
-      const v3 pqn = pn + ray_eps_vec(rd, 1e-4f * vs);
+      // the next point (ro + rd * tcur + nudge) is the next iteration's pq
       if (leaf.has_node) {
         const uint32_t nidx = rope_face(s, ch.node_base + leaf.idx_local, face);
         if (nidx == INVALID) { have_leaf = false; continue; }
-        const uint32_t nk = node_key(s, ch.node_base, nidx);
-        const v4 c = node_cube_from_key(rb, rs, nk);
-        leaf = descend_leaf_sparse(s, pqn, ch.node_base, nidx, V3(c.x, c.y, c.z), c.w);
-        const AnchorNode na = anchor_from_leaf(s, leaf, ch.node_base);
-        if (na.valid && (!an.valid || na.key != an.key)) an = na;
-        have_leaf = true;
+        const v4 c = node_cube_from_key(rb, rs, node_key(s, ch.node_base, nidx));
+        pend = true;
+        pend_anchor = true;
+        pend_idx = nidx;
+        pend_bmin = V3(c.x, c.y, c.z);
+        pend_size = c.w;
         continue;
       }
       if (leaf.has_anchor) {
+        const v3 pqn = (ro + rd * tcur) + ray_eps_vec(rd, 1e-4f * vs);
         if (point_in_cube(pqn, leaf.anchor_bmin, leaf.anchor_size)) {
-          leaf = descend_leaf_sparse(s, pqn, ch.node_base, leaf.anchor_idx, leaf.anchor_bmin, leaf.anchor_size);
-          have_leaf = true;
+          pend = true;
+          pend_anchor = false;
+          pend_idx = leaf.anchor_idx;
+          pend_bmin = leaf.anchor_bmin;
+          pend_size = leaf.anchor_size;
           continue;
         }
         const uint32_t nidx2 = rope_face(s, ch.node_base + leaf.anchor_idx, face);
         if (nidx2 == INVALID) { have_leaf = false; continue; }
-        const uint32_t nk2 = node_key(s, ch.node_base, nidx2);
-        const v4 c2 = node_cube_from_key(rb, rs, nk2);
-        leaf = descend_leaf_sparse(s, pqn, ch.node_base, nidx2, V3(c2.x, c2.y, c2.z), c2.w);
-        const AnchorNode na = anchor_from_leaf(s, leaf, ch.node_base);
-        if (na.valid && (!an.valid || na.key != an.key)) an = na;
-        have_leaf = true;
+        const v4 c2 = node_cube_from_key(rb, rs, node_key(s, ch.node_base, nidx2));
+        pend = true;
+        pend_anchor = true;
+        pend_idx = nidx2;
+        pend_bmin = V3(c2.x, c2.y, c2.z);
+        pend_size = c2.w;
         continue;
       }
       have_leaf = false;
@@ -1384,6 +1418,14 @@ __device__ __forceinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(co
     }
     tcur = fmax_(t_leave, tcur) + eps_step;
     have_leaf = false;
+  }
+  if (pend && pend_anchor) {
+    // the iteration limit ended the walk right after choosing a descent: the
+    // descent still updates the anchor the walk returns
+    const v3 pq = (ro + rd * tcur) + ray_eps_vec(rd, 1e-4f * vs);
+    const LeafState l2 = descend_leaf_sparse_ool(s, pq, ch.node_base, pend_idx, pend_bmin, pend_size);
+    const AnchorNode na = anchor_from_leaf(s, l2, ch.node_base);
+    if (na.valid && (!an.valid || na.key != an.key)) an = na;
   }
   return ChunkTraceResult{miss_hitgeom(), an.valid, an.key};
 }
