@@ -454,15 +454,16 @@ __device__ __noinline__ VoxTraceResult primary_trace(const Scene& s, const Frame
   }
   const float t_start = fmax_(t_hist - PRIMARY_HIT_MARGIN, 0.0f);
   const float t_end = fmin_(t_hist + PRIMARY_HIT_WINDOW, FOG_MAX_DIST);
-  if (hist_valid) {
-    ph.phase = 0u;
-    const VoxTraceResult h = trace_candidates(s, cslot, cmeta, c.ro, c.rd, t_start, t_end, hak != INVALID, hac, hak,
-                                              tile_count, ph);
-    if (h.best.hit != 0u) return h;
+  // phase 0: the hint window (when the history is valid); phase 1: the full
+  // trace when phase 0 found nothing.  One call site keeps one copy of the walk.
+  for (uint32_t phase = hist_valid ? 0u : 1u;; ++phase) {
+    const bool w = phase == 0u;
+    ph.phase = phase;
+    const VoxTraceResult h =
+        trace_candidates(s, cslot, cmeta, c.ro, c.rd, w ? t_start : 0.0f, w ? t_end : FOG_MAX_DIST,
+                         w && hak != INVALID, w ? hac : i3{0, 0, 0}, w ? hak : INVALID, tile_count, ph);
+    if (!w || h.best.hit != 0u) return h;
   }
-  ph.phase = 1u;
-  return trace_candidates(s, cslot, cmeta, c.ro, c.rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID, tile_count,
-                          ph);
 }
 
 // main_local_taa (taa.wgsl:26-69) for one pixel, fused after its shading.
