@@ -1255,6 +1255,33 @@ __device__ __forceinline__ void probe_record(ProbeHook& ph, float t0, float t1, 
   }
 }
 
+// The blades on top of a grass voxel the walk hit at (t, n)
+// (chunk_trace.wgsl:917-950): the cell from the hit point, corrected by the
+// column's colinfo top, then its grass slab from just before the hit.
+__device__ __noinline__ GrassHit grass_on_voxel_hit(const Scene& s, v3 ro, v3 rd, const Meta& ch, float t, v3 n,
+                                                    float t_enter, float t_exit) {
+  const float vs = vs_(s);
+  const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vs;
+  const i3 ov{ch.ox, ch.oy, ch.oz};
+  const v3 hp = ro + rd * t;
+  GrassCell cell = pick_grass_cell_in_chunk_with_bias(hp, n, rb, ov, vs, (int32_t)s.cam->chunk_size);
+  if (ch.colinfo_base != INVALID) {
+    int32_t lx = to_i32(floorf((hp.x - rb.x) / vs)), lz = to_i32(floorf((hp.z - rb.z) / vs));
+    lx = clampi(lx, 0, 63);
+    lz = clampi(lz, 0, 63);
+    const ColInfo ci = colinfo_decode(colinfo_entry_u16(s, ch.colinfo_base, (uint32_t)lx, (uint32_t)lz));
+    if (ci.valid && ci.mat == MAT_GRASS) {
+      const v3 id = V3((float)(ov.x + lx), (float)(ov.y + (int32_t)ci.y_vox), (float)(ov.z + lz));
+      cell = GrassCell{id * vs, id};
+    }
+  }
+  const float pad = (GRASS_LAYER_HEIGHT_VOX + 1.0f) * vs;
+  const float tmn = fmax_(t_enter, t - 0.01f * vs);
+  const float tmx = fmin_(t + pad, t_exit + pad);
+  return try_grass_slab_hit(s, ro, rd, tmn, tmx, cell.bmin_m, cell.id_vox, vs, s.cam->voxel_params[1],
+                            s.cam->voxel_params[2]);
+}
+
 __device__ __forceinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(const Scene& s, v3 ro, v3 rd, v3 inv, const Meta& ch,
                                                    float t_enter, float t_exit, bool use_anchor,
                                                    uint32_t anchor_key, const TraceOpts& opt, ProbeHook& ph) {
@@ -1344,18 +1371,12 @@ __device__ __forceinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(co
       if (ex.amb != 0u) { have_leaf = false; continue; }
       const uint32_t face = ex.face;
       // the next point (ro + rd * tcur + nudge) is the next iteration's pq
-      if (leaf.has_node) {
-        const uint32_t nidx = rope_face(s, ch.node_base + leaf.idx_local, face);
-        if (nidx == INVALID) { have_leaf = false; continue; }
-        const v4 c = node_cube_from_key(rb, rs, node_key(s, ch.node_base, nidx));
-        pend = true;
-        pend_anchor = true;
-        pend_idx = nidx;
-        pend_bmin = V3(c.x, c.y, c.z);
-        pend_size = c.w;
+      if (!leaf.has_node && !leaf.has_anchor) {
+        have_leaf = false;
         continue;
       }
-      if (leaf.has_anchor) {
+      if (!leaf.has_node) {
+        // an implicit air leaf: back into its anchor when the point is there
         const v3 pqn = (ro + rd * tcur) + ray_eps_vec(rd, 1e-4f * vs);
         if (point_in_cube(pqn, leaf.anchor_bmin, leaf.anchor_size)) {
           pend = true;
@@ -1365,17 +1386,16 @@ __device__ __forceinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(co
           pend_size = leaf.anchor_size;
           continue;
         }
-        const uint32_t nidx2 = rope_face(s, ch.node_base + leaf.anchor_idx, face);
-        if (nidx2 == INVALID) { have_leaf = false; continue; }
-        const v4 c2 = node_cube_from_key(rb, rs, node_key(s, ch.node_base, nidx2));
-        pend = true;
-        pend_anchor = true;
-        pend_idx = nidx2;
-        pend_bmin = V3(c2.x, c2.y, c2.z);
-        pend_size = c2.w;
-        continue;
       }
-      have_leaf = false;
+      // the rope of the leaf's node, or of the implicit leaf's anchor
+      const uint32_t nidx = rope_face(s, ch.node_base + (leaf.has_node ? leaf.idx_local : leaf.anchor_idx), face);
+      if (nidx == INVALID) { have_leaf = false; continue; }
+      const v4 c = node_cube_from_key(rb, rs, node_key(s, ch.node_base, nidx));
+      pend = true;
+      pend_anchor = true;
+      pend_idx = nidx;
+      pend_bmin = V3(c.x, c.y, c.z);
+      pend_size = c.w;
       continue;
     }
     if (leaf.mat == MAT_LEAF && !opt.geom_only) {
@@ -1394,22 +1414,7 @@ __device__ __forceinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(co
     if (bh.hit) {
       const uint32_t nd = ch.node_base + leaf.idx_local;
       if (!opt.geom_only && leaf.mat == MAT_GRASS) {
-        const v3 hp = ro + rd * bh.t;
-        GrassCell cell = pick_grass_cell_in_chunk_with_bias(hp, bh.n, rb, ov, vs, (int32_t)s.cam->chunk_size);
-        if (ch.colinfo_base != INVALID) {
-          int32_t lx = to_i32(floorf((hp.x - rb.x) / vs)), lz = to_i32(floorf((hp.z - rb.z) / vs));
-          lx = clampi(lx, 0, 63);
-          lz = clampi(lz, 0, 63);
-          const ColInfo ci = colinfo_decode(colinfo_entry_u16(s, ch.colinfo_base, (uint32_t)lx, (uint32_t)lz));
-          if (ci.valid && ci.mat == MAT_GRASS) {
-            const v3 id = V3((float)(ov.x + lx), (float)(ov.y + (int32_t)ci.y_vox), (float)(ov.z + lz));
-            cell = GrassCell{id * vs, id};
-          }
-        }
-        const float pad = (GRASS_LAYER_HEIGHT_VOX + 1.0f) * vs;
-        const float tmn = fmax_(t_enter, bh.t - 0.01f * vs);
-        const float tmx = fmin_(bh.t + pad, t_exit + pad);
-        const GrassHit gh = try_grass_slab_hit(s, ro, rd, tmn, tmx, cell.bmin_m, cell.id_vox, vs, time_s, strength);
+        const GrassHit gh = grass_on_voxel_hit(s, ro, rd, ch, bh.t, bh.n, t_enter, t_exit);
         if (gh.hit)
           return ChunkTraceResult{make_hit(MAT_GRASS, gh.t, gh.n, rb, rs, ch, nd, leaf.bmin, leaf.size), an.valid,
                                   an.key};
@@ -1449,6 +1454,7 @@ __device__ __forceinline__ ChunkTraceResult trace_chunk_interval_stream_macro(co
   const bool whole = !ms.enabled;
   for (uint32_t i = 0; i < 128u; ++i) {
     float seg_end = t_end, cell_exit = t_end;
+    bool empty = false;
     if (!whole) {
       if (tcur >= t_end) break;
       macro_dda_sync(ms, tcur);
@@ -1456,17 +1462,16 @@ __device__ __forceinline__ ChunkTraceResult trace_chunk_interval_stream_macro(co
       if (!st.valid) break;
       cell_exit = st.t_exit;
       seg_end = fmin_(st.t_exit, t_end);
-      if (st.empty) {
-        tcur = seg_end + eps_step;
-        if (ms.enabled && tcur >= st.t_exit) macro_dda_step(ms);
-        continue;
-      }
+      empty = st.empty;
     }
-    const ChunkTraceResult h =
-        trace_chunk_rope_interval_nomacro(s, ro, rd, inv, ch, tcur, seg_end, anchor_valid, anchor_key, opt, ph);
-    if (whole || h.hit.hit != 0u) return h;
-    anchor_valid = h.anchor_valid;
-    anchor_key = h.anchor_key;
+    if (!empty) {
+      const ChunkTraceResult h =
+          trace_chunk_rope_interval_nomacro(s, ro, rd, inv, ch, tcur, seg_end, anchor_valid, anchor_key, opt, ph);
+      if (whole || h.hit.hit != 0u) return h;
+      anchor_valid = h.anchor_valid;
+      anchor_key = h.anchor_key;
+    }
+    // on to the next macro cell (an empty cell is skipped whole)
     tcur = seg_end + eps_step;
     if (ms.enabled && tcur >= cell_exit) macro_dda_step(ms);
   }
