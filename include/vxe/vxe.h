@@ -358,7 +358,10 @@ vxe_status vxe_view_destroy(vxe_ctx* ctx, vxe_view* view);
  * grass_cells the per-frame grass cell table, which `tiles` includes. */
 typedef struct vxe_timings {
   double primary, local_taa, godray, composite, composite_taa, tiles, total;
-  double primary_trace, grass_cells;
+  /* extras: the trace stage of the wavefront schedule (walk, probe column
+   * DDAs, slab marches, pick, resolve), the grass table build, and the walk
+   * kernel (k_primary_trace) alone */
+  double primary_trace, grass_cells, trace_kernel;
 } vxe_timings;
 vxe_status vxe_get_timings(vxe_ctx* ctx, vxe_timings* out);
 

@@ -74,8 +74,9 @@ struct FrameState {
   DevBuf img[IMG_N];
   uint32_t iw = 0, ih = 0, pw = 0, ph = 0;
   int ping = 0;
-  // frame events: start, grass table, tiles, trace, shading, godray, composite
-  cudaEvent_t ev[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  // frame events: start, grass table, tiles, trace, shading, godray, composite,
+  // then the walk kernel's own start and end
+  cudaEvent_t ev[9] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   bool timed = false, timed_trace = false;
   // the frame as a captured CUDA graph
   cudaGraph_t fgraph = nullptr;
@@ -551,7 +552,9 @@ vxe_status frame_enqueue(vxe_ctx* c, FrameState& F, const FrameArgs& A, bool tim
     CK(cudaMemsetAsync(A.q_count, 0, 32, st));
     CK(cudaMemsetAsync(A.px_first, 0xFF, (size_t)npix * 8u, st));
     CK(cudaMemsetAsync(A.px_mask, 0, (size_t)npix * 8u, st));
+    if (timed) CK(cudaEventRecord(F.ev[7], st));
     k_primary_trace<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, st>>>(A);
+    if (timed) CK(cudaEventRecord(F.ev[8], st));
     k_probe_dda<<<grid((uint64_t)npix * kProbesPerPixel), SHADE_THREADS, 0, st>>>(A);
     k_slab_eval<<<grid((uint64_t)npix * kSlabsPerPixel), SHADE_THREADS, 0, st>>>(A);
     k_slab_pick<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
@@ -1108,6 +1111,11 @@ vxe_status vxe_get_timings(vxe_ctx* c, vxe_timings* t) {
   t->grass_cells = ms[0];
   t->tiles = (double)ms[0] + ms[1];
   t->primary_trace = c->fr.timed_trace ? ms[2] : 0.0;
+  if (c->fr.timed_trace) {
+    float mk = 0.0f;
+    CK(cudaEventElapsedTime(&mk, c->fr.ev[7], c->fr.ev[8]));
+    t->trace_kernel = mk;
+  }
   t->primary = (double)ms[2] + ms[3];
   t->godray = ms[4];
   t->composite = ms[5];

@@ -110,7 +110,7 @@ class Hit(C.Structure):
 
 class Timings(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("primary", "local_taa", "godray", "composite", "composite_taa", "tiles",
-                                           "total", "primary_trace", "grass_cells")]
+                                           "total", "primary_trace", "grass_cells", "trace_kernel")]
 
 
 class WorldParams(C.Structure):
