@@ -157,7 +157,7 @@ __device__ __noinline__ VoxTraceResult viewport_trace(const Scene& s, const uint
   VoxTraceResult vt{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
   ph.best_cand = INVALID;
   if (s.cam->chunk_count != 0u && cnt != 0u)
-    vt = trace_candidates(s, tile_slots + tile * TILE_CANDS, nullptr, ro, rd, 0.0f, FOG_MAX_DIST, false,
+    vt = trace_candidates<PROBE_DYNAMIC>(s, tile_slots + tile * TILE_CANDS, nullptr, ro, rd, 0.0f, FOG_MAX_DIST, false,
                           i3{0, 0, 0}, INVALID, cnt, ph);
   return vt;
 }

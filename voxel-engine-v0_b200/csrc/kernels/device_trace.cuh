@@ -1185,6 +1185,9 @@ __device__ __forceinline__ HitGeom make_hit(uint32_t mat, float t, v3 n, v3 rb, 
 // fallback).
 // ---------------------------------------------------------------------------
 enum : uint32_t { PROBE_INLINE = 0u, PROBE_RECORD = 1u };
+// The walk functions take the mode as a template argument (PM) so that a
+// kernel holds only the probe code it runs; PROBE_DYNAMIC reads ph.mode.
+constexpr uint32_t PROBE_DYNAMIC = 2u;
 
 struct ProbeRec {  // 56 B
   uint32_t pixel, seq, slot;
@@ -1282,6 +1285,7 @@ __device__ __noinline__ GrassHit grass_on_voxel_hit(const Scene& s, v3 ro, v3 rd
                             s.cam->voxel_params[2]);
 }
 
+template <uint32_t PM>
 __device__ __forceinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(const Scene& s, v3 ro, v3 rd, v3 inv, const Meta& ch,
                                                    float t_enter, float t_exit, bool use_anchor,
                                                    uint32_t anchor_key, const TraceOpts& opt, ProbeHook& ph) {
@@ -1351,7 +1355,8 @@ __device__ __forceinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(co
           const float t1p = fmin_(t_leave, t_exit);
           if (t1p >= t0p) {
             GrassHit gh{false, BIG, V3s(0.0f)};
-            if (ph.mode == PROBE_RECORD)
+            const bool rec = PM == PROBE_DYNAMIC ? ph.mode == PROBE_RECORD : PM == PROBE_RECORD;
+            if (rec)
               probe_record(ph, t0p, t1p, leaf.has_node ? ch.node_base + leaf.idx_local : INVALID, leaf.bmin,
                            leaf.size, an.valid, an.key);
             else
@@ -1435,6 +1440,7 @@ __device__ __forceinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(co
   return ChunkTraceResult{miss_hitgeom(), an.valid, an.key};
 }
 
+template <uint32_t PM>
 __device__ __forceinline__ ChunkTraceResult trace_chunk_interval_stream_macro(const Scene& s, v3 ro, v3 rd, v3 inv, const Meta& ch,
                                                    float t0_in, float t1_in, bool use_anchor, uint32_t anchor_key_in,
                                                    const TraceOpts& opt, ProbeHook& ph) {  // chunk_trace.wgsl:592-667
@@ -1466,7 +1472,7 @@ __device__ __forceinline__ ChunkTraceResult trace_chunk_interval_stream_macro(co
     }
     if (!empty) {
       const ChunkTraceResult h =
-          trace_chunk_rope_interval_nomacro(s, ro, rd, inv, ch, tcur, seg_end, anchor_valid, anchor_key, opt, ph);
+          trace_chunk_rope_interval_nomacro<PM>(s, ro, rd, inv, ch, tcur, seg_end, anchor_valid, anchor_key, opt, ph);
       if (whole || h.hit.hit != 0u) return h;
       anchor_valid = h.anchor_valid;
       anchor_key = h.anchor_key;

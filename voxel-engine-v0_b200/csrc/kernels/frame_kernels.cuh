@@ -267,6 +267,7 @@ __global__ void __launch_bounds__(TILE_THREADS) k_tiles(const __grid_constant__ 
 
 // trace_scene_voxels_candidates (chunk_trace.wgsl:1177-1265) over a tile list
 // staged in shared memory (slots + their ChunkMeta records).
+template <uint32_t PM>
 __device__ VoxTraceResult trace_candidates(const Scene& s, const uint32_t* cslot, const Meta* cmeta, v3 ro, v3 rd,
                                            float t_min, float t_max, bool anchor_valid_in, i3 anchor_chunk_in,
                                            uint32_t anchor_key_in, uint32_t cand_count, ProbeHook& ph) {
@@ -308,7 +309,7 @@ __device__ VoxTraceResult trace_candidates(const Scene& s, const uint32_t* cslot
     const uint32_t aku = ua ? anchor_key_in : INVALID;
     ph.slot = slot;
     ph.cand = i;
-    const ChunkTraceResult h = trace_chunk_interval_stream_macro(s, ro, rd, inv, ch, ce, cx, ua, aku, opt, ph);
+    const ChunkTraceResult h = trace_chunk_interval_stream_macro<PM>(s, ro, rd, inv, ch, ce, cx, ua, aku, opt, ph);
     if (h.hit.hit != 0u && h.hit.t < best.t) {
       best = h.hit;
       bav = h.anchor_valid;
@@ -418,6 +419,7 @@ __device__ __forceinline__ PrimaryCtx primary_ctx(const Scene& s, uint32_t gx, u
 }
 
 // History hint + voxel trace (ray_main.wgsl:274-325 and trace_primary_voxels :116-161).
+template <uint32_t PM>
 __device__ __noinline__ VoxTraceResult primary_trace(const Scene& s, const FrameArgs& A, const PrimaryCtx& c,
                                                      const uint32_t* cslot, const Meta* cmeta, uint32_t tile_count,
                                                      ProbeHook& ph) {
@@ -460,7 +462,7 @@ __device__ __noinline__ VoxTraceResult primary_trace(const Scene& s, const Frame
     const bool w = phase == 0u;
     ph.phase = phase;
     const VoxTraceResult h =
-        trace_candidates(s, cslot, cmeta, c.ro, c.rd, w ? t_start : 0.0f, w ? t_end : FOG_MAX_DIST,
+        trace_candidates<PM>(s, cslot, cmeta, c.ro, c.rd, w ? t_start : 0.0f, w ? t_end : FOG_MAX_DIST,
                          w && hak != INVALID, w ? hac : i3{0, 0, 0}, w ? hak : INVALID, tile_count, ph);
     if (!w || h.best.hit != 0u) return h;
   }
@@ -652,7 +654,7 @@ __global__ void __launch_bounds__(PRIMARY_THREADS) k_primary(const __grid_consta
   if (!block_pixel(A, &t, &gx, &gy)) return;
   const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
   ProbeHook ph = probe_hook_inline();
-  const VoxTraceResult vt = primary_trace(s, A, c, cslot[t], cmeta[t], ccount[t], ph);
+  const VoxTraceResult vt = primary_trace<PROBE_INLINE>(s, A, c, cslot[t], cmeta[t], ccount[t], ph);
   if (vt.in_grid && vt.best.hit != 0u) shade_voxel_pixel(s, A, c, vt.best, vt.anchor_valid, vt.anchor_key, vt.anchor_chunk);
   else shade_far_pixel(s, A, c);
 }
@@ -719,7 +721,7 @@ __global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace(const __grid_
     ph.recs = A.probe_recs;
     ph.rec_count = &A.q_count[4];
     ph.rec_cap = A.probe_cap;
-    const VoxTraceResult vt = primary_trace(s, A, c, cslot[t], cmeta[t], ccount[t], ph);
+    const VoxTraceResult vt = primary_trace<PROBE_RECORD>(s, A, c, cslot[t], cmeta[t], ccount[t], ph);
     vox = vt.in_grid && vt.best.hit != 0u;
     if (vox) store_pixhit(A.pix_hit + (size_t)pix * 5u, vt.best, vt);
     pend = ph.seq != 0u;
@@ -870,7 +872,7 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_primary_resolve(const __grid_
         const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
         const size_t tile = (size_t)(gy >> 3) * tiles_x + (gx >> 3);
         ProbeHook ph = probe_hook_inline();
-        const VoxTraceResult vt = primary_trace(s, A, c, A.tile_slots + tile * TILE_CANDS, nullptr,
+        const VoxTraceResult vt = primary_trace<PROBE_INLINE>(s, A, c, A.tile_slots + tile * TILE_CANDS, nullptr,
                                                 A.tile_count[tile], ph);
         vox = vt.in_grid && vt.best.hit != 0u;
         if (vox) store_pixhit(A.pix_hit + (size_t)pix * 5u, vt.best, vt);
@@ -1261,7 +1263,8 @@ __device__ __forceinline__ HitRec trace_query_ray(const Scene& s, v3 ro, v3 rd, 
     const float ce = fmax_(rt.x, 0.0f), cx = fmin_(rt.y, fmin_(tmax, FOG_MAX_DIST));
     if (cx < ce) return false;
     ProbeHook ph = probe_hook_inline();
-    const ChunkTraceResult h = trace_chunk_interval_stream_macro(s, ro, rd, inv, ch, ce, cx, false, INVALID, opt, ph);
+    const ChunkTraceResult h =
+        trace_chunk_interval_stream_macro<PROBE_INLINE>(s, ro, rd, inv, ch, ce, cx, false, INVALID, opt, ph);
     if (h.hit.hit != 0u) {
       best = h.hit;
       return true;

@@ -1810,8 +1810,8 @@ __global__ void __launch_bounds__(vxe::dev::PRIMARY_THREADS) k_hits_noalloc(cons
   VoxTraceResult vt{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
   ProbeHook ph = probe_hook_inline();
   if (s.cam->chunk_count != 0u && ccount[t] != 0u)
-    vt = trace_candidates(s, cslot[t], cmeta[t], ro, rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID, ccount[t],
-                          ph);
+    vt = trace_candidates<PROBE_INLINE>(s, cslot[t], cmeta[t], ro, rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID,
+                                        ccount[t], ph);
   HitRec rec = miss_rec();
   if (vt.in_grid && vt.best.hit != 0u) {
     HitGeom best = vt.best;
