@@ -62,7 +62,7 @@ struct FrameArgs {
   uint32_t* q_vox;    // pixel ids with a voxel hit
   uint32_t* q_far;    // pixel ids for heightfield / sky
   uint32_t* q_count;  // [0] voxel, [1] far, [2] fresh shadow, [3] light gather, [4] probes, [5] pending,
-                      // [6] slab tasks, [7] slab hits
+                      // [6] slab tasks, [7] slab hits, [8] far pixels queued by the walk
   uint32_t* q_shadow;  // voxel pixels that trace a fresh sun shadow this frame
   uint32_t* q_light;   // voxel pixels that gather local lights
   float* px_shadow;    // fresh sun transmittance per pixel (q_shadow pixels)
@@ -1004,10 +1004,15 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_shade_vox(const __grid_consta
   }
 }
 
+// PART 0: the far pixels the walk queued (q_count[8], copied right after the
+// walk), shaded while the grass probes resolve; PART 1: those the resolve
+// queued after them; PART 2: the whole queue.
+template <int PART>
 __global__ void __launch_bounds__(SHADE_THREADS) k_shade_far(const __grid_constant__ FrameArgs A) {
   const Scene s = make_scene(A, false);
-  const uint32_t n = A.q_count[1];
-  for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < n; i += gridDim.x * SHADE_THREADS) {
+  const uint32_t first = PART == 1 ? A.q_count[8] : 0u;
+  const uint32_t n = PART == 0 ? A.q_count[8] : A.q_count[1];
+  for (uint32_t i = first + blockIdx.x * SHADE_THREADS + threadIdx.x; i < n; i += gridDim.x * SHADE_THREADS) {
     const uint32_t pix = A.q_far[i];
     const PrimaryCtx c = primary_ctx(s, pix % A.iw, pix / A.iw, A.iw);
     shade_far_pixel(s, A, c);

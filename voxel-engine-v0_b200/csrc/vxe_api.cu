@@ -85,8 +85,16 @@ struct FrameState {
   uint64_t fgraph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 };
 
+// A second stream a frame forks to (far-pixel shading beside the probe
+// resolve and the voxel shading) and joins back before the godray pass.
+struct SideStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t fork = nullptr, mid = nullptr, join = nullptr;
+};
+
 struct BatchLane {
   cudaStream_t stream = nullptr;
+  SideStream side;
   DevBuf hdr, reqs, cams, tile_count, tile_slots, head;
   // deferred grass probes of viewport rays: per-ray arrays for ray_cap rays,
   // probe records and slab tasks in proportion, counters
@@ -124,6 +132,7 @@ struct vxe_ctx {
   DevBuf slot_lights;  // per slot: holds a LIGHT leaf (k_slot_lights)
   GrassTable gt;
   FrameState fr;  // the context's own frame
+  SideStream side;  // its fork stream
   vxe_camera_gpu cam{};
   vxe_clipmap_gpu clip{};
   // query scratch
@@ -270,7 +279,7 @@ size_t img_bytes(const FrameState& F, int i) {
     case IMG_PXLIGHT:
       return in * 16;
     case IMG_QCOUNT:
-      return 32;
+      return 64;
     default:
       return 0;
   }
@@ -531,7 +540,25 @@ void frame_fill(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& cam, FrameArgs&
 
 // The frame's launches on the compute stream (captured as-is by the graph
 // path; `timed` adds the per-pass events).
-vxe_status frame_enqueue(vxe_ctx* c, FrameState& F, const FrameArgs& A, bool timed, cudaStream_t st) {
+vxe_status side_ready(vxe_ctx* c, SideStream& S) {
+  if (S.s) return VXE_OK;
+  CK(cudaStreamCreateWithFlags(&S.s, cudaStreamNonBlocking));
+  for (cudaEvent_t* e : {&S.fork, &S.mid, &S.join}) CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  return VXE_OK;
+}
+
+void side_release(SideStream& S) {
+  if (S.s) {
+    cudaStreamSynchronize(S.s);
+    cudaStreamDestroy(S.s);
+  }
+  for (cudaEvent_t e : {S.fork, S.mid, S.join})
+    if (e) cudaEventDestroy(e);
+  S = SideStream{};
+}
+
+vxe_status frame_enqueue(vxe_ctx* c, FrameState& F, const FrameArgs& A, bool timed, cudaStream_t st,
+                         SideStream* side) {
   const uint32_t tiles_x = (F.iw + 7) / 8, tiles_y = (F.ih + 7) / 8;
   const uint32_t tiles = tiles_x * tiles_y;
   const uint32_t npix = F.iw * F.ih;
@@ -549,22 +576,39 @@ vxe_status frame_enqueue(vxe_ctx* c, FrameState& F, const FrameArgs& A, bool tim
       return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((threads + SHADE_THREADS - 1) / SHADE_THREADS,
                                                                 (uint64_t)c->shade_wave));
     };
-    CK(cudaMemsetAsync(A.q_count, 0, 32, st));
+    CK(cudaMemsetAsync(A.q_count, 0, 64, st));
+    vxe_status sr;
+    if (side && (sr = side_ready(c, *side)) != VXE_OK) return sr;
     CK(cudaMemsetAsync(A.px_first, 0xFF, (size_t)npix * 8u, st));
     CK(cudaMemsetAsync(A.px_mask, 0, (size_t)npix * 8u, st));
     if (timed) CK(cudaEventRecord(F.ev[7], st));
     k_primary_trace<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, st>>>(A);
     if (timed) CK(cudaEventRecord(F.ev[8], st));
+    if (side) {  // the walk's far pixels shade beside the probe passes
+      CK(cudaMemcpyAsync(A.q_count + 8, A.q_count + 1, 4, cudaMemcpyDeviceToDevice, st));
+      CK(cudaEventRecord(side->fork, st));
+      CK(cudaStreamWaitEvent(side->s, side->fork, 0));
+      k_shade_far<0><<<grid(npix), SHADE_THREADS, 0, side->s>>>(A);
+    }
     k_probe_dda<<<grid((uint64_t)npix * kProbesPerPixel), SHADE_THREADS, 0, st>>>(A);
     k_slab_eval<<<grid((uint64_t)npix * kSlabsPerPixel), SHADE_THREADS, 0, st>>>(A);
     k_slab_pick<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
     k_primary_resolve<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
     if (timed) CK(cudaEventRecord(F.ev[3], st));
+    if (side) {  // the far pixels the resolve queued, beside the voxel shading
+      CK(cudaEventRecord(side->mid, st));
+      CK(cudaStreamWaitEvent(side->s, side->mid, 0));
+      k_shade_far<1><<<grid(npix), SHADE_THREADS, 0, side->s>>>(A);
+      CK(cudaEventRecord(side->join, side->s));
+    }
     k_shade_prep<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
     k_shade_shadow<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
     k_shade_lights<<<grid((uint64_t)npix * 8u), SHADE_THREADS, 0, st>>>(A);
     k_shade_vox<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
-    k_shade_far<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
+    if (side)
+      CK(cudaStreamWaitEvent(st, side->join, 0));
+    else
+      k_shade_far<2><<<grid(npix), SHADE_THREADS, 0, st>>>(A);
   }
   if (timed) CK(cudaEventRecord(F.ev[4], st));
   k_godray<<<dim3((F.iw + POST_THREADS_X - 1) / POST_THREADS_X, (F.ih + POST_THREADS_Y - 1) / POST_THREADS_Y),
@@ -587,7 +631,7 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
   bool use_grass = false;
   if ((st = grass_table_acquire(c, c->compute, 0, c->cam, &use_grass)) != VXE_OK) return st;
   if (use_grass) grass_table_args(c, A);
-  if ((st = frame_enqueue(c, c->fr, A, timed, c->compute)) != VXE_OK) return st;
+  if ((st = frame_enqueue(c, c->fr, A, timed, c->compute, &c->side)) != VXE_OK) return st;
   if (use_grass && (st = grass_table_release(c, c->compute, 0)) != VXE_OK) return st;
   c->fr.timed = timed;
   c->fr.timed_trace = timed && !(c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL);
@@ -618,8 +662,9 @@ vxe_status launch_frame_graph(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& c
     F.fgraph_exec = nullptr;
     F.fgraph = nullptr;
     F.fgraph_nodes.clear();
+    if (st == c->compute && (rc = side_ready(c, c->side)) != VXE_OK) return rc;  // created outside the capture
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    rc = frame_enqueue(c, F, A, false, st);
+    rc = frame_enqueue(c, F, A, false, st, st == c->compute ? &c->side : nullptr);
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(st, &g);
     if (rc != VXE_OK) {
@@ -781,6 +826,7 @@ void vxe_destroy(vxe_ctx* c) {
       release(*b, L.stream);
     release_frame_state(L.scratch, L.stream);
     if (L.stream) cudaStreamSynchronize(L.stream);
+    side_release(L.side);
     if (L.graph) cudaGraphExecDestroy(L.graph);
     if (L.stage) cudaFreeHost(L.stage);
     for (auto& e : L.ev)
@@ -806,6 +852,7 @@ void vxe_destroy(vxe_ctx* c) {
   for (auto& e : c->gt.reader)
     if (e) cudaEventDestroy(e);
   if (c->upload_done) cudaEventDestroy(c->upload_done);
+  side_release(c->side);
   if (c->compute) cudaStreamDestroy(c->compute);
   if (c->upload) cudaStreamDestroy(c->upload);
   delete c;
@@ -1684,7 +1731,7 @@ vxe_status vxe_view_render_async(vxe_ctx* c, vxe_view* v, uint32_t lane, const v
   const int reader = 1 + (int)lane;
   if ((st = grass_table_acquire(c, L.stream, reader, vc, &use_grass)) != VXE_OK) return st;
   if (use_grass) grass_table_args(c, A);
-  if ((st = frame_enqueue(c, v->fr, A, false, L.stream)) != VXE_OK) return st;
+  if ((st = frame_enqueue(c, v->fr, A, false, L.stream, &L.side)) != VXE_OK) return st;
   if (use_grass && (st = grass_table_release(c, L.stream, reader)) != VXE_OK) return st;
   v->fr.ping = 1 - v->fr.ping;
   CK(cudaEventRecord(L.ev[1], L.stream));
