@@ -146,7 +146,8 @@ __device__ __forceinline__ uint32_t find_req(const BatchReq* reqs, uint32_t n, u
   return lo;
 }
 
-// Voxel trace of one cold viewport pixel (no history hint).
+// Voxel trace of one cold viewport pixel (no history hint); PM the probe mode.
+template <uint32_t PM>
 __device__ __noinline__ VoxTraceResult viewport_trace(const Scene& s, const uint32_t* tile_count,
                                                       const uint32_t* tile_slots, uint32_t tiles_x, uint32_t gx,
                                                       uint32_t gy, ProbeHook& ph) {
@@ -157,7 +158,7 @@ __device__ __noinline__ VoxTraceResult viewport_trace(const Scene& s, const uint
   VoxTraceResult vt{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
   ph.best_cand = INVALID;
   if (s.cam->chunk_count != 0u && cnt != 0u)
-    vt = trace_candidates<PROBE_DYNAMIC>(s, tile_slots + tile * TILE_CANDS, nullptr, ro, rd, 0.0f, FOG_MAX_DIST, false,
+    vt = trace_candidates<PM>(s, tile_slots + tile * TILE_CANDS, nullptr, ro, rd, 0.0f, FOG_MAX_DIST, false,
                           i3{0, 0, 0}, INVALID, cnt, ph);
   return vt;
 }
@@ -215,7 +216,7 @@ __device__ __forceinline__ HitRec viewport_finish(const Scene& s, uint32_t gx, u
 __device__ __forceinline__ HitRec viewport_pixel_hit(const Scene& s, const uint32_t* tile_count,
                                                      const uint32_t* tile_slots, uint32_t tiles_x, uint32_t gx,
                                                      uint32_t gy, ProbeHook& ph) {
-  const VoxTraceResult vt = viewport_trace(s, tile_count, tile_slots, tiles_x, gx, gy, ph);
+  const VoxTraceResult vt = viewport_trace<PROBE_INLINE>(s, tile_count, tile_slots, tiles_x, gx, gy, ph);
   return viewport_finish(s, gx, gy, vt.in_grid && vt.best.hit != 0u, vt.best);
 }
 
@@ -275,7 +276,9 @@ __device__ __forceinline__ void batch_finish(const BatchArgs& B, const Scene& s,
   }
 }
 
-// Processes one work item with the calling warp.
+// Processes one work item with the calling warp; DEFER: viewport rays record
+// their grass probes for the deferred passes (else they probe inline).
+template <bool DEFER>
 __device__ __forceinline__ void batch_item(const BatchArgs& B, const BatchHeader& H, const BatchReq& q,
                                            const Scene& s, uint32_t local, uint32_t lane) {
   if (q.kind == 0u) {
@@ -286,17 +289,17 @@ __device__ __forceinline__ void batch_item(const BatchArgs& B, const BatchHeader
       if (gx >= q.w || gy >= q.h) continue;
       ProbeHook ph = probe_hook_inline();
       const uint32_t ray = q.ray_base + gy * q.w + gx;
-      if (B.defer) {
+      if (DEFER) {
         ph.mode = PROBE_RECORD;
         ph.pixel = ray;
         ph.recs = B.probe_recs;
         ph.rec_count = &B.dcount[0];
         ph.rec_cap = B.probe_cap;
       }
-      const VoxTraceResult vt = viewport_trace(s, B.tile_count + q.tile_base,
+      const VoxTraceResult vt = viewport_trace<DEFER ? PROBE_RECORD : PROBE_INLINE>(s, B.tile_count + q.tile_base,
                                                B.tile_slots + (size_t)q.tile_base * TILE_CANDS, q.tiles_x, gx, gy, ph);
       const bool vox = vt.in_grid && vt.best.hit != 0u;
-      if (!B.defer) {
+      if (!DEFER) {
         store_rec_at(q.out, (size_t)gy * q.w + gx, viewport_finish(s, gx, gy, vox, vt.best));
       } else if (ph.seq != 0u) {  // met probes: k_batch_resolve decides
         if (vox) store_hitgeom(B.px_hit + (size_t)ray * 4u, vt.best);
@@ -341,6 +344,8 @@ __device__ __forceinline__ void batch_sorted_queries(const BatchArgs& B, const B
 
 // The persistent work-queue kernel (plain = 0) or one request per launch
 // with one warp per item (plain = 1, the per-request baseline).
+// DEFER must equal B.defer (one instantiation per probe mode).
+template <bool DEFER>
 __global__ void __launch_bounds__(BATCH_THREADS) k_batch_trace(const __grid_constant__ BatchArgs B) {
   __shared__ vxe_camera_gpu wcam[BATCH_THREADS / 32];
   __shared__ uint32_t wcam_id[BATCH_THREADS / 32];
@@ -365,7 +370,7 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_trace(const __grid_cons
     if (local >= n_local) return;
     load_cam(q.cam);
     const Scene s = batch_scene(B, &wcam[warp]);
-    batch_item(B, H, q, s, local, lane);
+    batch_item<DEFER>(B, H, q, s, local, lane);
     return;
   }
   for (;;) {
@@ -381,7 +386,7 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_trace(const __grid_cons
     const BatchReq q = B.reqs[r];
     load_cam(q.cam);
     const Scene s = batch_scene(B, &wcam[warp]);
-    batch_item(B, H, q, s, item - q.item_begin, lane);
+    batch_item<DEFER>(B, H, q, s, item - q.item_begin, lane);
   }
 }
 

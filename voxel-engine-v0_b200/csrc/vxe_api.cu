@@ -1296,7 +1296,10 @@ vxe_status lane_resources(vxe_ctx* c, BatchLane& L, uint32_t tiles, uint32_t vp_
     // Persistent grids: every SM filled to the kernels' occupancy limit.
     int sms = 0, tb = 0, lb = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tb, vxe::dev::k_batch_trace, vxe::dev::BATCH_THREADS, 0));
+    int tb0 = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tb, vxe::dev::k_batch_trace<true>, vxe::dev::BATCH_THREADS, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tb0, vxe::dev::k_batch_trace<false>, vxe::dev::BATCH_THREADS, 0));
+    tb = std::min(tb, tb0);  // the persistent grid fills every SM for either instantiation
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&lb, vxe::dev::k_batch_tiles, vxe::dev::TILE_THREADS, 0));
     c->b_trace_grid = sms * std::max(tb, 1);
     c->b_tile_grid = sms * std::max(lb, 1);
@@ -1415,7 +1418,10 @@ vxe_status launch_persistent(vxe_ctx* c, BatchLane& L, const BatchArgs& B, bool 
     k_qsort_scatter<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
   }
   k_batch_tiles<<<c->b_tile_grid, TILE_THREADS, 0, L.stream>>>(B);
-  k_batch_trace<<<c->b_trace_grid, BATCH_THREADS, 0, L.stream>>>(B);
+  if (B.defer)
+    k_batch_trace<true><<<c->b_trace_grid, BATCH_THREADS, 0, L.stream>>>(B);
+  else
+    k_batch_trace<false><<<c->b_trace_grid, BATCH_THREADS, 0, L.stream>>>(B);
   if (B.defer) {
     k_batch_probe_dda<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
     k_batch_slab_eval<<<c->shade_wave, BATCH_THREADS, 0, L.stream>>>(B);
@@ -1555,7 +1561,7 @@ vxe_status vxe_submit_batch_async(vxe_ctx* c, uint32_t lane, const vxe_request* 
         const uint32_t t = R[i].tiles_x * ((R[i].h + 7) / 8);
         k_batch_tiles<<<(t + TILE_THREADS - 1) / TILE_THREADS, TILE_THREADS, 0, L.stream>>>(B);
       }
-      k_batch_trace<<<(n_items + BATCH_THREADS / 32 - 1) / (BATCH_THREADS / 32), BATCH_THREADS, 0, L.stream>>>(B);
+      k_batch_trace<false><<<(n_items + BATCH_THREADS / 32 - 1) / (BATCH_THREADS / 32), BATCH_THREADS, 0, L.stream>>>(B);
     }
     CK(cudaGetLastError());
   } else if (opt->mode == VXE_BATCH_PERSISTENT) {
