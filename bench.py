@@ -273,24 +273,39 @@ def run_batch_serve(dev):
                  "speedup_vs_plain": round(out["plain"]["ms"] / out["persistent"]["ms"], 3)}
         reqs = make_arrivals(w, 2000.0, 20, seed=1)
         serve(r, w, reqs, torch, mem_budget=4 << 30, lanes=2)  # warm-up
-        rep = serve(r, w, make_arrivals(w, 1000.0, 120, seed=7), torch, mem_budget=4 << 30, lanes=2, max_batch=32)
-        base = serve_plain(r, w, make_arrivals(w, 1000.0, 120, seed=7), torch)
-        srv = {"workload": "120 Poisson requests at 1000 req/s, 70 % viewports / 30 % query batches",
-               "batched": rep.summary(), "plain": base.summary(),
+        # The served run depends on host timing (which arrivals share a batch):
+        # three runs each, the median one by completion time is reported.
+        def median_run(fn):
+            runs = sorted((fn() for _ in range(3)), key=lambda x: x.seconds)
+            return runs[1], [round(x.seconds, 4) for x in runs]
+
+        rep, rep_s = median_run(lambda: serve(r, w, make_arrivals(w, 1000.0, 120, seed=7), torch,
+                                              mem_budget=4 << 30, lanes=2, max_batch=32))
+        base, base_s = median_run(lambda: serve_plain(r, w, make_arrivals(w, 1000.0, 120, seed=7), torch))
+        srv = {"workload": "120 Poisson requests at 1000 req/s, 70 % viewports / 30 % query batches; "
+                           "median of 3 runs",
+               "batched": {**rep.summary(), "runs_seconds": rep_s}, "plain": {**base.summary(), "runs_seconds": base_s},
                "speedup_vs_plain": round(base.seconds / rep.seconds, 3)}
         # Sessions: frames of 16 clients whose TAA / godray / shadow histories
         # stay resident between requests (one view each), with query batches.
         sess = {}
         for rate in (1000.0, 200.0):
-            ss = make_sessions(w, 16, seed=3)
-            rep = serve(r, w, make_arrivals(w, rate, 160, seed=7, sessions=ss), torch, mem_budget=6 << 30, lanes=2,
-                        max_batch=16, sessions=ss)
-            ss = make_sessions(w, 16, seed=3)
-            base = serve_plain(r, w, make_arrivals(w, rate, 160, seed=7, sessions=ss), torch, sessions=ss)
+            def sess_served():
+                ss = make_sessions(w, 16, seed=3)
+                return serve(r, w, make_arrivals(w, rate, 160, seed=7, sessions=ss), torch, mem_budget=6 << 30,
+                             lanes=2, max_batch=16, sessions=ss)
+
+            def sess_plain():
+                ss = make_sessions(w, 16, seed=3)
+                return serve_plain(r, w, make_arrivals(w, rate, 160, seed=7, sessions=ss), torch, sessions=ss)
+
+            rep, _ = median_run(sess_served)
+            base, _ = median_run(sess_plain)
             sess[f"{int(rate)}_per_s"] = {"batched": rep.summary(), "plain": base.summary(),
                                           "speedup_vs_plain": round(base.seconds / rep.seconds, 3)}
         srv["sessions"] = {"workload": "160 Poisson requests, 70 % frames of 16 sessions (256^2-1920x1080 "
-                                       "present at render scale 0.5, histories resident) / 30 % query batches",
+                                       "present at render scale 0.5, histories resident) / 30 % query batches; "
+                                       "median of 3 runs",
                            **sess}
         return batch, srv
     finally:
@@ -481,9 +496,9 @@ def main():
                 "d2h_bytes_per_step": res["e2e"]["d2h_bytes_per_step"],
                 "frame_ms": round(e2e_s * 1e3 / args.steps, 3)},
         # per frame: k_grass_cells, k_tiles, k_primary_trace, k_probe_dda, k_slab_eval, k_slab_pick,
-        # k_primary_resolve, k_shade_prep, k_shade_shadow, k_shade_lights, k_shade_vox, k_shade_far, k_godray,
-        # k_composite
-        "gpu_launches": 14 * args.steps,
+        # k_primary_resolve, k_shade_prep, k_shade_shadow, k_shade_lights, k_shade_vox, k_shade_far x 2 (side
+        # stream), k_godray, k_composite
+        "gpu_launches": 15 * args.steps,
         "batch": batch,
         "serve": srv,
         "clocks": res["clocks"],
