@@ -167,7 +167,25 @@ __global__ void __launch_bounds__(GRASS_CELL_THREADS) k_grass_cells(const __grid
   const float time_s = A.cam.voxel_params[1], strength = A.cam.voxel_params[2];
   GrassBladeGeom B[GRASS_BLADE_COUNT];
   for (uint32_t i = 0; i < GRASS_BLADE_COUNT; ++i) grass_blade_geom(s, cb, id, time_s, strength, i, B[i]);
-  grass_rec_store(r, grass_blade_len(s, id), id, B);
+  const float blade_len = grass_blade_len(s, id);
+  grass_rec_store(r, blade_len, id, B);
+  // Columns within the lod-0 range of this camera also get their segment
+  // frames now (the values grass_frames_ready would build on first use).
+  if (A.grass_state && A.grass_frames &&
+      length(cb + V3s(0.5f * vs) - cam_pos(s)) < GRASS_LOD_MID_START + 1.0f + 4.0f * vs) {
+    const uint32_t segs = grass_lod_segs(0u);
+    const float inv_segs = 1.0f / fmax_((float)segs, 1.0f);
+    float4* F = A.grass_frames + g * GRASS_FRAME_F4;
+    for (uint32_t i = 0; i < GRASS_BLADE_COUNT; ++i)
+      for (uint32_t sg = 0; sg < segs; ++sg) {
+        const GrassSegFrame f = grass_seg_frame(B[i], blade_len, inv_segs, grass_taper_value(inv_segs, sg), sg);
+        float4* o = F + 3u * (i * segs + sg);
+        o[0] = make_float4(f.mid.x, f.mid.y, f.mid.z, f.half_w);
+        o[1] = make_float4(f.S.x, f.S.y, f.S.z, f.half_h);
+        o[2] = make_float4(f.T.x, f.T.y, f.T.z, 0.0f);
+      }
+    A.grass_state[g] = 2u;
+  }
 }
 
 // ---------------------------------------------------------------------------
