@@ -131,6 +131,7 @@ __device__ __forceinline__ Scene batch_scene(const BatchArgs& B, const vxe_camer
   s.grass_state = table ? B.grass_state : nullptr;
   s.grass_frames = table ? B.grass_frames : nullptr;
   s.slot_lights = nullptr;
+  s.slot_top = nullptr;
   return s;
 }
 

@@ -144,6 +144,10 @@ struct Scene {
   // Per chunk slot: 1 when the slot's nodes hold a LIGHT leaf (written with
   // the slot's uploads and meta writes); null when the pass has none.
   const uint32_t* __restrict__ slot_lights;
+  // Per chunk slot: the top (exclusive, in voxels above the chunk origin) of
+  // the slot's non-air leaves, 0 when the slot holds none; null when the pass
+  // has none.
+  const uint32_t* __restrict__ slot_top;
 };
 
 struct Node { uint32_t child_base, child_mask, material, key; };

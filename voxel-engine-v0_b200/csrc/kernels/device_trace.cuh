@@ -1998,7 +1998,11 @@ __device__ __noinline__ float sun_transmittance_geom_only(const Scene& s, v3 p, 
       const Meta ch2 = meta_at(s, slot);
       const float ce = start_t + t_local;
       const float cx2 = start_t + fmin_(tn, t_exit_local);
-      trans *= trace_chunk_shadow_trans_interval(s, ro, rd, ch2, ce, cx2);
+      // A rising ray that enters the chunk a voxel above its top solid leaf
+      // meets only air there: the chunk's factor is exactly 1.
+      const bool above = s.slot_top != nullptr && rd.y > 0.0f && slot < s.metas_n &&
+                         ro.y + rd.y * fmax_(ce, 0.0f) >= ((float)ch2.oy + (float)__ldg(&s.slot_top[slot]) + 1.0f) * vs;
+      if (!above) trans *= trace_chunk_shadow_trans_interval(s, ro, rd, ch2, ce, cx2);
       if (trans < MIN_TRANS) break;
     }
     if (tMaxX < tMaxY) {

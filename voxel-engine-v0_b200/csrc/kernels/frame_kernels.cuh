@@ -87,6 +87,7 @@ struct FrameArgs {
   uint32_t* grass_state;  // per record: lod-0 segment frames built?
   float4* grass_frames;   // per record: the frames
   const uint32_t* slot_lights;  // per slot: holds a LIGHT leaf
+  const uint32_t* slot_top;     // per slot: top of its non-air leaves (voxels)
   uint32_t grass_slot0;  // k_grass_cells: first slot of the launch
 };
 
@@ -122,6 +123,7 @@ __device__ __forceinline__ Scene make_scene(const FrameArgs& A, bool godray) {
   s.grass_state = A.grass_rec ? A.grass_state : nullptr;
   s.grass_frames = A.grass_rec ? A.grass_frames : nullptr;
   s.slot_lights = A.slot_lights;
+  s.slot_top = A.slot_top;
   return s;
 }
 
@@ -189,26 +191,42 @@ __global__ void __launch_bounds__(GRASS_CELL_THREADS) k_grass_cells(const __grid
 }
 
 // ---------------------------------------------------------------------------
-// Per-slot light flags: one block per slot of [slot0, slot0 + gridDim.x),
-// over the node records of its meta's range; 1 when one is a LIGHT leaf.
+// Per-slot flags: one block per slot of [slot0, slot0 + gridDim.x), over
+// the node records of its meta's range: whether one is a LIGHT leaf, and the
+// top of the non-air leaves (a leaf's cube from its key: coordinates in units
+// of the cube size 2^(log2(chunk) - level)).  Every point of the chunk above
+// that top is in an air leaf, an implicit air child or an empty macro cell.
 // ---------------------------------------------------------------------------
 constexpr int SLOT_LIGHT_THREADS = 256;
 
 __global__ void __launch_bounds__(SLOT_LIGHT_THREADS) k_slot_lights(const uint4* metas, uint64_t metas_n,
                                                                      const uint4* nodes, uint64_t nodes_n,
-                                                                     uint32_t slot0, uint32_t* out) {
+                                                                     uint32_t slot0, uint32_t chunk_size,
+                                                                     uint32_t* out, uint32_t* top_out) {
+  __shared__ uint32_t top_s;
   const uint32_t slot = slot0 + blockIdx.x;
   if (slot >= metas_n) return;
+  if (threadIdx.x == 0) top_s = 0u;
+  __syncthreads();
   const uint4 b = metas[(size_t)slot * 3u + 1u];  // node_base, node_count, macro_base, colinfo_base
   int any = 0;
+  uint32_t top = 0u;
   for (uint32_t i = threadIdx.x; i < b.y; i += SLOT_LIGHT_THREADS) {
     const uint64_t gi = (uint64_t)b.x + i;
     if (gi >= nodes_n) break;
     const uint4 n = nodes[gi];
     any |= (n.x == LEAF && n.z == MAT_LIGHT) ? 1 : 0;
+    if (n.x == LEAF && n.z != MAT_AIR) {
+      const uint32_t lvl = (n.w >> 18) & 7u, y = (n.w >> 6) & 63u;
+      top = max(top, (y + 1u) * (chunk_size >> lvl));
+    }
   }
+  atomicMax(&top_s, top);
   any = __syncthreads_or(any);
-  if (threadIdx.x == 0) out[slot] = any ? 1u : 0u;
+  if (threadIdx.x == 0) {
+    out[slot] = any ? 1u : 0u;
+    top_out[slot] = top_s;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1267,6 +1285,7 @@ __device__ __forceinline__ Scene make_query_scene(const QueryArgs& Q) {
   s.grass_state = nullptr;
   s.grass_frames = nullptr;
   s.slot_lights = nullptr;
+  s.slot_top = nullptr;
   s.grass_taper = nullptr;
   return s;
 }

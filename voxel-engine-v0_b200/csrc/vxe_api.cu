@@ -130,6 +130,7 @@ struct vxe_ctx {
   // arenas
   DevBuf nodes, ropes, metas, macro, colinfo, grid, clip_tex, errword;
   DevBuf slot_lights;  // per slot: holds a LIGHT leaf (k_slot_lights)
+  DevBuf slot_top;     // per slot: top of its non-air leaves, voxels (k_slot_lights)
   GrassTable gt;
   FrameState fr;  // the context's own frame
   SideStream side;  // its fork stream
@@ -368,6 +369,7 @@ void fill_scene_args(const vxe_ctx* c, FrameArgs& A) {
   A.err = (uint32_t*)c->errword.p;
   A.godray_alias = (c->flags & VXE_FLAG_GODRAY_MACRO_ALIAS) ? 1u : 0u;
   A.slot_lights = (const uint32_t*)c->slot_lights.p;
+  A.slot_top = (const uint32_t*)c->slot_top.p;
 }
 
 // Recomputes the light flags of slots [first, first + n) on the upload
@@ -375,8 +377,8 @@ void fill_scene_args(const vxe_ctx* c, FrameArgs& A) {
 vxe_status slot_lights_refresh(vxe_ctx* c, uint32_t first, uint32_t n) {
   if (n == 0 || !c->slot_lights.p) return VXE_OK;
   vxe::dev::k_slot_lights<<<n, vxe::dev::SLOT_LIGHT_THREADS, 0, c->upload>>>(
-      (const uint4*)c->metas.p, c->cfg.chunk_capacity, (const uint4*)c->nodes.p, c->cfg.node_capacity, first,
-      (uint32_t*)c->slot_lights.p);
+      (const uint4*)c->metas.p, c->cfg.chunk_capacity, (const uint4*)c->nodes.p, c->cfg.node_capacity, first, 64u,
+      (uint32_t*)c->slot_lights.p, (uint32_t*)c->slot_top.p);
   CK(cudaGetLastError());
   return VXE_OK;
 }
@@ -787,6 +789,7 @@ vxe_status vxe_create(const vxe_config* cfg, vxe_ctx** out) {
   if ((st = alloc(c, c->clip_tex, clip_bytes)) != VXE_OK) return bail(st);
   if ((st = alloc(c, c->errword, 4)) != VXE_OK) return bail(st);
   if ((st = alloc(c, c->slot_lights, cc * 4)) != VXE_OK) return bail(st);
+  if ((st = alloc(c, c->slot_top, cc * 4)) != VXE_OK) return bail(st);
   if (!(cfg->flags & VXE_FLAG_NO_GRASS_TABLE)) {
     if ((st = alloc(c, c->gt.rec, cc * 4096u * vxe::dev::GRASS_REC_F4 * 16u)) != VXE_OK) return bail(st);
     if ((st = alloc(c, c->gt.taper, vxe::dev::GRASS_TAPER_N * 4u)) != VXE_OK) return bail(st);
@@ -815,7 +818,7 @@ void vxe_destroy(vxe_ctx* c) {
   if (c->fr.fgraph) cudaGraphDestroy(c->fr.fgraph);
   for (auto& L : c->lanes)  // lanes read the arenas: drain them before freeing
     if (L.stream) cudaStreamSynchronize(L.stream);
-  for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword, &c->slot_lights,
+  for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword, &c->slot_lights, &c->slot_top,
                   &c->q_in, &c->q_out, &c->gt.rec, &c->gt.taper, &c->gt.state, &c->gt.frames})
     release(*b);
   for (auto& L : c->lanes) {
