@@ -312,6 +312,58 @@ def run_batch_serve(dev):
         r.close()
 
 
+def frame_series(sc, dev, steps: int, warmup: int, present=None):
+    """Frames of scene `sc` (static grid) timed by the context's events; returns ms per frame (mean) and rays."""
+    import torch
+
+    from vxe import _abi as A
+    from vxe.renderer import Renderer
+    from vxe.scenes import FrameDriver
+
+    drv = FrameDriver(sc)
+    ups = drv.initial_uploads()
+    w = drv.world
+    r = Renderer(sc.present[0], sc.present[1], sc.render_scale, node_capacity=w.node_capacity,
+                 chunk_capacity=w.chunk_capacity, grid_capacity=w.grid_capacity, clip_levels=sc.clip_levels,
+                 clip_res=sc.clip_res, flags=A.FLAG_GODRAY_MACRO_ALIAS, device=dev)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+    try:
+        r.upload_world(w, ups)
+        ms = []
+        for f in range(warmup + steps):
+            _, _, clip, cam = drv.step()
+            r.write_clipmap_updates(*clip)
+            r.write_camera(cam)
+            if f >= warmup:
+                flush.zero_()
+                torch.cuda.synchronize()
+                r.encode_compute(sync=False)
+                ms.append(r.read_gpu_timings_ms_blocking()["total"])
+            else:
+                r.encode_compute(sync=False)
+        r.synchronize()
+        assert r.read_error_word() == 0
+        return statistics.mean(ms), sc.internal[0] * sc.internal[1]
+    finally:
+        r.close()
+
+
+def run_configs(dev):
+    """Secondary frame lines: config 5 (32x8x32 chunks, 6-level 512^2 clipmap,
+    3840x2160 present / 1920x1080 internal) and config 2 at render scale 1.0."""
+    from vxe import scenes
+
+    out = {}
+    for key, sc in (("config5_4k", scenes.config5()),
+                    ("config2_scale1", scenes.config2(present=(1920, 1080), render_scale=1.0))):
+        sc.shift_every = 0
+        ms, rays = frame_series(sc, dev, steps=8, warmup=4)
+        out[key] = {"present": list(sc.present), "internal": list(sc.internal), "frame_ms": round(ms, 3),
+                    "mrays_per_s": round(rays / ms / 1e3, 3), "steps": 8, "warmup": 4,
+                    "l2": "flushed between steps"}
+    return out
+
+
 def run_e2e(args, sc, dev, world_size):
     import torch
 
@@ -462,9 +514,10 @@ def main():
     res = run_vxe(args, rank, world_size)
     if res is None:
         return
-    batch = srv = None
+    batch = srv = configs = None
     if not args.no_batch and world_size == 1:  # one GPU: the workloads north-star items 2 and 5 name
         batch, srv = run_batch_serve(0)
+        configs = run_configs(0)
     if world_size > 1:
         import torch
 
@@ -501,6 +554,7 @@ def main():
         "gpu_launches": 15 * args.steps,
         "batch": batch,
         "serve": srv,
+        "configs": configs,
         "clocks": res["clocks"],
         "device_error_word": res["error_word"],
     }

@@ -147,3 +147,11 @@ def test_upload_capacity_error_and_silent_skip():
         r.apply_chunk_uploads([bad])  # skipped like the reference
     finally:
         r.close()
+
+
+def test_config5_large_world_bit_exact():
+    # The 32x8x32-chunk world (8192 slots, caves above 0.5) with its 6-level
+    # 512^2 clipmap, at reduced resolution: bit-exact like the small worlds.
+    sc = scenes.config5(present=(320, 180))
+    res = run_parity(sc, frames=2)
+    assert all(r == {} for r in res), res

@@ -6,6 +6,8 @@
   5-level 256^2 toroidal clipmap, 1920x1080 present / 960x540 internal, a
   64-frame Catmull-Rom camera path at 0.15 m (1.5 voxels) per frame and a
   chunk-grid shift of +1 chunk in x every 16 frames.
+* ``config5``: 32x8x32 chunks with caves above 0.5, a 6-level 512^2 clipmap,
+  3840x2160 present / 1920x1080 internal, a 128-frame path.
 * ``features``: a small world with caves, carving, trees (wood + leaves) and
   light voxels so every shading path (leaf displacement, grass, voxel lights)
   is exercised by the parity tests.
@@ -105,6 +107,24 @@ def config2(seed: int = 12345, frames: int = 64, present=(1920, 1080), render_sc
                  node_capacity=12 << 20, shift_every=16, path=at)
 
 
+def config5(seed: int = 12345, frames: int = 128, present=(3840, 2160), render_scale: float = 0.5) -> Scene:
+    """32x8x32 chunks (204.8 x 51.2 x 204.8 m), 3D value-noise caves above 0.5, a
+    6-level 512^2 clipmap, 3840x2160 present / 1920x1080 internal, a 128-frame
+    Catmull-Rom path across the middle of the world."""
+    spec = WorldSpec(seed=seed, height_min=8, height_max=48, dirt_depth=3, carve_mod=0, cave_threshold=0.5)
+    rng = np.random.default_rng(seed + 5)
+    base = np.array([70.0, 7.5, 102.4])
+    pts = [base + np.array([-6.0 + 6.0 * i, rng.uniform(-0.5, 0.5), rng.uniform(-4.0, 4.0)]) for i in range(10)]
+    path = CatmullRomPath(pts, 0.15)
+
+    def at(f):
+        pos, yaw = path.at(f)
+        return pos, yaw, -0.12
+
+    return Scene("config5", spec, (0, 0, 0), (32, 8, 32), present, render_scale, 6, 512, frames,
+                 node_capacity=40 << 20, path=at)
+
+
 def features(seed: int = 777, present=(128, 80)) -> Scene:
     spec = WorldSpec(seed=seed, height_min=10, height_max=30, dirt_depth=3, carve_mod=50, cave_threshold=0.62,
                      height_scale_vox=48.0, features=3)
@@ -119,7 +139,7 @@ def features(seed: int = 777, present=(128, 80)) -> Scene:
     return Scene("features", spec, (0, 0, 0), (3, 1, 3), present, 1.0, 3, 128, 4, node_capacity=1 << 21, path=at)
 
 
-SCENES = {"config1": config1, "config2": config2, "features": features}
+SCENES = {"config1": config1, "config2": config2, "config5": config5, "features": features}
 
 
 class FrameDriver:
