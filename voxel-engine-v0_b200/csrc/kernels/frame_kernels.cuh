@@ -89,6 +89,8 @@ struct FrameArgs {
   const uint32_t* slot_lights;  // per slot: holds a LIGHT leaf
   const uint32_t* slot_top;     // per slot: top of its non-air leaves (voxels)
   uint32_t grass_slot0;  // k_grass_cells: first slot of the launch
+  uint32_t* grass_list;    // grass columns of the last full build (k_grass_cells appends; null: no list)
+  uint32_t* grass_list_n;  // their count
 };
 
 __device__ __forceinline__ Scene make_scene(const FrameArgs& A, bool godray) {
@@ -135,16 +137,9 @@ __device__ __forceinline__ Scene make_scene(const FrameArgs& A, bool godray) {
 // ---------------------------------------------------------------------------
 constexpr int GRASS_CELL_THREADS = 128;
 
-__global__ void __launch_bounds__(GRASS_CELL_THREADS) k_grass_cells(const __grid_constant__ FrameArgs A) {
-  const uint64_t g = (uint64_t)A.grass_slot0 * 4096u + (uint64_t)blockIdx.x * GRASS_CELL_THREADS + threadIdx.x;
-  const Scene s = make_scene(A, false);
-  if (g == 0u) {
-    for (uint32_t lod = 0; lod < 3u; ++lod) {
-      const uint32_t segs = grass_lod_segs(lod);
-      const float inv_segs = 1.0f / fmax_((float)segs, 1.0f);
-      for (uint32_t sg = 0; sg < 6u; ++sg) A.grass_taper[lod * 6u + sg] = sg < segs ? grass_taper_value(inv_segs, sg) : 0.0f;
-    }
-  }
+// Record g (slot g >> 12, column g & 4095) for this camera's wind; with
+// `list`, grass columns also append g to the grass column list.
+__device__ __forceinline__ void grass_column_build(const FrameArgs& A, const Scene& s, uint64_t g, bool list) {
   const uint32_t slot = (uint32_t)(g >> 12), col = (uint32_t)(g & 4095u);
   if (slot >= A.cam.chunk_count || (uint64_t)slot * 4096u >= A.grass_rec_n) return;
   float4* r = A.grass_rec + g * GRASS_REC_F4;
@@ -160,6 +155,13 @@ __global__ void __launch_bounds__(GRASS_CELL_THREADS) k_grass_cells(const __grid
   if (!(ci.valid && ci.mat == MAT_GRASS)) {
     r[0] = make_float4(0.0f, nan, nan, nan);
     return;
+  }
+  if (list) {  // warp-aggregated append
+    const uint32_t mask = __activemask(), lane = threadIdx.x & 31u, leader = __ffs(mask) - 1u;
+    uint32_t base = 0u;
+    if (lane == leader) base = atomicAdd(A.grass_list_n, (uint32_t)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    A.grass_list[base + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)g;
   }
   // The cell the column probe and the grass-voxel hit derive
   // (chunk_trace.wgsl:1434-1445).
@@ -188,6 +190,31 @@ __global__ void __launch_bounds__(GRASS_CELL_THREADS) k_grass_cells(const __grid
       }
     A.grass_state[g] = 2u;
   }
+}
+
+// Every column of slots [grass_slot0, ...): one thread per column; with a
+// grass list, the grass columns are appended to it.  Thread 0 also writes the
+// per-LOD blade taper.
+__global__ void __launch_bounds__(GRASS_CELL_THREADS) k_grass_cells(const __grid_constant__ FrameArgs A) {
+  const uint64_t g = (uint64_t)A.grass_slot0 * 4096u + (uint64_t)blockIdx.x * GRASS_CELL_THREADS + threadIdx.x;
+  const Scene s = make_scene(A, false);
+  if (g == 0u) {
+    for (uint32_t lod = 0; lod < 3u; ++lod) {
+      const uint32_t segs = grass_lod_segs(lod);
+      const float inv_segs = 1.0f / fmax_((float)segs, 1.0f);
+      for (uint32_t sg = 0; sg < 6u; ++sg) A.grass_taper[lod * 6u + sg] = sg < segs ? grass_taper_value(inv_segs, sg) : 0.0f;
+    }
+  }
+  grass_column_build(A, s, g, A.grass_list != nullptr);
+}
+
+// A new wind over an unchanged world: only the grass columns (the list of
+// the last full build) change; every other record keeps its NaN id.
+__global__ void __launch_bounds__(GRASS_CELL_THREADS) k_grass_wind(const __grid_constant__ FrameArgs A) {
+  const Scene s = make_scene(A, false);
+  const uint32_t n = *A.grass_list_n;
+  for (uint32_t i = blockIdx.x * GRASS_CELL_THREADS + threadIdx.x; i < n; i += gridDim.x * GRASS_CELL_THREADS)
+    grass_column_build(A, s, A.grass_list[i], false);
 }
 
 // ---------------------------------------------------------------------------

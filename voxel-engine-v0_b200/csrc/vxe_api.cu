@@ -58,7 +58,8 @@ enum Img {
 constexpr int kGrassReaders = 1 + VXE_BATCH_LANES;  // compute stream, lanes
 
 struct GrassTable {
-  DevBuf rec, taper, state, frames;
+  DevBuf rec, taper, state, frames, list, list_n;
+  bool list_valid = false;  // the grass column list matches the world's data
   bool valid = false;
   uint32_t time_bits = 0, strength_bits = 0, vs_bits = 0, chunk_count = 0;
   vxe_camera_gpu cam{};  // camera of the last full build (for slot refreshes)
@@ -398,7 +399,8 @@ void grass_table_args(const vxe_ctx* c, FrameArgs& A) {
 }
 
 // Records of slots [slot0, slot0 + n) for camera `cam` on stream `st`.
-vxe_status grass_table_fill(vxe_ctx* c, cudaStream_t st, const vxe_camera_gpu& cam, uint32_t slot0, uint32_t n) {
+vxe_status grass_table_fill(vxe_ctx* c, cudaStream_t st, const vxe_camera_gpu& cam, uint32_t slot0, uint32_t n,
+                            bool list = false) {
   using namespace vxe::dev;
   if (n == 0) return VXE_OK;
   FrameArgs A;
@@ -406,6 +408,11 @@ vxe_status grass_table_fill(vxe_ctx* c, cudaStream_t st, const vxe_camera_gpu& c
   A.cam = cam;
   grass_table_args(c, A);
   A.grass_slot0 = slot0;
+  if (list) {
+    A.grass_list = (uint32_t*)c->gt.list.p;
+    A.grass_list_n = (uint32_t*)c->gt.list_n.p;
+    CK(cudaMemsetAsync(c->gt.list_n.p, 0, 4, st));
+  }
   const uint64_t threads = (uint64_t)n * 4096u;
   k_grass_cells<<<(unsigned)((threads + GRASS_CELL_THREADS - 1) / GRASS_CELL_THREADS), GRASS_CELL_THREADS, 0, st>>>(A);
   CK(cudaGetLastError());
@@ -427,7 +434,21 @@ vxe_status grass_table_acquire(vxe_ctx* c, cudaStream_t st, int reader, const vx
     for (int i = 0; i < kGrassReaders; ++i)
       if (T.reader_used[i]) CK(cudaStreamWaitEvent(st, T.reader[i], 0));
     if (T.built_recorded) CK(cudaStreamWaitEvent(st, T.built, 0));
-    vxe_status s2 = grass_table_fill(c, st, cam, 0u, cam.chunk_count);
+    vxe_status s2 = VXE_OK;
+    if (T.valid && T.list_valid && T.vs_bits == vb && T.chunk_count == cam.chunk_count) {
+      // only the wind changed: rebuild the grass columns of the list
+      FrameArgs A;
+      fill_scene_args(c, A);
+      A.cam = cam;
+      grass_table_args(c, A);
+      A.grass_list = (uint32_t*)T.list.p;
+      A.grass_list_n = (uint32_t*)T.list_n.p;
+      vxe::dev::k_grass_wind<<<c->shade_wave, vxe::dev::GRASS_CELL_THREADS, 0, st>>>(A);
+      CK(cudaGetLastError());
+    } else {
+      s2 = grass_table_fill(c, st, cam, 0u, cam.chunk_count, true);
+      T.list_valid = true;
+    }
     if (s2 != VXE_OK) return s2;
     T.valid = true;
     T.time_bits = tb;
@@ -449,6 +470,7 @@ vxe_status grass_table_acquire(vxe_ctx* c, cudaStream_t st, int reader, const vx
 vxe_status grass_table_refresh(vxe_ctx* c, const vxe_chunk_upload* ups, uint32_t n) {
   GrassTable& T = c->gt;
   if (!T.valid || n == 0) return VXE_OK;
+  T.list_valid = false;  // the next wind change rebuilds every column
   if (T.built_recorded) CK(cudaStreamWaitEvent(c->upload, T.built, 0));
   std::vector<uint32_t> slots;
   slots.reserve(n);
@@ -794,6 +816,8 @@ vxe_status vxe_create(const vxe_config* cfg, vxe_ctx** out) {
     if ((st = alloc(c, c->gt.rec, cc * 4096u * vxe::dev::GRASS_REC_F4 * 16u)) != VXE_OK) return bail(st);
     if ((st = alloc(c, c->gt.taper, vxe::dev::GRASS_TAPER_N * 4u)) != VXE_OK) return bail(st);
     if ((st = alloc(c, c->gt.state, cc * 4096u * 4u)) != VXE_OK) return bail(st);
+    if ((st = alloc(c, c->gt.list, cc * 4096u * 4u)) != VXE_OK) return bail(st);
+    if ((st = alloc(c, c->gt.list_n, 4)) != VXE_OK) return bail(st);
     if ((st = alloc(c, c->gt.frames, cc * 4096u * vxe::dev::GRASS_FRAME_F4 * 16u)) != VXE_OK) return bail(st);
   }
   if (cudaEventCreateWithFlags(&c->gt.built, cudaEventDisableTiming) != cudaSuccess) return bail(VXE_ERR_DEVICE);
@@ -819,7 +843,8 @@ void vxe_destroy(vxe_ctx* c) {
   for (auto& L : c->lanes)  // lanes read the arenas: drain them before freeing
     if (L.stream) cudaStreamSynchronize(L.stream);
   for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword, &c->slot_lights, &c->slot_top,
-                  &c->q_in, &c->q_out, &c->gt.rec, &c->gt.taper, &c->gt.state, &c->gt.frames})
+                  &c->q_in, &c->q_out, &c->gt.rec, &c->gt.taper, &c->gt.state, &c->gt.frames,
+                  &c->gt.list, &c->gt.list_n})
     release(*b);
   for (auto& L : c->lanes) {
     if (L.stream) cudaStreamSynchronize(L.stream);
@@ -1053,6 +1078,7 @@ vxe_status vxe_write_meta(vxe_ctx* c, uint32_t first, const vxe_chunk_meta* meta
   if ((ws = slot_lights_refresh(c, first, n)) != VXE_OK) return ws;
   // a slot's records follow its meta (origin, colinfo base)
   if (n && c->gt.valid) {
+    c->gt.list_valid = false;  // the next wind change rebuilds every column
     if (c->gt.built_recorded) CK(cudaStreamWaitEvent(c->upload, c->gt.built, 0));
     const uint32_t hi = std::min(first + n, c->gt.chunk_count);
     if (hi > first) {
