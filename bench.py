@@ -348,6 +348,46 @@ def frame_series(sc, dev, steps: int, warmup: int, present=None):
         r.close()
 
 
+def run_clipmap(dev):
+    """Clipmap patch generation, config 5's 6 x 512^2 clipmap: a full rebuild
+    (every level new) and a one-texel scroll, on the host (the reference's
+    path: CPU texels, then an upload) vs on the device (texels written in place)."""
+    import time
+
+    import torch
+
+    from vxe import scenes
+    from vxe.renderer import Renderer
+    from vxe.world import Clipmap
+
+    sc = scenes.config5(present=(64, 36))
+    r = Renderer(64, 36, 1.0, node_capacity=1 << 12, chunk_capacity=4, grid_capacity=4, clip_levels=6, clip_res=512,
+                 device=dev)
+    out = {}
+    try:
+        for name, moves in (("full_rebuild", [(100.0, 100.0)]), ("scroll_1m", [(100.0, 100.0), (101.0, 100.0)])):
+            cpu, gpu = Clipmap(sc.spec, 6, 512, 1.0), Clipmap(sc.spec, 6, 512, 1.0)
+            for x, z in moves[:-1]:
+                r.write_clipmap_updates(*cpu.update(x, z))
+                gpu.update_device(r, x, z)
+            torch.cuda.synchronize(dev)
+            x, z = moves[-1]
+            t0 = time.perf_counter()
+            params, patches = cpu.update(x, z)
+            r.write_clipmap_updates(params, patches)
+            torch.cuda.synchronize(dev)  # the upload stream's copies have landed
+            t1 = time.perf_counter()
+            gpu.update_device(r, x, z)
+            torch.cuda.synchronize(dev)
+            t2 = time.perf_counter()
+            texels = int(sum(p[3] * p[4] for p in patches))
+            out[name] = {"texels": texels, "host_ms": round((t1 - t0) * 1e3, 3), "device_ms": round((t2 - t1) * 1e3, 3),
+                         "note": "host: CPU texels + upload; device: plan + kernel; wall clock to completion"}
+    finally:
+        r.close()
+    return out
+
+
 def run_configs(dev):
     """Secondary frame lines: config 5 (32x8x32 chunks, 6-level 512^2 clipmap,
     3840x2160 present / 1920x1080 internal) and config 2 at render scale 1.0."""
@@ -518,6 +558,7 @@ def main():
     if not args.no_batch and world_size == 1:  # one GPU: the workloads north-star items 2 and 5 name
         batch, srv = run_batch_serve(0)
         configs = run_configs(0)
+        configs["clipmap_patches"] = run_clipmap(0)
     if world_size > 1:
         import torch
 

@@ -500,6 +500,31 @@ vxe_status vxe_clipmap_update(vxe_clipmap_state* s, float cam_x, float cam_z,
                               vxe_clipmap_gpu* params, const vxe_clip_patch** patches,
                               uint32_t* n_patches);
 
+/* A patch's placement without its texels: storage rectangle (as
+ * vxe_clip_patch), first logical texel, and the level's origin and cell. */
+typedef struct vxe_clip_patch_geom {
+  uint32_t level, x, y, w, h;
+  uint32_t lx0, lz0;
+  float ox_m, oz_m, cell_m;
+} vxe_clip_patch_geom;
+#define VXE_CLIP_PATCHES_MAX 64 /* at most 4 per level (two wrapped strips per axis) */
+/* vxe_clipmap_update's state step without evaluating texels: the params, the
+ * patches' geometry and the world parameters the texels come from.  Geometry
+ * stays valid until the next update / plan / free. */
+vxe_status vxe_clipmap_plan(vxe_clipmap_state* s, float cam_x, float cam_z, vxe_clipmap_gpu* params,
+                            const vxe_clip_patch_geom** geoms, uint32_t* n_geoms, vxe_world_params* world);
+/* Clipmap patch generation on the device (no reference counterpart: the
+ * reference computes patches on the CPU, clipmap.rs:182-577, and uploads them
+ * with write_clipmap_updates): vxe_clipmap_plan, then the patches' texels are
+ * evaluated by a kernel straight into the context's clipmap texture on the
+ * upload stream, ordered like vxe_write_clipmap, and the params become the
+ * context's clipmap uniform.  The texels equal vxe_clipmap_update's bit for
+ * bit; no host texel data, no host-to-device copy. */
+vxe_status vxe_clipmap_update_device(vxe_ctx* ctx, vxe_clipmap_state* s, float cam_x, float cam_z);
+/* Copies the context's clipmap texture (levels x res x res floats) to host
+ * memory, after the writes queued so far. */
+vxe_status vxe_read_clipmap(vxe_ctx* ctx, float* host, size_t bytes);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

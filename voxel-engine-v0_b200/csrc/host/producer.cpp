@@ -23,6 +23,8 @@
 #include <new>
 #include <vector>
 
+#include "../common/terrain_noise.h"
+
 namespace {
 
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;
@@ -30,75 +32,19 @@ constexpr int kSide = 64;
 constexpr int kSide2 = kSide * kSide;
 constexpr int kSide3 = kSide2 * kSide;
 
-// ----------------------------------------------------------------------------
-// Hashing (world/hash.rs:2-32)
-// ----------------------------------------------------------------------------
-inline uint32_t mix32(uint32_t v) {
-  v ^= v >> 16;
-  v *= 0x7feb352du;
-  v ^= v >> 15;
-  v *= 0x846ca68bu;
-  v ^= v >> 16;
-  return v;
-}
-inline uint32_t hash2(uint32_t seed, int32_t x, int32_t z) {
-  return mix32(seed ^ ((uint32_t)x * 0x9e3779b1u) ^ ((uint32_t)z * 0x85ebca6bu));
-}
-inline uint32_t hash3(uint32_t seed, int32_t x, int32_t y, int32_t z) {
-  return mix32(seed ^ ((uint32_t)x * 0x9e3779b1u) ^ ((uint32_t)y * 0x85ebca6bu) ^
-               ((uint32_t)z * 0xc2b2ae35u));
-}
-inline double u01(uint32_t v) { return (double)v * (1.0 / 4294967296.0); }
-inline double fade(double t) { return t * t * (3.0 - 2.0 * t); }
-
-// ----------------------------------------------------------------------------
-// Project value noise (seeded).  Lattice noise with smoothstep interpolation.
-// ----------------------------------------------------------------------------
-double value_noise2(uint32_t seed, double x, double z) {
-  const double gx = std::floor(x), gz = std::floor(z);
-  const int32_t ix = (int32_t)gx, iz = (int32_t)gz;
-  const double fx = fade(x - gx), fz = fade(z - gz);
-  const double a = u01(hash2(seed, ix, iz)), b = u01(hash2(seed, ix + 1, iz));
-  const double c = u01(hash2(seed, ix, iz + 1)), d = u01(hash2(seed, ix + 1, iz + 1));
-  const double x0 = a + (b - a) * fx, x1 = c + (d - c) * fx;
-  return x0 + (x1 - x0) * fz;
-}
-
-double value_noise3(uint32_t seed, double x, double y, double z) {
-  const double gx = std::floor(x), gy = std::floor(y), gz = std::floor(z);
-  const int32_t ix = (int32_t)gx, iy = (int32_t)gy, iz = (int32_t)gz;
-  const double fx = fade(x - gx), fy = fade(y - gy), fz = fade(z - gz);
-  double c[2][2][2];
-  for (int k = 0; k < 2; ++k)
-    for (int j = 0; j < 2; ++j)
-      for (int i = 0; i < 2; ++i) c[k][j][i] = u01(hash3(seed, ix + i, iy + j, iz + k));
-  double yz[2][2];
-  for (int k = 0; k < 2; ++k)
-    for (int j = 0; j < 2; ++j) yz[k][j] = c[k][j][0] + (c[k][j][1] - c[k][j][0]) * fx;
-  const double z0 = yz[0][0] + (yz[0][1] - yz[0][0]) * fy;
-  const double z1 = yz[1][0] + (yz[1][1] - yz[1][0]) * fy;
-  return z0 + (z1 - z0) * fz;
-}
+// Hashing and value noise: terrain_noise.h (shared with the device).
+using vxe::terrain::fade;
+using vxe::terrain::hash2;
+using vxe::terrain::hash3;
+using vxe::terrain::mix32;
+using vxe::terrain::u01;
+using vxe::terrain::value_noise2;
+using vxe::terrain::value_noise3;
 
 struct World {
   vxe_world_params p;
 
-  int32_t ground(int32_t wx, int32_t wz) const {
-    // 4 octaves, persistence 0.5, lacunarity 2, mapped linearly onto
-    // [height_min, height_max].
-    double spacing = p.height_scale_vox > 0.f ? (double)p.height_scale_vox : 64.0;
-    double amp = 1.0, sum = 0.0, norm = 0.0;
-    for (int o = 0; o < 4; ++o) {
-      sum += amp * value_noise2(p.seed + 0x9E37u * (uint32_t)(o + 1), wx / spacing, wz / spacing);
-      norm += amp;
-      amp *= 0.5;
-      spacing *= 0.5;
-    }
-    const double n = sum / norm;  // [0, 1)
-    const int32_t span = p.height_max - p.height_min + 1;
-    int32_t h = p.height_min + (int32_t)std::floor(n * (double)span);
-    return std::min(std::max(h, p.height_min), p.height_max);
-  }
+  int32_t ground(int32_t wx, int32_t wz) const { return vxe::terrain::ground(p, wx, wz); }
 
   bool cave(int32_t wx, int32_t wy, int32_t wz) const {
     if (!(p.cave_threshold < 1.0f)) return false;
@@ -520,6 +466,8 @@ struct vxe_clipmap_state {
   uint32_t off_x[VXE_CLIP_LEVELS_MAX], off_z[VXE_CLIP_LEVELS_MAX];
   std::vector<std::vector<float>> data;
   std::vector<vxe_clip_patch> patches;
+  std::vector<vxe_clip_patch_geom> geoms;
+  bool with_data = true;  // false: record the geometry only (vxe_clipmap_plan)
 
   float sample(float wx_m, float wz_m) const {
     const float vs = 0.1f;
@@ -529,6 +477,12 @@ struct vxe_clipmap_state {
   // Patch of logical texels [lx0, lx0+w) x [lz0, lz0+h) placed at storage (sx, sz).
   void emit(uint32_t lvl, float ox_m, float oz_m, float cell, uint32_t lx0, uint32_t lz0, uint32_t w,
             uint32_t h, uint32_t sx, uint32_t sz) {
+    geoms.push_back(vxe_clip_patch_geom{lvl, sx, sz, w, h, lx0, lz0, ox_m, oz_m, cell});
+    if (!with_data) {
+      data.emplace_back();
+      patches.push_back(vxe_clip_patch{lvl, sx, sz, w, h, nullptr});
+      return;
+    }
     std::vector<float> d((size_t)w * h);
     for (uint32_t z = 0; z < h; ++z) {
       const float wz = oz_m + ((float)(lz0 + z) + 0.5f) * cell;
@@ -702,6 +656,7 @@ vxe_status vxe_clipmap_update(vxe_clipmap_state* s, float cam_x, float cam_z, vx
   if (!s || !params || !patches || !n_patches) return VXE_ERR_INVALID_ARG;
   s->data.clear();
   s->patches.clear();
+  s->geoms.clear();
   std::memset(params, 0, sizeof(*params));
   params->levels = s->levels;
   params->res = s->res;
@@ -783,9 +738,24 @@ vxe_status vxe_clipmap_update(vxe_clipmap_state* s, float cam_x, float cam_z, vx
   }
   // Levels beyond `levels` keep cell 1.0 like the reference's default fill.
   for (uint32_t i = s->levels; i < VXE_CLIP_LEVELS_MAX; ++i) params->level[i][2] = 1.0f;
-  for (size_t k = 0; k < s->patches.size(); ++k) s->patches[k].data = s->data[k].data();
+  for (size_t k = 0; k < s->patches.size(); ++k) s->patches[k].data = s->with_data ? s->data[k].data() : nullptr;
   *patches = s->patches.empty() ? nullptr : s->patches.data();
   *n_patches = (uint32_t)s->patches.size();
+  return VXE_OK;
+}
+
+vxe_status vxe_clipmap_plan(vxe_clipmap_state* s, float cam_x, float cam_z, vxe_clipmap_gpu* params,
+                            const vxe_clip_patch_geom** geoms, uint32_t* n_geoms, vxe_world_params* world) {
+  if (!s || !params || !geoms || !n_geoms || !world) return VXE_ERR_INVALID_ARG;
+  const vxe_clip_patch* patches = nullptr;
+  uint32_t n = 0;
+  s->with_data = false;
+  const vxe_status st = vxe_clipmap_update(s, cam_x, cam_z, params, &patches, &n);
+  s->with_data = true;
+  if (st != VXE_OK) return st;
+  *geoms = s->geoms.empty() ? nullptr : s->geoms.data();
+  *n_geoms = (uint32_t)s->geoms.size();
+  *world = s->world.p;
   return VXE_OK;
 }
 

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "kernels/batch_kernels.cuh"
+#include "common/terrain_noise.h"
 #include "kernels/frame_kernels.cuh"
 #include "vxe/vxe.h"
 
@@ -1108,6 +1109,94 @@ vxe_status vxe_write_grid(vxe_ctx* c, const uint32_t* grid, uint32_t n) {
 vxe_status vxe_write_camera(vxe_ctx* c, const vxe_camera_gpu* cam) {
   if (!c || !cam) return fail(c, VXE_ERR_INVALID_ARG, "null camera");
   c->cam = *cam;
+  return VXE_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// The texels of up to VXE_CLIP_PATCHES_MAX clipmap patches: patch k covers
+// texels [first[k], first[k + 1]) of the launch, row-major in its rectangle.
+struct ClipPlan {
+  vxe_world_params world;
+  float* tex;
+  uint32_t res, n;
+  uint32_t first[VXE_CLIP_PATCHES_MAX + 1];
+  vxe_clip_patch_geom g[VXE_CLIP_PATCHES_MAX];
+};
+
+__global__ void __launch_bounds__(256) k_clip_patches(const __grid_constant__ ClipPlan P) {
+  const uint32_t total = P.first[P.n];
+  for (uint32_t t = blockIdx.x * 256u + threadIdx.x; t < total; t += gridDim.x * 256u) {
+    uint32_t k = 0;
+    while (k + 1u < P.n && t >= P.first[k + 1u]) ++k;
+    const vxe_clip_patch_geom& g = P.g[k];
+    const uint32_t i = t - P.first[k], x = i % g.w, z = i / g.w;
+    // Patches are uploaded in order and a later one may cover the same
+    // storage texel (an x strip and a z strip of one level meet at a corner):
+    // the last one covering it writes it.
+    const uint32_t sx = g.x + x, sz = g.y + z;
+    bool later = false;
+    for (uint32_t j = k + 1u; j < P.n && !later; ++j) {
+      const vxe_clip_patch_geom& h = P.g[j];
+      later = h.level == g.level && sx >= h.x && sx < h.x + h.w && sz >= h.y && sz < h.y + h.h;
+    }
+    if (later) continue;
+    // the texel centre as clipmap.rs emits it
+    const float wz = g.oz_m + ((float)(g.lz0 + z) + 0.5f) * g.cell_m;
+    const float wx = g.ox_m + ((float)(g.lx0 + x) + 0.5f) * g.cell_m;
+    P.tex[((size_t)g.level * P.res + sz) * P.res + sx] = vxe::terrain::clip_sample(P.world, wx, wz);
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+vxe_status vxe_clipmap_update_device(vxe_ctx* c, vxe_clipmap_state* s, float cam_x, float cam_z) {
+  if (!c || !s) return fail(c, VXE_ERR_INVALID_ARG, "null clipmap arguments");
+  cudaSetDevice(c->device);
+  ClipPlan P;
+  std::memset(&P, 0, sizeof P);
+  vxe_clipmap_gpu params;
+  const vxe_clip_patch_geom* geoms = nullptr;
+  uint32_t n = 0;
+  vxe_status st = vxe_clipmap_plan(s, cam_x, cam_z, &params, &geoms, &n, &P.world);
+  if (st != VXE_OK) return fail(c, st, "vxe_clipmap_plan failed");
+  if (params.levels > c->cfg.clip_levels || (params.levels != 0 && params.res != c->cfg.clip_res))
+    return fail(c, VXE_ERR_CAPACITY, "clipmap %u x %u^2 does not fit the context's %u x %u^2", params.levels,
+                params.res, c->cfg.clip_levels, c->cfg.clip_res);
+  if (n > VXE_CLIP_PATCHES_MAX) return fail(c, VXE_ERR_CAPACITY, "%u clipmap patches > %u", n, VXE_CLIP_PATCHES_MAX);
+  P.tex = (float*)c->clip_tex.p;
+  P.res = c->cfg.clip_res;
+  P.n = n;
+  uint64_t total = 0;
+  for (uint32_t k = 0; k < n; ++k) {
+    P.g[k] = geoms[k];
+    P.first[k] = (uint32_t)total;
+    total += (uint64_t)geoms[k].w * geoms[k].h;
+  }
+  P.first[n] = (uint32_t)total;
+  if ((st = upload_after_readers(c)) != VXE_OK) return st;
+  if (total) {
+    const unsigned grid = (unsigned)std::min<uint64_t>((total + 255) / 256, (uint64_t)c->shade_wave);
+    k_clip_patches<<<grid, 256, 0, c->upload>>>(P);
+    CK(cudaGetLastError());
+  }
+  c->clip = params;
+  CK(cudaEventRecord(c->upload_done, c->upload));
+  c->upload_pending = true;
+  c->upload_recorded = true;
+  return VXE_OK;
+}
+
+vxe_status vxe_read_clipmap(vxe_ctx* c, float* host, size_t bytes) {
+  if (!c || !host) return fail(c, VXE_ERR_INVALID_ARG, "null clipmap read arguments");
+  if (bytes != c->clip_tex.bytes) return fail(c, VXE_ERR_INVALID_ARG, "clipmap is %zu bytes, got %zu", c->clip_tex.bytes, bytes);
+  cudaSetDevice(c->device);
+  CK(cudaStreamSynchronize(c->upload));
+  if (bytes) CK(cudaMemcpy(host, c->clip_tex.p, bytes, cudaMemcpyDeviceToHost));
   return VXE_OK;
 }
 

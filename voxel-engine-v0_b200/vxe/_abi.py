@@ -113,6 +113,11 @@ class Timings(C.Structure):
                                            "total", "primary_trace", "grass_cells", "trace_kernel")]
 
 
+class ClipPatchGeom(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("level", "x", "y", "w", "h", "lx0", "lz0")] + \
+               [(n, C.c_float) for n in ("ox_m", "oz_m", "cell_m")]
+
+
 class WorldParams(C.Structure):
     _fields_ = [("seed", C.c_uint32), ("height_min", C.c_int32), ("height_max", C.c_int32),
                 ("dirt_depth", C.c_int32), ("carve_mod", C.c_uint32), ("cave_threshold", C.c_float),
@@ -211,6 +216,10 @@ SIGNATURES = {
     "vxe_clipmap_free": (None, [C.c_void_p]),
     "vxe_clipmap_update": (C.c_int, [C.c_void_p, C.c_float, C.c_float, P(ClipmapGpu), P(P(ClipPatch)),
                                      P(C.c_uint32)]),
+    "vxe_clipmap_plan": (C.c_int, [C.c_void_p, C.c_float, C.c_float, P(ClipmapGpu), P(P(ClipPatchGeom)),
+                                   P(C.c_uint32), P(WorldParams)]),
+    "vxe_clipmap_update_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_float]),
+    "vxe_read_clipmap": (C.c_int, [C.c_void_p, P(C.c_float), C.c_size_t]),
 }
 
 

@@ -25,6 +25,7 @@ class Renderer:
         if st != A.VXE_OK:
             raise A.VxeError(st, "vxe_create")
         self._ctx = h
+        self.clip_levels, self.clip_res = clip_levels, clip_res
         self.render_scale = render_scale
         self.resize_output(width, height)
 
@@ -124,6 +125,13 @@ class Renderer:
         t = A.Timings()
         self._check(self._lib.vxe_get_timings(self._ctx, C.byref(t)), "vxe_get_timings")
         return {k: getattr(t, k) for k, _ in A.Timings._fields_}
+
+    def read_clipmap(self) -> np.ndarray:
+        """The clipmap texture (levels, res, res) after the writes queued so far."""
+        out = np.zeros((self.clip_levels, self.clip_res, self.clip_res), dtype=np.float32)
+        self._check(self._lib.vxe_read_clipmap(self._ctx, out.ctypes.data_as(C.POINTER(C.c_float)), out.nbytes),
+                    "vxe_read_clipmap")
+        return out
 
     def read_error_word(self) -> int:
         w = C.c_uint32()
