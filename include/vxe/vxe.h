@@ -263,6 +263,7 @@ vxe_status vxe_trace_rays(vxe_ctx* ctx, const float* origins, const float* dirs,
 vxe_status vxe_trace_rays_device(vxe_ctx* ctx, const float* d_origins, const float* d_dirs,
                                  uint32_t n, float tmax, vxe_hit* d_out);
 
+
 /* Batched requests (no reference counterpart; the reference renders one
  * viewport per frame and answers picking queries on the CPU).  A viewport
  * request yields the primary hit records of a cold frame (the records
@@ -446,6 +447,17 @@ typedef struct vxe_world_params {
   float height_scale_vox;   /* lattice spacing of the height noise octave 0 */
   uint32_t features;        /* bit0 trees (wood+leaf), bit1 light voxels */
 } vxe_world_params;
+
+/* Physics solidity (ChunkManagerQuery::solid_voxel_at, physics/world_query.rs:
+ * 80-112; the reference answers it on the CPU): for n voxel coordinates
+ * (x, y, z int32 triples, device memory) out[i] = 1 when solid.  A voxel of a
+ * chunk in the context's grid is solid at or below its column's colinfo top
+ * (empty column: never); elsewhere, with `world` non-null, at or below the
+ * seeded heightfield (the reference's fallback while a chunk streams in),
+ * else 0.  Launched on the compute stream.  The reference consults every
+ * resident or uploading chunk; here the chunks of the grid window. */
+vxe_status vxe_solid_voxels_device(vxe_ctx* ctx, const int32_t* d_vox, uint32_t n, const vxe_world_params* world,
+                                   uint8_t* d_out);
 
 typedef struct vxe_built_chunk {
   vxe_node* nodes;

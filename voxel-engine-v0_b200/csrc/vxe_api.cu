@@ -1347,6 +1347,57 @@ static void fill_query_args(const vxe_ctx* c, QueryArgs& Q) {
   Q.err = (uint32_t*)c->errword.p;
 }
 
+}  // extern "C"
+
+namespace {
+
+__global__ void __launch_bounds__(256) k_solid_voxels(const __grid_constant__ vxe::dev::FrameArgs A, const int32_t* vox,
+                                                      uint32_t n, vxe_world_params wp, uint32_t has_world,
+                                                      uint8_t* out) {
+  using namespace vxe::dev;
+  const Scene s = make_scene(A, false);
+  const int32_t cs = (int32_t)s.cam->chunk_size;
+  auto fdiv = [cs](int32_t a) { return a >= 0 ? a / cs : -((-a + cs - 1) / cs); };
+  for (uint32_t i = blockIdx.x * 256u + threadIdx.x; i < n; i += gridDim.x * 256u) {
+    const int32_t vx = vox[3u * i], vy = vox[3u * i + 1u], vz = vox[3u * i + 2u];
+    const int32_t cx = fdiv(vx), cy = fdiv(vy), cz = fdiv(vz);
+    const uint32_t slot = grid_lookup_slot(s, cx, cy, cz);
+    uint8_t solid = 0u;
+    if (slot != INVALID && slot < s.cam->chunk_count) {
+      const Meta m = meta_at(s, slot);
+      const uint32_t lx = (uint32_t)(vx - cx * cs), lz = (uint32_t)(vz - cz * cs);
+      const int32_t ly = vy - cy * cs;
+      const uint32_t top = colinfo_entry_u16(s, m.colinfo_base, lx, lz) & 0xFFu;
+      solid = (top != 255u && ly <= (int32_t)top) ? 1u : 0u;
+    } else if (has_world) {
+      solid = vy <= vxe::terrain::ground(wp, vx, vz) ? 1u : 0u;
+    }
+    out[i] = solid;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+vxe_status vxe_solid_voxels_device(vxe_ctx* c, const int32_t* d_vox, uint32_t n, const vxe_world_params* world,
+                                   uint8_t* d_out) {
+  if (!c || (n && (!d_vox || !d_out))) return fail(c, VXE_ERR_INVALID_ARG, "null solidity buffers");
+  if (n == 0) return VXE_OK;
+  if (c->cam.chunk_size != 64u) return fail(c, VXE_ERR_INVALID_ARG, "chunk_size must be 64 (colinfo layout)");
+  cudaSetDevice(c->device);
+  if (c->upload_recorded) CK(cudaStreamWaitEvent(c->compute, c->upload_done, 0));
+  vxe::dev::FrameArgs A;
+  fill_scene_args(c, A);
+  vxe_world_params wp;
+  std::memset(&wp, 0, sizeof wp);
+  if (world) wp = *world;
+  const unsigned grid = (unsigned)std::min<uint64_t>(((uint64_t)n + 255) / 256, (uint64_t)c->shade_wave);
+  k_solid_voxels<<<grid, 256, 0, c->compute>>>(A, d_vox, n, wp, world ? 1u : 0u, d_out);
+  CK(cudaGetLastError());
+  return VXE_OK;
+}
+
 vxe_status vxe_trace_rays_device(vxe_ctx* c, const float* d_o, const float* d_d, uint32_t n, float tmax, vxe_hit* d_out) {
   if (!c || (n && (!d_o || !d_d || !d_out))) return fail(c, VXE_ERR_INVALID_ARG, "null ray buffers");
   if (n == 0) return VXE_OK;

@@ -220,6 +220,7 @@ SIGNATURES = {
                                    P(C.c_uint32), P(WorldParams)]),
     "vxe_clipmap_update_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_float]),
     "vxe_read_clipmap": (C.c_int, [C.c_void_p, P(C.c_float), C.c_size_t]),
+    "vxe_solid_voxels_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, P(WorldParams), C.c_void_p]),
 }
 
 

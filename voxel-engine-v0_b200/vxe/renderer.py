@@ -126,6 +126,21 @@ class Renderer:
         self._check(self._lib.vxe_get_timings(self._ctx, C.byref(t)), "vxe_get_timings")
         return {k: getattr(t, k) for k, _ in A.Timings._fields_}
 
+    def solid_voxels(self, vox, world_params=None):
+        """Physics solidity of voxel coordinates `vox` (torch int32 tensor (n, 3) on
+        this context's device); returns a torch uint8 tensor (1 = solid).
+        `world_params` (A.WorldParams) enables the heightfield fallback."""
+        import torch
+
+        vox = vox.contiguous()
+        out = torch.empty(vox.shape[0], dtype=torch.uint8, device=vox.device)
+        wp = C.byref(world_params) if world_params is not None else None
+        torch.cuda.current_stream().synchronize()
+        self._check(self._lib.vxe_solid_voxels_device(self._ctx, vox.data_ptr(), vox.shape[0], wp, out.data_ptr()),
+                    "vxe_solid_voxels_device")
+        self.synchronize()
+        return out
+
     def read_clipmap(self) -> np.ndarray:
         """The clipmap texture (levels, res, res) after the writes queued so far."""
         out = np.zeros((self.clip_levels, self.clip_res, self.clip_res), dtype=np.float32)
