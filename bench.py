@@ -388,6 +388,80 @@ def run_clipmap(dev):
     return out
 
 
+def run_builder(dev, steps: int = 3, warmup: int = 2):
+    """Chunk builds, all 1024 chunks of the config-2 world (16 x 4 x 16, caves
+    above 0.6): the device builder (ground + material fill + octree/ropes
+    kernels, two calls of 512 chunks, device events per kernel) against the
+    host builder (the C++ port of svo/builder.rs) on all host cores on a
+    bounded sample.  e2e: World.prebuild_device, host copies of every chunk
+    included, wall clock."""
+    import os
+    import time
+
+    import torch
+
+    from vxe import _abi as A
+    from vxe import scenes
+    from vxe.renderer import Renderer
+    from vxe.world import World
+
+    sc = scenes.config2(present=(64, 36))
+    keys = [(x, y, z) for z in range(16) for y in range(4) for x in range(16)]
+    r = Renderer(64, 36, 1.0, node_capacity=1 << 12, chunk_capacity=4, grid_capacity=4, clip_levels=1, clip_res=16,
+                 device=dev)
+    wp = sc.spec.params()
+    parts = [torch.tensor(keys[i:i + A.BUILD_BATCH_MAX], dtype=torch.int32, device=f"cuda:{dev}")
+             for i in range(0, len(keys), A.BUILD_BATCH_MAX)]
+    try:
+        counts = [r.build_chunks(wp, c, node_cap=0)["counts"] for c in parts]
+        cap = int(max(int(c[:, 0].max()) for c in counts))
+        solid = int(sum(int(c[:, 1].sum()) for c in counts))
+        nodes_total = int(sum(int(c[:, 0].sum()) for c in counts))
+        per = {"ground": [], "fill": [], "svo": []}
+        for it in range(warmup + steps):
+            step = {"ground": 0.0, "fill": 0.0, "svo": 0.0}
+            for c in parts:
+                r.build_chunks(wp, c, node_cap=cap)
+                for k, v in r.build_timings().items():
+                    step[k] += v
+            if it >= warmup:
+                for k in per:
+                    per[k].append(step[k])
+        dev_ms = statistics.mean(per["ground"]) + statistics.mean(per["fill"]) + statistics.mean(per["svo"])
+        wd = World(sc.spec, sc.grid_origin, sc.grid_dims, sc.node_capacity)
+        wd.prebuild_device(r, keys[:64], batch=64)  # warm
+        wd = World(sc.spec, sc.grid_origin, sc.grid_dims, sc.node_capacity)
+        t0 = time.perf_counter()
+        wd.prebuild_device(r, keys, batch=256)
+        e2e_s = time.perf_counter() - t0
+    finally:
+        r.close()
+    # host builder on every host core, a bounded sample of 128 chunks spread over the grid
+    threads = os.cpu_count() or 1
+    sample = keys[::8]
+    wh = World(sc.spec, sc.grid_origin, sc.grid_dims, sc.node_capacity)
+    t0 = time.perf_counter()
+    wh.prebuild(sample, threads=threads)
+    host_s = time.perf_counter() - t0
+    # bytes the octree kernel must move per chunk: the 64^3 materials read,
+    # 32^3 level-5 state and offset words written and read back, node (16 B)
+    # and rope (32 B) records written
+    svo_bytes = len(keys) * (64 ** 3 + 32 ** 3 * 4 * 4 + 2048 * 4 + 16 * 4) + nodes_total * 48
+    return {
+        "workload": "1024 chunks of the config-2 world (16x4x16, 64^3 voxels each)",
+        "chunks_per_s": round(len(keys) / (dev_ms * 1e-3), 1),
+        "device_ms": round(dev_ms, 3),
+        "kernel_ms": {k: round(statistics.mean(v), 3) for k, v in per.items()},
+        "steps": steps, "warmup": warmup,
+        "nodes_total": nodes_total, "solid_voxels": solid, "node_cap": cap,
+        "svo_kernel_gbs": round(svo_bytes / (statistics.mean(per["svo"]) * 1e-3) / 1e9, 2),
+        "e2e": {"chunks_per_s": round(len(keys) / e2e_s, 1), "seconds": round(e2e_s, 3),
+                "note": "World.prebuild_device: device build + host copies of nodes/ropes/macro/colinfo"},
+        "cpu_baseline": {"chunks_per_s": round(len(sample) / host_s, 2), "cores": threads, "kind": "port",
+                         "sample": f"{len(sample)} chunks (every 8th of the grid), World.prebuild thread pool"},
+    }
+
+
 def run_configs(dev):
     """Secondary frame lines: config 5 (32x8x32 chunks, 6-level 512^2 clipmap,
     3840x2160 present / 1920x1080 internal) and config 2 at render scale 1.0."""
@@ -559,6 +633,7 @@ def main():
         batch, srv = run_batch_serve(0)
         configs = run_configs(0)
         configs["clipmap_patches"] = run_clipmap(0)
+        configs["chunk_builder"] = run_builder(0)
     if world_size > 1:
         import torch
 

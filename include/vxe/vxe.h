@@ -459,6 +459,32 @@ typedef struct vxe_world_params {
 vxe_status vxe_solid_voxels_device(vxe_ctx* ctx, const int32_t* d_vox, uint32_t n, const vxe_world_params* world,
                                    uint8_t* d_out);
 
+/* Chunk builder on the device.  The reference builds chunks on CPU worker
+ * threads (build_chunk_svo_sparse_cancelable_with_scratch, svo/builder.rs:
+ * 846-986, called from streaming/build_pool.rs:19-25); this runs the same
+ * pipeline -- material fill, colinfo, macro bits, ground min-mip, octree with
+ * stone / uniform collapse, ropes -- for n chunks at once and writes, for
+ * chunk i of the n chunk coordinates (int32 x, y, z triples), exactly the
+ * records vxe_build_chunk returns:
+ *   d_nodes[i*node_cap ...], d_ropes[i*node_cap ...]   node_count records
+ *   d_macro[i*16 ...], d_colinfo[i*2048 ...]
+ *   d_counts[2i] = node_count, d_counts[2i+1] = solid_voxels.
+ * All buffers are device memory.  A chunk whose node_count exceeds node_cap
+ * gets its counts, macro and colinfo words but no nodes or ropes: build it
+ * again with a larger cap (VXE_BUILD_NODE_CAP_MAX always fits; node_cap 0
+ * only counts).  Launched on the context's world-write stream;
+ * vxe_synchronize waits for it. */
+#define VXE_BUILD_NODE_CAP_MAX 299593u /* 1 + 8 + 8^2 + ... + 8^6 */
+#define VXE_BUILD_BATCH_MAX 512u
+vxe_status vxe_build_chunks_device(vxe_ctx* ctx, const vxe_world_params* world, const int32_t* d_coords, uint32_t n,
+                                   uint32_t node_cap, vxe_node* d_nodes, vxe_node_ropes* d_ropes, uint32_t* d_macro,
+                                   uint32_t* d_colinfo, uint32_t* d_counts);
+/* Device time (ms) of the last vxe_build_chunks_device call's kernels. */
+typedef struct vxe_build_timings {
+  double ground, fill, svo;
+} vxe_build_timings;
+vxe_status vxe_get_build_timings(vxe_ctx* ctx, vxe_build_timings* out);
+
 typedef struct vxe_built_chunk {
   vxe_node* nodes;
   vxe_node_ropes* ropes;

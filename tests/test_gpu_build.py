@@ -1,0 +1,113 @@
+"""The chunk builder on the device against the host builder (the C++ port of
+svo/builder.rs:846-986 and builder_svo.rs / builder_ropes.rs): nodes, ropes,
+macro words, colinfo words and counts byte for byte."""
+import numpy as np
+import pytest
+
+from vxe import _abi as A
+from vxe import scenes
+from vxe.renderer import Renderer
+from vxe.world import World, WorldSpec, build_chunk
+
+pytestmark = pytest.mark.gpu
+
+CARVE = WorldSpec(seed=12345, height_min=8, height_max=48, dirt_depth=3, carve_mod=50)
+FEATURES = WorldSpec(seed=99, height_min=10, height_max=40, dirt_depth=3, cave_threshold=0.55, features=3)
+PLAIN = WorldSpec(seed=7, height_min=20, height_max=100, dirt_depth=4, height_scale_vox=96.0, features=1)
+
+# surface chunks, negative coordinates, an all-air chunk, all-solid chunks
+# below the surface (the root collapses to one stone leaf without caves or
+# carving), the surface crossing chunk boundaries in y
+KEYS = [(0, 0, 0), (1, 0, -1), (-2, 0, 3), (5, 0, 5), (0, 3, 0), (0, -1, 0), (-3, -2, -4), (2, 1, 2), (7, 0, -6)]
+
+
+def _renderer():
+    return Renderer(64, 36, 1.0, node_capacity=1 << 16, chunk_capacity=16, grid_capacity=16, clip_levels=1,
+                    clip_res=16)
+
+
+def _compare(spec, keys, out):
+    counts = out["counts"].cpu().numpy().view(np.uint32)
+    macro = out["macro"].cpu().numpy().view(np.uint32)
+    colinfo = out["colinfo"].cpu().numpy().view(np.uint32)
+    for j, key in enumerate(keys):
+        ref = build_chunk(spec, *key)
+        n = len(ref.nodes)
+        assert counts[j, 0] == n, (key, counts[j, 0], n)
+        assert counts[j, 1] == ref.solid_voxels, key
+        assert np.array_equal(macro[j], ref.macro), key
+        assert np.array_equal(colinfo[j], ref.colinfo), key
+        nodes = out["nodes"][j, :n].cpu().numpy().view(np.uint32).reshape(-1)
+        ropes = out["ropes"][j, :n].cpu().numpy().view(np.uint32).reshape(-1)
+        assert np.array_equal(nodes, ref.nodes.view(np.uint32).reshape(-1)), key
+        assert np.array_equal(ropes, ref.ropes.view(np.uint32).reshape(-1)), key
+
+
+@pytest.mark.parametrize("spec", [CARVE, FEATURES, PLAIN], ids=["carve", "caves_trees_lights", "plain_trees"])
+def test_device_build_equals_host_builder(spec):
+    import torch
+
+    r = _renderer()
+    try:
+        coords = torch.tensor(KEYS, dtype=torch.int32, device="cuda:0")
+        out = r.build_chunks(spec.params(), coords)
+        _compare(spec, KEYS, out)
+        counts = out["counts"].cpu().numpy()
+        assert counts[:, 0].max() > 1000 and counts[:, 0].min() == 1  # full trees and collapsed roots
+        t = r.build_timings()
+        assert t["fill"] > 0 and t["svo"] > 0
+    finally:
+        r.close()
+
+
+def test_device_build_config2_grid_and_world_prebuild():
+    """Every chunk of the 16x4x16 config-2 grid in batches, through
+    World.prebuild_device, against World.prebuild on the host builder."""
+    import torch
+
+    sc = scenes.config2(present=(64, 36))
+    keys = [(x, y, z) for z in range(16) for y in range(4) for x in range(16)]
+    r = _renderer()
+    try:
+        wd = World(sc.spec, sc.grid_origin, sc.grid_dims, sc.node_capacity)
+        wd.prebuild_device(r, keys, batch=128)
+        rng = np.random.default_rng(3)
+        pick = [keys[i] for i in rng.choice(len(keys), 48, replace=False)]
+        for key in pick:
+            ref = build_chunk(sc.spec, *key)
+            got = wd.cache[key]
+            assert got.solid_voxels == ref.solid_voxels, key
+            assert np.array_equal(got.nodes.view(np.uint32), ref.nodes.view(np.uint32)), key
+            assert np.array_equal(got.ropes.view(np.uint32), ref.ropes.view(np.uint32)), key
+            assert np.array_equal(got.macro, ref.macro) and np.array_equal(got.colinfo, ref.colinfo), key
+        # the largest batch in one call
+        coords = torch.tensor(keys[:A.BUILD_BATCH_MAX] if len(keys) >= A.BUILD_BATCH_MAX else keys,
+                              dtype=torch.int32, device="cuda:0")
+        out = r.build_chunks(sc.spec.params(), coords, node_cap=70000)
+        counts = out["counts"].cpu().numpy().view(np.uint32)
+        for j in rng.choice(len(coords), 8, replace=False):
+            key = tuple(int(v) for v in coords[j].tolist())
+            if counts[j, 0] <= 70000:
+                _compare(sc.spec, [key], {k: v[j:j + 1] for k, v in out.items()})
+    finally:
+        r.close()
+
+
+def test_node_cap_overflow_still_reports_counts():
+    import torch
+
+    r = _renderer()
+    try:
+        keys = [(0, 0, 0), (0, -1, 0)]
+        coords = torch.tensor(keys, dtype=torch.int32, device="cuda:0")
+        out = r.build_chunks(CARVE.params(), coords, node_cap=64)
+        counts = out["counts"].cpu().numpy().view(np.uint32)
+        ref0 = build_chunk(CARVE, *keys[0])
+        assert counts[0, 0] == len(ref0.nodes) > 64
+        assert counts[0, 1] == ref0.solid_voxels
+        assert np.array_equal(out["colinfo"][0].cpu().numpy().view(np.uint32), ref0.colinfo)
+        # a count-only call (cap 0) also gives the counts
+        z = r.build_chunks(CARVE.params(), coords, node_cap=0)
+        assert np.array_equal(z["counts"].cpu().numpy(), out["counts"].cpu().numpy())
+    finally:
+        r.close()

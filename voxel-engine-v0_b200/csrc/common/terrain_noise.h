@@ -1,6 +1,7 @@
 // Seeded terrain noise of the synthetic worlds (world/hash.rs:2-32 hashing,
-// lattice value noise with smoothstep interpolation, 4-octave height field),
-// shared by the host producer and the device clipmap generator so both
+// lattice value noise with smoothstep interpolation, 4-octave height field,
+// caves, carving, trees and light voxels), shared by the host producer and
+// the device clipmap generator and chunk builder so all of them
 // evaluate the same binary64 operation sequence (no contraction on either
 // side: g++ -ffp-contract=off, nvcc -fmad=false).
 #pragma once
@@ -77,6 +78,72 @@ VXE_HD int32_t ground(const vxe_world_params& p, int32_t wx, int32_t wz) {
   const int32_t span = p.height_max - p.height_min + 1;
   const int32_t h = p.height_min + (int32_t)floor(n * (double)span);
   return h < p.height_min ? p.height_min : (h > p.height_max ? p.height_max : h);
+}
+
+// Cave carving: two octaves of 3D value noise above the threshold.
+VXE_HD bool cave(const vxe_world_params& p, int32_t wx, int32_t wy, int32_t wz) {
+  if (!(p.cave_threshold < 1.0f)) return false;
+  const uint32_t s = p.seed ^ 0xCA7E5EEDu;
+  const double v = (value_noise3(s, wx / 16.0, wy / 16.0, wz / 16.0) +
+                    0.5 * value_noise3(s + 7u, wx / 8.0, wy / 8.0, wz / 8.0)) /
+                   1.5;
+  return v > (double)p.cave_threshold;
+}
+
+// Trees: one candidate per 1 m cell (10 voxels); trunk of WOOD, crown LEAF.
+struct Tree {
+  int32_t x, z, base, trunk, r;
+};
+VXE_HD bool tree_at_cell(const vxe_world_params& p, int32_t mx, int32_t mz, Tree* t) {
+  const uint32_t h = hash2(p.seed ^ 0x7EEu, mx, mz);
+  if (h % 61u != 0u) return false;
+  t->x = mx * 10 + 5;
+  t->z = mz * 10 + 5;
+  t->base = ground(p, t->x, t->z) + 1;
+  t->trunk = 14 + (int32_t)((h >> 8) % 10u);
+  t->r = 5 + (int32_t)((h >> 16) % 4u);
+  return true;
+}
+
+// Decoration above the surface (g = column ground): light voxels, trees.
+VXE_HD uint8_t decor(const vxe_world_params& p, int32_t wx, int32_t wy, int32_t wz, int32_t g) {
+  if (p.features & 2u) {
+    if (wy == g + 1 && hash2(p.seed ^ 0x119u, wx, wz) % 331u == 0u) return VXE_MAT_LIGHT;
+  }
+  if (p.features & 1u) {
+    const int32_t mx0 = (int32_t)floor((wx - 14) / 10.0), mx1 = (int32_t)floor((wx + 14) / 10.0);
+    const int32_t mz0 = (int32_t)floor((wz - 14) / 10.0), mz1 = (int32_t)floor((wz + 14) / 10.0);
+    uint8_t best = VXE_MAT_AIR;
+    for (int32_t mz = mz0; mz <= mz1; ++mz)
+      for (int32_t mx = mx0; mx <= mx1; ++mx) {
+        Tree t;
+        if (!tree_at_cell(p, mx, mz, &t)) continue;
+        if (wx == t.x && wz == t.z && wy >= t.base && wy < t.base + t.trunk) return VXE_MAT_WOOD;
+        const int32_t cy = t.base + t.trunk;
+        const int32_t dx = wx - t.x, dy = wy - cy, dz = wz - t.z;
+        if (dx * dx + dy * dy + dz * dz <= t.r * t.r) best = VXE_MAT_LEAF;
+      }
+    return best;
+  }
+  return VXE_MAT_AIR;
+}
+
+// Material of world voxel (wx, wy, wz) over a column of ground height g.
+VXE_HD uint8_t material(const vxe_world_params& p, int32_t wx, int32_t wy, int32_t wz, int32_t g) {
+  uint8_t m;
+  if (wy < g) {
+    m = (wy >= g - p.dirt_depth) ? VXE_MAT_DIRT : VXE_MAT_STONE;
+  } else if (wy == g) {
+    m = VXE_MAT_GRASS;
+  } else {
+    m = VXE_MAT_AIR;
+  }
+  if (m != VXE_MAT_AIR) {
+    if (cave(p, wx, wy, wz)) m = VXE_MAT_AIR;
+    else if (p.carve_mod != 0u && hash3(p.seed ^ 0x5EEDu, wx, wy, wz) % p.carve_mod == 0u) m = VXE_MAT_AIR;
+  }
+  if (m == VXE_MAT_AIR && wy > g && p.features != 0u) m = decor(p, wx, wy, wz, g);
+  return m;
 }
 
 // Clipmap texel at world (x, z) metres: the surface height in metres

@@ -32,79 +32,15 @@ constexpr int kSide = 64;
 constexpr int kSide2 = kSide * kSide;
 constexpr int kSide3 = kSide2 * kSide;
 
-// Hashing and value noise: terrain_noise.h (shared with the device).
-using vxe::terrain::fade;
-using vxe::terrain::hash2;
-using vxe::terrain::hash3;
-using vxe::terrain::mix32;
-using vxe::terrain::u01;
-using vxe::terrain::value_noise2;
-using vxe::terrain::value_noise3;
+// Hashing, value noise and the material rules: terrain_noise.h (shared with
+// the device).
 
 struct World {
   vxe_world_params p;
 
   int32_t ground(int32_t wx, int32_t wz) const { return vxe::terrain::ground(p, wx, wz); }
-
-  bool cave(int32_t wx, int32_t wy, int32_t wz) const {
-    if (!(p.cave_threshold < 1.0f)) return false;
-    const uint32_t s = p.seed ^ 0xCA7E5EEDu;
-    const double v = (value_noise3(s, wx / 16.0, wy / 16.0, wz / 16.0) +
-                      0.5 * value_noise3(s + 7u, wx / 8.0, wy / 8.0, wz / 8.0)) /
-                     1.5;
-    return v > (double)p.cave_threshold;
-  }
-
-  // Trees: one candidate per 1 m cell (10 voxels); trunk of WOOD, crown LEAF.
-  struct Tree { int32_t x, z, base, trunk, r; };
-  bool tree_at_cell(int32_t mx, int32_t mz, Tree* t) const {
-    const uint32_t h = hash2(p.seed ^ 0x7EEu, mx, mz);
-    if (h % 61u != 0u) return false;
-    t->x = mx * 10 + 5;
-    t->z = mz * 10 + 5;
-    t->base = ground(t->x, t->z) + 1;
-    t->trunk = 14 + (int32_t)((h >> 8) % 10u);
-    t->r = 5 + (int32_t)((h >> 16) % 4u);
-    return true;
-  }
-
-  uint8_t decor(int32_t wx, int32_t wy, int32_t wz, int32_t g) const {
-    if (p.features & 2u) {
-      if (wy == g + 1 && hash2(p.seed ^ 0x119u, wx, wz) % 331u == 0u) return VXE_MAT_LIGHT;
-    }
-    if (p.features & 1u) {
-      const int32_t mx0 = (int32_t)std::floor((wx - 14) / 10.0), mx1 = (int32_t)std::floor((wx + 14) / 10.0);
-      const int32_t mz0 = (int32_t)std::floor((wz - 14) / 10.0), mz1 = (int32_t)std::floor((wz + 14) / 10.0);
-      uint8_t best = VXE_MAT_AIR;
-      for (int32_t mz = mz0; mz <= mz1; ++mz)
-        for (int32_t mx = mx0; mx <= mx1; ++mx) {
-          Tree t;
-          if (!tree_at_cell(mx, mz, &t)) continue;
-          if (wx == t.x && wz == t.z && wy >= t.base && wy < t.base + t.trunk) return VXE_MAT_WOOD;
-          const int32_t cy = t.base + t.trunk;
-          const int32_t dx = wx - t.x, dy = wy - cy, dz = wz - t.z;
-          if (dx * dx + dy * dy + dz * dz <= t.r * t.r) best = VXE_MAT_LEAF;
-        }
-      return best;
-    }
-    return VXE_MAT_AIR;
-  }
-
   uint8_t material(int32_t wx, int32_t wy, int32_t wz, int32_t g) const {
-    uint8_t m;
-    if (wy < g) {
-      m = (wy >= g - p.dirt_depth) ? VXE_MAT_DIRT : VXE_MAT_STONE;
-    } else if (wy == g) {
-      m = VXE_MAT_GRASS;
-    } else {
-      m = VXE_MAT_AIR;
-    }
-    if (m != VXE_MAT_AIR) {
-      if (cave(wx, wy, wz)) m = VXE_MAT_AIR;
-      else if (p.carve_mod != 0u && hash3(p.seed ^ 0x5EEDu, wx, wy, wz) % p.carve_mod == 0u) m = VXE_MAT_AIR;
-    }
-    if (m == VXE_MAT_AIR && wy > g && p.features != 0u) m = decor(wx, wy, wz, g);
-    return m;
+    return vxe::terrain::material(p, wx, wy, wz, g);
   }
 };
 

@@ -27,6 +27,7 @@
 #include "kernels/batch_kernels.cuh"
 #include "common/terrain_noise.h"
 #include "kernels/frame_kernels.cuh"
+#include "kernels/build_kernels.cuh"
 #include "vxe/vxe.h"
 
 using vxe::dev::FrameArgs;
@@ -133,6 +134,11 @@ struct vxe_ctx {
   DevBuf nodes, ropes, metas, macro, colinfo, grid, clip_tex, errword;
   DevBuf slot_lights;  // per slot: holds a LIGHT leaf (k_slot_lights)
   DevBuf slot_top;     // per slot: top of its non-air leaves, voxels (k_slot_lights)
+  // chunk builder: per-chunk scratch (materials, ground, level-5 cell states
+  // and child offsets) and events around its three kernels
+  DevBuf build_scratch;
+  cudaEvent_t build_ev[4] = {};
+  bool build_timed = false;
   GrassTable gt;
   FrameState fr;  // the context's own frame
   SideStream side;  // its fork stream
@@ -843,7 +849,7 @@ void vxe_destroy(vxe_ctx* c) {
   if (c->fr.fgraph) cudaGraphDestroy(c->fr.fgraph);
   for (auto& L : c->lanes)  // lanes read the arenas: drain them before freeing
     if (L.stream) cudaStreamSynchronize(L.stream);
-  for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword, &c->slot_lights, &c->slot_top,
+  for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword, &c->slot_lights, &c->slot_top, &c->build_scratch,
                   &c->q_in, &c->q_out, &c->gt.rec, &c->gt.taper, &c->gt.state, &c->gt.frames,
                   &c->gt.list, &c->gt.list_n})
     release(*b);
@@ -866,6 +872,8 @@ void vxe_destroy(vxe_ctx* c) {
     cudaStreamSynchronize(c->aux);
     cudaStreamDestroy(c->aux);
   }
+  for (auto& e : c->build_ev)
+    if (e) cudaEventDestroy(e);
   if (c->pool) cudaMemPoolDestroy(c->pool);
   for (auto& e : c->rd_ev)
     if (e) cudaEventDestroy(e);
@@ -1395,6 +1403,71 @@ vxe_status vxe_solid_voxels_device(vxe_ctx* c, const int32_t* d_vox, uint32_t n,
   const unsigned grid = (unsigned)std::min<uint64_t>(((uint64_t)n + 255) / 256, (uint64_t)c->shade_wave);
   k_solid_voxels<<<grid, 256, 0, c->compute>>>(A, d_vox, n, wp, world ? 1u : 0u, d_out);
   CK(cudaGetLastError());
+  return VXE_OK;
+}
+
+vxe_status vxe_build_chunks_device(vxe_ctx* c, const vxe_world_params* world, const int32_t* d_coords, uint32_t n,
+                                   uint32_t node_cap, vxe_node* d_nodes, vxe_node_ropes* d_ropes, uint32_t* d_macro,
+                                   uint32_t* d_colinfo, uint32_t* d_counts) {
+  namespace vb = vxe::build;
+  if (!c || !world) return fail(c, VXE_ERR_INVALID_ARG, "null builder arguments");
+  if (n == 0) return VXE_OK;
+  if (!d_coords || !d_macro || !d_colinfo || !d_counts || (node_cap && (!d_nodes || !d_ropes)))
+    return fail(c, VXE_ERR_INVALID_ARG, "null builder buffers");
+  if (n > VXE_BUILD_BATCH_MAX) return fail(c, VXE_ERR_CAPACITY, "%u chunks > %u per build call", n, VXE_BUILD_BATCH_MAX);
+  if (node_cap > VXE_BUILD_NODE_CAP_MAX)
+    return fail(c, VXE_ERR_INVALID_ARG, "node_cap %u > %u", node_cap, VXE_BUILD_NODE_CAP_MAX);
+  cudaSetDevice(c->device);
+  constexpr size_t kPerChunk = (size_t)vb::kVoxels + (size_t)vb::kColumns * 4 + (size_t)vb::kCells5 * 8;
+  const size_t need = kPerChunk * n;
+  if (c->build_scratch.bytes < need) {
+    vxe_status st = alloc(c, c->build_scratch, need);
+    if (st != VXE_OK) return st;
+  }
+  for (auto& e : c->build_ev)
+    if (!e) CK(cudaEventCreate(&e));
+  vb::BuildArgs B;
+  std::memset(&B, 0, sizeof B);
+  B.wp = *world;
+  B.coords = d_coords;
+  B.n = n;
+  char* base = (char*)c->build_scratch.p;
+  B.mat = (uint8_t*)base;
+  B.ground = (int32_t*)(base + (size_t)vb::kVoxels * n);
+  B.st5 = (uint32_t*)(base + ((size_t)vb::kVoxels + (size_t)vb::kColumns * 4) * n);
+  B.kb5 = B.st5 + (size_t)vb::kCells5 * n;
+  B.node_cap = node_cap;
+  B.nodes = d_nodes;
+  B.ropes = d_ropes;
+  B.macro = d_macro;
+  B.colinfo = d_colinfo;
+  B.counts = d_counts;
+  cudaStream_t st = c->upload;
+  CK(cudaEventRecord(c->build_ev[0], st));
+  vb::k_build_ground<<<n * 16u, 256, 0, st>>>(B);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->build_ev[1], st));
+  vb::k_build_fill<<<n * 1024u, 256, 0, st>>>(B);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->build_ev[2], st));
+  vb::k_build_svo<<<n, vb::SVO_THREADS, 0, st>>>(B);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->build_ev[3], st));
+  c->build_timed = true;
+  return VXE_OK;
+}
+
+vxe_status vxe_get_build_timings(vxe_ctx* c, vxe_build_timings* t) {
+  if (!c || !t) return fail(c, VXE_ERR_INVALID_ARG, "null build timings");
+  std::memset(t, 0, sizeof *t);
+  if (!c->build_timed) return VXE_OK;
+  cudaSetDevice(c->device);
+  CK(cudaEventSynchronize(c->build_ev[3]));
+  float ms[3];
+  for (int i = 0; i < 3; ++i) CK(cudaEventElapsedTime(&ms[i], c->build_ev[i], c->build_ev[i + 1]));
+  t->ground = ms[0];
+  t->fill = ms[1];
+  t->svo = ms[2];
   return VXE_OK;
 }
 

@@ -118,6 +118,14 @@ class ClipPatchGeom(C.Structure):
                [(n, C.c_float) for n in ("ox_m", "oz_m", "cell_m")]
 
 
+class BuildTimings(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("ground", "fill", "svo")]
+
+
+BUILD_NODE_CAP_MAX = 299593
+BUILD_BATCH_MAX = 512
+
+
 class WorldParams(C.Structure):
     _fields_ = [("seed", C.c_uint32), ("height_min", C.c_int32), ("height_max", C.c_int32),
                 ("dirt_depth", C.c_int32), ("carve_mod", C.c_uint32), ("cave_threshold", C.c_float),
@@ -221,6 +229,9 @@ SIGNATURES = {
     "vxe_clipmap_update_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_float]),
     "vxe_read_clipmap": (C.c_int, [C.c_void_p, P(C.c_float), C.c_size_t]),
     "vxe_solid_voxels_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, P(WorldParams), C.c_void_p]),
+    "vxe_build_chunks_device": (C.c_int, [C.c_void_p, P(WorldParams), C.c_void_p, C.c_uint32, C.c_uint32,
+                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "vxe_get_build_timings": (C.c_int, [C.c_void_p, P(BuildTimings)]),
 }
 
 

@@ -26,6 +26,7 @@ class Renderer:
             raise A.VxeError(st, "vxe_create")
         self._ctx = h
         self.clip_levels, self.clip_res = clip_levels, clip_res
+        self.device = device
         self.render_scale = render_scale
         self.resize_output(width, height)
 
@@ -140,6 +141,41 @@ class Renderer:
                     "vxe_solid_voxels_device")
         self.synchronize()
         return out
+
+    def build_chunks(self, world_params, coords, node_cap=None):
+        """Builds chunks on the device (the GPU counterpart of the chunk builder,
+        svo/builder.rs:846-986).  `coords`: torch int32 tensor (n, 3) of chunk
+        coordinates on this context's device, n <= BUILD_BATCH_MAX.  Returns a
+        dict of device tensors: nodes (n, cap, 4) u32, ropes (n, cap, 8) u32,
+        macro (n, 16), colinfo (n, 2048), counts (n, 2) = (node_count,
+        solid_voxels); a chunk whose node_count exceeds `node_cap` carries no
+        nodes or ropes (the default cap always fits)."""
+        import torch
+
+        coords = coords.to(torch.int32).contiguous()
+        n = coords.shape[0]
+        cap = A.BUILD_NODE_CAP_MAX if node_cap is None else int(node_cap)
+        dev = coords.device
+        out = {
+            "nodes": torch.empty((n, cap, 4), dtype=torch.int32, device=dev),
+            "ropes": torch.empty((n, cap, 8), dtype=torch.int32, device=dev),
+            "macro": torch.empty((n, A.MACRO_WORDS_PER_CHUNK), dtype=torch.int32, device=dev),
+            "colinfo": torch.empty((n, A.COLINFO_WORDS_PER_CHUNK), dtype=torch.int32, device=dev),
+            "counts": torch.empty((n, 2), dtype=torch.int32, device=dev),
+        }
+        torch.cuda.current_stream().synchronize()
+        self._check(self._lib.vxe_build_chunks_device(
+            self._ctx, C.byref(world_params), coords.data_ptr(), n, cap, out["nodes"].data_ptr(),
+            out["ropes"].data_ptr(), out["macro"].data_ptr(), out["colinfo"].data_ptr(), out["counts"].data_ptr()),
+            "vxe_build_chunks_device")
+        self.synchronize()
+        return out
+
+    def build_timings(self) -> dict:
+        """Device milliseconds of the last build_chunks call, per kernel."""
+        t = A.BuildTimings()
+        self._check(self._lib.vxe_get_build_timings(self._ctx, C.byref(t)), "vxe_get_build_timings")
+        return {"ground": t.ground, "fill": t.fill, "svo": t.svo}
 
     def read_clipmap(self) -> np.ndarray:
         """The clipmap texture (levels, res, res) after the writes queued so far."""

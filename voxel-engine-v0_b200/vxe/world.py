@@ -247,6 +247,27 @@ class World:
             for k, data in zip(todo, ex.map(self.builder, todo)):
                 self.cache[k] = data
 
+    def prebuild_device(self, renderer, keys, batch: int = 64) -> None:
+        """Builds missing chunks on the device (Renderer.build_chunks) in batches
+        and keeps the host copies the upload path reads; the results equal
+        prebuild()'s byte for byte."""
+        import torch
+
+        todo = [k for k in keys if k not in self.cache]
+        wp = self.spec.params()
+        for i in range(0, len(todo), batch):
+            part = todo[i:i + batch]
+            coords = torch.tensor(part, dtype=torch.int32, device=f"cuda:{renderer.device}")
+            out = renderer.build_chunks(wp, coords)
+            counts = out["counts"].cpu().numpy().view(np.uint32)
+            macro = out["macro"].cpu().numpy().view(np.uint32)
+            colinfo = out["colinfo"].cpu().numpy().view(np.uint32)
+            for j, key in enumerate(part):
+                n = int(counts[j, 0])
+                nodes = out["nodes"][j, :n].cpu().numpy().view(np.uint32).reshape(-1).view(A.NODE_DTYPE)
+                ropes = out["ropes"][j, :n].cpu().numpy().view(np.uint32).reshape(-1).view(A.ROPES_DTYPE)
+                self.cache[key] = ChunkData(key, nodes, ropes, macro[j].copy(), colinfo[j].copy(), int(counts[j, 1]))
+
     def populate(self) -> list[Upload]:
         self.prebuild(list(self.keys_in_grid()))
         ups = [self.add(k) for k in self.keys_in_grid() if k not in self.key_to_slot]

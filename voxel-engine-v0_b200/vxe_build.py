@@ -45,7 +45,7 @@ def _nvcc() -> str:
 def _sources():
     cu = sorted(CSRC.glob("*.cu"))
     cpp = sorted((CSRC / "host").glob("*.cpp"))
-    headers = sorted(CSRC.rglob("*.cuh")) + sorted(INCLUDE.rglob("*.h"))
+    headers = sorted(CSRC.rglob("*.cuh")) + sorted(CSRC.rglob("*.h")) + sorted(INCLUDE.rglob("*.h"))
     return cu, cpp, headers
 
 
