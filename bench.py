@@ -417,9 +417,9 @@ def run_builder(dev, steps: int = 3, warmup: int = 2):
         cap = int(max(int(c[:, 0].max()) for c in counts))
         solid = int(sum(int(c[:, 1].sum()) for c in counts))
         nodes_total = int(sum(int(c[:, 0].sum()) for c in counts))
-        per = {"ground": [], "fill": [], "svo": []}
+        per = {"columns": [], "svo": []}
         for it in range(warmup + steps):
-            step = {"ground": 0.0, "fill": 0.0, "svo": 0.0}
+            step = {"columns": 0.0, "svo": 0.0}
             for c in parts:
                 r.build_chunks(wp, c, node_cap=cap)
                 for k, v in r.build_timings().items():
@@ -427,7 +427,7 @@ def run_builder(dev, steps: int = 3, warmup: int = 2):
             if it >= warmup:
                 for k in per:
                     per[k].append(step[k])
-        dev_ms = statistics.mean(per["ground"]) + statistics.mean(per["fill"]) + statistics.mean(per["svo"])
+        dev_ms = statistics.mean(per["columns"]) + statistics.mean(per["svo"])
         wd = World(sc.spec, sc.grid_origin, sc.grid_dims, sc.node_capacity)
         wd.prebuild_device(r, keys[:64], batch=64)  # warm
         wd = World(sc.spec, sc.grid_origin, sc.grid_dims, sc.node_capacity)

@@ -481,7 +481,8 @@ vxe_status vxe_build_chunks_device(vxe_ctx* ctx, const vxe_world_params* world, 
                                    uint32_t* d_colinfo, uint32_t* d_counts);
 /* Device time (ms) of the last vxe_build_chunks_device call's kernels. */
 typedef struct vxe_build_timings {
-  double ground, fill, svo;
+  double columns; /* ground, materials, colinfo, level-5 cell states */
+  double svo;     /* octree levels 4..0, offsets, nodes, ropes, macro bits */
 } vxe_build_timings;
 vxe_status vxe_get_build_timings(vxe_ctx* ctx, vxe_build_timings* out);
 

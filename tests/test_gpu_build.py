@@ -55,7 +55,7 @@ def test_device_build_equals_host_builder(spec):
         counts = out["counts"].cpu().numpy()
         assert counts[:, 0].max() > 1000 and counts[:, 0].min() == 1  # full trees and collapsed roots
         t = r.build_timings()
-        assert t["fill"] > 0 and t["svo"] > 0
+        assert t["columns"] > 0 and t["svo"] > 0
     finally:
         r.close()
 

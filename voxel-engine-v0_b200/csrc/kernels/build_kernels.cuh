@@ -7,11 +7,16 @@
 // and ropes (builder_ropes.rs:76-195).  These kernels produce the same
 // records byte for byte for a batch of chunks:
 //
-//   k_build_ground  one thread per column: surface height (z*64 + x)
-//   k_build_fill    one thread per voxel: material (y*64*64 + z*64 + x)
-//   k_build_svo     one CTA per chunk: colinfo, macro bits, the octree cell
-//                   states bottom-up, one exclusive scan per level for the
-//                   packed child offsets, node emission, ropes top-down.
+//   k_build_columns  one thread per voxel column, 16 blocks per chunk: the
+//                    surface height, the 64 materials of the column, its
+//                    colinfo entry, and -- with the 2x2 neighbour columns
+//                    read by warp shuffles -- the level-1 ground minimum and
+//                    the state words of the level-5 cells (2^3 voxels) it
+//                    heads, plus a per-block solid voxel count;
+//   k_build_svo      one CTA per chunk: ground min-mip, the level-5 child
+//                    offsets (one exclusive scan), the cell states of
+//                    levels 4..0, their scans, node emission, ropes top-down,
+//                    macro bits.
 //
 // Octree cells.  A cell of level l (0 = the chunk, 6 = a voxel) holds
 // 2^(6-l) voxels per side; its cells are numbered px + pz*S + py*S*S with
@@ -60,10 +65,12 @@ __host__ __device__ constexpr uint32_t mip_off(int lv) {
 
 struct BuildArgs {
   vxe_world_params wp;
+  double cave_smin;      // least s = n1 + 0.5 n2 with s / 1.5 > cave threshold
   const int32_t* coords;  // n chunk coordinates (x, y, z)
   uint32_t n;
   uint8_t* mat;           // n * 64^3 materials
-  int32_t* ground;        // n * 64^2 surface heights
+  int32_t* mip1;          // n * 32^2 level-1 ground minima (2x2 columns)
+  uint32_t* solid_part;   // n * 16 solid voxel counts, one per column block
   uint32_t* st5;          // n * 32^3 level-5 state words
   uint32_t* kb5;          // n * 32^3 level-5 child offsets
   uint32_t node_cap;
@@ -73,23 +80,6 @@ struct BuildArgs {
   uint32_t* colinfo;      // n * 2048
   uint32_t* counts;       // n * 2: node_count, solid_voxels
 };
-
-__global__ void __launch_bounds__(256) k_build_ground(const __grid_constant__ BuildArgs B) {
-  const uint32_t chunk = blockIdx.x >> 4, col = ((blockIdx.x & 15u) << 8) | threadIdx.x;
-  if (chunk >= B.n) return;
-  const int32_t ox = B.coords[3 * chunk] * kSide, oz = B.coords[3 * chunk + 2] * kSide;
-  B.ground[(size_t)chunk * kColumns + col] = terrain::ground(B.wp, ox + (int32_t)(col & 63u), oz + (int32_t)(col >> 6));
-}
-
-__global__ void __launch_bounds__(256) k_build_fill(const __grid_constant__ BuildArgs B) {
-  const uint32_t chunk = blockIdx.x >> 10, i = ((blockIdx.x & 1023u) << 8) | threadIdx.x;
-  if (chunk >= B.n) return;
-  const int32_t ox = B.coords[3 * chunk] * kSide, oy = B.coords[3 * chunk + 1] * kSide,
-                oz = B.coords[3 * chunk + 2] * kSide;
-  const int32_t g = B.ground[(size_t)chunk * kColumns + (i & 4095u)];
-  B.mat[(size_t)chunk * kVoxels + i] =
-      terrain::material(B.wp, ox + (int32_t)(i & 63u), oy + (int32_t)(i >> 12), oz + (int32_t)((i >> 6) & 63u), g);
-}
 
 // Exclusive scan of one value per thread over the CTA; *total gets the sum.
 // Ends with a barrier, so `ws` may be reused at once.
@@ -146,6 +136,205 @@ __device__ __forceinline__ uint32_t voxel_state(uint32_t m) {
   return m ? (0x1u | (m << 8) | ST_LEAF | ST_FULL) : 0u;
 }
 
+// Materials of one voxel column, bottom-up.  terrain::material evaluated
+// with its per-column work done once, every value still going through the
+// same operations on the same operands, so the materials are the same:
+//   - cave noise: per octave (lattice 16 and 8 voxels) the x-interpolated
+//     lattice values of the current y cell are kept; moving up one cell
+//     reuses the upper row as the new lower one.  The y fraction of a lattice
+//     cell depends only on wy mod 16 (or 8), so its fade comes from a table
+//     filled with terrain::fade.  The cave test s / 1.5 > threshold is
+//     monotone in s = n1 + 0.5 n2, so it is s >= cave_smin, the least binary64
+//     s that passes, found on the host;
+//   - the light voxel test and the trees whose trunk or crown reaches the
+//     column are found once.
+struct ColumnMaterial {
+  int32_t wx, wz, g;
+  bool caves, light;
+  int32_t ix[2], iz[2], iy[2];
+  double fx[2], fz[2], yz[2][4];
+  uint32_t ntrees;
+  // trees reaching the column (at most the 4 x 4 candidate cells); kept apart
+  // from the scalars above so those stay in registers
+  struct T {
+    int32_t dxx, dzz, cy, r2, base, top;  // base = INT32_MAX unless the trunk is this column
+  };
+
+  __device__ void init(const vxe_world_params& p, int32_t x, int32_t z, int32_t ground, T (&trees)[16]) {
+    wx = x;
+    wz = z;
+    g = ground;
+    caves = p.cave_threshold < 1.0f;
+#pragma unroll
+    for (int o = 0; o < 2; ++o) {
+      const double div = o == 0 ? 16.0 : 8.0;
+      const double xx = wx / div, zz = wz / div;
+      const double gx = floor(xx), gz = floor(zz);
+      ix[o] = (int32_t)gx;
+      iz[o] = (int32_t)gz;
+      fx[o] = terrain::fade(xx - gx);
+      fz[o] = terrain::fade(zz - gz);
+      iy[o] = INT32_MIN;
+    }
+    light = (p.features & 2u) && terrain::hash2(p.seed ^ 0x119u, wx, wz) % 331u == 0u;
+    ntrees = 0;
+    if (p.features & 1u) {
+      const int32_t mx0 = (int32_t)floor((wx - 14) / 10.0), mx1 = (int32_t)floor((wx + 14) / 10.0);
+      const int32_t mz0 = (int32_t)floor((wz - 14) / 10.0), mz1 = (int32_t)floor((wz + 14) / 10.0);
+      for (int32_t mz = mz0; mz <= mz1; ++mz)
+        for (int32_t mx = mx0; mx <= mx1; ++mx) {
+          terrain::Tree t;
+          if (!terrain::tree_at_cell(p, mx, mz, &t)) continue;
+          const int32_t dx = wx - t.x, dz = wz - t.z;
+          const bool trunk = wx == t.x && wz == t.z;
+          if (!trunk && dx * dx + dz * dz > t.r * t.r) continue;  // neither trunk nor crown reaches the column
+          T& e = trees[ntrees++];
+          e.dxx = dx * dx;
+          e.dzz = dz * dz;
+          e.cy = t.base + t.trunk;
+          e.r2 = t.r * t.r;
+          e.base = trunk ? t.base : INT32_MAX;
+          e.top = t.base + t.trunk;
+        }
+    }
+  }
+
+  // x-interpolated lattice row (iy + j, iz + k) of octave o
+  __device__ __forceinline__ double row(uint32_t seed, int o, int32_t cy, int k) const {
+    const double a = terrain::u01(terrain::hash3(seed, ix[o], cy, iz[o] + k));
+    const double b = terrain::u01(terrain::hash3(seed, ix[o] + 1, cy, iz[o] + k));
+    return a + (b - a) * fx[o];
+  }
+
+  // value_noise3 at (wx, wy, wz) / (16 or 8) for octave o; fy = fade of the
+  // y fraction (table)
+  __device__ __forceinline__ double noise(uint32_t seed, int o, int32_t cy, double fy) {
+    if (cy != iy[o]) {
+      if (cy == iy[o] + 1) {
+        yz[o][0] = yz[o][1];
+        yz[o][2] = yz[o][3];
+      } else {
+        yz[o][0] = row(seed, o, cy, 0);
+        yz[o][2] = row(seed, o, cy, 1);
+      }
+      yz[o][1] = row(seed, o, cy + 1, 0);
+      yz[o][3] = row(seed, o, cy + 1, 1);
+      iy[o] = cy;
+    }
+    const double z0 = yz[o][0] + (yz[o][1] - yz[o][0]) * fy;
+    const double z1 = yz[o][2] + (yz[o][3] - yz[o][2]) * fy;
+    return z0 + (z1 - z0) * fz[o];
+  }
+
+  __device__ uint32_t at(const vxe_world_params& p, double cave_smin, const double* fade16, const double* fade8,
+                         int32_t wy, const T (&trees)[16]) {
+    uint32_t m;
+    if (wy < g) {
+      m = (wy >= g - p.dirt_depth) ? VXE_MAT_DIRT : VXE_MAT_STONE;
+    } else if (wy == g) {
+      m = VXE_MAT_GRASS;
+    } else {
+      m = VXE_MAT_AIR;
+    }
+    if (m != VXE_MAT_AIR) {
+      bool cave = false;
+      if (caves) {
+        const uint32_t s = p.seed ^ 0xCA7E5EEDu;
+        const double n1 = noise(s, 0, wy >> 4, fade16[wy & 15]);
+        const double n2 = noise(s + 7u, 1, wy >> 3, fade8[wy & 7]);
+        cave = n1 + 0.5 * n2 >= cave_smin;
+      }
+      if (cave) m = VXE_MAT_AIR;
+      else if (p.carve_mod != 0u && terrain::hash3(p.seed ^ 0x5EEDu, wx, wy, wz) % p.carve_mod == 0u) m = VXE_MAT_AIR;
+    }
+    if (m == VXE_MAT_AIR && wy > g && p.features != 0u) {
+      if (light && wy == g + 1) return VXE_MAT_LIGHT;
+      uint32_t best = VXE_MAT_AIR;
+      for (uint32_t i = 0; i < ntrees; ++i) {
+        const T& e = trees[i];
+        if (wy >= e.base && wy < e.top) return VXE_MAT_WOOD;
+        const int32_t dy = wy - e.cy;
+        if (e.dxx + dy * dy + e.dzz <= e.r2) best = VXE_MAT_LEAF;
+      }
+      m = best;
+    }
+    return m;
+  }
+};
+
+// Lane layout of a column block: 16 x 16 columns, warp w covering rows
+// z = 2w, 2w+1 with lane = x | (z & 1) << 4, so a 2x2 column group is lanes
+// {l, l^1, l^16, l^17}.  Every 8 layers the group holds 4 level-5 cells; the
+// lane of role r = (x & 1) | (z & 1) << 1 builds the state of cell r.
+__global__ void __launch_bounds__(256) k_build_columns(const __grid_constant__ BuildArgs B) {
+  __shared__ uint32_t red[8];
+  __shared__ double fade16[16], fade8[8];
+  if (threadIdx.x < 16) fade16[threadIdx.x] = terrain::fade((double)threadIdx.x / 16.0);
+  else if (threadIdx.x < 24) fade8[threadIdx.x - 16] = terrain::fade((double)(threadIdx.x - 16) / 8.0);
+  __syncthreads();
+  const uint32_t chunk = blockIdx.x >> 4, tile = blockIdx.x & 15u;
+  if (chunk >= B.n) return;
+  const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+  const uint32_t x = ((tile & 3u) << 4) | (lane & 15u), z = ((tile >> 2) << 4) | (w << 1) | (lane >> 4);
+  const uint32_t role = (x & 1u) | ((z & 1u) << 1);
+  const int32_t ox = B.coords[3 * chunk] * kSide, oy = B.coords[3 * chunk + 1] * kSide,
+                oz = B.coords[3 * chunk + 2] * kSide;
+  const int32_t wx = ox + (int32_t)x, wz = oz + (int32_t)z;
+  const int32_t g = terrain::ground(B.wp, wx, wz);
+  ColumnMaterial col;
+  ColumnMaterial::T trees[16];
+  col.init(B.wp, wx, wz, g, trees);
+  const int32_t gx = min(g, __shfl_xor_sync(0xFFFFFFFFu, g, 1));
+  const int32_t gmin = min(gx, __shfl_xor_sync(0xFFFFFFFFu, gx, 16));
+  if (role == 0u) B.mip1[(size_t)chunk * 1024u + (z >> 1) * 32u + (x >> 1)] = gmin;
+  uint8_t* mat = B.mat + (size_t)chunk * kVoxels + z * 64u + x;
+  uint32_t* st5 = B.st5 + (size_t)chunk * kCells5 + (z >> 1) * 32u + (x >> 1);
+  uint32_t top = 255u, top_m = 0u, solid = 0u;
+#pragma unroll 1
+  for (uint32_t kb = 0; kb < 8u; ++kb) {
+    uint64_t acc = 0;  // 16 bits per layer pair: materials of y = 2k, 2k+1
+#pragma unroll 1
+    for (uint32_t y = 8u * kb; y < 8u * kb + 8u; ++y) {
+      const uint32_t m = col.at(B.wp, B.cave_smin, fade16, fade8, oy + (int32_t)y, trees);
+      mat[y * 4096u] = (uint8_t)m;
+      if (m) {
+        top = y;
+        top_m = m;
+        ++solid;
+      }
+      acc |= (uint64_t)m << (8u * (y - 8u * kb));
+    }
+    // lane l sends the pair its partner needs: partner role = role ^ d
+    const uint32_t own = (uint32_t)(acc >> (16u * role)) & 0xFFFFu;
+    const uint32_t fx1 = __shfl_xor_sync(0xFFFFFFFFu, (uint32_t)(acc >> (16u * (role ^ 1u))) & 0xFFFFu, 1);
+    const uint32_t fz1 = __shfl_xor_sync(0xFFFFFFFFu, (uint32_t)(acc >> (16u * (role ^ 2u))) & 0xFFFFu, 16);
+    const uint32_t fxz = __shfl_xor_sync(0xFFFFFFFFu, (uint32_t)(acc >> (16u * (role ^ 3u))) & 0xFFFFu, 17);
+    uint32_t cs[8];
+#pragma unroll
+    for (int ci = 0; ci < 8; ++ci) {
+      // the column at offset d = (dx, dz) from the group's x-even / z-even
+      // column is the lane of role d, i.e. this lane ^ (d ^ role)
+      const uint32_t f = ((uint32_t)(ci & 1) | (uint32_t)((ci >> 1) & 2)) ^ role;
+      const uint32_t pair = f == 0u ? own : f == 1u ? fx1 : f == 2u ? fz1 : fxz;
+      cs[ci] = voxel_state((pair >> (8 * ((ci >> 1) & 1))) & 0xFFu);
+    }
+    const uint32_t k = 4u * kb + role;
+    st5[k * 1024u] = cell_state(cs, oy + (int32_t)(2u * k + 1u), gmin, B.wp.dirt_depth);
+  }
+  // colinfo (builder.rs:742-771): column pairs (x even, x odd) share a word
+  const uint32_t e = top | (top_m << 8), eo = __shfl_xor_sync(0xFFFFFFFFu, e, 1);
+  if ((lane & 1u) == 0u) B.colinfo[(size_t)chunk * VXE_COLINFO_WORDS_PER_CHUNK + ((z * 64u + x) >> 1)] = e | (eo << 16);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) solid += __shfl_xor_sync(0xFFFFFFFFu, solid, o);
+  if (lane == 0) red[w] = solid;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t sum = 0;
+    for (int i = 0; i < 8; ++i) sum += red[i];
+    B.solid_part[(size_t)chunk * 16u + tile] = sum;
+  }
+}
+
 __device__ __forceinline__ vxe_node node_of(uint32_t st, uint32_t kid_base, uint32_t key) {
   vxe_node n;
   if (st & ST_LEAF) {
@@ -161,65 +350,33 @@ __device__ __forceinline__ vxe_node node_of(uint32_t st, uint32_t kid_base, uint
   return n;
 }
 
-__device__ __forceinline__ uint32_t child_of(const vxe_node* nodes, uint32_t p, uint32_t ci) {
-  const vxe_node n = nodes[p];
+// builder_ropes.rs "down": the neighbour itself when it is a leaf (or
+// absent), else its child on the near side (`ci`), absent when not present.
+__device__ __forceinline__ uint32_t rope_down(uint32_t nei, const vxe_node& n, uint32_t ci) {
+  if (nei == kInvalid) return kInvalid;
+  if (n.child_base == kInvalid) return nei;
   if (!(n.child_mask & (1u << ci))) return kInvalid;
   return n.child_base + (uint32_t)__popc(n.child_mask & ((1u << ci) - 1u));
 }
 
-__device__ __forceinline__ uint32_t rope_down(const vxe_node* nodes, uint32_t nei, uint32_t ci) {
-  if (nei == kInvalid) return kInvalid;
-  if (nodes[nei].child_base == kInvalid) return nei;
-  return child_of(nodes, nei, ci);
-}
-
-__global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_constant__ BuildArgs B) {
+__global__ void __launch_bounds__(SVO_THREADS, 3) k_build_svo(const __grid_constant__ BuildArgs B) {
   __shared__ uint32_t st[kLowCells];
   __shared__ uint32_t kb[kLowCells];
   __shared__ int32_t mip[kMipWords];
   __shared__ uint32_t ws[SVO_WARPS];
-  __shared__ uint32_t red[SVO_WARPS];
   __shared__ uint32_t K[8];  // K[l]: entries of level l's node list (l = 1..6)
+  __shared__ uint32_t bases[8];
 
   const uint32_t chunk = blockIdx.x, t = threadIdx.x;
   if (chunk >= B.n) return;
   const uint8_t* mat = B.mat + (size_t)chunk * kVoxels;
-  const int32_t* ground = B.ground + (size_t)chunk * kColumns;
   uint32_t* st5 = B.st5 + (size_t)chunk * kCells5;
   uint32_t* kb5 = B.kb5 + (size_t)chunk * kCells5;
   const int32_t chunk_oy = B.coords[3 * chunk + 1] * kSide;
   const int32_t dirt = B.wp.dirt_depth;
 
-  // -- column tops -> colinfo (builder.rs:742-805), solid voxel count --------
-  {
-    uint32_t solid = 0;
-    const uint32_t* mw = reinterpret_cast<const uint32_t*>(mat);
-    for (uint32_t w = t; w < kColumns / 4u; w += SVO_THREADS) {  // 4 columns per word
-      uint32_t top[4] = {255u, 255u, 255u, 255u}, tm[4] = {0u, 0u, 0u, 0u};
-      for (uint32_t y = 0; y < 64u; ++y) {
-        const uint32_t v = mw[y * (kColumns / 4u) + w];
-        if (!v) continue;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const uint32_t m = (v >> (8 * k)) & 0xFFu;
-          if (m) { top[k] = y; tm[k] = m; ++solid; }
-        }
-      }
-      uint32_t* ci = B.colinfo + (size_t)chunk * VXE_COLINFO_WORDS_PER_CHUNK + 2u * w;
-      ci[0] = (top[0] | (tm[0] << 8)) | ((top[1] | (tm[1] << 8)) << 16);
-      ci[1] = (top[2] | (tm[2] << 8)) | ((top[3] | (tm[3] << 8)) << 16);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) solid += __shfl_xor_sync(0xFFFFFFFFu, solid, o);
-    if ((t & 31u) == 0) red[t >> 5] = solid;
-  }
-
   // -- ground min-mip levels 1..6 (mips.rs:4-90) ------------------------------
-  for (uint32_t i = t; i < 1024u; i += SVO_THREADS) {
-    const uint32_t x = i & 31u, z = i >> 5;
-    const int32_t* g = ground + (2u * z) * 64u + 2u * x;
-    mip[i] = min(min(g[0], g[1]), min(g[64], g[65]));
-  }
+  for (uint32_t i = t; i < 1024u; i += SVO_THREADS) mip[i] = B.mip1[(size_t)chunk * 1024u + i];
   __syncthreads();
   for (int lv = 2; lv <= 6; ++lv) {
     const uint32_t side = 64u >> lv, cside = side * 2u;
@@ -232,28 +389,16 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
     __syncthreads();
   }
 
-  // -- level 5 states + child offsets: 16 rounds of 2048 cells, 4 per thread --
+  // -- level-5 child offsets: 16 rounds of 2048 cells, 4 per thread -----------
   uint32_t carry = 0;
   for (uint32_t r = 0; r < 16u; ++r) {
-    const uint32_t c0 = r * 2048u + 4u * t;  // 4 consecutive px of one (py, pz) row
-    const uint32_t px0 = c0 & 31u, pz = (c0 >> 5) & 31u, py = c0 >> 10;
-    uint32_t s4[4], cnt[4], sum = 0;
-    uint64_t rows[2][2];
-#pragma unroll
-    for (int dy = 0; dy < 2; ++dy)
-#pragma unroll
-      for (int dz = 0; dz < 2; ++dz)
-        rows[dy][dz] = *reinterpret_cast<const uint64_t*>(mat + (2u * py + dy) * 4096u + (2u * pz + dz) * 64u + 2u * px0);
+    const uint32_t c0 = r * 2048u + 4u * t;
+    const uint4 s4 = *reinterpret_cast<const uint4*>(st5 + c0);
+    const uint32_t sv[4] = {s4.x, s4.y, s4.z, s4.w};
+    uint32_t cnt[4], sum = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      uint32_t cs[8];
-#pragma unroll
-      for (int ci = 0; ci < 8; ++ci)
-        cs[ci] = voxel_state((uint32_t)(rows[(ci >> 1) & 1][(ci >> 2) & 1] >> (8 * (2 * k + (ci & 1)))) & 0xFFu);
-      const int32_t top_y = chunk_oy + (int32_t)(py * 2u) + 1;
-      const int32_t gmin = mip[mip_off(1) + pz * 32u + px0 + k];
-      s4[k] = cell_state(cs, top_y, gmin, dirt);
-      cnt[k] = (s4[k] & ST_MASK) && !(s4[k] & ST_LEAF) ? (uint32_t)__popc(s4[k] & ST_MASK) : 0u;
+      cnt[k] = (sv[k] & ST_MASK) && !(sv[k] & ST_LEAF) ? (uint32_t)__popc(sv[k] & ST_MASK) : 0u;
       sum += cnt[k];
     }
     uint32_t total;
@@ -264,11 +409,10 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
     kv.y = off; off += cnt[1];
     kv.z = off; off += cnt[2];
     kv.w = off;
-    *reinterpret_cast<uint4*>(st5 + c0) = make_uint4(s4[0], s4[1], s4[2], s4[3]);
     *reinterpret_cast<uint4*>(kb5 + c0) = kv;
   }
   if (t == 0) K[6] = carry;
-  __syncthreads();  // st5 visible to the CTA
+  __syncthreads();
 
   // -- levels 4..0 states ---------------------------------------------------
   for (int l = 4; l >= 0; --l) {
@@ -318,16 +462,17 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
   __syncthreads();
 
   // bases[l] = first node of level l's list
-  uint32_t bases[8];
-  bases[0] = 0u;
-  bases[1] = 1u;
-#pragma unroll
-  for (int l = 2; l <= 7; ++l) bases[l] = bases[l - 1] + K[l - 1];
-  const uint32_t node_count = bases[6] + K[6];
+  if (t == 0) {
+    bases[0] = 0u;
+    bases[1] = 1u;
+    for (int l = 2; l <= 7; ++l) bases[l] = bases[l - 1] + K[l - 1];
+  }
+  __syncthreads();
+  const uint32_t node_count = bases[7];
 
   if (t == 0) {
     uint32_t solid = 0;
-    for (int w = 0; w < SVO_WARPS; ++w) solid += red[w];
+    for (int i = 0; i < 16; ++i) solid += B.solid_part[(size_t)chunk * 16u + i];
     B.counts[2u * chunk] = node_count;
     B.counts[2u * chunk + 1u] = solid;
   }
@@ -356,15 +501,20 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
       const uint32_t s = st[low_off(l) + i];
       if (!(s & ST_MASK) || (s & ST_LEAF)) continue;
       const uint32_t px = i & (side - 1u), pz = (i >> l) & (side - 1u), py = i >> (2 * l);
+      uint32_t cs[8], ckb[8];
+#pragma unroll
+      for (int ci = 0; ci < 8; ++ci) {  // all child loads first
+        const uint32_t c = ((2u * py + ((ci >> 1) & 1)) * cside + 2u * pz + ((ci >> 2) & 1)) * cside + 2u * px + (ci & 1);
+        const bool has = (s >> ci) & 1u;
+        cs[ci] = !has ? 0u : l == 4 ? st5[c] : st[low_off(l + 1) + c];
+        ckb[ci] = !has ? 0u : l == 4 ? kb5[c] : kb[low_off(l + 1) + c];
+      }
       uint32_t o = bases[l + 1] + kb[low_off(l) + i];
-#pragma unroll 1
+#pragma unroll
       for (int ci = 0; ci < 8; ++ci) {
-        if (!(s & (1u << ci))) continue;
+        if (!((s >> ci) & 1u)) continue;
         const uint32_t cx = 2u * px + (ci & 1), cy = 2u * py + ((ci >> 1) & 1), cz = 2u * pz + ((ci >> 2) & 1);
-        const uint32_t c = (cy * cside + cz) * cside + cx;
-        const uint32_t cs = l == 4 ? st5[c] : st[low_off(l + 1) + c];
-        const uint32_t ckb = l == 4 ? kb5[c] : kb[low_off(l + 1) + c];
-        nodes[o++] = node_of(cs, ckb + bases[l + 2], cell_key(cx, cy, cz, (uint32_t)l + 1u));
+        nodes[o++] = node_of(cs[ci], ckb[ci] + bases[l + 2], cell_key(cx, cy, cz, (uint32_t)l + 1u));
       }
     }
   }
@@ -372,15 +522,21 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
     const uint32_t s = st5[i];
     if (!(s & ST_MASK) || (s & ST_LEAF)) continue;
     const uint32_t px = i & 31u, pz = (i >> 5) & 31u, py = i >> 10;
+    uint32_t rows[2][2];  // the 2x2 voxel pairs (x, x+1) of the cell
+#pragma unroll
+    for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+      for (int dz = 0; dz < 2; ++dz)
+        rows[dy][dz] = *reinterpret_cast<const uint16_t*>(mat + (2u * py + dy) * 4096u + (2u * pz + dz) * 64u + 2u * px);
     uint32_t o = bases[6] + kb5[i];
-#pragma unroll 1
+#pragma unroll
     for (int ci = 0; ci < 8; ++ci) {
-      if (!(s & (1u << ci))) continue;
+      if (!((s >> ci) & 1u)) continue;
       const uint32_t cx = 2u * px + (ci & 1), cy = 2u * py + ((ci >> 1) & 1), cz = 2u * pz + ((ci >> 2) & 1);
       vxe_node n;
       n.child_base = kInvalid;
       n.child_mask = 0u;
-      n.material = mat[cy * 4096u + cz * 64u + cx];
+      n.material = (rows[(ci >> 1) & 1][(ci >> 2) & 1] >> (8 * (ci & 1))) & 0xFFu;
       n.key = cell_key(cx, cy, cz, 6u);
       nodes[o++] = n;
     }
@@ -401,23 +557,31 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
       const vxe_node pn = nodes[p];
       if (pn.child_base == kInvalid) continue;
       const vxe_node_ropes pr = ropes[p];
+      // the parent's 6 face neighbours, read once for all 8 children
+      const uint32_t nei[6] = {pr.px, pr.nx, pr.py, pr.ny, pr.pz, pr.nz};
+      vxe_node nn[6];
+#pragma unroll
+      for (int d = 0; d < 6; ++d) {
+        if (nei[d] != kInvalid) nn[d] = nodes[nei[d]];
+        else nn[d].child_base = nn[d].child_mask = 0u;
+      }
       uint32_t kid[8];
 #pragma unroll
       for (uint32_t ci = 0; ci < 8; ++ci)
         kid[ci] = (pn.child_mask & (1u << ci)) ? pn.child_base + (uint32_t)__popc(pn.child_mask & ((1u << ci) - 1u))
                                                 : kInvalid;
-#pragma unroll 1
+#pragma unroll
       for (uint32_t ci = 0; ci < 8; ++ci) {
         if (kid[ci] == kInvalid) continue;
         const uint32_t hx = ci & 1u, hy = (ci >> 1) & 1u, hz = (ci >> 2) & 1u;
         const uint32_t sx = kid[ci ^ 1u], sy = kid[ci ^ 2u], sz = kid[ci ^ 4u];
         vxe_node_ropes r;
-        r.px = (hx == 0 && sx != kInvalid) ? sx : rope_down(nodes, pr.px, 0u | (hy << 1) | (hz << 2));
-        r.nx = (hx == 1 && sx != kInvalid) ? sx : rope_down(nodes, pr.nx, 1u | (hy << 1) | (hz << 2));
-        r.py = (hy == 0 && sy != kInvalid) ? sy : rope_down(nodes, pr.py, hx | (0u << 1) | (hz << 2));
-        r.ny = (hy == 1 && sy != kInvalid) ? sy : rope_down(nodes, pr.ny, hx | (1u << 1) | (hz << 2));
-        r.pz = (hz == 0 && sz != kInvalid) ? sz : rope_down(nodes, pr.pz, hx | (hy << 1) | (0u << 2));
-        r.nz = (hz == 1 && sz != kInvalid) ? sz : rope_down(nodes, pr.nz, hx | (hy << 1) | (1u << 2));
+        r.px = (hx == 0 && sx != kInvalid) ? sx : rope_down(nei[0], nn[0], 0u | (hy << 1) | (hz << 2));
+        r.nx = (hx == 1 && sx != kInvalid) ? sx : rope_down(nei[1], nn[1], 1u | (hy << 1) | (hz << 2));
+        r.py = (hy == 0 && sy != kInvalid) ? sy : rope_down(nei[2], nn[2], hx | (0u << 1) | (hz << 2));
+        r.ny = (hy == 1 && sy != kInvalid) ? sy : rope_down(nei[3], nn[3], hx | (1u << 1) | (hz << 2));
+        r.pz = (hz == 0 && sz != kInvalid) ? sz : rope_down(nei[4], nn[4], hx | (hy << 1) | (0u << 2));
+        r.nz = (hz == 1 && sz != kInvalid) ? sz : rope_down(nei[5], nn[5], hx | (hy << 1) | (1u << 2));
         r._pad0 = r._pad1 = 0u;
         ropes[kid[ci]] = r;
       }

@@ -134,10 +134,10 @@ struct vxe_ctx {
   DevBuf nodes, ropes, metas, macro, colinfo, grid, clip_tex, errword;
   DevBuf slot_lights;  // per slot: holds a LIGHT leaf (k_slot_lights)
   DevBuf slot_top;     // per slot: top of its non-air leaves, voxels (k_slot_lights)
-  // chunk builder: per-chunk scratch (materials, ground, level-5 cell states
-  // and child offsets) and events around its three kernels
+  // chunk builder: per-chunk scratch (materials, ground minima, level-5 cell
+  // states and child offsets, solid counts) and events around its two kernels
   DevBuf build_scratch;
-  cudaEvent_t build_ev[4] = {};
+  cudaEvent_t build_ev[3] = {};
   bool build_timed = false;
   GrassTable gt;
   FrameState fr;  // the context's own frame
@@ -1386,6 +1386,31 @@ __global__ void __launch_bounds__(256) k_solid_voxels(const __grid_constant__ vx
 
 }  // namespace
 
+namespace {
+// The cave test of the seeded world, s / 1.5 > threshold with s = n1 + 0.5 n2
+// in [0, 1.5), is monotone in s: returns the least binary64 s >= 0 that
+// passes (bisection over the ordered bit patterns of [0, 2]), +inf when none.
+double cave_s_min(double thr) {
+  auto pass = [thr](double v) { return v / 1.5 > thr; };
+  if (pass(0.0)) return 0.0;
+  if (!pass(2.0)) return INFINITY;
+  uint64_t lo, hi;
+  const double zero = 0.0, two = 2.0;
+  std::memcpy(&lo, &zero, 8);
+  std::memcpy(&hi, &two, 8);
+  while (hi - lo > 1) {
+    const uint64_t mid = lo + (hi - lo) / 2;
+    double v;
+    std::memcpy(&v, &mid, 8);
+    if (pass(v)) hi = mid;
+    else lo = mid;
+  }
+  double r;
+  std::memcpy(&r, &hi, 8);
+  return r;
+}
+}  // namespace
+
 extern "C" {
 
 vxe_status vxe_solid_voxels_device(vxe_ctx* c, const int32_t* d_vox, uint32_t n, const vxe_world_params* world,
@@ -1418,7 +1443,9 @@ vxe_status vxe_build_chunks_device(vxe_ctx* c, const vxe_world_params* world, co
   if (node_cap > VXE_BUILD_NODE_CAP_MAX)
     return fail(c, VXE_ERR_INVALID_ARG, "node_cap %u > %u", node_cap, VXE_BUILD_NODE_CAP_MAX);
   cudaSetDevice(c->device);
-  constexpr size_t kPerChunk = (size_t)vb::kVoxels + (size_t)vb::kColumns * 4 + (size_t)vb::kCells5 * 8;
+  // per chunk: materials, level-1 ground minima, level-5 states and child
+  // offsets, solid counts of the 16 column blocks
+  constexpr size_t kPerChunk = (size_t)vb::kVoxels + 1024 * 4 + (size_t)vb::kCells5 * 8 + 16 * 4;
   const size_t need = kPerChunk * n;
   if (c->build_scratch.bytes < need) {
     vxe_status st = alloc(c, c->build_scratch, need);
@@ -1429,13 +1456,19 @@ vxe_status vxe_build_chunks_device(vxe_ctx* c, const vxe_world_params* world, co
   vb::BuildArgs B;
   std::memset(&B, 0, sizeof B);
   B.wp = *world;
+  B.cave_smin = cave_s_min((double)world->cave_threshold);
   B.coords = d_coords;
   B.n = n;
   char* base = (char*)c->build_scratch.p;
   B.mat = (uint8_t*)base;
-  B.ground = (int32_t*)(base + (size_t)vb::kVoxels * n);
-  B.st5 = (uint32_t*)(base + ((size_t)vb::kVoxels + (size_t)vb::kColumns * 4) * n);
-  B.kb5 = B.st5 + (size_t)vb::kCells5 * n;
+  base += (size_t)vb::kVoxels * n;
+  B.st5 = (uint32_t*)base;
+  base += (size_t)vb::kCells5 * 4 * n;
+  B.kb5 = (uint32_t*)base;
+  base += (size_t)vb::kCells5 * 4 * n;
+  B.mip1 = (int32_t*)base;
+  base += (size_t)1024 * 4 * n;
+  B.solid_part = (uint32_t*)base;
   B.node_cap = node_cap;
   B.nodes = d_nodes;
   B.ropes = d_ropes;
@@ -1444,15 +1477,12 @@ vxe_status vxe_build_chunks_device(vxe_ctx* c, const vxe_world_params* world, co
   B.counts = d_counts;
   cudaStream_t st = c->upload;
   CK(cudaEventRecord(c->build_ev[0], st));
-  vb::k_build_ground<<<n * 16u, 256, 0, st>>>(B);
+  vb::k_build_columns<<<n * 16u, 256, 0, st>>>(B);
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->build_ev[1], st));
-  vb::k_build_fill<<<n * 1024u, 256, 0, st>>>(B);
-  CK(cudaGetLastError());
-  CK(cudaEventRecord(c->build_ev[2], st));
   vb::k_build_svo<<<n, vb::SVO_THREADS, 0, st>>>(B);
   CK(cudaGetLastError());
-  CK(cudaEventRecord(c->build_ev[3], st));
+  CK(cudaEventRecord(c->build_ev[2], st));
   c->build_timed = true;
   return VXE_OK;
 }
@@ -1462,12 +1492,11 @@ vxe_status vxe_get_build_timings(vxe_ctx* c, vxe_build_timings* t) {
   std::memset(t, 0, sizeof *t);
   if (!c->build_timed) return VXE_OK;
   cudaSetDevice(c->device);
-  CK(cudaEventSynchronize(c->build_ev[3]));
-  float ms[3];
-  for (int i = 0; i < 3; ++i) CK(cudaEventElapsedTime(&ms[i], c->build_ev[i], c->build_ev[i + 1]));
-  t->ground = ms[0];
-  t->fill = ms[1];
-  t->svo = ms[2];
+  CK(cudaEventSynchronize(c->build_ev[2]));
+  float ms[2];
+  for (int i = 0; i < 2; ++i) CK(cudaEventElapsedTime(&ms[i], c->build_ev[i], c->build_ev[i + 1]));
+  t->columns = ms[0];
+  t->svo = ms[1];
   return VXE_OK;
 }
 

@@ -119,7 +119,7 @@ class ClipPatchGeom(C.Structure):
 
 
 class BuildTimings(C.Structure):
-    _fields_ = [(n, C.c_double) for n in ("ground", "fill", "svo")]
+    _fields_ = [(n, C.c_double) for n in ("columns", "svo")]
 
 
 BUILD_NODE_CAP_MAX = 299593

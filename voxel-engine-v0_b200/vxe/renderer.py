@@ -175,7 +175,7 @@ class Renderer:
         """Device milliseconds of the last build_chunks call, per kernel."""
         t = A.BuildTimings()
         self._check(self._lib.vxe_get_build_timings(self._ctx, C.byref(t)), "vxe_get_build_timings")
-        return {"ground": t.ground, "fill": t.fill, "svo": t.svo}
+        return {"columns": t.columns, "svo": t.svo}
 
     def read_clipmap(self) -> np.ndarray:
         """The clipmap texture (levels, res, res) after the writes queued so far."""

@@ -247,10 +247,12 @@ class World:
             for k, data in zip(todo, ex.map(self.builder, todo)):
                 self.cache[k] = data
 
-    def prebuild_device(self, renderer, keys, batch: int = 64) -> None:
+    def prebuild_device(self, renderer, keys, batch: int = 256) -> None:
         """Builds missing chunks on the device (Renderer.build_chunks) in batches
         and keeps the host copies the upload path reads; the results equal
-        prebuild()'s byte for byte."""
+        prebuild()'s byte for byte.  Per batch: a count-only build sizes the
+        node buffers, the full build follows, the valid node and rope rows are
+        compacted on the device and come back in one copy each."""
         import torch
 
         todo = [k for k in keys if k not in self.cache]
@@ -258,15 +260,22 @@ class World:
         for i in range(0, len(todo), batch):
             part = todo[i:i + batch]
             coords = torch.tensor(part, dtype=torch.int32, device=f"cuda:{renderer.device}")
-            out = renderer.build_chunks(wp, coords)
+            cap = int(renderer.build_chunks(wp, coords, node_cap=0)["counts"][:, 0].max())
+            out = renderer.build_chunks(wp, coords, node_cap=cap)
+            cnt = out["counts"][:, 0]
+            keep = torch.arange(cap, device=coords.device)[None, :] < cnt[:, None]
+            nodes = out["nodes"][keep].cpu().numpy().view(np.uint32)
+            ropes = out["ropes"][keep].cpu().numpy().view(np.uint32)
             counts = out["counts"].cpu().numpy().view(np.uint32)
             macro = out["macro"].cpu().numpy().view(np.uint32)
             colinfo = out["colinfo"].cpu().numpy().view(np.uint32)
+            first = 0
             for j, key in enumerate(part):
                 n = int(counts[j, 0])
-                nodes = out["nodes"][j, :n].cpu().numpy().view(np.uint32).reshape(-1).view(A.NODE_DTYPE)
-                ropes = out["ropes"][j, :n].cpu().numpy().view(np.uint32).reshape(-1).view(A.ROPES_DTYPE)
-                self.cache[key] = ChunkData(key, nodes, ropes, macro[j].copy(), colinfo[j].copy(), int(counts[j, 1]))
+                self.cache[key] = ChunkData(key, nodes[first:first + n].reshape(-1).view(A.NODE_DTYPE),
+                                            ropes[first:first + n].reshape(-1).view(A.ROPES_DTYPE), macro[j],
+                                            colinfo[j], int(counts[j, 1]))
+                first += n
 
     def populate(self) -> list[Upload]:
         self.prebuild(list(self.keys_in_grid()))
