@@ -359,7 +359,7 @@ __device__ __forceinline__ uint32_t rope_down(uint32_t nei, const vxe_node& n, u
   return n.child_base + (uint32_t)__popc(n.child_mask & ((1u << ci) - 1u));
 }
 
-__global__ void __launch_bounds__(SVO_THREADS, 3) k_build_svo(const __grid_constant__ BuildArgs B) {
+__global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_constant__ BuildArgs B) {
   __shared__ uint32_t st[kLowCells];
   __shared__ uint32_t kb[kLowCells];
   __shared__ int32_t mip[kMipWords];
@@ -389,35 +389,32 @@ __global__ void __launch_bounds__(SVO_THREADS, 3) k_build_svo(const __grid_const
     __syncthreads();
   }
 
-  // -- level-5 child offsets: 16 rounds of 2048 cells, 4 per thread -----------
-  uint32_t carry = 0;
-  for (uint32_t r = 0; r < 16u; ++r) {
-    const uint32_t c0 = r * 2048u + 4u * t;
-    const uint4 s4 = *reinterpret_cast<const uint4*>(st5 + c0);
-    const uint32_t sv[4] = {s4.x, s4.y, s4.z, s4.w};
-    uint32_t cnt[4], sum = 0;
+  // -- levels 4..0 states (level 5 comes from the column kernel) -------------
+  for (uint32_t j = 0; j < 8u; j += 2u) {  // level 4: two cells per step, 8 st5 loads each
+    uint2 q[2][4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      cnt[k] = (sv[k] & ST_MASK) && !(sv[k] & ST_LEAF) ? (uint32_t)__popc(sv[k] & ST_MASK) : 0u;
-      sum += cnt[k];
+    for (uint32_t u = 0; u < 2u; ++u) {
+      const uint32_t i = t + SVO_THREADS * (j + u), px = i & 15u, pz = (i >> 4) & 15u, py = i >> 8;
+#pragma unroll
+      for (uint32_t d = 0; d < 4u; ++d)  // d = dy * 2 + dz
+        q[u][d] = *reinterpret_cast<const uint2*>(st5 + ((2u * py + (d >> 1)) * 32u + 2u * pz + (d & 1u)) * 32u + 2u * px);
     }
-    uint32_t total;
-    uint32_t off = carry + block_excl_scan(sum, ws, &total);
-    carry += total;
-    uint4 kv;
-    kv.x = off; off += cnt[0];
-    kv.y = off; off += cnt[1];
-    kv.z = off; off += cnt[2];
-    kv.w = off;
-    *reinterpret_cast<uint4*>(kb5 + c0) = kv;
+#pragma unroll
+    for (uint32_t u = 0; u < 2u; ++u) {
+      const uint32_t i = t + SVO_THREADS * (j + u), px = i & 15u, pz = (i >> 4) & 15u, py = i >> 8;
+      uint32_t cs[8];
+#pragma unroll
+      for (int ci = 0; ci < 8; ++ci) {
+        const uint2 v = q[u][((ci >> 1) & 1) * 2 + ((ci >> 2) & 1)];
+        cs[ci] = (ci & 1) ? v.y : v.x;
+      }
+      st[low_off(4) + i] = cell_state(cs, chunk_oy + (int32_t)(py * 4u + 3u), mip[mip_off(2) + pz * 16u + px], dirt);
+    }
   }
-  if (t == 0) K[6] = carry;
   __syncthreads();
-
-  // -- levels 4..0 states ---------------------------------------------------
-  for (int l = 4; l >= 0; --l) {
+  for (int l = 3; l >= 0; --l) {
     const uint32_t side = 1u << l, cells = side * side * side, cside = side * 2u;
-    const uint32_t* cst = l == 4 ? st5 : st + low_off(l + 1);
+    const uint32_t* cst = st + low_off(l + 1);
     const uint32_t psize = 64u >> l;
     for (uint32_t i = t; i < cells; i += SVO_THREADS) {
       const uint32_t px = i & (side - 1u), pz = (i >> l) & (side - 1u), py = i >> (2 * l);
@@ -460,14 +457,79 @@ __global__ void __launch_bounds__(SVO_THREADS, 3) k_build_svo(const __grid_const
     }
   }
   __syncthreads();
-
-  // bases[l] = first node of level l's list
+  // bases[l] = first node of level l's list (l = 1..6)
   if (t == 0) {
     bases[0] = 0u;
     bases[1] = 1u;
-    for (int l = 2; l <= 7; ++l) bases[l] = bases[l - 1] + K[l - 1];
+    for (int l = 2; l <= 6; ++l) bases[l] = bases[l - 1] + K[l - 1];
   }
   __syncthreads();
+
+  // -- level-5 child offsets and the voxel list: 16 rounds of 2048 cells, 4
+  // consecutive cells (one row of 8 voxels in x) per thread; each round's
+  // loads are issued before the previous round's scan.  Voxel records go out
+  // as their offsets become known, each one only below node_cap.
+  const uint32_t cap = B.node_cap;
+  vxe_node* nodes = B.nodes + (size_t)chunk * cap;
+  vxe_node_ropes* ropes = B.ropes + (size_t)chunk * cap;
+  uint32_t carry = 0;
+  uint4 s4;
+  uint64_t rows[4];  // d = dy * 2 + dz: the 8 voxels (x = 8 * (t & 7) ...) of each row
+  auto load_round = [&](uint32_t r, uint4& sv, uint64_t (&rw)[4]) {
+    const uint32_t c0 = r * 2048u + 4u * t, px0 = c0 & 31u, pz = (c0 >> 5) & 31u, py = c0 >> 10;
+    sv = *reinterpret_cast<const uint4*>(st5 + c0);
+#pragma unroll
+    for (uint32_t d = 0; d < 4u; ++d)
+      rw[d] = *reinterpret_cast<const uint64_t*>(mat + (2u * py + (d >> 1)) * 4096u + (2u * pz + (d & 1u)) * 64u + 2u * px0);
+  };
+  load_round(0, s4, rows);
+#pragma unroll 1
+  for (uint32_t r = 0; r < 16u; ++r) {
+    const uint32_t c0 = r * 2048u + 4u * t, px0 = c0 & 31u, pz = (c0 >> 5) & 31u, py = c0 >> 10;
+    const uint32_t sv[4] = {s4.x, s4.y, s4.z, s4.w};
+    const uint64_t rw[4] = {rows[0], rows[1], rows[2], rows[3]};
+    if (r + 1u < 16u) load_round(r + 1u, s4, rows);
+    uint32_t cnt[4], sum = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      cnt[k] = (sv[k] & ST_MASK) && !(sv[k] & ST_LEAF) ? (uint32_t)__popc(sv[k] & ST_MASK) : 0u;
+      sum += cnt[k];
+    }
+    uint32_t total;
+    const uint32_t off0 = carry + block_excl_scan(sum, ws, &total);
+    carry += total;
+    uint32_t off = off0;
+    uint4 kv;
+    kv.x = off; off += cnt[0];
+    kv.y = off; off += cnt[1];
+    kv.z = off; off += cnt[2];
+    kv.w = off;
+    *reinterpret_cast<uint4*>(kb5 + c0) = kv;
+    uint32_t o = bases[6] + off0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (!cnt[k]) continue;
+#pragma unroll
+      for (int ci = 0; ci < 8; ++ci) {
+        if (!((sv[k] >> ci) & 1u)) continue;
+        const uint32_t cx = 2u * (px0 + k) + (ci & 1), cy = 2u * py + ((ci >> 1) & 1), cz = 2u * pz + ((ci >> 2) & 1);
+        if (o < cap) {
+          vxe_node n;
+          n.child_base = kInvalid;
+          n.child_mask = 0u;
+          n.material = (uint32_t)(rw[((ci >> 1) & 1) * 2 + ((ci >> 2) & 1)] >> (8 * (2 * k + (ci & 1)))) & 0xFFu;
+          n.key = cell_key(cx, cy, cz, 6u);
+          nodes[o] = n;
+        }
+        ++o;
+      }
+    }
+  }
+  if (t == 0) {
+    K[6] = carry;
+    bases[7] = bases[6] + carry;
+  }
+  __syncthreads();  // kb5 and the voxel records visible to the CTA
   const uint32_t node_count = bases[7];
 
   if (t == 0) {
@@ -485,10 +547,7 @@ __global__ void __launch_bounds__(SVO_THREADS, 3) k_build_svo(const __grid_const
     }
     B.macro[(size_t)chunk * VXE_MACRO_WORDS_PER_CHUNK + t] = word;
   }
-  if (node_count > B.node_cap) return;  // the caller rebuilds with a larger cap
-
-  vxe_node* nodes = B.nodes + (size_t)chunk * B.node_cap;
-  vxe_node_ropes* ropes = B.ropes + (size_t)chunk * B.node_cap;
+  if (node_count > cap) return;  // the caller rebuilds with a larger cap
 
   // -- emission: the root, then each internal cell's children ---------------
   if (t == 0) {
@@ -516,29 +575,6 @@ __global__ void __launch_bounds__(SVO_THREADS, 3) k_build_svo(const __grid_const
         const uint32_t cx = 2u * px + (ci & 1), cy = 2u * py + ((ci >> 1) & 1), cz = 2u * pz + ((ci >> 2) & 1);
         nodes[o++] = node_of(cs[ci], ckb[ci] + bases[l + 2], cell_key(cx, cy, cz, (uint32_t)l + 1u));
       }
-    }
-  }
-  for (uint32_t i = t; i < kCells5; i += SVO_THREADS) {  // level-5 parents, voxel children
-    const uint32_t s = st5[i];
-    if (!(s & ST_MASK) || (s & ST_LEAF)) continue;
-    const uint32_t px = i & 31u, pz = (i >> 5) & 31u, py = i >> 10;
-    uint32_t rows[2][2];  // the 2x2 voxel pairs (x, x+1) of the cell
-#pragma unroll
-    for (int dy = 0; dy < 2; ++dy)
-#pragma unroll
-      for (int dz = 0; dz < 2; ++dz)
-        rows[dy][dz] = *reinterpret_cast<const uint16_t*>(mat + (2u * py + dy) * 4096u + (2u * pz + dz) * 64u + 2u * px);
-    uint32_t o = bases[6] + kb5[i];
-#pragma unroll
-    for (int ci = 0; ci < 8; ++ci) {
-      if (!((s >> ci) & 1u)) continue;
-      const uint32_t cx = 2u * px + (ci & 1), cy = 2u * py + ((ci >> 1) & 1), cz = 2u * pz + ((ci >> 2) & 1);
-      vxe_node n;
-      n.child_base = kInvalid;
-      n.child_mask = 0u;
-      n.material = (rows[(ci >> 1) & 1][(ci >> 2) & 1] >> (8 * (ci & 1))) & 0xFFu;
-      n.key = cell_key(cx, cy, cz, 6u);
-      nodes[o++] = n;
     }
   }
   __syncthreads();  // node records visible to the CTA
