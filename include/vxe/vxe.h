@@ -479,7 +479,30 @@ vxe_status vxe_solid_voxels_device(vxe_ctx* ctx, const int32_t* d_vox, uint32_t 
 vxe_status vxe_build_chunks_device(vxe_ctx* ctx, const vxe_world_params* world, const int32_t* d_coords, uint32_t n,
                                    uint32_t node_cap, vxe_node* d_nodes, vxe_node_ropes* d_ropes, uint32_t* d_macro,
                                    uint32_t* d_colinfo, uint32_t* d_counts);
-/* Device time (ms) of the last vxe_build_chunks_device call's kernels. */
+/* Resident chunk builds: the same builder writing straight into the
+ * context's world -- the device counterpart of building on the CPU and then
+ * uploading (streaming/build_pool.rs -> streaming/upload.rs, ChunkUpload,
+ * streaming/types.rs:87-103).  For each place: nodes and ropes at
+ * [node_base, node_base + node_count), macro words at slot * 16, colinfo
+ * words at slot * 2048 and the slot's meta record (origin, node_base, the
+ * built node count, macro / colinfo bases, macro_empty).  node_count reserves
+ * the arena range: take it from a counting build (vxe_build_chunks_device
+ * with node_cap 0).  A chunk that needs more nodes than reserved gets no
+ * nodes, an empty meta (node_count 0, macro_empty 1) and error word bit
+ * VXE_ERR_WORD_BUILD.  Ordered like vxe_upload_chunks (after the frames and
+ * batches in flight unless VXE_FLAG_UPLOADS_UNORDERED), with the same grass
+ * table and light flag refresh of the written slots; the grid is written
+ * with vxe_write_grid as for uploads. */
+typedef struct vxe_build_place {
+  int32_t cx, cy, cz;
+  uint32_t slot;
+  uint32_t node_base;
+  uint32_t node_count;
+} vxe_build_place;
+#define VXE_ERR_WORD_BUILD (1u << 7)
+vxe_status vxe_build_chunks_resident(vxe_ctx* ctx, const vxe_world_params* world, const vxe_build_place* places,
+                                     uint32_t n);
+/* Device time (ms) of the last vxe_build_chunks_device / _resident call's kernels. */
 typedef struct vxe_build_timings {
   double columns; /* ground, materials, colinfo, level-5 cell states */
   double svo;     /* octree levels 4..0, offsets, nodes, ropes, macro bits */

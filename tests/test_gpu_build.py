@@ -111,3 +111,53 @@ def test_node_cap_overflow_still_reports_counts():
         assert np.array_equal(z["counts"].cpu().numpy(), out["counts"].cpu().numpy())
     finally:
         r.close()
+
+
+def test_resident_build_renders_like_host_upload():
+    """World.populate_device (counting build, then the resident build into the
+    context's arenas) against World.populate + upload of the host-built chunks:
+    the same slots and arena ranges, and the same frame bit for bit."""
+    from vxe.scenes import FrameDriver
+
+    sc = scenes.config2(present=(640, 360))
+    drv = FrameDriver(sc)
+    ups = drv.initial_uploads()
+    _, _, clip, cam = drv.step()
+    w = drv.world
+    kw = dict(node_capacity=w.node_capacity, chunk_capacity=w.chunk_capacity, grid_capacity=w.grid_capacity,
+              clip_levels=sc.clip_levels, clip_res=sc.clip_res)
+    ra = Renderer(sc.present[0], sc.present[1], sc.render_scale, **kw)
+    rb = Renderer(sc.present[0], sc.present[1], sc.render_scale, **kw)
+    try:
+        ra.upload_world(w, ups)
+        wb = World(sc.spec, sc.grid_origin, sc.grid_dims, sc.node_capacity)
+        wb.populate_device(rb, batch=300)  # several resident builds
+        assert wb.key_to_slot == w.key_to_slot and wb.alloc == w.alloc
+        assert np.array_equal(wb.grid, w.grid)
+        images = []
+        for r in (ra, rb):
+            r.write_clipmap_updates(*clip)
+            r.write_camera(cam)
+            r.encode_compute()
+            images.append([r.read_image(i).tobytes() for i in (A.IMG_OUTPUT, A.IMG_COLOR, A.IMG_DEPTH)])
+            assert r.read_error_word() == 0
+        assert images[0] == images[1]
+    finally:
+        ra.close()
+        rb.close()
+
+
+def test_resident_build_reports_a_short_reservation():
+    r = _renderer()
+    try:
+        wp = CARVE.params()
+        key = (0, 0, 0)
+        n = len(build_chunk(CARVE, *key).nodes)
+        with pytest.raises(A.VxeError):  # two places on one slot
+            r.build_resident(wp, [(key, 0, 0, n), ((1, 0, 0), 0, n, n)])
+        r.build_resident(wp, [(key, 1, 0, n - 1)])
+        assert r.read_error_word() & A.ERR_WORD_BUILD
+        r.build_resident(wp, [(key, 1, 0, n)])
+        assert r.read_error_word() == 0
+    finally:
+        r.close()

@@ -78,8 +78,26 @@ struct BuildArgs {
   vxe_node_ropes* ropes;  // n * node_cap
   uint32_t* macro;        // n * 16
   uint32_t* colinfo;      // n * 2048
-  uint32_t* counts;       // n * 2: node_count, solid_voxels
+  uint32_t* counts;       // n * 2: node_count, solid_voxels (may be null)
+  // Resident builds: chunk i goes to its place -- nodes and ropes at
+  // node_base (at most node_count of them), macro and colinfo words and the
+  // meta record at its slot -- instead of the i-indexed layout above.
+  const vxe_build_place* place;
+  vxe_chunk_meta* metas;
+  uint32_t* error_word;
 };
+
+// Error word bit of a resident build whose chunk needs more nodes than its
+// place reserves (its meta then marks it empty).
+constexpr uint32_t ERR_BUILD = 1u << 7;
+
+__device__ __forceinline__ int32_t chunk_coord(const BuildArgs& B, uint32_t chunk, int axis) {
+  if (B.place) return axis == 0 ? B.place[chunk].cx : axis == 1 ? B.place[chunk].cy : B.place[chunk].cz;
+  return B.coords[3 * chunk + axis];
+}
+__device__ __forceinline__ uint32_t chunk_slot(const BuildArgs& B, uint32_t chunk) {
+  return B.place ? B.place[chunk].slot : chunk;
+}
 
 // Exclusive scan of one value per thread over the CTA; *total gets the sum.
 // Ends with a barrier, so `ws` may be reused at once.
@@ -277,8 +295,8 @@ __global__ void __launch_bounds__(256) k_build_columns(const __grid_constant__ B
   const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
   const uint32_t x = ((tile & 3u) << 4) | (lane & 15u), z = ((tile >> 2) << 4) | (w << 1) | (lane >> 4);
   const uint32_t role = (x & 1u) | ((z & 1u) << 1);
-  const int32_t ox = B.coords[3 * chunk] * kSide, oy = B.coords[3 * chunk + 1] * kSide,
-                oz = B.coords[3 * chunk + 2] * kSide;
+  const int32_t ox = chunk_coord(B, chunk, 0) * kSide, oy = chunk_coord(B, chunk, 1) * kSide,
+                oz = chunk_coord(B, chunk, 2) * kSide;
   const int32_t wx = ox + (int32_t)x, wz = oz + (int32_t)z;
   const int32_t g = terrain::ground(B.wp, wx, wz);
   ColumnMaterial col;
@@ -323,7 +341,8 @@ __global__ void __launch_bounds__(256) k_build_columns(const __grid_constant__ B
   }
   // colinfo (builder.rs:742-771): column pairs (x even, x odd) share a word
   const uint32_t e = top | (top_m << 8), eo = __shfl_xor_sync(0xFFFFFFFFu, e, 1);
-  if ((lane & 1u) == 0u) B.colinfo[(size_t)chunk * VXE_COLINFO_WORDS_PER_CHUNK + ((z * 64u + x) >> 1)] = e | (eo << 16);
+  if ((lane & 1u) == 0u)
+    B.colinfo[(size_t)chunk_slot(B, chunk) * VXE_COLINFO_WORDS_PER_CHUNK + ((z * 64u + x) >> 1)] = e | (eo << 16);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) solid += __shfl_xor_sync(0xFFFFFFFFu, solid, o);
   if (lane == 0) red[w] = solid;
@@ -372,7 +391,7 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
   const uint8_t* mat = B.mat + (size_t)chunk * kVoxels;
   uint32_t* st5 = B.st5 + (size_t)chunk * kCells5;
   uint32_t* kb5 = B.kb5 + (size_t)chunk * kCells5;
-  const int32_t chunk_oy = B.coords[3 * chunk + 1] * kSide;
+  const int32_t chunk_oy = chunk_coord(B, chunk, 1) * kSide;
   const int32_t dirt = B.wp.dirt_depth;
 
   // -- ground min-mip levels 1..6 (mips.rs:4-90) ------------------------------
@@ -469,9 +488,10 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
   // consecutive cells (one row of 8 voxels in x) per thread; each round's
   // loads are issued before the previous round's scan.  Voxel records go out
   // as their offsets become known, each one only below node_cap.
-  const uint32_t cap = B.node_cap;
-  vxe_node* nodes = B.nodes + (size_t)chunk * cap;
-  vxe_node_ropes* ropes = B.ropes + (size_t)chunk * cap;
+  const uint32_t cap = B.place ? B.place[chunk].node_count : B.node_cap;
+  const size_t first = B.place ? (size_t)B.place[chunk].node_base : (size_t)chunk * cap;
+  vxe_node* nodes = B.nodes + first;
+  vxe_node_ropes* ropes = B.ropes + first;
   uint32_t carry = 0;
   uint4 s4;
   uint64_t rows[4];  // d = dy * 2 + dz: the 8 voxels (x = 8 * (t & 7) ...) of each row
@@ -535,8 +555,27 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
   if (t == 0) {
     uint32_t solid = 0;
     for (int i = 0; i < 16; ++i) solid += B.solid_part[(size_t)chunk * 16u + i];
-    B.counts[2u * chunk] = node_count;
-    B.counts[2u * chunk + 1u] = solid;
+    if (B.counts) {
+      B.counts[2u * chunk] = node_count;
+      B.counts[2u * chunk + 1u] = solid;
+    }
+    if (B.place) {  // ChunkMetaGpu of the slot (macro_empty <=> no solid voxel)
+      const vxe_build_place& pl = B.place[chunk];
+      const bool fits = node_count <= pl.node_count;
+      vxe_chunk_meta m;
+      m.origin[0] = pl.cx * kSide;
+      m.origin[1] = pl.cy * kSide;
+      m.origin[2] = pl.cz * kSide;
+      m.origin[3] = 0;
+      m.node_base = pl.node_base;
+      m.node_count = fits ? node_count : 0u;
+      m.macro_base = pl.slot * VXE_MACRO_WORDS_PER_CHUNK;
+      m.colinfo_base = pl.slot * VXE_COLINFO_WORDS_PER_CHUNK;
+      m.macro_empty = fits ? (solid == 0u ? 1u : 0u) : 1u;
+      m._pad0 = m._pad1 = m._pad2 = 0u;
+      B.metas[pl.slot] = m;
+      if (!fits) atomicOr(B.error_word, ERR_BUILD);
+    }
   }
   // macro bits: bit mx + 8*(my + 8*mz) <=> level-3 cell present (builder.rs:809-841)
   if (t < VXE_MACRO_WORDS_PER_CHUNK) {
@@ -545,7 +584,7 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
       const uint32_t bit = 32u * t + b, mx = bit & 7u, my = (bit >> 3) & 7u, mz = bit >> 6;
       if (st[low_off(3) + mx + (mz << 3) + (my << 6)] & ST_MASK) word |= 1u << b;
     }
-    B.macro[(size_t)chunk * VXE_MACRO_WORDS_PER_CHUNK + t] = word;
+    B.macro[(size_t)chunk_slot(B, chunk) * VXE_MACRO_WORDS_PER_CHUNK + t] = word;
   }
   if (node_count > cap) return;  // the caller rebuilds with a larger cap
 

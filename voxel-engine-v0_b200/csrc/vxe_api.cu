@@ -137,6 +137,7 @@ struct vxe_ctx {
   // chunk builder: per-chunk scratch (materials, ground minima, level-5 cell
   // states and child offsets, solid counts) and events around its two kernels
   DevBuf build_scratch;
+  DevBuf build_places;  // vxe_build_place records of a resident build
   cudaEvent_t build_ev[3] = {};
   bool build_timed = false;
   GrassTable gt;
@@ -474,20 +475,15 @@ vxe_status grass_table_acquire(vxe_ctx* c, cudaStream_t st, int reader, const vx
 
 // After chunk uploads: rebuild the records of the uploaded slots on the
 // upload stream, ordered after the copies (and after the last full build).
-vxe_status grass_table_refresh(vxe_ctx* c, const vxe_chunk_upload* ups, uint32_t n) {
+// `slots`: sorted, without repeats.
+vxe_status grass_table_refresh(vxe_ctx* c, const std::vector<uint32_t>& slots) {
   GrassTable& T = c->gt;
-  if (!T.valid || n == 0) return VXE_OK;
+  if (!T.valid || slots.empty()) return VXE_OK;
   T.list_valid = false;  // the next wind change rebuilds every column
   if (T.built_recorded) CK(cudaStreamWaitEvent(c->upload, T.built, 0));
-  std::vector<uint32_t> slots;
-  slots.reserve(n);
-  for (uint32_t i = 0; i < n; ++i)
-    if (ups[i].slot < T.chunk_count) slots.push_back(ups[i].slot);
-  std::sort(slots.begin(), slots.end());
-  slots.erase(std::unique(slots.begin(), slots.end()), slots.end());
-  for (size_t i = 0; i < slots.size();) {  // one launch per run of consecutive slots
+  for (size_t i = 0; i < slots.size() && slots[i] < T.chunk_count;) {  // one launch per run of consecutive slots
     size_t j = i + 1;
-    while (j < slots.size() && slots[j] == slots[j - 1] + 1) ++j;
+    while (j < slots.size() && slots[j] == slots[j - 1] + 1 && slots[j] < T.chunk_count) ++j;
     vxe_status st = grass_table_fill(c, c->upload, T.cam, slots[i], (uint32_t)(j - i));
     if (st != VXE_OK) return st;
     i = j;
@@ -849,7 +845,7 @@ void vxe_destroy(vxe_ctx* c) {
   if (c->fr.fgraph) cudaGraphDestroy(c->fr.fgraph);
   for (auto& L : c->lanes)  // lanes read the arenas: drain them before freeing
     if (L.stream) cudaStreamSynchronize(L.stream);
-  for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword, &c->slot_lights, &c->slot_top, &c->build_scratch,
+  for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword, &c->slot_lights, &c->slot_top, &c->build_scratch, &c->build_places,
                   &c->q_in, &c->q_out, &c->gt.rec, &c->gt.taper, &c->gt.state, &c->gt.frames,
                   &c->gt.list, &c->gt.list_n})
     release(*b);
@@ -1015,6 +1011,28 @@ vxe_status upload_after_readers(vxe_ctx* c) {
 
 }  // namespace
 
+namespace {
+// After chunk records of `slots` were written on the upload stream: their
+// grass cell records and light flags are refreshed on the same stream and
+// the next pass on any stream waits for all of it.
+vxe_status chunks_written(vxe_ctx* c, std::vector<uint32_t>& slots) {
+  std::sort(slots.begin(), slots.end());
+  slots.erase(std::unique(slots.begin(), slots.end()), slots.end());
+  vxe_status st = grass_table_refresh(c, slots);
+  if (st != VXE_OK) return st;
+  for (size_t i = 0; i < slots.size();) {  // one launch per run of consecutive slots
+    size_t j = i + 1;
+    while (j < slots.size() && slots[j] == slots[j - 1] + 1) ++j;
+    if ((st = slot_lights_refresh(c, slots[i], (uint32_t)(j - i))) != VXE_OK) return st;
+    i = j;
+  }
+  CK(cudaEventRecord(c->upload_done, c->upload));
+  c->upload_pending = true;
+  c->upload_recorded = true;
+  return VXE_OK;
+}
+}  // namespace
+
 extern "C" {
 
 vxe_status vxe_upload_chunks(vxe_ctx* c, const vxe_chunk_upload* ups, uint32_t n) {
@@ -1055,26 +1073,11 @@ vxe_status vxe_upload_chunks(vxe_ctx* c, const vxe_chunk_upload* ups, uint32_t n
         (rs = ring_copy(c, (char*)c->colinfo.p + cb * 4, u.colinfo_words, VXE_COLINFO_WORDS_PER_CHUNK * 4)) != VXE_OK)
       return rs;
   }
-  vxe_status gst = grass_table_refresh(c, ups, n);
-  if (gst != VXE_OK) return gst;
-  {
-    std::vector<uint32_t> slots;
-    slots.reserve(n);
-    for (uint32_t i = 0; i < n; ++i)
-      if (ups[i].slot < c->cfg.chunk_capacity) slots.push_back(ups[i].slot);
-    std::sort(slots.begin(), slots.end());
-    slots.erase(std::unique(slots.begin(), slots.end()), slots.end());
-    for (size_t i = 0; i < slots.size();) {  // one launch per run of consecutive slots
-      size_t j = i + 1;
-      while (j < slots.size() && slots[j] == slots[j - 1] + 1) ++j;
-      if ((gst = slot_lights_refresh(c, slots[i], (uint32_t)(j - i))) != VXE_OK) return gst;
-      i = j;
-    }
-  }
-  CK(cudaEventRecord(c->upload_done, c->upload));
-  c->upload_pending = true;
-  c->upload_recorded = true;
-  return VXE_OK;
+  std::vector<uint32_t> slots;
+  slots.reserve(n);
+  for (uint32_t i = 0; i < n; ++i)
+    if (ups[i].slot < c->cfg.chunk_capacity) slots.push_back(ups[i].slot);
+  return chunks_written(c, slots);
 }
 
 vxe_status vxe_write_meta(vxe_ctx* c, uint32_t first, const vxe_chunk_meta* metas, uint32_t n) {
@@ -1331,6 +1334,7 @@ vxe_status vxe_read_error_word(vxe_ctx* c, uint32_t* word) {
   if (!c || !word) return VXE_ERR_INVALID_ARG;
   cudaSetDevice(c->device);
   CK(cudaStreamSynchronize(c->compute));
+  CK(cudaStreamSynchronize(c->upload));  // resident builds report here too
   CK(cudaMemcpy(word, c->errword.p, 4, cudaMemcpyDeviceToHost));
   CK(fill_sync(c->errword.p, 0, 4));
   return VXE_OK;
@@ -1411,6 +1415,45 @@ double cave_s_min(double thr) {
 }
 }  // namespace
 
+namespace {
+// Scratch, events and the two builder kernels on the world-write stream.
+vxe_status build_launch(vxe_ctx* c, vxe::build::BuildArgs& B, uint32_t n) {
+  namespace vb = vxe::build;
+  // per chunk: materials, level-1 ground minima, level-5 states and child
+  // offsets, solid counts of the 16 column blocks
+  constexpr size_t kPerChunk = (size_t)vb::kVoxels + 1024 * 4 + (size_t)vb::kCells5 * 8 + 16 * 4;
+  const size_t need = kPerChunk * n;
+  if (c->build_scratch.bytes < need) {
+    vxe_status st = alloc(c, c->build_scratch, need);
+    if (st != VXE_OK) return st;
+  }
+  for (auto& e : c->build_ev)
+    if (!e) CK(cudaEventCreate(&e));
+  B.cave_smin = cave_s_min((double)B.wp.cave_threshold);
+  B.n = n;
+  char* base = (char*)c->build_scratch.p;
+  B.mat = (uint8_t*)base;
+  base += (size_t)vb::kVoxels * n;
+  B.st5 = (uint32_t*)base;
+  base += (size_t)vb::kCells5 * 4 * n;
+  B.kb5 = (uint32_t*)base;
+  base += (size_t)vb::kCells5 * 4 * n;
+  B.mip1 = (int32_t*)base;
+  base += (size_t)1024 * 4 * n;
+  B.solid_part = (uint32_t*)base;
+  cudaStream_t st = c->upload;
+  CK(cudaEventRecord(c->build_ev[0], st));
+  vb::k_build_columns<<<n * 16u, 256, 0, st>>>(B);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->build_ev[1], st));
+  vb::k_build_svo<<<n, vb::SVO_THREADS, 0, st>>>(B);
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->build_ev[2], st));
+  c->build_timed = true;
+  return VXE_OK;
+}
+}  // namespace
+
 extern "C" {
 
 vxe_status vxe_solid_voxels_device(vxe_ctx* c, const int32_t* d_vox, uint32_t n, const vxe_world_params* world,
@@ -1443,48 +1486,67 @@ vxe_status vxe_build_chunks_device(vxe_ctx* c, const vxe_world_params* world, co
   if (node_cap > VXE_BUILD_NODE_CAP_MAX)
     return fail(c, VXE_ERR_INVALID_ARG, "node_cap %u > %u", node_cap, VXE_BUILD_NODE_CAP_MAX);
   cudaSetDevice(c->device);
-  // per chunk: materials, level-1 ground minima, level-5 states and child
-  // offsets, solid counts of the 16 column blocks
-  constexpr size_t kPerChunk = (size_t)vb::kVoxels + 1024 * 4 + (size_t)vb::kCells5 * 8 + 16 * 4;
-  const size_t need = kPerChunk * n;
-  if (c->build_scratch.bytes < need) {
-    vxe_status st = alloc(c, c->build_scratch, need);
-    if (st != VXE_OK) return st;
-  }
-  for (auto& e : c->build_ev)
-    if (!e) CK(cudaEventCreate(&e));
   vb::BuildArgs B;
   std::memset(&B, 0, sizeof B);
   B.wp = *world;
-  B.cave_smin = cave_s_min((double)world->cave_threshold);
   B.coords = d_coords;
-  B.n = n;
-  char* base = (char*)c->build_scratch.p;
-  B.mat = (uint8_t*)base;
-  base += (size_t)vb::kVoxels * n;
-  B.st5 = (uint32_t*)base;
-  base += (size_t)vb::kCells5 * 4 * n;
-  B.kb5 = (uint32_t*)base;
-  base += (size_t)vb::kCells5 * 4 * n;
-  B.mip1 = (int32_t*)base;
-  base += (size_t)1024 * 4 * n;
-  B.solid_part = (uint32_t*)base;
   B.node_cap = node_cap;
   B.nodes = d_nodes;
   B.ropes = d_ropes;
   B.macro = d_macro;
   B.colinfo = d_colinfo;
   B.counts = d_counts;
-  cudaStream_t st = c->upload;
-  CK(cudaEventRecord(c->build_ev[0], st));
-  vb::k_build_columns<<<n * 16u, 256, 0, st>>>(B);
-  CK(cudaGetLastError());
-  CK(cudaEventRecord(c->build_ev[1], st));
-  vb::k_build_svo<<<n, vb::SVO_THREADS, 0, st>>>(B);
-  CK(cudaGetLastError());
-  CK(cudaEventRecord(c->build_ev[2], st));
-  c->build_timed = true;
-  return VXE_OK;
+  return build_launch(c, B, n);
+}
+
+vxe_status vxe_build_chunks_resident(vxe_ctx* c, const vxe_world_params* world, const vxe_build_place* places,
+                                     uint32_t n) {
+  namespace vb = vxe::build;
+  if (!c || !world || (n && !places)) return fail(c, VXE_ERR_INVALID_ARG, "null resident build arguments");
+  if (n == 0) return VXE_OK;
+  if (n > VXE_BUILD_BATCH_MAX) return fail(c, VXE_ERR_CAPACITY, "%u chunks > %u per build call", n, VXE_BUILD_BATCH_MAX);
+  std::vector<uint32_t> slots(n);
+  std::vector<std::pair<uint64_t, uint64_t>> ranges(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    const vxe_build_place& pl = places[i];
+    if (pl.slot >= c->cfg.chunk_capacity || (uint64_t)pl.node_base + pl.node_count > c->cfg.node_capacity ||
+        pl.node_count > VXE_BUILD_NODE_CAP_MAX)
+      return fail(c, VXE_ERR_CAPACITY, "place %u (slot %u, node_base %u, count %u) exceeds capacity", i, pl.slot,
+                  pl.node_base, pl.node_count);
+    slots[i] = pl.slot;
+    ranges[i] = {pl.node_base, (uint64_t)pl.node_base + pl.node_count};
+  }
+  std::vector<uint32_t> sorted = slots;
+  std::sort(sorted.begin(), sorted.end());
+  if (std::adjacent_find(sorted.begin(), sorted.end()) != sorted.end())
+    return fail(c, VXE_ERR_INVALID_ARG, "two places share a slot");
+  std::sort(ranges.begin(), ranges.end());
+  for (uint32_t i = 1; i < n; ++i)
+    if (ranges[i].first < ranges[i - 1].second) return fail(c, VXE_ERR_INVALID_ARG, "two places share arena nodes");
+  cudaSetDevice(c->device);
+  if (!(c->flags & VXE_FLAG_UPLOADS_UNORDERED)) {
+    vxe_status ws = upload_after_readers(c);
+    if (ws != VXE_OK) return ws;
+  }
+  const size_t pbytes = sizeof(vxe_build_place) * n;
+  if (c->build_places.bytes < pbytes) {
+    vxe_status st = alloc(c, c->build_places, sizeof(vxe_build_place) * VXE_BUILD_BATCH_MAX);
+    if (st != VXE_OK) return st;
+  }
+  vxe_status st = ring_copy(c, c->build_places.p, places, pbytes);
+  if (st != VXE_OK) return st;
+  vb::BuildArgs B;
+  std::memset(&B, 0, sizeof B);
+  B.wp = *world;
+  B.place = (const vxe_build_place*)c->build_places.p;
+  B.nodes = (vxe_node*)c->nodes.p;
+  B.ropes = (vxe_node_ropes*)c->ropes.p;
+  B.macro = (uint32_t*)c->macro.p;
+  B.colinfo = (uint32_t*)c->colinfo.p;
+  B.metas = (vxe_chunk_meta*)c->metas.p;
+  B.error_word = (uint32_t*)c->errword.p;
+  if ((st = build_launch(c, B, n)) != VXE_OK) return st;
+  return chunks_written(c, slots);
 }
 
 vxe_status vxe_get_build_timings(vxe_ctx* c, vxe_build_timings* t) {

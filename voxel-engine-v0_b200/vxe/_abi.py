@@ -122,6 +122,12 @@ class BuildTimings(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("columns", "svo")]
 
 
+class BuildPlace(C.Structure):
+    _fields_ = [("cx", C.c_int32), ("cy", C.c_int32), ("cz", C.c_int32), ("slot", C.c_uint32),
+                ("node_base", C.c_uint32), ("node_count", C.c_uint32)]
+
+
+ERR_WORD_BUILD = 1 << 7
 BUILD_NODE_CAP_MAX = 299593
 BUILD_BATCH_MAX = 512
 
@@ -232,6 +238,7 @@ SIGNATURES = {
     "vxe_build_chunks_device": (C.c_int, [C.c_void_p, P(WorldParams), C.c_void_p, C.c_uint32, C.c_uint32,
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "vxe_get_build_timings": (C.c_int, [C.c_void_p, P(BuildTimings)]),
+    "vxe_build_chunks_resident": (C.c_int, [C.c_void_p, P(WorldParams), P(BuildPlace), C.c_uint32]),
 }
 
 

@@ -171,6 +171,16 @@ class Renderer:
         self.synchronize()
         return out
 
+    def build_resident(self, world_params, places) -> None:
+        """Builds chunks on the device straight into this context's world.
+        `places`: (key, slot, node_base, node_count) tuples, node_count from a
+        counting build (build_chunks(..., node_cap=0))."""
+        arr = (A.BuildPlace * max(1, len(places)))()
+        for i, (key, slot, base, n) in enumerate(places):
+            arr[i] = A.BuildPlace(key[0], key[1], key[2], slot, base, n)
+        self._check(self._lib.vxe_build_chunks_resident(self._ctx, C.byref(world_params), arr, len(places)),
+                    "vxe_build_chunks_resident")
+
     def build_timings(self) -> dict:
         """Device milliseconds of the last build_chunks call, per kernel."""
         t = A.BuildTimings()

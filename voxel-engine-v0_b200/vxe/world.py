@@ -277,6 +277,38 @@ class World:
                                             colinfo[j], int(counts[j, 1]))
                 first += n
 
+    def populate_device(self, renderer, batch: int = 512) -> None:
+        """populate() with every chunk built on the device straight into
+        `renderer`'s world: a counting build per batch gives the node counts,
+        slots and arena ranges are taken exactly as add() takes them, the
+        resident build writes nodes, ropes, macro / colinfo words and metas
+        in place, and the grid follows.  No chunk data passes through the host,
+        so this world's host mirrors (nodes, ropes, macro, colinfo, metas) stay
+        empty for these chunks."""
+        import torch
+
+        keys = [k for k in self.keys_in_grid() if k not in self.key_to_slot]
+        wp = self.spec.params()
+        for i in range(0, len(keys), batch):
+            part = keys[i:i + batch]
+            coords = torch.tensor(part, dtype=torch.int32, device=f"cuda:{renderer.device}")
+            counts = renderer.build_chunks(wp, coords, node_cap=0)["counts"].cpu().numpy().view(np.uint32)
+            places = []
+            for key, (n, _solid) in zip(part, counts.tolist()):
+                base = self.arena.alloc(n)
+                if base is None:
+                    raise MemoryError(f"node arena full adding chunk {key} ({n} nodes)")
+                slot = len(self.slot_to_key)
+                if slot >= self.chunk_capacity:
+                    raise MemoryError("chunk slots exhausted")
+                self.slot_to_key.append(key)
+                self.key_to_slot[key] = slot
+                self.alloc[key] = (base, n)
+                places.append((key, slot, base, n))
+            renderer.build_resident(wp, places)
+        self.rebuild_grid()
+        renderer.write_chunk_grid(self.grid)
+
     def populate(self) -> list[Upload]:
         self.prebuild(list(self.keys_in_grid()))
         ups = [self.add(k) for k in self.keys_in_grid() if k not in self.key_to_slot]
