@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched / served workloads")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--profile-steps", type=int, default=0, help="render N steps only (for ncu), no JSON")
+    ap.add_argument("--build-profile", type=int, default=0,
+                    help="build the first N config-2 chunks (a counting build, then the full build) only, for ncu")
     return ap.parse_args()
 
 
@@ -493,6 +495,27 @@ def run_builder(dev, steps: int = 3, warmup: int = 2):
     }
 
 
+def build_profile(n: int) -> None:
+    """The chunk builder on the first n chunks of the config-2 grid: a counting
+    build (node_cap 0), then the full build; prints the kernels' device ms."""
+    import torch
+
+    from vxe import scenes
+    from vxe.renderer import Renderer
+
+    sc = scenes.config2(present=(64, 36))
+    keys = [(x, y, z) for z in range(16) for y in range(4) for x in range(16)][:n]
+    r = Renderer(64, 36, 1.0, node_capacity=1 << 12, chunk_capacity=4, grid_capacity=4, clip_levels=1, clip_res=16)
+    try:
+        c = torch.tensor(keys, dtype=torch.int32, device="cuda:0")
+        wp = sc.spec.params()
+        cap = int(r.build_chunks(wp, c, node_cap=0)["counts"][:, 0].max())
+        r.build_chunks(wp, c, node_cap=cap)
+        print(json.dumps({"chunks": len(keys), "node_cap": cap, "kernel_ms": r.build_timings()}))
+    finally:
+        r.close()
+
+
 def run_configs(dev):
     """Secondary frame lines: config 5 (32x8x32 chunks, 6-level 512^2 clipmap,
     3840x2160 present / 1920x1080 internal) and config 2 at render scale 1.0."""
@@ -650,6 +673,8 @@ def main():
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
     if args.impl == "reference":
         return main_reference(args, rank, world_size)
+    if args.build_profile:
+        return build_profile(args.build_profile)
     if world_size > 1:
         import datetime
 
