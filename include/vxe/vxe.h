@@ -381,6 +381,18 @@ typedef enum vxe_image {
 /* "IN" = the history the next frame reads, "OUT" = the one it writes. */
 vxe_status vxe_image_size(const vxe_ctx* ctx, vxe_image img, size_t* bytes);
 vxe_status vxe_read_image(vxe_ctx* ctx, vxe_image img, void* host, size_t bytes);
+/* Asynchronous read-back (none in the reference, whose output goes to the
+ * swapchain; the pipelined counterpart of vxe_read_image): queues a copy of
+ * `img` -- as the frames queued so far leave
+ * it -- into `host` on a copy stream and returns a ticket.  The next frame's
+ * write of that image waits for the copy: for VXE_IMG_OUTPUT only its final
+ * composite pass does, so the copy overlaps that frame's earlier passes; for
+ * any other image the whole next frame does.  `host` must stay valid until
+ * the copy has landed; pinned memory (cudaHostAlloc) makes the copy
+ * asynchronous.  vxe_read_image_wait blocks until the copy of `ticket` has
+ * landed; vxe_synchronize waits for all of them. */
+vxe_status vxe_read_image_async(vxe_ctx* ctx, vxe_image img, void* host, size_t bytes, uint64_t* ticket);
+vxe_status vxe_read_image_wait(vxe_ctx* ctx, uint64_t ticket);
 vxe_status vxe_write_image(vxe_ctx* ctx, vxe_image img, const void* host, size_t bytes);
 
 /* Device error word (bounds checks / bounded waits); cleared on read. */

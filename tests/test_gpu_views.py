@@ -93,3 +93,63 @@ def test_world_writes_wait_for_frames_in_flight():
         for v in views:
             v.close()
         r.close()
+
+
+def test_async_output_reads_equal_sync_reads():
+    """Pipelined read-back: frame i's output copied on the copy stream while
+    frame i+1 is queued behind it (the composite waits for the copy), two host
+    buffers, each waited one step later -- the same bytes as reading every
+    frame synchronously; an image other than the output delays the whole next
+    frame and reads back the same too."""
+    import torch
+
+    sc = config2(present=(640, 360))
+    sc.shift_every = 3
+    runs = []
+    for pipelined in (False, True):
+        drv = FrameDriver(sc)
+        ups = drv.initial_uploads()
+        w = drv.world
+        r = Renderer(sc.present[0], sc.present[1], sc.render_scale, node_capacity=w.node_capacity,
+                     chunk_capacity=w.chunk_capacity, grid_capacity=w.grid_capacity, clip_levels=sc.clip_levels,
+                     clip_res=sc.clip_res)
+        try:
+            r.upload_world(w, ups)
+            pw, ph = sc.present
+            iw, ih = r.internal
+            bufs = [torch.empty((ph, pw, 4), dtype=torch.float32).pin_memory().numpy() for _ in range(2)]
+            depth = [torch.empty((ih, iw), dtype=torch.float32).pin_memory().numpy() for _ in range(2)]
+            outs, depths, prev = [], [], None
+            for f in range(6):
+                u, g, clip, cam = drv.step()
+                if u:
+                    r.apply_chunk_uploads(u)
+                if g:
+                    r.write_chunk_grid(w.grid)
+                r.write_clipmap_updates(*clip)
+                r.write_camera(cam)
+                if pipelined:
+                    r.encode_compute(sync=False)
+                    t = r.read_image_async(A.IMG_OUTPUT, bufs[f % 2])
+                    td = r.read_image_async(A.IMG_DEPTH, depth[f % 2])
+                    if prev is not None:
+                        r.read_image_wait(prev[0])
+                        r.read_image_wait(prev[1])
+                        outs.append(bufs[(f - 1) % 2].tobytes())
+                        depths.append(depth[(f - 1) % 2].tobytes())
+                    prev = (t, td)
+                else:
+                    r.encode_compute()
+                    outs.append(r.read_image(A.IMG_OUTPUT).tobytes())
+                    depths.append(r.read_image(A.IMG_DEPTH).tobytes())
+            if pipelined:
+                r.read_image_wait(prev[0])
+                r.read_image_wait(prev[1])
+                outs.append(bufs[5 % 2].tobytes())
+                depths.append(depth[5 % 2].tobytes())
+            runs.append((outs, depths))
+        finally:
+            r.close()
+    assert runs[0][0] == runs[1][0]
+    assert runs[0][1] == runs[1][1]
+    assert len(set(runs[0][0])) > 1  # the frames differ

@@ -86,6 +86,9 @@ struct FrameState {
   cudaGraphExec_t fgraph_exec = nullptr;
   std::vector<cudaGraphNode_t> fgraph_nodes;
   uint64_t fgraph_key[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  // set by launch_frame while an asynchronous read of the output image is in
+  // flight: the composite (its writer) waits for it, the earlier passes do not
+  cudaEvent_t composite_wait = nullptr;
 };
 
 // A second stream a frame forks to (far-pixel shading beside the probe
@@ -136,6 +139,14 @@ struct vxe_ctx {
   DevBuf slot_top;     // per slot: top of its non-air leaves, voxels (k_slot_lights)
   // chunk builder: per-chunk scratch (materials, ground minima, level-5 cell
   // states and child offsets, solid counts) and events around its two kernels
+  // asynchronous image reads: a copy stream and one event per ticket slot;
+  // out_pending / any_pending: the last output / other image copy not yet
+  // waited for by a frame
+  cudaStream_t copy = nullptr;
+  cudaEvent_t copy_ev[8] = {};
+  uint64_t copy_seq = 0;
+  bool out_pending = false, any_pending = false;
+  cudaEvent_t out_ev = nullptr, any_ev = nullptr;
   DevBuf build_scratch;
   DevBuf build_places;  // vxe_build_place records of a resident build
   cudaEvent_t build_ev[3] = {};
@@ -641,6 +652,7 @@ vxe_status frame_enqueue(vxe_ctx* c, FrameState& F, const FrameArgs& A, bool tim
   k_godray<<<dim3((F.iw + POST_THREADS_X - 1) / POST_THREADS_X, (F.ih + POST_THREADS_Y - 1) / POST_THREADS_Y),
              dim3(POST_THREADS_X, POST_THREADS_Y), 0, st>>>(A);
   if (timed) CK(cudaEventRecord(F.ev[5], st));
+  if (F.composite_wait) CK(cudaStreamWaitEvent(st, F.composite_wait, 0));
   k_composite<<<dim3((F.pw + POST_THREADS_X - 1) / POST_THREADS_X, (F.ph + POST_THREADS_Y - 1) / POST_THREADS_Y),
                 dim3(POST_THREADS_X, POST_THREADS_Y), 0, st>>>(A);
   if (timed) CK(cudaEventRecord(F.ev[6], st));
@@ -652,13 +664,21 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
   vxe_status st = frame_validate(c, c->fr, c->cam);
   if (st != VXE_OK) return st;
   if (c->upload_recorded) CK(cudaStreamWaitEvent(c->compute, c->upload_done, 0));
+  if (c->any_pending) {  // an image other than the output: before any pass
+    CK(cudaStreamWaitEvent(c->compute, c->any_ev, 0));
+    c->any_pending = false;
+  }
   FrameArgs A;
   frame_fill(c, c->fr, c->cam, A);
   if (timed) CK(cudaEventRecord(c->fr.ev[0], c->compute));
   bool use_grass = false;
   if ((st = grass_table_acquire(c, c->compute, 0, c->cam, &use_grass)) != VXE_OK) return st;
   if (use_grass) grass_table_args(c, A);
-  if ((st = frame_enqueue(c, c->fr, A, timed, c->compute, &c->side)) != VXE_OK) return st;
+  c->fr.composite_wait = c->out_pending ? c->out_ev : nullptr;
+  st = frame_enqueue(c, c->fr, A, timed, c->compute, &c->side);
+  c->fr.composite_wait = nullptr;
+  if (st != VXE_OK) return st;
+  c->out_pending = false;
   if (use_grass && (st = grass_table_release(c, c->compute, 0)) != VXE_OK) return st;
   c->fr.timed = timed;
   c->fr.timed_trace = timed && !(c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL);
@@ -675,6 +695,11 @@ vxe_status launch_frame_graph(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& c
   vxe_status rc = frame_validate(c, F, cam);
   if (rc != VXE_OK) return rc;
   if (c->upload_recorded) CK(cudaStreamWaitEvent(st, c->upload_done, 0));
+  if (&F == &c->fr) {  // asynchronous reads of the context's images land first
+    if (c->out_pending) CK(cudaStreamWaitEvent(st, c->out_ev, 0));
+    if (c->any_pending) CK(cudaStreamWaitEvent(st, c->any_ev, 0));
+    c->out_pending = c->any_pending = false;
+  }
   FrameArgs A;
   frame_fill(c, F, cam, A);
   bool use_grass = false;
@@ -841,6 +866,12 @@ void vxe_destroy(vxe_ctx* c) {
   cudaSetDevice(c->device);
   if (c->compute) cudaStreamSynchronize(c->compute);
   if (c->upload) cudaStreamSynchronize(c->upload);
+  if (c->copy) {
+    cudaStreamSynchronize(c->copy);
+    cudaStreamDestroy(c->copy);
+  }
+  for (auto& e : c->copy_ev)
+    if (e) cudaEventDestroy(e);
   if (c->fr.fgraph_exec) cudaGraphExecDestroy(c->fr.fgraph_exec);
   if (c->fr.fgraph) cudaGraphDestroy(c->fr.fgraph);
   for (auto& L : c->lanes)  // lanes read the arenas: drain them before freeing
@@ -919,6 +950,7 @@ vxe_status vxe_resize(vxe_ctx* c, uint32_t present_w, uint32_t present_h, float 
     return fail(c, VXE_ERR_INVALID_ARG, "bad resize arguments");
   cudaSetDevice(c->device);
   CK(cudaStreamSynchronize(c->compute));
+  if (c->copy) CK(cudaStreamSynchronize(c->copy));
   set_dims(c->fr, present_w, present_h, render_scale);
   return alloc_images(c, c->fr);
 }
@@ -1273,6 +1305,7 @@ vxe_status vxe_synchronize(vxe_ctx* c) {
   cudaSetDevice(c->device);
   CK(cudaStreamSynchronize(c->compute));
   CK(cudaStreamSynchronize(c->upload));
+  if (c->copy) CK(cudaStreamSynchronize(c->copy));
   return VXE_OK;
 }
 
@@ -1315,6 +1348,42 @@ vxe_status vxe_read_image(vxe_ctx* c, vxe_image im, void* host, size_t bytes) {
   cudaSetDevice(c->device);
   CK(cudaStreamSynchronize(c->compute));
   CK(cudaMemcpy(host, c->fr.img[i].p, bytes, cudaMemcpyDeviceToHost));
+  return VXE_OK;
+}
+
+vxe_status vxe_read_image_async(vxe_ctx* c, vxe_image im, void* host, size_t bytes, uint64_t* ticket) {
+  if (!c || !host) return VXE_ERR_INVALID_ARG;
+  const int i = map_image(c->fr, im);
+  if (i < 0 || !c->fr.img[i].p) return fail(c, VXE_ERR_INVALID_ARG, "image %d not available", (int)im);
+  if (bytes != c->fr.img[i].bytes) return fail(c, VXE_ERR_INVALID_ARG, "image %d is %zu bytes, got %zu", (int)im, c->fr.img[i].bytes, bytes);
+  cudaSetDevice(c->device);
+  if (!c->copy) CK(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking));
+  for (auto& e : c->copy_ev)
+    if (!e) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaEvent_t& slot = c->copy_ev[c->copy_seq % 8];
+  CK(cudaEventRecord(slot, c->compute));  // after the frame work queued so far
+  CK(cudaStreamWaitEvent(c->copy, slot, 0));
+  CK(cudaMemcpyAsync(host, c->fr.img[i].p, bytes, cudaMemcpyDeviceToHost, c->copy));
+  CK(cudaEventRecord(slot, c->copy));
+  if (i == IMG_OUTPUT) {
+    c->out_ev = slot;
+    c->out_pending = true;
+  } else {
+    c->any_ev = slot;
+    c->any_pending = true;
+  }
+  if (ticket) *ticket = c->copy_seq;
+  ++c->copy_seq;
+  return VXE_OK;
+}
+
+vxe_status vxe_read_image_wait(vxe_ctx* c, uint64_t ticket) {
+  if (!c) return VXE_ERR_INVALID_ARG;
+  if (ticket >= c->copy_seq) return fail(c, VXE_ERR_INVALID_ARG, "no image read %llu queued", (unsigned long long)ticket);
+  cudaSetDevice(c->device);
+  // copies run in order on one stream: a slot re-recorded by a later copy
+  // completes after this one
+  CK(cudaEventSynchronize(c->copy_ev[ticket % 8]));
   return VXE_OK;
 }
 

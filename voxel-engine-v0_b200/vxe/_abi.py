@@ -239,6 +239,8 @@ SIGNATURES = {
                                           C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "vxe_get_build_timings": (C.c_int, [C.c_void_p, P(BuildTimings)]),
     "vxe_build_chunks_resident": (C.c_int, [C.c_void_p, P(WorldParams), P(BuildPlace), C.c_uint32]),
+    "vxe_read_image_async": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, P(C.c_uint64)]),
+    "vxe_read_image_wait": (C.c_int, [C.c_void_p, C.c_uint64]),
 }
 
 

@@ -210,6 +210,19 @@ class Renderer:
         A.IMG_OUTPUT_HIST_IN: ("p", 4, np.float32), A.IMG_OUTPUT_HIST_OUT: ("p", 4, np.float32),
     }
 
+    def read_image_async(self, img: int, out: np.ndarray) -> int:
+        """Queues a copy of image `img` into `out` (pinned host memory for an
+        asynchronous copy; keep it alive until the wait) and returns a ticket
+        for read_image_wait.  The next frame's write of the image waits for
+        the copy (for the output only its composite pass)."""
+        t = C.c_uint64()
+        self._check(self._lib.vxe_read_image_async(self._ctx, img, out.ctypes.data, out.nbytes, C.byref(t)),
+                    "vxe_read_image_async")
+        return t.value
+
+    def read_image_wait(self, ticket: int) -> None:
+        self._check(self._lib.vxe_read_image_wait(self._ctx, ticket), "vxe_read_image_wait")
+
     def read_image(self, img: int) -> np.ndarray:
         if img == A.IMG_HITS:
             w, h = self.internal

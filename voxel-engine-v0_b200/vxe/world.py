@@ -178,8 +178,9 @@ class World:
 
     def _write_slot(self, slot: int, key, node_base: int, data: ChunkData) -> np.ndarray:
         n = len(data.nodes)
-        self.nodes[node_base:node_base + n] = data.nodes
-        self.ropes[node_base:node_base + n] = data.ropes
+        # plain word copies (a structured-array assignment copies field by field)
+        self.nodes.view(np.uint32)[4 * node_base:4 * (node_base + n)] = data.nodes.view(np.uint32).reshape(-1)
+        self.ropes.view(np.uint32)[8 * node_base:8 * (node_base + n)] = data.ropes.view(np.uint32).reshape(-1)
         self.macro[slot * 16:(slot + 1) * 16] = data.macro
         self.colinfo[slot * 2048:(slot + 1) * 2048] = data.colinfo
         meta = self._meta_for(slot, key, node_base, data)
