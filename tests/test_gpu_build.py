@@ -161,3 +161,28 @@ def test_resident_build_reports_a_short_reservation():
         assert r.read_error_word() == 0
     finally:
         r.close()
+
+
+def test_device_build_random_worlds():
+    """Random world parameters (cave thresholds, carving, heights, lattice
+    spacing, features) and random chunks, byte for byte against the host
+    builder; the cave thresholds exercise the exact threshold compare."""
+    import torch
+
+    rng = np.random.default_rng(2024)
+    r = _renderer()
+    try:
+        for w in range(6):
+            lo = int(rng.integers(-40, 60))
+            spec = WorldSpec(seed=int(rng.integers(0, 2 ** 32 - 1)), height_min=lo,
+                             height_max=lo + int(rng.integers(0, 120)), dirt_depth=int(rng.integers(0, 8)),
+                             carve_mod=int(rng.choice([0, 0, 7, 50, 331])),
+                             cave_threshold=float(rng.choice([2.0, rng.uniform(0.3, 0.95)])),
+                             height_scale_vox=float(rng.choice([16.0, 48.0, 64.0, 100.0])),
+                             features=int(rng.integers(0, 4)))
+            keys = [(int(rng.integers(-30, 30)), int(rng.integers(-2, 3)), int(rng.integers(-30, 30)))
+                    for _ in range(5)]
+            coords = torch.tensor(keys, dtype=torch.int32, device="cuda:0")
+            _compare(spec, keys, r.build_chunks(spec.params(), coords))
+    finally:
+        r.close()
