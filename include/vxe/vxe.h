@@ -514,6 +514,20 @@ typedef struct vxe_build_place {
 #define VXE_ERR_WORD_BUILD (1u << 7)
 vxe_status vxe_build_chunks_resident(vxe_ctx* ctx, const vxe_world_params* world, const vxe_build_place* places,
                                      uint32_t n);
+/* Dense-slot moves on the device (the slot compaction of
+ * streaming/manager/slots.rs:163-766: unloading a chunk moves the last slot
+ * into its hole).  Moves run in order; each copies the slot's meta record
+ * (macro / colinfo bases rewritten for the new slot), its 16 macro words and
+ * 2048 colinfo words; node data stays where the arena holds it.  With
+ * resident builds this keeps a streamed world entirely on the device (only
+ * node counts come back to the host).  Ordered like vxe_upload_chunks, with
+ * the grass / light refresh of the destination slots; the grid follows with
+ * vxe_write_grid. */
+typedef struct vxe_slot_move {
+  uint32_t from, to;
+} vxe_slot_move;
+#define VXE_MOVE_SLOTS_MAX 4096u
+vxe_status vxe_move_slots(vxe_ctx* ctx, const vxe_slot_move* moves, uint32_t n);
 /* Device time (ms) of the last vxe_build_chunks_device / _resident call's kernels. */
 typedef struct vxe_build_timings {
   double columns; /* ground, materials, colinfo, level-5 cell states */

@@ -186,3 +186,47 @@ def test_device_build_random_worlds():
             _compare(spec, keys, r.build_chunks(spec.params(), coords))
     finally:
         r.close()
+
+
+def test_device_streaming_renders_like_host_streaming():
+    """A world kept on the device (resident builds, device slot moves at each
+    grid shift) against the host path (host builds, uploads of the moved and
+    new chunks): the same slots and arena ranges after every shift and the
+    same frames bit for bit, across three shifts (one back to the origin)."""
+    sc = scenes.config2(present=(480, 270))
+    sc.shift_every = 2
+    kw = dict(node_capacity=sc.node_capacity, chunk_capacity=int(np.prod(sc.grid_dims)),
+              grid_capacity=int(np.prod(sc.grid_dims)), clip_levels=sc.clip_levels, clip_res=sc.clip_res)
+    from vxe.scenes import FrameDriver
+
+    rh = Renderer(sc.present[0], sc.present[1], sc.render_scale, **kw)
+    rd = Renderer(sc.present[0], sc.present[1], sc.render_scale, **kw)
+    try:
+        dh, dd = FrameDriver(sc), FrameDriver(sc, device_renderer=rd)
+        rh.upload_world(dh.world, dh.initial_uploads())
+        assert dd.initial_uploads() == []
+        for f in range(6):
+            if f == 5:  # back to the first origin on both sides
+                rh.apply_chunk_uploads(dh.world.shift(-2, 0, 0))
+                rh.write_chunk_grid(dh.world.grid)
+                dd.world.shift_device(rd, -2, 0, 0)
+            uh, gh, clip, cam = dh.step()
+            ud, gd, clip_d, cam_d = dd.step()
+            assert ud == [] and not gd
+            if uh:
+                rh.apply_chunk_uploads(uh)
+            if gh:
+                rh.write_chunk_grid(dh.world.grid)
+            assert dd.world.key_to_slot == dh.world.key_to_slot and dd.world.alloc == dh.world.alloc
+            assert np.array_equal(dd.world.grid, dh.world.grid)
+            imgs = []
+            for r, c, cm in ((rh, clip, cam), (rd, clip_d, cam_d)):
+                r.write_clipmap_updates(*c)
+                r.write_camera(cm)
+                r.encode_compute()
+                imgs.append([r.read_image(i).tobytes() for i in (A.IMG_OUTPUT, A.IMG_DEPTH)])
+            assert imgs[0] == imgs[1], f
+        assert rh.read_error_word() == 0 and rd.read_error_word() == 0
+    finally:
+        rh.close()
+        rd.close()

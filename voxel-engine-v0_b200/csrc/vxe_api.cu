@@ -149,6 +149,7 @@ struct vxe_ctx {
   cudaEvent_t out_ev = nullptr, any_ev = nullptr;
   DevBuf build_scratch;
   DevBuf build_places;  // vxe_build_place records of a resident build
+  DevBuf move_buf;      // vxe_slot_move records
   cudaEvent_t build_ev[3] = {};
   bool build_timed = false;
   GrassTable gt;
@@ -876,7 +877,7 @@ void vxe_destroy(vxe_ctx* c) {
   if (c->fr.fgraph) cudaGraphDestroy(c->fr.fgraph);
   for (auto& L : c->lanes)  // lanes read the arenas: drain them before freeing
     if (L.stream) cudaStreamSynchronize(L.stream);
-  for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword, &c->slot_lights, &c->slot_top, &c->build_scratch, &c->build_places,
+  for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword, &c->slot_lights, &c->slot_top, &c->build_scratch, &c->build_places, &c->move_buf,
                   &c->q_in, &c->q_out, &c->gt.rec, &c->gt.taper, &c->gt.state, &c->gt.frames,
                   &c->gt.list, &c->gt.list_n})
     release(*b);
@@ -1460,6 +1461,31 @@ __global__ void __launch_bounds__(256) k_solid_voxels(const __grid_constant__ vx
 }  // namespace
 
 namespace {
+// Dense-slot moves in order, one CTA: a slot's meta record (its macro and
+// colinfo bases follow the slot), 16 macro words and 2048 colinfo words.
+__global__ void __launch_bounds__(1024) k_move_slots(const uint2* moves, uint32_t n, uint4* metas, uint32_t* macro,
+                                                    uint32_t* colinfo) {
+  const uint32_t t = threadIdx.x;
+  for (uint32_t m = 0; m < n; ++m) {
+    const uint2 mv = moves[m];
+    if (t < VXE_MACRO_WORDS_PER_CHUNK)
+      macro[(size_t)mv.y * VXE_MACRO_WORDS_PER_CHUNK + t] = macro[(size_t)mv.x * VXE_MACRO_WORDS_PER_CHUNK + t];
+    for (uint32_t i = t; i < VXE_COLINFO_WORDS_PER_CHUNK; i += 1024u)
+      colinfo[(size_t)mv.y * VXE_COLINFO_WORDS_PER_CHUNK + i] = colinfo[(size_t)mv.x * VXE_COLINFO_WORDS_PER_CHUNK + i];
+    if (t < 3u) {
+      uint4 w = metas[(size_t)mv.x * 3u + t];
+      if (t == 1u) {
+        w.z = mv.y * VXE_MACRO_WORDS_PER_CHUNK;
+        w.w = mv.y * VXE_COLINFO_WORDS_PER_CHUNK;
+      }
+      metas[(size_t)mv.y * 3u + t] = w;
+    }
+    __syncthreads();  // a later move may read this one's destination
+  }
+}
+}  // namespace
+
+namespace {
 // The cave test of the seeded world, s / 1.5 > threshold with s = n1 + 0.5 n2
 // in [0, 1.5), is monotone in s: returns the least binary64 s >= 0 that
 // passes (bisection over the ordered bit patterns of [0, 2]), +inf when none.
@@ -1616,6 +1642,34 @@ vxe_status vxe_build_chunks_resident(vxe_ctx* c, const vxe_world_params* world, 
   B.error_word = (uint32_t*)c->errword.p;
   if ((st = build_launch(c, B, n)) != VXE_OK) return st;
   return chunks_written(c, slots);
+}
+
+vxe_status vxe_move_slots(vxe_ctx* c, const vxe_slot_move* moves, uint32_t n) {
+  if (!c || (n && !moves)) return fail(c, VXE_ERR_INVALID_ARG, "null slot moves");
+  if (n == 0) return VXE_OK;
+  if (n > VXE_MOVE_SLOTS_MAX) return fail(c, VXE_ERR_CAPACITY, "%u slot moves > %u per call", n, VXE_MOVE_SLOTS_MAX);
+  std::vector<uint32_t> dst(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    if (moves[i].from >= c->cfg.chunk_capacity || moves[i].to >= c->cfg.chunk_capacity)
+      return fail(c, VXE_ERR_CAPACITY, "slot move %u (%u -> %u) outside %u slots", i, moves[i].from, moves[i].to,
+                  c->cfg.chunk_capacity);
+    dst[i] = moves[i].to;
+  }
+  cudaSetDevice(c->device);
+  if (!(c->flags & VXE_FLAG_UPLOADS_UNORDERED)) {
+    vxe_status ws = upload_after_readers(c);
+    if (ws != VXE_OK) return ws;
+  }
+  if (c->move_buf.bytes < sizeof(vxe_slot_move) * n) {
+    vxe_status st = alloc(c, c->move_buf, sizeof(vxe_slot_move) * VXE_MOVE_SLOTS_MAX);
+    if (st != VXE_OK) return st;
+  }
+  vxe_status st = ring_copy(c, c->move_buf.p, moves, sizeof(vxe_slot_move) * n);
+  if (st != VXE_OK) return st;
+  k_move_slots<<<1, 1024, 0, c->upload>>>((const uint2*)c->move_buf.p, n, (uint4*)c->metas.p, (uint32_t*)c->macro.p,
+                                          (uint32_t*)c->colinfo.p);
+  CK(cudaGetLastError());
+  return chunks_written(c, dst);
 }
 
 vxe_status vxe_get_build_timings(vxe_ctx* c, vxe_build_timings* t) {

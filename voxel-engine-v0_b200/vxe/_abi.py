@@ -128,6 +128,10 @@ class BuildPlace(C.Structure):
 
 
 ERR_WORD_BUILD = 1 << 7
+
+
+class SlotMove(C.Structure):
+    _fields_ = [("from_", C.c_uint32), ("to", C.c_uint32)]
 BUILD_NODE_CAP_MAX = 299593
 BUILD_BATCH_MAX = 512
 
@@ -241,6 +245,7 @@ SIGNATURES = {
     "vxe_build_chunks_resident": (C.c_int, [C.c_void_p, P(WorldParams), P(BuildPlace), C.c_uint32]),
     "vxe_read_image_async": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, P(C.c_uint64)]),
     "vxe_read_image_wait": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "vxe_move_slots": (C.c_int, [C.c_void_p, P(SlotMove), C.c_uint32]),
 }
 
 

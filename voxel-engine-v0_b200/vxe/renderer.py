@@ -181,6 +181,13 @@ class Renderer:
         self._check(self._lib.vxe_build_chunks_resident(self._ctx, C.byref(world_params), arr, len(places)),
                     "vxe_build_chunks_resident")
 
+    def move_slots(self, moves) -> None:
+        """Dense-slot moves on the device, in order: (from, to) pairs."""
+        if not moves:
+            return
+        arr = (A.SlotMove * len(moves))(*[A.SlotMove(f, t) for f, t in moves])
+        self._check(self._lib.vxe_move_slots(self._ctx, arr, len(moves)), "vxe_move_slots")
+
     def build_timings(self) -> dict:
         """Device milliseconds of the last build_chunks call, per kernel."""
         t = A.BuildTimings()

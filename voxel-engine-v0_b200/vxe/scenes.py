@@ -145,8 +145,12 @@ SCENES = {"config1": config1, "config2": config2, "config5": config5, "features"
 class FrameDriver:
     """Produces per-frame inputs (uploads, grid, clipmap patches, camera) for a scene."""
 
-    def __init__(self, scene: Scene):
+    def __init__(self, scene: Scene, device_renderer=None):
+        """`device_renderer`: keep the world on that renderer's device -- chunks
+        built resident there, grid shifts by device slot moves (step() then
+        returns no uploads and writes the grid itself)."""
         self.scene = scene
+        self.device = device_renderer
         self.world = World(scene.spec, scene.grid_origin, scene.grid_dims, scene.node_capacity,
                            chunk_capacity=int(np.prod(scene.grid_dims)))
         self.clip = Clipmap(scene.spec, scene.clip_levels, scene.clip_res, 1.0) if scene.clip_levels else None
@@ -154,6 +158,9 @@ class FrameDriver:
         self.frame = 0
 
     def initial_uploads(self):
+        if self.device is not None:
+            self.world.populate_device(self.device)
+            return []
         return self.world.populate()
 
     def step(self):
@@ -162,8 +169,11 @@ class FrameDriver:
         f = self.frame
         uploads, grid_changed = [], False
         if sc.shift_every and f > 0 and f % sc.shift_every == 0:
-            uploads = self.world.shift(1, 0, 0)
-            grid_changed = True
+            if self.device is not None:
+                self.world.shift_device(self.device, 1, 0, 0)
+            else:
+                uploads = self.world.shift(1, 0, 0)
+                grid_changed = True
         pos, yaw, pitch = sc.path(f)
         clip = None
         if self.clip is not None:

@@ -278,17 +278,13 @@ class World:
                                             colinfo[j], int(counts[j, 1]))
                 first += n
 
-    def populate_device(self, renderer, batch: int = 512) -> None:
-        """populate() with every chunk built on the device straight into
-        `renderer`'s world: a counting build per batch gives the node counts,
-        slots and arena ranges are taken exactly as add() takes them, the
-        resident build writes nodes, ropes, macro / colinfo words and metas
-        in place, and the grid follows.  No chunk data passes through the host,
-        so this world's host mirrors (nodes, ropes, macro, colinfo, metas) stay
-        empty for these chunks."""
+    def _add_device(self, renderer, keys, batch: int = 512) -> None:
+        """add() for `keys`, built on the device straight into `renderer`'s
+        world: a counting build per batch gives the node counts, slots and
+        arena ranges are taken exactly as add() takes them, the resident build
+        writes nodes, ropes, macro / colinfo words and metas in place."""
         import torch
 
-        keys = [k for k in self.keys_in_grid() if k not in self.key_to_slot]
         wp = self.spec.params()
         for i in range(0, len(keys), batch):
             part = keys[i:i + batch]
@@ -307,6 +303,38 @@ class World:
                 self.alloc[key] = (base, n)
                 places.append((key, slot, base, n))
             renderer.build_resident(wp, places)
+
+    def populate_device(self, renderer, batch: int = 512) -> None:
+        """populate() with every chunk built on the device straight into
+        `renderer`'s world (_add_device), then the grid.  No chunk data passes
+        through the host, so this world's host mirrors (nodes, ropes, macro,
+        colinfo, metas) stay empty for these chunks."""
+        self._add_device(renderer, [k for k in self.keys_in_grid() if k not in self.key_to_slot], batch)
+        self.rebuild_grid()
+        renderer.write_chunk_grid(self.grid)
+
+    def shift_device(self, renderer, dx: int, dy: int, dz: int) -> None:
+        """shift() for a world kept on the device: chunks that left free their
+        arena range and the last slot moves into each hole (vxe_move_slots, in
+        the order remove() takes them), entering chunks are built resident
+        (_add_device), then the grid -- the same slots, arena ranges and
+        device records as shift() followed by the uploads it returns."""
+        self.grid_origin = (self.grid_origin[0] + dx, self.grid_origin[1] + dy, self.grid_origin[2] + dz)
+        want = set(self.keys_in_grid())
+        moves = []
+        for k in [k for k in self.slot_to_key if k not in want]:
+            slot = self.key_to_slot.pop(k)
+            base, n = self.alloc.pop(k)
+            self.arena.release(base, n)
+            last = len(self.slot_to_key) - 1
+            if slot != last:
+                mkey = self.slot_to_key[last]
+                self.slot_to_key[slot] = mkey
+                self.key_to_slot[mkey] = slot
+                moves.append((last, slot))
+            self.slot_to_key.pop()
+        renderer.move_slots(moves)
+        self._add_device(renderer, [k for k in self.keys_in_grid() if k not in self.key_to_slot])
         self.rebuild_grid()
         renderer.write_chunk_grid(self.grid)
 
