@@ -542,21 +542,25 @@ def run_e2e(args, sc, dev, world_size):
 
     drv = r = None
 
-    def setup():
-        """A fresh driver, world and renderer: both read-back modes run the same frames."""
+    def setup(device_streaming=False):
+        """A fresh driver, world and renderer: every mode runs the same frames.
+        Host streaming: chunks entering the grid at the shifts are built on the
+        host before timing (the reference builds them on its worker pool) and
+        their upload is timed.  Device streaming: they are built resident on
+        the device inside the timed region and slots move on the device."""
         nonlocal drv, r
-        drv = FrameDriver(sc)
+        cap = int(np.prod(sc.grid_dims))
+        r = Renderer(sc.present[0], sc.present[1], sc.render_scale, node_capacity=sc.node_capacity,
+                     chunk_capacity=cap, grid_capacity=cap, clip_levels=sc.clip_levels, clip_res=sc.clip_res,
+                     flags=A.FLAG_GODRAY_MACRO_ALIAS, device=dev)
+        drv = FrameDriver(sc, device_renderer=r if device_streaming else None)
         ups = drv.initial_uploads()
-        # Chunks entering the grid at the shifts are built on the host before timing
-        # (the reference builds them on its worker pool); their upload is timed.
-        for ox in range(1, 4):
-            for iz in range(sc.grid_dims[2]):
-                for iy in range(sc.grid_dims[1]):
-                    drv.world.chunk((ox + sc.grid_dims[0] - 1, iy, iz))
-        r = Renderer(sc.present[0], sc.present[1], sc.render_scale, node_capacity=drv.world.node_capacity,
-                     chunk_capacity=drv.world.chunk_capacity, grid_capacity=drv.world.grid_capacity,
-                     clip_levels=sc.clip_levels, clip_res=sc.clip_res, flags=A.FLAG_GODRAY_MACRO_ALIAS, device=dev)
-        r.upload_world(drv.world, ups)
+        if not device_streaming:
+            for ox in range(1, 4):
+                for iz in range(sc.grid_dims[2]):
+                    for iy in range(sc.grid_dims[1]):
+                        drv.world.chunk((ox + sc.grid_dims[0] - 1, iy, iz))
+            r.upload_world(drv.world, ups)
 
     pw, ph = sc.present
     host_out = [torch.empty((ph, pw, 4), dtype=torch.float32).pin_memory().numpy() for _ in range(2)]
@@ -568,14 +572,25 @@ def run_e2e(args, sc, dev, world_size):
         queued on the copy stream (returns the ticket)."""
         nonlocal h2d, d2h
         back = []
+        b = 464
+        drv.last_shift = None
         if drv.frame >= 64:
             # restart the path: the grid returns to its first origin
             drv.frame = 0
-            back = drv.world.shift(-drv.world.grid_origin[0], 0, 0)
+            if drv.device is not None:
+                built, moved = drv.world.shift_device(r, -drv.world.grid_origin[0], 0, 0)
+                # coords + places + slot moves + grid in, node counts out
+                b += 36 * built + 8 * moved + drv.world.grid.nbytes
+                d2h += 8 * built
+            else:
+                back = drv.world.shift(-drv.world.grid_origin[0], 0, 0)
         uploads, grid_changed, clip, cam = drv.step()
+        if drv.last_shift is not None:
+            built, moved = drv.last_shift
+            b += 36 * built + 8 * moved + drv.world.grid.nbytes
+            d2h += 8 * built
         if back:
             uploads, grid_changed = back + uploads, True
-        b = 464
         if uploads:
             r.apply_chunk_uploads(uploads)
             b += sum(48 + (len(u.data.nodes) * 48 + 16 * 4 + 2048 * 4 if u.data is not None else 0) for u in uploads)
@@ -622,13 +637,35 @@ def run_e2e(args, sc, dev, world_size):
 
     setup()
     dt = timed(True)
+    bytes_host = (h2d, d2h)
     r.close()
     setup()
     serial_s = timed(False)
     r.close()
+    setup(device_streaming=True)
+    dev_s = timed(True)
+    bytes_dev = (h2d, d2h)
+    r.close()
+    h2d, d2h = bytes_host
     rays = sc.internal[0] * sc.internal[1] * args.steps
     return {"seconds": dt, "rays": rays, "h2d_bytes_per_step": h2d // args.steps,
-            "d2h_bytes_per_step": d2h // args.steps, "serial_seconds": serial_s}
+            "d2h_bytes_per_step": d2h // args.steps, "serial_seconds": serial_s,
+            "device_streaming": {"seconds": dev_s, "h2d_bytes_per_step": bytes_dev[0] // args.steps,
+                                 "d2h_bytes_per_step": bytes_dev[1] // args.steps}}
+
+
+def device_streaming_line(e2e: dict, steps: int, n: int):
+    """The e2e frames with the world streamed on the device (resident builds of
+    the entering chunks and device slot moves inside the timed region)."""
+    ds = e2e.get("device_streaming")
+    if not ds or not ds["seconds"] == ds["seconds"]:
+        return None
+    return {"value": round(replica_value(e2e["rays"], n, ds["seconds"]), 3), "unit": UNIT,
+            "frame_ms": round(ds["seconds"] * 1e3 / steps, 3), "h2d_bytes_per_step": ds["h2d_bytes_per_step"],
+            "d2h_bytes_per_step": ds["d2h_bytes_per_step"],
+            "note": "pipelined read-back; chunks entering at the grid shifts built resident on the device "
+                    "(counting build + count read-back + resident build) and slots moved on the device, "
+                    "inside the timed region"}
 
 
 def cpu_sample(seconds: float, present, threads: int):
@@ -753,7 +790,8 @@ def main():
                 "frame_ms": round(e2e_s * 1e3 / args.steps, 3),
                 "mode": "pipelined: step i's output read back on the copy stream while frame i+1 runs "
                         "(vxe_read_image_async, waited one step later; every output lands inside the timed region)",
-                "serial_frame_ms": round(res["e2e"]["serial_seconds"] * 1e3 / args.steps, 3)},
+                "serial_frame_ms": round(res["e2e"]["serial_seconds"] * 1e3 / args.steps, 3),
+                "device_streaming": device_streaming_line(res["e2e"], args.steps, n)},
         # per frame: k_grass_cells, k_tiles, k_primary_trace, k_probe_dda, k_slab_eval, k_slab_pick,
         # k_primary_resolve, k_shade_prep, k_shade_shadow, k_shade_lights, k_shade_vox, k_shade_far x 2 (side
         # stream), k_godray, k_composite

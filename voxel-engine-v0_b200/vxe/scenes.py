@@ -151,6 +151,7 @@ class FrameDriver:
         returns no uploads and writes the grid itself)."""
         self.scene = scene
         self.device = device_renderer
+        self.last_shift = None  # (chunks built, slots moved) of the last device shift
         self.world = World(scene.spec, scene.grid_origin, scene.grid_dims, scene.node_capacity,
                            chunk_capacity=int(np.prod(scene.grid_dims)))
         self.clip = Clipmap(scene.spec, scene.clip_levels, scene.clip_res, 1.0) if scene.clip_levels else None
@@ -170,7 +171,7 @@ class FrameDriver:
         uploads, grid_changed = [], False
         if sc.shift_every and f > 0 and f % sc.shift_every == 0:
             if self.device is not None:
-                self.world.shift_device(self.device, 1, 0, 0)
+                self.last_shift = self.world.shift_device(self.device, 1, 0, 0)
             else:
                 uploads = self.world.shift(1, 0, 0)
                 grid_changed = True

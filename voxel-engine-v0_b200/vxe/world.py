@@ -313,12 +313,13 @@ class World:
         self.rebuild_grid()
         renderer.write_chunk_grid(self.grid)
 
-    def shift_device(self, renderer, dx: int, dy: int, dz: int) -> None:
+    def shift_device(self, renderer, dx: int, dy: int, dz: int) -> tuple:
         """shift() for a world kept on the device: chunks that left free their
         arena range and the last slot moves into each hole (vxe_move_slots, in
         the order remove() takes them), entering chunks are built resident
         (_add_device), then the grid -- the same slots, arena ranges and
-        device records as shift() followed by the uploads it returns."""
+        device records as shift() followed by the uploads it returns.  Returns
+        (chunks built, slots moved)."""
         self.grid_origin = (self.grid_origin[0] + dx, self.grid_origin[1] + dy, self.grid_origin[2] + dz)
         want = set(self.keys_in_grid())
         moves = []
@@ -334,9 +335,11 @@ class World:
                 moves.append((last, slot))
             self.slot_to_key.pop()
         renderer.move_slots(moves)
-        self._add_device(renderer, [k for k in self.keys_in_grid() if k not in self.key_to_slot])
+        new = [k for k in self.keys_in_grid() if k not in self.key_to_slot]
+        self._add_device(renderer, new)
         self.rebuild_grid()
         renderer.write_chunk_grid(self.grid)
+        return len(new), len(moves)
 
     def populate(self) -> list[Upload]:
         self.prebuild(list(self.keys_in_grid()))
