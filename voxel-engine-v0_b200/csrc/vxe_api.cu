@@ -1395,6 +1395,7 @@ vxe_status vxe_write_image(vxe_ctx* c, vxe_image im, const void* host, size_t by
   if (bytes != c->fr.img[i].bytes) return fail(c, VXE_ERR_INVALID_ARG, "image %d is %zu bytes, got %zu", (int)im, c->fr.img[i].bytes, bytes);
   cudaSetDevice(c->device);
   CK(cudaStreamSynchronize(c->compute));
+  if (c->copy) CK(cudaStreamSynchronize(c->copy));  // an asynchronous read of this image may be in flight
   CK(cudaMemcpy(c->fr.img[i].p, host, bytes, cudaMemcpyHostToDevice));
   CK(cudaStreamSynchronize(cudaStreamLegacy));  // a pageable copy may still be landing
   return VXE_OK;
