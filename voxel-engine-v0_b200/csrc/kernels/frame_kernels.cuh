@@ -588,9 +588,10 @@ __device__ __forceinline__ float shadow_blend(const Scene& s, const FrameArgs& A
 }
 
 // `light` is gather_voxel_lights' result when lights_wanted(best).
+// `depth_written`: k_shade_prep already stored this pixel's depth.
 __device__ __noinline__ void shade_voxel_final(const Scene& s, const FrameArgs& A, const PrimaryCtx& c,
                                                const HitGeom& best, float shadow_out, v3 light, bool anchor_valid,
-                                               uint32_t anchor_key, i3 anchor_chunk) {
+                                               uint32_t anchor_key, i3 anchor_chunk, bool depth_written) {
   const float vs = vs_(s);
   const v3 ro = c.ro, rd = c.rd;
   const v3 sky_up = sky_bg(V3(0.0f, 1.0f, 0.0f));
@@ -612,7 +613,7 @@ __device__ __noinline__ void shade_voxel_final(const Scene& s, const FrameArgs& 
     ak = anchor_key;
   }
   A.color[c.pix] = make_float4(col.x, col.y, col.z, 1.0f);
-  A.depth[c.pix] = t_scene;
+  if (!depth_written) A.depth[c.pix] = t_scene;
   A.hist_out[c.pix] = make_uint4(__float_as_uint(t_scene), ak, pxy, pz);
   A.shadow_out[c.pix] = shadow_out;
   if (A.hits) store_rec(A.hits + c.pix * 2u, make_rec(best, ro, rd, vs, true));
@@ -632,7 +633,7 @@ __device__ __noinline__ void shade_voxel_pixel(const Scene& s, const FrameArgs& 
   }
   v3 light = V3s(0.0f);
   if (lights_wanted(best)) light = gather_voxel_lights(s, c.ro + c.rd * best.t, best.n, best.root_bmin);
-  shade_voxel_final(s, A, c, best, shadow_out, light, anchor_valid, anchor_key, anchor_chunk);
+  shade_voxel_final(s, A, c, best, shadow_out, light, anchor_valid, anchor_key, anchor_chunk, false);
 }
 
 // Heightfield then sky (ray_main.wgsl:224-269 / 327-372 / 473-516) + outputs.
@@ -984,6 +985,7 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_shade_prep(const __grid_const
         src[0] = make_uint4(__float_as_uint(g.t), __float_as_uint(g.n.x), __float_as_uint(g.n.y),
                             __float_as_uint(g.n.z));
       }
+      A.depth[pix] = fmin_(g.t, FOG_MAX_DIST);  // final: godray may start before k_shade_vox
       fresh = shadow_fresh(c);
       light = lights_wanted(g);
       if (light && !lights_possible(s, (c.ro + c.rd * g.t) + g.n * (0.75f * vs_(s)))) {
@@ -1063,7 +1065,8 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_shade_vox(const __grid_consta
       const float4 l = A.px_light[pix];
       light = V3(l.x, l.y, l.z);
     }
-    shade_voxel_final(s, A, c, g, shadow_out, light, e.w != 0u, f.x, i3{(int32_t)f.y, (int32_t)f.z, (int32_t)f.w});
+    shade_voxel_final(s, A, c, g, shadow_out, light, e.w != 0u, f.x, i3{(int32_t)f.y, (int32_t)f.z, (int32_t)f.w},
+                      true);
   }
 }
 

@@ -95,7 +95,7 @@ struct FrameState {
 // resolve and the voxel shading) and joins back before the godray pass.
 struct SideStream {
   cudaStream_t s = nullptr;
-  cudaEvent_t fork = nullptr, mid = nullptr, join = nullptr;
+  cudaEvent_t fork = nullptr, mid = nullptr, prep = nullptr, join = nullptr;
 };
 
 struct BatchLane {
@@ -582,7 +582,7 @@ void frame_fill(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& cam, FrameArgs&
 vxe_status side_ready(vxe_ctx* c, SideStream& S) {
   if (S.s) return VXE_OK;
   CK(cudaStreamCreateWithFlags(&S.s, cudaStreamNonBlocking));
-  for (cudaEvent_t* e : {&S.fork, &S.mid, &S.join}) CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  for (cudaEvent_t* e : {&S.fork, &S.mid, &S.prep, &S.join}) CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   return VXE_OK;
 }
 
@@ -591,7 +591,7 @@ void side_release(SideStream& S) {
     cudaStreamSynchronize(S.s);
     cudaStreamDestroy(S.s);
   }
-  for (cudaEvent_t e : {S.fork, S.mid, S.join})
+  for (cudaEvent_t e : {S.fork, S.mid, S.prep, S.join})
     if (e) cudaEventDestroy(e);
   S = SideStream{};
 }
@@ -638,9 +638,20 @@ vxe_status frame_enqueue(vxe_ctx* c, FrameState& F, const FrameArgs& A, bool tim
       CK(cudaEventRecord(side->mid, st));
       CK(cudaStreamWaitEvent(side->s, side->mid, 0));
       k_shade_far<1><<<grid(npix), SHADE_THREADS, 0, side->s>>>(A);
-      CK(cudaEventRecord(side->join, side->s));
     }
     k_shade_prep<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
+    if (side) {
+      // Every depth is final here (voxel pixels' from k_shade_prep, far
+      // pixels' from k_shade_far), and godray reads nothing else the shading
+      // writes: it runs beside the rest of the voxel shading.
+      CK(cudaEventRecord(side->prep, st));
+      CK(cudaStreamWaitEvent(side->s, side->prep, 0));
+      if (timed) CK(cudaEventRecord(F.ev[4], side->s));
+      k_godray<<<dim3((F.iw + POST_THREADS_X - 1) / POST_THREADS_X, (F.ih + POST_THREADS_Y - 1) / POST_THREADS_Y),
+                 dim3(POST_THREADS_X, POST_THREADS_Y), 0, side->s>>>(A);
+      if (timed) CK(cudaEventRecord(F.ev[5], side->s));
+      CK(cudaEventRecord(side->join, side->s));
+    }
     k_shade_shadow<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
     k_shade_lights<<<grid((uint64_t)npix * 8u), SHADE_THREADS, 0, st>>>(A);
     k_shade_vox<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
@@ -649,10 +660,12 @@ vxe_status frame_enqueue(vxe_ctx* c, FrameState& F, const FrameArgs& A, bool tim
     else
       k_shade_far<2><<<grid(npix), SHADE_THREADS, 0, st>>>(A);
   }
-  if (timed) CK(cudaEventRecord(F.ev[4], st));
-  k_godray<<<dim3((F.iw + POST_THREADS_X - 1) / POST_THREADS_X, (F.ih + POST_THREADS_Y - 1) / POST_THREADS_Y),
-             dim3(POST_THREADS_X, POST_THREADS_Y), 0, st>>>(A);
-  if (timed) CK(cudaEventRecord(F.ev[5], st));
+  if (!side || (c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL)) {
+    if (timed) CK(cudaEventRecord(F.ev[4], st));
+    k_godray<<<dim3((F.iw + POST_THREADS_X - 1) / POST_THREADS_X, (F.ih + POST_THREADS_Y - 1) / POST_THREADS_Y),
+               dim3(POST_THREADS_X, POST_THREADS_Y), 0, st>>>(A);
+    if (timed) CK(cudaEventRecord(F.ev[5], st));
+  }
   if (F.composite_wait) CK(cudaStreamWaitEvent(st, F.composite_wait, 0));
   k_composite<<<dim3((F.pw + POST_THREADS_X - 1) / POST_THREADS_X, (F.ph + POST_THREADS_Y - 1) / POST_THREADS_Y),
                 dim3(POST_THREADS_X, POST_THREADS_Y), 0, st>>>(A);
