@@ -233,7 +233,7 @@ def run_vxe(args, rank: int, world_size: int):
 
 
 def run_batch_serve(dev):
-    """Batched (north-star item 2) and served (item 5) workloads on the config-2 world.
+    """Batched and served workloads (mixed viewport / query batches; Poisson request serving) on the config-2 world.
 
     batch: the config-3 request mix (24 viewports 128^2-1920x1080, 40 query
     batches 1e3-1e6 rays, seeded) as one persistent batch vs one plain launch
@@ -753,7 +753,7 @@ def main():
     if res is None:
         return
     batch = srv = configs = None
-    if not args.no_batch and world_size == 1:  # one GPU: the workloads north-star items 2 and 5 name
+    if not args.no_batch and world_size == 1:  # one GPU: the batched, served, secondary-config and builder lines
         batch, srv = run_batch_serve(0)
         configs = run_configs(0)
         configs["clipmap_patches"] = run_clipmap(0)
