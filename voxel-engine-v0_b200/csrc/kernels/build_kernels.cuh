@@ -308,6 +308,18 @@ __global__ void __launch_bounds__(256) k_build_columns(const __grid_constant__ B
   uint8_t* mat = B.mat + (size_t)chunk * kVoxels + z * 64u + x;
   uint32_t* st5 = B.st5 + (size_t)chunk * kCells5 + (z >> 1) * 32u + (x >> 1);
   uint32_t top = 255u, top_m = 0u, solid = 0u;
+  if (__all_sync(0xFFFFFFFFu, B.wp.features == 0u && oy > g)) {
+    // Every voxel of the warp's 32 columns lies above its surface and the
+    // world has no decorations: all air.  Materials and level-5 states are
+    // zero; stored as 16-byte rows (16 x of one z row / 4 cells of one row).
+    const uint32_t z0 = ((tile >> 2) << 4) | (w << 1), x0 = (tile & 3u) << 4;
+    uint8_t* m0 = B.mat + (size_t)chunk * kVoxels + z0 * 64u + x0;
+    for (uint32_t j = lane; j < 128u; j += 32u)  // 64 layers x 2 rows
+      *reinterpret_cast<uint4*>(m0 + (j >> 1) * 4096u + (j & 1u) * 64u) = make_uint4(0u, 0u, 0u, 0u);
+    uint32_t* s0 = B.st5 + (size_t)chunk * kCells5 + (z0 >> 1) * 32u + (x0 >> 1);
+    for (uint32_t j = lane; j < 64u; j += 32u)  // 32 cell layers x 8 cells
+      *reinterpret_cast<uint4*>(s0 + (j >> 1) * 1024u + (j & 1u) * 4u) = make_uint4(0u, 0u, 0u, 0u);
+  } else {
 #pragma unroll 1
   for (uint32_t kb = 0; kb < 8u; ++kb) {
     uint64_t acc = 0;  // 16 bits per layer pair: materials of y = 2k, 2k+1
@@ -338,6 +350,7 @@ __global__ void __launch_bounds__(256) k_build_columns(const __grid_constant__ B
     }
     const uint32_t k = 4u * kb + role;
     st5[k * 1024u] = cell_state(cs, oy + (int32_t)(2u * k + 1u), gmin, B.wp.dirt_depth);
+  }
   }
   // colinfo (builder.rs:742-771): column pairs (x even, x odd) share a word
   const uint32_t e = top | (top_m << 8), eo = __shfl_xor_sync(0xFFFFFFFFu, e, 1);
@@ -378,6 +391,33 @@ __device__ __forceinline__ uint32_t rope_down(uint32_t nei, const vxe_node& n, u
   return n.child_base + (uint32_t)__popc(n.child_mask & ((1u << ci) - 1u));
 }
 
+// Counts and, for a resident build, the slot's ChunkMetaGpu (macro_empty <=>
+// no solid voxel); a resident chunk needing more nodes than its place
+// reserves gets an empty meta and the error bit.
+__device__ void write_counts_meta(const BuildArgs& B, uint32_t chunk, uint32_t node_count, uint32_t solid) {
+  if (B.counts) {
+    B.counts[2u * chunk] = node_count;
+    B.counts[2u * chunk + 1u] = solid;
+  }
+  if (B.place) {
+    const vxe_build_place& pl = B.place[chunk];
+    const bool fits = node_count <= pl.node_count;
+    vxe_chunk_meta m;
+    m.origin[0] = pl.cx * kSide;
+    m.origin[1] = pl.cy * kSide;
+    m.origin[2] = pl.cz * kSide;
+    m.origin[3] = 0;
+    m.node_base = pl.node_base;
+    m.node_count = fits ? node_count : 0u;
+    m.macro_base = pl.slot * VXE_MACRO_WORDS_PER_CHUNK;
+    m.colinfo_base = pl.slot * VXE_COLINFO_WORDS_PER_CHUNK;
+    m.macro_empty = fits ? (solid == 0u ? 1u : 0u) : 1u;
+    m._pad0 = m._pad1 = m._pad2 = 0u;
+    B.metas[pl.slot] = m;
+    if (!fits) atomicOr(B.error_word, ERR_BUILD);
+  }
+}
+
 __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_constant__ BuildArgs B) {
   __shared__ uint32_t st[kLowCells];
   __shared__ uint32_t kb[kLowCells];
@@ -393,6 +433,27 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
   uint32_t* kb5 = B.kb5 + (size_t)chunk * kCells5;
   const int32_t chunk_oy = chunk_coord(B, chunk, 1) * kSide;
   const int32_t dirt = B.wp.dirt_depth;
+  uint32_t solid = 0;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) solid += B.solid_part[(size_t)chunk * 16u + i];
+  if (solid == 0u) {
+    // No solid voxel: the list is the root alone, an air leaf with no
+    // neighbours; every macro bit is clear (what the general path gives).
+    const uint32_t cap = B.place ? B.place[chunk].node_count : B.node_cap;
+    if (t < VXE_MACRO_WORDS_PER_CHUNK) B.macro[(size_t)chunk_slot(B, chunk) * VXE_MACRO_WORDS_PER_CHUNK + t] = 0u;
+    if (t == 0) {
+      write_counts_meta(B, chunk, 1u, 0u);
+      if (cap >= 1u) {
+        const size_t node0 = B.place ? (size_t)B.place[chunk].node_base : (size_t)chunk * cap;
+        B.nodes[node0] = node_of(ST_LEAF, 0u, 0u);
+        vxe_node_ropes r;
+        r.px = r.nx = r.py = r.ny = r.pz = r.nz = kInvalid;
+        r._pad0 = r._pad1 = 0u;
+        B.ropes[node0] = r;
+      }
+    }
+    return;
+  }
 
   // -- ground min-mip levels 1..6 (mips.rs:4-90) ------------------------------
   for (uint32_t i = t; i < 1024u; i += SVO_THREADS) mip[i] = B.mip1[(size_t)chunk * 1024u + i];
@@ -552,31 +613,7 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
   __syncthreads();  // kb5 and the voxel records visible to the CTA
   const uint32_t node_count = bases[7];
 
-  if (t == 0) {
-    uint32_t solid = 0;
-    for (int i = 0; i < 16; ++i) solid += B.solid_part[(size_t)chunk * 16u + i];
-    if (B.counts) {
-      B.counts[2u * chunk] = node_count;
-      B.counts[2u * chunk + 1u] = solid;
-    }
-    if (B.place) {  // ChunkMetaGpu of the slot (macro_empty <=> no solid voxel)
-      const vxe_build_place& pl = B.place[chunk];
-      const bool fits = node_count <= pl.node_count;
-      vxe_chunk_meta m;
-      m.origin[0] = pl.cx * kSide;
-      m.origin[1] = pl.cy * kSide;
-      m.origin[2] = pl.cz * kSide;
-      m.origin[3] = 0;
-      m.node_base = pl.node_base;
-      m.node_count = fits ? node_count : 0u;
-      m.macro_base = pl.slot * VXE_MACRO_WORDS_PER_CHUNK;
-      m.colinfo_base = pl.slot * VXE_COLINFO_WORDS_PER_CHUNK;
-      m.macro_empty = fits ? (solid == 0u ? 1u : 0u) : 1u;
-      m._pad0 = m._pad1 = m._pad2 = 0u;
-      B.metas[pl.slot] = m;
-      if (!fits) atomicOr(B.error_word, ERR_BUILD);
-    }
-  }
+  if (t == 0) write_counts_meta(B, chunk, node_count, solid);
   // macro bits: bit mx + 8*(my + 8*mz) <=> level-3 cell present (builder.rs:809-841)
   if (t < VXE_MACRO_WORDS_PER_CHUNK) {
     uint32_t word = 0;
