@@ -391,6 +391,19 @@ __device__ __forceinline__ uint32_t rope_down(uint32_t nei, const vxe_node& n, u
   return n.child_base + (uint32_t)__popc(n.child_mask & ((1u << ci) - 1u));
 }
 
+// Node index of the present level-l cell (x, y, z), l = 1..5, whose parent
+// is internal: its parent's child offset plus its rank among the parent's
+// present children (state words and offsets of levels 4..0 in shared memory).
+__device__ __forceinline__ uint32_t level_node(const uint32_t* st, const uint32_t* kb, const uint32_t* bases, int l,
+                                               uint32_t x, uint32_t y, uint32_t z) {
+  const int pl = l - 1;
+  const uint32_t ps = 1u << pl;
+  const uint32_t pi = (x >> 1) + ((z >> 1) + (y >> 1) * ps) * ps;
+  const uint32_t ci = (x & 1u) | ((y & 1u) << 1) | ((z & 1u) << 2);
+  const uint32_t mask = st[low_off(pl) + pi] & ST_MASK;
+  return bases[l] + kb[low_off(pl) + pi] + (uint32_t)__popc(mask & ((1u << ci) - 1u));
+}
+
 // Counts and, for a resident build, the slot's ChunkMetaGpu (macro_empty <=>
 // no solid voxel); a resident chunk needing more nodes than its place
 // reserves gets an empty meta and the error bit.
@@ -590,6 +603,7 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       if (!cnt[k]) continue;
+      const uint32_t parent = level_node(st, kb, bases, 5, px0 + k, py, pz);
 #pragma unroll
       for (int ci = 0; ci < 8; ++ci) {
         if (!((sv[k] >> ci) & 1u)) continue;
@@ -601,6 +615,7 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
           n.material = (uint32_t)(rw[((ci >> 1) & 1) * 2 + ((ci >> 2) & 1)] >> (8 * (2 * k + (ci & 1)))) & 0xFFu;
           n.key = cell_key(cx, cy, cz, 6u);
           nodes[o] = n;
+          ropes[o]._pad0 = parent;  // until the rope pass writes the record
         }
         ++o;
       }
@@ -645,10 +660,12 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
         ckb[ci] = !has ? 0u : l == 4 ? kb5[c] : kb[low_off(l + 1) + c];
       }
       uint32_t o = bases[l + 1] + kb[low_off(l) + i];
+      const uint32_t parent = l == 0 ? 0u : level_node(st, kb, bases, l, px, py, pz);
 #pragma unroll
       for (int ci = 0; ci < 8; ++ci) {
         if (!((s >> ci) & 1u)) continue;
         const uint32_t cx = 2u * px + (ci & 1), cy = 2u * py + ((ci >> 1) & 1), cz = 2u * pz + ((ci >> 2) & 1);
+        ropes[o]._pad0 = parent;  // until the rope pass writes the record
         nodes[o++] = node_of(cs[ci], ckb[ci] + bases[l + 2], cell_key(cx, cy, cz, (uint32_t)l + 1u));
       }
     }
@@ -663,40 +680,36 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
     ropes[0] = r;
   }
   __syncthreads();
-  for (int l = 0; l <= 5; ++l) {  // parents in level l's list
-    const uint32_t lo = bases[l], hi = l == 0 ? 1u : bases[l] + K[l];
-    for (uint32_t p = lo + t; p < hi; p += SVO_THREADS) {
+  // One thread per node of level l's list (consecutive lanes, consecutive
+  // records): its parent (parked in the pad word at emission), the parent's
+  // ropes and children give its 6 ropes; siblings read the same parent and
+  // neighbour records, so those loads hit L1.
+  for (int l = 1; l <= 6; ++l) {
+    const uint32_t lo = bases[l], hi = bases[l] + K[l];
+    for (uint32_t k = lo + t; k < hi; k += SVO_THREADS) {
+      const uint32_t p = ropes[k]._pad0;
+      const uint32_t key = nodes[k].key;
+      const uint32_t hx = key & 1u, hy = (key >> 6) & 1u, hz = (key >> 12) & 1u;
+      const uint32_t ci = hx | (hy << 1) | (hz << 2);
       const vxe_node pn = nodes[p];
-      if (pn.child_base == kInvalid) continue;
       const vxe_node_ropes pr = ropes[p];
-      // the parent's 6 face neighbours, read once for all 8 children
-      const uint32_t nei[6] = {pr.px, pr.nx, pr.py, pr.ny, pr.pz, pr.nz};
-      vxe_node nn[6];
-#pragma unroll
-      for (int d = 0; d < 6; ++d) {
-        if (nei[d] != kInvalid) nn[d] = nodes[nei[d]];
-        else nn[d].child_base = nn[d].child_mask = 0u;
-      }
-      uint32_t kid[8];
-#pragma unroll
-      for (uint32_t ci = 0; ci < 8; ++ci)
-        kid[ci] = (pn.child_mask & (1u << ci)) ? pn.child_base + (uint32_t)__popc(pn.child_mask & ((1u << ci) - 1u))
-                                                : kInvalid;
-#pragma unroll
-      for (uint32_t ci = 0; ci < 8; ++ci) {
-        if (kid[ci] == kInvalid) continue;
-        const uint32_t hx = ci & 1u, hy = (ci >> 1) & 1u, hz = (ci >> 2) & 1u;
-        const uint32_t sx = kid[ci ^ 1u], sy = kid[ci ^ 2u], sz = kid[ci ^ 4u];
-        vxe_node_ropes r;
-        r.px = (hx == 0 && sx != kInvalid) ? sx : rope_down(nei[0], nn[0], 0u | (hy << 1) | (hz << 2));
-        r.nx = (hx == 1 && sx != kInvalid) ? sx : rope_down(nei[1], nn[1], 1u | (hy << 1) | (hz << 2));
-        r.py = (hy == 0 && sy != kInvalid) ? sy : rope_down(nei[2], nn[2], hx | (0u << 1) | (hz << 2));
-        r.ny = (hy == 1 && sy != kInvalid) ? sy : rope_down(nei[3], nn[3], hx | (1u << 1) | (hz << 2));
-        r.pz = (hz == 0 && sz != kInvalid) ? sz : rope_down(nei[4], nn[4], hx | (hy << 1) | (0u << 2));
-        r.nz = (hz == 1 && sz != kInvalid) ? sz : rope_down(nei[5], nn[5], hx | (hy << 1) | (1u << 2));
-        r._pad0 = r._pad1 = 0u;
-        ropes[kid[ci]] = r;
-      }
+      auto kid = [&](uint32_t c) -> uint32_t {
+        return (pn.child_mask & (1u << c)) ? pn.child_base + (uint32_t)__popc(pn.child_mask & ((1u << c) - 1u))
+                                           : kInvalid;
+      };
+      auto down = [&](uint32_t nei, uint32_t c) -> uint32_t {
+        return nei == kInvalid ? kInvalid : rope_down(nei, nodes[nei], c);
+      };
+      const uint32_t sx = kid(ci ^ 1u), sy = kid(ci ^ 2u), sz = kid(ci ^ 4u);
+      vxe_node_ropes r;
+      r.px = (hx == 0 && sx != kInvalid) ? sx : down(pr.px, 0u | (hy << 1) | (hz << 2));
+      r.nx = (hx == 1 && sx != kInvalid) ? sx : down(pr.nx, 1u | (hy << 1) | (hz << 2));
+      r.py = (hy == 0 && sy != kInvalid) ? sy : down(pr.py, hx | (0u << 1) | (hz << 2));
+      r.ny = (hy == 1 && sy != kInvalid) ? sy : down(pr.ny, hx | (1u << 1) | (hz << 2));
+      r.pz = (hz == 0 && sz != kInvalid) ? sz : down(pr.pz, hx | (hy << 1) | (0u << 2));
+      r.nz = (hz == 1 && sz != kInvalid) ? sz : down(pr.nz, hx | (hy << 1) | (1u << 2));
+      r._pad0 = r._pad1 = 0u;
+      ropes[k] = r;
     }
     __syncthreads();
   }
