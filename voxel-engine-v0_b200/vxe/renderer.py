@@ -142,6 +142,11 @@ class Renderer:
         self.synchronize()
         return out
 
+    @property
+    def torch_device(self) -> str:
+        """The torch device string of this context's GPU."""
+        return f"cuda:{self.device}"
+
     def build_chunks(self, world_params, coords, node_cap=None):
         """Builds chunks on the device (the GPU counterpart of the chunk builder,
         svo/builder.rs:846-986).  `coords`: torch int32 tensor (n, 3) of chunk

@@ -260,7 +260,7 @@ class World:
         wp = self.spec.params()
         for i in range(0, len(todo), batch):
             part = todo[i:i + batch]
-            coords = torch.tensor(part, dtype=torch.int32, device=f"cuda:{renderer.device}")
+            coords = torch.tensor(part, dtype=torch.int32, device=renderer.torch_device)
             cap = int(renderer.build_chunks(wp, coords, node_cap=0)["counts"][:, 0].max())
             out = renderer.build_chunks(wp, coords, node_cap=cap)
             cnt = out["counts"][:, 0]
@@ -288,7 +288,7 @@ class World:
         wp = self.spec.params()
         for i in range(0, len(keys), batch):
             part = keys[i:i + batch]
-            coords = torch.tensor(part, dtype=torch.int32, device=f"cuda:{renderer.device}")
+            coords = torch.tensor(part, dtype=torch.int32, device=renderer.torch_device)
             counts = renderer.build_chunks(wp, coords, node_cap=0)["counts"].cpu().numpy().view(np.uint32)
             places = []
             for key, (n, _solid) in zip(part, counts.tolist()):
