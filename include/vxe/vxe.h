@@ -487,7 +487,7 @@ vxe_status vxe_solid_voxels_device(vxe_ctx* ctx, const int32_t* d_vox, uint32_t 
  * only counts).  Launched on the context's world-write stream;
  * vxe_synchronize waits for it. */
 #define VXE_BUILD_NODE_CAP_MAX 299593u /* 1 + 8 + 8^2 + ... + 8^6 */
-#define VXE_BUILD_BATCH_MAX 512u
+#define VXE_BUILD_BATCH_MAX 2048u
 vxe_status vxe_build_chunks_device(vxe_ctx* ctx, const vxe_world_params* world, const int32_t* d_coords, uint32_t n,
                                    uint32_t node_cap, vxe_node* d_nodes, vxe_node_ropes* d_ropes, uint32_t* d_macro,
                                    uint32_t* d_colinfo, uint32_t* d_counts);

@@ -133,7 +133,7 @@ ERR_WORD_BUILD = 1 << 7
 class SlotMove(C.Structure):
     _fields_ = [("from_", C.c_uint32), ("to", C.c_uint32)]
 BUILD_NODE_CAP_MAX = 299593
-BUILD_BATCH_MAX = 512
+BUILD_BATCH_MAX = 2048
 
 
 class WorldParams(C.Structure):

@@ -278,7 +278,7 @@ class World:
                                             colinfo[j], int(counts[j, 1]))
                 first += n
 
-    def _add_device(self, renderer, keys, batch: int = 512) -> None:
+    def _add_device(self, renderer, keys, batch: int = 2048) -> None:
         """add() for `keys`, built on the device straight into `renderer`'s
         world: a counting build per batch gives the node counts, slots and
         arena ranges are taken exactly as add() takes them, the resident build
@@ -304,7 +304,7 @@ class World:
                 places.append((key, slot, base, n))
             renderer.build_resident(wp, places)
 
-    def populate_device(self, renderer, batch: int = 512) -> None:
+    def populate_device(self, renderer, batch: int = 2048) -> None:
         """populate() with every chunk built on the device straight into
         `renderer`'s world (_add_device), then the grid.  No chunk data passes
         through the host, so this world's host mirrors (nodes, ropes, macro,
