@@ -230,3 +230,34 @@ def test_device_streaming_renders_like_host_streaming():
     finally:
         rh.close()
         rd.close()
+
+
+def test_builder_and_slot_move_argument_checks():
+    """Oversized batches, caps and out-of-range slots are refused before any
+    launch, with the context still usable."""
+    import torch
+
+    r = _renderer()
+    try:
+        wp = CARVE.params()
+        too_many = torch.zeros((A.BUILD_BATCH_MAX + 1, 3), dtype=torch.int32, device="cuda:0")
+        with pytest.raises(A.VxeError):
+            r.build_chunks(wp, too_many, node_cap=0)
+        with pytest.raises(A.VxeError):
+            r.build_chunks(wp, too_many[:1], node_cap=A.BUILD_NODE_CAP_MAX + 1)
+        with pytest.raises(A.VxeError):  # slot outside the context's 16
+            r.build_resident(wp, [((0, 0, 0), 16, 0, 10)])
+        with pytest.raises(A.VxeError):  # nodes outside the arena
+            r.build_resident(wp, [((0, 0, 0), 0, (1 << 16) - 5, 10)])
+        with pytest.raises(A.VxeError):  # two places on the same arena nodes
+            r.build_resident(wp, [((0, 0, 0), 0, 0, 10), ((1, 0, 0), 1, 5, 10)])
+        with pytest.raises(A.VxeError):
+            r.move_slots([(0, 16)])
+        # still usable: a real build and a move
+        key = (0, 0, 0)
+        n = len(build_chunk(CARVE, *key).nodes)
+        r.build_resident(wp, [(key, 2, 0, n)])
+        r.move_slots([(2, 3)])
+        assert r.read_error_word() == 0
+    finally:
+        r.close()
