@@ -12,11 +12,15 @@
 //                    colinfo entry, and -- with the 2x2 neighbour columns
 //                    read by warp shuffles -- the level-1 ground minimum and
 //                    the state words of the level-5 cells (2^3 voxels) it
-//                    heads, plus a per-block solid voxel count;
-//   k_build_svo      one CTA per chunk: ground min-mip, the level-5 child
-//                    offsets (one exclusive scan), the cell states of
-//                    levels 4..0, their scans, node emission, ropes top-down,
-//                    macro bits.
+//                    heads, plus a per-block solid voxel count (a warp
+//                    whose columns all lie above the surface of a world
+//                    without decorations stores zero rows instead);
+//   k_build_svo      one CTA per chunk: ground min-mip, the cell states of
+//                    levels 4..0 and their scans, the level-5 child offsets
+//                    (16 rounds of one exclusive scan, voxel records written
+//                    as they go), node emission, ropes top-down (one thread
+//                    per node), macro bits; a chunk with no solid voxel
+//                    writes its lone air root and returns.
 //
 // Octree cells.  A cell of level l (0 = the chunk, 6 = a voxel) holds
 // 2^(6-l) voxels per side; its cells are numbered px + pz*S + py*S*S with
