@@ -553,7 +553,7 @@ def run_e2e(args, sc, dev, world_size):
         r = Renderer(sc.present[0], sc.present[1], sc.render_scale, node_capacity=sc.node_capacity,
                      chunk_capacity=cap, grid_capacity=cap, clip_levels=sc.clip_levels, clip_res=sc.clip_res,
                      flags=A.FLAG_GODRAY_MACRO_ALIAS, device=dev)
-        drv = FrameDriver(sc, device_renderer=r if device_streaming else None)
+        drv = FrameDriver(sc, device_renderer=r if device_streaming else None, mirror=False)
         ups = drv.initial_uploads()
         if not device_streaming:
             for ox in range(1, 4):

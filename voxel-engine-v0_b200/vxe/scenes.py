@@ -145,15 +145,16 @@ SCENES = {"config1": config1, "config2": config2, "config5": config5, "features"
 class FrameDriver:
     """Produces per-frame inputs (uploads, grid, clipmap patches, camera) for a scene."""
 
-    def __init__(self, scene: Scene, device_renderer=None):
+    def __init__(self, scene: Scene, device_renderer=None, mirror: bool = True):
         """`device_renderer`: keep the world on that renderer's device -- chunks
         built resident there, grid shifts by device slot moves (step() then
-        returns no uploads and writes the grid itself)."""
+        returns no uploads and writes the grid itself).  `mirror`: the world
+        keeps host copies of the node and rope arenas (World)."""
         self.scene = scene
         self.device = device_renderer
         self.last_shift = None  # (chunks built, slots moved) of the last device shift
         self.world = World(scene.spec, scene.grid_origin, scene.grid_dims, scene.node_capacity,
-                           chunk_capacity=int(np.prod(scene.grid_dims)))
+                           chunk_capacity=int(np.prod(scene.grid_dims)), mirror=mirror)
         self.clip = Clipmap(scene.spec, scene.clip_levels, scene.clip_res, 1.0) if scene.clip_levels else None
         self.prev_vp = None
         self.frame = 0

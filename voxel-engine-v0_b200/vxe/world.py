@@ -126,7 +126,12 @@ class World:
     """A resident grid of chunks around ``grid_origin`` with host mirrors."""
 
     def __init__(self, spec: WorldSpec, grid_origin, grid_dims, node_capacity: int, chunk_capacity: int | None = None,
-                 builder=None):
+                 builder=None, mirror: bool = True):
+        """`mirror`: keep host copies of the node and rope arenas (what the
+        CPU oracle and the host-side tests read); a streaming loop that only
+        uploads can leave them out -- the chunk cache keeps each chunk's
+        records for its uploads."""
+        self.mirror = mirror
         self.spec = spec
         self.grid_origin = tuple(int(v) for v in grid_origin)
         self.grid_dims = tuple(int(v) for v in grid_dims)
@@ -135,8 +140,8 @@ class World:
         self.grid_capacity = nx * ny * nz
         self.arena = NodeArena(node_capacity)
         self.node_capacity = node_capacity
-        self.nodes = np.zeros(node_capacity, dtype=A.NODE_DTYPE)
-        self.ropes = np.zeros(node_capacity, dtype=A.ROPES_DTYPE)
+        self.nodes = np.zeros(node_capacity if mirror else 0, dtype=A.NODE_DTYPE)
+        self.ropes = np.zeros(node_capacity if mirror else 0, dtype=A.ROPES_DTYPE)
         self.metas = np.zeros((self.chunk_capacity, 12), dtype=np.uint32)
         self.macro = np.zeros(self.chunk_capacity * A.MACRO_WORDS_PER_CHUNK, dtype=np.uint32)
         self.colinfo = np.zeros(self.chunk_capacity * A.COLINFO_WORDS_PER_CHUNK, dtype=np.uint32)
@@ -178,9 +183,10 @@ class World:
 
     def _write_slot(self, slot: int, key, node_base: int, data: ChunkData) -> np.ndarray:
         n = len(data.nodes)
-        # plain word copies (a structured-array assignment copies field by field)
-        self.nodes.view(np.uint32)[4 * node_base:4 * (node_base + n)] = data.nodes.view(np.uint32).reshape(-1)
-        self.ropes.view(np.uint32)[8 * node_base:8 * (node_base + n)] = data.ropes.view(np.uint32).reshape(-1)
+        if self.mirror:
+            # plain word copies (a structured-array assignment copies field by field)
+            self.nodes.view(np.uint32)[4 * node_base:4 * (node_base + n)] = data.nodes.view(np.uint32).reshape(-1)
+            self.ropes.view(np.uint32)[8 * node_base:8 * (node_base + n)] = data.ropes.view(np.uint32).reshape(-1)
         self.macro[slot * 16:(slot + 1) * 16] = data.macro
         self.colinfo[slot * 2048:(slot + 1) * 2048] = data.colinfo
         meta = self._meta_for(slot, key, node_base, data)
