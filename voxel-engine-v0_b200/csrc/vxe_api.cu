@@ -191,6 +191,8 @@ struct vxe_view {
 
 namespace {
 
+vxe_status stage_block_add(vxe_ctx* c);
+
 vxe_status fail(vxe_ctx* c, vxe_status st, const char* fmt, ...) {
   if (c) {
     char buf[512];
@@ -870,6 +872,12 @@ vxe_status vxe_create(const vxe_config* cfg, vxe_ctx** out) {
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device) == cudaSuccess && sms > 0)
       c->shade_wave = sms * 16;
+  }
+  // two pinned staging blocks up front: a stream's first chunk uploads need
+  // them, and allocating pinned memory then would hold the host for ms
+  for (int i = 0; i < 2; ++i) {
+    const vxe_status sb = stage_block_add(c);
+    if (sb != VXE_OK) return bail(sb);
   }
   *out = c;
   return VXE_OK;
