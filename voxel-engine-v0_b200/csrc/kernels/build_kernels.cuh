@@ -19,7 +19,7 @@
 //                    levels 4..0 and their scans, the level-5 child offsets
 //                    (16 rounds of one exclusive scan, voxel records written
 //                    as they go), node emission, ropes top-down (one thread
-//                    per node), macro bits; a chunk with no solid voxel
+//                    per node, its parent found from its key), macro bits; a chunk with no solid voxel
 //                    writes its lone air root and returns.
 //
 // Octree cells.  A cell of level l (0 = the chunk, 6 = a voxel) holds
@@ -607,7 +607,6 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       if (!cnt[k]) continue;
-      const uint32_t parent = level_node(st, kb, bases, 5, px0 + k, py, pz);
 #pragma unroll
       for (int ci = 0; ci < 8; ++ci) {
         if (!((sv[k] >> ci) & 1u)) continue;
@@ -619,7 +618,6 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
           n.material = (uint32_t)(rw[((ci >> 1) & 1) * 2 + ((ci >> 2) & 1)] >> (8 * (2 * k + (ci & 1)))) & 0xFFu;
           n.key = cell_key(cx, cy, cz, 6u);
           nodes[o] = n;
-          ropes[o]._pad0 = parent;  // until the rope pass writes the record
         }
         ++o;
       }
@@ -664,12 +662,10 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
         ckb[ci] = !has ? 0u : l == 4 ? kb5[c] : kb[low_off(l + 1) + c];
       }
       uint32_t o = bases[l + 1] + kb[low_off(l) + i];
-      const uint32_t parent = l == 0 ? 0u : level_node(st, kb, bases, l, px, py, pz);
 #pragma unroll
       for (int ci = 0; ci < 8; ++ci) {
         if (!((s >> ci) & 1u)) continue;
         const uint32_t cx = 2u * px + (ci & 1), cy = 2u * py + ((ci >> 1) & 1), cz = 2u * pz + ((ci >> 2) & 1);
-        ropes[o]._pad0 = parent;  // until the rope pass writes the record
         nodes[o++] = node_of(cs[ci], ckb[ci] + bases[l + 2], cell_key(cx, cy, cz, (uint32_t)l + 1u));
       }
     }
@@ -685,15 +681,18 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
   }
   __syncthreads();
   // One thread per node of level l's list (consecutive lanes, consecutive
-  // records): its parent (parked in the pad word at emission), the parent's
-  // ropes and children give its 6 ropes; siblings read the same parent and
-  // neighbour records, so those loads hit L1.
+  // records): its parent -- the node of the cell above it, found from its key
+  // and the shared level states -- and the parent's ropes and children give
+  // its 6 ropes; siblings read the same parent and neighbour records, so those
+  // loads hit L1.
   for (int l = 1; l <= 6; ++l) {
     const uint32_t lo = bases[l], hi = bases[l] + K[l];
     for (uint32_t k = lo + t; k < hi; k += SVO_THREADS) {
-      const uint32_t p = ropes[k]._pad0;
       const uint32_t key = nodes[k].key;
       const uint32_t hx = key & 1u, hy = (key >> 6) & 1u, hz = (key >> 12) & 1u;
+      const uint32_t p = l == 1 ? 0u
+                                : level_node(st, kb, bases, l - 1, (key & 63u) >> 1, ((key >> 6) & 63u) >> 1,
+                                             ((key >> 12) & 63u) >> 1);
       const uint32_t ci = hx | (hy << 1) | (hz << 2);
       const vxe_node pn = nodes[p];
       const vxe_node_ropes pr = ropes[p];
