@@ -56,6 +56,10 @@ constexpr uint32_t ST_LEAF = 1u << 16;
 constexpr uint32_t ST_FULL = 1u << 17;
 constexpr int SVO_THREADS = 512;
 constexpr int SVO_WARPS = SVO_THREADS / 32;
+// Voxel records of one level-5 round staged in (dynamic) shared memory so
+// they leave as contiguous stores; a round with more writes them directly.
+constexpr uint32_t kStageNodes = 2048u;
+constexpr size_t kStageBytes = kStageNodes * 16u;
 // Shared state words of levels 4..0 (4096 + 512 + 64 + 8 + 1 cells).
 constexpr uint32_t kLowCells = 4681u;
 __host__ __device__ constexpr uint32_t low_off(int l) {
@@ -442,6 +446,7 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
   __shared__ uint32_t ws[SVO_WARPS];
   __shared__ uint32_t K[8];  // K[l]: entries of level l's node list (l = 1..6)
   __shared__ uint32_t bases[8];
+  extern __shared__ uint4 stage[];  // kStageNodes voxel records of one level-5 round
 
   const uint32_t chunk = blockIdx.x, t = threadIdx.x;
   if (chunk >= B.n) return;
@@ -594,8 +599,10 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
       sum += cnt[k];
     }
     uint32_t total;
+    const uint32_t round0 = carry;
     const uint32_t off0 = carry + block_excl_scan(sum, ws, &total);
     carry += total;
+    const bool staged = total <= kStageNodes;  // block-uniform
     uint32_t off = off0;
     uint4 kv;
     kv.x = off; off += cnt[0];
@@ -611,16 +618,20 @@ __global__ void __launch_bounds__(SVO_THREADS, 2) k_build_svo(const __grid_const
       for (int ci = 0; ci < 8; ++ci) {
         if (!((sv[k] >> ci) & 1u)) continue;
         const uint32_t cx = 2u * (px0 + k) + (ci & 1), cy = 2u * py + ((ci >> 1) & 1), cz = 2u * pz + ((ci >> 2) & 1);
-        if (o < cap) {
-          vxe_node n;
-          n.child_base = kInvalid;
-          n.child_mask = 0u;
-          n.material = (uint32_t)(rw[((ci >> 1) & 1) * 2 + ((ci >> 2) & 1)] >> (8 * (2 * k + (ci & 1)))) & 0xFFu;
-          n.key = cell_key(cx, cy, cz, 6u);
-          nodes[o] = n;
-        }
+        const uint32_t mat_ci =
+            (uint32_t)(rw[((ci >> 1) & 1) * 2 + ((ci >> 2) & 1)] >> (8 * (2 * k + (ci & 1)))) & 0xFFu;
+        const uint4 rec = make_uint4(kInvalid, 0u, mat_ci, cell_key(cx, cy, cz, 6u));
+        if (staged) stage[o - bases[6] - round0] = rec;
+        else if (o < cap) *reinterpret_cast<uint4*>(nodes + o) = rec;
         ++o;
       }
+    }
+    if (staged) {  // the round's records leave shared memory as one contiguous run
+      __syncthreads();
+      const uint32_t first = bases[6] + round0;
+      for (uint32_t i = t; i < total; i += SVO_THREADS)
+        if (first + i < cap) *reinterpret_cast<uint4*>(nodes + first + i) = stage[i];
+      // the next round's scan barriers order these reads before its stores
     }
   }
   if (t == 0) {

@@ -1563,7 +1563,8 @@ vxe_status build_launch(vxe_ctx* c, vxe::build::BuildArgs& B, uint32_t n) {
   vb::k_build_columns<<<n * 16u, 256, 0, st>>>(B);
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->build_ev[1], st));
-  vb::k_build_svo<<<n, vb::SVO_THREADS, 0, st>>>(B);
+  CK(cudaFuncSetAttribute(vb::k_build_svo, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vb::kStageBytes));
+  vb::k_build_svo<<<n, vb::SVO_THREADS, vb::kStageBytes, st>>>(B);
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->build_ev[2], st));
   c->build_timed = true;
