@@ -104,42 +104,6 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def build_world(present, resident_all: bool):
-    from vxe import scenes
-    from vxe.world import World
-
-    sc = scenes.config2(present=present)
-    # Every chunk the 64-frame path visits: grid origins x = 0..3 -> chunk x 0..18.
-    dims = (sc.grid_dims[0] + 3, sc.grid_dims[1], sc.grid_dims[2]) if resident_all else sc.grid_dims
-    world = World(sc.spec, sc.grid_origin, dims, sc.node_capacity, chunk_capacity=int(np.prod(dims)))
-    return sc, world
-
-
-def grid_window(world, ox: int, dims):
-    """chunk_grid for a 16x4x16 window at origin x = ox over a world holding more slots."""
-    nx, ny, nz = dims
-    g = np.full(nx * ny * nz, 0xFFFFFFFF, dtype=np.uint32)
-    for iz in range(nz):
-        for iy in range(ny):
-            for ix in range(nx):
-                s = world.key_to_slot.get((ox + ix, iy, iz))
-                if s is not None:
-                    g[(iz * ny + iy) * nx + ix] = s
-    return g
-
-
-def camera_for(sc, f, ox, prev_vp, chunk_count):
-    from vxe.world import build_camera
-
-    pos, yaw, pitch = sc.path(f)
-    cam = build_camera(pos, yaw, pitch, sc.present, sc.internal, frame_index=f + 1, time_s=f / 60.0, world=None,
-                       jitter=True, prev_view_proj=prev_vp)
-    cam.chunk_count = chunk_count
-    cam.grid_origin_chunk[0], cam.grid_origin_chunk[1], cam.grid_origin_chunk[2] = ox, 0, 0
-    cam.grid_dims[0], cam.grid_dims[1], cam.grid_dims[2] = sc.grid_dims
-    return cam, pos
-
-
 def run_vxe(args, rank: int, world_size: int):
     import torch
 
@@ -150,32 +114,20 @@ def run_vxe(args, rank: int, world_size: int):
     dev = rank if torch.cuda.device_count() > rank else 0
     torch.cuda.set_device(dev)
     present = tuple(int(v) for v in args.present.split("x"))
-    sc, world = build_world(present, resident_all=True)
-    ups = world.populate()
+    from vxe.scenes import ResidentPathDriver, config2
+
+    sc = config2(present=present)
+    drv = ResidentPathDriver(sc)
+    ups = drv.initial_uploads()
+    world = drv.world
     r = Renderer(sc.present[0], sc.present[1], sc.render_scale, node_capacity=world.node_capacity,
                  chunk_capacity=world.chunk_capacity, grid_capacity=int(np.prod(sc.grid_dims)),
                  clip_levels=sc.clip_levels, clip_res=sc.clip_res, flags=A.FLAG_GODRAY_MACRO_ALIAS, device=dev)
     r.apply_chunk_uploads(ups)
-    clip = Clipmap(sc.spec, sc.clip_levels, sc.clip_res, 1.0)
     rays_per_frame = sc.internal[0] * sc.internal[1]
-    prev_vp = None
-    last_ox = None
-
-    def frame_inputs(step):
-        nonlocal prev_vp, last_ox
-        f = step % 64
-        ox = f // 16
-        cam, pos = camera_for(sc, f, ox, prev_vp, world.chunk_count)
-        prev_vp = cam.view_proj
-        params, patches = clip.update(float(pos[0]), float(pos[2]))
-        grid = None
-        if ox != last_ox:
-            grid = grid_window(world, ox, sc.grid_dims)
-            last_ox = ox
-        return cam, params, patches, grid
 
     def submit(step):
-        cam, params, patches, grid = frame_inputs(step)
+        cam, params, patches, grid = drv.inputs(step)
         if grid is not None:
             r.write_chunk_grid(grid)
         r.write_clipmap_updates(params, patches)
@@ -678,7 +630,9 @@ def device_streaming_line(e2e: dict, steps: int, n: int):
 
 
 def cpu_sample(seconds: float, present, threads: int):
-    """Times the oracle (scalar C++ restatement of the WGSL) on full frames."""
+    """Times the oracle (scalar C++ restatement of the WGSL) on full frames of
+    the path.  The frame inputs (camera, clipmap patches, streamed chunks) are
+    produced between the timed renders; only the passes are timed."""
     from oracle import oracle as O
     from vxe.scenes import FrameDriver, config2
 
@@ -688,15 +642,17 @@ def cpu_sample(seconds: float, present, threads: int):
     runner = O.OracleFrameRunner(drv.world, sc.internal, sc.present, drv.clip.tex, sc.clip_res)
     frames = 0
     ctr = None
-    t0 = time.perf_counter()
     elapsed = 0.0
     while elapsed < seconds or frames == 0:
+        if drv.frame >= 64:
+            drv.frame = 0
         uploads, gc, clip, cam = drv.step()
+        t0 = time.perf_counter()
         runner.render(cam, clip[0], threads=threads)
+        elapsed += time.perf_counter() - t0
         if ctr is None:
             ctr = (runner.primary_ctr.as_dict(), runner.godray_ctr.as_dict(), runner.trace_ctr.as_dict())
         frames += 1
-        elapsed = time.perf_counter() - t0
     rays = frames * sc.internal[0] * sc.internal[1]
     return {"rays": rays, "seconds": elapsed, "frames": frames, "counters": ctr}
 
@@ -783,17 +739,14 @@ def main():
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": n, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded value-noise world)",
-        "config": {"workload": WORKLOAD, "present": list(map(int, args.present.split("x"))),
-                   "internal": res["internal"],
-                   "parallelism": "replicas" if n > 1 else "single",
-                   "l2": "flushed between steps (512 MiB memset), per-step CUDA events",
-                   "frame_ms": {"tiles": round(statistics.mean(res["tiles_ms"]), 4),
-                                "primary": round(statistics.mean(res["primary_ms"]), 4),
-                                "primary_trace": round(statistics.mean(res["trace_ms"]), 4),
-                                "k_primary_trace": round(statistics.mean(res["walk_ms"]), 4),
-                                "grass_cells": round(statistics.mean(res["grass_ms"]), 4),
-                                "godray": round(statistics.mean(res["godray_ms"]), 4),
-                                "composite": round(statistics.mean(res["composite_ms"]), 4)}},
+        "config": bench_config(tuple(map(int, args.present.split("x"))), res["internal"], n),
+        "frame_ms": {"tiles": round(statistics.mean(res["tiles_ms"]), 4),
+                     "primary": round(statistics.mean(res["primary_ms"]), 4),
+                     "primary_trace": round(statistics.mean(res["trace_ms"]), 4),
+                     "k_primary_trace": round(statistics.mean(res["walk_ms"]), 4),
+                     "grass_cells": round(statistics.mean(res["grass_ms"]), 4),
+                     "godray": round(statistics.mean(res["godray_ms"]), 4),
+                     "composite": round(statistics.mean(res["composite_ms"]), 4)},
         "e2e": {"value": round(e2e_val, 3), "unit": UNIT, "h2d_bytes_per_step": res["e2e"]["h2d_bytes_per_step"],
                 "d2h_bytes_per_step": res["e2e"]["d2h_bytes_per_step"],
                 "frame_ms": round(e2e_s * 1e3 / args.steps, 3),
@@ -852,8 +805,18 @@ def main():
 
 
 def main_reference(args, rank, world_size):
+    """The reference arm: the reference's passes as the CPU restatement of its
+    WGSL (oracle/) on all host cores, one full frame of the same workload per
+    step.  Its frame inputs come from a host-only build of the producers
+    (oracle/libref_producer.so), so this process maps no CUDA library of this
+    repository; the producer work between frames is not timed."""
     if rank != 0:
         return
+    from vxe import _abi as A
+
+    import vxe_build
+
+    A.use_host_library(vxe_build.build_ref_producer())
     threads = os.cpu_count() or 1
     present = tuple(int(v) for v in args.present.split("x"))
     from oracle import oracle as O
@@ -868,28 +831,35 @@ def main_reference(args, rank, world_size):
         if drv.frame >= 64:
             drv.frame = 0
         _, _, clip, cam = drv.step()
+        t0 = time.perf_counter()
         runner.render(cam, clip[0], threads=threads)
+        return time.perf_counter() - t0
 
     for _ in range(args.warmup):
         step()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        step()
-    dt = time.perf_counter() - t0
+    dt = sum(step() for _ in range(args.steps))
     rays = sc.internal[0] * sc.internal[1] * args.steps
     v = rays / dt / 1e6
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": 1,
+        "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": max(1, world_size),
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded value-noise world)",
-        "config": {"workload": WORKLOAD, "present": list(present), "internal": list(sc.internal)},
+        "config": bench_config(present, sc.internal, max(1, world_size)),
         "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": "full frames of the same workload, one per step"},
+                         "sample": "full frames of the same workload, one per step (path frames "
+                                   f"{args.warmup}..{args.warmup + args.steps - 1}); passes timed, producers not"},
         "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "reference is Rust+WGSL; no Rust toolchain or graphics stack here, so this arm runs the C++ "
                 "scalar restatement of its WGSL (oracle/) on the host cores",
     }))
+
+
+def bench_config(present, internal, n):
+    """The `config` object of both arms' lines (the same workload keys)."""
+    return {"workload": WORKLOAD, "present": list(present), "internal": list(internal),
+            "parallelism": "replicas" if n > 1 else "single",
+            "l2": "GPU arm: flushed between steps (512 MiB memset), per-step CUDA events"}
 
 
 if __name__ == "__main__":

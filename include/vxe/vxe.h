@@ -398,6 +398,51 @@ vxe_status vxe_write_image(vxe_ctx* ctx, vxe_image img, const void* host, size_t
 /* Device error word (bounds checks / bounded waits); cleared on read. */
 vxe_status vxe_read_error_word(vxe_ctx* ctx, uint32_t* word);
 
+/* Primary-pass work counters (ray_main.wgsl:32-74, binding 17
+ * `profile_counts`): while the camera's profile_flags has bit 0 set, each
+ * frame of the context adds, per pixel, what main_primary's profile_inc /
+ * profile_add calls add -- VOXEL: the tile's candidate count per voxel trace
+ * phase run; GRASS: 1 per grass-slab refinement that hit; HDR: 1 per
+ * heightfield shade, 2 per voxel shade; FOG: fog_profile_weight(t) per shaded
+ * pixel; SHADOW: 2 per fresh sun shadow, 1 per reused one.  The counts
+ * accumulate over frames until reset.
+ *   vxe_reset_profile_counts  Renderer::reset_primary_profile_counts
+ *                             (render/state/mod.rs:448-455); ordered after the
+ *                             frames already enqueued
+ *   vxe_read_profile_counts   Renderer::encode_primary_profile_readback +
+ *                             read_primary_profile_counts_blocking
+ *                             (render/state/mod.rs:457-491); waits for the
+ *                             context's frames */
+#define VXE_PROFILE_COUNT 5u
+enum { VXE_PROFILE_VOXEL = 0, VXE_PROFILE_GRASS = 1, VXE_PROFILE_HDR = 2, VXE_PROFILE_FOG = 3,
+       VXE_PROFILE_SHADOW = 4 };
+vxe_status vxe_reset_profile_counts(vxe_ctx* ctx);
+vxe_status vxe_read_profile_counts(vxe_ctx* ctx, uint32_t counts[VXE_PROFILE_COUNT]);
+
+/* Wavefront record limits (no reference counterpart).  The trace stage
+ * stores every grass-column probe the voxel walk meets and every grass slab a
+ * probe's column DDA finds, and marches them in kernels of their own; a pixel
+ * whose records do not all fit walks again with the probes inline (the
+ * reference's order), with the same result.  These cap the records stored
+ * per frame or batch below the buffers' sizes (0 = the buffer size): a knob
+ * for tests of the re-walk path and for runs with smaller buffers. */
+vxe_status vxe_set_record_limits(vxe_ctx* ctx, uint32_t probe_records, uint32_t slab_tasks);
+
+/* Work counts of the context's last frame (no reference counterpart; waits
+ * for the frame).  Wavefront schedule only: zeros with
+ * VXE_FLAG_PRIMARY_MEGAKERNEL. */
+typedef struct vxe_frame_stats {
+  uint32_t voxel_pixels;    /* pixels shaded as voxel hits */
+  uint32_t far_pixels;      /* pixels shaded as heightfield or sky */
+  uint32_t probes;          /* grass-column probes the walk met (stored or not) */
+  uint32_t pending_pixels;  /* pixels whose walk met probes */
+  uint32_t slab_tasks;      /* grass slabs found by the probes' column DDAs */
+  uint32_t slab_hits;       /* slabs whose march hit */
+  uint32_t rewalk_pixels;   /* pending pixels walked again with inline probes */
+  uint32_t _pad;
+} vxe_frame_stats;
+vxe_status vxe_get_frame_stats(vxe_ctx* ctx, vxe_frame_stats* out);
+
 /* Scene buffers the caller already holds on the device, in the layouts of the
  * structs above (used by vxe_trace_primary_hits_noalloc). */
 typedef struct vxe_scene_view {
@@ -429,8 +474,11 @@ typedef struct vxe_scene_view {
  *     (w*h records, w,h = cam->render_present_px[0..1]) are device pointers.
  *   stream: a cudaStream_t (NULL = legacy default stream).  The call returns
  *     after the work on `stream` has finished.
- * The first call on a device resolves the scratch address on that device and
- * should come before any stream capture.  Calls share the one scratch array,
+ * The first call on a device resolves the scratch address on that device (so
+ * does the first call after the device's context was re-created, e.g. after
+ * cudaDeviceReset) and should come before any stream capture.  A CUDA error
+ * already pending on the calling thread is reported as VXE_ERR_DEVICE before
+ * anything is launched, and left pending.  Calls share the one scratch array,
  * so calls that overlap on the GPU (different streams, threads or devices
  * sharing a context) race; serialise them. */
 #define VXE_NOALLOC_MAX_TILES 36864u

@@ -46,7 +46,7 @@ class FrameIO(C.Structure):
         (n, C.c_void_p) for n in ("primary_hist_in", "shadow_in", "local_hist_in", "godray_hist_in",
                                   "output_hist_in", "color", "depth", "local", "primary_hist_out", "shadow_out",
                                   "local_hist_out", "godray_out", "output_pre_taa", "output", "output_hist_out",
-                                  "hits")]
+                                  "hits", "profile")]
 
 
 _lib = None
@@ -101,17 +101,24 @@ class OracleFrameRunner:
         self.color, self.depth, self.local = z4(n), np.zeros(n, dtype=np.float32), z4(n)
         self.pre_taa, self.output = z4(p), z4(p)
         self.hits = np.zeros(n, dtype=A.HIT_DTYPE)
+        # profile_counts (VOXEL, GRASS, HDR, FOG, SHADOW), accumulated over
+        # frames rendered with cam.profile_flags & 1 until reset
+        self.profile = np.zeros(5, dtype=np.uint32)
         self.ping = 0
         self.primary_ctr = OraCounters()
         self.godray_ctr = OraCounters()
 
-    def scene(self, cam, clip_params) -> OraScene:
+    def scene(self, cam, clip_params, grid=None) -> OraScene:
+        """`grid`: a chunk grid to read instead of the world's own (a window
+        of the camera's grid dims over a world holding more slots)."""
         w = self.world
+        g = w.grid if grid is None else np.ascontiguousarray(grid, dtype=np.uint32)
+        self._grid_ref = g
         s = OraScene()
         s.cam = C.addressof(cam)
         s.chunks, s.chunks_n = w.metas.ctypes.data, w.metas.shape[0]
         s.nodes, s.nodes_n = w.nodes.ctypes.data, len(w.nodes)
-        s.grid, s.grid_n = w.grid.ctypes.data, len(w.grid)
+        s.grid, s.grid_n = g.ctypes.data, len(g)
         s.macro_words, s.macro_n = w.macro.ctypes.data, len(w.macro)
         s.ropes, s.ropes_n = w.ropes.ctypes.data, len(w.ropes)
         s.colinfo, s.colinfo_n = w.colinfo.ctypes.data, len(w.colinfo)
@@ -123,7 +130,7 @@ class OracleFrameRunner:
         s.godray_macro_alias = 1 if self.godray_alias else 0
         return s
 
-    def render(self, cam, clip_params, threads: int | None = None) -> None:
+    def render(self, cam, clip_params, threads: int | None = None, grid=None) -> None:
         p, q = self.ping, 1 - self.ping
         io = FrameIO(self.iw, self.ih, self.pw, self.ph)
         io.primary_hist_in = self.hist[p].ctypes.data
@@ -139,7 +146,8 @@ class OracleFrameRunner:
         io.output_pre_taa, io.output = self.pre_taa.ctypes.data, self.output.ctypes.data
         io.output_hist_out = self.ohist[q].ctypes.data
         io.hits = self.hits.ctypes.data
-        sc = self.scene(cam, clip_params)
+        io.profile = self.profile.ctypes.data
+        sc = self.scene(cam, clip_params, grid)
         self.primary_ctr = OraCounters()
         self.godray_ctr = OraCounters()
         self.trace_ctr = OraCounters()  # the voxel trace phase of the primary pass

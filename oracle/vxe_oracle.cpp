@@ -2206,7 +2206,21 @@ struct FrameIO {
   float* output;               // pw*ph*4
   float* output_hist_out;      // pw*ph*4
   vxe_hit* hits;               // iw*ih (optional)
+  // profile_counts (ray_main.wgsl:32-74): VOXEL, GRASS, HDR, FOG, SHADOW,
+  // added to when cam.profile_flags & 1 (optional)
+  uint32_t* profile;
 };
+
+// profile_inc / profile_add (ray_main.wgsl:64-74)
+enum : uint32_t { PROFILE_VOXEL = 0, PROFILE_GRASS = 1, PROFILE_HDR = 2, PROFILE_FOG = 3, PROFILE_SHADOW = 4 };
+inline void profile_add(const Scene& s, const FrameIO& io, uint32_t idx, uint32_t v) {
+  if (io.profile && (s.cam->profile_flags & 1u) != 0u) __atomic_fetch_add(&io.profile[idx], v, __ATOMIC_RELAXED);
+}
+// fog_profile_weight (ray_main.wgsl:89-93)
+inline uint32_t fog_profile_weight(float t_scene) {
+  const float fog_norm = clampf(t_scene / FOG_MAX_DIST, 0.0f, 1.0f);
+  return std::max(1u, to_u32(fog_norm * 256.0f));
+}
 
 inline v4 load4(const float* img, uint32_t w, int32_t x, int32_t y) {
   const float* p = img + ((size_t)y * w + (uint32_t)x) * 4;
@@ -2306,11 +2320,18 @@ void primary_pixel(const Scene& s, const FrameIO& io, const TileList& tl, uint32
         const v3 gb = V3(cell.bmin_m.x, hp.y - vs, cell.bmin_m.z);
         const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, hf.t, gb, cell.id_vox, vs, s.cam->voxel_params[1],
                                                s.cam->voxel_params[2]);
-        if (gh.hit) { hf.t = gh.t; hf.n = gh.n; }
+        if (gh.hit) {
+          hf.t = gh.t;
+          hf.n = gh.n;
+          profile_add(s, io, PROFILE_GRASS, 1u);
+        }
       }
+      // shade_heightfield (ray_main.wgsl:100-114)
+      profile_add(s, io, PROFILE_HDR, 1u);
       const v3 surface = shade_clip_hit(s, ro, rd, hf, sky_up);
       const float t_scene = fmin_(hf.t, FOG_MAX_DIST);
       const v3 col = apply_fog(s, surface, ro, rd, t_scene, sky_bg(rd));
+      profile_add(s, io, PROFILE_FOG, fog_profile_weight(t_scene));
       t_store = t_scene;
       HitGeom g = miss_hitgeom();
       g.hit = 1; g.t = hf.t; g.n = hf.n; g.mat = hf.mat;
@@ -2323,7 +2344,10 @@ void primary_pixel(const Scene& s, const FrameIO& io, const TileList& tl, uint32
   };
 
   if (s.cam->chunk_count == 0u) {
-    heightfield_or_sky();
+    // no voxel chunks (ray_main.wgsl:219-231): the heightfield is traced but
+    // not used; the pixel is sky
+    const v3 sky = sky_color(s, rd);
+    write_common(sky, FOG_MAX_DIST, f_bits(t_store), 0u, 0u, 0u);
   } else {
     float t_hist = 0.0f;
     bool hist_valid = false;
@@ -2366,12 +2390,15 @@ void primary_pixel(const Scene& s, const FrameIO& io, const TileList& tl, uint32
     if (has_tc) {
       bool done = false;
       if (hist_valid) {
+        profile_add(s, io, PROFILE_VOXEL, std::max(1u, tile_count));
         const VoxTraceResult h = trace_scene_voxels_candidates(s, tl, ro, rd, t_start, t_end, hak != INVALID, hac,
                                                                hak, tile_count);
         if (h.best.hit != 0u) { vt = h; done = true; }
       }
-      if (!done)
+      if (!done) {
+        profile_add(s, io, PROFILE_VOXEL, std::max(1u, tile_count));
         vt = trace_scene_voxels_candidates(s, tl, ro, rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID, tile_count);
+      }
     }
     if (s.trace_ctr) {
       Counters& t = *s.trace_ctr;
@@ -2397,10 +2424,15 @@ void primary_pixel(const Scene& s, const FrameIO& io, const TileList& tl, uint32
         const GrassCell cell = pick_grass_cell_in_chunk_with_bias(hp, rd, best.root_bmin, ov, vs, csv);
         const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, best.t, cell.bmin_m, cell.id_vox, vs,
                                                s.cam->voxel_params[1], s.cam->voxel_params[2]);
-        if (gh.hit) { best.t = gh.t; best.n = gh.n; }
+        if (gh.hit) {
+          best.t = gh.t;
+          best.n = gh.n;
+          profile_add(s, io, PROFILE_GRASS, 1u);
+        }
       }
       const v3 hp = ro + rd * best.t;
       const v3 hps = hp + best.n * (0.75f * vs);
+      profile_add(s, io, PROFILE_SHADOW, (seed & SHADOW_SUBSAMPLE_MASK) == 0u ? 2u : 1u);
       if ((seed & SHADOW_SUBSAMPLE_MASK) == 0u) {
         float sh = io.shadow_in[pix];
         const v2 uvp = prev_uv_from_world(s, hp);
@@ -2423,8 +2455,10 @@ void primary_pixel(const Scene& s, const FrameIO& io, const TileList& tl, uint32
         local_out = gather_voxel_lights(s, hpl, best.n, best.root_bmin) * alb;
         local_w = 1.0f;
       }
+      profile_add(s, io, PROFILE_HDR, 2u);
       const float t_scene = fmin_(best.t, FOG_MAX_DIST);
       const v3 col = apply_fog(s, base_hdr, ro, rd, t_scene, sky_bg(rd));
+      profile_add(s, io, PROFILE_FOG, fog_profile_weight(t_scene));
       t_store = t_scene;
       uint32_t pxy = 0, pz = 0, ak = 0;
       if (vt.anchor_valid) {

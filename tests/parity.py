@@ -76,15 +76,25 @@ def make_renderer(scene, world, flags=A.FLAG_GODRAY_MACRO_ALIAS | A.FLAG_HIT_REC
 
 
 def run_parity(scene, frames: int, threads: int | None = None, godray_alias: bool = True, on_frame=None,
-               extra_flags: int = 0, graph: bool = False):
-    """Renders `frames` frames on both sides; returns a list of per-frame mismatch dicts."""
-    drv = FrameDriver(scene)
+               extra_flags: int = 0, graph: bool = False, flags: int | None = None, start_frame: int = 0,
+               cam_hook=None, setup=None):
+    """Renders `frames` frames on both sides; returns a list of per-frame mismatch dicts.
+
+    `flags`: the context flags (default: hit records + debug intermediates +
+    the godray alias, | extra_flags).  `start_frame`: first path frame.
+    `cam_hook(cam)`: edits each frame's camera before both sides see it.
+    `setup(renderer)`: called once after the world upload."""
+    drv = FrameDriver(scene, start_frame=start_frame)
     ups = drv.initial_uploads()
-    flags = A.FLAG_HIT_RECORDS | A.FLAG_DEBUG_INTERMEDIATES | (A.FLAG_GODRAY_MACRO_ALIAS if godray_alias else 0)
-    flags |= extra_flags
+    if flags is None:
+        flags = A.FLAG_HIT_RECORDS | A.FLAG_DEBUG_INTERMEDIATES | (A.FLAG_GODRAY_MACRO_ALIAS if godray_alias else 0)
+        flags |= extra_flags
+    godray_alias = bool(flags & A.FLAG_GODRAY_MACRO_ALIAS)
     r = make_renderer(scene, drv.world, flags)
     try:
         r.upload_world(drv.world, ups)
+        if setup is not None:
+            setup(r)
         ora = O.OracleFrameRunner(drv.world, scene.internal, scene.present,
                                   drv.clip.tex if drv.clip else None, scene.clip_res, godray_alias=godray_alias)
         results = []
@@ -100,6 +110,8 @@ def run_parity(scene, frames: int, threads: int | None = None, godray_alias: boo
             else:
                 params = drv.empty_clip()
                 r.write_clipmap_updates(params, [])
+            if cam_hook is not None:
+                cam_hook(cam)
             r.write_camera(cam)
             if graph:
                 r.render_frame_graph()
@@ -111,7 +123,42 @@ def run_parity(scene, frames: int, threads: int | None = None, godray_alias: boo
             bad = compare_frame(g, o)
             results.append(bad)
             if on_frame:
-                on_frame(g, o, bad)
+                on_frame(g, o, bad, r, ora)
+        assert r.read_error_word() == 0
+        return results
+    finally:
+        r.close()
+
+
+def run_resident_parity(scene, frames, flags=A.FLAG_GODRAY_MACRO_ALIAS, threads=None):
+    """The device-resident frames of a shifting path (vxe.scenes.ResidentPathDriver:
+    every chunk the path visits uploaded once, grid windows rewritten at the
+    shifts) for the path frames in `frames`, on both sides; per-frame mismatch
+    dicts."""
+    from vxe.scenes import ResidentPathDriver
+
+    drv = ResidentPathDriver(scene)
+    ups = drv.initial_uploads()
+    w = drv.world
+    r = Renderer(scene.present[0], scene.present[1], scene.render_scale, node_capacity=w.node_capacity,
+                 chunk_capacity=w.chunk_capacity, grid_capacity=int(np.prod(scene.grid_dims)),
+                 clip_levels=scene.clip_levels, clip_res=scene.clip_res, flags=flags)
+    try:
+        r.apply_chunk_uploads(ups)
+        ora = O.OracleFrameRunner(w, scene.internal, scene.present, drv.clip.tex, scene.clip_res,
+                                  godray_alias=bool(flags & A.FLAG_GODRAY_MACRO_ALIAS))
+        grid = None
+        results = []
+        for f in frames:
+            cam, params, patches, g = drv.inputs(f)
+            if g is not None:
+                grid = g
+                r.write_chunk_grid(grid)
+            r.write_clipmap_updates(params, patches)
+            r.write_camera(cam)
+            r.encode_compute()
+            ora.render(cam, params, threads=threads, grid=grid)
+            results.append(compare_frame(read_gpu_frame(r), ora.outputs()))
         assert r.read_error_word() == 0
         return results
     finally:

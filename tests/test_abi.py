@@ -53,3 +53,43 @@ def test_camera_packing_is_consistent():
     c /= np.linalg.norm(c)
     f = np.array([np.sin(0.3) * np.cos(-0.2), np.sin(-0.2), np.cos(0.3) * np.cos(-0.2)])
     assert np.allclose(c, f, atol=1e-5)
+
+
+def test_noalloc_argument_checks_return_before_any_device_call():
+    # vxe_trace_primary_hits_noalloc validates its arguments before touching
+    # the device (these calls need no GPU; the pointers are never read).
+    lib = A.lib()
+    fake = 256
+    sv = A.SceneView(fake, fake, 100, fake, fake, fake, 4, 8, fake, None, 0, 0)
+    clip = A.ClipmapGpu()
+    cam = A.CameraGpu()
+    cam.chunk_size = 64
+    cam.chunk_count = 2
+    cam.render_present_px[0], cam.render_present_px[1] = 64, 32
+    cam.grid_dims[0], cam.grid_dims[1], cam.grid_dims[2] = 2, 2, 2
+
+    def call(s=sv, c=cam, cl=clip, hits=fake):
+        return lib.vxe_trace_primary_hits_noalloc(C.byref(s), C.byref(c), C.byref(cl), hits, None)
+
+    def variant(**kw):
+        c = A.CameraGpu()
+        C.memmove(C.byref(c), C.byref(cam), C.sizeof(c))
+        for k, v in kw.items():
+            if isinstance(v, tuple):
+                getattr(c, k)[:len(v)] = list(v)
+            else:
+                setattr(c, k, v)
+        return c
+
+    assert call(hits=None) == 1                                   # no output buffer
+    assert call(c=variant(chunk_size=32)) == 1                    # colinfo layout needs 64
+    assert call(c=variant(render_present_px=(0, 32))) == 1        # empty image
+    assert call(c=variant(render_present_px=(4096, 2304))) == 2   # beyond VXE_NOALLOC_MAX_TILES
+    assert call(c=variant(grid_dims=(4, 2, 2))) == 2              # more cells than the grid holds
+    assert call(c=variant(chunk_count=5)) == 2                    # more chunks than the metas hold
+    lv = A.ClipmapGpu()
+    lv.levels, lv.res = 2, 256
+    assert call(cl=lv) == 1                                       # clipmap levels without a texture
+    nul = A.SceneView(*[getattr(sv, f) for f, _ in A.SceneView._fields_])
+    nul.nodes = None
+    assert call(s=nul) == 1                                       # missing scene buffer

@@ -11,6 +11,11 @@ from vxe.scenes import FrameDriver, config2
 pytestmark = pytest.mark.gpu
 
 
+# what the module's world fixture wrote besides the world: the clipmap (host
+# mirror, uniform, resolution) and the context camera
+_WRITTEN = {}
+
+
 @pytest.fixture(scope="module")
 def world_renderer():
     import torch
@@ -26,6 +31,7 @@ def world_renderer():
     r.upload_world(w, ups)
     r.write_clipmap_updates(*clip)
     r.write_camera(cam)
+    _WRITTEN.update(clip=(drv.clip, clip[0], sc.clip_res), camera=cam)
     yield torch, w, r
     r.close()
 
@@ -85,3 +91,30 @@ def test_viewport_requests_match_cold_frames(world_renderer):
         want = r.read_image(A.IMG_HITS)
         got = _records(out)
         assert got.tobytes() == want.tobytes()
+
+
+def test_config3_batch_sample_matches_oracle(world_renderer):
+    # A sample of the config-3 mix (one viewport, four incoherent query
+    # batches, seeded) traced in one persistent batch, checked against the
+    # oracle directly: queries against its trace_rays, the viewport against
+    # the hit records of its cold frame (no history hint).
+    from oracle import oracle as O
+
+    torch, world, r = world_renderer
+    clipmap, clip_params, clip_res = _WRITTEN["clip"]
+    b = make_batch(world, torch, seed=5, n_viewports=1, n_queries=4, vp_range=((200, 480), (120, 270)),
+                   q_range=(2e3, 5e4))
+    r.submit_batch(b.requests, (8, 4), 1, A.BATCH_PERSISTENT)
+    for k, req, out, inp in zip(b.kinds, b.requests, b.outputs, _query_inputs(b)):
+        got = _records(out)
+        if k == "q":
+            o, d = inp
+            ref, _ = O.trace_rays(world, _WRITTEN["camera"], o, d, 120.0)
+            assert got.tobytes() == ref.tobytes()
+            assert (got["face"] != 255).mean() > 0.05
+        else:
+            w, h = req.width, req.height
+            ora = O.OracleFrameRunner(world, (w, h), (w, h), clipmap.tex, clip_res)
+            ora.render(req.camera, clip_params)
+            assert got.tobytes() == ora.hits.tobytes()
+            assert (got["face"] != 255).mean() > 0.3

@@ -155,3 +155,175 @@ def test_config5_large_world_bit_exact():
     sc = scenes.config5(present=(320, 180))
     res = run_parity(sc, frames=2)
     assert all(r == {} for r in res), res
+
+
+# ---------------------------------------------------------------------------
+# The bench's own configurations, at full size
+# ---------------------------------------------------------------------------
+def test_config2_1080p_streamed_frames_14_to_17_bit_exact():
+    # The end-to-end workload at its size: 1920x1080 present / 960x540
+    # internal, the context flags of the bench (godray alias only), path
+    # frames 14..17 with the frame-16 grid shift and its chunk uploads (slot
+    # moves, new chunks, grid rewrite) inside the run.
+    sc = scenes.config2()
+    res = run_parity(sc, frames=4, start_frame=14, flags=A.FLAG_GODRAY_MACRO_ALIAS)
+    assert all(r == {} for r in res), res
+
+
+def test_config2_1080p_resident_frames_15_16_bit_exact():
+    # The device-resident workload the bench's `value` times: every chunk of
+    # the path uploaded once, the frame-16 shift a grid-window rewrite.
+    from parity import run_resident_parity
+
+    res = run_resident_parity(scenes.config2(), frames=[15, 16])
+    assert all(r == {} for r in res), res
+
+
+def test_config5_4k_frames_bit_exact():
+    # 32x8x32 chunks, 6-level 512^2 clipmap, 3840x2160 present / 1920x1080
+    # internal: two frames with histories feeding back.
+    sc = scenes.config5()
+    res = run_parity(sc, frames=2, flags=A.FLAG_GODRAY_MACRO_ALIAS | A.FLAG_HIT_RECORDS)
+    assert all(r == {} for r in res), res
+
+
+@pytest.mark.parametrize("limits", [(64, 0), (0, 64), (1, 1)])
+def test_probe_overflow_rewalk_bit_exact(limits):
+    # Grass probes or slab tasks that do not fit the (capped) record buffers
+    # send their pixels to k_primary_resolve's inline re-walk; the frames stay
+    # bit-exact and the re-walk counter shows the path ran.
+    sc = scenes.config2(present=(320, 180))
+    stats = []
+
+    def on_frame(g, o, bad, r, ora):
+        stats.append(r.frame_stats())
+
+    res = run_parity(sc, frames=2, setup=lambda r: r.set_record_limits(*limits), on_frame=on_frame)
+    assert all(r == {} for r in res), res
+    assert all(s["rewalk_pixels"] > 0 for s in stats), stats
+    assert all(s["pending_pixels"] >= s["rewalk_pixels"] for s in stats), stats
+
+
+def test_probe_records_fit_without_rewalk_on_bench_frame():
+    # At the default buffer sizes the bench frame stores every probe and slab.
+    sc = scenes.config2(present=(640, 360))
+    stats = []
+    res = run_parity(sc, frames=1, on_frame=lambda g, o, bad, r, ora: stats.append(r.frame_stats()))
+    assert res == [{}], res
+    s = stats[0]
+    assert s["probes"] > 0 and s["slab_tasks"] > 0 and s["pending_pixels"] > 0, s
+    assert s["voxel_pixels"] + s["far_pixels"] == 320 * 180, s
+
+
+def test_no_chunks_draws_sky_like_the_reference():
+    # With chunk_count 0 main_primary traces the heightfield but writes sky
+    # (ray_main.wgsl:219-231): every depth is FOG_MAX_DIST.
+    sc = scenes.config2(present=(160, 90))
+
+    def empty(cam):
+        cam.chunk_count = 0
+
+    seen = []
+    res = run_parity(sc, frames=2, cam_hook=empty, on_frame=lambda g, o, bad, r, ora: seen.append(g["depth"]))
+    assert all(r == {} for r in res), res
+    assert all(np.all(d == 120.0) for d in seen)
+
+
+def test_profile_counts_match_oracle():
+    # profile_counts (ray_main.wgsl:32-74) with cam.profile_flags & 1 over
+    # temporal frames (hint-window and full traces, grass refinements,
+    # heightfield and voxel shading, fresh and reused shadows).
+    sc = scenes.features()
+    counts = []
+
+    def on(cam):
+        cam.profile_flags = 1
+
+    def on_frame(g, o, bad, r, ora):
+        counts.append((r.read_primary_profile_counts_blocking().copy(), ora.profile.copy()))
+
+    res = run_parity(sc, frames=3, cam_hook=on, on_frame=on_frame)
+    assert all(r == {} for r in res), res
+    for gpu, ref in counts:
+        assert np.array_equal(gpu, ref), (gpu, ref)
+    assert counts[-1][0][A.PROFILE_VOXEL] > 0 and counts[-1][0][A.PROFILE_SHADOW] > 0
+
+
+def test_profile_counts_config2_wavefront_and_megakernel():
+    # The same counts from the wavefront schedule (deferred probes, re-walks
+    # under capped records) and the megakernel, on the config-2 world.
+    for extra, limits in ((0, (0, 0)), (0, (16, 16)), (A.FLAG_PRIMARY_MEGAKERNEL, (0, 0))):
+        sc = scenes.config2(present=(320, 180))
+        counts = []
+
+        def on(cam):
+            cam.profile_flags = 1
+
+        def on_frame(g, o, bad, r, ora):
+            counts.append((r.read_primary_profile_counts_blocking().copy(), ora.profile.copy()))
+
+        res = run_parity(sc, frames=2, cam_hook=on, on_frame=on_frame, extra_flags=extra,
+                         setup=lambda r: r.set_record_limits(*limits))
+        assert all(r == {} for r in res), res
+        for gpu, ref in counts:
+            assert np.array_equal(gpu, ref), (extra, limits, gpu, ref)
+
+
+def test_profile_counts_stay_zero_with_flag_off_and_reset():
+    sc = scenes.features()
+    seen = []
+    res = run_parity(sc, frames=1, on_frame=lambda g, o, bad, r, ora: seen.append(r.read_primary_profile_counts_blocking()))
+    assert res == [{}]
+    assert not seen[0].any()
+
+    def on(cam):
+        cam.profile_flags = 1
+
+    def on_frame(g, o, bad, r, ora):
+        assert r.read_primary_profile_counts_blocking().any()
+        r.reset_primary_profile_counts()
+        assert not r.read_primary_profile_counts_blocking().any()
+
+    run_parity(sc, frames=1, cam_hook=on, on_frame=on_frame)
+
+
+def test_corrupt_upload_sets_error_word_and_matches_oracle():
+    # A chunk upload whose root points its children past the node arena
+    # (child_base made on the host): every device read through it is bounds
+    # checked, sets the node bit of the error word and returns a zero record,
+    # exactly as the oracle's checked reads do (its oob counter); the images
+    # stay finite and equal the oracle's.
+    from oracle import oracle as O
+    from parity import compare_frame, make_renderer, read_gpu_frame
+
+    sc = scenes.config1()
+    drv = FrameDriver(sc)
+    ups = drv.initial_uploads()
+    w = drv.world
+    u = ups[0]
+    base = u.node_base
+    bad_child = w.node_capacity + 12345
+    w.nodes[base]["child_base"] = bad_child  # host mirror the oracle reads
+    nodes = u.data.nodes.copy()
+    nodes[0]["child_base"] = bad_child
+    u.data.nodes = nodes
+    r = make_renderer(sc, w)
+    try:
+        r.upload_world(w, ups)
+        _, _, clip, cam = drv.step()
+        params = drv.empty_clip()
+        r.write_clipmap_updates(params, [])
+        r.write_camera(cam)
+        with pytest.raises(A.VxeError) as ei:
+            r.encode_compute()  # synchronous: reports the error word
+        assert ei.value.status == 6  # VXE_ERR_BOUNDS
+        word = r.read_error_word()
+        ora = O.OracleFrameRunner(w, sc.internal, sc.present, None, sc.clip_res)
+        ora.render(cam, params)
+        assert ora.primary_ctr.oob > 0
+        assert word & 1, hex(word)  # node reads out of range
+        g = read_gpu_frame(r)
+        assert compare_frame(g, ora.outputs()) == {}
+        assert np.isfinite(g["output"]).all() and np.isfinite(g["color"]).all()
+    finally:
+        r.close()

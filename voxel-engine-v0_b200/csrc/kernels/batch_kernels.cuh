@@ -189,6 +189,7 @@ __device__ __noinline__ HitRec viewport_far_rec(const Scene& s, uint32_t gx, uin
   const float vs = vs_(s);
   const v3 ro = cam_pos(s);
   const v3 rd = ray_dir_from_pixel(s, V2((float)gx + 0.5f, (float)gy + 0.5f));
+  if (s.cam->chunk_count == 0u) return miss_rec();  // no chunks: sky (ray_main.wgsl:219-231)
   ClipHit hf = clip_trace_heightfield(s, ro, rd, 0.0f, FOG_MAX_DIST);
   if (!hf.hit) return miss_rec();
   if (hf.mat == MAT_GRASS) {
@@ -305,7 +306,7 @@ __device__ __forceinline__ void batch_item(const BatchArgs& B, const BatchHeader
       } else if (ph.seq != 0u) {  // met probes: k_batch_resolve decides
         if (vox) store_hitgeom(B.px_hit + (size_t)ray * 4u, vt.best);
         const uint32_t stored = ph.seq > 0xFFFFFFu ? 0u : ph.recorded;
-        B.px_probe[ray] = make_uint2(probe_summary(ph.seq, ph.best_cand, ph.phase, vox), stored);
+        B.px_probe[ray] = make_uint2(probe_summary(ph.seq, ph.best_cand, ph.phase, ph.first_phase == 0u, vox), stored);
         enqueue_active(B.q_pending, &B.dcount[1], ray);
       } else {
         batch_finish(B, s, q, ray, gx, gy, vox, vt.best);

@@ -1204,6 +1204,7 @@ struct ProbeHook {
   uint32_t slot;       // chunk slot of the walk in progress
   uint32_t cand;       // its index in the candidate list
   uint32_t phase;      // 0 hint-window trace, 1 full trace
+  uint32_t first_phase;  // phase the primary trace started in (2: it did not trace)
   uint32_t best_cand;  // candidate index of the trace's current best (INVALID: none)
   uint32_t pixel;
   uint32_t recorded;   // probes stored
@@ -1219,6 +1220,7 @@ __device__ __forceinline__ ProbeHook probe_hook_inline() {
   h.slot = INVALID;
   h.cand = 0u;
   h.phase = 1u;
+  h.first_phase = 2u;
   h.best_cand = INVALID;
   h.pixel = 0u;
   h.recorded = 0u;

@@ -91,7 +91,23 @@ struct FrameArgs {
   uint32_t grass_slot0;  // k_grass_cells: first slot of the launch
   uint32_t* grass_list;    // grass columns of the last full build (k_grass_cells appends; null: no list)
   uint32_t* grass_list_n;  // their count
+  // profile_counts (ray_main.wgsl:32-74): VOXEL, GRASS, HDR, FOG, SHADOW,
+  // added to when cam.profile_flags & 1 (null: not counted)
+  uint32_t* profile;
 };
+
+// profile_inc / profile_add (ray_main.wgsl:64-74).  The flag is uniform over
+// the launch (a kernel parameter), so with it off this is one predicated
+// branch.
+enum : uint32_t { PROFILE_VOXEL = 0u, PROFILE_GRASS = 1u, PROFILE_HDR = 2u, PROFILE_FOG = 3u, PROFILE_SHADOW = 4u };
+__device__ __forceinline__ void profile_add(const FrameArgs& A, uint32_t idx, uint32_t v) {
+  if (A.profile != nullptr && (A.cam.profile_flags & 1u) != 0u) atomicAdd(&A.profile[idx], v);
+}
+// fog_profile_weight (ray_main.wgsl:89-93)
+__device__ __forceinline__ uint32_t fog_profile_weight(float t_scene) {
+  const float fog_norm = clampf(t_scene / FOG_MAX_DIST, 0.0f, 1.0f);
+  return max(1u, to_u32(fog_norm * 256.0f));
+}
 
 __device__ __forceinline__ Scene make_scene(const FrameArgs& A, bool godray) {
   Scene s;
@@ -521,7 +537,8 @@ __device__ __noinline__ VoxTraceResult primary_trace(const Scene& s, const Frame
   const float t_end = fmin_(t_hist + PRIMARY_HIT_WINDOW, FOG_MAX_DIST);
   // phase 0: the hint window (when the history is valid); phase 1: the full
   // trace when phase 0 found nothing.  One call site keeps one copy of the walk.
-  for (uint32_t phase = hist_valid ? 0u : 1u;; ++phase) {
+  ph.first_phase = hist_valid ? 0u : 1u;
+  for (uint32_t phase = ph.first_phase;; ++phase) {
     const bool w = phase == 0u;
     ph.phase = phase;
     const VoxTraceResult h =
@@ -529,6 +546,15 @@ __device__ __noinline__ VoxTraceResult primary_trace(const Scene& s, const Frame
                          w && hak != INVALID, w ? hac : i3{0, 0, 0}, w ? hak : INVALID, tile_count, ph);
     if (!w || h.best.hit != 0u) return h;
   }
+}
+
+// PROFILE_VOXEL of trace_primary_voxels (ray_main.wgsl:130-148): the tile's
+// candidate count once per trace phase run; `last_phase` is the phase that
+// gave the answer (1 when none did).
+__device__ __forceinline__ void profile_voxel(const FrameArgs& A, uint32_t first_phase, uint32_t last_phase,
+                                              uint32_t tile_count) {
+  if (first_phase > 1u) return;
+  profile_add(A, PROFILE_VOXEL, max(1u, tile_count) * (last_phase - first_phase + 1u));
 }
 
 // main_local_taa (taa.wgsl:26-69) for one pixel, fused after its shading.
@@ -552,8 +578,8 @@ __device__ __forceinline__ void local_taa_store(const FrameArgs& A, size_t pix, 
 //                        history mixed with a fresh sun transmittance
 //   gather_voxel_lights  local light gather (8 rays)
 //   shade_voxel_final    surface shading, fog, outputs, fused local TAA.
-__device__ __forceinline__ void grass_refine(const Scene& s, const PrimaryCtx& c, HitGeom& best) {
-  if (best.mat != MAT_GRASS) return;
+__device__ __forceinline__ bool grass_refine(const Scene& s, const PrimaryCtx& c, HitGeom& best) {
+  if (best.mat != MAT_GRASS) return false;
   const float vs = vs_(s);
   const int32_t csv = (int32_t)s.cam->chunk_size;
   const i3 ov{to_i32(floorf(best.root_bmin.x / vs + 0.5f)), to_i32(floorf(best.root_bmin.y / vs + 0.5f)),
@@ -563,6 +589,7 @@ __device__ __forceinline__ void grass_refine(const Scene& s, const PrimaryCtx& c
   const GrassHit gh = try_grass_slab_hit(s, c.ro, c.rd, 0.0f, best.t, cell.bmin_m, cell.id_vox, vs,
                                          s.cam->voxel_params[1], s.cam->voxel_params[2]);
   if (gh.hit) { best.t = gh.t; best.n = gh.n; }
+  return gh.hit;
 }
 
 __device__ __forceinline__ bool shadow_fresh(const PrimaryCtx& c) { return (c.seed & SHADOW_SUBSAMPLE_MASK) == 0u; }
@@ -606,6 +633,9 @@ __device__ __noinline__ void shade_voxel_final(const Scene& s, const FrameArgs& 
   }
   const float t_scene = fmin_(best.t, FOG_MAX_DIST);
   const v3 col = apply_fog(s, base_hdr, ro, rd, t_scene, sky_bg(rd));
+  profile_add(A, PROFILE_SHADOW, shadow_fresh(c) ? 2u : 1u);
+  profile_add(A, PROFILE_HDR, 2u);
+  profile_add(A, PROFILE_FOG, fog_profile_weight(t_scene));
   uint32_t pxy = 0u, pz = 0u, ak = 0u;
   if (anchor_valid) {
     pxy = pack_i16x2(anchor_chunk.x, anchor_chunk.y);
@@ -623,7 +653,7 @@ __device__ __noinline__ void shade_voxel_final(const Scene& s, const FrameArgs& 
 // The whole voxel-hit shading of one pixel (megakernel schedule).
 __device__ __noinline__ void shade_voxel_pixel(const Scene& s, const FrameArgs& A, const PrimaryCtx& c, HitGeom best,
                                                bool anchor_valid, uint32_t anchor_key, i3 anchor_chunk) {
-  grass_refine(s, c, best);
+  if (grass_refine(s, c, best)) profile_add(A, PROFILE_GRASS, 1u);
   float shadow_out;
   if (shadow_fresh(c)) {
     const float cur = sun_transmittance_geom_only(s, shadow_origin(s, c, best), SUN_DIR);
@@ -643,7 +673,10 @@ __device__ __noinline__ void shade_far_pixel(const Scene& s, const FrameArgs& A,
   HitRec rec = miss_rec();
   v3 col;
   float depth, t_store = 0.0f;
-  ClipHit hf = clip_trace_heightfield(s, ro, rd, 0.0f, FOG_MAX_DIST);
+  // With no voxel chunks the reference traces the heightfield but draws sky
+  // (ray_main.wgsl:219-231).
+  ClipHit hf{false, BIG, V3s(0.0f), MAT_AIR};
+  if (s.cam->chunk_count != 0u) hf = clip_trace_heightfield(s, ro, rd, 0.0f, FOG_MAX_DIST);
   if (hf.hit) {
     if (hf.mat == MAT_GRASS) {
       const v3 hp = ro + rd * hf.t;
@@ -651,11 +684,17 @@ __device__ __noinline__ void shade_far_pixel(const Scene& s, const FrameArgs& A,
       const v3 gb = V3(cell.bmin_m.x, hp.y - vs, cell.bmin_m.z);
       const GrassHit gh = try_grass_slab_hit(s, ro, rd, 0.0f, hf.t, gb, cell.id_vox, vs, s.cam->voxel_params[1],
                                              s.cam->voxel_params[2]);
-      if (gh.hit) { hf.t = gh.t; hf.n = gh.n; }
+      if (gh.hit) {
+        hf.t = gh.t;
+        hf.n = gh.n;
+        profile_add(A, PROFILE_GRASS, 1u);
+      }
     }
     const v3 surface = shade_clip_hit(s, ro, rd, hf, sky_bg(V3(0.0f, 1.0f, 0.0f)));
     const float t_scene = fmin_(hf.t, FOG_MAX_DIST);
     col = apply_fog(s, surface, ro, rd, t_scene, sky_bg(rd));
+    profile_add(A, PROFILE_HDR, 1u);
+    profile_add(A, PROFILE_FOG, fog_profile_weight(t_scene));
     depth = t_scene;
     t_store = t_scene;
     HitGeom g = miss_hitgeom();
@@ -719,6 +758,7 @@ __global__ void __launch_bounds__(PRIMARY_THREADS) k_primary(const __grid_consta
   const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
   ProbeHook ph = probe_hook_inline();
   const VoxTraceResult vt = primary_trace<PROBE_INLINE>(s, A, c, cslot[t], cmeta[t], ccount[t], ph);
+  profile_voxel(A, ph.first_phase, ph.phase, ccount[t]);
   if (vt.in_grid && vt.best.hit != 0u) shade_voxel_pixel(s, A, c, vt.best, vt.anchor_valid, vt.anchor_key, vt.anchor_chunk);
   else shade_far_pixel(s, A, c);
 }
@@ -749,9 +789,12 @@ __device__ __forceinline__ void enqueue(uint32_t* q, uint32_t* counter, bool min
 __device__ __forceinline__ uint32_t warp_uniform_end(uint32_t n) { return (n + 31u) & ~31u; }
 
 // Walk summary of a pixel that met probes (px_probe.x): probes met (24 bits),
-// candidate index of the voxel answer, its trace phase, voxel-hit bit.
-__device__ __forceinline__ uint32_t probe_summary(uint32_t met, uint32_t best_cand, uint32_t phase, bool vox) {
-  return min(met, 0xFFFFFFu) | ((best_cand & 31u) << 24) | ((phase & 1u) << 29) | (vox ? 0x80000000u : 0u);
+// candidate index of the voxel answer, its trace phase, whether the trace
+// began with the hint window, voxel-hit bit.
+__device__ __forceinline__ uint32_t probe_summary(uint32_t met, uint32_t best_cand, uint32_t phase, bool hinted,
+                                                  bool vox) {
+  return min(met, 0xFFFFFFu) | ((best_cand & 31u) << 24) | ((phase & 1u) << 29) | (hinted ? 0x40000000u : 0u) |
+         (vox ? 0x80000000u : 0u);
 }
 
 // Order of probe hits: trace phase (hint window first), t, candidate index,
@@ -793,7 +836,9 @@ __global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace(const __grid_
       // more probes than the summary counts: every stored one is still used,
       // the pixel just walks again
       const uint32_t stored = ph.seq > 0xFFFFFFu ? 0u : ph.recorded;
-      A.px_probe[pix] = make_uint2(probe_summary(ph.seq, ph.best_cand, ph.phase, vox), stored);
+      A.px_probe[pix] = make_uint2(probe_summary(ph.seq, ph.best_cand, ph.phase, ph.first_phase == 0u, vox), stored);
+    } else {
+      profile_voxel(A, ph.first_phase, ph.phase, ccount[t]);  // the walk is the reference's (no probe met)
     }
   }
   enqueue(A.q_vox, &A.q_count[0], active && vox && !pend, pix);
@@ -901,6 +946,8 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_primary_resolve(const __grid_
       pix = A.q_pending[i];
       const uint2 pp = A.px_probe[pix];
       const uint32_t met = pp.x & 0xFFFFFFu, vcand = (pp.x >> 24) & 31u, vphase = (pp.x >> 29) & 1u;
+      const uint32_t first_phase = (pp.x & 0x40000000u) != 0u ? 0u : 1u;
+      uint32_t answer_phase = vphase;  // phase of the answer (1 when there is none)
       vox = (pp.x >> 31) != 0u;
       const unsigned long long first = A.px_first[pix];
       bool walk = pp.y < met;  // some probes were not evaluated
@@ -915,6 +962,7 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_primary_resolve(const __grid_
           probe_wins = res.x < vt || (res.x == vt && pcand <= vcand);
         }
         if (probe_wins) {
+          answer_phase = pphase;
           const Meta ch = meta_at(s, r.slot);
           const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vs;
           const float rs = (float)s.cam->chunk_size * vs;
@@ -931,15 +979,19 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_primary_resolve(const __grid_
           walk = (((vphase ? pm.y : pm.x) >> vcand) & 1u) != 0u;
         }
       }
+      const uint32_t gx = pix % A.iw, gy = pix / A.iw;
+      const size_t tile = (size_t)(gy >> 3) * tiles_x + (gx >> 3);
       if (walk) {
-        const uint32_t gx = pix % A.iw, gy = pix / A.iw;
+        atomicAdd(&A.q_count[9], 1u);
         const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
-        const size_t tile = (size_t)(gy >> 3) * tiles_x + (gx >> 3);
         ProbeHook ph = probe_hook_inline();
         const VoxTraceResult vt = primary_trace<PROBE_INLINE>(s, A, c, A.tile_slots + tile * TILE_CANDS, nullptr,
                                                 A.tile_count[tile], ph);
         vox = vt.in_grid && vt.best.hit != 0u;
         if (vox) store_pixhit(A.pix_hit + (size_t)pix * 5u, vt.best, vt);
+        profile_voxel(A, ph.first_phase, ph.phase, A.tile_count[tile]);
+      } else {
+        profile_voxel(A, first_phase, vox ? answer_phase : 1u, A.tile_count[tile]);
       }
     }
     enqueue(A.q_vox, &A.q_count[0], active && vox, pix);
@@ -981,7 +1033,7 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_shade_prep(const __grid_const
       uint4* src = A.pix_hit + (size_t)pix * 5u;
       HitGeom g = load_pixhit(s, src);
       if (g.mat == MAT_GRASS) {
-        grass_refine(s, c, g);
+        if (grass_refine(s, c, g)) profile_add(A, PROFILE_GRASS, 1u);
         src[0] = make_uint4(__float_as_uint(g.t), __float_as_uint(g.n.x), __float_as_uint(g.n.y),
                             __float_as_uint(g.n.z));
       }

@@ -137,6 +137,9 @@ struct vxe_ctx {
   DevBuf nodes, ropes, metas, macro, colinfo, grid, clip_tex, errword;
   DevBuf slot_lights;  // per slot: holds a LIGHT leaf (k_slot_lights)
   DevBuf slot_top;     // per slot: top of its non-air leaves, voxels (k_slot_lights)
+  DevBuf profile;      // profile_counts of the context's frames (5 words)
+  // caps on the wavefront's stored grass probes and slab tasks (0: the buffers' sizes)
+  uint32_t probe_limit = 0, slab_limit = 0;
   // chunk builder: per-chunk scratch (materials, ground minima, level-5 cell
   // states and child offsets, solid counts) and events around its two kernels
   // asynchronous image reads: a copy stream and one event per ticket slot;
@@ -568,9 +571,11 @@ void frame_fill(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& cam, FrameArgs&
   A.px_light = (float4*)S->img[IMG_PXLIGHT].p;
   A.probe_recs = (vxe::dev::ProbeRec*)S->img[IMG_PROBE_RECS].p;
   A.probe_cap = (uint32_t)std::min<size_t>(S->img[IMG_PROBE_RECS].bytes / sizeof(vxe::dev::ProbeRec), 0xFFFFFFFFu);
+  if (c->probe_limit) A.probe_cap = std::min(A.probe_cap, c->probe_limit);
   A.slab_tasks = (uint4*)S->img[IMG_SLAB_TASKS].p;
   A.slab_res = (float4*)S->img[IMG_SLAB_RES].p;
   A.slab_cap = (uint32_t)std::min<size_t>(S->img[IMG_SLAB_TASKS].bytes / 32u, 0xFFFFFFFFu);
+  if (c->slab_limit) A.slab_cap = std::min(A.slab_cap, c->slab_limit);
   A.px_first = (unsigned long long*)S->img[IMG_PXFIRST].p;
   A.px_probe = (uint2*)S->img[IMG_PXPROBE].p;
   A.slab_hits = (uint32_t*)S->img[IMG_SLAB_HITS].p;
@@ -686,6 +691,7 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
   }
   FrameArgs A;
   frame_fill(c, c->fr, c->cam, A);
+  A.profile = (uint32_t*)c->profile.p;
   if (timed) CK(cudaEventRecord(c->fr.ev[0], c->compute));
   bool use_grass = false;
   if ((st = grass_table_acquire(c, c->compute, 0, c->cam, &use_grass)) != VXE_OK) return st;
@@ -718,6 +724,7 @@ vxe_status launch_frame_graph(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& c
   }
   FrameArgs A;
   frame_fill(c, F, cam, A);
+  if (&F == &c->fr) A.profile = (uint32_t*)c->profile.p;
   bool use_grass = false;
   if ((rc = grass_table_acquire(c, st, reader, cam, &use_grass)) != VXE_OK) return rc;
   if (use_grass) grass_table_args(c, A);
@@ -856,6 +863,8 @@ vxe_status vxe_create(const vxe_config* cfg, vxe_ctx** out) {
   if ((st = alloc(c, c->errword, 4)) != VXE_OK) return bail(st);
   if ((st = alloc(c, c->slot_lights, cc * 4)) != VXE_OK) return bail(st);
   if ((st = alloc(c, c->slot_top, cc * 4)) != VXE_OK) return bail(st);
+  if ((st = alloc(c, c->profile, 32)) != VXE_OK) return bail(st);
+  if (fill_sync(c->profile.p, 0, 32) != cudaSuccess) return bail(VXE_ERR_DEVICE);
   if (!(cfg->flags & VXE_FLAG_NO_GRASS_TABLE)) {
     if ((st = alloc(c, c->gt.rec, cc * 4096u * vxe::dev::GRASS_REC_F4 * 16u)) != VXE_OK) return bail(st);
     if ((st = alloc(c, c->gt.taper, vxe::dev::GRASS_TAPER_N * 4u)) != VXE_OK) return bail(st);
@@ -898,7 +907,7 @@ void vxe_destroy(vxe_ctx* c) {
   if (c->fr.fgraph) cudaGraphDestroy(c->fr.fgraph);
   for (auto& L : c->lanes)  // lanes read the arenas: drain them before freeing
     if (L.stream) cudaStreamSynchronize(L.stream);
-  for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword, &c->slot_lights, &c->slot_top, &c->build_scratch, &c->build_places, &c->move_buf,
+  for (auto* b : {&c->nodes, &c->ropes, &c->metas, &c->macro, &c->colinfo, &c->grid, &c->clip_tex, &c->errword, &c->slot_lights, &c->slot_top, &c->profile, &c->build_scratch, &c->build_places, &c->move_buf,
                   &c->q_in, &c->q_out, &c->gt.rec, &c->gt.taper, &c->gt.state, &c->gt.frames,
                   &c->gt.list, &c->gt.list_n})
     release(*b);
@@ -1432,6 +1441,46 @@ vxe_status vxe_read_error_word(vxe_ctx* c, uint32_t* word) {
   return VXE_OK;
 }
 
+vxe_status vxe_set_record_limits(vxe_ctx* c, uint32_t probe_records, uint32_t slab_tasks) {
+  if (!c) return VXE_ERR_INVALID_ARG;
+  c->probe_limit = probe_records;
+  c->slab_limit = slab_tasks;
+  return VXE_OK;
+}
+
+vxe_status vxe_get_frame_stats(vxe_ctx* c, vxe_frame_stats* out) {
+  if (!c || !out) return VXE_ERR_INVALID_ARG;
+  std::memset(out, 0, sizeof *out);
+  if (!c->fr.img[IMG_QCOUNT].p || (c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL)) return VXE_OK;
+  cudaSetDevice(c->device);
+  CK(cudaStreamSynchronize(c->compute));
+  uint32_t q[16];
+  CK(cudaMemcpy(q, c->fr.img[IMG_QCOUNT].p, sizeof q, cudaMemcpyDeviceToHost));
+  out->voxel_pixels = q[0];
+  out->far_pixels = q[1];
+  out->probes = q[4];
+  out->pending_pixels = q[5];
+  out->slab_tasks = q[6];
+  out->slab_hits = q[7];
+  out->rewalk_pixels = q[9];
+  return VXE_OK;
+}
+
+vxe_status vxe_reset_profile_counts(vxe_ctx* c) {
+  if (!c) return VXE_ERR_INVALID_ARG;
+  cudaSetDevice(c->device);
+  CK(cudaMemsetAsync(c->profile.p, 0, c->profile.bytes, c->compute));  // after the frames enqueued so far
+  return VXE_OK;
+}
+
+vxe_status vxe_read_profile_counts(vxe_ctx* c, uint32_t counts[VXE_PROFILE_COUNT]) {
+  if (!c || !counts) return VXE_ERR_INVALID_ARG;
+  cudaSetDevice(c->device);
+  CK(cudaStreamSynchronize(c->compute));
+  CK(cudaMemcpy(counts, c->profile.p, VXE_PROFILE_COUNT * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  return VXE_OK;
+}
+
 static void fill_query_args(const vxe_ctx* c, QueryArgs& Q) {
   std::memset(&Q, 0, sizeof Q);
   Q.cam = c->cam;
@@ -1544,8 +1593,10 @@ vxe_status build_launch(vxe_ctx* c, vxe::build::BuildArgs& B, uint32_t n) {
     vxe_status st = alloc(c, c->build_scratch, need);
     if (st != VXE_OK) return st;
   }
-  for (auto& e : c->build_ev)
-    if (!e) CK(cudaEventCreate(&e));
+  if (!c->build_ev[0]) {  // first build on this context: events, and the octree kernel's staging size
+    for (auto& e : c->build_ev) CK(cudaEventCreate(&e));
+    CK(cudaFuncSetAttribute(vb::k_build_svo, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vb::kStageBytes));
+  }
   B.cave_smin = cave_s_min((double)B.wp.cave_threshold);
   B.n = n;
   char* base = (char*)c->build_scratch.p;
@@ -1563,7 +1614,6 @@ vxe_status build_launch(vxe_ctx* c, vxe::build::BuildArgs& B, uint32_t n) {
   vb::k_build_columns<<<n * 16u, 256, 0, st>>>(B);
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->build_ev[1], st));
-  CK(cudaFuncSetAttribute(vb::k_build_svo, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vb::kStageBytes));
   vb::k_build_svo<<<n, vb::SVO_THREADS, vb::kStageBytes, st>>>(B);
   CK(cudaGetLastError());
   CK(cudaEventRecord(c->build_ev[2], st));
@@ -1858,10 +1908,12 @@ BatchArgs batch_args(const vxe_ctx* c, const BatchLane& L) {
   B.head = (uint32_t*)L.head.p;
   B.probe_recs = (vxe::dev::ProbeRec*)L.probe_recs.p;
   B.probe_cap = L.ray_cap * kBatchProbesPerRay;
+  if (c->probe_limit) B.probe_cap = std::min(B.probe_cap, c->probe_limit);
   B.slab_tasks = (uint4*)L.slab_tasks.p;
   B.slab_res = (float4*)L.slab_res.p;
   B.slab_hits = (uint32_t*)L.slab_hits.p;
   B.slab_cap = L.ray_cap * kBatchSlabsPerRay;
+  if (c->slab_limit) B.slab_cap = std::min(B.slab_cap, c->slab_limit);
   B.ray_cap = L.ray_cap;
   B.px_first = (unsigned long long*)L.px_first.p;
   B.px_task = (uint32_t*)L.px_task.p;
@@ -2307,18 +2359,41 @@ constexpr size_t kNoallocWords = kNoallocSlotOff + (size_t)VXE_NOALLOC_MAX_TILES
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoallocWords];
 
 // In host code g_noalloc_scratch is only a stand-in symbol, not a device
-// address; the address is resolved per device with that device current.
+// address; the address is resolved per device with that device current, and
+// again when the device's context changed since (after cudaDeviceReset the
+// module loads again, possibly at another address).
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 uint32_t* g_noalloc_addr[kMaxDevices] = {};
+void* g_noalloc_ctx[kMaxDevices] = {};
+
+// The current driver context (cuCtxGetCurrent through the runtime's entry
+// point lookup, so the library needs no link against the driver library);
+// null if it cannot be had.
+void* current_context() {
+  using GetCurrent = int (*)(void**);
+  static GetCurrent fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return (GetCurrent)f;
+  }();
+  void* ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
 
 vxe_status noalloc_scratch(int dev, uint32_t** out) {
   if (dev < 0 || dev >= kMaxDevices) return VXE_ERR_NO_DEVICE;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
+  void* ctx = current_context();
+  if (!g_noalloc_addr[dev] || !ctx || ctx != g_noalloc_ctx[dev]) {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return VXE_ERR_DEVICE;
     g_noalloc_addr[dev] = (uint32_t*)p;
+    g_noalloc_ctx[dev] = ctx;
   }
   *out = g_noalloc_addr[dev];
   return VXE_OK;
@@ -2357,7 +2432,7 @@ __global__ void __launch_bounds__(vxe::dev::PRIMARY_THREADS) k_hits_noalloc(cons
       if (gh.hit) { best.t = gh.t; best.n = gh.n; }
     }
     rec = make_rec(best, ro, rd, vs, true);
-  } else {
+  } else if (s.cam->chunk_count != 0u) {  // no chunks: sky (ray_main.wgsl:219-231)
     ClipHit hf = clip_trace_heightfield(s, ro, rd, 0.0f, FOG_MAX_DIST);
     if (hf.hit) {
       if (hf.mat == MAT_GRASS) {
@@ -2397,6 +2472,9 @@ extern "C" vxe_status vxe_trace_primary_hits_noalloc(const vxe_scene_view* sv, c
     return VXE_ERR_INVALID_ARG;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return VXE_ERR_NO_DEVICE;
+  // An error the caller left pending is not this call's: report it without
+  // launching, and leave it for the caller (peek does not clear it).
+  if (cudaPeekAtLastError() != cudaSuccess) return VXE_ERR_DEVICE;
   uint32_t* scratch = nullptr;
   vxe_status st = noalloc_scratch(dev, &scratch);
   if (st != VXE_OK) return st;

@@ -165,6 +165,13 @@ class SceneView(C.Structure):
 
 
 NOALLOC_MAX_TILES = 36864
+PROFILE_COUNT = 5
+PROFILE_VOXEL, PROFILE_GRASS, PROFILE_HDR, PROFILE_FOG, PROFILE_SHADOW = range(5)
+
+
+class FrameStats(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in ("voxel_pixels", "far_pixels", "probes", "pending_pixels", "slab_tasks",
+                                           "slab_hits", "rewalk_pixels", "_pad")]
 
 REQ_VIEWPORT, REQ_QUERY = 0, 1
 BATCH_PERSISTENT, BATCH_PLAIN, BATCH_GRAPH = 0, 1, 2
@@ -212,6 +219,10 @@ SIGNATURES = {
     "vxe_read_image": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
     "vxe_write_image": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
     "vxe_read_error_word": (C.c_int, [C.c_void_p, P(C.c_uint32)]),
+    "vxe_reset_profile_counts": (C.c_int, [C.c_void_p]),
+    "vxe_read_profile_counts": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "vxe_set_record_limits": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
+    "vxe_get_frame_stats": (C.c_int, [C.c_void_p, P(FrameStats)]),
     "vxe_debug_detmath": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
     "vxe_trace_primary_hits_noalloc": (C.c_int, [P(SceneView), P(CameraGpu), P(ClipmapGpu), C.c_void_p,
                                                   C.c_void_p]),
@@ -271,6 +282,36 @@ def lib() -> C.CDLL:
             fn.argtypes = args
         _lib = l
     return _lib
+
+
+# The host-side producers (chunk builder, camera packing, clipmap state) are
+# plain C++ with no device code.  A process that must not map the CUDA library
+# (a CPU-only consumer of the producers, such as a CPU timing of the passes)
+# registers a host-only build of the same sources here.
+HOST_SYMBOLS = ("vxe_build_chunk", "vxe_free_chunk", "vxe_chunk_materials", "vxe_ground_height",
+                "vxe_build_from_materials", "vxe_build_camera", "vxe_clipmap_new", "vxe_clipmap_free",
+                "vxe_clipmap_update", "vxe_clipmap_plan")
+_host_lib = None
+
+
+def use_host_library(path) -> C.CDLL:
+    """Routes the host-side producer calls (HOST_SYMBOLS) to the library at
+    `path`, a host-only build of the producer sources, instead of libvxe.so."""
+    global _host_lib
+    l = C.CDLL(str(path))
+    for name in HOST_SYMBOLS:
+        res, args = SIGNATURES[name]
+        fn = getattr(l, name)
+        fn.restype = res
+        fn.argtypes = args
+    _host_lib = l
+    return l
+
+
+def host_lib() -> C.CDLL:
+    """The library serving the host-side producer calls: libvxe.so unless
+    use_host_library() registered a host-only build."""
+    return _host_lib if _host_lib is not None else lib()
 
 
 def check_layout() -> None:

@@ -211,6 +211,25 @@ class Renderer:
         self._check(self._lib.vxe_read_error_word(self._ctx, C.byref(w)), "vxe_read_error_word")
         return w.value
 
+    # -- primary profile counters (render/state/mod.rs:448-491) -------------------
+    def reset_primary_profile_counts(self) -> None:
+        self._check(self._lib.vxe_reset_profile_counts(self._ctx), "vxe_reset_profile_counts")
+
+    def read_primary_profile_counts_blocking(self) -> np.ndarray:
+        """VOXEL, GRASS, HDR, FOG, SHADOW counts of the frames since the last reset."""
+        out = np.zeros(A.PROFILE_COUNT, dtype=np.uint32)
+        self._check(self._lib.vxe_read_profile_counts(self._ctx, out.ctypes.data), "vxe_read_profile_counts")
+        return out
+
+    # -- wavefront diagnostics ----------------------------------------------------
+    def set_record_limits(self, probe_records: int = 0, slab_tasks: int = 0) -> None:
+        self._check(self._lib.vxe_set_record_limits(self._ctx, probe_records, slab_tasks), "vxe_set_record_limits")
+
+    def frame_stats(self) -> dict:
+        st = A.FrameStats()
+        self._check(self._lib.vxe_get_frame_stats(self._ctx, C.byref(st)), "vxe_get_frame_stats")
+        return {k: int(getattr(st, k)) for k, _ in A.FrameStats._fields_ if not k.startswith("_")}
+
     # -- images -----------------------------------------------------------------
     _IMG_SHAPES = {
         A.IMG_COLOR: ("i", 4, np.float32), A.IMG_DEPTH: ("i", 1, np.float32), A.IMG_LOCAL: ("i", 4, np.float32),

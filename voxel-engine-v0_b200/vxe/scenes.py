@@ -145,19 +145,24 @@ SCENES = {"config1": config1, "config2": config2, "config5": config5, "features"
 class FrameDriver:
     """Produces per-frame inputs (uploads, grid, clipmap patches, camera) for a scene."""
 
-    def __init__(self, scene: Scene, device_renderer=None, mirror: bool = True):
+    def __init__(self, scene: Scene, device_renderer=None, mirror: bool = True, start_frame: int = 0):
         """`device_renderer`: keep the world on that renderer's device -- chunks
         built resident there, grid shifts by device slot moves (step() then
         returns no uploads and writes the grid itself).  `mirror`: the world
-        keeps host copies of the node and rope arenas (World)."""
+        keeps host copies of the node and rope arenas (World).  `start_frame`:
+        the first path frame step() produces; the grid starts where the shifts
+        of the earlier frames left it (histories start empty)."""
         self.scene = scene
         self.device = device_renderer
         self.last_shift = None  # (chunks built, slots moved) of the last device shift
-        self.world = World(scene.spec, scene.grid_origin, scene.grid_dims, scene.node_capacity,
+        origin = tuple(scene.grid_origin)
+        if scene.shift_every and start_frame > 0:
+            origin = (origin[0] + (start_frame - 1) // scene.shift_every, origin[1], origin[2])
+        self.world = World(scene.spec, origin, scene.grid_dims, scene.node_capacity,
                            chunk_capacity=int(np.prod(scene.grid_dims)), mirror=mirror)
         self.clip = Clipmap(scene.spec, scene.clip_levels, scene.clip_res, 1.0) if scene.clip_levels else None
         self.prev_vp = None
-        self.frame = 0
+        self.frame = start_frame
 
     def initial_uploads(self):
         if self.device is not None:
@@ -190,3 +195,56 @@ class FrameDriver:
         p = A.ClipmapGpu()
         p.res = self.scene.clip_res
         return p
+
+
+class ResidentPathDriver:
+    """The frames of a shifting path over a world that holds every chunk the
+    path visits: the grid window of frame f starts at x = f // shift_every, so
+    a grid shift rewrites the grid and moves no chunk.  Frame f of the path is
+    frame f % frames.  This is the device-resident workload: every chunk is
+    uploaded once, before the frames."""
+
+    def __init__(self, scene: Scene, shifts: int = 3):
+        self.scene = scene
+        nx, ny, nz = scene.grid_dims
+        dims = (nx + shifts, ny, nz)
+        self.world = World(scene.spec, scene.grid_origin, dims, scene.node_capacity, chunk_capacity=int(np.prod(dims)))
+        self.clip = Clipmap(scene.spec, scene.clip_levels, scene.clip_res, 1.0)
+        self.prev_vp = None
+        self.last_ox = None
+
+    def initial_uploads(self):
+        return self.world.populate()
+
+    def grid_window(self, ox: int) -> np.ndarray:
+        """chunk_grid of the scene's grid dims at origin x = ox over the world's slots."""
+        nx, ny, nz = self.scene.grid_dims
+        g = np.full(nx * ny * nz, A.INVALID_U32, dtype=np.uint32)
+        oy, oz = self.scene.grid_origin[1], self.scene.grid_origin[2]
+        for iz in range(nz):
+            for iy in range(ny):
+                for ix in range(nx):
+                    s = self.world.key_to_slot.get((ox + ix, oy + iy, oz + iz))
+                    if s is not None:
+                        g[(iz * ny + iy) * nx + ix] = s
+        return g
+
+    def inputs(self, step: int):
+        """(camera, clipmap params, clipmap patches, grid or None when unchanged) of path frame step % frames."""
+        sc = self.scene
+        f = step % sc.frames
+        ox = sc.grid_origin[0] + (f // sc.shift_every if sc.shift_every else 0)
+        pos, yaw, pitch = sc.path(f)
+        cam = build_camera(pos, yaw, pitch, sc.present, sc.internal, frame_index=f + 1, time_s=f / 60.0, world=None,
+                           jitter=sc.jitter, prev_view_proj=self.prev_vp)
+        cam.chunk_count = self.world.chunk_count
+        cam.grid_origin_chunk[0], cam.grid_origin_chunk[1], cam.grid_origin_chunk[2] = \
+            ox, sc.grid_origin[1], sc.grid_origin[2]
+        cam.grid_dims[0], cam.grid_dims[1], cam.grid_dims[2] = sc.grid_dims
+        self.prev_vp = cam.view_proj
+        params, patches = self.clip.update(float(pos[0]), float(pos[2]))
+        grid = None
+        if ox != self.last_ox:
+            grid = self.grid_window(ox)
+            self.last_ox = ox
+        return cam, params, patches, grid

@@ -56,7 +56,7 @@ class ChunkData:
 
 def build_chunk(spec: WorldSpec, cx: int, cy: int, cz: int) -> ChunkData:
     """Runs the C++ port of the reference chunk builder (svo/builder.rs:846-986)."""
-    lib = A.lib()
+    lib = A.host_lib()
     wp = spec.params()
     out = A.BuiltChunk()
     st = lib.vxe_build_chunk(C.byref(wp), cx, cy, cz, C.byref(out))
@@ -75,14 +75,14 @@ def build_chunk(spec: WorldSpec, cx: int, cy: int, cz: int) -> ChunkData:
 
 def chunk_materials(spec: WorldSpec, cx: int, cy: int, cz: int) -> np.ndarray:
     m = np.zeros(64 * 64 * 64, dtype=np.uint8)
-    st = A.lib().vxe_chunk_materials(C.byref(spec.params()), cx, cy, cz, m.ctypes.data)
+    st = A.host_lib().vxe_chunk_materials(C.byref(spec.params()), cx, cy, cz, m.ctypes.data)
     if st != A.VXE_OK:
         raise A.VxeError(st, "vxe_chunk_materials")
     return m.reshape(64, 64, 64)  # [y, z, x]
 
 
 def ground_height(spec: WorldSpec, wx: int, wz: int) -> int:
-    return int(A.lib().vxe_ground_height(C.byref(spec.params()), wx, wz))
+    return int(A.host_lib().vxe_ground_height(C.byref(spec.params()), wx, wz))
 
 
 class NodeArena:
@@ -386,7 +386,7 @@ class Clipmap:
 
     def __init__(self, spec: WorldSpec, levels: int, res: int = 256, base_cell_m: float = 1.0):
         self.levels, self.res = levels, res
-        self._h = A.lib().vxe_clipmap_new(C.byref(spec.params()), levels, res, base_cell_m)
+        self._h = A.host_lib().vxe_clipmap_new(C.byref(spec.params()), levels, res, base_cell_m)
         if not self._h:
             raise A.VxeError(A.STATUS_NAMES and 1, "vxe_clipmap_new")
         self.tex = np.zeros((levels, res, res), dtype=np.float32)  # host mirror of the layers
@@ -397,7 +397,7 @@ class Clipmap:
         params = A.ClipmapGpu()
         pp = C.POINTER(A.ClipPatch)()
         n = C.c_uint32()
-        st = A.lib().vxe_clipmap_update(self._h, cam_x, cam_z, C.byref(params), C.byref(pp), C.byref(n))
+        st = A.host_lib().vxe_clipmap_update(self._h, cam_x, cam_z, C.byref(params), C.byref(pp), C.byref(n))
         if st != A.VXE_OK:
             raise A.VxeError(st, "vxe_clipmap_update")
         patches = []
@@ -420,7 +420,7 @@ class Clipmap:
         h = getattr(self, "_h", None)
         if h:
             try:
-                A.lib().vxe_clipmap_free(h)
+                A.host_lib().vxe_clipmap_free(h)
             except Exception:
                 pass
             self._h = None
@@ -447,7 +447,7 @@ def build_camera(pos, yaw, pitch, present, internal, frame_index, time_s, world:
         p.has_prev = 1
         C.memmove(C.byref(p.prev_view_proj), C.byref(prev_view_proj), C.sizeof(A.Mat4))
     cam = A.CameraGpu()
-    st = A.lib().vxe_build_camera(C.byref(p), C.byref(cam))
+    st = A.host_lib().vxe_build_camera(C.byref(p), C.byref(cam))
     if st != A.VXE_OK:
         raise A.VxeError(st, "vxe_build_camera")
     return cam

@@ -5,6 +5,9 @@
   every float operation is a single IEEE binary32 op.
 * ``oracle/liboracle_vxe.so`` -- the CPU restatement used by tests and the
   CPU baseline (``-ffp-contract=off``, no fast math).
+* ``oracle/libref_producer.so`` -- the host-side producers (chunk builder,
+  camera packing, clipmap state: ``csrc/host/producer.cpp``) built by g++
+  alone, so that the CPU timing of the reference path maps no CUDA library.
 
 Both are rebuilt only when a source is newer than the library.
 """
@@ -23,6 +26,7 @@ CSRC = PKG / "csrc"
 LIB = PKG / "vxe" / "libvxe.so"
 ORACLE_SRC = REPO / "oracle" / "vxe_oracle.cpp"
 ORACLE_LIB = REPO / "oracle" / "liboracle_vxe.so"
+REF_PRODUCER_LIB = REPO / "oracle" / "libref_producer.so"
 BUILD_DIR = PKG / "_build"
 
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
@@ -99,9 +103,21 @@ def build_oracle(verbose: bool = False, force: bool = False) -> Path:
     return ORACLE_LIB
 
 
+def build_ref_producer(verbose: bool = False, force: bool = False) -> Path:
+    src = CSRC / "host" / "producer.cpp"
+    deps = [src, CSRC / "common" / "terrain_noise.h", INCLUDE / "vxe" / "vxe.h", INCLUDE / "vxe" / "detmath.h"]
+    if not force and not _stale(REF_PRODUCER_LIB, deps):
+        return REF_PRODUCER_LIB
+    tmp = REF_PRODUCER_LIB.with_suffix(".so.tmp")
+    _run(["g++", *CXX_FLAGS, "-shared", "-o", tmp, src, "-lpthread"], verbose)
+    os.replace(tmp, REF_PRODUCER_LIB)
+    return REF_PRODUCER_LIB
+
+
 def build_all(verbose: bool = False, force: bool = False) -> None:
     build_lib(verbose=verbose, force=force)
     build_oracle(verbose=verbose, force=force)
+    build_ref_producer(verbose=verbose, force=force)
 
 
 if __name__ == "__main__":
