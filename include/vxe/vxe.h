@@ -439,7 +439,8 @@ typedef struct vxe_frame_stats {
   uint32_t slab_tasks;      /* grass slabs found by the probes' column DDAs */
   uint32_t slab_hits;       /* slabs whose march hit */
   uint32_t rewalk_pixels;   /* pending pixels walked again with inline probes */
-  uint32_t _pad;
+  uint32_t full_trace_pixels; /* pixels whose walk ran the full trace (no valid
+                                 history hint, or nothing in its window) */
 } vxe_frame_stats;
 vxe_status vxe_get_frame_stats(vxe_ctx* ctx, vxe_frame_stats* out);
 
@@ -490,6 +491,14 @@ vxe_status vxe_trace_primary_hits_noalloc(const vxe_scene_view* scene, const vxe
  * 3 pow(x, y), 4 min(x, y), 5 max(x, y).  Used to prove host/device bit
  * equality of the functions every pass depends on. */
 vxe_status vxe_debug_detmath(int which, const float* x, const float* y, float* out, uint32_t n);
+
+/* Diagnostic (no reference counterpart): the device's L2 read bandwidth, the
+ * roof of kernels whose working set stays in L2 (the world's node, rope,
+ * meta, macro and colinfo records).  Reads an L2-resident buffer of `bytes`
+ * (a few tens of MB; allocated and freed by the call) with 16-byte loads,
+ * `launches` times after three warm-up launches; *gbs = bytes read / time
+ * (CUDA events). */
+vxe_status vxe_measure_l2_bandwidth(int device, uint64_t bytes, uint32_t launches, double* gbs);
 
 /* ------------------------------------------------------------------------ */
 /* Producer side (C++ port of src/svo, streaming meta, clipmap, camera)      */

@@ -77,14 +77,15 @@ def make_renderer(scene, world, flags=A.FLAG_GODRAY_MACRO_ALIAS | A.FLAG_HIT_REC
 
 def run_parity(scene, frames: int, threads: int | None = None, godray_alias: bool = True, on_frame=None,
                extra_flags: int = 0, graph: bool = False, flags: int | None = None, start_frame: int = 0,
-               cam_hook=None, setup=None):
+               cam_hook=None, setup=None, budgeted: bool = False):
     """Renders `frames` frames on both sides; returns a list of per-frame mismatch dicts.
 
     `flags`: the context flags (default: hit records + debug intermediates +
     the godray alias, | extra_flags).  `start_frame`: first path frame.
     `cam_hook(cam)`: edits each frame's camera before both sides see it.
-    `setup(renderer)`: called once after the world upload."""
-    drv = FrameDriver(scene, start_frame=start_frame)
+    `setup(renderer)`: called once after the world upload.  `budgeted`:
+    chunk streaming under the per-frame upload budget (FrameDriver)."""
+    drv = FrameDriver(scene, start_frame=start_frame, budgeted=budgeted)
     ups = drv.initial_uploads()
     if flags is None:
         flags = A.FLAG_HIT_RECORDS | A.FLAG_DEBUG_INTERMEDIATES | (A.FLAG_GODRAY_MACRO_ALIAS if godray_alias else 0)

@@ -327,3 +327,20 @@ def test_corrupt_upload_sets_error_word_and_matches_oracle():
         assert np.isfinite(g["output"]).all() and np.isfinite(g["color"]).all()
     finally:
         r.close()
+
+
+def test_budgeted_streaming_frames_bit_exact():
+    # Host streaming through the reference's per-frame upload budget
+    # (take_budgeted): at the grid shift the slot rewrites go first and the
+    # entering chunks join the grid over the next frames as their uploads are
+    # taken; every frame matches the oracle on the same grid.
+    sc = scenes.config2(present=(320, 180))
+    sc.shift_every = 2
+    res = run_parity(sc, frames=4, budgeted=True)
+    assert all(r == {} for r in res), res
+    # the shift's uploads do not fit one frame's budget
+    d = FrameDriver(sc, budgeted=True)
+    d.initial_uploads()
+    for _ in range(3):
+        ups, _, _, _ = d.step()
+    assert len(d.queue) > 0 and d.world.uploading

@@ -80,6 +80,7 @@ struct FrameArgs {
   uint2* px_mask;                 // per pixel: candidate chunks with a probe hit, hint / full trace
   uint2* px_probe;                // per pixel: walk summary (probe_summary) | probes stored
   uint32_t* q_pending;            // pixels whose walk met probes, q_count[5] of them
+  uint32_t* q_full;               // pixels whose walk goes on to the full trace, q_count[10] of them
   // per-frame grass cell table: written by k_grass_cells, read by the rest
   float4* grass_rec;
   uint64_t grass_rec_n;  // records (slots * 4096)
@@ -371,17 +372,29 @@ __device__ VoxTraceResult trace_candidates(const Scene& s, const uint32_t* cslot
   const float rs = (float)s.cam->chunk_size * vsz;
   const uint32_t maxc = min(cand_count, MAX_TILE_CHUNKS);
   const TraceOpts opt{false};
-  for (uint32_t i = 0; i < maxc; ++i) {
-    const uint32_t slot = cslot[i];
-    if (slot == INVALID || slot >= s.cam->chunk_count) continue;
-    const Meta ch = cmeta ? cmeta[i] : meta_at(s, slot);  // staged in shared memory, or read through L1
-    if (ch.macro_empty != 0u) continue;
-    const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vsz;
-    const v2 rt = intersect_aabb(ro, rd, rb, rb + V3s(rs));
-    const float ce = fmax_(rt.x, t_enter), cx = fmin_(rt.y, t_exit);
-    if (cx < ce) continue;
-    if (best.hit != 0u && ce >= best.t) continue;
-    if (chunk_heightfield_early_skip(s, ro, rd, ce, cx, ch, vsz)) continue;
+  for (uint32_t i = 0;; ++i) {
+    // Each lane first passes over the candidates it does not walk (no slot,
+    // an empty chunk, missed, behind the best hit, skipped by the heightfield
+    // test) in this inner loop, so that the lanes of a warp enter the chunk
+    // walk together even when they walk different candidates.
+    Meta ch;
+    float ce = 0.0f, cx = 0.0f;
+    uint32_t slot = INVALID;
+    for (; i < maxc; ++i) {
+      slot = cslot[i];
+      if (slot == INVALID || slot >= s.cam->chunk_count) continue;
+      ch = cmeta ? cmeta[i] : meta_at(s, slot);  // staged in shared memory, or read through L1
+      if (ch.macro_empty != 0u) continue;
+      const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vsz;
+      const v2 rt = intersect_aabb(ro, rd, rb, rb + V3s(rs));
+      ce = fmax_(rt.x, t_enter);
+      cx = fmin_(rt.y, t_exit);
+      if (cx < ce) continue;
+      if (best.hit != 0u && ce >= best.t) continue;
+      if (chunk_heightfield_early_skip(s, ro, rd, ce, cx, ch, vsz)) continue;
+      break;
+    }
+    if (i >= maxc) break;
     const int32_t csz = (int32_t)s.cam->chunk_size;
     const i3 cc{ch.ox / csz, ch.oy / csz, ch.oz / csz};
     const bool ua = anchor_valid_in && chunk_coords_neighbor(cc, anchor_chunk_in);
@@ -497,19 +510,21 @@ __device__ __forceinline__ PrimaryCtx primary_ctx(const Scene& s, uint32_t gx, u
   return c;
 }
 
-// History hint + voxel trace (ray_main.wgsl:274-325 and trace_primary_voxels :116-161).
-template <uint32_t PM>
-__device__ __noinline__ VoxTraceResult primary_trace(const Scene& s, const FrameArgs& A, const PrimaryCtx& c,
-                                                     const uint32_t* cslot, const Meta* cmeta, uint32_t tile_count,
-                                                     ProbeHook& ph) {
-  VoxTraceResult vt{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
-  if (s.cam->chunk_count == 0u || tile_count == 0u) return vt;
+// The primary-hit history hint (ray_main.wgsl:274-318): the previous hit
+// distance at this pixel, accepted when its reprojection agrees in depth and
+// motion; with it the window the first trace phase searches and the anchor.
+struct PrimaryHint {
+  bool valid;
+  float t_start, t_end;
+  uint32_t anchor_key;  // INVALID: none
+  i3 anchor_chunk;
+};
+
+__device__ __forceinline__ PrimaryHint primary_hint(const Scene& s, const FrameArgs& A, const PrimaryCtx& c) {
   const uint32_t W = A.iw, H = A.ih;
   const v2 res = V2((float)W, (float)H);
   float t_hist = 0.0f;
-  bool hist_valid = false;
-  uint32_t hak = INVALID;
-  i3 hac{0, 0, 0};
+  PrimaryHint h{false, 0.0f, 0.0f, INVALID, i3{0, 0, 0}};
   const v2 uv = c.px / res;
   const float t_guess = __uint_as_float(A.hist_in[c.pix].x);
   if (t_guess > 1e-3f) {
@@ -525,25 +540,37 @@ __device__ __noinline__ VoxTraceResult primary_trace(const Scene& s, const Frame
       const float motion_ok = 1.0f - smooth(PRIMARY_HIT_MOTION_PX0, PRIMARY_HIT_MOTION_PX1, vel);
       if (t_prev > 1e-3f && depth_ok > 0.5f && motion_ok > 0.5f) {
         t_hist = t_prev;
-        hist_valid = true;
+        h.valid = true;
         if ((hp.w & 0x80000000u) != 0u) {
-          hak = hp.y;
-          hac = i3{unpack_i16(hp.z), unpack_i16(hp.z >> 16), unpack_i16(hp.w)};
+          h.anchor_key = hp.y;
+          h.anchor_chunk = i3{unpack_i16(hp.z), unpack_i16(hp.z >> 16), unpack_i16(hp.w)};
         }
       }
     }
   }
-  const float t_start = fmax_(t_hist - PRIMARY_HIT_MARGIN, 0.0f);
-  const float t_end = fmin_(t_hist + PRIMARY_HIT_WINDOW, FOG_MAX_DIST);
+  h.t_start = fmax_(t_hist - PRIMARY_HIT_MARGIN, 0.0f);
+  h.t_end = fmin_(t_hist + PRIMARY_HIT_WINDOW, FOG_MAX_DIST);
+  return h;
+}
+
+// History hint + voxel trace (ray_main.wgsl:274-325 and trace_primary_voxels :116-161).
+template <uint32_t PM>
+__device__ __noinline__ VoxTraceResult primary_trace(const Scene& s, const FrameArgs& A, const PrimaryCtx& c,
+                                                     const uint32_t* cslot, const Meta* cmeta, uint32_t tile_count,
+                                                     ProbeHook& ph) {
+  VoxTraceResult vt{false, miss_hitgeom(), 0.0f, false, INVALID, i3{0, 0, 0}};
+  if (s.cam->chunk_count == 0u || tile_count == 0u) return vt;
+  const PrimaryHint hh = primary_hint(s, A, c);
   // phase 0: the hint window (when the history is valid); phase 1: the full
   // trace when phase 0 found nothing.  One call site keeps one copy of the walk.
-  ph.first_phase = hist_valid ? 0u : 1u;
+  ph.first_phase = hh.valid ? 0u : 1u;
   for (uint32_t phase = ph.first_phase;; ++phase) {
     const bool w = phase == 0u;
     ph.phase = phase;
     const VoxTraceResult h =
-        trace_candidates<PM>(s, cslot, cmeta, c.ro, c.rd, w ? t_start : 0.0f, w ? t_end : FOG_MAX_DIST,
-                         w && hak != INVALID, w ? hac : i3{0, 0, 0}, w ? hak : INVALID, tile_count, ph);
+        trace_candidates<PM>(s, cslot, cmeta, c.ro, c.rd, w ? hh.t_start : 0.0f, w ? hh.t_end : FOG_MAX_DIST,
+                             w && hh.anchor_key != INVALID, w ? hh.anchor_chunk : i3{0, 0, 0},
+                             w ? hh.anchor_key : INVALID, tile_count, ph);
     if (!w || h.best.hit != 0u) return h;
   }
 }
@@ -806,9 +833,41 @@ __device__ __forceinline__ unsigned long long slab_key(uint32_t phase, float t, 
          (unsigned long long)(it & 63u);
 }
 
-// Voxel walk with the grass column probes stored, not evaluated.  Pixels that
-// met no probe are final here; the rest wait for k_probe_dda, k_slab_eval,
-// k_slab_pick and k_primary_resolve.
+// The end of a pixel's walk in record mode: the voxel answer's PixHit, and
+// for pixels that met probes the walk summary (the rest is final).
+__device__ __forceinline__ void walk_finish(const FrameArgs& A, uint32_t pix, const VoxTraceResult& vt,
+                                            const ProbeHook& ph, uint32_t tile_count, bool* vox, bool* pend) {
+  *vox = vt.in_grid && vt.best.hit != 0u;
+  if (*vox) store_pixhit(A.pix_hit + (size_t)pix * 5u, vt.best, vt);
+  *pend = ph.seq != 0u;
+  if (*pend) {
+    // more probes than the summary counts: every stored one is still used,
+    // the pixel just walks again
+    const uint32_t stored = ph.seq > 0xFFFFFFu ? 0u : ph.recorded;
+    A.px_probe[pix] = make_uint2(probe_summary(ph.seq, ph.best_cand, ph.phase, ph.first_phase == 0u, *vox), stored);
+  } else {
+    profile_voxel(A, ph.first_phase, ph.phase, tile_count);  // the walk is the reference's (no probe met)
+  }
+}
+
+__device__ __forceinline__ ProbeHook probe_hook_record(const FrameArgs& A, uint32_t pix) {
+  ProbeHook ph = probe_hook_inline();
+  ph.mode = PROBE_RECORD;
+  ph.pixel = pix;
+  ph.recs = A.probe_recs;
+  ph.rec_count = &A.q_count[4];
+  ph.rec_cap = A.probe_cap;
+  return ph;
+}
+
+// Voxel walk with the grass column probes stored, not evaluated, in two
+// launches: this one runs the hint-window phase of the pixels whose history
+// is valid; pixels that need the full trace (no valid history, or nothing
+// found in the window) go to a queue that k_primary_trace_full walks with
+// full warps, so the long walks of a few pixels do not hold the warps of the
+// many that end in the window.  Pixels that met no probe are final after
+// their walk; the rest wait for k_probe_dda, k_slab_eval, k_slab_pick and
+// k_primary_resolve.
 __global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace(const __grid_constant__ FrameArgs A) {
   __shared__ uint32_t cslot[2][TILE_CANDS];
   __shared__ Meta cmeta[2][TILE_CANDS];
@@ -817,33 +876,70 @@ __global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace(const __grid_
   stage_tiles(s, A, cslot, cmeta, ccount);
   uint32_t t, gx, gy;
   const bool active = block_pixel(A, &t, &gx, &gy);
-  bool vox = false, pend = false;
+  bool vox = false, pend = false, full = false;
   uint32_t pix = 0u;
   if (active) {
     const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
     pix = (uint32_t)c.pix;
-    ProbeHook ph = probe_hook_inline();
-    ph.mode = PROBE_RECORD;
-    ph.pixel = pix;
-    ph.recs = A.probe_recs;
-    ph.rec_count = &A.q_count[4];
-    ph.rec_cap = A.probe_cap;
-    const VoxTraceResult vt = primary_trace<PROBE_RECORD>(s, A, c, cslot[t], cmeta[t], ccount[t], ph);
-    vox = vt.in_grid && vt.best.hit != 0u;
-    if (vox) store_pixhit(A.pix_hit + (size_t)pix * 5u, vt.best, vt);
-    pend = ph.seq != 0u;
-    if (pend) {
-      // more probes than the summary counts: every stored one is still used,
-      // the pixel just walks again
-      const uint32_t stored = ph.seq > 0xFFFFFFu ? 0u : ph.recorded;
-      A.px_probe[pix] = make_uint2(probe_summary(ph.seq, ph.best_cand, ph.phase, ph.first_phase == 0u, vox), stored);
-    } else {
-      profile_voxel(A, ph.first_phase, ph.phase, ccount[t]);  // the walk is the reference's (no probe met)
+    if (s.cam->chunk_count != 0u && ccount[t] != 0u) {
+      const PrimaryHint hh = primary_hint(s, A, c);
+      if (hh.valid) {
+        ProbeHook ph = probe_hook_record(A, pix);
+        ph.first_phase = 0u;
+        ph.phase = 0u;
+        const VoxTraceResult vt = trace_candidates<PROBE_RECORD>(s, cslot[t], cmeta[t], c.ro, c.rd, hh.t_start,
+                                                                 hh.t_end, hh.anchor_key != INVALID, hh.anchor_chunk,
+                                                                 hh.anchor_key, ccount[t], ph);
+        if (vt.best.hit != 0u) {
+          walk_finish(A, pix, vt, ph, ccount[t], &vox, &pend);
+        } else {
+          full = true;  // carry the probe count and the hint bit to the full trace
+          A.px_probe[pix] = make_uint2(ph.seq, ph.recorded | 0x80000000u);
+        }
+      } else {
+        full = true;
+        A.px_probe[pix] = make_uint2(0u, 0u);
+      }
     }
   }
   enqueue(A.q_vox, &A.q_count[0], active && vox && !pend, pix);
-  enqueue(A.q_far, &A.q_count[1], active && !vox && !pend, pix);
+  enqueue(A.q_far, &A.q_count[1], active && !vox && !pend && !full, pix);
   enqueue(A.q_pending, &A.q_count[5], active && pend, pix);
+  enqueue(A.q_full, &A.q_count[10], active && full, pix);
+}
+
+// The full-trace phase (phase 1) of the pixels k_primary_trace queued, one
+// lane each; the tile candidate lists and their metas come from global
+// memory (L1 / L2).
+__global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace_full(const __grid_constant__ FrameArgs A) {
+  const Scene s = make_scene(A, false);
+  const uint32_t n = A.q_count[10], end = warp_uniform_end(n);
+  const uint32_t tiles_x = (A.iw + 7u) / 8u;
+  for (uint32_t i = blockIdx.x * PRIMARY_THREADS + threadIdx.x; i < end; i += gridDim.x * PRIMARY_THREADS) {
+    const bool active = i < n;
+    bool vox = false, pend = false;
+    uint32_t pix = 0u;
+    if (active) {
+      pix = A.q_full[i];
+      const uint32_t gx = pix % A.iw, gy = pix / A.iw;
+      const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
+      const size_t tile = (size_t)(gy >> 3) * tiles_x + (gx >> 3);
+      const uint32_t tc = A.tile_count[tile];
+      const uint2 carry = A.px_probe[pix];
+      ProbeHook ph = probe_hook_record(A, pix);
+      ph.seq = carry.x;
+      ph.recorded = carry.y & 0x7FFFFFFFu;
+      ph.first_phase = (carry.y & 0x80000000u) != 0u ? 0u : 1u;
+      ph.phase = 1u;
+      const VoxTraceResult vt = trace_candidates<PROBE_RECORD>(s, A.tile_slots + tile * TILE_CANDS, nullptr, c.ro,
+                                                               c.rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID,
+                                                               tc, ph);
+      walk_finish(A, pix, vt, ph, tc, &vox, &pend);
+    }
+    enqueue(A.q_vox, &A.q_count[0], active && vox && !pend, pix);
+    enqueue(A.q_far, &A.q_count[1], active && !vox && !pend, pix);
+    enqueue(A.q_pending, &A.q_count[5], active && pend, pix);
+  }
 }
 
 // One lane per stored probe: the probe's column DDA with the walk's

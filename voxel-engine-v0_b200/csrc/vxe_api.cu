@@ -46,7 +46,7 @@ enum Img {
   IMG_GOD0, IMG_GOD1, IMG_PRE_TAA, IMG_OUTPUT, IMG_OHIST0, IMG_OHIST1, IMG_HITS, IMG_TILE_COUNT, IMG_TILE_SLOTS,
   IMG_PIXHIT, IMG_QVOX, IMG_QFAR, IMG_QCOUNT, IMG_QSHADOW, IMG_QLIGHT, IMG_PXSHADOW, IMG_PXLIGHT,
   IMG_PROBE_RECS, IMG_SLAB_TASKS, IMG_SLAB_RES, IMG_SLAB_HITS, IMG_PXFIRST, IMG_PXPROBE, IMG_PXMASK, IMG_PXTASK,
-  IMG_QPENDING,
+  IMG_QPENDING, IMG_QFULL,
   IMG_N
 };
 
@@ -290,6 +290,7 @@ size_t img_bytes(const FrameState& F, int i) {
     case IMG_PIXHIT:
       return in * 80;
     case IMG_QVOX: case IMG_QFAR: case IMG_QSHADOW: case IMG_QLIGHT: case IMG_PXSHADOW: case IMG_QPENDING:
+    case IMG_QFULL:
       return in * 4;
     case IMG_PROBE_RECS:
       return in * kProbesPerPixel * sizeof(vxe::dev::ProbeRec);
@@ -582,6 +583,7 @@ void frame_fill(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& cam, FrameArgs&
   A.px_task = (uint32_t*)S->img[IMG_PXTASK].p;
   A.px_mask = (uint2*)S->img[IMG_PXMASK].p;
   A.q_pending = (uint32_t*)S->img[IMG_QPENDING].p;
+  A.q_full = (uint32_t*)S->img[IMG_QFULL].p;
 }
 
 // The frame's launches on the compute stream (captured as-is by the graph
@@ -629,6 +631,7 @@ vxe_status frame_enqueue(vxe_ctx* c, FrameState& F, const FrameArgs& A, bool tim
     CK(cudaMemsetAsync(A.px_mask, 0, (size_t)npix * 8u, st));
     if (timed) CK(cudaEventRecord(F.ev[7], st));
     k_primary_trace<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, st>>>(A);
+    k_primary_trace_full<<<grid(npix), PRIMARY_THREADS, 0, st>>>(A);
     if (timed) CK(cudaEventRecord(F.ev[8], st));
     if (side) {  // the walk's far pixels shade beside the probe passes
       CK(cudaMemcpyAsync(A.q_count + 8, A.q_count + 1, 4, cudaMemcpyDeviceToDevice, st));
@@ -1463,6 +1466,7 @@ vxe_status vxe_get_frame_stats(vxe_ctx* c, vxe_frame_stats* out) {
   out->slab_tasks = q[6];
   out->slab_hits = q[7];
   out->rewalk_pixels = q[9];
+  out->full_trace_pixels = q[10];
   return VXE_OK;
 }
 
@@ -2339,6 +2343,53 @@ extern "C" vxe_status vxe_debug_detmath(int which, const float* x, const float* 
       st = VXE_ERR_DEVICE;
   }
   cudaFree(d);
+  return st;
+}
+
+// L2 read bandwidth: every thread reads 16-byte words of an L2-resident
+// buffer in a grid-stride loop (consecutive lanes, consecutive words), so
+// after the first pass each launch streams the buffer from L2.
+__global__ void __launch_bounds__(512) k_l2_read(const uint4* __restrict__ p, size_t n, uint32_t* sink) {
+  uint32_t acc = 0u;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const uint4 v = __ldcg(p + i);
+    acc ^= v.x ^ v.y ^ v.z ^ v.w;
+  }
+  if (acc == 0x9E3779B9u) sink[0] = acc;  // keeps the loads; the buffer is zero, so never taken
+}
+
+extern "C" vxe_status vxe_measure_l2_bandwidth(int device, uint64_t bytes, uint32_t launches, double* gbs) {
+  if (!gbs || bytes < (1u << 20) || launches == 0) return VXE_ERR_INVALID_ARG;
+  *gbs = 0.0;
+  if (cudaSetDevice(device) != cudaSuccess) return VXE_ERR_NO_DEVICE;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms <= 0)
+    return VXE_ERR_DEVICE;
+  void* buf = nullptr;
+  if (cudaMalloc(&buf, bytes + 256) != cudaSuccess) return VXE_ERR_OOM;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  vxe_status st = VXE_OK;
+  const size_t n = bytes / 16;
+  const unsigned grid = (unsigned)sms * 4u;  // 4 blocks of 512 threads per SM
+  uint32_t* sink = (uint32_t*)((char*)buf + bytes);
+  if (cudaMemset(buf, 0, bytes + 256) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+      cudaEventCreate(&e1) != cudaSuccess) {
+    st = VXE_ERR_DEVICE;
+  } else {
+    for (int w = 0; w < 3; ++w) k_l2_read<<<grid, 512>>>((const uint4*)buf, n, sink);  // resident in L2
+    cudaEventRecord(e0);
+    for (uint32_t i = 0; i < launches; ++i) k_l2_read<<<grid, 512>>>((const uint4*)buf, n, sink);
+    cudaEventRecord(e1);
+    float ms = 0.0f;
+    if (cudaGetLastError() != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess || ms <= 0.0f)
+      st = VXE_ERR_DEVICE;
+    else
+      *gbs = (double)(n * 16) * launches / (ms * 1e-3) / 1e9;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(buf);
   return st;
 }
 

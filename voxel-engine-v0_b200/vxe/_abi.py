@@ -171,7 +171,7 @@ PROFILE_VOXEL, PROFILE_GRASS, PROFILE_HDR, PROFILE_FOG, PROFILE_SHADOW = range(5
 
 class FrameStats(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in ("voxel_pixels", "far_pixels", "probes", "pending_pixels", "slab_tasks",
-                                           "slab_hits", "rewalk_pixels", "_pad")]
+                                           "slab_hits", "rewalk_pixels", "full_trace_pixels")]
 
 REQ_VIEWPORT, REQ_QUERY = 0, 1
 BATCH_PERSISTENT, BATCH_PLAIN, BATCH_GRAPH = 0, 1, 2
@@ -223,6 +223,7 @@ SIGNATURES = {
     "vxe_read_profile_counts": (C.c_int, [C.c_void_p, C.c_void_p]),
     "vxe_set_record_limits": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
     "vxe_get_frame_stats": (C.c_int, [C.c_void_p, P(FrameStats)]),
+    "vxe_measure_l2_bandwidth": (C.c_int, [C.c_int, C.c_uint64, C.c_uint32, P(C.c_double)]),
     "vxe_debug_detmath": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
     "vxe_trace_primary_hits_noalloc": (C.c_int, [P(SceneView), P(CameraGpu), P(ClipmapGpu), C.c_void_p,
                                                   C.c_void_p]),

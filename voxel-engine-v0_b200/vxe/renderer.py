@@ -76,14 +76,16 @@ class Renderer:
             C.memmove(C.byref(d.meta), u.meta.ctypes.data, 48)
             d.node_base = u.node_base
             if u.data is not None:
-                nodes = np.ascontiguousarray(u.data.nodes)
-                ropes = np.ascontiguousarray(u.data.ropes)
                 macro = np.ascontiguousarray(u.data.macro, dtype=np.uint32)
                 colinfo = np.ascontiguousarray(u.data.colinfo, dtype=np.uint32)
-                keep += [nodes, ropes, macro, colinfo]
-                d.node_count = len(nodes)
-                d.nodes, d.ropes = nodes.ctypes.data, ropes.ctypes.data
+                keep += [macro, colinfo]
                 d.macro_words, d.colinfo_words = macro.ctypes.data, colinfo.ctypes.data
+                if not u.rewrite:  # a slot rewrite leaves the node records where they are
+                    nodes = np.ascontiguousarray(u.data.nodes)
+                    ropes = np.ascontiguousarray(u.data.ropes)
+                    keep += [nodes, ropes]
+                    d.node_count = len(nodes)
+                    d.nodes, d.ropes = nodes.ctypes.data, ropes.ctypes.data
         self._check(self._lib.vxe_upload_chunks(self._ctx, arr, len(uploads)), "vxe_upload_chunks")
 
     def upload_world(self, world: World, uploads: list[Upload]) -> None:

@@ -20,7 +20,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi as A
-from .world import Clipmap, World, WorldSpec, build_camera, ground_height
+from .world import Clipmap, UploadQueue, World, WorldSpec, build_camera, ground_height
 
 
 @dataclass
@@ -145,21 +145,25 @@ SCENES = {"config1": config1, "config2": config2, "config5": config5, "features"
 class FrameDriver:
     """Produces per-frame inputs (uploads, grid, clipmap patches, camera) for a scene."""
 
-    def __init__(self, scene: Scene, device_renderer=None, mirror: bool = True, start_frame: int = 0):
+    def __init__(self, scene: Scene, device_renderer=None, mirror: bool = True, start_frame: int = 0,
+                 budgeted: bool = False):
         """`device_renderer`: keep the world on that renderer's device -- chunks
         built resident there, grid shifts by device slot moves (step() then
         returns no uploads and writes the grid itself).  `mirror`: the world
         keeps host copies of the node and rope arenas (World).  `start_frame`:
         the first path frame step() produces; the grid starts where the shifts
-        of the earlier frames left it (histories start empty)."""
+        of the earlier frames left it (histories start empty).  `budgeted`:
+        host streaming through the reference's per-frame upload budget
+        (UploadQueue.take_budgeted); chunks join the grid once uploaded."""
         self.scene = scene
         self.device = device_renderer
         self.last_shift = None  # (chunks built, slots moved) of the last device shift
         origin = tuple(scene.grid_origin)
         if scene.shift_every and start_frame > 0:
             origin = (origin[0] + (start_frame - 1) // scene.shift_every, origin[1], origin[2])
+        self.queue = UploadQueue() if budgeted else None
         self.world = World(scene.spec, origin, scene.grid_dims, scene.node_capacity,
-                           chunk_capacity=int(np.prod(scene.grid_dims)), mirror=mirror)
+                           chunk_capacity=int(np.prod(scene.grid_dims)), mirror=mirror, queue=self.queue)
         self.clip = Clipmap(scene.spec, scene.clip_levels, scene.clip_res, 1.0) if scene.clip_levels else None
         self.prev_vp = None
         self.frame = start_frame
@@ -168,7 +172,13 @@ class FrameDriver:
         if self.device is not None:
             self.world.populate_device(self.device)
             return []
-        return self.world.populate()
+        ups = self.world.populate()
+        if self.queue is not None:  # the first frame's budget would leave chunks out: take them all now
+            while len(self.queue):
+                part = self.queue.take_budgeted(self.world)
+                ups += part
+                self.world.mark_uploaded(part)
+        return ups
 
     def step(self):
         """Returns (uploads, grid_changed, clip (params, patches) or None, camera) for the next frame."""
@@ -181,6 +191,10 @@ class FrameDriver:
             else:
                 uploads = self.world.shift(1, 0, 0)
                 grid_changed = True
+        if self.queue is not None and len(self.queue):
+            uploads = self.queue.take_budgeted(self.world)
+            self.world.mark_uploaded(uploads)
+            grid_changed = True
         pos, yaw, pitch = sc.path(f)
         clip = None
         if self.clip is not None:
