@@ -223,9 +223,17 @@ def run_batch_serve(dev):
         for mode, name in [(A.BATCH_PLAIN, "plain"), (A.BATCH_PERSISTENT, "persistent"), (A.BATCH_GRAPH, "graph")]:
             ms = min(r.submit_batch(b.requests, (8, 4), 1, mode).ms for _ in range(3))
             out[name] = {"ms": round(ms, 3), "mrays_per_s": round(b.rays / ms / 1e3, 3)}
+        # the B200 schedule (deferred probes, finishing queues, coherent
+        # query order) one request at a time: separates the schedule's gain
+        # from the batching's
+        ms = min(sum(r.submit_batch([q], (8, 4), 1, A.BATCH_PERSISTENT).ms for q in b.requests) for _ in range(2))
+        out["per_request_b200_schedule"] = {"ms": round(ms, 3), "mrays_per_s": round(b.rays / ms / 1e3, 3)}
         batch = {"workload": "config-3 mix: 24 viewports + 40 query batches, seed 3", "rays": int(b.rays),
                  "tile": [8, 4], "rays_per_thread": 1, **out,
-                 "speedup_vs_plain": round(out["plain"]["ms"] / out["persistent"]["ms"], 3)}
+                 "plain": {**out["plain"], "mode": "one plain launch per request, the reference's inline probes"},
+                 "speedup_vs_plain": round(out["plain"]["ms"] / out["persistent"]["ms"], 3),
+                 "speedup_vs_per_request_b200_schedule":
+                     round(out["per_request_b200_schedule"]["ms"] / out["persistent"]["ms"], 3)}
         reqs = make_arrivals(w, 2000.0, 20, seed=1)
         serve(r, w, reqs, torch, mem_budget=4 << 30, lanes=2)  # warm-up
         # The served run depends on host timing (which arrivals share a batch):
@@ -265,6 +273,133 @@ def run_batch_serve(dev):
         return batch, srv
     finally:
         r.close()
+
+
+def run_serve_config4(dev, count: int = 120):
+    """Config 4: Poisson serving at 200 / 500 / 1000 / 2000 req/s (70 %
+    one-off viewports 256^2-1920x1080, 30 % query batches 1k-256k rays) over a
+    4096-chunk resident arena (32x4x32 chunks of the config-2 terrain, built on
+    the device), 10 chunk re-uploads per 16 ms tick on the upload stream,
+    admission by the device's free memory (cudaMemGetInfo) less 4 GiB.
+    Batched (continuous batching over 2 lanes) vs the plain one-request-at-a-
+    time server (one plain launch per request); median of 3 runs per rate."""
+    import torch
+
+    from vxe.renderer import Renderer
+    from vxe.scenes import config2
+    from vxe.serve import device_memory_budget, make_arrivals, serve, serve_plain
+    from vxe.world import World
+
+    sc = config2(present=(64, 36))
+    dims = (32, 4, 32)
+    w = World(sc.spec, (0, 0, 0), dims, 48 << 20, chunk_capacity=int(np.prod(dims)), mirror=False)
+    r = Renderer(64, 36, 1.0, node_capacity=w.node_capacity, chunk_capacity=w.chunk_capacity,
+                 grid_capacity=w.grid_capacity, clip_levels=sc.clip_levels, clip_res=sc.clip_res, device=dev)
+    out = {}
+    try:
+        w.populate_device(r)
+        w.prebuild(list(w.slot_to_key))  # host copies the re-uploads send
+        pos = np.array([102.4, 9.0, 102.4])
+        from vxe.world import build_camera
+
+        cam = build_camera(pos, 0.3, -0.1, (64, 36), (64, 36), frame_index=1, time_s=0.0, world=w, jitter=False)
+        r.write_camera(cam)
+        r.synchronize()
+        budget = device_memory_budget(torch, device=dev)
+        serve(r, w, make_arrivals(w, 2000.0, 20, seed=1), torch, mem_budget=budget, lanes=2)  # warm-up
+
+        def median_run(fn):
+            runs = sorted((fn() for _ in range(3)), key=lambda x: x.seconds)
+            return runs[1]
+
+        for rate in (200.0, 500.0, 1000.0, 2000.0):
+            rep = median_run(lambda: serve(r, w, make_arrivals(w, rate, count, seed=7), torch, mem_budget=budget,
+                                           lanes=2, max_batch=32))
+            base = median_run(lambda: serve_plain(r, w, make_arrivals(w, rate, count, seed=7), torch))
+            out[f"{int(rate)}_per_s"] = {"batched": rep.summary(), "plain": base.summary(),
+                                         "speedup_vs_plain": round(base.seconds / rep.seconds, 3)}
+        out["workload"] = (f"{count} Poisson requests per rate, 70 % viewports / 30 % query batches, 4096-chunk "
+                           "arena (32x4x32), 10 re-uploads per 16 ms tick, admission budget = free device memory "
+                           "- 4 GiB; median of 3 runs")
+        out["admission_budget_bytes"] = int(budget)
+    finally:
+        r.close()
+    return out
+
+
+def config5_with_queries(dev, frames: int = 128, seed: int = 5):
+    """Config 5 as specified: the 128-frame camera path over the 32x8x32-chunk
+    world at 3840x2160 present / 1920x1080 internal, with a served ray-query
+    batch of 64k-1M incoherent rays (log-uniform) issued on a batch lane
+    before each frame so the two overlap on the device.  Wall clock over the
+    whole run (every frame and batch complete when it stops)."""
+    import math
+
+    import torch
+
+    from vxe import _abi as A
+    from vxe import scenes
+    from vxe.renderer import Renderer
+    from vxe.scenes import FrameDriver
+
+    sc = scenes.config5()
+    cells = int(np.prod(sc.grid_dims))
+    r = Renderer(sc.present[0], sc.present[1], sc.render_scale, node_capacity=sc.node_capacity,
+                 chunk_capacity=cells, grid_capacity=cells, clip_levels=sc.clip_levels,
+                 clip_res=sc.clip_res, flags=A.FLAG_GODRAY_MACRO_ALIAS, device=dev)
+    rng = np.random.default_rng(seed)
+    try:
+        drv = FrameDriver(sc, device_renderer=r, mirror=False)  # the world built on the device
+        drv.initial_uploads()
+        w = drv.world
+        lo, hi = w.world_aabb_m()
+        # path frame 0 (the clipmap's first full build) untimed
+        _, _, clip, cam = drv.step()
+        r.write_clipmap_updates(*clip)
+        r.write_camera(cam)
+        r.encode_compute()
+        frames -= 1
+        batches = []
+        for _ in range(frames):
+            n = int(round(math.exp(rng.uniform(math.log(64e3), math.log(1e6)))))
+            o = rng.uniform(lo, hi, size=(n, 3)).astype(np.float32)
+            d = rng.normal(size=(n, 3))
+            d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+            to, td = torch.from_numpy(o).to(f"cuda:{dev}"), torch.from_numpy(d).to(f"cuda:{dev}")
+            res = torch.empty(n * 32, dtype=torch.uint8, device=f"cuda:{dev}")
+            q = A.Request()
+            q.kind, q.ray_count, q.tmax = A.REQ_QUERY, n, 120.0
+            q.d_origins, q.d_dirs, q.d_out = to.data_ptr(), td.data_ptr(), res.data_ptr()
+            batches.append((q, (to, td, res)))
+        torch.cuda.synchronize(dev)
+        frame_ms, q_rays = [], 0
+        t0 = time.perf_counter()
+        for f in range(frames):
+            uploads, grid_changed, clip, cam = drv.step()
+            if f > 0:
+                r.batch_wait(0, block=True)
+            q = batches[f][0]
+            r.submit_batch_async(0, [q], (8, 4), 1, A.BATCH_PERSISTENT)
+            q_rays += q.ray_count
+            r.write_clipmap_updates(*clip)
+            r.write_camera(cam)
+            r.encode_compute(sync=False)
+            frame_ms.append(r.read_gpu_timings_ms_blocking()["total"])
+        r.batch_wait(0, block=True)
+        r.synchronize()
+        dt = time.perf_counter() - t0
+        assert r.read_error_word() == 0
+    finally:
+        r.close()
+    frays = frames * sc.internal[0] * sc.internal[1]
+    return {"workload": "config5: 32x8x32 chunks (caves > 0.5), 6-level 512^2 clipmap, 3840x2160 present / "
+                        "1920x1080 internal, 128-frame path (frames 1..127 timed), one 64k-1M-ray query batch per "
+                        "frame on a lane",
+            "frames": frames, "frame_ms_mean": round(statistics.mean(frame_ms), 3),
+            "frame_ms_p99": round(float(np.percentile(frame_ms, 99)), 3),
+            "query_rays": int(q_rays), "frame_rays": int(frays), "seconds": round(dt, 4),
+            "mrays_per_s": round((frays + q_rays) / dt / 1e6, 3),
+            "note": "wall clock over the run; frame_ms from the context's events (the query batches overlap)"}
 
 
 def frame_series(sc, dev, steps: int, warmup: int, present=None):
@@ -371,6 +506,7 @@ def run_builder(dev, steps: int = 3, warmup: int = 2):
         counts = [r.build_chunks(wp, c, node_cap=0)["counts"] for c in parts]
         cap = int(max(int(c[:, 0].max()) for c in counts))
         solid = int(sum(int(c[:, 1].sum()) for c in counts))
+        working = int(sum(int((c[:, 1] > 0).sum()) for c in counts))  # all-air chunks return at once
         nodes_total = int(sum(int(c[:, 0].sum()) for c in counts))
         per = {"columns": [], "svo": []}
         for it in range(warmup + steps):
@@ -422,18 +558,20 @@ def run_builder(dev, steps: int = 3, warmup: int = 2):
     t0 = time.perf_counter()
     wh.prebuild(sample, threads=threads)
     host_s = time.perf_counter() - t0
-    # bytes the octree kernel must move per chunk: the 64^3 materials read,
-    # 32^3 level-5 state and offset words written and read back, node (16 B)
-    # and rope (32 B) records written
-    svo_bytes = len(keys) * (64 ** 3 + 32 ** 3 * 4 * 4 + 2048 * 4 + 16 * 4) + nodes_total * 48
+    # bytes the octree kernel must move per chunk that holds a solid voxel
+    # (an all-air chunk writes its lone air root and returns): the 64^3
+    # materials read, 32^3 level-5 state and offset words written and read
+    # back, colinfo and macro words, node (16 B) and rope (32 B) records written
+    svo_bytes = working * (64 ** 3 + 32 ** 3 * 4 * 4 + 2048 * 4 + 16 * 4) + nodes_total * 48
     return {
         "workload": "1024 chunks of the config-2 world (16x4x16, 64^3 voxels each)",
         "chunks_per_s": round(len(keys) / (dev_ms * 1e-3), 1),
         "device_ms": round(dev_ms, 3),
         "kernel_ms": {k: round(statistics.mean(v), 3) for k, v in per.items()},
         "steps": steps, "warmup": warmup,
-        "nodes_total": nodes_total, "solid_voxels": solid, "node_cap": cap,
+        "nodes_total": nodes_total, "solid_voxels": solid, "node_cap": cap, "chunks_with_solid_voxels": working,
         "svo_kernel_gbs": round(svo_bytes / (statistics.mean(per["svo"]) * 1e-3) / 1e9, 2),
+        "svo_kernel_gbs_note": "algorithmic bytes of the chunks holding solid voxels / k_build_svo time",
         "e2e": {"resident_chunks_per_s": round(len(keys) / statistics.median(res_s), 1),
                 "resident_seconds": round(statistics.median(res_s), 4),
                 "host_build_upload_chunks_per_s": round(len(keys) / statistics.median(host_s2), 1),
@@ -657,6 +795,48 @@ def cpu_sample(seconds: float, present, threads: int):
     return {"rays": rays, "seconds": elapsed, "frames": frames, "counters": ctr}
 
 
+def cpu_table(threads: int) -> dict:
+    """The oracle's rays/s on 1 host thread and on `threads`, bounded samples:
+    config 1 (one 64^3 chunk, 256x144 rays, cold full frames) and the config-2
+    1080p frame's primary pass over tile rows 30..37 (path frame 5, after four
+    warm frames on all threads)."""
+    from oracle import oracle as O
+    from vxe.scenes import FrameDriver, config1, config2
+
+    out = {}
+    sc = config1()
+    drv = FrameDriver(sc)
+    drv.initial_uploads()
+    _, _, _, cam = drv.step()
+    clip = drv.empty_clip()
+    row = {}
+    for nt in (1, threads):
+        runner = O.OracleFrameRunner(drv.world, sc.internal, sc.present, None, sc.clip_res)
+        frames, t0 = 0, time.perf_counter()
+        while frames < 3 or time.perf_counter() - t0 < 1.0:
+            runner.ping = 0  # cold frames
+            runner.render(cam, clip, threads=nt)
+            frames += 1
+        dt = time.perf_counter() - t0
+        row[f"{nt}_threads"] = round(frames * sc.internal[0] * sc.internal[1] / dt / 1e6, 4)
+    out["config1_full_frame_mrays_per_s"] = row
+    sc = config2()
+    drv = FrameDriver(sc)
+    drv.initial_uploads()
+    runner = O.OracleFrameRunner(drv.world, sc.internal, sc.present, drv.clip.tex, sc.clip_res)
+    for _ in range(5):
+        _, _, clip, cam = drv.step()
+        runner.render(cam, clip[0], threads=threads)
+    _, _, clip, cam = drv.step()
+    row = {}
+    for nt in (1, threads):
+        t0 = time.perf_counter()
+        rays = runner.primary_rows(cam, clip[0], 30, 38, threads=nt)
+        row[f"{nt}_threads"] = round(rays / (time.perf_counter() - t0) / 1e6, 4)
+    out["config2_1080p_primary_rows_30_37_mrays_per_s"] = row
+    return out
+
+
 def record_bytes(c: dict) -> int:
     """Full record sizes of the loads the oracle counted: node 16, rope 32, meta 48, grid / macro / colinfo
     words and clip texels 4."""
@@ -734,7 +914,9 @@ def main():
     batch = srv = configs = None
     if not args.no_batch and world_size == 1:  # one GPU: the batched, served, secondary-config and builder lines
         batch, srv = run_batch_serve(0)
+        srv["config4"] = run_serve_config4(0)
         configs = run_configs(0)
+        configs["config5_with_queries"] = config5_with_queries(0)
         configs["clipmap_patches"] = run_clipmap(0)
         configs["chunk_builder"] = run_builder(0)
     if world_size > 1:
@@ -796,7 +978,8 @@ def main():
         cs = cpu_sample(args.cpu_seconds, present, threads)
         line["cpu_baseline"] = {"value": round(cs["rays"] / cs["seconds"] / 1e6, 4), "unit": UNIT, "cores": threads,
                                 "kind": "port",
-                                "sample": f"{cs['frames']} full frames of the same workload (path frames 0..{cs['frames'] - 1})"}
+                                "sample": f"{cs['frames']} full frames of the same workload (path frames 0..{cs['frames'] - 1})",
+                                "table": cpu_table(threads)}
         tb = algorithmic_trace_bytes(cs["counters"][2], res["rays_per_frame"])
         achieved = tb / trace_s / 1e9
         roof.update({"achieved": round(achieved, 2), "frac": round(achieved / peak, 5),

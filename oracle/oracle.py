@@ -156,6 +156,27 @@ class OracleFrameRunner:
         assert rc == 0
         self.ping = q
 
+    def primary_rows(self, cam, clip_params, tile_y0: int, tile_y1: int, threads: int | None = None) -> int:
+        """The primary pass (with local TAA) over tile rows [tile_y0, tile_y1)
+        only, without touching the histories' ping-pong; returns the rays
+        traced.  For bounded CPU timings."""
+        p, q = self.ping, 1 - self.ping
+        io = FrameIO(self.iw, self.ih, self.pw, self.ph)
+        io.primary_hist_in = self.hist[p].ctypes.data
+        io.shadow_in = self.shadow[p].ctypes.data
+        io.local_hist_in = self.lhist[p].ctypes.data
+        io.color, io.depth, io.local = self.color.ctypes.data, self.depth.ctypes.data, self.local.ctypes.data
+        io.primary_hist_out = self.hist[q].ctypes.data
+        io.shadow_out = self.shadow[q].ctypes.data
+        io.local_hist_out = self.lhist[q].ctypes.data
+        sc = self.scene(cam, clip_params)
+        ctr = OraCounters()
+        rc = lib().ora_primary_rows(C.byref(sc), C.byref(io), tile_y0, tile_y1, threads or default_threads(),
+                                    C.byref(ctr))
+        assert rc == 0
+        y0, y1 = min(tile_y0 * 8, self.ih), min(tile_y1 * 8, self.ih)
+        return (y1 - y0) * self.iw
+
     # Frame outputs after render() (the "IN" buffers of the next frame).
     def outputs(self) -> dict:
         p = self.ping

@@ -432,14 +432,17 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_probe_dda(const __grid_
     const Meta ch = meta_at(s, r.slot);
     const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vs;
     const i3 ov{ch.ox, ch.oy, ch.oz};
-    bool lost = r.seq > 0xFFFFFu;
+    bool lost = probe_seq(r) == PROBE_SEQ_LOST;
     grass_columns_dda(s, ro, rd, safe_inv3(rd), r.t0, r.t1, rb, ov, vs, ch.colinfo_base,
                       [&](uint32_t it, float t, float tNext, v3 id) {
+                        // the part of the column step inside the cell's grass
+                        // slab (try_grass_slab_hit's first step): an empty one
+                        // is no task
+                        const v2 iv = grass_slab_interval(ro, rd, t, tNext, id * vs, vs);
+                        if (iv.y <= iv.x) return false;
                         const uint32_t j = atomicAdd(&B.dcount[2], 1u);
                         if (j < B.slab_cap) {
-                          B.slab_tasks[2u * j] = make_uint4(i, it, __float_as_uint(t), __float_as_uint(tNext));
-                          B.slab_tasks[2u * j + 1u] = make_uint4(__float_as_uint(id.x), __float_as_uint(id.y),
-                                                                 __float_as_uint(id.z), 0u);
+                          B.slab_tasks[j] = slab_task(i, it, iv.x, iv.y, id, ch);
                         } else {
                           lost = true;
                         }
@@ -453,24 +456,25 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_slab_eval(const __grid_
   const uint32_t n_reqs = B.hdr->n_reqs;
   const uint32_t n = min(B.dcount[2], B.slab_cap);
   for (uint32_t j = blockIdx.x * BATCH_THREADS + threadIdx.x; j < n; j += gridDim.x * BATCH_THREADS) {
-    const uint4 a = B.slab_tasks[2u * j], b = B.slab_tasks[2u * j + 1u];
+    const uint4 a = B.slab_tasks[j];
     const ProbeRec r = B.probe_recs[a.x];
     const BatchRay br = batch_ray(B, n_reqs, r.pixel);
     const Scene s = batch_scene(B, &B.cams[br.q->cam]);
     const float vs = vs_(s);
     const v3 ro = cam_pos(s);
     const v3 rd = ray_dir_from_pixel(s, V2((float)br.gx + 0.5f, (float)br.gy + 0.5f));
-    const v3 id = V3(__uint_as_float(b.x), __uint_as_float(b.y), __uint_as_float(b.z));
-    const GrassHit gh = try_grass_slab_hit(s, ro, rd, __uint_as_float(a.z), __uint_as_float(a.w), id * vs, id, vs,
-                                           s.cam->voxel_params[1], s.cam->voxel_params[2]);
+    const v3 id = slab_task_cell(a, meta_at(s, r.slot));
+    const float t0 = __uint_as_float(a.z);  // the slab interval (non-empty)
+    const GrassHit gh = grass_layer_trace_lod(s, ro, rd, t0, __uint_as_float(a.w), id * vs, id, s.cam->voxel_params[1],
+                                              s.cam->voxel_params[2], grass_lod_from_t(t0));
     if (gh.hit) {
       if (__float_as_uint(gh.t) & 0x80000000u) {
         atomicMin(&B.px_probe[r.pixel].y, 0u);
         continue;
       }
-      const uint32_t cand = r.cand_phase & 0xFFu, phase = r.cand_phase >> 8;
+      const uint32_t cand = probe_cand(r), phase = probe_phase(r);
       B.slab_res[j] = make_float4(gh.t, gh.n.x, gh.n.y, gh.n.z);
-      atomicMin(&B.px_first[r.pixel], slab_key(phase, gh.t, cand, r.seq, a.y));
+      atomicMin(&B.px_first[r.pixel], slab_key(phase, gh.t, cand, probe_seq(r), slab_task_step(a)));
       atomicOr(phase ? &B.px_mask[r.pixel].y : &B.px_mask[r.pixel].x, 1u << (cand & 31u));
       B.slab_hits[atomicAdd(&B.dcount[3], 1u)] = j;
     }
@@ -481,9 +485,9 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_slab_pick(const __grid_
   const uint32_t n = min(B.dcount[3], B.slab_cap);
   for (uint32_t i = blockIdx.x * BATCH_THREADS + threadIdx.x; i < n; i += gridDim.x * BATCH_THREADS) {
     const uint32_t j = B.slab_hits[i];
-    const uint4 a = B.slab_tasks[2u * j];
+    const uint4 a = B.slab_tasks[j];
     const ProbeRec r = B.probe_recs[a.x];
-    const unsigned long long key = slab_key(r.cand_phase >> 8, B.slab_res[j].x, r.cand_phase & 0xFFu, r.seq, a.y);
+    const unsigned long long key = slab_key(probe_phase(r), B.slab_res[j].x, probe_cand(r), probe_seq(r), slab_task_step(a));
     const unsigned long long first = B.px_first[r.pixel];
     if (key == first) B.px_task[r.pixel] = j;
     else if (slab_hit_shadows_first(first, key)) atomicMin(&B.px_probe[r.pixel].y, 0u);
@@ -509,8 +513,8 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_resolve(const __grid_co
     if (!walk && first != ~0ull) {
       const uint32_t j = B.px_task[ray];
       const float4 res = B.slab_res[j];
-      const ProbeRec r = B.probe_recs[B.slab_tasks[2u * j].x];
-      const uint32_t pcand = r.cand_phase & 0xFFu, pphase = r.cand_phase >> 8;
+      const ProbeRec r = B.probe_recs[B.slab_tasks[j].x];
+      const uint32_t pcand = probe_cand(r), pphase = probe_phase(r);
       bool probe_wins = true;
       if (vox && pphase == vphase) {
         const float vt = __uint_as_float(B.px_hit[(size_t)ray * 4u].x);

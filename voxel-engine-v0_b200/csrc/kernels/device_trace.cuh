@@ -1189,14 +1189,40 @@ enum : uint32_t { PROBE_INLINE = 0u, PROBE_RECORD = 1u };
 // kernel holds only the probe code it runs; PROBE_DYNAMIC reads ph.mode.
 constexpr uint32_t PROBE_DYNAMIC = 2u;
 
-struct ProbeRec {  // 56 B
-  uint32_t pixel, seq, slot;
+// A stored probe: three 16-byte words, written and read as vectors.
+struct __align__(16) ProbeRec {
+  uint32_t pixel, slot;
   float t0, t1;
-  uint32_t cand_phase;  // candidate index | trace phase << 8 (0 hint window, 1 full)
+  uint32_t tag;         // probe order (20 bits; PROBE_SEQ_LOST: beyond what it counts) | candidate index << 20
+                        // | trace phase << 25 (0 hint window, 1 full) | anchor valid << 26
   uint32_t node;        // hit-record leaf node (INVALID: implicit leaf)
-  float leaf_bmin[3], leaf_size;
-  uint32_t anchor_valid, anchor_key;
+  uint32_t anchor_key;
+  float leaf_size;
+  float leaf_bmin[3];
+  uint32_t _pad;
 };
+constexpr uint32_t PROBE_SEQ_LOST = 0xFFFFFu;
+
+// A grass slab to march (16 B): its probe, the column (x, z within the
+// probe's chunk, the column top's y within the chunk) and the column DDA
+// step, and the part of the step's interval inside the slab
+// (grass_slab_interval).  The cell id is the chunk origin + those offsets,
+// the same integers the column DDA converted.
+__device__ __forceinline__ uint4 slab_task(uint32_t probe, uint32_t it, float t, float t_next, v3 id, const Meta& ch) {
+  const uint32_t lx = (uint32_t)((int32_t)id.x - ch.ox), ly = (uint32_t)((int32_t)id.y - ch.oy),
+                 lz = (uint32_t)((int32_t)id.z - ch.oz);
+  return make_uint4(probe, (lx & 63u) | ((lz & 63u) << 6) | ((ly & 63u) << 12) | ((it & 63u) << 18),
+                    __float_as_uint(t), __float_as_uint(t_next));
+}
+__device__ __forceinline__ uint32_t slab_task_step(const uint4& a) { return (a.y >> 18) & 63u; }
+__device__ __forceinline__ v3 slab_task_cell(const uint4& a, const Meta& ch) {
+  return V3((float)(ch.ox + (int32_t)(a.y & 63u)), (float)(ch.oy + (int32_t)((a.y >> 12) & 63u)),
+            (float)(ch.oz + (int32_t)((a.y >> 6) & 63u)));
+}
+__device__ __forceinline__ uint32_t probe_seq(const ProbeRec& r) { return r.tag & 0xFFFFFu; }
+__device__ __forceinline__ uint32_t probe_cand(const ProbeRec& r) { return (r.tag >> 20) & 31u; }
+__device__ __forceinline__ uint32_t probe_phase(const ProbeRec& r) { return (r.tag >> 25) & 1u; }
+__device__ __forceinline__ bool probe_anchor_valid(const ProbeRec& r) { return ((r.tag >> 26) & 1u) != 0u; }
 
 struct ProbeHook {
   uint32_t mode;
@@ -1241,21 +1267,12 @@ __device__ __forceinline__ void probe_record(ProbeHook& ph, float t0, float t1, 
   base = __shfl_sync(mask, base, leader);
   const uint32_t idx = base + (uint32_t)__popc(mask & ((1u << lane) - 1u));
   if (idx < ph.rec_cap) {
-    ProbeRec r;
-    r.pixel = ph.pixel;
-    r.seq = ph.seq;
-    r.slot = ph.slot;
-    r.t0 = t0;
-    r.t1 = t1;
-    r.cand_phase = ph.cand | (ph.phase << 8);
-    r.node = node;
-    r.leaf_bmin[0] = leaf_bmin.x;
-    r.leaf_bmin[1] = leaf_bmin.y;
-    r.leaf_bmin[2] = leaf_bmin.z;
-    r.leaf_size = leaf_size;
-    r.anchor_valid = anchor_valid ? 1u : 0u;
-    r.anchor_key = anchor_key;
-    ph.recs[idx] = r;
+    const uint32_t tag = min(ph.seq, PROBE_SEQ_LOST) | ((ph.cand & 31u) << 20) | ((ph.phase & 1u) << 25) |
+                         (anchor_valid ? (1u << 26) : 0u);
+    uint4* d = reinterpret_cast<uint4*>(ph.recs + idx);
+    d[0] = make_uint4(ph.pixel, ph.slot, __float_as_uint(t0), __float_as_uint(t1));
+    d[1] = make_uint4(tag, node, anchor_key, __float_as_uint(leaf_size));
+    d[2] = make_uint4(__float_as_uint(leaf_bmin.x), __float_as_uint(leaf_bmin.y), __float_as_uint(leaf_bmin.z), 0u);
     ++ph.recorded;
   }
 }

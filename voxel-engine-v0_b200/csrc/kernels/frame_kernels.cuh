@@ -71,7 +71,7 @@ struct FrameArgs {
   // -> k_slab_pick -> k_primary_resolve)
   ProbeRec* probe_recs;           // stored probes, q_count[4] of them (capped)
   uint32_t probe_cap;
-  uint4* slab_tasks;              // 2 x uint4 per grass column slab to march, q_count[6] of them
+  uint4* slab_tasks;              // one uint4 (slab_task) per grass column slab to march, q_count[6] of them
   float4* slab_res;               // per slab task: hit t, normal (written on hits)
   uint32_t* slab_hits;            // slab tasks that hit, q_count[7] of them
   uint32_t slab_cap;
@@ -955,14 +955,17 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_probe_dda(const __grid_consta
     const Meta ch = meta_at(s, r.slot);
     const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vs;
     const i3 ov{ch.ox, ch.oy, ch.oz};
-    bool lost = r.seq > 0xFFFFFu;
+    bool lost = probe_seq(r) == PROBE_SEQ_LOST;
     grass_columns_dda(s, c.ro, c.rd, safe_inv3(c.rd), r.t0, r.t1, rb, ov, vs, ch.colinfo_base,
                       [&](uint32_t it, float t, float tNext, v3 id) {
+                        // the part of the column step inside the cell's grass
+                        // slab (try_grass_slab_hit's first step): an empty one
+                        // is no task
+                        const v2 iv = grass_slab_interval(c.ro, c.rd, t, tNext, id * vs, vs);
+                        if (iv.y <= iv.x) return false;
                         const uint32_t j = atomicAdd(&A.q_count[6], 1u);
                         if (j < A.slab_cap) {
-                          A.slab_tasks[2u * j] = make_uint4(i, it, __float_as_uint(t), __float_as_uint(tNext));
-                          A.slab_tasks[2u * j + 1u] = make_uint4(__float_as_uint(id.x), __float_as_uint(id.y),
-                                                                 __float_as_uint(id.z), 0u);
+                          A.slab_tasks[j] = slab_task(i, it, iv.x, iv.y, id, ch);
                         } else {
                           lost = true;
                         }
@@ -980,20 +983,21 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_slab_eval(const __grid_consta
   const float vs = vs_(s);
   const float time_s = s.cam->voxel_params[1], strength = s.cam->voxel_params[2];
   for (uint32_t j = blockIdx.x * SHADE_THREADS + threadIdx.x; j < n; j += gridDim.x * SHADE_THREADS) {
-    const uint4 a = A.slab_tasks[2u * j], b = A.slab_tasks[2u * j + 1u];
+    const uint4 a = A.slab_tasks[j];
     const ProbeRec r = A.probe_recs[a.x];
     const PrimaryCtx c = primary_ctx(s, r.pixel % A.iw, r.pixel / A.iw, A.iw);
-    const v3 id = V3(__uint_as_float(b.x), __uint_as_float(b.y), __uint_as_float(b.z));
-    const GrassHit gh = try_grass_slab_hit(s, c.ro, c.rd, __uint_as_float(a.z), __uint_as_float(a.w), id * vs, id, vs,
-                                           time_s, strength);
+    const v3 id = slab_task_cell(a, meta_at(s, r.slot));
+    const float t0 = __uint_as_float(a.z);  // the slab interval (non-empty)
+    const GrassHit gh = grass_layer_trace_lod(s, c.ro, c.rd, t0, __uint_as_float(a.w), id * vs, id, time_s, strength,
+                                              grass_lod_from_t(t0));
     if (gh.hit) {
       if (__float_as_uint(gh.t) & 0x80000000u) {  // not ordered by the key: walk again
         atomicMin(&A.px_probe[r.pixel].y, 0u);
         continue;
       }
-      const uint32_t cand = r.cand_phase & 0xFFu, phase = r.cand_phase >> 8;
+      const uint32_t cand = probe_cand(r), phase = probe_phase(r);
       A.slab_res[j] = make_float4(gh.t, gh.n.x, gh.n.y, gh.n.z);
-      atomicMin(&A.px_first[r.pixel], slab_key(phase, gh.t, cand, r.seq, a.y));
+      atomicMin(&A.px_first[r.pixel], slab_key(phase, gh.t, cand, probe_seq(r), slab_task_step(a)));
       atomicOr(phase ? &A.px_mask[r.pixel].y : &A.px_mask[r.pixel].x, 1u << (cand & 31u));
       A.slab_hits[atomicAdd(&A.q_count[7], 1u)] = j;
     }
@@ -1017,10 +1021,10 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_slab_pick(const __grid_consta
   const uint32_t n = min(A.q_count[7], A.slab_cap);
   for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < n; i += gridDim.x * SHADE_THREADS) {
     const uint32_t j = A.slab_hits[i];
-    const uint4 a = A.slab_tasks[2u * j];
+    const uint4 a = A.slab_tasks[j];
     const ProbeRec r = A.probe_recs[a.x];
     const unsigned long long key =
-        slab_key(r.cand_phase >> 8, A.slab_res[j].x, r.cand_phase & 0xFFu, r.seq, a.y);
+        slab_key(probe_phase(r), A.slab_res[j].x, probe_cand(r), probe_seq(r), slab_task_step(a));
     const unsigned long long first = A.px_first[r.pixel];
     if (key == first) A.px_task[r.pixel] = j;
     else if (slab_hit_shadows_first(first, key)) atomicMin(&A.px_probe[r.pixel].y, 0u);
@@ -1050,8 +1054,8 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_primary_resolve(const __grid_
       if (!walk && first != ~0ull) {
         const uint32_t j = A.px_task[pix];
         const float4 res = A.slab_res[j];
-        const ProbeRec r = A.probe_recs[A.slab_tasks[2u * j].x];
-        const uint32_t pcand = r.cand_phase & 0xFFu, pphase = r.cand_phase >> 8;
+        const ProbeRec r = A.probe_recs[A.slab_tasks[j].x];
+        const uint32_t pcand = probe_cand(r), pphase = probe_phase(r);
         bool probe_wins = true;
         if (vox && pphase == vphase) {
           const float vt = __uint_as_float(A.pix_hit[(size_t)pix * 5u].x);
@@ -1065,7 +1069,7 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_primary_resolve(const __grid_
           const int32_t csz = (int32_t)s.cam->chunk_size;
           const HitGeom g = make_hit(MAT_GRASS, res.x, V3(res.y, res.z, res.w), rb, rs, ch, r.node,
                                      V3(r.leaf_bmin[0], r.leaf_bmin[1], r.leaf_bmin[2]), r.leaf_size);
-          const VoxTraceResult vr{true, g, 0.0f, r.anchor_valid != 0u, r.anchor_key,
+          const VoxTraceResult vr{true, g, 0.0f, probe_anchor_valid(r), r.anchor_key,
                                   i3{ch.ox / csz, ch.oy / csz, ch.oz / csz}};
           store_pixhit(A.pix_hit + (size_t)pix * 5u, g, vr);
           vox = true;

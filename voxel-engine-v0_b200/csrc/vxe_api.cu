@@ -295,7 +295,7 @@ size_t img_bytes(const FrameState& F, int i) {
     case IMG_PROBE_RECS:
       return in * kProbesPerPixel * sizeof(vxe::dev::ProbeRec);
     case IMG_SLAB_TASKS:
-      return in * kSlabsPerPixel * 32;
+      return in * kSlabsPerPixel * 16;
     case IMG_SLAB_RES:
       return in * kSlabsPerPixel * 16;
     case IMG_SLAB_HITS:
@@ -575,7 +575,7 @@ void frame_fill(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& cam, FrameArgs&
   if (c->probe_limit) A.probe_cap = std::min(A.probe_cap, c->probe_limit);
   A.slab_tasks = (uint4*)S->img[IMG_SLAB_TASKS].p;
   A.slab_res = (float4*)S->img[IMG_SLAB_RES].p;
-  A.slab_cap = (uint32_t)std::min<size_t>(S->img[IMG_SLAB_TASKS].bytes / 32u, 0xFFFFFFFFu);
+  A.slab_cap = (uint32_t)std::min<size_t>(S->img[IMG_SLAB_TASKS].bytes / 16u, 0xFFFFFFFFu);
   if (c->slab_limit) A.slab_cap = std::min(A.slab_cap, c->slab_limit);
   A.px_first = (unsigned long long*)S->img[IMG_PXFIRST].p;
   A.px_probe = (uint2*)S->img[IMG_PXPROBE].p;
@@ -1849,7 +1849,7 @@ vxe_status lane_resources(vxe_ctx* c, BatchLane& L, uint32_t tiles, uint32_t vp_
     if ((st = alloc_on(c, L.q_refine, cap * 4, L.stream)) != VXE_OK) return st;
     if ((st = alloc_on(c, L.q_far, cap * 4, L.stream)) != VXE_OK) return st;
     if ((st = alloc_on(c, L.probe_recs, cap * kBatchProbesPerRay * sizeof(vxe::dev::ProbeRec), L.stream)) != VXE_OK) return st;
-    if ((st = alloc_on(c, L.slab_tasks, cap * kBatchSlabsPerRay * 32, L.stream)) != VXE_OK) return st;
+    if ((st = alloc_on(c, L.slab_tasks, cap * kBatchSlabsPerRay * 16, L.stream)) != VXE_OK) return st;
     if ((st = alloc_on(c, L.slab_res, cap * kBatchSlabsPerRay * 16, L.stream)) != VXE_OK) return st;
     if ((st = alloc_on(c, L.slab_hits, cap * kBatchSlabsPerRay * 4, L.stream)) != VXE_OK) return st;
     if (!L.dcount.p && (st = alloc_on(c, L.dcount, 32, L.stream)) != VXE_OK) return st;

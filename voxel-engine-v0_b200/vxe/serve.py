@@ -14,7 +14,8 @@ uniform directions).  A render request is either
 The server loop
 
   * admits waiting requests in arrival order while their device footprint fits
-    the memory budget: a session's view (its history footprint: 5 RGBA32F +
+    the memory budget (by default the device's free memory at start, from
+    cudaMemGetInfo, less a reserve): a session's view (its history footprint: 5 RGBA32F +
     2 R32F at internal size and 2 RGBA32F at present size, plus scratch) is
     created when the session is first admitted and stays until memory is
     needed by another session (least recently used idle view first); a
@@ -242,7 +243,10 @@ def _reupload(renderer, world, resident, rng, count):
         key = resident[int(i)]
         slot = world.key_to_slot[key]
         base, _ = world.alloc[key]
-        ups.append(Upload(slot, world.metas[slot].copy(), base, world.chunk(key)))
+        data = world.chunk(key)
+        # the meta from the slot's bookkeeping (a world built on the device
+        # keeps no host meta records)
+        ups.append(Upload(slot, world._meta_for(slot, key, base, data), base, data, key=key))
     renderer.apply_chunk_uploads(ups)
     return len(ups)
 
@@ -255,9 +259,19 @@ def _frame_camera(world, sessions, r: SRequest):
     return cam
 
 
-def serve(renderer, world: World, requests, torch, mem_budget: int, lanes: int = 2, tile=(8, 4), rpt: int = 1,
+def device_memory_budget(torch, reserve: int = 4 << 30, device: int = 0) -> int:
+    """Admission budget from the device's free memory (cudaMemGetInfo) less a
+    reserve for everything the server does not count (the context's lanes
+    growing, the allocator's slack)."""
+    free, _total = torch.cuda.mem_get_info(device)
+    return max(0, int(free) - int(reserve))
+
+
+def serve(renderer, world: World, requests, torch, mem_budget: int | None, lanes: int = 2, tile=(8, 4), rpt: int = 1,
           max_batch: int = 64, reuploads_per_tick: int = 10, tick_s: float = 0.016, keep_outputs: bool = False,
           mode: int = A.BATCH_PERSISTENT, sessions=None) -> ServeReport:
+    if mem_budget is None:
+        mem_budget = device_memory_budget(torch, device=renderer.device)
     reqs = sorted(requests, key=lambda r: r.arrival)
     pending = deque(reqs)
     waiting = deque()
@@ -342,6 +356,7 @@ def serve(renderer, world: World, requests, torch, mem_budget: int, lanes: int =
     lat = [(r.done - r.arrival) * 1e3 for r in reqs]
     extra = ({"views_created": views.created, "view_evictions": views.evictions, "lane_bytes": lane_bytes}
              if sessions else {})
+    extra["admission_budget_bytes"] = int(mem_budget)
     return ServeReport(lat, sum(r.rays for r in reqs), seconds, batches, max_inflight, uploads, extra)
 
 
