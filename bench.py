@@ -255,20 +255,30 @@ def run_batch_serve(dev):
         for rate in (1000.0, 200.0):
             def sess_served():
                 ss = make_sessions(w, 16, seed=3)
-                return serve(r, w, make_arrivals(w, rate, 160, seed=7, sessions=ss), torch, mem_budget=6 << 30,
+                return serve(r, w, make_arrivals(w, rate, 160, seed=7, sessions=ss), torch, mem_budget=None,
                              lanes=2, max_batch=16, sessions=ss)
 
             def sess_plain():
                 ss = make_sessions(w, 16, seed=3)
                 return serve_plain(r, w, make_arrivals(w, rate, 160, seed=7, sessions=ss), torch, sessions=ss)
 
+            def sess_single_launch():
+                ss = make_sessions(w, 16, seed=3)
+                return serve_plain(r, w, make_arrivals(w, rate, 160, seed=7, sessions=ss), torch, sessions=ss,
+                                   single_launch_pass=True)
+
             rep, _ = median_run(sess_served)
             base, _ = median_run(sess_plain)
+            single = sess_single_launch()
             sess[f"{int(rate)}_per_s"] = {"batched": rep.summary(), "plain": base.summary(),
-                                          "speedup_vs_plain": round(base.seconds / rep.seconds, 3)}
+                                          "plain_single_launch_pass": single.summary(),
+                                          "speedup_vs_plain": round(base.seconds / rep.seconds, 3),
+                                          "speedup_vs_plain_single_launch_pass": round(single.seconds / rep.seconds, 3)}
         srv["sessions"] = {"workload": "160 Poisson requests, 70 % frames of 16 sessions (256^2-1920x1080 "
                                        "present at render scale 0.5, histories resident) / 30 % query batches; "
-                                       "median of 3 runs",
+                                       "median of 3 runs; plain = one request at a time in the wavefront "
+                                       "schedule, plain_single_launch_pass = one request at a time, one kernel "
+                                       "per pass (one run)",
                            **sess}
         return batch, srv
     finally:
@@ -951,10 +961,10 @@ def main():
                         "host buffers; every output lands inside the timed region)",
                 "serial_frame_ms": round(res["e2e"]["serial_seconds"] * 1e3 / args.steps, 3),
                 "device_streaming": device_streaming_line(res["e2e"], args.steps, n)},
-        # per frame: k_grass_cells, k_tiles, k_primary_trace, k_primary_trace_full, k_probe_dda, k_slab_eval,
-        # k_slab_pick, k_primary_resolve, k_shade_prep, k_shade_shadow, k_shade_lights, k_shade_vox,
-        # k_shade_far x 2 (side stream), k_godray, k_composite
-        "gpu_launches": 16 * args.steps,
+        # per frame: k_grass_cells, k_tiles, k_primary_trace, k_probe_dda, k_slab_eval, k_slab_pick,
+        # k_primary_resolve, k_shade_prep, k_shade_shadow, k_shade_lights, k_shade_vox, k_shade_far x 2 (side
+        # stream), k_godray, k_composite
+        "gpu_launches": 15 * args.steps,
         "batch": batch,
         "serve": srv,
         "configs": configs,

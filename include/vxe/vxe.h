@@ -14,6 +14,21 @@
  *  - Host pointers are borrowed for the duration of the call only.
  *  - Device pointers returned in vxe_frame_out stay valid until the next
  *    vxe_render_frame / vxe_resize / vxe_destroy on the same ctx.
+ *
+ * Device bounds checks
+ *  The passes read node, rope, meta, grid, macro, colinfo and clipmap
+ *  records at indices taken from other records.  Two builds of this library
+ *  export the same entry points and differ only in those reads:
+ *  - libvxe.so clamps every such index into its buffer: never a read outside
+ *    the buffers, no branch on the traversal's hot path (the reads of the
+ *    traversal are about half its kernel time otherwise); records that point
+ *    outside their chunk give wrong images and no error report;
+ *  - libvxe_checked.so reads a zero record for an index outside its buffer
+ *    and sets a bit of the context's error word (vxe_read_error_word;
+ *    vxe_render_frame and the allocation-free entry point then return
+ *    VXE_ERR_BOUNDS).
+ *  Valid records give identical results with either.  Use the checked build
+ *  to validate a new producer's records.
  */
 #ifndef VXE_VXE_H
 #define VXE_VXE_H
@@ -159,8 +174,8 @@ enum {
   /* Keep the intermediate images (local_img, output_pre_taa) that the fused
    * kernels otherwise never materialise; used by parity tests. */
   VXE_FLAG_DEBUG_INTERMEDIATES = 1u << 3,
-  /* Device-side bounds checks on every arena index (sets the error word). */
-  VXE_FLAG_CHECKED = 1u << 4,
+  /* (bit 4 is unused: device bounds checks are a build of the library,
+   * see "Device bounds checks" above) */
   /* Run the primary pass as one kernel per pixel (trace + shading) instead of
    * the default wavefront (trace kernel -> per-class shading kernels).  Both
    * produce identical images. */
@@ -349,6 +364,14 @@ uint64_t vxe_view_lane_bytes(const vxe_ctx* ctx, uint32_t present_w, uint32_t pr
 vxe_status vxe_view_create(vxe_ctx* ctx, uint32_t present_w, uint32_t present_h, float render_scale,
                            vxe_view** out);
 vxe_status vxe_view_render_async(vxe_ctx* ctx, vxe_view* view, uint32_t lane, const vxe_camera_gpu* camera);
+/* One frame of each of n (<= VXE_MAX_VIEWS_PER_LAUNCH) distinct views on a
+ * lane, every pass launched once for all of them: small views fill the GPU
+ * together instead of one small launch after another.  Each view's frame is
+ * the one vxe_view_render_async renders for the same camera; the lane holds
+ * one set of working buffers per view of the launch. */
+#define VXE_MAX_VIEWS_PER_LAUNCH 8u
+vxe_status vxe_view_render_batch_async(vxe_ctx* ctx, vxe_view* const* views, const vxe_camera_gpu* cameras,
+                                       uint32_t n, uint32_t lane);
 vxe_status vxe_view_read_image(vxe_ctx* ctx, vxe_view* view, int image, void* host, size_t bytes);
 vxe_status vxe_view_destroy(vxe_ctx* ctx, vxe_view* view);
 
@@ -491,6 +514,16 @@ vxe_status vxe_trace_primary_hits_noalloc(const vxe_scene_view* scene, const vxe
  * 3 pow(x, y), 4 min(x, y), 5 max(x, y).  Used to prove host/device bit
  * equality of the functions every pass depends on. */
 vxe_status vxe_debug_detmath(int which, const float* x, const float* y, float* out, uint32_t n);
+
+/* Diagnostic (no reference counterpart): the grass blade march on the device
+ * for n host inputs, without the per-frame cell table.  which = 0:
+ * try_grass_slab_hit (grass.wgsl:494-538), 17 floats per input (ray origin
+ * and direction, t_min, t_max, cell minimum corner, cell id, voxel size, wind
+ * time, wind strength) -> 5 floats (hit, t, normal); which = 1:
+ * grass_sdf_lod (grass.wgsl:192-350), 13 floats per input (point, cell
+ * minimum corner, cell id, voxel size, wind time, wind strength, lod) -> 1
+ * float.  Used to compare the march with the CPU restatement input by input. */
+vxe_status vxe_debug_grass(int which, uint32_t n, const float* in, float* out);
 
 /* Diagnostic (no reference counterpart): the device's L2 read bandwidth, the
  * roof of kernels whose working set stays in L2 (the world's node, rope,

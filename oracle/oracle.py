@@ -71,6 +71,8 @@ def lib():
                                      C.c_int, C.POINTER(OraCounters)]
         l.ora_detmath.restype = None
         l.ora_detmath.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
+        l.ora_debug_grass.restype = None
+        l.ora_debug_grass.argtypes = [C.c_int, C.c_uint32, C.c_void_p, C.c_void_p]
         l.ora_sizeof_frameio.restype = C.c_uint64
         assert l.ora_sizeof_frameio() == C.sizeof(FrameIO), "FrameIO layout mismatch"
         _lib = l
@@ -216,4 +218,14 @@ def detmath(which: int, x, y=None):
     y = np.ascontiguousarray(y if y is not None else np.zeros_like(x), dtype=np.float32)
     out = np.zeros_like(x)
     lib().ora_detmath(which, x.ctypes.data, y.ctypes.data, out.ctypes.data, len(x))
+    return out
+
+
+def debug_grass(which: int, inputs):
+    """The oracle's grass march (0: try_grass_slab_hit, 17 floats per input ->
+    5) or SDF (1: grass_sdf_lod, 13 floats -> 1) on host inputs."""
+    a = np.ascontiguousarray(inputs, dtype=np.float32)
+    n = a.shape[0]
+    out = np.zeros((n, 5 if which == 0 else 1), dtype=np.float32)
+    lib().ora_debug_grass(which, n, a.ctypes.data, out.ctypes.data)
     return out

@@ -2981,4 +2981,43 @@ void ora_detmath(int which, const float* x, const float* y, float* out, uint32_t
 
 uint64_t ora_sizeof_frameio(void) { return sizeof(FrameIO); }
 
+// Grass march pieces on host inputs (the device counterpart is
+// vxe_debug_grass): which 0 = try_grass_slab_hit, 17 floats in (ro, rd,
+// t_min, t_max, cb, id, voxel size, time, strength) -> 5 out (hit, t, n);
+// which 1 = grass_sdf_lod, 13 floats in (p, cb, id, voxel size, time,
+// strength, lod) -> 1 out.
+void ora_debug_grass(int which, uint32_t n, const float* in, float* out) {
+  Counters c;
+  vxe_camera_gpu cam;
+  std::memset(&cam, 0, sizeof cam);
+  Scene s;
+  std::memset((void*)&s, 0, sizeof s);
+  s.cam = &cam;
+  s.ctr = &c;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (which == 0) {
+      const float* a = in + (size_t)i * 17;
+      cam.voxel_params[0] = a[14];
+      cam.voxel_params[1] = a[15];
+      cam.voxel_params[2] = a[16];
+      const GrassHit g = try_grass_slab_hit(s, V3(a[0], a[1], a[2]), V3(a[3], a[4], a[5]), a[6], a[7],
+                                            V3(a[8], a[9], a[10]), V3(a[11], a[12], a[13]), a[14], a[15], a[16]);
+      float* o = out + (size_t)i * 5;
+      o[0] = g.hit ? 1.0f : 0.0f;
+      o[1] = g.t;
+      o[2] = g.n.x;
+      o[3] = g.n.y;
+      o[4] = g.n.z;
+    } else {
+      const float* a = in + (size_t)i * 13;
+      cam.voxel_params[0] = a[9];
+      cam.voxel_params[1] = a[10];
+      cam.voxel_params[2] = a[11];
+      out[i] = grass_sdf_lod(s, V3(a[0], a[1], a[2]), V3(a[3], a[4], a[5]), V3(a[6], a[7], a[8]), a[10], a[11],
+                             (uint32_t)a[12]);
+    }
+  }
+}
+
+
 }  // extern "C"

@@ -69,10 +69,11 @@ def read_gpu_frame(r: Renderer) -> dict:
     return out
 
 
-def make_renderer(scene, world, flags=A.FLAG_GODRAY_MACRO_ALIAS | A.FLAG_HIT_RECORDS | A.FLAG_DEBUG_INTERMEDIATES):
+def make_renderer(scene, world, flags=A.FLAG_GODRAY_MACRO_ALIAS | A.FLAG_HIT_RECORDS | A.FLAG_DEBUG_INTERMEDIATES,
+                  checked: bool = False):
     return Renderer(scene.present[0], scene.present[1], scene.render_scale, node_capacity=world.node_capacity,
                     chunk_capacity=world.chunk_capacity, grid_capacity=world.grid_capacity,
-                    clip_levels=max(1, scene.clip_levels), clip_res=scene.clip_res, flags=flags)
+                    clip_levels=max(1, scene.clip_levels), clip_res=scene.clip_res, flags=flags, checked=checked)
 
 
 def run_parity(scene, frames: int, threads: int | None = None, godray_alias: bool = True, on_frame=None,

@@ -15,12 +15,13 @@ def declared_functions():
 
 
 def test_every_declared_symbol_is_exported_and_bound():
-    lib = A.lib()
     names = declared_functions()
     assert len(names) >= 30
-    for n in names:
-        assert hasattr(lib, n), f"{n} missing from libvxe.so"
-        assert n in A.SIGNATURES, f"{n} has no ctypes signature"
+    for checked in (False, True):  # libvxe.so and libvxe_checked.so
+        lib = A.lib(checked)
+        for n in names:
+            assert hasattr(lib, n), f"{n} missing from {'libvxe_checked.so' if checked else 'libvxe.so'}"
+            assert n in A.SIGNATURES, f"{n} has no ctypes signature"
     assert set(A.SIGNATURES) == set(names)
 
 

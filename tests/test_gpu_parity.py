@@ -289,10 +289,11 @@ def test_profile_counts_stay_zero_with_flag_off_and_reset():
 
 def test_corrupt_upload_sets_error_word_and_matches_oracle():
     # A chunk upload whose root points its children past the node arena
-    # (child_base made on the host): every device read through it is bounds
-    # checked, sets the node bit of the error word and returns a zero record,
-    # exactly as the oracle's checked reads do (its oob counter); the images
-    # stay finite and equal the oracle's.
+    # (child_base made on the host), rendered by the checked build
+    # (libvxe_checked.so): every device read through it is bounds checked,
+    # sets the node bit of the error word and returns a zero record, exactly
+    # as the oracle's checked reads do (its oob counter); the images stay
+    # finite and equal the oracle's.
     from oracle import oracle as O
     from parity import compare_frame, make_renderer, read_gpu_frame
 
@@ -307,7 +308,7 @@ def test_corrupt_upload_sets_error_word_and_matches_oracle():
     nodes = u.data.nodes.copy()
     nodes[0]["child_base"] = bad_child
     u.data.nodes = nodes
-    r = make_renderer(sc, w)
+    r = make_renderer(sc, w, checked=True)
     try:
         r.upload_world(w, ups)
         _, _, clip, cam = drv.step()
@@ -344,3 +345,30 @@ def test_budgeted_streaming_frames_bit_exact():
     for _ in range(3):
         ups, _, _, _ = d.step()
     assert len(d.queue) > 0 and d.world.uploading
+
+
+def test_corrupt_upload_clamped_build_stays_in_bounds():
+    # The same corrupt chunk on the default build (clamped reads): the frame
+    # completes with finite images and, on valid records elsewhere, the
+    # unchanged results; nothing is reported.
+    from parity import make_renderer
+
+    sc = scenes.config1()
+    drv = FrameDriver(sc)
+    ups = drv.initial_uploads()
+    u = ups[0]
+    nodes = u.data.nodes.copy()
+    nodes[0]["child_base"] = drv.world.node_capacity + 12345
+    u.data.nodes = nodes
+    r = make_renderer(sc, drv.world)
+    try:
+        r.upload_world(drv.world, ups)
+        _, _, clip, cam = drv.step()
+        r.write_clipmap_updates(drv.empty_clip(), [])
+        r.write_camera(cam)
+        r.encode_compute()
+        assert r.read_error_word() == 0
+        out = r.read_image(A.IMG_OUTPUT)
+        assert np.isfinite(out).all()
+    finally:
+        r.close()

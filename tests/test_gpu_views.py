@@ -153,3 +153,47 @@ def test_async_output_reads_equal_sync_reads():
     assert runs[0][0] == runs[1][0]
     assert runs[0][1] == runs[1][1]
     assert len(set(runs[0][0])) > 1  # the frames differ
+
+
+def test_views_rendered_in_one_launch_equal_views_rendered_alone():
+    # vxe_view_render_batch_async: several views of different sizes and
+    # cameras, every pass launched once for all of them, give each view the
+    # frames it gets rendered alone -- over frames with histories feeding back
+    # (and the histories' ping-pong) and on both lanes.
+    from vxe.serve import make_sessions
+
+    sc = config2(present=(320, 180))
+    drv = FrameDriver(sc)
+    ups = drv.initial_uploads()
+    _, _, clip, cam = drv.step()
+    w = drv.world
+    r = Renderer(sc.present[0], sc.present[1], sc.render_scale, node_capacity=w.node_capacity,
+                 chunk_capacity=w.chunk_capacity, grid_capacity=w.grid_capacity, clip_levels=sc.clip_levels,
+                 clip_res=sc.clip_res)
+    sessions = make_sessions(w, 5, seed=9, size_range=((96, 640), (64, 360)))
+    together, alone = [], []
+    try:
+        r.upload_world(w, ups)
+        r.write_clipmap_updates(*clip)
+        r.write_camera(cam)
+        together = [r.view(s.w, s.h, s.render_scale) for s in sessions]
+        alone = [r.view(s.w, s.h, s.render_scale) for s in sessions]
+        prev = [None] * len(sessions)
+        for f in range(3):
+            cams = []
+            for i, s in enumerate(sessions):
+                c = s.camera(w, f, prev[i])
+                prev[i] = c.view_proj
+                cams.append(c)
+            r.render_views_async(f % 2, list(zip(together, cams)))
+            for v, c in zip(alone, cams):
+                v.render_async(1 - f % 2, c)
+            for img in (A.IMG_OUTPUT, A.IMG_COLOR, A.IMG_DEPTH, A.IMG_PRIMARY_HIST_IN, A.IMG_GODRAY_IN):
+                for i, (a, b) in enumerate(zip(together, alone)):
+                    assert a.read_image(img).tobytes() == b.read_image(img).tobytes(), (f, img, i)
+            r.batch_wait(0, block=True)
+            r.batch_wait(1, block=True)
+    finally:
+        for v in together + alone:
+            v.close()
+        r.close()

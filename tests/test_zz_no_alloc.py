@@ -69,18 +69,21 @@ def test_noalloc_hits_equal_context_hits_on_two_calls():
         st = lib.vxe_trace_primary_hits_noalloc(C.byref(sv), C.byref(big), C.byref(clip_params), d_hits.data_ptr(),
                                                 stream)
         assert st == 2  # VXE_ERR_CAPACITY
-        # a scene whose node records end after the first root: every read past
-        # it is bounds checked (zero record, error word) and reported
+        # a scene whose node records end after the first root, on the checked
+        # build: every read past it is bounds checked (zero record, error
+        # word) and reported; its next call clears its error word and is
+        # exact again
         short = A.SceneView(*[getattr(sv, f) for f, _ in A.SceneView._fields_])
         short.node_count = 1
-        st = lib.vxe_trace_primary_hits_noalloc(C.byref(short), C.byref(cams[0]), C.byref(clip_params),
+        chk = A.lib(checked=True)
+        st = chk.vxe_trace_primary_hits_noalloc(C.byref(short), C.byref(cams[0]), C.byref(clip_params),
                                                 d_hits.data_ptr(), stream)
         assert st == 6  # VXE_ERR_BOUNDS
-        # the next call clears the shared error word and is exact again
-        st = lib.vxe_trace_primary_hits_noalloc(C.byref(sv), C.byref(cams[1]), C.byref(clip_params),
-                                                d_hits.data_ptr(), stream)
-        assert st == A.VXE_OK
-        assert d_hits.cpu().numpy().view(A.HIT_DTYPE).tobytes() == want.tobytes()
+        for l in (chk, lib):
+            st = l.vxe_trace_primary_hits_noalloc(C.byref(sv), C.byref(cams[1]), C.byref(clip_params),
+                                                  d_hits.data_ptr(), stream)
+            assert st == A.VXE_OK
+            assert d_hits.cpu().numpy().view(A.HIT_DTYPE).tobytes() == want.tobytes()
     finally:
         r.close()
         bufs.clear()

@@ -154,12 +154,25 @@ struct Node { uint32_t child_base, child_mask, material, key; };
 
 __device__ __forceinline__ void flag(const Scene& s, uint32_t bit) { atomicOr(s.err, bit); }
 
+// Reads of the world's records at data-derived indices.  Two builds of the
+// library differ only here:
+//   VXE_DEVICE_CHECKS 0 (libvxe.so): every index is clamped into its buffer:
+//     no branch and no atomic on the traversal's hot path, never a read
+//     outside the buffers; records that point outside their chunk give wrong
+//     images but no fault (the robust-access behaviour WGSL allows);
+//   VXE_DEVICE_CHECKS 1 (libvxe_checked.so): an index outside its buffer
+//     reads as a zero record and sets a bit of the context's error word
+//     (vxe_read_error_word; vxe_render_frame returns VXE_ERR_BOUNDS).
+// Records that are in range give the same values in both builds.
+#ifndef VXE_DEVICE_CHECKS
+#define VXE_DEVICE_CHECKS 0
+#endif
+#if VXE_DEVICE_CHECKS
 __device__ __forceinline__ Node node_global(const Scene& s, uint32_t gi) {
   if (gi >= s.nodes_n) { flag(s, ERR_NODE); return Node{0u, 0u, 0u, 0u}; }
   const uint4 n = __ldg(&s.nodes[gi]);
   return Node{n.x, n.y, n.z, n.w};
 }
-__device__ __forceinline__ Node node_at(const Scene& s, uint32_t base, uint32_t local) { return node_global(s, base + local); }
 __device__ __forceinline__ uint32_t node_key(const Scene& s, uint32_t base, uint32_t local) {
   const uint32_t gi = base + local;
   if (gi >= s.nodes_n) { flag(s, ERR_NODE); return 0u; }
@@ -199,6 +212,46 @@ __device__ __forceinline__ float clip_texel(const Scene& s, int32_t sx, int32_t 
   }
   return __ldg(&s.clip_tex[((size_t)level * s.clip_res + (uint32_t)sz) * s.clip_res + (uint32_t)sx]);
 }
+#else
+// (every buffer holds at least one record: the context's capacities and the
+// scene-view checks guarantee n >= 1)
+__device__ __forceinline__ uint64_t clamp_index(uint64_t i, uint64_t n) { return i < n ? i : n - 1u; }
+__device__ __forceinline__ Node node_global(const Scene& s, uint32_t gi) {
+  const uint4 n = __ldg(&s.nodes[clamp_index(gi, s.nodes_n)]);
+  return Node{n.x, n.y, n.z, n.w};
+}
+__device__ __forceinline__ uint32_t node_key(const Scene& s, uint32_t base, uint32_t local) {
+  return __ldg(&s.nodes[clamp_index(base + local, s.nodes_n)].w);
+}
+__device__ __forceinline__ Meta meta_at(const Scene& s, uint32_t slot) {
+  const size_t i = (size_t)clamp_index(slot, s.metas_n) * 3u;
+  const uint4 a = __ldg(&s.metas[i]);
+  const uint4 b = __ldg(&s.metas[i + 1u]);
+  const uint32_t e = __ldg(&s.metas[i + 2u].x);
+  return Meta{(int32_t)a.x, (int32_t)a.y, (int32_t)a.z, b.x, b.z, b.w, e};
+}
+__device__ __forceinline__ uint32_t meta_empty(const Scene& s, uint32_t slot) {
+  return __ldg(&s.metas[(size_t)clamp_index(slot, s.metas_n) * 3u + 2u].x);
+}
+__device__ __forceinline__ uint32_t grid_at(const Scene& s, uint32_t idx) { return __ldg(&s.grid[clamp_index(idx, s.grid_n)]); }
+__device__ __forceinline__ uint32_t macro_word(const Scene& s, uint32_t idx) {
+  return __ldg(&s.macro[clamp_index(idx, s.macro_n)]);
+}
+__device__ __forceinline__ uint32_t colinfo_word(const Scene& s, uint32_t idx) {
+  return __ldg(&s.colinfo[clamp_index(idx, s.colinfo_n)]);
+}
+__device__ __forceinline__ uint32_t rope_face(const Scene& s, uint32_t gi, uint32_t face) {
+  return __ldg(&s.ropes[(size_t)clamp_index(gi, s.ropes_n) * 8u + face]);
+}
+__device__ __forceinline__ float clip_texel(const Scene& s, int32_t sx, int32_t sz, uint32_t level) {
+  if (s.clip_layers == 0u || s.clip_res == 0u) return 0.0f;  // no clipmap texture
+  const uint32_t r1 = s.clip_res - 1u;
+  const uint32_t l = min(level, s.clip_layers - 1u), x = min((uint32_t)max(sx, 0), r1),
+                 z = min((uint32_t)max(sz, 0), r1);
+  return __ldg(&s.clip_tex[((size_t)l * s.clip_res + z) * s.clip_res + x]);
+}
+#endif
+__device__ __forceinline__ Node node_at(const Scene& s, uint32_t base, uint32_t local) { return node_global(s, base + local); }
 
 __device__ __forceinline__ v3 cam_pos(const Scene& s) { return V3(s.cam->cam_pos[0], s.cam->cam_pos[1], s.cam->cam_pos[2]); }
 __device__ __forceinline__ float vs_(const Scene& s) { return s.cam->voxel_params[0]; }

@@ -1478,39 +1478,24 @@ __device__ __forceinline__ ChunkTraceResult trace_chunk_interval_stream_macro(co
   // site for the leaf walk keeps it inlined once.
   const bool whole = !ms.enabled;
   for (uint32_t i = 0; i < 128u; ++i) {
-    // Each lane first skips its run of empty macro cells (one iteration of
-    // the reference loop each) in this inner loop, so that the lanes of a
-    // warp enter the leaf walk together.
     float seg_end = t_end, cell_exit = t_end;
-    bool walk = false;
-    for (; i < 128u; ++i) {
-      seg_end = t_end;
-      cell_exit = t_end;
-      bool empty = false;
-      if (!whole) {
-        if (tcur >= t_end) break;
-        macro_dda_sync(ms, tcur);
-        const MacroStep st = macro_dda_current(s, ms, ch.macro_base);
-        if (!st.valid) break;
-        cell_exit = st.t_exit;
-        seg_end = fmin_(st.t_exit, t_end);
-        empty = st.empty;
-      }
-      if (!empty) {
-        walk = true;
-        break;
-      }
-      // an empty cell is skipped whole
-      tcur = seg_end + eps_step;
-      if (ms.enabled && tcur >= cell_exit) macro_dda_step(ms);
+    bool empty = false;
+    if (!whole) {
+      if (tcur >= t_end) break;
+      macro_dda_sync(ms, tcur);
+      const MacroStep st = macro_dda_current(s, ms, ch.macro_base);
+      if (!st.valid) break;
+      cell_exit = st.t_exit;
+      seg_end = fmin_(st.t_exit, t_end);
+      empty = st.empty;
     }
-    if (!walk) break;
-    const ChunkTraceResult h =
-        trace_chunk_rope_interval_nomacro<PM>(s, ro, rd, inv, ch, tcur, seg_end, anchor_valid, anchor_key, opt, ph);
-    if (whole || h.hit.hit != 0u) return h;
-    anchor_valid = h.anchor_valid;
-    anchor_key = h.anchor_key;
-    // on to the next macro cell
+    if (!empty) {
+      const ChunkTraceResult h =
+          trace_chunk_rope_interval_nomacro<PM>(s, ro, rd, inv, ch, tcur, seg_end, anchor_valid, anchor_key, opt, ph);
+      if (whole || h.hit.hit != 0u) return h;
+      anchor_valid = h.anchor_valid;
+      anchor_key = h.anchor_key;
+    }
     tcur = seg_end + eps_step;
     if (ms.enabled && tcur >= cell_exit) macro_dda_step(ms);
   }

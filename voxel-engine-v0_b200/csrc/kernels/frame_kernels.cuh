@@ -80,7 +80,6 @@ struct FrameArgs {
   uint2* px_mask;                 // per pixel: candidate chunks with a probe hit, hint / full trace
   uint2* px_probe;                // per pixel: walk summary (probe_summary) | probes stored
   uint32_t* q_pending;            // pixels whose walk met probes, q_count[5] of them
-  uint32_t* q_full;               // pixels whose walk goes on to the full trace, q_count[10] of them
   // per-frame grass cell table: written by k_grass_cells, read by the rest
   float4* grass_rec;
   uint64_t grass_rec_n;  // records (slots * 4096)
@@ -109,6 +108,13 @@ __device__ __forceinline__ uint32_t fog_profile_weight(float t_scene) {
   const float fog_norm = clampf(t_scene / FOG_MAX_DIST, 0.0f, 1.0f);
   return max(1u, to_u32(fog_norm * 256.0f));
 }
+
+// The arguments of up to kMaxViewsPerLaunch views' frames, rendered by one
+// launch of each pass: blockIdx.z selects the view.
+constexpr uint32_t kMaxViewsPerLaunch = 8u;
+struct FrameArgsViews {
+  FrameArgs v[kMaxViewsPerLaunch];
+};
 
 __device__ __forceinline__ Scene make_scene(const FrameArgs& A, bool godray) {
   Scene s;
@@ -333,7 +339,7 @@ __device__ __noinline__ void build_tile_list(const Scene& s, uint32_t tx, uint32
   for (uint32_t i = 0; i < TILE_CANDS; ++i) out_slots[i] = i < limit ? sl[i][lane] : INVALID;
 }
 
-__global__ void __launch_bounds__(TILE_THREADS) k_tiles(const __grid_constant__ FrameArgs A) {
+__device__ __forceinline__ void k_tiles_body(const FrameArgs& A) {
   __shared__ uint32_t sl[MAX_TILE_CHUNKS][TILE_THREADS];
   __shared__ float en[MAX_TILE_CHUNKS][TILE_THREADS];
   const uint32_t lane = threadIdx.x;
@@ -343,6 +349,10 @@ __global__ void __launch_bounds__(TILE_THREADS) k_tiles(const __grid_constant__ 
   const Scene s = make_scene(A, false);
   build_tile_list(s, tile % tiles_x, tile / tiles_x, lane, sl, en, &A.tile_count[tile],
                   &A.tile_slots[(size_t)tile * TILE_CANDS]);
+}
+__global__ void __launch_bounds__(TILE_THREADS) k_tiles(const __grid_constant__ FrameArgs A) { k_tiles_body(A); }
+__global__ void __launch_bounds__(TILE_THREADS) k_tiles_views(const __grid_constant__ FrameArgsViews V) {
+  k_tiles_body(V.v[blockIdx.z]);
 }
 
 // trace_scene_voxels_candidates (chunk_trace.wgsl:1177-1265) over a tile list
@@ -372,29 +382,17 @@ __device__ VoxTraceResult trace_candidates(const Scene& s, const uint32_t* cslot
   const float rs = (float)s.cam->chunk_size * vsz;
   const uint32_t maxc = min(cand_count, MAX_TILE_CHUNKS);
   const TraceOpts opt{false};
-  for (uint32_t i = 0;; ++i) {
-    // Each lane first passes over the candidates it does not walk (no slot,
-    // an empty chunk, missed, behind the best hit, skipped by the heightfield
-    // test) in this inner loop, so that the lanes of a warp enter the chunk
-    // walk together even when they walk different candidates.
-    Meta ch;
-    float ce = 0.0f, cx = 0.0f;
-    uint32_t slot = INVALID;
-    for (; i < maxc; ++i) {
-      slot = cslot[i];
-      if (slot == INVALID || slot >= s.cam->chunk_count) continue;
-      ch = cmeta ? cmeta[i] : meta_at(s, slot);  // staged in shared memory, or read through L1
-      if (ch.macro_empty != 0u) continue;
-      const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vsz;
-      const v2 rt = intersect_aabb(ro, rd, rb, rb + V3s(rs));
-      ce = fmax_(rt.x, t_enter);
-      cx = fmin_(rt.y, t_exit);
-      if (cx < ce) continue;
-      if (best.hit != 0u && ce >= best.t) continue;
-      if (chunk_heightfield_early_skip(s, ro, rd, ce, cx, ch, vsz)) continue;
-      break;
-    }
-    if (i >= maxc) break;
+  for (uint32_t i = 0; i < maxc; ++i) {
+    const uint32_t slot = cslot[i];
+    if (slot == INVALID || slot >= s.cam->chunk_count) continue;
+    const Meta ch = cmeta ? cmeta[i] : meta_at(s, slot);
+    if (ch.macro_empty != 0u) continue;
+    const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vsz;
+    const v2 rt = intersect_aabb(ro, rd, rb, rb + V3s(rs));
+    const float ce = fmax_(rt.x, t_enter), cx = fmin_(rt.y, t_exit);
+    if (cx < ce) continue;
+    if (best.hit != 0u && ce >= best.t) continue;
+    if (chunk_heightfield_early_skip(s, ro, rd, ce, cx, ch, vsz)) continue;
     const int32_t csz = (int32_t)s.cam->chunk_size;
     const i3 cc{ch.ox / csz, ch.oy / csz, ch.oz / csz};
     const bool ua = anchor_valid_in && chunk_coords_neighbor(cc, anchor_chunk_in);
@@ -860,15 +858,15 @@ __device__ __forceinline__ ProbeHook probe_hook_record(const FrameArgs& A, uint3
   return ph;
 }
 
-// Voxel walk with the grass column probes stored, not evaluated, in two
-// launches: this one runs the hint-window phase of the pixels whose history
-// is valid; pixels that need the full trace (no valid history, or nothing
-// found in the window) go to a queue that k_primary_trace_full walks with
-// full warps, so the long walks of a few pixels do not hold the warps of the
-// many that end in the window.  Pixels that met no probe are final after
-// their walk; the rest wait for k_probe_dda, k_slab_eval, k_slab_pick and
-// k_primary_resolve.
-__global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace(const __grid_constant__ FrameArgs A) {
+// Voxel walk with the grass column probes stored, not evaluated (both trace
+// phases: the hint window, then the full trace when the window held no voxel
+// hit).  Pixels that met no probe are final here; the rest wait for
+// k_probe_dda, k_slab_eval, k_slab_pick and k_primary_resolve.  (Running the
+// full-trace phase as a second launch over a compacted queue of the pixels
+// that need it was measured slower: 2.49 vs 2.32 ms per 1080p frame.)
+__device__ __forceinline__ void k_primary_trace_body(const FrameArgs& A) {
+  // a block beyond this view's tiles (a launch over views of different sizes)
+  if (blockIdx.x * 2u >= (A.iw + 7u) / 8u || blockIdx.y >= (A.ih + 7u) / 8u) return;
   __shared__ uint32_t cslot[2][TILE_CANDS];
   __shared__ Meta cmeta[2][TILE_CANDS];
   __shared__ uint32_t ccount[2];
@@ -881,71 +879,26 @@ __global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace(const __grid_
   if (active) {
     const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
     pix = (uint32_t)c.pix;
-    if (s.cam->chunk_count != 0u && ccount[t] != 0u) {
-      const PrimaryHint hh = primary_hint(s, A, c);
-      if (hh.valid) {
-        ProbeHook ph = probe_hook_record(A, pix);
-        ph.first_phase = 0u;
-        ph.phase = 0u;
-        const VoxTraceResult vt = trace_candidates<PROBE_RECORD>(s, cslot[t], cmeta[t], c.ro, c.rd, hh.t_start,
-                                                                 hh.t_end, hh.anchor_key != INVALID, hh.anchor_chunk,
-                                                                 hh.anchor_key, ccount[t], ph);
-        if (vt.best.hit != 0u) {
-          walk_finish(A, pix, vt, ph, ccount[t], &vox, &pend);
-        } else {
-          full = true;  // carry the probe count and the hint bit to the full trace
-          A.px_probe[pix] = make_uint2(ph.seq, ph.recorded | 0x80000000u);
-        }
-      } else {
-        full = true;
-        A.px_probe[pix] = make_uint2(0u, 0u);
-      }
-    }
+    ProbeHook ph = probe_hook_record(A, pix);
+    const VoxTraceResult vt = primary_trace<PROBE_RECORD>(s, A, c, cslot[t], cmeta[t], ccount[t], ph);
+    walk_finish(A, pix, vt, ph, ccount[t], &vox, &pend);
+    full = ph.first_phase <= 1u && ph.phase == 1u;
   }
   enqueue(A.q_vox, &A.q_count[0], active && vox && !pend, pix);
-  enqueue(A.q_far, &A.q_count[1], active && !vox && !pend && !full, pix);
+  enqueue(A.q_far, &A.q_count[1], active && !vox && !pend, pix);
   enqueue(A.q_pending, &A.q_count[5], active && pend, pix);
-  enqueue(A.q_full, &A.q_count[10], active && full, pix);
+  const uint32_t nfull = __popc(__ballot_sync(0xFFFFFFFFu, full));  // frame statistics
+  if ((threadIdx.x & 31u) == 0u && nfull != 0u) atomicAdd(&A.q_count[10], nfull);
 }
-
-// The full-trace phase (phase 1) of the pixels k_primary_trace queued, one
-// lane each; the tile candidate lists and their metas come from global
-// memory (L1 / L2).
-__global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace_full(const __grid_constant__ FrameArgs A) {
-  const Scene s = make_scene(A, false);
-  const uint32_t n = A.q_count[10], end = warp_uniform_end(n);
-  const uint32_t tiles_x = (A.iw + 7u) / 8u;
-  for (uint32_t i = blockIdx.x * PRIMARY_THREADS + threadIdx.x; i < end; i += gridDim.x * PRIMARY_THREADS) {
-    const bool active = i < n;
-    bool vox = false, pend = false;
-    uint32_t pix = 0u;
-    if (active) {
-      pix = A.q_full[i];
-      const uint32_t gx = pix % A.iw, gy = pix / A.iw;
-      const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
-      const size_t tile = (size_t)(gy >> 3) * tiles_x + (gx >> 3);
-      const uint32_t tc = A.tile_count[tile];
-      const uint2 carry = A.px_probe[pix];
-      ProbeHook ph = probe_hook_record(A, pix);
-      ph.seq = carry.x;
-      ph.recorded = carry.y & 0x7FFFFFFFu;
-      ph.first_phase = (carry.y & 0x80000000u) != 0u ? 0u : 1u;
-      ph.phase = 1u;
-      const VoxTraceResult vt = trace_candidates<PROBE_RECORD>(s, A.tile_slots + tile * TILE_CANDS, nullptr, c.ro,
-                                                               c.rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID,
-                                                               tc, ph);
-      walk_finish(A, pix, vt, ph, tc, &vox, &pend);
-    }
-    enqueue(A.q_vox, &A.q_count[0], active && vox && !pend, pix);
-    enqueue(A.q_far, &A.q_count[1], active && !vox && !pend, pix);
-    enqueue(A.q_pending, &A.q_count[5], active && pend, pix);
-  }
+__global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace(const __grid_constant__ FrameArgs A) { k_primary_trace_body(A); }
+__global__ void __launch_bounds__(PRIMARY_THREADS) k_primary_trace_views(const __grid_constant__ FrameArgsViews V) {
+  k_primary_trace_body(V.v[blockIdx.z]);
 }
 
 // One lane per stored probe: the probe's column DDA with the walk's
 // arguments, storing one task per grass slab it would march.  A probe whose
 // tasks do not all fit sends its pixel to the inline walk (stored count 0).
-__global__ void __launch_bounds__(SHADE_THREADS) k_probe_dda(const __grid_constant__ FrameArgs A) {
+__device__ __forceinline__ void k_probe_dda_body(const FrameArgs& A) {
   const Scene s = make_scene(A, false);
   const uint32_t n = min(A.q_count[4], A.probe_cap);
   const float vs = vs_(s);
@@ -974,10 +927,14 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_probe_dda(const __grid_consta
     if (lost) atomicMin(&A.px_probe[r.pixel].y, 0u);
   }
 }
+__global__ void __launch_bounds__(SHADE_THREADS) k_probe_dda(const __grid_constant__ FrameArgs A) { k_probe_dda_body(A); }
+__global__ void __launch_bounds__(SHADE_THREADS) k_probe_dda_views(const __grid_constant__ FrameArgsViews V) {
+  k_probe_dda_body(V.v[blockIdx.z]);
+}
 
 // One lane per grass slab: try_grass_slab_hit (the blade march).  A hit
 // lowers its pixel's nearest-hit key and marks its chunk.
-__global__ void __launch_bounds__(SHADE_THREADS) k_slab_eval(const __grid_constant__ FrameArgs A) {
+__device__ __forceinline__ void k_slab_eval_body(const FrameArgs& A) {
   const Scene s = make_scene(A, false);
   const uint32_t n = min(A.q_count[6], A.slab_cap);
   const float vs = vs_(s);
@@ -1003,6 +960,10 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_slab_eval(const __grid_consta
     }
   }
 }
+__global__ void __launch_bounds__(SHADE_THREADS) k_slab_eval(const __grid_constant__ FrameArgs A) { k_slab_eval_body(A); }
+__global__ void __launch_bounds__(SHADE_THREADS) k_slab_eval_views(const __grid_constant__ FrameArgsViews V) {
+  k_slab_eval_body(V.v[blockIdx.z]);
+}
 
 // True when hit `key` cannot stand for its chunk: an earlier probe of the
 // same chunk and trace phase also hit.  Successive probe intervals meet at a
@@ -1017,7 +978,7 @@ __device__ __forceinline__ bool slab_hit_shadows_first(unsigned long long first,
 
 // Finds, per pixel, the slab task whose key is the pixel's nearest; pixels
 // where that hit is not its chunk's first are sent to the inline walk.
-__global__ void __launch_bounds__(SHADE_THREADS) k_slab_pick(const __grid_constant__ FrameArgs A) {
+__device__ __forceinline__ void k_slab_pick_body(const FrameArgs& A) {
   const uint32_t n = min(A.q_count[7], A.slab_cap);
   for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < n; i += gridDim.x * SHADE_THREADS) {
     const uint32_t j = A.slab_hits[i];
@@ -1030,11 +991,15 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_slab_pick(const __grid_consta
     else if (slab_hit_shadows_first(first, key)) atomicMin(&A.px_probe[r.pixel].y, 0u);
   }
 }
+__global__ void __launch_bounds__(SHADE_THREADS) k_slab_pick(const __grid_constant__ FrameArgs A) { k_slab_pick_body(A); }
+__global__ void __launch_bounds__(SHADE_THREADS) k_slab_pick_views(const __grid_constant__ FrameArgsViews V) {
+  k_slab_pick_body(V.v[blockIdx.z]);
+}
 
 // Pixels that met probes: the nearer of the nearest probe hit and the voxel
 // answer (see the comment above ProbeRec), or, when that cannot be decided
 // from the parts, the reference walk with inline probes.
-__global__ void __launch_bounds__(SHADE_THREADS) k_primary_resolve(const __grid_constant__ FrameArgs A) {
+__device__ __forceinline__ void k_primary_resolve_body(const FrameArgs& A) {
   const Scene s = make_scene(A, false);
   const uint32_t n = A.q_count[5], end = warp_uniform_end(n);
   const uint32_t tiles_x = (A.iw + 7u) / 8u;
@@ -1098,6 +1063,10 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_primary_resolve(const __grid_
     enqueue(A.q_far, &A.q_count[1], active && !vox, pix);
   }
 }
+__global__ void __launch_bounds__(SHADE_THREADS) k_primary_resolve(const __grid_constant__ FrameArgs A) { k_primary_resolve_body(A); }
+__global__ void __launch_bounds__(SHADE_THREADS) k_primary_resolve_views(const __grid_constant__ FrameArgsViews V) {
+  k_primary_resolve_body(V.v[blockIdx.z]);
+}
 
 __device__ __forceinline__ HitGeom load_pixhit(const Scene& s, const uint4* src) {
   const uint4 a = src[0], b = src[1], d = src[2], e = src[3];
@@ -1121,7 +1090,7 @@ __device__ __forceinline__ HitGeom load_pixhit(const Scene& s, const uint4* src)
 // a grid-stride loop whose trip count is uniform per warp (queues are read on
 // the device), so the warp-wide enqueue and shuffles see every lane.
 
-__global__ void __launch_bounds__(SHADE_THREADS) k_shade_prep(const __grid_constant__ FrameArgs A) {
+__device__ __forceinline__ void k_shade_prep_body(const FrameArgs& A) {
   const Scene s = make_scene(A, false);
   const uint32_t n = A.q_count[0], end = warp_uniform_end(n);
   for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < end; i += gridDim.x * SHADE_THREADS) {
@@ -1151,8 +1120,12 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_shade_prep(const __grid_const
     enqueue(A.q_light, &A.q_count[3], light, pix);
   }
 }
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_prep(const __grid_constant__ FrameArgs A) { k_shade_prep_body(A); }
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_prep_views(const __grid_constant__ FrameArgsViews V) {
+  k_shade_prep_body(V.v[blockIdx.z]);
+}
 
-__global__ void __launch_bounds__(SHADE_THREADS) k_shade_shadow(const __grid_constant__ FrameArgs A) {
+__device__ __forceinline__ void k_shade_shadow_body(const FrameArgs& A) {
   const Scene s = make_scene(A, false);
   const uint32_t n = A.q_count[2];
   for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < n; i += gridDim.x * SHADE_THREADS) {
@@ -1162,10 +1135,14 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_shade_shadow(const __grid_con
     A.px_shadow[pix] = sun_transmittance_geom_only(s, shadow_origin(s, c, g), SUN_DIR);
   }
 }
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_shadow(const __grid_constant__ FrameArgs A) { k_shade_shadow_body(A); }
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_shadow_views(const __grid_constant__ FrameArgsViews V) {
+  k_shade_shadow_body(V.v[blockIdx.z]);
+}
 
 // Eight lanes per pixel, one light ray each; the group's first lane adds the
 // eight results in ray order (the reference loop's order and early stop).
-__global__ void __launch_bounds__(SHADE_THREADS) k_shade_lights(const __grid_constant__ FrameArgs A) {
+__device__ __forceinline__ void k_shade_lights_body(const FrameArgs& A) {
   const Scene s = make_scene(A, false);
   const uint32_t lane = threadIdx.x & 31u, ray = lane & 7u, group0 = lane & ~7u;
   const uint32_t n = A.q_count[3], groups = n * 8u, end = warp_uniform_end(groups);
@@ -1200,8 +1177,12 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_shade_lights(const __grid_con
     }
   }
 }
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_lights(const __grid_constant__ FrameArgs A) { k_shade_lights_body(A); }
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_lights_views(const __grid_constant__ FrameArgsViews V) {
+  k_shade_lights_body(V.v[blockIdx.z]);
+}
 
-__global__ void __launch_bounds__(SHADE_THREADS) k_shade_vox(const __grid_constant__ FrameArgs A) {
+__device__ __forceinline__ void k_shade_vox_body(const FrameArgs& A) {
   const Scene s = make_scene(A, false);
   const uint32_t n = A.q_count[0];
   for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < n; i += gridDim.x * SHADE_THREADS) {
@@ -1221,12 +1202,16 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_shade_vox(const __grid_consta
                       true);
   }
 }
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_vox(const __grid_constant__ FrameArgs A) { k_shade_vox_body(A); }
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_vox_views(const __grid_constant__ FrameArgsViews V) {
+  k_shade_vox_body(V.v[blockIdx.z]);
+}
 
 // PART 0: the far pixels the walk queued (q_count[8], copied right after the
 // walk), shaded while the grass probes resolve; PART 1: those the resolve
 // queued after them; PART 2: the whole queue.
 template <int PART>
-__global__ void __launch_bounds__(SHADE_THREADS) k_shade_far(const __grid_constant__ FrameArgs A) {
+__device__ __forceinline__ void k_shade_far_body(const FrameArgs& A) {
   const Scene s = make_scene(A, false);
   const uint32_t first = PART == 1 ? A.q_count[8] : 0u;
   const uint32_t n = PART == 0 ? A.q_count[8] : A.q_count[1];
@@ -1236,13 +1221,19 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_shade_far(const __grid_consta
     shade_far_pixel(s, A, c);
   }
 }
+template <int PART>
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_far(const __grid_constant__ FrameArgs A) { k_shade_far_body<PART>(A); }
+template <int PART>
+__global__ void __launch_bounds__(SHADE_THREADS) k_shade_far_views(const __grid_constant__ FrameArgsViews V) {
+  k_shade_far_body<PART>(V.v[blockIdx.z]);
+}
 
 // ---------------------------------------------------------------------------
 // Godray pass
 // ---------------------------------------------------------------------------
 constexpr int POST_THREADS_X = 32, POST_THREADS_Y = 4;
 
-__global__ void __launch_bounds__(POST_THREADS_X* POST_THREADS_Y) k_godray(const __grid_constant__ FrameArgs A) {
+__device__ __forceinline__ void k_godray_body(const FrameArgs& A) {
   const uint32_t gx = blockIdx.x * POST_THREADS_X + threadIdx.x;
   const uint32_t gy = blockIdx.y * POST_THREADS_Y + threadIdx.y;
   if (gx >= A.iw || gy >= A.ih) return;
@@ -1304,11 +1295,15 @@ __global__ void __launch_bounds__(POST_THREADS_X* POST_THREADS_Y) k_godray(const
   const v3 oc = godray_compress(vmax(ol, V3s(0.0f)));
   A.god_out[(size_t)gy * W + gx] = make_float4(oc.x, oc.y, oc.z, t_hist);
 }
+__global__ void __launch_bounds__(POST_THREADS_X* POST_THREADS_Y) k_godray(const __grid_constant__ FrameArgs A) { k_godray_body(A); }
+__global__ void __launch_bounds__(POST_THREADS_X* POST_THREADS_Y) k_godray_views(const __grid_constant__ FrameArgsViews V) {
+  k_godray_body(V.v[blockIdx.z]);
+}
 
 // ---------------------------------------------------------------------------
 // Composite pass (+ fused composite TAA)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(POST_THREADS_X* POST_THREADS_Y) k_composite(const __grid_constant__ FrameArgs A) {
+__device__ __forceinline__ void k_composite_body(const FrameArgs& A) {
   const uint32_t gx = blockIdx.x * POST_THREADS_X + threadIdx.x;
   const uint32_t gy = blockIdx.y * POST_THREADS_Y + threadIdx.y;
   if (gx >= A.pw || gy >= A.ph) return;
@@ -1414,6 +1409,10 @@ __global__ void __launch_bounds__(POST_THREADS_X* POST_THREADS_Y) k_composite(co
   const float4 o = make_float4(taa.x, taa.y, taa.z, 1.0f);
   A.output[opix] = o;
   A.out_hist_out[opix] = o;
+}
+__global__ void __launch_bounds__(POST_THREADS_X* POST_THREADS_Y) k_composite(const __grid_constant__ FrameArgs A) { k_composite_body(A); }
+__global__ void __launch_bounds__(POST_THREADS_X* POST_THREADS_Y) k_composite_views(const __grid_constant__ FrameArgsViews V) {
+  k_composite_body(V.v[blockIdx.z]);
 }
 
 // ---------------------------------------------------------------------------

@@ -20,6 +20,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <new>
 #include <string>
 #include <vector>
@@ -46,7 +47,7 @@ enum Img {
   IMG_GOD0, IMG_GOD1, IMG_PRE_TAA, IMG_OUTPUT, IMG_OHIST0, IMG_OHIST1, IMG_HITS, IMG_TILE_COUNT, IMG_TILE_SLOTS,
   IMG_PIXHIT, IMG_QVOX, IMG_QFAR, IMG_QCOUNT, IMG_QSHADOW, IMG_QLIGHT, IMG_PXSHADOW, IMG_PXLIGHT,
   IMG_PROBE_RECS, IMG_SLAB_TASKS, IMG_SLAB_RES, IMG_SLAB_HITS, IMG_PXFIRST, IMG_PXPROBE, IMG_PXMASK, IMG_PXTASK,
-  IMG_QPENDING, IMG_QFULL,
+  IMG_QPENDING,
   IMG_N
 };
 
@@ -121,6 +122,8 @@ struct BatchLane {
   // per-frame working buffers (tile lists, queues, probe and slab records)
   // of the viewport sessions rendered on this lane, sized for the largest
   FrameState scratch;
+  // one set per view of a multi-view launch (vxe_view_render_batch_async)
+  FrameState mscratch[vxe::dev::kMaxViewsPerLaunch];
 };
 
 }  // namespace
@@ -290,7 +293,6 @@ size_t img_bytes(const FrameState& F, int i) {
     case IMG_PIXHIT:
       return in * 80;
     case IMG_QVOX: case IMG_QFAR: case IMG_QSHADOW: case IMG_QLIGHT: case IMG_PXSHADOW: case IMG_QPENDING:
-    case IMG_QFULL:
       return in * 4;
     case IMG_PROBE_RECS:
       return in * kProbesPerPixel * sizeof(vxe::dev::ProbeRec);
@@ -583,7 +585,6 @@ void frame_fill(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& cam, FrameArgs&
   A.px_task = (uint32_t*)S->img[IMG_PXTASK].p;
   A.px_mask = (uint2*)S->img[IMG_PXMASK].p;
   A.q_pending = (uint32_t*)S->img[IMG_QPENDING].p;
-  A.q_full = (uint32_t*)S->img[IMG_QFULL].p;
 }
 
 // The frame's launches on the compute stream (captured as-is by the graph
@@ -631,7 +632,6 @@ vxe_status frame_enqueue(vxe_ctx* c, FrameState& F, const FrameArgs& A, bool tim
     CK(cudaMemsetAsync(A.px_mask, 0, (size_t)npix * 8u, st));
     if (timed) CK(cudaEventRecord(F.ev[7], st));
     k_primary_trace<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, st>>>(A);
-    k_primary_trace_full<<<grid(npix), PRIMARY_THREADS, 0, st>>>(A);
     if (timed) CK(cudaEventRecord(F.ev[8], st));
     if (side) {  // the walk's far pixels shade beside the probe passes
       CK(cudaMemcpyAsync(A.q_count + 8, A.q_count + 1, 4, cudaMemcpyDeviceToDevice, st));
@@ -680,6 +680,59 @@ vxe_status frame_enqueue(vxe_ctx* c, FrameState& F, const FrameArgs& A, bool tim
   k_composite<<<dim3((F.pw + POST_THREADS_X - 1) / POST_THREADS_X, (F.ph + POST_THREADS_Y - 1) / POST_THREADS_Y),
                 dim3(POST_THREADS_X, POST_THREADS_Y), 0, st>>>(A);
   if (timed) CK(cudaEventRecord(F.ev[6], st));
+  CK(cudaGetLastError());
+  return VXE_OK;
+}
+
+// The wavefront frame of n views (vxe_view_render_batch_async): each pass is
+// one launch over all of them (blockIdx.z = view), sized for the largest.
+vxe_status views_enqueue(vxe_ctx* c, const vxe::dev::FrameArgsViews& V, uint32_t n, uint32_t max_iw,
+                         uint32_t max_ih, uint32_t max_pw, uint32_t max_ph, uint64_t max_pix, cudaStream_t st,
+                         SideStream* side) {
+  using namespace vxe::dev;
+  const uint32_t tiles_x = (max_iw + 7) / 8, tiles_y = (max_ih + 7) / 8;
+  const uint32_t per_view = std::max<uint32_t>(1u, (uint32_t)c->shade_wave / n);
+  auto grid = [&](uint64_t threads) {
+    return dim3((unsigned)std::max<uint64_t>(1, std::min<uint64_t>((threads + SHADE_THREADS - 1) / SHADE_THREADS,
+                                                                    (uint64_t)per_view)),
+                1, n);
+  };
+  for (uint32_t i = 0; i < n; ++i) {
+    const FrameArgs& A = V.v[i];
+    const size_t npix = (size_t)A.iw * A.ih;
+    CK(cudaMemsetAsync(A.q_count, 0, 64, st));
+    CK(cudaMemsetAsync(A.px_first, 0xFF, npix * 8u, st));
+    CK(cudaMemsetAsync(A.px_mask, 0, npix * 8u, st));
+  }
+  vxe_status sr = side_ready(c, *side);
+  if (sr != VXE_OK) return sr;
+  k_tiles_views<<<dim3((tiles_x * tiles_y + TILE_THREADS - 1) / TILE_THREADS, 1, n), TILE_THREADS, 0, st>>>(V);
+  k_primary_trace_views<<<dim3((tiles_x + 1) / 2, tiles_y, n), PRIMARY_THREADS, 0, st>>>(V);
+  for (uint32_t i = 0; i < n; ++i)  // the walk's far pixels shade beside the probe passes
+    CK(cudaMemcpyAsync(V.v[i].q_count + 8, V.v[i].q_count + 1, 4, cudaMemcpyDeviceToDevice, st));
+  CK(cudaEventRecord(side->fork, st));
+  CK(cudaStreamWaitEvent(side->s, side->fork, 0));
+  k_shade_far_views<0><<<grid(max_pix), SHADE_THREADS, 0, side->s>>>(V);
+  k_probe_dda_views<<<grid(max_pix * kProbesPerPixel), SHADE_THREADS, 0, st>>>(V);
+  k_slab_eval_views<<<grid(max_pix * kSlabsPerPixel), SHADE_THREADS, 0, st>>>(V);
+  k_slab_pick_views<<<grid(max_pix), SHADE_THREADS, 0, st>>>(V);
+  k_primary_resolve_views<<<grid(max_pix), SHADE_THREADS, 0, st>>>(V);
+  CK(cudaEventRecord(side->mid, st));
+  CK(cudaStreamWaitEvent(side->s, side->mid, 0));
+  k_shade_far_views<1><<<grid(max_pix), SHADE_THREADS, 0, side->s>>>(V);
+  k_shade_prep_views<<<grid(max_pix), SHADE_THREADS, 0, st>>>(V);
+  CK(cudaEventRecord(side->prep, st));
+  CK(cudaStreamWaitEvent(side->s, side->prep, 0));
+  k_godray_views<<<dim3((max_iw + POST_THREADS_X - 1) / POST_THREADS_X, (max_ih + POST_THREADS_Y - 1) / POST_THREADS_Y, n),
+                   dim3(POST_THREADS_X, POST_THREADS_Y), 0, side->s>>>(V);
+  CK(cudaEventRecord(side->join, side->s));
+  k_shade_shadow_views<<<grid(max_pix), SHADE_THREADS, 0, st>>>(V);
+  k_shade_lights_views<<<grid(max_pix * 8u), SHADE_THREADS, 0, st>>>(V);
+  k_shade_vox_views<<<grid(max_pix), SHADE_THREADS, 0, st>>>(V);
+  CK(cudaStreamWaitEvent(st, side->join, 0));
+  k_composite_views<<<dim3((max_pw + POST_THREADS_X - 1) / POST_THREADS_X, (max_ph + POST_THREADS_Y - 1) / POST_THREADS_Y,
+                           n),
+                      dim3(POST_THREADS_X, POST_THREADS_Y), 0, st>>>(V);
   CK(cudaGetLastError());
   return VXE_OK;
 }
@@ -921,6 +974,7 @@ void vxe_destroy(vxe_ctx* c) {
                     &L.q_pending, &L.q_refine, &L.q_far, &L.dcount, &L.q_keys, &L.q_perm, &L.bin_count})
       release(*b, L.stream);
     release_frame_state(L.scratch, L.stream);
+    for (auto& m : L.mscratch) release_frame_state(m, L.stream);
     if (L.stream) cudaStreamSynchronize(L.stream);
     side_release(L.side);
     if (L.graph) cudaGraphExecDestroy(L.graph);
@@ -2184,8 +2238,8 @@ vxe_status lane_ready(vxe_ctx* c, uint32_t lane) {
 // Grows the lane's per-frame working buffers to cover an iw x ih frame.  The
 // lane's queued frames may still use the old buffers: those are freed after
 // them, in stream order.
-vxe_status lane_scratch(vxe_ctx* c, BatchLane& L, uint32_t iw, uint32_t ih) {
-  FrameState& S = L.scratch;
+vxe_status lane_scratch(vxe_ctx* c, BatchLane& L, uint32_t iw, uint32_t ih, FrameState* set = nullptr) {
+  FrameState& S = set ? *set : L.scratch;
   if (S.img[IMG_PIXHIT].p && S.iw >= iw && S.ih >= ih) return VXE_OK;
   S.iw = S.pw = std::max(S.iw, iw);
   S.ih = S.ph = std::max(S.ih, ih);
@@ -2287,6 +2341,96 @@ vxe_status vxe_view_render_async(vxe_ctx* c, vxe_view* v, uint32_t lane, const v
   return VXE_OK;
 }
 
+vxe_status vxe_view_render_batch_async(vxe_ctx* c, vxe_view* const* views, const vxe_camera_gpu* cams, uint32_t n,
+                                       uint32_t lane) {
+  using namespace vxe::dev;
+  if (!c || (n && (!views || !cams))) return fail(c, VXE_ERR_INVALID_ARG, "null view arguments");
+  if (n == 0) return VXE_OK;
+  if (n > kMaxViewsPerLaunch)
+    return fail(c, VXE_ERR_CAPACITY, "%u views in one launch > %u", n, kMaxViewsPerLaunch);
+  if (c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL) {  // the one-kernel schedule renders view by view
+    for (uint32_t i = 0; i < n; ++i) {
+      const vxe_status st = vxe_view_render_async(c, views[i], lane, &cams[i]);
+      if (st != VXE_OK) return st;
+    }
+    return VXE_OK;
+  }
+  cudaSetDevice(c->device);
+  vxe_status st = lane_ready(c, lane);
+  if (st != VXE_OK) return st;
+  BatchLane& L = c->lanes[lane];
+  std::vector<vxe_camera_gpu> vc(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    vxe_view* v = views[i];
+    if (!v) return fail(c, VXE_ERR_INVALID_ARG, "null view %u", i);
+    for (uint32_t j = 0; j < i; ++j)
+      if (views[j] == v) return fail(c, VXE_ERR_INVALID_ARG, "view %u appears twice in one launch", i);
+    vc[i] = cams[i];
+    vc[i].chunk_size = c->cam.chunk_size;
+    vc[i].chunk_count = c->cam.chunk_count;
+    for (int k = 0; k < 4; ++k) {
+      vc[i].grid_origin_chunk[k] = c->cam.grid_origin_chunk[k];
+      vc[i].grid_dims[k] = c->cam.grid_dims[k];
+    }
+    if ((st = frame_validate(c, v->fr, vc[i])) != VXE_OK) return st;
+    for (int k = 0; k < IMG_N; ++k)
+      if (!img_is_scratch(k) && img_enabled(c, k) != (v->fr.img[k].p != nullptr))
+        return fail(c, VXE_ERR_INVALID_ARG, "view %u was created under other image flags", i);
+  }
+  for (uint32_t i = 0; i < n; ++i)
+    if ((st = lane_scratch(c, L, views[i]->fr.iw, views[i]->fr.ih, &L.mscratch[i])) != VXE_OK) return st;
+  if (!L.busy) CK(cudaEventRecord(L.ev[0], L.stream));
+  if (c->upload_recorded) CK(cudaStreamWaitEvent(L.stream, c->upload_done, 0));
+  for (uint32_t i = 0; i < n; ++i) {  // each view's frames run in order
+    vxe_view* v = views[i];
+    if (v->last_stream && v->last_stream != L.stream) {
+      CK(cudaEventRecord(v->done, v->last_stream));
+      CK(cudaStreamWaitEvent(L.stream, v->done, 0));
+    }
+  }
+  // The grass cell table serves the launch when every view's camera matches
+  // its tag (same wind); otherwise the marches derive their cells.
+  const int reader = 1 + (int)lane;
+  bool use_grass = false;
+  if ((st = grass_table_acquire(c, L.stream, reader, vc[0], &use_grass)) != VXE_OK) return st;
+  for (uint32_t i = 1; i < n && use_grass; ++i)
+    use_grass = vc[i].voxel_params[0] == vc[0].voxel_params[0] && vc[i].voxel_params[1] == vc[0].voxel_params[1] &&
+                vc[i].voxel_params[2] == vc[0].voxel_params[2] && vc[i].chunk_count == vc[0].chunk_count;
+  auto* V = new (std::nothrow) FrameArgsViews;  // 12 KB: off the stack
+  if (!V) return fail(c, VXE_ERR_OOM, "view arguments");
+  std::unique_ptr<FrameArgsViews> hold(V);
+  std::memset(V, 0, sizeof *V);
+  uint32_t max_iw = 0, max_ih = 0, max_pw = 0, max_ph = 0;
+  uint64_t max_pix = 0, rays = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    FrameState& F = views[i]->fr;
+    frame_fill(c, F, vc[i], V->v[i], &L.mscratch[i]);
+    if (use_grass) grass_table_args(c, V->v[i]);
+    max_iw = std::max(max_iw, F.iw);
+    max_ih = std::max(max_ih, F.ih);
+    max_pw = std::max(max_pw, F.pw);
+    max_ph = std::max(max_ph, F.ph);
+    max_pix = std::max<uint64_t>(max_pix, (uint64_t)F.iw * F.ih);
+    rays += (uint64_t)F.iw * F.ih;
+  }
+  if ((st = views_enqueue(c, *V, n, max_iw, max_ih, max_pw, max_ph, max_pix, L.stream, &L.side)) != VXE_OK)
+    return st;
+  if ((st = grass_table_release(c, L.stream, reader)) != VXE_OK) return st;
+  for (uint32_t i = 0; i < n; ++i) {
+    views[i]->fr.ping = 1 - views[i]->fr.ping;
+    views[i]->last_stream = L.stream;
+  }
+  CK(cudaEventRecord(L.ev[1], L.stream));
+  if (!L.busy) {
+    L.rays = 0;
+    L.items = 0;
+    L.tiles = 0;
+  }
+  L.busy = true;
+  L.rays += rays;
+  return VXE_OK;
+}
+
 vxe_status vxe_view_read_image(vxe_ctx* c, vxe_view* v, int image, void* host, size_t bytes) {
   if (!c || !v || !host) return fail(c, VXE_ERR_INVALID_ARG, "null view arguments");
   const int i = map_image(v->fr, (vxe_image)image);
@@ -2340,6 +2484,61 @@ extern "C" vxe_status vxe_debug_detmath(int which, const float* x, const float* 
     k_detmath<<<(n + 255) / 256, 256>>>(which, d, d + n, d + 2 * (size_t)n, n);
     if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
         cudaMemcpy(out, d + 2 * (size_t)n, (size_t)n * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+      st = VXE_ERR_DEVICE;
+  }
+  cudaFree(d);
+  return st;
+}
+
+namespace {
+// One grass march (which 0) or SDF evaluation (which 1) per thread on
+// caller inputs, for host/device comparisons (vxe_debug_grass).
+__global__ void k_debug_grass(int which, const float* in, float* out, uint32_t n) {
+  using namespace vxe::dev;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  vxe_camera_gpu cam;
+  memset(&cam, 0, sizeof cam);
+  Scene s;
+  memset(&s, 0, sizeof s);
+  s.cam = &cam;
+  if (which == 0) {
+    const float* a = in + (size_t)i * 17;
+    cam.voxel_params[0] = a[14];
+    cam.voxel_params[1] = a[15];
+    cam.voxel_params[2] = a[16];
+    const GrassHit g = try_grass_slab_hit(s, V3(a[0], a[1], a[2]), V3(a[3], a[4], a[5]), a[6], a[7],
+                                          V3(a[8], a[9], a[10]), V3(a[11], a[12], a[13]), a[14], a[15], a[16]);
+    float* o = out + (size_t)i * 5;
+    o[0] = g.hit ? 1.0f : 0.0f;
+    o[1] = g.t;
+    o[2] = g.n.x;
+    o[3] = g.n.y;
+    o[4] = g.n.z;
+  } else {
+    const float* a = in + (size_t)i * 13;
+    cam.voxel_params[0] = a[9];
+    cam.voxel_params[1] = a[10];
+    cam.voxel_params[2] = a[11];
+    out[i] = grass_sdf_lod(s, V3(a[0], a[1], a[2]), V3(a[3], a[4], a[5]), V3(a[6], a[7], a[8]), a[10], a[11],
+                           (uint32_t)a[12]);
+  }
+}
+}  // namespace
+
+extern "C" vxe_status vxe_debug_grass(int which, uint32_t n, const float* in, float* out) {
+  if (!in || !out || which < 0 || which > 1) return VXE_ERR_INVALID_ARG;
+  if (n == 0) return VXE_OK;
+  const size_t nin = (size_t)n * (which == 0 ? 17u : 13u), nout = (size_t)n * (which == 0 ? 5u : 1u);
+  float* d = nullptr;
+  if (cudaMalloc(&d, (nin + nout) * 4) != cudaSuccess) return VXE_ERR_OOM;
+  vxe_status st = VXE_OK;
+  if (cudaMemcpy(d, in, nin * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+    st = VXE_ERR_DEVICE;
+  } else {
+    k_debug_grass<<<(n + 127) / 128, 128>>>(which, d, d + nin, n);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(out, d + nin, nout * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
       st = VXE_ERR_DEVICE;
   }
   cudaFree(d);

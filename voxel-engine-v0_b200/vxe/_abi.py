@@ -13,6 +13,9 @@ from pathlib import Path
 import numpy as np
 
 LIB_PATH = Path(__file__).resolve().parent / "libvxe.so"
+# the same library with device bounds checks (zero records + error word for
+# out-of-range indices instead of clamped reads)
+CHECKED_LIB_PATH = Path(__file__).resolve().parent / "libvxe_checked.so"
 
 VXE_OK = 0
 STATUS_NAMES = {
@@ -32,7 +35,6 @@ FLAG_GODRAY_MACRO_ALIAS = 1 << 0
 FLAG_SILENT_CAPACITY_SKIP = 1 << 1
 FLAG_HIT_RECORDS = 1 << 2
 FLAG_DEBUG_INTERMEDIATES = 1 << 3
-FLAG_CHECKED = 1 << 4
 FLAG_PRIMARY_MEGAKERNEL = 1 << 5
 FLAG_NO_GRASS_TABLE = 1 << 6
 FLAG_UPLOADS_UNORDERED = 1 << 7
@@ -176,6 +178,7 @@ class FrameStats(C.Structure):
 REQ_VIEWPORT, REQ_QUERY = 0, 1
 BATCH_PERSISTENT, BATCH_PLAIN, BATCH_GRAPH = 0, 1, 2
 MAX_BATCH_REQUESTS = 256
+MAX_VIEWS_PER_LAUNCH = 8
 
 
 class Request(C.Structure):
@@ -223,6 +226,7 @@ SIGNATURES = {
     "vxe_read_profile_counts": (C.c_int, [C.c_void_p, C.c_void_p]),
     "vxe_set_record_limits": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
     "vxe_get_frame_stats": (C.c_int, [C.c_void_p, P(FrameStats)]),
+    "vxe_debug_grass": (C.c_int, [C.c_int, C.c_uint32, C.c_void_p, C.c_void_p]),
     "vxe_measure_l2_bandwidth": (C.c_int, [C.c_int, C.c_uint64, C.c_uint32, P(C.c_double)]),
     "vxe_debug_detmath": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
     "vxe_trace_primary_hits_noalloc": (C.c_int, [P(SceneView), P(CameraGpu), P(ClipmapGpu), C.c_void_p,
@@ -234,6 +238,7 @@ SIGNATURES = {
     "vxe_view_lane_bytes": (C.c_uint64, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float]),
     "vxe_view_create": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, P(C.c_void_p)]),
     "vxe_view_render_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, P(CameraGpu)]),
+    "vxe_view_render_batch_async": (C.c_int, [C.c_void_p, P(C.c_void_p), P(CameraGpu), C.c_uint32, C.c_uint32]),
     "vxe_view_read_image": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]),
     "vxe_view_destroy": (C.c_int, [C.c_void_p, C.c_void_p]),
     "vxe_build_chunk": (C.c_int, [P(WorldParams), C.c_int32, C.c_int32, C.c_int32, P(BuiltChunk)]),
@@ -267,22 +272,23 @@ class VxeError(RuntimeError):
         super().__init__(f"{where}: {STATUS_NAMES.get(status, status)}" + (f" ({msg})" if msg else ""))
 
 
-_lib = None
+_libs = {}
 
 
-def lib() -> C.CDLL:
-    """Loads libvxe.so.  There is no fallback: a missing library is an error."""
-    global _lib
-    if _lib is None:
-        if not LIB_PATH.exists():
-            raise FileNotFoundError(f"{LIB_PATH} is missing; run `python voxel-engine-v0_b200/vxe_build.py` first")
-        l = C.CDLL(str(LIB_PATH))
+def lib(checked: bool = False) -> C.CDLL:
+    """Loads libvxe.so (or, with `checked`, libvxe_checked.so).  There is no
+    fallback: a missing library is an error."""
+    path = CHECKED_LIB_PATH if checked else LIB_PATH
+    if path not in _libs:
+        if not path.exists():
+            raise FileNotFoundError(f"{path} is missing; run `python voxel-engine-v0_b200/vxe_build.py` first")
+        l = C.CDLL(str(path))
         for name, (res, args) in SIGNATURES.items():
             fn = getattr(l, name)
             fn.restype = res
             fn.argtypes = args
-        _lib = l
-    return _lib
+        _libs[path] = l
+    return _libs[path]
 
 
 # The host-side producers (chunk builder, camera packing, clipmap state) are

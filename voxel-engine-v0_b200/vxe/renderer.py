@@ -17,8 +17,11 @@ from .world import Upload, World
 class Renderer:
     def __init__(self, width: int, height: int, render_scale: float = 0.5, *, node_capacity: int,
                  chunk_capacity: int, grid_capacity: int, clip_levels: int = 16, clip_res: int = 256,
-                 flags: int = A.FLAG_GODRAY_MACRO_ALIAS, device: int = 0):
-        self._lib = A.lib()
+                 flags: int = A.FLAG_GODRAY_MACRO_ALIAS, device: int = 0, checked: bool = False):
+        """`checked`: run on libvxe_checked.so (device bounds checks reported
+        in the error word) instead of libvxe.so (clamped reads)."""
+        self._lib = A.lib(checked)
+        self.checked = checked
         cfg = A.Config(node_capacity, chunk_capacity, grid_capacity, clip_levels, clip_res, flags, device, 0)
         h = C.c_void_p()
         st = self._lib.vxe_create(C.byref(cfg), C.byref(h))
@@ -306,6 +309,18 @@ class Renderer:
 
     def view(self, width: int, height: int, render_scale: float) -> "View":
         return View(self, width, height, render_scale)
+
+    def render_views_async(self, lane: int, views_and_cameras) -> None:
+        """One frame of each (view, camera) pair on `lane`, every pass launched
+        once for up to MAX_VIEWS_PER_LAUNCH views (vxe_view_render_batch_async);
+        longer lists go in several launches."""
+        items = list(views_and_cameras)
+        for i in range(0, len(items), A.MAX_VIEWS_PER_LAUNCH):
+            part = items[i:i + A.MAX_VIEWS_PER_LAUNCH]
+            hs = (C.c_void_p * len(part))(*[v._h.value for v, _ in part])
+            cams = (A.CameraGpu * len(part))(*[cam for _, cam in part])
+            self._check(self._lib.vxe_view_render_batch_async(self._ctx, hs, cams, len(part), lane),
+                        "vxe_view_render_batch_async")
 
     # -- queries ----------------------------------------------------------------
     def trace_rays(self, origins: np.ndarray, dirs: np.ndarray, tmax: float) -> np.ndarray:

@@ -22,8 +22,9 @@ The server loop
     one-off viewport or query counts its outputs and inputs,
   * starts work on any free lane with everything admitted so far -- one
     persistent batch for viewports and queries, then the session frames on the
-    same lane's stream -- so work that arrives while other lanes run overlaps
-    with them on the device,
+    same lane's stream, every pass of up to 8 sessions' frames in one launch
+    (vxe_view_render_batch_async) -- so work that arrives while other lanes
+    run overlaps with them on the device,
   * keeps a session's frames in order (one in flight at a time),
   * re-uploads chunks on the context's upload stream every tick (the reference
     applies streamed uploads every frame),
@@ -277,10 +278,11 @@ def serve(renderer, world: World, requests, torch, mem_budget: int | None, lanes
     waiting = deque()
     inflight = {}       # lane -> requests
     busy_sessions = set()
-    # each lane that renders session frames holds working buffers for the
-    # largest session
+    # each lane that renders session frames holds one set of working buffers
+    # per view of a launch, each for the largest session
     lane_bytes = max((renderer.view_lane_bytes(s.w, s.h, s.render_scale) for s in sessions or []), default=0)
-    reserved = lanes * lane_bytes
+    per_launch = min(max_batch, A.MAX_VIEWS_PER_LAUNCH, len(sessions or []))
+    reserved = lanes * lane_bytes * max(1, per_launch)
     views = _Views(renderer, sessions or [])
     rng = np.random.default_rng(99)
     resident = [k for k in world.slot_to_key if not world.chunk(k).macro_empty]
@@ -340,9 +342,11 @@ def serve(renderer, world: World, requests, torch, mem_budget: int | None, lanes
                         rq = [_to_request(r, torch) for r in batch]
                         torch.cuda.current_stream().synchronize()  # query inputs are on the device
                         renderer.submit_batch_async(lane, rq, tile, rpt, mode)
-                    for r in frames:
-                        views.get(r.session).render_async(lane, _frame_camera(world, sessions, r))
-                        busy_sessions.add(r.session)
+                    # the admitted frames of every session: each pass launched
+                    # once for up to MAX_VIEWS_PER_LAUNCH views
+                    renderer.render_views_async(lane, [(views.get(r.session), _frame_camera(world, sessions, r))
+                                                       for r in frames])
+                    busy_sessions.update(r.session for r in frames)
                     inflight[lane] = batch + frames
                     batches += 1
                     max_inflight = max(max_inflight, len(inflight))
@@ -360,10 +364,17 @@ def serve(renderer, world: World, requests, torch, mem_budget: int | None, lanes
     return ServeReport(lat, sum(r.rays for r in reqs), seconds, batches, max_inflight, uploads, extra)
 
 
-def serve_plain(renderer, world: World, requests, torch, keep_outputs: bool = False, sessions=None) -> ServeReport:
-    """Baseline: FIFO, one request at a time (frames alone on lane 0, batches as plain launches)."""
+def serve_plain(renderer, world: World, requests, torch, keep_outputs: bool = False, sessions=None,
+                single_launch_pass: bool = False) -> ServeReport:
+    """Baseline: FIFO, one request at a time (frames alone on lane 0, batches as
+    plain launches).  `single_launch_pass`: frames in the one-kernel-per-pass
+    schedule (VXE_FLAG_PRIMARY_MEGAKERNEL: the reference's pass structure)
+    instead of the wavefront."""
     reqs = sorted(requests, key=lambda r: r.arrival)
     views = _Views(renderer, sessions or [])
+    flags0 = renderer.flags
+    if single_launch_pass:
+        renderer.set_flags(flags0 | A.FLAG_PRIMARY_MEGAKERNEL)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     try:
@@ -388,5 +399,6 @@ def serve_plain(renderer, world: World, requests, torch, keep_outputs: bool = Fa
         seconds = time.perf_counter() - t0
     finally:
         views.close()
+        renderer.set_flags(flags0)
     lat = [(r.done - r.arrival) * 1e3 for r in reqs]
     return ServeReport(lat, sum(r.rays for r in reqs), seconds, len(reqs), 1, 0)

@@ -693,9 +693,9 @@ class Clipmap:
     def update_device(self, renderer, cam_x: float, cam_z: float):
         """The same update with the patch texels evaluated on the device straight
         into `renderer`'s clipmap (no host texels; the host mirror is not updated)."""
-        st = A.lib().vxe_clipmap_update_device(renderer._ctx, self._h, cam_x, cam_z)
+        st = renderer._lib.vxe_clipmap_update_device(renderer._ctx, self._h, cam_x, cam_z)
         if st != A.VXE_OK:
-            raise A.VxeError(st, "vxe_clipmap_update_device", A.lib().vxe_last_error(renderer._ctx).decode())
+            raise A.VxeError(st, "vxe_clipmap_update_device", renderer._lib.vxe_last_error(renderer._ctx).decode())
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -2,7 +2,10 @@
 
 * ``vxe/libvxe.so`` -- the product: sm_100a CUDA passes + C ABI + C++
   producers, compiled with ``-fmad=false -prec-div=true -prec-sqrt=true`` so
-  every float operation is a single IEEE binary32 op.
+  every float operation is a single IEEE binary32 op; reads of the world's
+  records at data-derived indices are clamped into their buffers.
+* ``vxe/libvxe_checked.so`` -- the same with device bounds checks: an index
+  outside its buffer reads a zero record and sets the context's error word.
 * ``oracle/liboracle_vxe.so`` -- the CPU restatement used by tests and the
   CPU baseline (``-ffp-contract=off``, no fast math).
 * ``oracle/libref_producer.so`` -- the host-side producers (chunk builder,
@@ -24,6 +27,7 @@ REPO = PKG.parent
 INCLUDE = REPO / "include"
 CSRC = PKG / "csrc"
 LIB = PKG / "vxe" / "libvxe.so"
+LIB_CHECKED = PKG / "vxe" / "libvxe_checked.so"
 ORACLE_SRC = REPO / "oracle" / "vxe_oracle.cpp"
 ORACLE_LIB = REPO / "oracle" / "liboracle_vxe.so"
 REF_PRODUCER_LIB = REPO / "oracle" / "libref_producer.so"
@@ -69,28 +73,31 @@ def _run(cmd, verbose):
     return r
 
 
-def build_lib(verbose: bool = False, force: bool = False, ptxas_verbose: bool = False) -> Path:
+def build_lib(verbose: bool = False, force: bool = False, ptxas_verbose: bool = False, checked: bool = False) -> Path:
+    target = LIB_CHECKED if checked else LIB
     cu, cpp, headers = _sources()
-    if not force and not _stale(LIB, cu + cpp + headers + [Path(__file__)]):
-        return LIB
-    BUILD_DIR.mkdir(exist_ok=True)
+    if not force and not _stale(target, cu + cpp + headers + [Path(__file__)]):
+        return target
+    bdir = BUILD_DIR / ("checked" if checked else "fast")
+    bdir.mkdir(parents=True, exist_ok=True)
     nvcc = _nvcc()
     objs = []
     for src in cu:
-        obj = BUILD_DIR / (src.stem + ".o")
+        obj = bdir / (src.stem + ".o")
         extra = ["-Xptxas", "-v"] if ptxas_verbose else []
-        r = _run([nvcc, *NVCC_FLAGS, *extra, "-c", src, "-o", obj], verbose)
+        r = _run([nvcc, *NVCC_FLAGS, f"-DVXE_DEVICE_CHECKS={1 if checked else 0}", *extra, "-c", src, "-o", obj],
+                 verbose)
         if ptxas_verbose:
             print(r.stderr)
         objs.append(obj)
     for src in cpp:
-        obj = BUILD_DIR / (src.stem + ".o")
+        obj = bdir / (src.stem + ".o")
         _run(["g++", *CXX_FLAGS, "-c", src, "-o", obj], verbose)
         objs.append(obj)
-    tmp = LIB.with_suffix(".so.tmp")
+    tmp = target.with_suffix(".so.tmp")
     _run([nvcc, ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs], verbose)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, target)
+    return target
 
 
 def build_oracle(verbose: bool = False, force: bool = False) -> Path:
@@ -116,6 +123,7 @@ def build_ref_producer(verbose: bool = False, force: bool = False) -> Path:
 
 def build_all(verbose: bool = False, force: bool = False) -> None:
     build_lib(verbose=verbose, force=force)
+    build_lib(verbose=verbose, force=force, checked=True)
     build_oracle(verbose=verbose, force=force)
     build_ref_producer(verbose=verbose, force=force)
 
