@@ -1333,13 +1333,16 @@ __device__ __forceinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(co
     if (tcur > t_exit) break;
     const v3 p = ro + rd * tcur;
     const v3 pq = p + ray_eps_vec(rd, 1e-4f * vs);
-    // the pending descent, then (as after any descent) a re-descent from the
-    // anchor or the root when the leaf does not hold the point
+    // the pending descent (the one the reference makes at the end of the
+    // previous iteration), then the reference's check at the top of an
+    // iteration: a re-descent from the anchor or the root when the leaf does
+    // not hold the point.  That re-descent is not checked again.
     for (uint32_t pass = 0; pass < 2u; ++pass) {
       uint32_t si;
       v3 sb;
       float ss;
       bool upd = true;
+      const bool pending = pend;
       if (pend) {
         si = pend_idx;
         sb = pend_bmin;
@@ -1360,6 +1363,7 @@ __device__ __forceinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(co
         if (na.valid && (!an.valid || na.key != an.key)) an = na;
       }
       have_leaf = true;
+      if (!pending) break;
     }
     const CubeSlab slab = cube_slab_inv(ro, inv, leaf.bmin, leaf.size);
     const float t_leave = slab.t_exit;
