@@ -982,9 +982,9 @@ def main():
             "kernel": "trace stage: k_primary_trace + k_probe_dda + k_slab_eval + k_slab_pick + k_primary_resolve",
             "peak_kind": peak_kind, "launch_ms": round(trace_s * 1e3, 4),
             "walk_kernel_ms": round(statistics.mean(res["walk_ms"]), 4)}
+    present = tuple(int(v) for v in args.present.split("x"))
     if not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        present = tuple(int(v) for v in args.present.split("x"))
         cs = cpu_sample(args.cpu_seconds, present, threads)
         line["cpu_baseline"] = {"value": round(cs["rays"] / cs["seconds"] / 1e6, 4), "unit": UNIT, "cores": threads,
                                 "kind": "port",
@@ -1003,14 +1003,12 @@ def main():
         roof["primary_pass"] = {"kernels": "k_primary_trace + k_shade_vox + k_shade_far",
                                 "achieved": round(pa, 2), "frac": round(pa / peak, 5),
                                 "algorithmic_bytes_per_frame": ab, "ms": round(prim_s * 1e3, 4)}
-    # DRAM bytes of the trace stage per frame from the committed ncu summary
-    traffic = REPO / "profiles" / "trace_stage_config2_dram.md"
-    if traffic.exists():
-        import re
-
-        m = re.search(r"dram_bytes_per_stage_1080p:\s*([0-9]+)", traffic.read_text())
-        if m:
-            roof["traffic"] = int(m.group(1))
+    # DRAM bytes of the trace stage per 1080p frame: one ncu capture of the
+    # same five kernels on this workload (data file beside the profiles)
+    traffic = REPO / "profiles" / "trace_stage_config2_1080p_dram.json"
+    if traffic.exists() and present == (1920, 1080):
+        roof["traffic"] = int(json.loads(traffic.read_text())["dram_bytes_per_stage"])
+        roof["traffic_source"] = "ncu dram__bytes_read.sum + dram__bytes_write.sum, frame 1 of this path"
     line["roofline"] = roof
     print(json.dumps(line))
 
