@@ -618,17 +618,18 @@ def build_profile(n: int) -> None:
 
 
 def run_configs(dev):
-    """Secondary frame lines: config 5 (32x8x32 chunks, 6-level 512^2 clipmap,
-    3840x2160 present / 1920x1080 internal) and config 2 at render scale 1.0."""
+    """Secondary frame lines: config 1 (one 64^3 chunk, 256x144 frames),
+    config 5 (32x8x32 chunks, 6-level 512^2 clipmap, 3840x2160 present /
+    1920x1080 internal) and config 2 at render scale 1.0."""
     from vxe import scenes
 
     out = {}
-    for key, sc in (("config5_4k", scenes.config5()),
-                    ("config2_scale1", scenes.config2(present=(1920, 1080), render_scale=1.0))):
+    for key, sc, steps in (("config1", scenes.config1(), 32), ("config5_4k", scenes.config5(), 8),
+                           ("config2_scale1", scenes.config2(present=(1920, 1080), render_scale=1.0), 8)):
         sc.shift_every = 0
-        ms, rays = frame_series(sc, dev, steps=8, warmup=4)
-        out[key] = {"present": list(sc.present), "internal": list(sc.internal), "frame_ms": round(ms, 3),
-                    "mrays_per_s": round(rays / ms / 1e3, 3), "steps": 8, "warmup": 4,
+        ms, rays = frame_series(sc, dev, steps=steps, warmup=4)
+        out[key] = {"present": list(sc.present), "internal": list(sc.internal), "frame_ms": round(ms, 4),
+                    "mrays_per_s": round(rays / ms / 1e3, 3), "steps": steps, "warmup": 4,
                     "l2": "flushed between steps"}
     return out
 
