@@ -5,11 +5,20 @@
  * differ between vendors and from libm on the host, which would make a
  * bit-exact CPU/GPU comparison impossible.  Every function here is written
  * from the mathematics (Cody & Waite argument reduction, "Software Manual for
- * the Elementary Functions", 1980, plus truncated Taylor / atanh series) and
- * evaluated in IEEE binary64 with a fixed operation order, then rounded once
- * to binary32.  Compiled without FMA contraction (host: -ffp-contract=off,
- * device: -fmad=false) both sides produce identical bits; the relative error
- * of every float result is below 1 ulp (checked in tests/test_detmath.py).
+ * the Elementary Functions", 1980, plus truncated Taylor / atanh series) with a
+ * fixed operation order.  Only correctly rounded IEEE operations are used:
+ * +, -, *, /, and fused multiply-adds written out explicitly (vxe_fmaf,
+ * vxe_fma: one rounding on every machine).  Compiled without FMA contraction
+ * (host: -ffp-contract=off, device: -fmad=false), both sides therefore produce
+ * identical bits.
+ *
+ * exp, sin and cos are evaluated in binary32, with fused multiply-adds in the
+ * argument reduction and in the Horner steps: exp within 1 ulp, sin and cos
+ * within 1.5 ulp (8e-8 absolute near their zeros), inside WGSL's own bounds
+ * for these builtins (exp 3 + 2|x| ulp, sin / cos 2^-11 absolute on [-pi, pi]).
+ * sin and cos of |x| > 65536 use a binary64 reduction.  pow needs log x to
+ * more bits than binary32 holds, so it is evaluated in binary64 and rounded
+ * once: within 1 ulp.  The bounds are checked in tests/test_detmath.py.
  */
 #ifndef VXE_DETMATH_H
 #define VXE_DETMATH_H
@@ -67,69 +76,125 @@ VXE_HD double vxe_floor_d(double x) {
 #endif
 }
 
+VXE_HD float vxe_u2f(uint32_t u) {
+#if defined(__CUDA_ARCH__)
+  return __uint_as_float(u);
+#else
+  float f;
+  memcpy(&f, &u, sizeof(f));
+  return f;
+#endif
+}
+
+/* Fused multiply-adds (one rounding) and round-to-nearest-even; correctly
+ * rounded on both sides. */
+VXE_HD float vxe_fmaf(float a, float b, float c) {
+#if defined(__CUDA_ARCH__)
+  return __fmaf_rn(a, b, c);
+#else
+  return __builtin_fmaf(a, b, c);
+#endif
+}
+
+VXE_HD double vxe_fma(double a, double b, double c) {
+#if defined(__CUDA_ARCH__)
+  return __fma_rn(a, b, c);
+#else
+  return __builtin_fma(a, b, c);
+#endif
+}
+
+VXE_HD float vxe_rintf(float x) {
+#if defined(__CUDA_ARCH__)
+  return rintf(x);
+#else
+  return __builtin_rintf(x);
+#endif
+}
+
+/* 2^k for integer k in [-126, 127]. */
+VXE_HD float vxe_pow2if(int k) { return vxe_u2f((uint32_t)(k + 127) << 23); }
+
 /* 2^k for integer k in [-1022, 1023] built from its bit pattern. */
 VXE_HD double vxe_pow2i(int k) { return vxe_u2d((uint64_t)(int64_t)(k + 1023) << 52); }
 
-/* e^x in binary64 (|x| <= 745 handled; beyond returns inf / 0). */
+/* e^x in binary64 to 2^-32 relative, for results rounded to binary32
+ * (|x| <= 745 handled; beyond returns inf / 0). */
 VXE_HD double vxe_exp_d(double x) {
   if (x != x) return x;
   if (x > 709.0) return vxe_u2d(0x7FF0000000000000ull);
   if (x < -745.0) return 0.0;
   const double kd = vxe_floor_d(x * VXE_LOG2E + 0.5);
   const int k = (int)kd;
-  const double r = (x - kd * VXE_LN2_1) - kd * VXE_LN2_2; /* |r| <= 0.3466 */
-  /* Taylor series of e^r to degree 12, Horner form. */
-  double p = 2.08767569878681e-09;
-  p = p * r + 2.505210838544172e-08;
-  p = p * r + 2.755731922398589e-07;
-  p = p * r + 2.7557319223985893e-06;
-  p = p * r + 2.48015873015873e-05;
-  p = p * r + 0.0001984126984126984;
-  p = p * r + 0.001388888888888889;
-  p = p * r + 0.008333333333333333;
-  p = p * r + 0.041666666666666664;
-  p = p * r + 0.16666666666666666;
-  p = p * r + 0.5;
-  p = p * r + 1.0;
-  p = p * r + 1.0;
+  const double r = vxe_fma(-kd, VXE_LN2_2, vxe_fma(-kd, VXE_LN2_1, x)); /* |r| <= 0.3466 */
+  /* Taylor series of e^r to degree 8 (truncation below 2^-32: enough for a
+   * result rounded to binary32), Horner form. */
+  double p = 1.0 / 40320.0;
+  p = vxe_fma(p, r, 1.0 / 5040.0);
+  p = vxe_fma(p, r, 1.0 / 720.0);
+  p = vxe_fma(p, r, 1.0 / 120.0);
+  p = vxe_fma(p, r, 1.0 / 24.0);
+  p = vxe_fma(p, r, 1.0 / 6.0);
+  p = vxe_fma(p, r, 0.5);
+  p = vxe_fma(p, r, 1.0);
+  p = vxe_fma(p, r, 1.0);
   if (k < -1000) return (p * vxe_pow2i(k + 200)) * vxe_pow2i(-200);
   return p * vxe_pow2i(k);
 }
 
-/* Natural log in binary64 for x > 0 (0 -> -inf, x < 0 or NaN -> NaN). */
-VXE_HD double vxe_log_d(double x) {
-  if (x != x || x < 0.0) return vxe_u2d(0x7FF8000000000000ull);
-  if (x == 0.0) return vxe_u2d(0xFFF0000000000000ull);
-  if (x == vxe_u2d(0x7FF0000000000000ull)) return x;
-  uint64_t u = vxe_d2u(x);
-  int e = (int)((u >> 52) & 0x7FF);
-  if (e == 0) { /* subnormal binary64: normalise */
-    x = x * 18014398509481984.0; /* 2^54 */
-    u = vxe_d2u(x);
-    e = (int)((u >> 52) & 0x7FF) - 54;
+VXE_HD uint32_t vxe_f2u(float f) {
+#if defined(__CUDA_ARCH__)
+  return __float_as_uint(f);
+#else
+  uint32_t u;
+  memcpy(&u, &f, sizeof(u));
+  return u;
+#endif
+}
+
+/* 1/x correctly rounded in binary32. */
+VXE_HD float vxe_rcpf(float x) {
+#if defined(__CUDA_ARCH__)
+  return __frcp_rn(x);
+#else
+  return 1.0f / x;
+#endif
+}
+
+/* Natural log of a finite binary32 x > 0, in binary64 to about 2^-40
+ * absolute (for pow).  x = 2^e m with m in [sqrt(1/2), sqrt(2)); log m =
+ * 2 atanh(s), s = (m-1)/(m+1), |s| <= 0.1716, the division as a binary32
+ * reciprocal and one Newton step. */
+VXE_HD double vxe_log_f(float x) {
+  uint32_t u = vxe_f2u(x);
+  int e = (int)((u >> 23) & 0xFFu);
+  if (e == 0) { /* subnormal: normalise (exact) */
+    u = vxe_f2u(x * 16777216.0f);
+    e = (int)((u >> 23) & 0xFFu) - 24;
   }
-  e -= 1023;
-  double m = vxe_u2d((u & 0x000FFFFFFFFFFFFFull) | 0x3FF0000000000000ull); /* [1,2) */
+  e -= 127;
+  double m = (double)vxe_u2f((u & 0x007FFFFFu) | 0x3F800000u); /* [1,2) */
   if (m > 1.4142135623730951) {
     m = m * 0.5;
     e += 1;
   }
-  /* log m = 2 atanh(s), s = (m-1)/(m+1), |s| <= 0.1716 */
-  const double s = (m - 1.0) / (m + 1.0);
+  const double d = m + 1.0; /* exact: m has 24 significant bits */
+  double r = (double)vxe_rcpf((float)d);
+  r = vxe_fma(r, vxe_fma(-d, r, 1.0), r);
+  const double s = (m - 1.0) * r;
   const double s2 = s * s;
-  double q = 1.0 / 19.0;
-  q = q * s2 + 1.0 / 17.0;
-  q = q * s2 + 1.0 / 15.0;
-  q = q * s2 + 1.0 / 13.0;
-  q = q * s2 + 1.0 / 11.0;
-  q = q * s2 + 1.0 / 9.0;
-  q = q * s2 + 1.0 / 7.0;
-  q = q * s2 + 1.0 / 5.0;
-  q = q * s2 + 1.0 / 3.0;
-  q = q * s2 + 1.0;
+  /* 2 atanh(s) = 2 s (1 + s^2/3 + ...), terms to s^15 (below 2^-41) */
+  double q = 1.0 / 15.0;
+  q = vxe_fma(q, s2, 1.0 / 13.0);
+  q = vxe_fma(q, s2, 1.0 / 11.0);
+  q = vxe_fma(q, s2, 1.0 / 9.0);
+  q = vxe_fma(q, s2, 1.0 / 7.0);
+  q = vxe_fma(q, s2, 1.0 / 5.0);
+  q = vxe_fma(q, s2, 1.0 / 3.0);
+  q = vxe_fma(q, s2, 1.0);
   const double lm = 2.0 * s * q;
   const double ed = (double)e;
-  return (ed * VXE_LN2_1 + lm) + ed * VXE_LN2_2;
+  return vxe_fma(ed, VXE_LN2_2, vxe_fma(ed, VXE_LN2_1, lm));
 }
 
 /* sin / cos of r for |r| <= pi/4 (Taylor to degree 15 / 16). */
@@ -165,12 +230,52 @@ VXE_HD double vxe_reduce_pio2(double x, int* q) {
   return ((x - kd * VXE_PIO2_1) - kd * VXE_PIO2_2) - kd * VXE_PIO2_3;
 }
 
-VXE_HD_CALL float vxe_sinf(float xf) {
-  const double x = (double)xf;
+/* binary32 pi/2 split into three pieces (the first is pi/2 rounded to
+ * binary32), for the fused reduction below. */
+#define VXE_PIO2F_1 1.5707963705062866f
+#define VXE_PIO2F_2 -4.371138828673793e-08f
+#define VXE_PIO2F_3 -1.7151245100058819e-15f
+
+/* x - k pi/2 for |x| <= 65536 (|k| < 2^16): every product enters a fused
+ * multiply-add unrounded, so only the three sums round. */
+VXE_HD float vxe_reduce_pio2f(float x, int* q) {
+  const float kf = vxe_rintf(x * 0.6366197466850281f);
+  *q = (int)kf & 3;
+  float r = vxe_fmaf(-kf, VXE_PIO2F_1, x);
+  r = vxe_fmaf(-kf, VXE_PIO2F_2, r);
+  return vxe_fmaf(-kf, VXE_PIO2F_3, r);
+}
+
+/* sin r and cos r for |r| <= pi/4 (+ rounding): Taylor series to degree 11
+ * and 12 (truncation below 2^-29), Horner form in r^2. */
+VXE_HD float vxe_sin_polyf(float r) {
+  const float s = r * r;
+  float p = -1.0f / 39916800.0f;
+  p = vxe_fmaf(p, s, 1.0f / 362880.0f);
+  p = vxe_fmaf(p, s, -1.0f / 5040.0f);
+  p = vxe_fmaf(p, s, 1.0f / 120.0f);
+  p = vxe_fmaf(p, s, -1.0f / 6.0f);
+  return vxe_fmaf(r * s, p, r);
+}
+
+VXE_HD float vxe_cos_polyf(float r) {
+  const float s = r * r;
+  float p = 1.0f / 479001600.0f;
+  p = vxe_fmaf(p, s, -1.0f / 3628800.0f);
+  p = vxe_fmaf(p, s, 1.0f / 40320.0f);
+  p = vxe_fmaf(p, s, -1.0f / 720.0f);
+  p = vxe_fmaf(p, s, 1.0f / 24.0f);
+  p = vxe_fmaf(p, s, -0.5f);
+  return vxe_fmaf(s, p, 1.0f);
+}
+
+/* sin / cos of |x| > 65536 (and NaN / inf): binary64 reduction. */
+VXE_HD float vxe_sincos_wide(double x, int cosine) {
   if (x != x || x - x != 0.0) return (float)(x - x); /* NaN for NaN / inf */
-  if (x > 1e18 || x < -1e18) return 0.0f;              /* beyond the reduction */
+  if (x > 1e18 || x < -1e18) return cosine ? 1.0f : 0.0f; /* beyond the reduction */
   int q;
   const double r = vxe_reduce_pio2(x, &q);
+  q = (q + cosine) & 3;
   double v;
   if (q == 0) v = vxe_sin_poly(r);
   else if (q == 1) v = vxe_cos_poly(r);
@@ -179,29 +284,61 @@ VXE_HD_CALL float vxe_sinf(float xf) {
   return (float)v;
 }
 
-VXE_HD_CALL float vxe_cosf(float xf) {
-  const double x = (double)xf;
-  if (x != x || x - x != 0.0) return (float)(x - x);
-  if (x > 1e18 || x < -1e18) return 1.0f;
+VXE_HD_CALL float vxe_sinf(float x) {
+  if (!(x >= -65536.0f && x <= 65536.0f)) return vxe_sincos_wide((double)x, 0);
   int q;
-  const double r = vxe_reduce_pio2(x, &q);
-  double v;
-  if (q == 0) v = vxe_cos_poly(r);
-  else if (q == 1) v = -vxe_sin_poly(r);
-  else if (q == 2) v = -vxe_cos_poly(r);
-  else v = vxe_sin_poly(r);
-  return (float)v;
+  const float r = vxe_reduce_pio2f(x, &q);
+  if (q == 0) return vxe_sin_polyf(r);
+  if (q == 1) return vxe_cos_polyf(r);
+  if (q == 2) return -vxe_sin_polyf(r);
+  return -vxe_cos_polyf(r);
 }
 
-VXE_HD_CALL float vxe_expf(float x) { return (float)vxe_exp_d((double)x); }
+VXE_HD_CALL float vxe_cosf(float x) {
+  if (!(x >= -65536.0f && x <= 65536.0f)) return vxe_sincos_wide((double)x, 1);
+  int q;
+  const float r = vxe_reduce_pio2f(x, &q);
+  if (q == 0) return vxe_cos_polyf(r);
+  if (q == 1) return -vxe_sin_polyf(r);
+  if (q == 2) return -vxe_cos_polyf(r);
+  return vxe_sin_polyf(r);
+}
+
+/* e^x in binary32: x = k ln 2 + r (fused Cody-Waite, ln 2 split at 16
+ * significant bits), e^r = 1 + r q(r) with q the Taylor series of
+ * (e^r - 1) / r to degree 7, then the exact scale by 2^k. */
+VXE_HD_CALL float vxe_expf(float x) {
+  if (x != x) return x;
+  if (x > 88.72283935546875f) return vxe_u2f(0x7F800000u);
+  if (x < -103.97208404541015625f) return 0.0f;
+  const float kf = vxe_rintf(x * 1.4426950216293335f);
+  float r = vxe_fmaf(-kf, 0.693145751953125f, x);
+  r = vxe_fmaf(-kf, 1.428606765330187e-06f, r);
+  float q = 1.0f / 40320.0f;
+  q = vxe_fmaf(q, r, 1.0f / 5040.0f);
+  q = vxe_fmaf(q, r, 1.0f / 720.0f);
+  q = vxe_fmaf(q, r, 1.0f / 120.0f);
+  q = vxe_fmaf(q, r, 1.0f / 24.0f);
+  q = vxe_fmaf(q, r, 1.0f / 6.0f);
+  q = vxe_fmaf(q, r, 0.5f);
+  q = vxe_fmaf(q, r, 1.0f);
+  const float e = vxe_fmaf(r, q, 1.0f);
+  const int k = (int)kf;
+  if (k > 127) return (e * 2.0f) * vxe_pow2if(k - 1);
+  if (k < -125) return (e * vxe_pow2if(k + 64)) * vxe_pow2if(-64);
+  return e * vxe_pow2if(k);
+}
 
 /* pow for the non-negative bases the passes use: pow(0, y>0) = 0,
  * pow(x, 0) = 1, negative bases give NaN (WGSL leaves them undefined). */
 VXE_HD_CALL float vxe_powf(float x, float y) {
   if (y == 0.0f) return 1.0f;
-  if (x == 0.0f) return y > 0.0f ? 0.0f : vxe_u2d(0x7FF0000000000000ull);
+  if (x == 0.0f) return y > 0.0f ? 0.0f : vxe_u2f(0x7F800000u);
   if (x == 1.0f) return 1.0f;
-  return (float)vxe_exp_d((double)y * vxe_log_d((double)x));
+  if (!(x > 0.0f)) return vxe_u2f(0x7FC00000u);                      /* negative or NaN base */
+  if (x == vxe_u2f(0x7F800000u)) return y > 0.0f ? x : 0.0f;         /* +inf base */
+  if (y != y) return y;
+  return (float)vxe_exp_d((double)y * vxe_log_f(x));
 }
 
 #endif /* VXE_DETMATH_H */

@@ -11,20 +11,23 @@ def ulp_err(got, ref64):
     return np.abs(got - ref64) / np.maximum(spacing, np.finfo(np.float32).tiny)
 
 
-def test_sin_cos_within_one_ulp():
+def test_sin_cos_within_one_and_a_half_ulp():
     rng = np.random.default_rng(1)
-    x = np.concatenate([rng.uniform(-10, 10, 20000), rng.uniform(-5e5, 5e5, 20000)]).astype(np.float32)
+    # binary32 path (|x| <= 65536) and the binary64 reduction beyond it
+    x = np.concatenate([rng.uniform(-10, 10, 200000), rng.uniform(-65536, 65536, 200000),
+                        rng.uniform(-5e5, 5e5, 50000)]).astype(np.float32)
     for which, fn in ((0, np.sin), (1, np.cos)):
         got = O.detmath(which, x)
         ref = fn(x.astype(np.float64))
-        # absolute error near zeros of sin/cos is measured against 1 ulp of 1.0
+        # near the zeros of sin/cos the error is measured in absolute terms
         err = np.abs(got.astype(np.float64) - ref)
-        assert (err <= np.maximum(np.spacing(np.abs(ref).astype(np.float32)).astype(np.float64), 6e-8)).all()
+        assert (err <= np.maximum(1.5 * np.spacing(np.abs(ref).astype(np.float32)).astype(np.float64), 8e-8)).all()
 
 
 def test_exp_within_one_ulp():
     rng = np.random.default_rng(2)
-    x = rng.uniform(-80, 80, 40000).astype(np.float32)
+    x = np.concatenate([rng.uniform(-80, 80, 200000), rng.uniform(-1, 1, 100000),
+                        rng.uniform(-103, -87, 50000)]).astype(np.float32)
     got = O.detmath(2, x)
     assert ulp_err(got, np.exp(x.astype(np.float64))).max() <= 1.0
 
