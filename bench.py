@@ -193,8 +193,9 @@ def run_batch_serve(dev):
     probes), device time from the lane's CUDA events, best of 3.
     serve: 120 Poisson requests at 1000 req/s (70 % viewports 256^2-1920x1080,
     30 % query batches 1k-256k rays), continuous batching over 2 lanes with a
-    4 GiB admission budget and 10 chunk re-uploads per 16 ms tick, vs the plain
-    one-request-at-a-time server; latency = completion - arrival (host clock).
+    4 GiB admission budget, vs the plain one-request-at-a-time server; both
+    re-upload 10 resident chunks per 16 ms tick; latency = completion -
+    arrival (host clock).
     serve.sessions: the same with session frames (resident histories) at a
     saturating (1000 req/s) and a light (200 req/s) load.
     """
@@ -245,8 +246,8 @@ def run_batch_serve(dev):
         rep, rep_s = median_run(lambda: serve(r, w, make_arrivals(w, 1000.0, 120, seed=7), torch,
                                               mem_budget=4 << 30, lanes=2, max_batch=32))
         base, base_s = median_run(lambda: serve_plain(r, w, make_arrivals(w, 1000.0, 120, seed=7), torch))
-        srv = {"workload": "120 Poisson requests at 1000 req/s, 70 % viewports / 30 % query batches; "
-                           "median of 3 runs",
+        srv = {"workload": "120 Poisson requests at 1000 req/s, 70 % viewports / 30 % query batches, "
+                           "10 chunk re-uploads per 16 ms tick in both servers; median of 3 runs",
                "batched": {**rep.summary(), "runs_seconds": rep_s}, "plain": {**base.summary(), "runs_seconds": base_s},
                "speedup_vs_plain": round(base.seconds / rep.seconds, 3)}
         # Sessions: frames of 16 clients whose TAA / godray / shadow histories
@@ -255,16 +256,16 @@ def run_batch_serve(dev):
         for rate in (1000.0, 200.0):
             def sess_served():
                 ss = make_sessions(w, 16, seed=3)
-                return serve(r, w, make_arrivals(w, rate, 160, seed=7, sessions=ss), torch, mem_budget=None,
+                return serve(r, w, make_arrivals(w, rate, 240, seed=7, sessions=ss), torch, mem_budget=None,
                              lanes=2, max_batch=16, sessions=ss)
 
             def sess_plain():
                 ss = make_sessions(w, 16, seed=3)
-                return serve_plain(r, w, make_arrivals(w, rate, 160, seed=7, sessions=ss), torch, sessions=ss)
+                return serve_plain(r, w, make_arrivals(w, rate, 240, seed=7, sessions=ss), torch, sessions=ss)
 
             def sess_single_launch():
                 ss = make_sessions(w, 16, seed=3)
-                return serve_plain(r, w, make_arrivals(w, rate, 160, seed=7, sessions=ss), torch, sessions=ss,
+                return serve_plain(r, w, make_arrivals(w, rate, 240, seed=7, sessions=ss), torch, sessions=ss,
                                    single_launch_pass=True)
 
             rep, _ = median_run(sess_served)
@@ -274,11 +275,12 @@ def run_batch_serve(dev):
                                           "plain_single_launch_pass": single.summary(),
                                           "speedup_vs_plain": round(base.seconds / rep.seconds, 3),
                                           "speedup_vs_plain_single_launch_pass": round(single.seconds / rep.seconds, 3)}
-        srv["sessions"] = {"workload": "160 Poisson requests, 70 % frames of 16 sessions (256^2-1920x1080 "
+        srv["sessions"] = {"workload": "240 Poisson requests, 70 % frames of 16 sessions (256^2-1920x1080 "
                                        "present at render scale 0.5, histories resident) / 30 % query batches; "
                                        "median of 3 runs; plain = one request at a time in the wavefront "
                                        "schedule, plain_single_launch_pass = one request at a time, one kernel "
-                                       "per pass (one run)",
+                                       "per pass (one run); every server re-uploads 10 resident chunks per 16 ms "
+                                       "tick",
                            **sess}
         return batch, srv
     finally:
@@ -329,8 +331,8 @@ def run_serve_config4(dev, count: int = 120):
             out[f"{int(rate)}_per_s"] = {"batched": rep.summary(), "plain": base.summary(),
                                          "speedup_vs_plain": round(base.seconds / rep.seconds, 3)}
         out["workload"] = (f"{count} Poisson requests per rate, 70 % viewports / 30 % query batches, 4096-chunk "
-                           "arena (32x4x32), 10 re-uploads per 16 ms tick, admission budget = free device memory "
-                           "- 4 GiB; median of 3 runs")
+                           "arena (32x4x32), 10 re-uploads per 16 ms tick in both servers, admission budget = free "
+                           "device memory - 4 GiB; median of 3 runs")
         out["admission_budget_bytes"] = int(budget)
     finally:
         r.close()
@@ -432,7 +434,7 @@ def frame_series(sc, dev, steps: int, warmup: int, present=None):
         ms = []
         for f in range(warmup + steps):
             _, _, clip, cam = drv.step()
-            r.write_clipmap_updates(*clip)
+            r.write_clipmap_updates(*(clip if clip is not None else (drv.empty_clip(), [])))  # config 1: none
             r.write_camera(cam)
             if f >= warmup:
                 flush.zero_()

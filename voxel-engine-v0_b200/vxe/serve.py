@@ -365,16 +365,24 @@ def serve(renderer, world: World, requests, torch, mem_budget: int | None, lanes
 
 
 def serve_plain(renderer, world: World, requests, torch, keep_outputs: bool = False, sessions=None,
-                single_launch_pass: bool = False) -> ServeReport:
+                single_launch_pass: bool = False, reuploads_per_tick: int = 10,
+                tick_s: float = 0.016) -> ServeReport:
     """Baseline: FIFO, one request at a time (frames alone on lane 0, batches as
-    plain launches).  `single_launch_pass`: frames in the one-kernel-per-pass
+    plain launches), with the same chunk re-upload ticks as `serve` between
+    requests.  `single_launch_pass`: frames in the one-kernel-per-pass
     schedule (VXE_FLAG_PRIMARY_MEGAKERNEL: the reference's pass structure)
     instead of the wavefront."""
     reqs = sorted(requests, key=lambda r: r.arrival)
     views = _Views(renderer, sessions or [])
     flags0 = renderer.flags
+    flags = flags0 | A.FLAG_UPLOADS_UNORDERED
     if single_launch_pass:
-        renderer.set_flags(flags0 | A.FLAG_PRIMARY_MEGAKERNEL)
+        flags |= A.FLAG_PRIMARY_MEGAKERNEL
+    renderer.set_flags(flags)
+    rng = np.random.default_rng(99)
+    resident = [k for k in world.slot_to_key if not world.chunk(k).macro_empty]
+    uploads = 0
+    next_tick = 0.0
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     try:
@@ -382,6 +390,10 @@ def serve_plain(renderer, world: World, requests, torch, keep_outputs: bool = Fa
             now = time.perf_counter() - t0
             if r.arrival > now:
                 time.sleep(r.arrival - now)
+                now = time.perf_counter() - t0
+            while reuploads_per_tick and now >= next_tick:
+                uploads += _reupload(renderer, world, resident, rng, reuploads_per_tick)
+                next_tick += tick_s
             if r.kind == "f":
                 v = views.get(r.session)
                 v.render_async(0, _frame_camera(world, sessions, r))
@@ -401,4 +413,4 @@ def serve_plain(renderer, world: World, requests, torch, keep_outputs: bool = Fa
         views.close()
         renderer.set_flags(flags0)
     lat = [(r.done - r.arrival) * 1e3 for r in reqs]
-    return ServeReport(lat, sum(r.rays for r in reqs), seconds, len(reqs), 1, 0)
+    return ServeReport(lat, sum(r.rays for r in reqs), seconds, len(reqs), 1, uploads)
