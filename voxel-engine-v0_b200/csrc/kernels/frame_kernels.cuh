@@ -94,6 +94,9 @@ struct FrameArgs {
   // profile_counts (ray_main.wgsl:32-74): VOXEL, GRASS, HDR, FOG, SHADOW,
   // added to when cam.profile_flags & 1 (null: not counted)
   uint32_t* profile;
+  // Godray integrals of the walk's far pixels, made beside the probe passes
+  // (k_godray_far; w = 1 where made, cleared each frame); null: none.
+  float4* god_pre;
 };
 
 // profile_inc / profile_add (ray_main.wgsl:64-74).  The flag is uniform over
@@ -1233,6 +1236,36 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_shade_far_views(const __grid_
 // ---------------------------------------------------------------------------
 constexpr int POST_THREADS_X = 32, POST_THREADS_Y = 4;
 
+// The godray ray of pixel (gx, gy) with depth t_c (main_godray,
+// ray_main.wgsl:520-535): the jittered direction and march length.
+struct GodrayPixel {
+  v3 ro, rd;
+  float t_end, j4, j_phase;
+  bool fog_ok;
+};
+__device__ __forceinline__ GodrayPixel godray_pixel(const Scene& s, uint32_t gx, uint32_t gy, float t_c) {
+  GodrayPixel g;
+  g.ro = cam_pos(s);
+  const v2 qpx = V2((float)gx, (float)gy);
+  const float fi = (float)(s.cam->frame_index & 1023u);
+  const v2 fj = V2(fi, fi * 1.371f);
+  g.j4 = 0.20f * (hash12(qpx * J0_SCALE + fj) - 0.5f);
+  g.j_phase = hash12(qpx * 0.91f + fj * 0.73f + V2(31.7f, 12.3f)) - 0.5f;
+  const float qstep = 0.03f;
+  const float dq = (hash12(qpx * 1.37f + fj * 1.19f + V2(9.2f, 1.1f)) - 0.5f) * qstep;
+  const v2 j_rd = V2(hash12(qpx + fj + V2(1.7f, 9.2f)) - 0.5f, hash12(qpx + fj * 1.13f + V2(8.3f, 2.1f)) - 0.5f);
+  g.t_end = fmin_(floorf((t_c + dq) / qstep) * qstep, GODRAY_MAX_DIST);
+  g.fog_ok = fog_density_godray(s) > 0.0f;
+  const v2 pxc = V2((float)gx + 0.5f, (float)gy + 0.5f) + j_rd * 0.35f;
+  g.rd = ray_dir_from_pixel(s, pxc);
+  return g;
+}
+// Its in-scatter.
+__device__ __forceinline__ v3 godray_pixel_integral(const Scene& s, const GodrayPixel& g) {
+  if (g.fog_ok && g.t_end > 0.0f) return godray_integrate_1(s, g.ro, g.rd, g.t_end, g.j4, g.j_phase);
+  return V3s(0.0f);
+}
+
 __device__ __forceinline__ void k_godray_body(const FrameArgs& A) {
   const uint32_t gx = blockIdx.x * POST_THREADS_X + threadIdx.x;
   const uint32_t gy = blockIdx.y * POST_THREADS_Y + threadIdx.y;
@@ -1242,9 +1275,6 @@ __device__ __forceinline__ void k_godray_body(const FrameArgs& A) {
   const int32_t Wi = (int32_t)W, Hi = (int32_t)H;
   const v3 ro = cam_pos(s);
   const int32_t x = (int32_t)gx, y = (int32_t)gy;
-  const v2 qpx = V2((float)gx, (float)gy);
-  const float fi = (float)(s.cam->frame_index & 1023u);
-  const v2 fj = V2(fi, fi * 1.371f);
   const float* D = A.depth;
   const float t_c = D[(size_t)y * W + x];
   const float t_l = D[(size_t)y * W + clampi(x - 1, 0, Wi - 1)], t_r = D[(size_t)y * W + clampi(x + 1, 0, Wi - 1)];
@@ -1254,18 +1284,11 @@ __device__ __forceinline__ void k_godray_body(const FrameArgs& A) {
   const float span = (dmax - dmin) / fmax_(dmin, 1e-3f);
   const float stable = 1.0f - smooth(0.06f, 0.30f, span);
   const float t_hist = dmin;
-  const float j4 = 0.20f * (hash12(qpx * J0_SCALE + fj) - 0.5f);
-  const float j_phase = hash12(qpx * 0.91f + fj * 0.73f + V2(31.7f, 12.3f)) - 0.5f;
-  const float qstep = 0.03f;
-  const float dq = (hash12(qpx * 1.37f + fj * 1.19f + V2(9.2f, 1.1f)) - 0.5f) * qstep;
-  const v2 j_rd = V2(hash12(qpx + fj + V2(1.7f, 9.2f)) - 0.5f, hash12(qpx + fj * 1.13f + V2(8.3f, 2.1f)) - 0.5f);
-  const float t_end = fmin_(floorf((t_c + dq) / qstep) * qstep, GODRAY_MAX_DIST);
-  const bool fog_ok = fog_density_godray(s) > 0.0f;
-  const v2 pxc = V2((float)gx + 0.5f, (float)gy + 0.5f) + j_rd * 0.35f;
-  const v3 rd = ray_dir_from_pixel(s, pxc);
-  v3 cur = V3s(0.0f);
-  if (fog_ok && t_end > 0.0f) cur = godray_integrate_1(s, ro, rd, t_end, j4, j_phase);
-  const v3 p_ws = ro + rd * t_hist;
+  const GodrayPixel g = godray_pixel(s, gx, gy, t_c);
+  const float4 pre = A.god_pre ? A.god_pre[(size_t)gy * W + gx] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  // made beside the probe passes for a far pixel of the walk
+  const v3 cur = pre.w != 0.0f ? V3(pre.x, pre.y, pre.z) : godray_pixel_integral(s, g);
+  const v3 p_ws = ro + g.rd * t_hist;
   const v2 uvp = prev_uv_from_world(s, p_ws);
   v3 hl = cur;
   float hv = 0.0f;
@@ -1294,6 +1317,24 @@ __device__ __forceinline__ void k_godray_body(const FrameArgs& A) {
   const v3 ol = vmix(cur, hc, hw);
   const v3 oc = godray_compress(vmax(ol, V3s(0.0f)));
   A.god_out[(size_t)gy * W + gx] = make_float4(oc.x, oc.y, oc.z, t_hist);
+}
+
+// The godray integrals of the walk's far pixels (queue entries [0,
+// q_count[8]) of q_far), whose depths k_shade_far<0> has made final: run on
+// the side stream beside the probe passes, read by k_godray.
+__device__ __forceinline__ void k_godray_far_body(const FrameArgs& A) {
+  if (A.god_pre == nullptr) return;
+  const Scene s = make_scene(A, true);
+  const uint32_t n = A.q_count[8];
+  for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < n; i += gridDim.x * SHADE_THREADS) {
+    const uint32_t pix = A.q_far[i];
+    const v3 cur = godray_pixel_integral(s, godray_pixel(s, pix % A.iw, pix / A.iw, A.depth[pix]));
+    A.god_pre[pix] = make_float4(cur.x, cur.y, cur.z, 1.0f);
+  }
+}
+__global__ void __launch_bounds__(SHADE_THREADS) k_godray_far(const __grid_constant__ FrameArgs A) { k_godray_far_body(A); }
+__global__ void __launch_bounds__(SHADE_THREADS) k_godray_far_views(const __grid_constant__ FrameArgsViews V) {
+  k_godray_far_body(V.v[blockIdx.z]);
 }
 __global__ void __launch_bounds__(POST_THREADS_X* POST_THREADS_Y) k_godray(const __grid_constant__ FrameArgs A) { k_godray_body(A); }
 __global__ void __launch_bounds__(POST_THREADS_X* POST_THREADS_Y) k_godray_views(const __grid_constant__ FrameArgsViews V) {

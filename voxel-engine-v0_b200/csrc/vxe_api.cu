@@ -47,7 +47,7 @@ enum Img {
   IMG_GOD0, IMG_GOD1, IMG_PRE_TAA, IMG_OUTPUT, IMG_OHIST0, IMG_OHIST1, IMG_HITS, IMG_TILE_COUNT, IMG_TILE_SLOTS,
   IMG_PIXHIT, IMG_QVOX, IMG_QFAR, IMG_QCOUNT, IMG_QSHADOW, IMG_QLIGHT, IMG_PXSHADOW, IMG_PXLIGHT,
   IMG_PROBE_RECS, IMG_SLAB_TASKS, IMG_SLAB_RES, IMG_SLAB_HITS, IMG_PXFIRST, IMG_PXPROBE, IMG_PXMASK, IMG_PXTASK,
-  IMG_QPENDING,
+  IMG_QPENDING, IMG_GODPRE,
   IMG_N
 };
 
@@ -306,7 +306,7 @@ size_t img_bytes(const FrameState& F, int i) {
       return in * 4;
     case IMG_PXFIRST: case IMG_PXPROBE: case IMG_PXMASK:
       return in * 8;
-    case IMG_PXLIGHT:
+    case IMG_PXLIGHT: case IMG_GODPRE:
       return in * 16;
     case IMG_QCOUNT:
       return 64;
@@ -585,6 +585,7 @@ void frame_fill(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& cam, FrameArgs&
   A.px_task = (uint32_t*)S->img[IMG_PXTASK].p;
   A.px_mask = (uint2*)S->img[IMG_PXMASK].p;
   A.q_pending = (uint32_t*)S->img[IMG_QPENDING].p;
+  A.god_pre = (c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL) ? nullptr : (float4*)S->img[IMG_GODPRE].p;
 }
 
 // The frame's launches on the compute stream (captured as-is by the graph
@@ -630,6 +631,7 @@ vxe_status frame_enqueue(vxe_ctx* c, FrameState& F, const FrameArgs& A, bool tim
     if (side && (sr = side_ready(c, *side)) != VXE_OK) return sr;
     CK(cudaMemsetAsync(A.px_first, 0xFF, (size_t)npix * 8u, st));
     CK(cudaMemsetAsync(A.px_mask, 0, (size_t)npix * 8u, st));
+    if (A.god_pre) CK(cudaMemsetAsync(A.god_pre, 0, (size_t)npix * 16u, st));
     if (timed) CK(cudaEventRecord(F.ev[7], st));
     k_primary_trace<<<dim3((tiles_x + 1) / 2, tiles_y), PRIMARY_THREADS, 0, st>>>(A);
     if (timed) CK(cudaEventRecord(F.ev[8], st));
@@ -638,6 +640,8 @@ vxe_status frame_enqueue(vxe_ctx* c, FrameState& F, const FrameArgs& A, bool tim
       CK(cudaEventRecord(side->fork, st));
       CK(cudaStreamWaitEvent(side->s, side->fork, 0));
       k_shade_far<0><<<grid(npix), SHADE_THREADS, 0, side->s>>>(A);
+      // their godray integrals too, while the compute stream runs the probes
+      k_godray_far<<<grid(npix), SHADE_THREADS, 0, side->s>>>(A);
     }
     k_probe_dda<<<grid((uint64_t)npix * kProbesPerPixel), SHADE_THREADS, 0, st>>>(A);
     k_slab_eval<<<grid((uint64_t)npix * kSlabsPerPixel), SHADE_THREADS, 0, st>>>(A);
@@ -703,6 +707,7 @@ vxe_status views_enqueue(vxe_ctx* c, const vxe::dev::FrameArgsViews& V, uint32_t
     CK(cudaMemsetAsync(A.q_count, 0, 64, st));
     CK(cudaMemsetAsync(A.px_first, 0xFF, npix * 8u, st));
     CK(cudaMemsetAsync(A.px_mask, 0, npix * 8u, st));
+    if (A.god_pre) CK(cudaMemsetAsync(A.god_pre, 0, npix * 16u, st));
   }
   vxe_status sr = side_ready(c, *side);
   if (sr != VXE_OK) return sr;
@@ -713,6 +718,7 @@ vxe_status views_enqueue(vxe_ctx* c, const vxe::dev::FrameArgsViews& V, uint32_t
   CK(cudaEventRecord(side->fork, st));
   CK(cudaStreamWaitEvent(side->s, side->fork, 0));
   k_shade_far_views<0><<<grid(max_pix), SHADE_THREADS, 0, side->s>>>(V);
+  k_godray_far_views<<<grid(max_pix), SHADE_THREADS, 0, side->s>>>(V);
   k_probe_dda_views<<<grid(max_pix * kProbesPerPixel), SHADE_THREADS, 0, st>>>(V);
   k_slab_eval_views<<<grid(max_pix * kSlabsPerPixel), SHADE_THREADS, 0, st>>>(V);
   k_slab_pick_views<<<grid(max_pix), SHADE_THREADS, 0, st>>>(V);
