@@ -45,7 +45,7 @@ WORKLOAD = ("config2 plain pipeline: 16x4x16 chunks (caves > 0.6), 5-level 256^2
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=24)
+    ap.add_argument("--steps", type=int, default=64)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="vxe", choices=["vxe", "reference"])
     ap.add_argument("--present", default="1920x1080")
@@ -60,28 +60,68 @@ def parse():
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks / throttle reasons while the timed region runs."""
+    """Samples the SM clock and the clock-event (throttle) reasons while the
+    timed region runs: NVML every 10 ms (read-only queries), nvidia-smi
+    every 200 ms where NVML is unavailable."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, index: int):
         self.index = index
-        self.samples = []
+        self.samples = []  # (sm MHz, max sm MHz, set of active reason names)
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+
+    def _nvml_handle(self):
+        try:
+            import pynvml
+            import torch
+
+            # this CUDA device's NVML handle by its PCI address, as the bytes
+            # "dddddddd:bb:dd.0" (the binding passes an integer through as a
+            # pointer, so only a bytes string goes in)
+            pr = torch.cuda.get_device_properties(self.index)
+            ids = (getattr(pr, "pci_domain_id", None), getattr(pr, "pci_bus_id", None),
+                   getattr(pr, "pci_device_id", None))
+            if not all(isinstance(v, int) for v in ids):
+                return None
+            bus = f"{ids[0]:08X}:{ids[1]:02X}:{ids[2]:02X}.0".encode()
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            bits = {"hw_slowdown": pynvml.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": pynvml.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": pynvml.nvmlClocksEventReasonSwPowerCap}
+            return pynvml, h, bits
+        except Exception:
+            return None
 
     def _run(self):
+        nv = self._nvml_handle()
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                if out.returncode == 0 and out.stdout.strip():
-                    self.samples.append([s.strip() for s in out.stdout.strip().split(",")])
+                if nv is not None:
+                    pynvml, h, bits = nv
+                    sm = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                    mx = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+                    r = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((sm, mx, {n for n, b in bits.items() if r & b}))
+                else:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5)
+                    if out.returncode == 0 and out.stdout.strip():
+                        f = [v.strip() for v in out.stdout.strip().split(",")]
+                        num = lambda v: float(v) if v.replace(".", "").isdigit() else None  # noqa: E731
+                        self.samples.append((num(f[1]), num(f[2]), {self.REASONS[i] for i in range(4)
+                                                                     if len(f) > 5 + i and f[5 + i].lower() == "active"}))
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(0.01 if nv is not None else 0.2)
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
@@ -95,11 +135,9 @@ class ClockSampler:
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 5 + i and
-                          s[5 + i].lower() == "active"})
+        sm = [s[0] for s in self.samples if s[0] is not None]
+        mx = [s[1] for s in self.samples if s[1] is not None]
+        reasons = sorted(set().union(*(s[2] for s in self.samples)))
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(self.samples)}
 

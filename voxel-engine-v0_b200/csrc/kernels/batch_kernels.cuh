@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(BATCH_THREADS) k_batch_probe_dda(const __grid_
   }
 }
 
-__global__ void __launch_bounds__(BATCH_THREADS) k_batch_slab_eval(const __grid_constant__ BatchArgs B) {
+__global__ void __launch_bounds__(BATCH_THREADS, SLAB_MIN_BLOCKS) k_batch_slab_eval(const __grid_constant__ BatchArgs B) {
   const uint32_t n_reqs = B.hdr->n_reqs;
   const uint32_t n = min(B.dcount[2], B.slab_cap);
   for (uint32_t j = blockIdx.x * BATCH_THREADS + threadIdx.x; j < n; j += gridDim.x * BATCH_THREADS) {
