@@ -490,10 +490,10 @@ __device__ __forceinline__ v3 xyz(float4 v) { return V3(v.x, v.y, v.z); }
 // ---------------------------------------------------------------------------
 constexpr int PRIMARY_THREADS = 128;  // two 8x8 logical tiles per block
 constexpr int SHADE_THREADS = 128;
-// Blocks per SM the heavier shading kernels are compiled for (64 registers a
-// thread instead of 96-128: measured 0.09 ms faster per 1080p frame than
-// without the bound, 0.05 of it from 6 to 8 blocks).
-constexpr int SHADE_MIN_BLOCKS = 8;
+// Blocks per SM the heavier shading kernels are compiled for (48 registers a
+// thread instead of 96-128, a few spills: measured 0.11 ms faster per 1080p
+// frame than without the bound; 6, 8 and 10 blocks gave 0.05, 0.09, 0.11).
+constexpr int SHADE_MIN_BLOCKS = 10;
 // Blocks per SM of the blade-march kernels (64 registers a thread instead of
 // 80: more marches in flight, measured 0.08 ms faster per 1080p frame).
 constexpr int SLAB_MIN_BLOCKS = 8;
