@@ -7,8 +7,8 @@
  * from the mathematics (Cody & Waite argument reduction, "Software Manual for
  * the Elementary Functions", 1980, plus truncated Taylor / atanh series) with a
  * fixed operation order.  Only correctly rounded IEEE operations are used:
- * +, -, *, /, and fused multiply-adds written out explicitly (vxe_fmaf,
- * vxe_fma: one rounding on every machine).  Compiled without FMA contraction
+ * +, -, *, /, and fused multiply-adds written out explicitly (vxe_fmaf:
+ * one rounding on every machine).  Compiled without FMA contraction
  * (host: -ffp-contract=off, device: -fmad=false), both sides therefore produce
  * identical bits.
  *
@@ -16,9 +16,10 @@
  * argument reduction and in the Horner steps: exp within 1 ulp, sin and cos
  * within 1.5 ulp (8e-8 absolute near their zeros), inside WGSL's own bounds
  * for these builtins (exp 3 + 2|x| ulp, sin / cos 2^-11 absolute on [-pi, pi]).
- * sin and cos of |x| > 65536 use a binary64 reduction.  pow needs log x to
- * more bits than binary32 holds, so it is evaluated in binary64 and rounded
- * once: within 1 ulp.  The bounds are checked in tests/test_detmath.py.
+ * sin and cos of |x| > 65536 use a binary64 reduction.  pow carries log x
+ * and y log x as unevaluated binary32 pairs: within 1.25 ulp for exponents up
+ * to 8, 3.5 ulp at 96 (the error grows with |y log x|).  The bounds are
+ * checked in tests/test_detmath.py.
  */
 #ifndef VXE_DETMATH_H
 #define VXE_DETMATH_H
@@ -42,11 +43,6 @@
 #define VXE_PIO2_2 6.077100506303966e-11
 #define VXE_PIO2_3 2.0222662487959506e-21
 #define VXE_TWO_OVER_PI 0.6366197723675814
-/* ln 2 split, first piece with 32 significant bits. */
-#define VXE_LN2_1 0.6931471803691238
-#define VXE_LN2_2 1.9082149292705877e-10
-#define VXE_LOG2E 1.4426950408889634
-#define VXE_LN2 0.6931471805599453
 
 VXE_HD uint64_t vxe_d2u(double d) {
 #if defined(__CUDA_ARCH__)
@@ -96,14 +92,6 @@ VXE_HD float vxe_fmaf(float a, float b, float c) {
 #endif
 }
 
-VXE_HD double vxe_fma(double a, double b, double c) {
-#if defined(__CUDA_ARCH__)
-  return __fma_rn(a, b, c);
-#else
-  return __builtin_fma(a, b, c);
-#endif
-}
-
 VXE_HD float vxe_rintf(float x) {
 #if defined(__CUDA_ARCH__)
   return rintf(x);
@@ -114,33 +102,6 @@ VXE_HD float vxe_rintf(float x) {
 
 /* 2^k for integer k in [-126, 127]. */
 VXE_HD float vxe_pow2if(int k) { return vxe_u2f((uint32_t)(k + 127) << 23); }
-
-/* 2^k for integer k in [-1022, 1023] built from its bit pattern. */
-VXE_HD double vxe_pow2i(int k) { return vxe_u2d((uint64_t)(int64_t)(k + 1023) << 52); }
-
-/* e^x in binary64 to 2^-32 relative, for results rounded to binary32
- * (|x| <= 745 handled; beyond returns inf / 0). */
-VXE_HD double vxe_exp_d(double x) {
-  if (x != x) return x;
-  if (x > 709.0) return vxe_u2d(0x7FF0000000000000ull);
-  if (x < -745.0) return 0.0;
-  const double kd = vxe_floor_d(x * VXE_LOG2E + 0.5);
-  const int k = (int)kd;
-  const double r = vxe_fma(-kd, VXE_LN2_2, vxe_fma(-kd, VXE_LN2_1, x)); /* |r| <= 0.3466 */
-  /* Taylor series of e^r to degree 8 (truncation below 2^-32: enough for a
-   * result rounded to binary32), Horner form. */
-  double p = 1.0 / 40320.0;
-  p = vxe_fma(p, r, 1.0 / 5040.0);
-  p = vxe_fma(p, r, 1.0 / 720.0);
-  p = vxe_fma(p, r, 1.0 / 120.0);
-  p = vxe_fma(p, r, 1.0 / 24.0);
-  p = vxe_fma(p, r, 1.0 / 6.0);
-  p = vxe_fma(p, r, 0.5);
-  p = vxe_fma(p, r, 1.0);
-  p = vxe_fma(p, r, 1.0);
-  if (k < -1000) return (p * vxe_pow2i(k + 200)) * vxe_pow2i(-200);
-  return p * vxe_pow2i(k);
-}
 
 VXE_HD uint32_t vxe_f2u(float f) {
 #if defined(__CUDA_ARCH__)
@@ -159,42 +120,6 @@ VXE_HD float vxe_rcpf(float x) {
 #else
   return 1.0f / x;
 #endif
-}
-
-/* Natural log of a finite binary32 x > 0, in binary64 to about 2^-40
- * absolute (for pow).  x = 2^e m with m in [sqrt(1/2), sqrt(2)); log m =
- * 2 atanh(s), s = (m-1)/(m+1), |s| <= 0.1716, the division as a binary32
- * reciprocal and one Newton step. */
-VXE_HD double vxe_log_f(float x) {
-  uint32_t u = vxe_f2u(x);
-  int e = (int)((u >> 23) & 0xFFu);
-  if (e == 0) { /* subnormal: normalise (exact) */
-    u = vxe_f2u(x * 16777216.0f);
-    e = (int)((u >> 23) & 0xFFu) - 24;
-  }
-  e -= 127;
-  double m = (double)vxe_u2f((u & 0x007FFFFFu) | 0x3F800000u); /* [1,2) */
-  if (m > 1.4142135623730951) {
-    m = m * 0.5;
-    e += 1;
-  }
-  const double d = m + 1.0; /* exact: m has 24 significant bits */
-  double r = (double)vxe_rcpf((float)d);
-  r = vxe_fma(r, vxe_fma(-d, r, 1.0), r);
-  const double s = (m - 1.0) * r;
-  const double s2 = s * s;
-  /* 2 atanh(s) = 2 s (1 + s^2/3 + ...), terms to s^15 (below 2^-41) */
-  double q = 1.0 / 15.0;
-  q = vxe_fma(q, s2, 1.0 / 13.0);
-  q = vxe_fma(q, s2, 1.0 / 11.0);
-  q = vxe_fma(q, s2, 1.0 / 9.0);
-  q = vxe_fma(q, s2, 1.0 / 7.0);
-  q = vxe_fma(q, s2, 1.0 / 5.0);
-  q = vxe_fma(q, s2, 1.0 / 3.0);
-  q = vxe_fma(q, s2, 1.0);
-  const double lm = 2.0 * s * q;
-  const double ed = (double)e;
-  return vxe_fma(ed, VXE_LN2_2, vxe_fma(ed, VXE_LN2_1, lm));
 }
 
 /* sin / cos of r for |r| <= pi/4 (Taylor to degree 15 / 16). */
@@ -330,15 +255,74 @@ VXE_HD_CALL float vxe_expf(float x) {
 }
 
 /* pow for the non-negative bases the passes use: pow(0, y>0) = 0,
- * pow(x, 0) = 1, negative bases give NaN (WGSL leaves them undefined). */
+ * pow(x, 0) = 1, negative bases give NaN (WGSL leaves them undefined).
+ * Binary32 throughout: log x as an unevaluated sum hi + lo (x = 2^e m, m in
+ * [sqrt(1/2), sqrt(2)), log m = 2 atanh(s) with s = (m-1)/(m+1) split hi + lo
+ * by a fused residual, the larger parts summed by two-sums), y log x as
+ * hi + lo (fused products), then e^t as in vxe_expf with the low part added
+ * to the reduced argument. */
 VXE_HD_CALL float vxe_powf(float x, float y) {
   if (y == 0.0f) return 1.0f;
   if (x == 0.0f) return y > 0.0f ? 0.0f : vxe_u2f(0x7F800000u);
   if (x == 1.0f) return 1.0f;
-  if (!(x > 0.0f)) return vxe_u2f(0x7FC00000u);                      /* negative or NaN base */
-  if (x == vxe_u2f(0x7F800000u)) return y > 0.0f ? x : 0.0f;         /* +inf base */
+  if (!(x > 0.0f)) return vxe_u2f(0x7FC00000u);
+  if (x == vxe_u2f(0x7F800000u)) return y > 0.0f ? x : 0.0f;
   if (y != y) return y;
-  return (float)vxe_exp_d((double)y * vxe_log_f(x));
+  uint32_t u = vxe_f2u(x);
+  int e = (int)((u >> 23) & 0xFFu);
+  if (e == 0) {
+    u = vxe_f2u(x * 16777216.0f);
+    e = (int)((u >> 23) & 0xFFu) - 24;
+  }
+  e -= 127;
+  float m = vxe_u2f((u & 0x007FFFFFu) | 0x3F800000u);
+  if (m > 1.41421356f) {
+    m = m * 0.5f;
+    e += 1;
+  }
+  const float num = m - 1.0f;                     /* exact */
+  const float den = m + 1.0f;                     /* den + dlo = m + 1 exactly (two-sum) */
+  const float bb = den - m;
+  const float dlo = (m - (den - bb)) + (1.0f - bb);
+  const float rd = vxe_rcpf(den);
+  const float s_hi = num * rd;
+  const float res = vxe_fmaf(-s_hi, dlo, vxe_fmaf(-s_hi, den, num));
+  const float s_lo = res * rd;
+  const float s2 = s_hi * s_hi;
+  float q = 2.0f / 13.0f;
+  q = vxe_fmaf(q, s2, 2.0f / 11.0f);
+  q = vxe_fmaf(q, s2, 2.0f / 9.0f);
+  q = vxe_fmaf(q, s2, 2.0f / 7.0f);
+  q = vxe_fmaf(q, s2, 2.0f / 5.0f);
+  q = vxe_fmaf(q, s2, 2.0f / 3.0f);
+  const float tail = (s2 * s_hi) * q;             /* log m - 2 s */
+  const float ef = (float)e;
+  const float a = ef * 0.693145751953125f;        /* exact: 16-bit constant, |e| < 2^8 */
+  const float b = 2.0f * s_hi;
+  const float l_hi = a + b;                        /* two-sum of a + b */
+  const float bv = l_hi - a;
+  const float l_err = (a - (l_hi - bv)) + (b - bv);
+  const float l_lo = l_err + (2.0f * s_lo + tail) + ef * 1.428606765330187e-06f;
+  const float t_hi = y * l_hi;
+  const float t_lo = vxe_fmaf(y, l_lo, vxe_fmaf(y, l_hi, -t_hi));
+  if (t_hi > 88.72283935546875f) return vxe_u2f(0x7F800000u);
+  if (t_hi < -103.97208404541015625f) return 0.0f;
+  const float kf = vxe_rintf(t_hi * 1.4426950216293335f);
+  float r = vxe_fmaf(-kf, 0.693145751953125f, t_hi);  /* exact */
+  r = vxe_fmaf(-kf, 1.428606765330187e-06f, r) + t_lo;
+  float p = 1.0f / 40320.0f;
+  p = vxe_fmaf(p, r, 1.0f / 5040.0f);
+  p = vxe_fmaf(p, r, 1.0f / 720.0f);
+  p = vxe_fmaf(p, r, 1.0f / 120.0f);
+  p = vxe_fmaf(p, r, 1.0f / 24.0f);
+  p = vxe_fmaf(p, r, 1.0f / 6.0f);
+  p = vxe_fmaf(p, r, 0.5f);
+  p = vxe_fmaf(p, r, 1.0f);
+  const float ex = vxe_fmaf(r, p, 1.0f);
+  const int k = (int)kf;
+  if (k > 127) return (ex * 2.0f) * vxe_pow2if(k - 1);
+  if (k < -125) return (ex * vxe_pow2if(k + 64)) * vxe_pow2if(-64);
+  return ex * vxe_pow2if(k);
 }
 
 #endif /* VXE_DETMATH_H */
