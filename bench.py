@@ -45,7 +45,7 @@ WORKLOAD = ("config2 plain pipeline: 16x4x16 chunks (caves > 0.6), 5-level 256^2
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--steps", type=int, default=48)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--impl", default="vxe", choices=["vxe", "reference"])
     ap.add_argument("--present", default="1920x1080")
