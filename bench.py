@@ -21,6 +21,8 @@ internal over a streamed world of 16x4x16 chunks with 3D caves, a 5-level
 from __future__ import annotations
 
 import argparse
+import contextlib
+import gc
 import json
 import os
 import statistics
@@ -57,6 +59,19 @@ def parse():
     ap.add_argument("--build-profile", type=int, default=0,
                     help="build the first N config-2 chunks (a counting build, then the full build) only, for ncu")
     return ap.parse_args()
+
+
+@contextlib.contextmanager
+def no_gc():
+    """Timed regions run without the cyclic garbage collector: a collection
+    over the host's world objects would pause the host loop that feeds the
+    GPU.  Collected before, re-enabled after."""
+    gc.collect()
+    gc.disable()
+    try:
+        yield
+    finally:
+        gc.enable()
 
 
 class ClockSampler:
@@ -187,7 +202,7 @@ def run_vxe(args, rank: int, world_size: int):
         torch.distributed.barrier()
     torch.cuda.synchronize()
     step_ms, prim_ms, god_ms, comp_ms, tile_ms, trace_ms, grass_ms, walk_ms = [], [], [], [], [], [], [], []
-    with ClockSampler(dev) as clocks:
+    with ClockSampler(dev) as clocks, no_gc():
         for s in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
@@ -207,6 +222,7 @@ def run_vxe(args, rank: int, world_size: int):
     total_ms = float(sum(step_ms))
     err = r.read_error_word()
     r.close()
+    del r, drv, world, ups, flush  # the device-resident workload's host objects
     # ---- end to end through the C ABI with host buffers (streaming world)
     if args.no_e2e:
         e2e = {"seconds": float("nan"), "rays": 0, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
@@ -283,7 +299,8 @@ def run_batch_serve(dev):
         # The served run depends on host timing (which arrivals share a batch):
         # three runs each, the median one by completion time is reported.
         def median_run(fn):
-            runs = sorted((fn() for _ in range(SERVE_RUNS)), key=lambda x: x.seconds)
+            with no_gc():
+                runs = sorted((fn() for _ in range(SERVE_RUNS)), key=lambda x: x.seconds)
             return runs[SERVE_RUNS // 2], [round(x.seconds, 4) for x in runs]
 
         rep, rep_s = median_run(lambda: serve(r, w, make_arrivals(w, 1000.0, 120, seed=7), torch,
@@ -364,7 +381,8 @@ def run_serve_config4(dev, count: int = 120):
         serve(r, w, make_arrivals(w, 2000.0, 20, seed=1), torch, mem_budget=budget, lanes=2)  # warm-up
 
         def median_run(fn):
-            runs = sorted((fn() for _ in range(SERVE_RUNS)), key=lambda x: x.seconds)
+            with no_gc():
+                runs = sorted((fn() for _ in range(SERVE_RUNS)), key=lambda x: x.seconds)
             return runs[SERVE_RUNS // 2]
 
         for rate in (200.0, 500.0, 1000.0, 2000.0):
@@ -774,18 +792,19 @@ def run_e2e(args, sc, dev, world_size):
         h2d = d2h = 0
         if world_size > 1:
             torch.distributed.barrier()
-        t0 = time.perf_counter()
-        pending = []  # tickets of the outputs not yet waited for, oldest first
-        for i in range(args.steps):
-            t = one(i, pipelined)
-            if t is not None:
-                pending.append(t)
-            if len(pending) > PIPELINE_DEPTH:
-                r.read_image_wait(pending.pop(0))  # step i - depth's output is in host memory
-        for t in pending:
-            r.read_image_wait(t)
-        r.synchronize()
-        dt = time.perf_counter() - t0
+        with no_gc():
+            t0 = time.perf_counter()
+            pending = []  # tickets of the outputs not yet waited for, oldest first
+            for i in range(args.steps):
+                t = one(i, pipelined)
+                if t is not None:
+                    pending.append(t)
+                if len(pending) > PIPELINE_DEPTH:
+                    r.read_image_wait(pending.pop(0))  # step i - depth's output is in host memory
+            for t in pending:
+                r.read_image_wait(t)
+            r.synchronize()
+            dt = time.perf_counter() - t0
         if world_size > 1:
             torch.distributed.barrier()
         return dt
