@@ -872,7 +872,17 @@ __device__ __forceinline__ HitGeom miss_hitgeom() {  // chunk_trace.wgsl:40-51
   return h;
 }
 
-struct ChunkTraceResult { HitGeom hit; bool anchor_valid; uint32_t anchor_key; };
+// A chunk walk's result.  `gov`: the hit is a grass voxel whose blade march
+// (grass_on_voxel_hit over [gov_t0, gov_t1]) the walk left to a later pass;
+// that march may replace the hit's t and n.
+struct ChunkTraceResult {
+  HitGeom hit;
+  bool anchor_valid;
+  uint32_t anchor_key;
+  bool gov = false;
+  float gov_t0 = 0.0f, gov_t1 = 0.0f;  // the walk's interval, for the march
+  float gov_lo = 0.0f, gov_hi = 0.0f;  // the march's slab interval: its hit t lies in it
+};
 
 __device__ __forceinline__ bool point_in_cube(v3 p, v3 bmin, float size) {  // chunk_trace.wgsl:54-59
   const v3 bmax = bmin + V3s(size);
@@ -1234,6 +1244,7 @@ struct ProbeHook {
   uint32_t best_cand;  // candidate index of the trace's current best (INVALID: none)
   uint32_t pixel;
   uint32_t recorded;   // probes stored
+  bool defer_gov;      // leave the blade march of a grass-voxel hit to a later pass
   ProbeRec* recs;
   uint32_t* rec_count;
   uint32_t rec_cap;
@@ -1250,6 +1261,7 @@ __device__ __forceinline__ ProbeHook probe_hook_inline() {
   h.best_cand = INVALID;
   h.pixel = 0u;
   h.recorded = 0u;
+  h.defer_gov = false;
   h.recs = nullptr;
   h.rec_count = nullptr;
   h.rec_cap = 0u;
@@ -1279,9 +1291,11 @@ __device__ __forceinline__ void probe_record(ProbeHook& ph, float t0, float t1, 
 
 // The blades on top of a grass voxel the walk hit at (t, n)
 // (chunk_trace.wgsl:917-950): the cell from the hit point, corrected by the
-// column's colinfo top, then its grass slab from just before the hit.
-__device__ __noinline__ GrassHit grass_on_voxel_hit(const Scene& s, v3 ro, v3 rd, const Meta& ch, float t, v3 n,
-                                                    float t_enter, float t_exit) {
+// column's colinfo top, then its grass slab from just before the hit.  This
+// part gives the cell and the slab interval the march would cover
+// (try_grass_slab_hit's first step); empty when y <= x.
+__device__ __forceinline__ v2 grass_on_voxel_interval(const Scene& s, v3 ro, v3 rd, const Meta& ch, float t, v3 n,
+                                                     float t_enter, float t_exit, GrassCell* cell_out) {
   const float vs = vs_(s);
   const v3 rb = V3((float)ch.ox, (float)ch.oy, (float)ch.oz) * vs;
   const i3 ov{ch.ox, ch.oy, ch.oz};
@@ -1300,8 +1314,18 @@ __device__ __noinline__ GrassHit grass_on_voxel_hit(const Scene& s, v3 ro, v3 rd
   const float pad = (GRASS_LAYER_HEIGHT_VOX + 1.0f) * vs;
   const float tmn = fmax_(t_enter, t - 0.01f * vs);
   const float tmx = fmin_(t + pad, t_exit + pad);
-  return try_grass_slab_hit(s, ro, rd, tmn, tmx, cell.bmin_m, cell.id_vox, vs, s.cam->voxel_params[1],
-                            s.cam->voxel_params[2]);
+  *cell_out = cell;
+  return grass_slab_interval(ro, rd, tmn, tmx, cell.bmin_m, vs);
+}
+
+// ... and the march over it (try_grass_slab_hit).
+__device__ __noinline__ GrassHit grass_on_voxel_hit(const Scene& s, v3 ro, v3 rd, const Meta& ch, float t, v3 n,
+                                                    float t_enter, float t_exit) {
+  GrassCell cell;
+  const v2 iv = grass_on_voxel_interval(s, ro, rd, ch, t, n, t_enter, t_exit, &cell);
+  if (iv.y <= iv.x) return GrassHit{false, BIG, V3s(0.0f)};
+  return grass_layer_trace_lod(s, ro, rd, iv.x, iv.y, cell.bmin_m, cell.id_vox, s.cam->voxel_params[1],
+                               s.cam->voxel_params[2], grass_lod_from_t(iv.x));
 }
 
 template <uint32_t PM>
@@ -1441,6 +1465,21 @@ __device__ __forceinline__ ChunkTraceResult trace_chunk_rope_interval_nomacro(co
     const BoxHit bh = cube_hit_normal_from_slab(rd, slab, tmin_iter, t_exit);
     if (bh.hit) {
       const uint32_t nd = ch.node_base + leaf.idx_local;
+      if (!opt.geom_only && leaf.mat == MAT_GRASS && ph.defer_gov) {
+        // the march is left to k_gov_eval; its hit t lies in the slab
+        // interval, and an empty interval is no hit
+        ChunkTraceResult r{make_hit(leaf.mat, bh.t, bh.n, rb, rs, ch, nd, leaf.bmin, leaf.size), an.valid, an.key};
+        GrassCell cell;
+        const v2 iv = grass_on_voxel_interval(s, ro, rd, ch, bh.t, bh.n, t_enter, t_exit, &cell);
+        if (iv.y > iv.x) {
+          r.gov = true;
+          r.gov_t0 = t_enter;
+          r.gov_t1 = t_exit;
+          r.gov_lo = iv.x;
+          r.gov_hi = iv.y;
+        }
+        return r;
+      }
       if (!opt.geom_only && leaf.mat == MAT_GRASS) {
         const GrassHit gh = grass_on_voxel_hit(s, ro, rd, ch, bh.t, bh.n, t_enter, t_exit);
         if (gh.hit)
@@ -1513,6 +1552,12 @@ struct VoxTraceResult {
   bool anchor_valid;
   uint32_t anchor_key;
   i3 anchor_chunk;
+  // deferred blade march of the answer (ChunkTraceResult::gov): 0 none,
+  // 1 pending (its interval and chunk slot below), 2 another chunk's result
+  // could win once the marches are known (the pixel walks again)
+  uint32_t gov_state = 0u;
+  float gov_t0 = 0.0f, gov_t1 = 0.0f;
+  uint32_t gov_slot = 0u;
 };
 
 // Visits the chunk-grid cells crossed by a ray (chunk_trace.wgsl:1028-1151).

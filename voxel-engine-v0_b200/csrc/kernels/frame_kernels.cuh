@@ -79,6 +79,8 @@ struct FrameArgs {
   uint32_t* px_task;              // per pixel: the slab task with that key
   uint2* px_mask;                 // per pixel: candidate chunks with a probe hit, hint / full trace
   uint2* px_probe;                // per pixel: walk summary (probe_summary) | probes stored
+  uint4* px_gov = nullptr;        // per pending pixel: deferred blade march of its answer (gov_state,
+                                  // interval, chunk slot); 3 / 4 once k_gov_eval ran it (hit / miss)
   uint32_t* q_pending;            // pixels whose walk met probes, q_count[5] of them
   // per-frame grass cell table: written by k_grass_cells, read by the rest
   float4* grass_rec;
@@ -96,7 +98,7 @@ struct FrameArgs {
   uint32_t* profile;
   // Godray integrals of the walk's far pixels, made beside the probe passes
   // (k_godray_far; w = 1 where made, cleared each frame); null: none.
-  float4* god_pre;
+  float4* god_pre = nullptr;
 };
 
 // profile_inc / profile_add (ray_main.wgsl:64-74).  The flag is uniform over
@@ -385,6 +387,17 @@ __device__ VoxTraceResult trace_candidates(const Scene& s, const uint32_t* cslot
   const float rs = (float)s.cam->chunk_size * vsz;
   const uint32_t maxc = min(cand_count, MAX_TILE_CHUNKS);
   const TraceOpts opt{false};
+  // With a deferred blade march (ChunkTraceResult::gov) a chunk's final t is
+  // its voxel hit's or one in the march's slab interval: only bounded.  The
+  // skip test takes the nearest upper bound, so every chunk the reference
+  // walks is walked here; the answer is decided at the end when no other
+  // chunk's lower bound reaches its upper bound (with no deferred march
+  // these are the plain t's and this is the reference's loop).
+  float skip_t = BIG;
+  float lo_gov = BIG, lo_plain = BIG;  // lowest final t of the other chunks, deferred / plain
+  bool a_gov = false;
+  float a_t0 = 0.0f, a_t1 = 0.0f, a_hi = 0.0f, a_lo = 0.0f;
+  uint32_t a_slot = 0u;
   for (uint32_t i = 0; i < maxc; ++i) {
     const uint32_t slot = cslot[i];
     if (slot == INVALID || slot >= s.cam->chunk_count) continue;
@@ -394,7 +407,7 @@ __device__ VoxTraceResult trace_candidates(const Scene& s, const uint32_t* cslot
     const v2 rt = intersect_aabb(ro, rd, rb, rb + V3s(rs));
     const float ce = fmax_(rt.x, t_enter), cx = fmin_(rt.y, t_exit);
     if (cx < ce) continue;
-    if (best.hit != 0u && ce >= best.t) continue;
+    if (ce >= skip_t) continue;
     if (chunk_heightfield_early_skip(s, ro, rd, ce, cx, ch, vsz)) continue;
     const int32_t csz = (int32_t)s.cam->chunk_size;
     const i3 cc{ch.ox / csz, ch.oy / csz, ch.oz / csz};
@@ -403,15 +416,42 @@ __device__ VoxTraceResult trace_candidates(const Scene& s, const uint32_t* cslot
     ph.slot = slot;
     ph.cand = i;
     const ChunkTraceResult h = trace_chunk_interval_stream_macro<PM>(s, ro, rd, inv, ch, ce, cx, ua, aku, opt, ph);
-    if (h.hit.hit != 0u && h.hit.t < best.t) {
+    if (h.hit.hit == 0u) continue;
+    const float lo = h.gov ? fmin_(h.hit.t, h.gov_lo) : h.hit.t;
+    const float hi = h.gov ? fmax_(h.hit.t, h.gov_hi) : h.hit.t;
+    skip_t = fmin_(skip_t, hi);
+    if (h.hit.t < best.t) {
+      if (best.hit != 0u) {  // the previous answer becomes another chunk
+        if (a_gov) lo_gov = fmin_(lo_gov, a_lo);
+        else lo_plain = fmin_(lo_plain, best.t);
+      }
       best = h.hit;
       bav = h.anchor_valid;
       bak = h.anchor_key;
       bac = cc;
       ph.best_cand = i;
+      a_gov = h.gov;
+      a_t0 = h.gov_t0;
+      a_t1 = h.gov_t1;
+      a_lo = lo;
+      a_hi = hi;
+      a_slot = slot;
+    } else if (h.gov) {
+      lo_gov = fmin_(lo_gov, lo);
+    } else {
+      lo_plain = fmin_(lo_plain, h.hit.t);
     }
   }
-  return VoxTraceResult{true, best, t_exit, bav, bak, bac};
+  VoxTraceResult r{true, best, t_exit, bav, bak, bac};
+  if (best.hit != 0u) {
+    const float up = a_gov ? a_hi : best.t;
+    if (lo_gov <= up || (a_gov && lo_plain <= up)) r.gov_state = 2u;
+    else if (a_gov) r.gov_state = 1u;
+    r.gov_t0 = a_t0;
+    r.gov_t1 = a_t1;
+    r.gov_slot = a_slot;
+  }
+  return r;
 }
 
 // ---------------------------------------------------------------------------
@@ -847,8 +887,10 @@ __device__ __forceinline__ void walk_finish(const FrameArgs& A, uint32_t pix, co
                                             const ProbeHook& ph, uint32_t tile_count, bool* vox, bool* pend) {
   *vox = vt.in_grid && vt.best.hit != 0u;
   if (*vox) store_pixhit(A.pix_hit + (size_t)pix * 5u, vt.best, vt);
-  *pend = ph.seq != 0u;
+  const uint32_t gs = *vox ? vt.gov_state : 0u;
+  *pend = ph.seq != 0u || gs != 0u;
   if (*pend) {
+    A.px_gov[pix] = make_uint4(gs, __float_as_uint(vt.gov_t0), __float_as_uint(vt.gov_t1), vt.gov_slot);
     // more probes than the summary counts: every stored one is still used,
     // the pixel just walks again
     const uint32_t stored = ph.seq > 0xFFFFFFu ? 0u : ph.recorded;
@@ -865,6 +907,7 @@ __device__ __forceinline__ ProbeHook probe_hook_record(const FrameArgs& A, uint3
   ph.recs = A.probe_recs;
   ph.rec_count = &A.q_count[4];
   ph.rec_cap = A.probe_cap;
+  ph.defer_gov = A.px_gov != nullptr;
   return ph;
 }
 
@@ -1006,6 +1049,37 @@ __global__ void __launch_bounds__(SHADE_THREADS) k_slab_pick_views(const __grid_
   k_slab_pick_body(V.v[blockIdx.z]);
 }
 
+// The blade marches the walk deferred (grass_on_voxel_hit of a grass-voxel
+// answer, px_gov state 1), one lane per pending pixel: a hit replaces the
+// answer's t and n in its PixHit record (state 3), a miss keeps the voxel
+// hit (state 4).
+__device__ __forceinline__ void k_gov_eval_body(const FrameArgs& A) {
+  if (A.px_gov == nullptr) return;
+  const Scene s = make_scene(A, false);
+  const uint32_t n = A.q_count[5];
+  for (uint32_t i = blockIdx.x * SHADE_THREADS + threadIdx.x; i < n; i += gridDim.x * SHADE_THREADS) {
+    const uint32_t pix = A.q_pending[i];
+    const uint4 gv = A.px_gov[pix];
+    if (gv.x != 1u) continue;
+    uint4* rec = A.pix_hit + (size_t)pix * 5u;
+    const uint4 h0 = rec[0];
+    const PrimaryCtx c = primary_ctx(s, pix % A.iw, pix / A.iw, A.iw);
+    const GrassHit gh = grass_on_voxel_hit(s, c.ro, c.rd, meta_at(s, gv.w), __uint_as_float(h0.x),
+                                           V3(__uint_as_float(h0.y), __uint_as_float(h0.z), __uint_as_float(h0.w)),
+                                           __uint_as_float(gv.y), __uint_as_float(gv.z));
+    if (gh.hit)
+      rec[0] = make_uint4(__float_as_uint(gh.t), __float_as_uint(gh.n.x), __float_as_uint(gh.n.y),
+                          __float_as_uint(gh.n.z));
+    A.px_gov[pix].x = gh.hit ? 3u : 4u;
+  }
+}
+__global__ void __launch_bounds__(SHADE_THREADS, SLAB_MIN_BLOCKS) k_gov_eval(const __grid_constant__ FrameArgs A) {
+  k_gov_eval_body(A);
+}
+__global__ void __launch_bounds__(SHADE_THREADS, SLAB_MIN_BLOCKS) k_gov_eval_views(const __grid_constant__ FrameArgsViews V) {
+  k_gov_eval_body(V.v[blockIdx.z]);
+}
+
 // Pixels that met probes: the nearer of the nearest probe hit and the voxel
 // answer (see the comment above ProbeRec), or, when that cannot be decided
 // from the parts, the reference walk with inline probes.
@@ -1025,7 +1099,9 @@ __device__ __forceinline__ void k_primary_resolve_body(const FrameArgs& A) {
       uint32_t answer_phase = vphase;  // phase of the answer (1 when there is none)
       vox = (pp.x >> 31) != 0u;
       const unsigned long long first = A.px_first[pix];
-      bool walk = pp.y < met;  // some probes were not evaluated
+      // some probes were not evaluated, or a deferred blade march left the
+      // answer open
+      bool walk = pp.y < met || (A.px_gov != nullptr && A.px_gov[pix].x == 2u);
       if (!walk && first != ~0ull) {
         const uint32_t j = A.px_task[pix];
         const float4 res = A.slab_res[j];

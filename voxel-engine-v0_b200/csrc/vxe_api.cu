@@ -47,7 +47,7 @@ enum Img {
   IMG_GOD0, IMG_GOD1, IMG_PRE_TAA, IMG_OUTPUT, IMG_OHIST0, IMG_OHIST1, IMG_HITS, IMG_TILE_COUNT, IMG_TILE_SLOTS,
   IMG_PIXHIT, IMG_QVOX, IMG_QFAR, IMG_QCOUNT, IMG_QSHADOW, IMG_QLIGHT, IMG_PXSHADOW, IMG_PXLIGHT,
   IMG_PROBE_RECS, IMG_SLAB_TASKS, IMG_SLAB_RES, IMG_SLAB_HITS, IMG_PXFIRST, IMG_PXPROBE, IMG_PXMASK, IMG_PXTASK,
-  IMG_QPENDING, IMG_GODPRE,
+  IMG_QPENDING, IMG_GODPRE, IMG_PXGOV,
   IMG_N
 };
 
@@ -306,7 +306,7 @@ size_t img_bytes(const FrameState& F, int i) {
       return in * 4;
     case IMG_PXFIRST: case IMG_PXPROBE: case IMG_PXMASK:
       return in * 8;
-    case IMG_PXLIGHT: case IMG_GODPRE:
+    case IMG_PXLIGHT: case IMG_GODPRE: case IMG_PXGOV:
       return in * 16;
     case IMG_QCOUNT:
       return 64;
@@ -584,6 +584,8 @@ void frame_fill(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& cam, FrameArgs&
   A.slab_hits = (uint32_t*)S->img[IMG_SLAB_HITS].p;
   A.px_task = (uint32_t*)S->img[IMG_PXTASK].p;
   A.px_mask = (uint2*)S->img[IMG_PXMASK].p;
+  // the wavefront walk leaves grass-voxel blade marches to k_gov_eval
+  A.px_gov = (c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL) ? nullptr : (uint4*)S->img[IMG_PXGOV].p;
   A.q_pending = (uint32_t*)S->img[IMG_QPENDING].p;
   A.god_pre = (c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL) ? nullptr : (float4*)S->img[IMG_GODPRE].p;
 }
@@ -646,6 +648,7 @@ vxe_status frame_enqueue(vxe_ctx* c, FrameState& F, const FrameArgs& A, bool tim
     k_probe_dda<<<grid((uint64_t)npix * kProbesPerPixel), SHADE_THREADS, 0, st>>>(A);
     k_slab_eval<<<grid((uint64_t)npix * kSlabsPerPixel), SHADE_THREADS, 0, st>>>(A);
     k_slab_pick<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
+    k_gov_eval<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
     k_primary_resolve<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
     if (timed) CK(cudaEventRecord(F.ev[3], st));
     if (side) {  // the far pixels the resolve queued, beside the voxel shading
@@ -722,6 +725,7 @@ vxe_status views_enqueue(vxe_ctx* c, const vxe::dev::FrameArgsViews& V, uint32_t
   k_probe_dda_views<<<grid(max_pix * kProbesPerPixel), SHADE_THREADS, 0, st>>>(V);
   k_slab_eval_views<<<grid(max_pix * kSlabsPerPixel), SHADE_THREADS, 0, st>>>(V);
   k_slab_pick_views<<<grid(max_pix), SHADE_THREADS, 0, st>>>(V);
+  k_gov_eval_views<<<grid(max_pix), SHADE_THREADS, 0, st>>>(V);
   k_primary_resolve_views<<<grid(max_pix), SHADE_THREADS, 0, st>>>(V);
   CK(cudaEventRecord(side->mid, st));
   CK(cudaStreamWaitEvent(side->s, side->mid, 0));
