@@ -1027,9 +1027,9 @@ def main():
                 "serial_frame_ms": round(res["e2e"]["serial_seconds"] * 1e3 / args.steps, 3),
                 "device_streaming": device_streaming_line(res["e2e"], args.steps, n)},
         # per frame: k_grass_wind, k_tiles, k_primary_trace, k_probe_dda, k_slab_eval, k_slab_pick,
-        # k_primary_resolve, k_shade_prep, k_shade_shadow, k_shade_lights, k_shade_vox, k_shade_far x 2 and
-        # k_godray_far (side stream), k_godray, k_composite
-        "gpu_launches": 16 * args.steps,
+        # k_gov_eval, k_primary_resolve, k_shade_prep, k_shade_shadow, k_shade_lights, k_shade_vox,
+        # k_shade_far x 2 and k_godray_far (side stream), k_godray, k_composite
+        "gpu_launches": 17 * args.steps,
         "batch": batch,
         "serve": srv,
         "configs": configs,
