@@ -1272,6 +1272,7 @@ __device__ __forceinline__ ProbeHook probe_hook_inline() {
 // atomic.
 __device__ __forceinline__ void probe_record(ProbeHook& ph, float t0, float t1, uint32_t node, v3 leaf_bmin,
                                              float leaf_size, bool anchor_valid, uint32_t anchor_key) {
+  if (ph.recs == nullptr) return;  // counting only
   const uint32_t mask = __activemask();
   const uint32_t lane = threadIdx.x & 31u, leader = __ffs(mask) - 1u;
   uint32_t base = 0u;

@@ -1094,14 +1094,32 @@ __device__ __forceinline__ void k_primary_resolve_body(const FrameArgs& A) {
     if (active) {
       pix = A.q_pending[i];
       const uint2 pp = A.px_probe[pix];
-      const uint32_t met = pp.x & 0xFFFFFFu, vcand = (pp.x >> 24) & 31u, vphase = (pp.x >> 29) & 1u;
-      const uint32_t first_phase = (pp.x & 0x40000000u) != 0u ? 0u : 1u;
-      uint32_t answer_phase = vphase;  // phase of the answer (1 when there is none)
+      const uint32_t met = pp.x & 0xFFFFFFu;
+      uint32_t vcand = (pp.x >> 24) & 31u, vphase = (pp.x >> 29) & 1u;
+      uint32_t first_phase = (pp.x & 0x40000000u) != 0u ? 0u : 1u;
       vox = (pp.x >> 31) != 0u;
+      if (A.px_gov != nullptr && A.px_gov[pix].x == 2u) {
+        // A deferred blade march left the voxel answer open: the walk again
+        // with its blade marches inline (probes only counted; their hits are
+        // the first walk's) gives the voxel answer, with the same probes
+        // before it.
+        const uint32_t gx = pix % A.iw, gy = pix / A.iw;
+        const size_t tile = (size_t)(gy >> 3) * tiles_x + (gx >> 3);
+        const PrimaryCtx c = primary_ctx(s, gx, gy, A.iw);
+        ProbeHook ph = probe_hook_inline();
+        ph.mode = PROBE_RECORD;  // recs stay null: probes are counted, not stored
+        ph.pixel = pix;
+        const VoxTraceResult vt = primary_trace<PROBE_RECORD>(s, A, c, A.tile_slots + tile * TILE_CANDS, nullptr,
+                                                              A.tile_count[tile], ph);
+        vox = vt.in_grid && vt.best.hit != 0u;
+        if (vox) store_pixhit(A.pix_hit + (size_t)pix * 5u, vt.best, vt);
+        vcand = ph.best_cand & 31u;  // as probe_summary keeps it
+        vphase = ph.phase & 1u;
+        first_phase = ph.first_phase;
+      }
+      uint32_t answer_phase = vphase;  // phase of the answer (1 when there is none)
       const unsigned long long first = A.px_first[pix];
-      // some probes were not evaluated, or a deferred blade march left the
-      // answer open
-      bool walk = pp.y < met || (A.px_gov != nullptr && A.px_gov[pix].x == 2u);
+      bool walk = pp.y < met;  // some probes were not evaluated
       if (!walk && first != ~0ull) {
         const uint32_t j = A.px_task[pix];
         const float4 res = A.slab_res[j];
