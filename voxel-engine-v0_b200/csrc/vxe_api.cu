@@ -90,6 +90,10 @@ struct FrameState {
   // set by launch_frame while an asynchronous read of the output image is in
   // flight: the composite (its writer) waits for it, the earlier passes do not
   cudaEvent_t composite_wait = nullptr;
+  // set by launch_frame when the grass cell table is (re)built on the side
+  // stream beside the walk: the first pass that reads the table (the blade
+  // marches) waits for it, the walk and the probe DDAs do not
+  cudaEvent_t table_wait = nullptr;
 };
 
 // A second stream a frame forks to (far-pixel shading beside the probe
@@ -97,6 +101,7 @@ struct FrameState {
 struct SideStream {
   cudaStream_t s = nullptr;
   cudaEvent_t fork = nullptr, mid = nullptr, prep = nullptr, join = nullptr;
+  cudaEvent_t pre = nullptr, table = nullptr;  // frame start -> side, grass table ready -> compute
 };
 
 struct BatchLane {
@@ -595,7 +600,8 @@ void frame_fill(vxe_ctx* c, FrameState& F, const vxe_camera_gpu& cam, FrameArgs&
 vxe_status side_ready(vxe_ctx* c, SideStream& S) {
   if (S.s) return VXE_OK;
   CK(cudaStreamCreateWithFlags(&S.s, cudaStreamNonBlocking));
-  for (cudaEvent_t* e : {&S.fork, &S.mid, &S.prep, &S.join}) CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  for (cudaEvent_t* e : {&S.fork, &S.mid, &S.prep, &S.join, &S.pre, &S.table})
+    CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   return VXE_OK;
 }
 
@@ -604,7 +610,7 @@ void side_release(SideStream& S) {
     cudaStreamSynchronize(S.s);
     cudaStreamDestroy(S.s);
   }
-  for (cudaEvent_t e : {S.fork, S.mid, S.prep, S.join})
+  for (cudaEvent_t e : {S.fork, S.mid, S.prep, S.join, S.pre, S.table})
     if (e) cudaEventDestroy(e);
   S = SideStream{};
 }
@@ -646,6 +652,7 @@ vxe_status frame_enqueue(vxe_ctx* c, FrameState& F, const FrameArgs& A, bool tim
       k_godray_far<<<grid(npix), SHADE_THREADS, 0, side->s>>>(A);
     }
     k_probe_dda<<<grid((uint64_t)npix * kProbesPerPixel), SHADE_THREADS, 0, st>>>(A);
+    if (F.table_wait) CK(cudaStreamWaitEvent(st, F.table_wait, 0));
     k_slab_eval<<<grid((uint64_t)npix * kSlabsPerPixel), SHADE_THREADS, 0, st>>>(A);
     k_slab_pick<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
     k_gov_eval<<<grid(npix), SHADE_THREADS, 0, st>>>(A);
@@ -759,12 +766,27 @@ vxe_status launch_frame(vxe_ctx* c, bool timed) {
   frame_fill(c, c->fr, c->cam, A);
   A.profile = (uint32_t*)c->profile.p;
   if (timed) CK(cudaEventRecord(c->fr.ev[0], c->compute));
+  // In the wavefront schedule the walk reads nothing of the grass cell table
+  // (its blade marches are deferred), so the table's per-frame rebuild runs
+  // on the side stream beside the tile lists and the walk; the blade marches
+  // wait for it.
+  const bool table_beside = !(c->flags & VXE_FLAG_PRIMARY_MEGAKERNEL);
+  cudaStream_t gst = c->compute;
+  if (table_beside) {
+    if ((st = side_ready(c, c->side)) != VXE_OK) return st;
+    CK(cudaEventRecord(c->side.pre, c->compute));
+    CK(cudaStreamWaitEvent(c->side.s, c->side.pre, 0));
+    gst = c->side.s;
+  }
   bool use_grass = false;
-  if ((st = grass_table_acquire(c, c->compute, 0, c->cam, &use_grass)) != VXE_OK) return st;
+  if ((st = grass_table_acquire(c, gst, 0, c->cam, &use_grass)) != VXE_OK) return st;
   if (use_grass) grass_table_args(c, A);
+  if (table_beside) CK(cudaEventRecord(c->side.table, gst));
+  c->fr.table_wait = table_beside ? c->side.table : nullptr;
   c->fr.composite_wait = c->out_pending ? c->out_ev : nullptr;
   st = frame_enqueue(c, c->fr, A, timed, c->compute, &c->side);
   c->fr.composite_wait = nullptr;
+  c->fr.table_wait = nullptr;
   if (st != VXE_OK) return st;
   c->out_pending = false;
   if (use_grass && (st = grass_table_release(c, c->compute, 0)) != VXE_OK) return st;
