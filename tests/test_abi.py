@@ -57,40 +57,40 @@ def test_camera_packing_is_consistent():
 
 
 def test_noalloc_argument_checks_return_before_any_device_call():
-    # vxe_trace_primary_hits_noalloc validates its arguments before touching
-    # the device (these calls need no GPU; the pointers are never read).
-    lib = A.lib()
-    fake = 256
-    sv = A.SceneView(fake, fake, 100, fake, fake, fake, 4, 8, fake, None, 0, 0)
-    clip = A.ClipmapGpu()
-    cam = A.CameraGpu()
-    cam.chunk_size = 64
-    cam.chunk_count = 2
-    cam.render_present_px[0], cam.render_present_px[1] = 64, 32
-    cam.grid_dims[0], cam.grid_dims[1], cam.grid_dims[2] = 2, 2, 2
+    """vxe_trace_primary_hits_noalloc validates its arguments on the host
+    before it touches the CUDA runtime, so these calls need no GPU.  Every
+    call here fails exactly one check; the device pointers are placeholders
+    that the host code never dereferences, so no call may pass validation."""
+    fake = 0x1000  # a non-null placeholder for a device buffer
+    base_sv = dict(nodes=fake, ropes=fake, node_count=8, metas=fake, macro_words=fake, colinfo_words=fake,
+                   chunk_capacity=4, grid_cells=8, grid=fake, clip_tex=fake, clip_layers=2, clip_res=64)
 
-    def call(s=sv, c=cam, cl=clip, hits=fake):
-        return lib.vxe_trace_primary_hits_noalloc(C.byref(s), C.byref(c), C.byref(cl), hits, None)
+    def call(sv=None, size=(64, 48), chunk_size=64, chunk_count=2, grid_dims=(2, 2, 2), levels=2, res=64,
+             hits=fake, null_scene=False):
+        v = A.SceneView(**{**base_sv, **(sv or {})})
+        cam = A.CameraGpu()
+        cam.chunk_size, cam.chunk_count = chunk_size, chunk_count
+        cam.render_present_px[0], cam.render_present_px[1] = size
+        for k in range(3):
+            cam.grid_dims[k] = grid_dims[k]
+        clip = A.ClipmapGpu()
+        clip.levels, clip.res = levels, res
+        return A.lib().vxe_trace_primary_hits_noalloc(None if null_scene else C.byref(v), C.byref(cam),
+                                                      C.byref(clip), hits, None)
 
-    def variant(**kw):
-        c = A.CameraGpu()
-        C.memmove(C.byref(c), C.byref(cam), C.sizeof(c))
-        for k, v in kw.items():
-            if isinstance(v, tuple):
-                getattr(c, k)[:len(v)] = list(v)
-            else:
-                setattr(c, k, v)
-        return c
-
-    assert call(hits=None) == 1                                   # no output buffer
-    assert call(c=variant(chunk_size=32)) == 1                    # colinfo layout needs 64
-    assert call(c=variant(render_present_px=(0, 32))) == 1        # empty image
-    assert call(c=variant(render_present_px=(4096, 2304))) == 2   # beyond VXE_NOALLOC_MAX_TILES
-    assert call(c=variant(grid_dims=(4, 2, 2))) == 2              # more cells than the grid holds
-    assert call(c=variant(chunk_count=5)) == 2                    # more chunks than the metas hold
-    lv = A.ClipmapGpu()
-    lv.levels, lv.res = 2, 256
-    assert call(cl=lv) == 1                                       # clipmap levels without a texture
-    nul = A.SceneView(*[getattr(sv, f) for f, _ in A.SceneView._fields_])
-    nul.nodes = None
-    assert call(s=nul) == 1                                       # missing scene buffer
+    INVALID, CAPACITY = 1, 2
+    assert call(null_scene=True) == INVALID
+    assert call(hits=None) == INVALID
+    assert call(sv=dict(nodes=None)) == INVALID
+    assert call(sv=dict(node_count=0)) == INVALID
+    assert call(sv=dict(grid_cells=0)) == INVALID
+    assert call(chunk_size=32) == INVALID  # the column words assume 64^3 chunks
+    assert call(size=(0, 48)) == INVALID
+    # 4096 x 2304 internal is 512 x 288 tiles of 8x8, beyond the fixed scratch
+    assert 512 * 288 > A.NOALLOC_MAX_TILES
+    assert call(size=(4096, 2304)) == CAPACITY
+    assert call(grid_dims=(2, 2, 3)) == CAPACITY  # 12 grid cells > 8
+    assert call(chunk_count=5) == CAPACITY  # more chunks than slots
+    assert call(levels=3) == INVALID  # more clipmap levels than layers
+    assert call(res=32) == INVALID  # resolution differs from the texture's
+    assert call(sv=dict(clip_tex=None)) == INVALID  # levels but no texture
