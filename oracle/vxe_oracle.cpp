@@ -17,15 +17,19 @@
 // Compile with -ffp-contract=off (no FMA contraction) so every float op is a
 // single IEEE binary32 operation, exactly as the device code evaluates it.
 //
-// Parity status: the reference is Rust + WGSL and cannot run here (no Rust
-// toolchain, no graphics stack), so this restatement is "parity unpinned"
-// against the reference itself; it is pinned against the reference's
-// structural invariants in tests/ (see tests/test_oracle_kat.py).
+// Parity status: the reference is Rust + WGSL and cannot run whole here (no
+// Rust toolchain, no graphics stack), so this restatement is pinned only in
+// part against the reference itself: its pure shading helpers are compared
+// bit for bit with the reference's own WGSL translated to C++
+// (oracle/wgsl_to_cpp.py, oracle_shading_eval below,
+// tests/test_oracle_wgsl_pin.py); the traversal is checked against an
+// independent FP64 voxel DDA (tests/test_oracle_kat.py).
 #include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -3017,6 +3021,136 @@ void ora_debug_grass(int which, uint32_t n, const float* in, float* out) {
                              (uint32_t)a[12]);
     }
   }
+}
+
+
+// Pin interface (test infrastructure): the oracle's restatements of the
+// reference's pure shading helpers behind the flat-slot calling convention of
+// the library oracle/wgsl_to_cpp.py builds from the reference's own WGSL, so a
+// test compares the two function by function.  Parameters and results are
+// float slots (vecN = N slots; u32 passes its bit pattern); cam_pos4 and
+// voxel_params4 stand in for the camera uniform.  Returns -1 for a name it
+// does not know.
+int oracle_shading_eval(const char* name, const float* in, float* out, unsigned n, const float* cam_pos4,
+                        const float* voxel_params4) {
+  vxe_camera_gpu cam;
+  std::memset(&cam, 0, sizeof cam);
+  for (int k = 0; k < 4; ++k) {
+    cam.cam_pos[k] = cam_pos4[k];
+    cam.voxel_params[k] = voxel_params4[k];
+  }
+  Counters ctr;
+  Scene sc{};
+  sc.cam = &cam;
+  sc.ctr = &ctr;
+  const Scene& s = sc;
+  auto f1 = [](const float*& a) { return *a++; };
+  auto v2_ = [](const float*& a) { const v2 r{a[0], a[1]}; a += 2; return r; };
+  auto v3_ = [](const float*& a) { const v3 r{a[0], a[1], a[2]}; a += 3; return r; };
+  auto u1 = [](const float*& a) { uint32_t u; std::memcpy(&u, a++, 4); return u; };
+  auto put1 = [](float*& o, float x) { *o++ = x; };
+  auto putu = [](float*& o, uint32_t x) { std::memcpy(o++, &x, 4); };
+  auto put2 = [](float*& o, v2 x) { *o++ = x.x; *o++ = x.y; };
+  auto put3 = [](float*& o, v3 x) { *o++ = x.x; *o++ = x.y; *o++ = x.z; };
+  auto put4 = [](float*& o, v4 x) { *o++ = x.x; *o++ = x.y; *o++ = x.z; *o++ = x.w; };
+  struct Entry {
+    const char* name;
+    unsigned in_w, out_w;
+  };
+  static const Entry widths[] = {
+      {"hash_u32", 1, 1}, {"hash12", 2, 1}, {"hash31", 3, 1}, {"value_noise", 2, 1}, {"fbm", 2, 1},
+      {"hash1", 3, 1}, {"wind_field", 4, 3}, {"clamp_len", 4, 3}, {"grass_wind_xz", 5, 2},
+      {"grass_blade_params", 4, 4}, {"sdf_box", 9, 1}, {"phase_mie", 1, 1}, {"phase_blended", 1, 1},
+      {"sky_bg", 3, 3}, {"sky_sun", 3, 3}, {"sky_color", 3, 3}, {"fog_color_from_sky", 6, 3},
+      {"fog_inscatter", 6, 3}, {"fog_optical_depth_with_base", 8, 1}, {"apply_fog", 13, 3},
+      {"cloud_height01", 1, 1}, {"cloud_coverage_at_xz", 3, 1}, {"cloud_density", 4, 1},
+      {"cloud_light_transmittance", 4, 1}, {"cloud_sun_transmittance_fast", 6, 1}, {"cloud_density_godray", 4, 1},
+      {"cloud_sun_transmittance_godray", 6, 1}, {"tonemap_filmic_hable", 3, 3}, {"tonemap_filmic_white_scale", 4, 3},
+      {"bright_extract_hue", 4, 3}, {"intersect_aabb", 12, 2}, {"safe_inv", 1, 1}, {"ray_eps_vec", 4, 3},
+      {"macro_cell_size", 1, 1}, {"grass_lod_from_t", 1, 1}, {"hemi_ambient", 6, 3}, {"color_for_material", 1, 3},
+      {"apply_material_variation", 7, 3}, {"grass_wind_dir_xz", 4, 2}, {"grass_blade_slivers", 6, 1},
+      {"grass_blade_field", 5, 1}, {"grass_top_albedo", 7, 3}, {"base_albedo", 5, 3}, {"material_roughness", 1, 1},
+      {"material_f0", 1, 1}, {"material_emission", 1, 3}, {"approx_pow_0p75", 1, 1}, {"approx_pow_0p55", 1, 1},
+      {"exp_neg_fast", 1, 1}, {"godray_steps_for_tend", 1, 1}, {"godray_decompress", 3, 3},
+      {"godray_compress", 3, 3}, {"rot_about_axis", 7, 3}, {"sphere_dir_local", 2, 3}};
+  const Entry* e = nullptr;
+  for (const Entry& w : widths)
+    if (!std::strcmp(w.name, name)) e = &w;
+  if (!e) return -1;
+  const std::string nm(name);
+  for (unsigned k = 0; k < n; ++k) {
+    const float* a = in + (size_t)k * e->in_w;
+    float* o = out + (size_t)k * e->out_w;
+    if (nm == "hash_u32") putu(o, hash_u32(u1(a)));
+    else if (nm == "hash12") put1(o, hash12(v2_(a)));
+    else if (nm == "hash31") put1(o, hash31(v3_(a)));
+    else if (nm == "value_noise") put1(o, value_noise(v2_(a)));
+    else if (nm == "fbm") put1(o, fbm(v2_(a)));
+    else if (nm == "hash1") put1(o, hash1(v3_(a)));
+    else if (nm == "wind_field") { const v3 p = v3_(a); put3(o, wind_field(p, f1(a))); }
+    else if (nm == "clamp_len") { const v3 v = v3_(a); put3(o, clamp_len(v, f1(a))); }
+    else if (nm == "grass_wind_xz") { const v3 r = v3_(a); const float t = f1(a); put2(o, grass_wind_xz(r, t, f1(a))); }
+    else if (nm == "grass_blade_params") { const v3 id = v3_(a); put4(o, grass_blade_params(id, u1(a))); }
+    else if (nm == "sdf_box") { const v3 p = v3_(a), c = v3_(a); put1(o, sdf_box(p, c, v3_(a))); }
+    else if (nm == "phase_mie") put1(o, phase_mie(f1(a)));
+    else if (nm == "phase_blended") put1(o, phase_blended(f1(a)));
+    else if (nm == "sky_bg") put3(o, sky_bg(v3_(a)));
+    else if (nm == "sky_sun") put3(o, sky_sun(v3_(a)));
+    else if (nm == "sky_color") put3(o, sky_color(s, v3_(a)));
+    else if (nm == "fog_color_from_sky") { const v3 rd = v3_(a); put3(o, fog_color_from_sky(rd, v3_(a))); }
+    else if (nm == "fog_inscatter") { const v3 rd = v3_(a); put3(o, fog_inscatter(rd, v3_(a))); }
+    else if (nm == "fog_optical_depth_with_base") {
+      const float b = f1(a);
+      const v3 ro = v3_(a), rd = v3_(a);
+      put1(o, fog_optical_depth_with_base(b, ro, rd, f1(a)));
+    } else if (nm == "apply_fog") {
+      const v3 su = v3_(a), ro = v3_(a), rd = v3_(a);
+      const float t = f1(a);
+      put3(o, apply_fog(s, su, ro, rd, t, v3_(a)));
+    } else if (nm == "cloud_height01") put1(o, cloud_height01(f1(a)));
+    else if (nm == "cloud_coverage_at_xz") { const v2 xz = v2_(a); put1(o, cloud_coverage_at_xz(xz, f1(a))); }
+    else if (nm == "cloud_density") { const v3 p = v3_(a); put1(o, cloud_density(p, f1(a))); }
+    else if (nm == "cloud_light_transmittance") { const v3 p = v3_(a); put1(o, cloud_light_transmittance(p, f1(a))); }
+    else if (nm == "cloud_sun_transmittance_fast") { const v3 p = v3_(a); put1(o, cloud_sun_transmittance_fast(s, p, v3_(a))); }
+    else if (nm == "cloud_density_godray") { const v3 p = v3_(a); put1(o, cloud_density_godray(p, f1(a))); }
+    else if (nm == "cloud_sun_transmittance_godray") { const v3 p = v3_(a); put1(o, cloud_sun_transmittance_godray(s, p, v3_(a))); }
+    else if (nm == "tonemap_filmic_hable") put3(o, hable(v3_(a)));
+    else if (nm == "tonemap_filmic_white_scale") { const v3 x = v3_(a); put3(o, tonemap_white(x, f1(a))); }
+    else if (nm == "bright_extract_hue") { const v3 x = v3_(a); put3(o, bright_extract_hue(x, f1(a))); }
+    else if (nm == "intersect_aabb") {
+      const v3 ro = v3_(a), rd = v3_(a), b0 = v3_(a);
+      put2(o, intersect_aabb(ro, rd, b0, v3_(a)));
+    } else if (nm == "safe_inv") put1(o, safe_inv(f1(a)));
+    else if (nm == "ray_eps_vec") { const v3 rd = v3_(a); put3(o, ray_eps_vec(rd, f1(a))); }
+    else if (nm == "macro_cell_size") put1(o, macro_cell_size(f1(a)));
+    else if (nm == "grass_lod_from_t") putu(o, grass_lod_from_t(f1(a)));
+    else if (nm == "hemi_ambient") { const v3 nn = v3_(a); put3(o, hemi_ambient(nn, v3_(a))); }
+    else if (nm == "color_for_material") put3(o, color_for_material(u1(a)));
+    else if (nm == "apply_material_variation") {
+      const v3 b = v3_(a);
+      const uint32_t m = u1(a);
+      put3(o, apply_material_variation(b, m, v3_(a)));
+    } else if (nm == "grass_wind_dir_xz") { const v3 p = v3_(a); put2(o, grass_wind_dir_xz(p, f1(a))); }
+    else if (nm == "grass_blade_slivers") {
+      const v3 p = v3_(a);
+      const float t = f1(a), fr = f1(a);
+      put1(o, grass_blade_slivers(p, t, fr, f1(a)));
+    } else if (nm == "grass_blade_field") { const v3 p = v3_(a); const float t = f1(a); put1(o, grass_blade_field(p, t, f1(a))); }
+    else if (nm == "grass_top_albedo") { const v3 b = v3_(a), hp = v3_(a); put3(o, grass_top_albedo(s, b, hp, f1(a))); }
+    else if (nm == "base_albedo") { const uint32_t m = u1(a); const v3 hp = v3_(a); put3(o, base_albedo(m, hp, f1(a))); }
+    else if (nm == "material_roughness") put1(o, material_roughness(u1(a)));
+    else if (nm == "material_f0") put1(o, material_f0(u1(a)));
+    else if (nm == "material_emission") put3(o, material_emission(u1(a)));
+    else if (nm == "approx_pow_0p75") put1(o, approx_pow_0p75(f1(a)));
+    else if (nm == "approx_pow_0p55") put1(o, approx_pow_0p55(f1(a)));
+    else if (nm == "exp_neg_fast") put1(o, exp_neg_fast(f1(a)));
+    else if (nm == "godray_steps_for_tend") putu(o, godray_steps_for_tend(f1(a)));
+    else if (nm == "godray_decompress") put3(o, godray_decompress(v3_(a)));
+    else if (nm == "godray_compress") put3(o, godray_compress(v3_(a)));
+    else if (nm == "rot_about_axis") { const v3 v = v3_(a), ax = v3_(a); put3(o, rot_about_axis(v, ax, f1(a))); }
+    else if (nm == "sphere_dir_local") { const uint32_t i = u1(a); put3(o, sphere_dir_local(i, u1(a))); }
+  }
+  return 0;
 }
 
 

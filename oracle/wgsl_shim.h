@@ -1,0 +1,314 @@
+// WGSL types and builtins in C++, for the translated reference shader
+// functions of oracle/_ref (test infrastructure: only the pin test of the
+// oracle uses it, never the product).
+//
+// The translation (oracle/wgsl_to_cpp.py) turns `vec3<f32>` into `vec3f`,
+// `.xz` into `.xz()`, `u32(x)` into `wgsl_u32(x)` and so on; this header
+// supplies those names with the semantics the oracle documents for the WGSL
+// builtins: mix(a,b,t) = a*(1-t) + b*t, smoothstep per the WGSL spec,
+// clamp = min(max(x, lo), hi), min/max as IEEE minimumNumber/maximumNumber,
+// normalize(v) = v * (1/sqrt(dot(v,v))), saturating float -> integer
+// conversion, and sin/cos/exp/pow from include/vxe/detmath.h.  With the same
+// elementary functions on both sides, any difference between a translated
+// reference function and the oracle's restatement of it is a difference in
+// the restatement.
+#pragma once
+
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <type_traits>
+
+#include "vxe/detmath.h"
+
+namespace wgsl {
+
+using f32 = float;
+using u32 = uint32_t;
+using i32 = int32_t;
+
+inline float wmin(float a, float b) {
+  if (a != a) return b;
+  if (b != b) return a;
+  if (a < b) return a;
+  if (b < a) return b;
+  return std::signbit(a) ? a : b;
+}
+inline float wmax(float a, float b) {
+  if (a != a) return b;
+  if (b != b) return a;
+  if (a > b) return a;
+  if (b > a) return b;
+  return std::signbit(a) ? b : a;
+}
+inline u32 wmin(u32 a, u32 b) { return a < b ? a : b; }
+inline u32 wmax(u32 a, u32 b) { return a > b ? a : b; }
+inline i32 wmin(i32 a, i32 b) { return a < b ? a : b; }
+inline i32 wmax(i32 a, i32 b) { return a > b ? a : b; }
+
+template <class T, int N>
+struct vec {
+  T v[N];
+  T& operator[](int i) { return v[i]; }
+  const T& operator[](int i) const { return v[i]; }
+};
+
+template <class T>
+struct vec<T, 2> {
+  T x, y;
+  vec() : x(), y() {}
+  explicit vec(T s) : x(s), y(s) {}
+  vec(T a, T b) : x(a), y(b) {}
+  T& operator[](int i) { return i == 0 ? x : y; }
+  const T& operator[](int i) const { return i == 0 ? x : y; }
+};
+
+template <class T>
+struct vec<T, 3> {
+  T x, y, z;
+  vec() : x(), y(), z() {}
+  explicit vec(T s) : x(s), y(s), z(s) {}
+  vec(T a, T b, T c) : x(a), y(b), z(c) {}
+  vec(vec<T, 2> a, T c) : x(a.x), y(a.y), z(c) {}
+  vec(T a, vec<T, 2> b) : x(a), y(b.x), z(b.y) {}
+  vec<T, 2> xy() const { return {x, y}; }
+  vec<T, 2> xz() const { return {x, z}; }
+  vec<T, 3> xyz() const { return *this; }
+  T& operator[](int i) { return i == 0 ? x : (i == 1 ? y : z); }
+  const T& operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+};
+
+template <class T>
+struct vec<T, 4> {
+  T x, y, z, w;
+  vec() : x(), y(), z(), w() {}
+  explicit vec(T s) : x(s), y(s), z(s), w(s) {}
+  vec(T a, T b, T c, T d) : x(a), y(b), z(c), w(d) {}
+  vec(vec<T, 3> a, T d) : x(a.x), y(a.y), z(a.z), w(d) {}
+  vec(vec<T, 2> a, T c, T d) : x(a.x), y(a.y), z(c), w(d) {}
+  vec(vec<T, 2> a, vec<T, 2> b) : x(a.x), y(a.y), z(b.x), w(b.y) {}
+  vec<T, 2> xy() const { return {x, y}; }
+  vec<T, 2> xz() const { return {x, z}; }
+  vec<T, 3> xyz() const { return {x, y, z}; }
+  T& operator[](int i) { return i == 0 ? x : (i == 1 ? y : (i == 2 ? z : w)); }
+  const T& operator[](int i) const { return i == 0 ? x : (i == 1 ? y : (i == 2 ? z : w)); }
+};
+
+using vec2f = vec<float, 2>;
+using vec3f = vec<float, 3>;
+using vec4f = vec<float, 4>;
+using vec2i = vec<i32, 2>;
+using vec3i = vec<i32, 3>;
+using vec4i = vec<i32, 4>;
+using vec2u = vec<u32, 2>;
+using vec3u = vec<u32, 3>;
+using vec4u = vec<u32, 4>;
+
+// Component-wise application.
+template <class T, int N, class F>
+inline vec<T, N> cw(const vec<T, N>& a, F f) {
+  vec<T, N> r;
+  for (int i = 0; i < N; ++i) r[i] = f(a[i]);
+  return r;
+}
+template <class T, int N, class F>
+inline vec<T, N> cw2(const vec<T, N>& a, const vec<T, N>& b, F f) {
+  vec<T, N> r;
+  for (int i = 0; i < N; ++i) r[i] = f(a[i], b[i]);
+  return r;
+}
+
+// Scalar operands of any arithmetic type convert to the vector's component
+// type (WGSL's abstract literals take the type of the other operand).
+#define WGSL_VEC_OP(op)                                                                      \
+  template <class T, int N>                                                                  \
+  inline vec<T, N> operator op(const vec<T, N>& a, const vec<T, N>& b) {                      \
+    return cw2(a, b, [](T p, T q) { return p op q; });                                       \
+  }                                                                                          \
+  template <class T, int N, class S, class = std::enable_if_t<std::is_arithmetic_v<S>>>      \
+  inline vec<T, N> operator op(const vec<T, N>& a, S s0) {                                   \
+    const T s = (T)s0;                                                                       \
+    return cw(a, [s](T p) { return p op s; });                                               \
+  }                                                                                          \
+  template <class T, int N, class S, class = std::enable_if_t<std::is_arithmetic_v<S>>>      \
+  inline vec<T, N> operator op(S s0, const vec<T, N>& a) {                                   \
+    const T s = (T)s0;                                                                       \
+    return cw(a, [s](T p) { return s op p; });                                               \
+  }                                                                                          \
+  template <class T, int N>                                                                  \
+  inline vec<T, N>& operator op##=(vec<T, N>& a, const vec<T, N>& b) { return a = a op b; }   \
+  template <class T, int N, class S, class = std::enable_if_t<std::is_arithmetic_v<S>>>      \
+  inline vec<T, N>& operator op##=(vec<T, N>& a, S s) { return a = a op s; }
+WGSL_VEC_OP(+)
+WGSL_VEC_OP(-)
+WGSL_VEC_OP(*)
+WGSL_VEC_OP(/)
+#undef WGSL_VEC_OP
+
+// mat2x2<f32>: two columns; m * v sums column by column (c0 * v.x + c1 * v.y).
+struct mat2x2f {
+  vec2f c0, c1;
+  mat2x2f(float a, float b, float c, float d) : c0(a, b), c1(c, d) {}
+};
+inline vec2f operator*(const mat2x2f& m, const vec2f& v) { return m.c0 * v.x + m.c1 * v.y; }
+
+template <class T, int N>
+inline vec<T, N> operator-(const vec<T, N>& a) {
+  return cw(a, [](T p) { return -p; });
+}
+
+// Scalars (WGSL spellings).
+inline float abs(float x) { return std::fabs(x); }
+inline i32 abs(i32 x) { return x < 0 ? -x : x; }
+inline float floor(float x) { return std::floor(x); }
+inline float ceil(float x) { return std::ceil(x); }
+inline float round(float x) { return std::nearbyint(x); }
+inline float trunc(float x) { return std::trunc(x); }
+inline float fract(float x) { return x - std::floor(x); }
+inline float sqrt(float x) { return std::sqrt(x); }
+inline float inverseSqrt(float x) { return 1.0f / std::sqrt(x); }
+inline float sin(float x) { return vxe_sinf(x); }
+inline float cos(float x) { return vxe_cosf(x); }
+inline float exp(float x) { return vxe_expf(x); }
+inline float pow(float x, float y) { return vxe_powf(x, y); }
+inline float min(float a, float b) { return wmin(a, b); }
+inline float max(float a, float b) { return wmax(a, b); }
+inline u32 min(u32 a, u32 b) { return wmin(a, b); }
+inline u32 max(u32 a, u32 b) { return wmax(a, b); }
+inline i32 min(i32 a, i32 b) { return wmin(a, b); }
+inline i32 max(i32 a, i32 b) { return wmax(a, b); }
+inline float clamp(float x, float lo, float hi) { return wmin(wmax(x, lo), hi); }
+inline u32 clamp(u32 x, u32 lo, u32 hi) { return wmin(wmax(x, lo), hi); }
+inline i32 clamp(i32 x, i32 lo, i32 hi) { return wmin(wmax(x, lo), hi); }
+inline float mix(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+inline float smoothstep(float e0, float e1, float x) {
+  const float t = clamp((x - e0) / (e1 - e0), 0.0f, 1.0f);
+  return t * t * (3.0f - 2.0f * t);
+}
+inline float step(float edge, float x) { return x < edge ? 0.0f : 1.0f; }
+inline float sign(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
+inline float saturate(float x) { return clamp(x, 0.0f, 1.0f); }
+
+// Vectors.
+#define WGSL_VEC_FN1(name)                                                \
+  template <class T, int N>                                               \
+  inline vec<T, N> name(const vec<T, N>& a) {                             \
+    return cw(a, [](T p) { return name(p); });                            \
+  }
+WGSL_VEC_FN1(abs)
+WGSL_VEC_FN1(floor)
+WGSL_VEC_FN1(ceil)
+WGSL_VEC_FN1(round)
+WGSL_VEC_FN1(trunc)
+WGSL_VEC_FN1(fract)
+WGSL_VEC_FN1(sqrt)
+WGSL_VEC_FN1(sin)
+WGSL_VEC_FN1(cos)
+WGSL_VEC_FN1(exp)
+WGSL_VEC_FN1(sign)
+WGSL_VEC_FN1(saturate)
+#undef WGSL_VEC_FN1
+
+template <class T, int N>
+inline vec<T, N> min(const vec<T, N>& a, const vec<T, N>& b) {
+  return cw2(a, b, [](T p, T q) { return min(p, q); });
+}
+template <class T, int N>
+inline vec<T, N> max(const vec<T, N>& a, const vec<T, N>& b) {
+  return cw2(a, b, [](T p, T q) { return max(p, q); });
+}
+template <class T, int N>
+inline vec<T, N> pow(const vec<T, N>& a, const vec<T, N>& b) {
+  return cw2(a, b, [](T p, T q) { return pow(p, q); });
+}
+template <class T, int N>
+inline vec<T, N> clamp(const vec<T, N>& x, const vec<T, N>& lo, const vec<T, N>& hi) {
+  vec<T, N> r;
+  for (int i = 0; i < N; ++i) r[i] = clamp(x[i], lo[i], hi[i]);
+  return r;
+}
+template <class T, int N>
+inline vec<T, N> clamp(const vec<T, N>& x, T lo, T hi) {
+  return cw(x, [lo, hi](T p) { return clamp(p, lo, hi); });
+}
+template <int N>
+inline vec<float, N> mix(const vec<float, N>& a, const vec<float, N>& b, float t) {
+  vec<float, N> r;
+  for (int i = 0; i < N; ++i) r[i] = mix(a[i], b[i], t);
+  return r;
+}
+template <int N>
+inline vec<float, N> mix(const vec<float, N>& a, const vec<float, N>& b, const vec<float, N>& t) {
+  vec<float, N> r;
+  for (int i = 0; i < N; ++i) r[i] = mix(a[i], b[i], t[i]);
+  return r;
+}
+template <int N>
+inline vec<float, N> smoothstep(float e0, float e1, const vec<float, N>& x) {
+  return cw(x, [e0, e1](float p) { return smoothstep(e0, e1, p); });
+}
+template <int N>
+inline vec<float, N> step(const vec<float, N>& e, const vec<float, N>& x) {
+  return cw2(e, x, [](float p, float q) { return step(p, q); });
+}
+// dot sums left to right: ((a.x*b.x + a.y*b.y) + a.z*b.z) + a.w*b.w
+template <class T, int N>
+inline T dot(const vec<T, N>& a, const vec<T, N>& b) {
+  T s = a[0] * b[0];
+  for (int i = 1; i < N; ++i) s = s + a[i] * b[i];
+  return s;
+}
+inline vec3f cross(const vec3f& a, const vec3f& b) {
+  return vec3f(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+template <int N>
+inline float length(const vec<float, N>& a) {
+  return std::sqrt(dot(a, a));
+}
+template <int N>
+inline vec<float, N> normalize(const vec<float, N>& a) {
+  const float inv = 1.0f / std::sqrt(dot(a, a));
+  return a * inv;
+}
+inline float length(float a) { return std::fabs(a); }
+
+template <class T>
+inline T wgsl_select(T f, T t, bool c) {
+  return c ? t : f;
+}
+
+// Conversions with WGSL semantics (float -> integer saturates, NaN -> 0).
+inline float wgsl_f32(float x) { return x; }
+inline float wgsl_f32(u32 x) { return (float)x; }
+inline float wgsl_f32(i32 x) { return (float)x; }
+inline float wgsl_f32(bool x) { return x ? 1.0f : 0.0f; }
+inline u32 wgsl_u32(float f) {
+  if (f != f || f <= 0.0f) return 0u;
+  if (f >= 4294967296.0f) return 0xFFFFFFFFu;
+  return (u32)f;
+}
+inline u32 wgsl_u32(u32 x) { return x; }
+inline u32 wgsl_u32(i32 x) { return (u32)x; }
+inline u32 wgsl_u32(bool x) { return x ? 1u : 0u; }
+inline i32 wgsl_i32(float f) {
+  if (f != f) return 0;
+  if (f >= 2147483648.0f) return INT32_MAX;
+  if (f <= -2147483648.0f) return INT32_MIN;
+  return (i32)f;
+}
+inline i32 wgsl_i32(i32 x) { return x; }
+inline i32 wgsl_i32(u32 x) { return (i32)x; }
+inline u32 bitcast_u32(float f) {
+  u32 u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+inline u32 bitcast_u32(i32 i) { return (u32)i; }
+inline float bitcast_f32(u32 u) {
+  float f;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+}  // namespace wgsl

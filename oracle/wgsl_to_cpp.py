@@ -1,0 +1,236 @@
+"""Translates pure helper functions of the reference's WGSL into C++ (test
+infrastructure for pinning the oracle; never part of the product).
+
+The reference is Rust + WGSL: its shaders cannot run here (no graphics stack)
+and its host cannot be built (no Rust toolchain).  Its pure shading helpers
+(sky, sun, clouds, fog, phase, tonemap, wind, hashes, value noise) are plain
+arithmetic, though, and WGSL's syntax for them is close to C++.  This script
+rewrites them mechanically, at build time, from the shader sources where they
+lie, into oracle/_ref/ref_wgsl.cpp over oracle/wgsl_shim.h (vector types and
+builtins with WGSL semantics), and compiles that into oracle/_ref/libref_wgsl.so.
+Nothing of the reference is committed: oracle/_ref is git-ignored.
+
+The library exports
+    int ref_wgsl_eval(const char* name, const float* in, float* out, unsigned n)
+    int ref_wgsl_widths(const char* name, unsigned* in_w, unsigned* out_w)
+    void ref_wgsl_set_cam(const float* cam_pos4, const float* voxel_params4)
+over the exported functions: parameters and results are flattened into float
+slots (vecN = N slots; u32 / i32 / bool pass their bit patterns), n calls in a
+row.  The oracle exports the same interface over its own restatements
+(oracle_shading_eval), so a test compares the two function by function.
+
+Usage: python oracle/wgsl_to_cpp.py <reference shader dir> <out .cpp>
+"""
+from __future__ import annotations
+
+import re
+import sys
+from pathlib import Path
+
+FILES = ["common.wgsl", "ray/wind.wgsl", "ray/phase.wgsl", "ray/fog.wgsl", "ray/clouds.wgsl", "ray/sky.wgsl",
+         "ray/composite.wgsl", "ray/grass.wgsl", "ray/shading.wgsl", "ray/godrays.wgsl", "ray/light.wgsl"]
+
+# The functions the pin compares (each with its whole call closure).
+EXPORTS = ["hash_u32", "hash12", "hash31", "value_noise", "fbm", "hash1", "wind_field", "clamp_len",
+           "grass_wind_xz", "grass_blade_params", "sdf_box", "phase_mie", "phase_blended", "sky_bg", "sky_sun",
+           "sky_color", "fog_color_from_sky", "fog_inscatter", "fog_optical_depth_with_base",
+           "fog_transmittance_primary", "fog_transmittance_godray", "apply_fog", "cloud_height01",
+           "cloud_coverage_at_xz", "cloud_density", "cloud_light_transmittance", "cloud_sun_transmittance_fast",
+           "cloud_density_godray", "cloud_sun_transmittance_godray", "tonemap_filmic_hable",
+           "tonemap_filmic_white_scale", "gamma_encode", "bright_extract_hue", "intersect_aabb", "safe_inv",
+           "ray_eps_vec", "macro_cell_size", "grass_lod_from_t", "hemi_ambient", "color_for_material",
+           "apply_material_variation", "grass_wind_dir_xz", "grass_blade_slivers", "grass_blade_field",
+           "grass_top_albedo", "base_albedo", "material_roughness", "material_f0", "material_emission",
+           "approx_pow_0p75", "approx_pow_0p55", "exp_neg_fast", "godray_steps_for_tend", "godray_decompress",
+           "godray_compress", "rot_about_axis", "sphere_dir_local"]
+
+TYPE_MAP = {"f32": "float", "u32": "uint32_t", "i32": "int32_t", "bool": "bool"}
+WIDTH = {"float": 1, "uint32_t": 1, "int32_t": 1, "bool": 1, "vec2f": 2, "vec3f": 3, "vec4f": 4}
+
+
+def strip_comments(src: str) -> str:
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return re.sub(r"//[^\n]*", "", src)
+
+
+def match_brace(src: str, i: int) -> int:
+    """Index just past the brace block that opens at src[i] == '{'."""
+    depth = 0
+    for j in range(i, len(src)):
+        if src[j] == "{":
+            depth += 1
+        elif src[j] == "}":
+            depth -= 1
+            if depth == 0:
+                return j + 1
+    raise ValueError("unbalanced braces")
+
+
+def conv_type(t: str) -> str:
+    t = t.strip()
+    t = re.sub(r"\bvec([234])<f32>", r"vec\1f", t)
+    t = re.sub(r"\bvec([234])<i32>", r"vec\1i", t)
+    t = re.sub(r"\bvec([234])<u32>", r"vec\1u", t)
+    t = re.sub(r"\bmat2x2<f32>", "mat2x2f", t)
+    t = re.sub(r"\barray<\s*([^,>]+)\s*,\s*([^>]+)>", lambda m: f"std::array<{conv_type(m.group(1))}, {m.group(2).strip()}>", t)
+    return TYPE_MAP.get(t, t)
+
+
+def conv_expr(s: str) -> str:
+    """WGSL statements / expressions -> C++ over wgsl_shim.h."""
+    s = re.sub(r"\bvec([234])<f32>", r"vec\1f", s)
+    s = re.sub(r"\bvec([234])<i32>", r"vec\1i", s)
+    s = re.sub(r"\bvec([234])<u32>", r"vec\1u", s)
+    s = re.sub(r"\bmat2x2<f32>", "mat2x2f", s)
+    s = re.sub(r"\bbitcast<u32>\s*\(", "bitcast_u32(", s)
+    s = re.sub(r"\bbitcast<f32>\s*\(", "bitcast_f32(", s)
+    s = re.sub(r"\bbitcast<i32>\s*\(", "bitcast_i32(", s)
+    # declarations
+    s = re.sub(r"\blet\s+(\w+)\s*:\s*([^=;]+?)\s*=", lambda m: f"const {conv_type(m.group(2))} {m.group(1)} =", s)
+    s = re.sub(r"\blet\s+(\w+)\s*=", r"const auto \1 =", s)
+    s = re.sub(r"\bconst\s+(\w+)\s*:\s*([^=;]+?)\s*=", lambda m: f"const {conv_type(m.group(2))} {m.group(1)} =", s)
+    s = re.sub(r"\bconst\s+(\w+)\s*=", r"const auto \1 =", s)
+    s = re.sub(r"\bvar\s+(\w+)\s*:\s*([^=;]+?)\s*=", lambda m: f"{conv_type(m.group(2))} {m.group(1)} =", s)
+    s = re.sub(r"\bvar\s+(\w+)\s*:\s*([^=;]+?)\s*;", lambda m: f"{conv_type(m.group(2))} {m.group(1)}{{}};", s)
+    s = re.sub(r"\bvar\s+(\w+)\s*=", r"auto \1 =", s)
+    # conversions, builtins with other C++ names, swizzles, loops
+    s = re.sub(r"\bf32\s*\(", "wgsl_f32(", s)
+    s = re.sub(r"\bu32\s*\(", "wgsl_u32(", s)
+    s = re.sub(r"\bi32\s*\(", "wgsl_i32(", s)
+    s = re.sub(r"\bf32\b", "float", s)
+    s = re.sub(r"\bu32\b", "uint32_t", s)
+    s = re.sub(r"\bi32\b", "int32_t", s)
+    s = re.sub(r"\bselect\s*\(", "wgsl_select(", s)
+    s = re.sub(r"\.(xyz|xz|xy)\b", r".\1()", s)
+    s = re.sub(r"\bloop\s*\{", "for (;;) {", s)
+    # literals: WGSL floats are f32 (C++ would make them double)
+    s = re.sub(r"(?<![\w.])(\d+)i\b", r"\1", s)
+    s = re.sub(r"(?<![\w.])(\d+)f\b", r"\1.0f", s)
+    s = re.sub(r"(?<![\w.])(\d+\.\d*|\.\d+)([eE][-+]?\d+)?(?![\w.])", r"\1\2f", s)
+    s = re.sub(r"(?<![\w.])(\d+)([eE][-+]?\d+)(?![\w.])", r"\1.0\2f", s)
+    return s
+
+
+def parse(shader_dir: Path):
+    consts, fns = [], {}
+    for rel in FILES:
+        src = strip_comments((shader_dir / rel).read_text())
+        i = 0
+        while i < len(src):
+            m = re.compile(r"\s*(const|fn|struct|@|alias|override|var|enable)").match(src, i)
+            if not m:
+                i += 1
+                continue
+            kind = m.group(1)
+            if kind == "const":
+                end = src.index(";", m.end())
+                cm = re.match(r"\s*const\s+(\w+)\s*(?::\s*([^=]+?))?\s*=\s*(.*)", src[i:end], flags=re.S)
+                if cm:
+                    consts.append((cm.group(1), cm.group(2), cm.group(3)))
+                i = end + 1
+            elif kind == "fn":
+                fm = re.compile(r"\s*fn\s+(\w+)\s*\((.*?)\)\s*(?:->\s*([^{]+?))?\s*\{", re.S).match(src, i)
+                end = match_brace(src, fm.end() - 1)
+                fns[fm.group(1)] = (fm.group(2), fm.group(3), src[fm.end():end - 1], rel)
+                i = end
+            elif kind == "struct":
+                sm = re.compile(r"\s*struct\s+\w+\s*\{").match(src, i)
+                i = match_brace(src, sm.end() - 1)
+            else:
+                end = src.find(";", m.end())
+                brace = src.find("{", m.end())
+                i = (end + 1) if end >= 0 and (brace < 0 or end < brace) else (match_brace(src, brace) if brace >= 0 else len(src))
+    return consts, fns
+
+
+def closure(fns, roots):
+    out, todo = [], list(roots)
+    while todo:
+        f = todo.pop()
+        if f in out or f not in fns:
+            continue
+        out.append(f)
+        for callee in re.findall(r"\b(\w+)\s*\(", fns[f][2]):
+            if callee in fns and callee not in out:
+                todo.append(callee)
+    return out
+
+
+def params_of(ptext: str):
+    ps = []
+    for p in [p.strip() for p in ptext.split(",") if p.strip()]:
+        name, ty = p.split(":", 1)
+        ps.append((name.strip(), conv_type(ty)))
+    return ps
+
+
+def main(shader_dir: Path, out: Path) -> None:
+    consts, fns = parse(shader_dir)
+    names = closure(fns, EXPORTS)
+    lines = ["// Generated by oracle/wgsl_to_cpp.py from the reference's WGSL; not committed.",
+             '#include "wgsl_shim.h"', "#include <cstring>", "namespace wgsl {",
+             "struct CamShim { vec4f cam_pos; vec4f voxel_params; };", "static CamShim cam;"]
+    for name, ty, expr in consts:
+        ty_c = conv_type(ty) if ty else "auto"
+        lines.append(f"static const {ty_c} {name} = {conv_expr(expr.strip())};")
+    sigs = {}
+    for f in names:
+        ptext, ret, body, rel = fns[f]
+        ps = params_of(ptext)
+        rt = conv_type(ret) if ret else "void"
+        sigs[f] = (ps, rt)
+        lines.append(f"{rt} {f}({', '.join(f'{t} {n}' for n, t in ps)});")
+    for f in names:
+        ptext, ret, body, rel = fns[f]
+        ps, rt = sigs[f]
+        lines.append(f"// {rel}")
+        lines.append(f"{rt} {f}({', '.join(f'{t} {n}' for n, t in ps)}) {{{conv_expr(body)}}}")
+    lines.append("}  // namespace wgsl")
+    # the flat-slot dispatcher
+    lines += ["using namespace wgsl;",
+              "template <class T> static T get_slot(const float*& p) { T v; std::memcpy(&v, p, 4); ++p; return v; }",
+              "static float get_f(const float*& p) { return *p++; }",
+              "template <int N> static vec<float, N> get_v(const float*& p) { vec<float, N> v; for (int i = 0; i < N; ++i) v[i] = *p++; return v; }",
+              "static void put(float*& o, float v) { *o++ = v; }",
+              "static void put(float*& o, uint32_t v) { std::memcpy(o++, &v, 4); }",
+              "static void put(float*& o, int32_t v) { std::memcpy(o++, &v, 4); }",
+              "template <int N> static void put(float*& o, const vec<float, N>& v) { for (int i = 0; i < N; ++i) *o++ = v[i]; }",
+              'extern "C" void ref_wgsl_set_cam(const float* p, const float* vp) { for (int i = 0; i < 4; ++i) { cam.cam_pos[i] = p[i]; cam.voxel_params[i] = vp[i]; } }',
+              'extern "C" int ref_wgsl_widths(const char* name, unsigned* in_w, unsigned* out_w) {']
+    table = []
+    for f in EXPORTS:
+        if f not in sigs:
+            continue
+        ps, rt = sigs[f]
+        if rt not in WIDTH or any(t not in WIDTH for _, t in ps):
+            continue
+        table.append(f)
+        lines.append(f'  if (!std::strcmp(name, "{f}")) {{ *in_w = {sum(WIDTH[t] for _, t in ps)}; *out_w = {WIDTH[rt]}; return 0; }}')
+    lines += ["  return -1;", "}",
+              'extern "C" int ref_wgsl_eval(const char* name, const float* in, float* out, unsigned n) {',
+              "  unsigned iw = 0, ow = 0;", "  if (ref_wgsl_widths(name, &iw, &ow) != 0) return -1;",
+              "  for (unsigned k = 0; k < n; ++k) {",
+              "    const float* p = in + (size_t)k * iw; float* o = out + (size_t)k * ow;"]
+    for f in table:
+        ps, rt = sigs[f]
+        args = []
+        for _, t in ps:
+            if t == "float":
+                args.append("get_f(p)")
+            elif t in ("uint32_t", "int32_t"):
+                args.append(f"get_slot<{t}>(p)")
+            elif t == "bool":
+                args.append("(get_slot<uint32_t>(p) != 0u)")
+            else:
+                args.append(f"get_v<{WIDTH[t]}>(p)")
+        # arguments are read in order into locals first (evaluation order)
+        decl = "; ".join(f"const auto a{i} = {a}" for i, a in enumerate(args))
+        call = f"{f}({', '.join(f'a{i}' for i in range(len(args)))})"
+        lines.append(f'    if (!std::strcmp(name, "{f}")) {{ {decl}{";" if decl else ""} put(o, {call}); continue; }}')
+    lines += ["  }", "  return 0;", "}"]
+    out.parent.mkdir(parents=True, exist_ok=True)
+    out.write_text("\n".join(lines) + "\n")
+
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1]), Path(sys.argv[2]))

@@ -1,0 +1,183 @@
+"""Pins the oracle's shading restatements to the reference's own WGSL.
+
+The reference's pure shading helpers (sky, sun, clouds, fog, phase, tonemap,
+wind, hashes, value noise) are translated mechanically from its WGSL into C++
+at build time (oracle/wgsl_to_cpp.py -> oracle/_ref/libref_wgsl.so, over
+oracle/wgsl_shim.h).  The oracle restates the same functions by hand
+(oracle/vxe_oracle.cpp, oracle_shading_eval).  With the same elementary
+functions on both sides, every output must be identical bit for bit on
+seeded inputs: a difference is a mis-reading in the restatement.
+
+The translated library is built only where the reference's sources are
+present; elsewhere these tests are skipped.
+"""
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+REPO = Path(__file__).resolve().parents[1]
+REF_LIB = REPO / "oracle" / "_ref" / "libref_wgsl.so"
+ORACLE_LIB = REPO / "oracle" / "liboracle_vxe.so"
+
+# the camera uniform the sky / fog / cloud helpers read: position and
+# voxel_params = [voxel size, time_s, wind strength, fog density]
+CAM_POS = np.array([12.5, 31.0, -7.25, 0.0], np.float32)
+VOXEL_PARAMS = np.array([0.1, 7.3, 2.0, 0.002], np.float32)
+
+FUNCS = ["hash_u32", "hash12", "hash31", "value_noise", "fbm", "hash1", "wind_field", "clamp_len", "grass_wind_xz",
+         "grass_blade_params", "sdf_box", "phase_mie", "phase_blended", "sky_bg", "sky_sun", "sky_color",
+         "fog_color_from_sky", "fog_inscatter", "fog_optical_depth_with_base", "apply_fog", "cloud_height01",
+         "cloud_coverage_at_xz", "cloud_density", "cloud_light_transmittance", "cloud_sun_transmittance_fast",
+         "cloud_density_godray", "cloud_sun_transmittance_godray", "tonemap_filmic_hable",
+         "tonemap_filmic_white_scale", "bright_extract_hue", "intersect_aabb", "safe_inv", "ray_eps_vec",
+         "macro_cell_size", "grass_lod_from_t", "hemi_ambient", "color_for_material", "apply_material_variation",
+         "grass_wind_dir_xz", "grass_blade_slivers", "grass_blade_field", "grass_top_albedo", "base_albedo",
+         "material_roughness", "material_f0", "material_emission", "approx_pow_0p75", "approx_pow_0p55",
+         "exp_neg_fast", "godray_steps_for_tend", "godray_decompress", "godray_compress", "rot_about_axis",
+         "sphere_dir_local"]
+
+
+def load_libs():
+    if not REF_LIB.exists():
+        pytest.skip("the reference's WGSL was not translated here (no reference sources on this machine)")
+    ref = C.CDLL(str(REF_LIB))
+    ora = C.CDLL(str(ORACLE_LIB))
+    fp = C.POINTER(C.c_float)
+    ref.ref_wgsl_eval.argtypes = [C.c_char_p, fp, fp, C.c_uint]
+    ref.ref_wgsl_widths.argtypes = [C.c_char_p, C.POINTER(C.c_uint), C.POINTER(C.c_uint)]
+    ref.ref_wgsl_set_cam.argtypes = [fp, fp]
+    ora.oracle_shading_eval.argtypes = [C.c_char_p, fp, fp, C.c_uint, fp, fp]
+    ref.ref_wgsl_set_cam(CAM_POS.ctypes.data_as(fp), VOXEL_PARAMS.ctypes.data_as(fp))
+    return ref, ora
+
+
+def _dirs(rng, n, up_bias=0.0):
+    d = rng.normal(size=(n, 3))
+    d[:, 1] += up_bias
+    return d / np.linalg.norm(d, axis=1, keepdims=True)
+
+
+def gen_inputs(name: str, n: int, seed: int = 7) -> np.ndarray:
+    """Seeded inputs in the ranges the frame passes these functions."""
+    rng = np.random.default_rng(seed + sum(map(ord, name)))
+    u = lambda lo, hi, k=1: rng.uniform(lo, hi, size=(n, k))
+    sun = np.array([0.61237244, 0.5, 0.61237244])
+    if name == "hash_u32":
+        return rng.integers(0, 2**32, size=(n, 1), dtype=np.uint64).astype(np.uint32).view(np.float32)
+    if name in ("hash12", "value_noise", "fbm"):
+        x = u(-600, 600, 2)
+    elif name in ("hash31", "hash1"):
+        x = np.concatenate([np.floor(u(-200, 200, 3)), u(-200, 200, 3)])[:n]
+    elif name == "wind_field":
+        x = np.hstack([u(-100, 100), u(-2, 20), u(-100, 100), u(0, 120)])
+    elif name == "clamp_len":
+        x = np.hstack([u(-4, 4, 3), u(0.05, 3)])
+    elif name == "grass_wind_xz":
+        x = np.hstack([u(-100, 100), u(0, 12), u(-100, 100), u(0, 120), u(0, 3)])
+    elif name == "grass_blade_params":
+        ids = np.floor(u(-640, 640, 3)).astype(np.float32)
+        i = rng.integers(0, 5, size=(n, 1)).astype(np.uint32).view(np.float32)
+        return np.ascontiguousarray(np.hstack([ids, i]), np.float32)
+    elif name == "sdf_box":
+        x = np.hstack([u(-1, 1, 3), u(-0.5, 0.5, 3), u(0.01, 0.4, 3)])
+    elif name in ("phase_mie", "phase_blended"):
+        x = u(-1, 1)
+    elif name in ("sky_bg", "sky_color"):
+        x = _dirs(rng, n, 0.3)
+    elif name == "sky_sun":  # half of the rays near the sun disc
+        d = _dirs(rng, n)
+        near = sun + 0.02 * rng.normal(size=(n, 3))
+        d[: n // 2] = (near / np.linalg.norm(near, axis=1, keepdims=True))[: n // 2]
+        x = d
+    elif name in ("fog_color_from_sky", "fog_inscatter"):
+        x = np.hstack([_dirs(rng, n), u(0, 2, 3)])
+    elif name == "fog_optical_depth_with_base":
+        d = _dirs(rng, n)
+        d[: n // 8, 1] = rng.uniform(-5e-5, 5e-5, n // 8)  # the near-horizontal branch
+        x = np.hstack([u(-0.01, 0.05), u(-50, 50), u(0, 60), u(-50, 50), d, u(0, 120)])
+    elif name == "apply_fog":
+        x = np.hstack([u(0, 3, 3), u(-50, 50), u(0, 60), u(-50, 50), _dirs(rng, n), u(0, 120), u(0, 2, 3)])
+    elif name == "cloud_height01":
+        x = u(150, 270)
+    elif name == "cloud_coverage_at_xz":
+        x = np.hstack([u(-3000, 3000, 2), u(0, 200)])
+    elif name in ("cloud_density", "cloud_light_transmittance", "cloud_density_godray"):
+        x = np.hstack([u(-3000, 3000), u(160, 260), u(-3000, 3000), u(0, 200)])
+    elif name in ("cloud_sun_transmittance_fast", "cloud_sun_transmittance_godray"):
+        x = np.hstack([u(-3000, 3000), u(0, 300), u(-3000, 3000), _dirs(rng, n, 2.0)])
+    elif name == "tonemap_filmic_hable":
+        x = u(0, 20, 3)
+    elif name == "tonemap_filmic_white_scale":
+        x = np.hstack([u(0, 20, 3), u(1, 12)])
+    elif name == "bright_extract_hue":
+        x = np.hstack([u(0, 10, 3), u(0, 2)])
+    elif name == "intersect_aabb":  # boxes around and away from the origin, some axis-parallel rays
+        d = _dirs(rng, n)
+        d[: n // 8, 0] = 0.0
+        lo = u(-2, 2, 3)
+        x = np.hstack([u(-3, 3, 3), d, lo, lo + u(0.1, 2, 3)])
+    elif name == "safe_inv":
+        x = np.concatenate([u(-2, 2), u(-2e-8, 2e-8)])[:n]
+    elif name == "ray_eps_vec":
+        d = _dirs(rng, n)
+        d[: n // 8, 1] = 0.0
+        x = np.hstack([d, u(1e-5, 1e-2)])
+    elif name in ("macro_cell_size", "grass_lod_from_t", "godray_steps_for_tend"):
+        x = u(0, 130)
+    elif name == "hemi_ambient":
+        x = np.hstack([_dirs(rng, n), u(0, 2, 3)])
+    elif name in ("color_for_material", "material_roughness", "material_f0", "material_emission"):
+        return rng.integers(0, 8, size=(n, 1)).astype(np.uint32).view(np.float32)
+    elif name == "apply_material_variation":
+        m = rng.integers(0, 8, size=(n, 1)).astype(np.uint32).view(np.float32)
+        return np.ascontiguousarray(np.hstack([u(0, 1, 3).astype(np.float32), m, u(-60, 60, 3).astype(np.float32)]))
+    elif name == "grass_wind_dir_xz":
+        x = np.hstack([u(-100, 100), u(0, 12), u(-100, 100), u(0, 120)])
+    elif name == "grass_blade_slivers":
+        x = np.hstack([u(-60, 60, 3), u(0, 120), u(0.5, 40), u(0, 1)])
+    elif name == "grass_blade_field":
+        x = np.hstack([u(-60, 60, 3), u(0, 120), u(0, 60)])
+    elif name == "grass_top_albedo":
+        x = np.hstack([u(0, 1, 3), u(-60, 60, 3), u(0, 60)])
+    elif name == "base_albedo":
+        m = rng.integers(0, 8, size=(n, 1)).astype(np.uint32).view(np.float32)
+        return np.ascontiguousarray(np.hstack([m, u(-60, 60, 3).astype(np.float32), u(0, 120).astype(np.float32)]))
+    elif name in ("approx_pow_0p75", "approx_pow_0p55", "exp_neg_fast"):
+        x = u(-0.5, 3)
+    elif name in ("godray_decompress", "godray_compress"):
+        x = u(0, 4, 3)
+    elif name == "rot_about_axis":
+        x = np.hstack([u(-1, 1, 3), _dirs(rng, n), u(-7, 7)])
+    elif name == "sphere_dir_local":
+        cnt = rng.integers(1, 17, size=(n, 1))
+        i = rng.integers(0, 16, size=(n, 1)) % cnt
+        return np.ascontiguousarray(np.hstack([i, cnt]).astype(np.uint32).view(np.float32))
+    else:
+        raise KeyError(name)
+    return np.ascontiguousarray(x, np.float32)
+
+
+def _eval(lib, fn_name, name, x, out_w, extra=()):
+    fp = C.POINTER(C.c_float)
+    out = np.full((len(x), out_w), np.nan, np.float32)
+    rc = getattr(lib, fn_name)(name.encode(), x.ctypes.data_as(fp), out.ctypes.data_as(fp), len(x), *extra)
+    assert rc == 0, f"{fn_name} does not know {name}"
+    return out
+
+
+@pytest.mark.parametrize("name", FUNCS)
+def test_oracle_shading_equals_translated_reference_wgsl(name):
+    ref, ora = load_libs()
+    iw, ow = C.c_uint(), C.c_uint()
+    assert ref.ref_wgsl_widths(name.encode(), C.byref(iw), C.byref(ow)) == 0, f"{name} not translated"
+    x = gen_inputs(name, 4096)
+    assert x.shape[1] == iw.value
+    fp = C.POINTER(C.c_float)
+    want = _eval(ref, "ref_wgsl_eval", name, x, ow.value)
+    got = _eval(ora, "oracle_shading_eval", name, x, ow.value,
+                (CAM_POS.ctypes.data_as(fp), VOXEL_PARAMS.ctypes.data_as(fp)))
+    diff = np.flatnonzero((want.view(np.uint32) != got.view(np.uint32)).any(axis=1))
+    assert diff.size == 0, (f"{name}: {diff.size} of {len(x)} inputs differ, first input {x[diff[0]]}: "
+                            f"reference {want[diff[0]]}, oracle {got[diff[0]]}")

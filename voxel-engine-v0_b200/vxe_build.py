@@ -31,6 +31,12 @@ LIB_CHECKED = PKG / "vxe" / "libvxe_checked.so"
 ORACLE_SRC = REPO / "oracle" / "vxe_oracle.cpp"
 ORACLE_LIB = REPO / "oracle" / "liboracle_vxe.so"
 REF_PRODUCER_LIB = REPO / "oracle" / "libref_producer.so"
+# The reference's pure shading helpers, translated from its WGSL where it lies
+# (only in a checkout that has the reference; the GPU box does not) into a
+# git-ignored library that pins the oracle (tests/test_oracle_wgsl_pin.py).
+REF_SHADERS = Path("/root/reference/src/shaders")
+REF_WGSL_DIR = REPO / "oracle" / "_ref"
+REF_WGSL_LIB = REF_WGSL_DIR / "libref_wgsl.so"
 BUILD_DIR = PKG / "_build"
 
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
@@ -121,11 +127,30 @@ def build_ref_producer(verbose: bool = False, force: bool = False) -> Path:
     return REF_PRODUCER_LIB
 
 
+def build_ref_wgsl(verbose: bool = False, force: bool = False):
+    """oracle/_ref/libref_wgsl.so from the reference's WGSL (oracle/wgsl_to_cpp.py); None without the reference."""
+    if not REF_SHADERS.is_dir():
+        return None
+    translator = REPO / "oracle" / "wgsl_to_cpp.py"
+    shim = REPO / "oracle" / "wgsl_shim.h"
+    wgsl = sorted(REF_SHADERS.rglob("*.wgsl"))
+    deps = [translator, shim, INCLUDE / "vxe" / "detmath.h", *wgsl]
+    if not force and not _stale(REF_WGSL_LIB, deps):
+        return REF_WGSL_LIB
+    cpp = REF_WGSL_DIR / "ref_wgsl.cpp"
+    _run([sys.executable, translator, REF_SHADERS, cpp], verbose)
+    tmp = REF_WGSL_LIB.with_suffix(".so.tmp")
+    _run(["g++", *CXX_FLAGS, f"-I{REPO / 'oracle'}", "-shared", "-o", tmp, cpp], verbose)
+    os.replace(tmp, REF_WGSL_LIB)
+    return REF_WGSL_LIB
+
+
 def build_all(verbose: bool = False, force: bool = False) -> None:
     build_lib(verbose=verbose, force=force)
     build_lib(verbose=verbose, force=force, checked=True)
     build_oracle(verbose=verbose, force=force)
     build_ref_producer(verbose=verbose, force=force)
+    build_ref_wgsl(verbose=verbose, force=force)
 
 
 if __name__ == "__main__":
