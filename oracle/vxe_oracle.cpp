@@ -19,11 +19,11 @@
 //
 // Parity status: the reference is Rust + WGSL and cannot run whole here (no
 // Rust toolchain, no graphics stack), so this restatement is pinned only in
-// part against the reference itself: its pure shading helpers are compared
-// bit for bit with the reference's own WGSL translated to C++
-// (oracle/wgsl_to_cpp.py, oracle_shading_eval below,
-// tests/test_oracle_wgsl_pin.py); the traversal is checked against an
-// independent FP64 voxel DDA (tests/test_oracle_kat.py).
+// part against the reference itself: its pure shading helpers and its chunk
+// walk are compared bit for bit with the reference's own WGSL translated to
+// C++ (oracle/wgsl_to_cpp.py; oracle_shading_eval and ora_trace_chunk below;
+// tests/test_oracle_wgsl_pin.py), and the scene traversal is checked against
+// an independent FP64 voxel DDA (tests/test_oracle_kat.py).
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -3023,6 +3023,51 @@ void ora_debug_grass(int which, uint32_t n, const float* in, float* out) {
   }
 }
 
+
+// Pin interface (test infrastructure): one chunk walk,
+// trace_chunk_interval_stream_macro (chunk_trace.wgsl:592-667) with the
+// grass probes of the primary trace, per ray, in the slot layout of the
+// library oracle/wgsl_to_cpp.py builds from the reference's own WGSL:
+//   rays: n x 12 slots: ro (3), rd (3), t0, t1, slot (u32 bits),
+//         use_anchor (u32), anchor_key (u32), unused
+//   out:  n x 16 slots: hit (u32), mat (u32), t, n (3), root_bmin (3),
+//         root_size, node_base (u32), macro_base (u32), anchor_valid (u32),
+//         anchor_key (u32), two unused
+int ora_trace_chunk(const ora_scene* sc, const float* rays, float* out, uint32_t n) {
+  if (!sc) return 1;
+  Counters ctr;
+  const Scene s = make_scene(sc, &ctr, false);
+  const TraceOpts opt{false};
+  auto putu = [](float*& o, uint32_t x) { std::memcpy(o++, &x, 4); };
+  for (uint32_t k = 0; k < n; ++k) {
+    const float* p = rays + (size_t)k * 12;
+    float* o = out + (size_t)k * 16;
+    const v3 ro = V3(p[0], p[1], p[2]), rd = V3(p[3], p[4], p[5]);
+    uint32_t slot, use_anchor, key;
+    std::memcpy(&slot, p + 8, 4);
+    std::memcpy(&use_anchor, p + 9, 4);
+    std::memcpy(&key, p + 10, 4);
+    const ChunkTraceResult r =
+        trace_chunk_interval_stream_macro(s, ro, rd, safe_inv3(rd), chunk_at(s, slot), p[6], p[7], use_anchor != 0u, key, opt);
+    putu(o, r.hit.hit);
+    putu(o, r.hit.mat);
+    *o++ = r.hit.t;
+    *o++ = r.hit.n.x;
+    *o++ = r.hit.n.y;
+    *o++ = r.hit.n.z;
+    *o++ = r.hit.root_bmin.x;
+    *o++ = r.hit.root_bmin.y;
+    *o++ = r.hit.root_bmin.z;
+    *o++ = r.hit.root_size;
+    putu(o, r.hit.node_base);
+    putu(o, r.hit.macro_base);
+    putu(o, r.anchor_valid ? 1u : 0u);
+    putu(o, r.anchor_key);
+    *o++ = 0.0f;
+    *o++ = 0.0f;
+  }
+  return ctr.oob != 0 ? 2 : 0;
+}
 
 // Pin interface (test infrastructure): the oracle's restatements of the
 // reference's pure shading helpers behind the flat-slot calling convention of

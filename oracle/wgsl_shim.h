@@ -47,6 +47,44 @@ inline u32 wmax(u32 a, u32 b) { return a > b ? a : b; }
 inline i32 wmin(i32 a, i32 b) { return a < b ? a : b; }
 inline i32 wmax(i32 a, i32 b) { return a > b ? a : b; }
 
+// Conversions with WGSL semantics (float -> integer saturates, NaN -> 0).
+inline float wgsl_f32(float x) { return x; }
+inline float wgsl_f32(u32 x) { return (float)x; }
+inline float wgsl_f32(i32 x) { return (float)x; }
+inline float wgsl_f32(bool x) { return x ? 1.0f : 0.0f; }
+inline u32 wgsl_u32(float f) {
+  if (f != f || f <= 0.0f) return 0u;
+  if (f >= 4294967296.0f) return 0xFFFFFFFFu;
+  return (u32)f;
+}
+inline u32 wgsl_u32(u32 x) { return x; }
+inline u32 wgsl_u32(i32 x) { return (u32)x; }
+inline u32 wgsl_u32(bool x) { return x ? 1u : 0u; }
+inline i32 wgsl_i32(float f) {
+  if (f != f) return 0;
+  if (f >= 2147483648.0f) return INT32_MAX;
+  if (f <= -2147483648.0f) return INT32_MIN;
+  return (i32)f;
+}
+inline i32 wgsl_i32(i32 x) { return x; }
+inline i32 wgsl_i32(u32 x) { return (i32)x; }
+template <class T>
+inline T wgsl_conv(float x) {
+  if constexpr (std::is_same_v<T, float>) return x;
+  else if constexpr (std::is_same_v<T, u32>) return wgsl_u32(x);
+  else return wgsl_i32(x);
+}
+template <class T>
+inline T wgsl_conv(u32 x) {
+  if constexpr (std::is_same_v<T, float>) return (float)x;
+  else return (T)x;
+}
+template <class T>
+inline T wgsl_conv(i32 x) {
+  if constexpr (std::is_same_v<T, float>) return (float)x;
+  else return (T)x;
+}
+
 template <class T, int N>
 struct vec {
   T v[N];
@@ -60,6 +98,8 @@ struct vec<T, 2> {
   vec() : x(), y() {}
   explicit vec(T s) : x(s), y(s) {}
   vec(T a, T b) : x(a), y(b) {}
+  template <class U>
+  explicit vec(const vec<U, 2>& o) : x(wgsl_conv<T>(o.x)), y(wgsl_conv<T>(o.y)) {}
   T& operator[](int i) { return i == 0 ? x : y; }
   const T& operator[](int i) const { return i == 0 ? x : y; }
 };
@@ -72,6 +112,8 @@ struct vec<T, 3> {
   vec(T a, T b, T c) : x(a), y(b), z(c) {}
   vec(vec<T, 2> a, T c) : x(a.x), y(a.y), z(c) {}
   vec(T a, vec<T, 2> b) : x(a), y(b.x), z(b.y) {}
+  template <class U>
+  explicit vec(const vec<U, 3>& o) : x(wgsl_conv<T>(o.x)), y(wgsl_conv<T>(o.y)), z(wgsl_conv<T>(o.z)) {}
   vec<T, 2> xy() const { return {x, y}; }
   vec<T, 2> xz() const { return {x, z}; }
   vec<T, 3> xyz() const { return *this; }
@@ -88,6 +130,9 @@ struct vec<T, 4> {
   vec(vec<T, 3> a, T d) : x(a.x), y(a.y), z(a.z), w(d) {}
   vec(vec<T, 2> a, T c, T d) : x(a.x), y(a.y), z(c), w(d) {}
   vec(vec<T, 2> a, vec<T, 2> b) : x(a.x), y(a.y), z(b.x), w(b.y) {}
+  template <class U>
+  explicit vec(const vec<U, 4>& o)
+      : x(wgsl_conv<T>(o.x)), y(wgsl_conv<T>(o.y)), z(wgsl_conv<T>(o.z)), w(wgsl_conv<T>(o.w)) {}
   vec<T, 2> xy() const { return {x, y}; }
   vec<T, 2> xz() const { return {x, z}; }
   vec<T, 3> xyz() const { return {x, y, z}; }
@@ -152,6 +197,35 @@ struct mat2x2f {
   mat2x2f(float a, float b, float c, float d) : c0(a, b), c1(c, d) {}
 };
 inline vec2f operator*(const mat2x2f& m, const vec2f& v) { return m.c0 * v.x + m.c1 * v.y; }
+
+// mat3x3<f32>: three columns; m * v sums column by column.
+struct mat3x3f {
+  vec3f c[3];
+  mat3x3f() = default;
+  mat3x3f(vec3f a, vec3f b, vec3f d) : c{a, b, d} {}
+  vec3f& operator[](int i) { return c[i]; }
+  const vec3f& operator[](int i) const { return c[i]; }
+};
+inline vec3f operator*(const mat3x3f& m, const vec3f& v) { return m.c[0] * v.x + m.c[1] * v.y + m.c[2] * v.z; }
+
+// mat4x4<f32>: four columns, laid out as the uniform buffer holds them.
+struct mat4x4f {
+  vec4f c[4];
+};
+inline vec4f operator*(const mat4x4f& m, const vec4f& v) {
+  return m.c[0] * v.x + m.c[1] * v.y + m.c[2] * v.z + m.c[3] * v.w;
+}
+
+// A read-only storage buffer (array<T>): an index past the end reads a zero
+// record, as the oracle's checked reads do.
+template <class T>
+struct Buf {
+  const T* p = nullptr;
+  uint64_t n = 0;
+  T operator[](uint64_t i) const { return i < n ? p[i] : T{}; }
+  T operator[](int32_t i) const { return i >= 0 ? (*this)[(uint64_t)i] : T{}; }
+  T operator[](uint32_t i) const { return (*this)[(uint64_t)i]; }
+};
 
 template <class T, int N>
 inline vec<T, N> operator-(const vec<T, N>& a) {
@@ -278,33 +352,27 @@ inline T wgsl_select(T f, T t, bool c) {
   return c ? t : f;
 }
 
-// Conversions with WGSL semantics (float -> integer saturates, NaN -> 0).
-inline float wgsl_f32(float x) { return x; }
-inline float wgsl_f32(u32 x) { return (float)x; }
-inline float wgsl_f32(i32 x) { return (float)x; }
-inline float wgsl_f32(bool x) { return x ? 1.0f : 0.0f; }
-inline u32 wgsl_u32(float f) {
-  if (f != f || f <= 0.0f) return 0u;
-  if (f >= 4294967296.0f) return 0xFFFFFFFFu;
-  return (u32)f;
-}
-inline u32 wgsl_u32(u32 x) { return x; }
-inline u32 wgsl_u32(i32 x) { return (u32)x; }
-inline u32 wgsl_u32(bool x) { return x ? 1u : 0u; }
-inline i32 wgsl_i32(float f) {
-  if (f != f) return 0;
-  if (f >= 2147483648.0f) return INT32_MAX;
-  if (f <= -2147483648.0f) return INT32_MIN;
-  return (i32)f;
-}
-inline i32 wgsl_i32(i32 x) { return x; }
-inline i32 wgsl_i32(u32 x) { return (i32)x; }
+inline u32 countOneBits(u32 x) { return (u32)__builtin_popcount(x); }
+inline u32 countLeadingZeros(u32 x) { return x == 0u ? 32u : (u32)__builtin_clz(x); }
+inline u32 countTrailingZeros(u32 x) { return x == 0u ? 32u : (u32)__builtin_ctz(x); }
+inline u32 firstLeadingBit(u32 x) { return x == 0u ? 0xFFFFFFFFu : 31u - (u32)__builtin_clz(x); }
 inline u32 bitcast_u32(float f) {
   u32 u;
   std::memcpy(&u, &f, 4);
   return u;
 }
 inline u32 bitcast_u32(i32 i) { return (u32)i; }
+inline i32 bitcast_i32(u32 u) { return (i32)u; }
+inline i32 bitcast_i32(float f) {
+  i32 i;
+  std::memcpy(&i, &f, 4);
+  return i;
+}
+inline float bitcast_f32(i32 i) {
+  float f;
+  std::memcpy(&f, &i, 4);
+  return f;
+}
 inline float bitcast_f32(u32 u) {
   float f;
   std::memcpy(&f, &u, 4);

@@ -1,23 +1,32 @@
-"""Translates pure helper functions of the reference's WGSL into C++ (test
+"""Translates the reference's WGSL shader functions into C++ (test
 infrastructure for pinning the oracle; never part of the product).
 
 The reference is Rust + WGSL: its shaders cannot run here (no graphics stack)
-and its host cannot be built (no Rust toolchain).  Its pure shading helpers
-(sky, sun, clouds, fog, phase, tonemap, wind, hashes, value noise) are plain
-arithmetic, though, and WGSL's syntax for them is close to C++.  This script
-rewrites them mechanically, at build time, from the shader sources where they
-lie, into oracle/_ref/ref_wgsl.cpp over oracle/wgsl_shim.h (vector types and
-builtins with WGSL semantics), and compiles that into oracle/_ref/libref_wgsl.so.
-Nothing of the reference is committed: oracle/_ref is git-ignored.
+and its host cannot be built (no Rust toolchain).  Most of its shader code is
+plain f32 / u32 arithmetic over structs and read-only storage buffers, though,
+and WGSL's syntax for it is close to C++.  This script rewrites the functions
+in EXPORTS, with their whole call closure, mechanically and at build time from
+the shader sources where they lie, into oracle/_ref/ref_wgsl.cpp over
+oracle/wgsl_shim.h (vector and matrix types, builtins with WGSL semantics,
+storage buffers that read zero past their end), and compiles that into
+oracle/_ref/libref_wgsl.so.  Nothing of the reference is committed:
+oracle/_ref is git-ignored.  The rewrite is textual: declarations (let / var /
+const), types, struct definitions and constructors (brace initialisation),
+function pointers (`ptr<function, T>` -> `T*`), conversions, swizzles (.xy
+.xz .xyz), f32 literals, and the scene bindings as globals.
 
 The library exports
     int ref_wgsl_eval(const char* name, const float* in, float* out, unsigned n)
     int ref_wgsl_widths(const char* name, unsigned* in_w, unsigned* out_w)
     void ref_wgsl_set_cam(const float* cam_pos4, const float* voxel_params4)
-over the exported functions: parameters and results are flattened into float
-slots (vecN = N slots; u32 / i32 / bool pass their bit patterns), n calls in a
-row.  The oracle exports the same interface over its own restatements
-(oracle_shading_eval), so a test compares the two function by function.
+over the exported functions with scalar and vector parameters: parameters
+and results are flattened into float slots (vecN = N slots; u32 / i32 / bool
+pass their bit patterns), n calls in a row; and, for the chunk walk,
+    void ref_wgsl_set_scene(...)   (the world's host arrays and camera fields)
+    int ref_wgsl_trace_chunk(const float* rays, float* out, unsigned n)
+The oracle exports the same interfaces over its own restatements
+(oracle_shading_eval, ora_trace_chunk), so a test compares the two function
+by function.
 
 Usage: python oracle/wgsl_to_cpp.py <reference shader dir> <out .cpp>
 """
@@ -28,7 +37,8 @@ import sys
 from pathlib import Path
 
 FILES = ["common.wgsl", "ray/wind.wgsl", "ray/phase.wgsl", "ray/fog.wgsl", "ray/clouds.wgsl", "ray/sky.wgsl",
-         "ray/composite.wgsl", "ray/grass.wgsl", "ray/shading.wgsl", "ray/godrays.wgsl", "ray/light.wgsl"]
+         "ray/composite.wgsl", "ray/grass.wgsl", "ray/shading.wgsl", "ray/godrays.wgsl", "ray/light.wgsl",
+         "ray/aabb.wgsl", "ray/svo_query.wgsl", "ray/leaves.wgsl", "clipmap.wgsl", "ray/chunk_trace.wgsl"]
 
 # The functions the pin compares (each with its whole call closure).
 EXPORTS = ["hash_u32", "hash12", "hash31", "value_noise", "fbm", "hash1", "wind_field", "clamp_len",
@@ -42,7 +52,65 @@ EXPORTS = ["hash_u32", "hash12", "hash31", "value_noise", "fbm", "hash1", "wind_
            "apply_material_variation", "grass_wind_dir_xz", "grass_blade_slivers", "grass_blade_field",
            "grass_top_albedo", "base_albedo", "material_roughness", "material_f0", "material_emission",
            "approx_pow_0p75", "approx_pow_0p55", "exp_neg_fast", "godray_steps_for_tend", "godray_decompress",
-           "godray_compress", "rot_about_axis", "sphere_dir_local"]
+           "godray_compress", "rot_about_axis", "sphere_dir_local", "trace_chunk_interval_stream_macro"]
+
+# The chunk walk (chunk_trace.wgsl, trace_chunk_interval_stream_macro) over a
+# world the caller holds in host memory, in the layouts of include/vxe/vxe.h
+# (which are the shader's structs byte for byte).
+#   rays: n x 12 slots: ro (3), rd (3), t0, t1, slot (u32), use_anchor (u32),
+#         anchor_key (u32), unused
+#   out:  n x 16 slots: hit (u32), mat (u32), t, n (3), root_bmin (3),
+#         root_size, node_base (u32), macro_base (u32), anchor_valid (u32),
+#         anchor_key (u32), two unused
+CHUNK_WALK_EXPORT = r"""
+static_assert(sizeof(Node) == 16 && sizeof(NodeRopes) == 32 && sizeof(ChunkMeta) == 48, "buffer layouts");
+extern "C" void ref_wgsl_set_scene(const void* chunk_metas, uint64_t chunks_n, const void* node_recs, uint64_t nodes_n,
+                                   const uint32_t* grid, uint64_t grid_n, const uint32_t* macro_words,
+                                   uint64_t macro_n, const void* rope_recs, uint64_t ropes_n,
+                                   const uint32_t* colinfo_words, uint64_t colinfo_n, const float* cam_pos4,
+                                   const float* voxel_params4, uint32_t chunk_size, uint32_t chunk_count,
+                                   const int32_t* grid_origin4, const uint32_t* grid_dims4) {
+  wgsl::chunks = Buf<ChunkMeta>{(const ChunkMeta*)chunk_metas, chunks_n};
+  wgsl::nodes = Buf<Node>{(const Node*)node_recs, nodes_n};
+  wgsl::chunk_grid = Buf<uint32_t>{grid, grid_n};
+  wgsl::macro_occ = Buf<uint32_t>{macro_words, macro_n};
+  wgsl::node_ropes = Buf<NodeRopes>{(const NodeRopes*)rope_recs, ropes_n};
+  wgsl::chunk_colinfo = Buf<uint32_t>{colinfo_words, colinfo_n};
+  for (int i = 0; i < 4; ++i) {
+    cam.cam_pos[i] = cam_pos4[i];
+    cam.voxel_params[i] = voxel_params4[i];
+    cam.grid_origin_chunk[i] = grid_origin4[i];
+    cam.grid_dims[i] = grid_dims4[i];
+  }
+  cam.chunk_size = chunk_size;
+  cam.chunk_count = chunk_count;
+}
+extern "C" int ref_wgsl_trace_chunk(const float* rays, float* out, unsigned n) {
+  for (unsigned k = 0; k < n; ++k) {
+    const float* p = rays + (size_t)k * 12;
+    float* o = out + (size_t)k * 16;
+    const vec3f ro = get_v<3>(p), rd = get_v<3>(p);
+    const float t0 = get_f(p), t1 = get_f(p);
+    const uint32_t slot = get_slot<uint32_t>(p), use_anchor = get_slot<uint32_t>(p), key = get_slot<uint32_t>(p);
+    const vec3f inv = vec3f(safe_inv(rd.x), safe_inv(rd.y), safe_inv(rd.z));
+    const ChunkTraceResult r = trace_chunk_interval_stream_macro(ro, rd, inv, wgsl::chunks[slot], t0, t1,
+                                                                 use_anchor != 0u, key, 0u);
+    put(o, r.hit.hit);
+    put(o, r.hit.mat);
+    put(o, r.hit.t);
+    put(o, r.hit.n);
+    put(o, r.hit.root_bmin);
+    put(o, r.hit.root_size);
+    put(o, r.hit.node_base);
+    put(o, r.hit.macro_base);
+    put(o, (uint32_t)(r.anchor_valid ? 1u : 0u));
+    put(o, r.anchor_key);
+    put(o, 0.0f);
+    put(o, 0.0f);
+  }
+  return 0;
+}
+"""
 
 TYPE_MAP = {"f32": "float", "u32": "uint32_t", "i32": "int32_t", "bool": "bool"}
 WIDTH = {"float": 1, "uint32_t": 1, "int32_t": 1, "bool": 1, "vec2f": 2, "vec3f": 3, "vec4f": 4}
@@ -72,6 +140,11 @@ def conv_type(t: str) -> str:
     t = re.sub(r"\bvec([234])<i32>", r"vec\1i", t)
     t = re.sub(r"\bvec([234])<u32>", r"vec\1u", t)
     t = re.sub(r"\bmat2x2<f32>", "mat2x2f", t)
+    t = re.sub(r"\bmat4x4<f32>", "mat4x4f", t)
+    t = re.sub(r"\bmat3x3<f32>", "mat3x3f", t)
+    pm = re.match(r"ptr<\s*function\s*,\s*(.+)>$", t)
+    if pm:
+        return conv_type(pm.group(1)) + "*"
     t = re.sub(r"\barray<\s*([^,>]+)\s*,\s*([^>]+)>", lambda m: f"std::array<{conv_type(m.group(1))}, {m.group(2).strip()}>", t)
     return TYPE_MAP.get(t, t)
 
@@ -82,6 +155,8 @@ def conv_expr(s: str) -> str:
     s = re.sub(r"\bvec([234])<i32>", r"vec\1i", s)
     s = re.sub(r"\bvec([234])<u32>", r"vec\1u", s)
     s = re.sub(r"\bmat2x2<f32>", "mat2x2f", s)
+    s = re.sub(r"\bmat3x3<f32>", "mat3x3f", s)
+    s = re.sub(r"\bmat4x4<f32>", "mat4x4f", s)
     s = re.sub(r"\bbitcast<u32>\s*\(", "bitcast_u32(", s)
     s = re.sub(r"\bbitcast<f32>\s*\(", "bitcast_f32(", s)
     s = re.sub(r"\bbitcast<i32>\s*\(", "bitcast_i32(", s)
@@ -111,8 +186,48 @@ def conv_expr(s: str) -> str:
     return s
 
 
+def split_top(text: str, sep: str = ","):
+    """Splits on `sep` outside <> and ()."""
+    parts, depth, cur = [], 0, ""
+    for ch in text:
+        if ch in "<(":
+            depth += 1
+        elif ch in ">)":
+            depth -= 1
+        if ch == sep and depth == 0:
+            parts.append(cur)
+            cur = ""
+        else:
+            cur += ch
+    parts.append(cur)
+    return [q.strip() for q in parts if q.strip()]
+
+
+def brace_ctors(s: str, names) -> str:
+    """`S(a, b)` -> `S{a, b}` for every struct name S."""
+    if not names:
+        return s
+    pat = re.compile(r"\b(" + "|".join(sorted(names, key=len, reverse=True)) + r")\s*\(")
+    pos = 0
+    while True:
+        m = pat.search(s, pos)
+        if not m:
+            return s
+        open_i = m.end() - 1
+        depth = 0
+        for j in range(open_i, len(s)):
+            if s[j] == "(":
+                depth += 1
+            elif s[j] == ")":
+                depth -= 1
+                if depth == 0:
+                    break
+        s = s[:open_i] + "{" + s[open_i + 1:j] + "}" + s[j + 1:]
+        pos = open_i + 1
+
+
 def parse(shader_dir: Path):
-    consts, fns = [], {}
+    consts, fns, structs, bindings = [], {}, [], []
     for rel in FILES:
         src = strip_comments((shader_dir / rel).read_text())
         i = 0
@@ -134,13 +249,29 @@ def parse(shader_dir: Path):
                 fns[fm.group(1)] = (fm.group(2), fm.group(3), src[fm.end():end - 1], rel)
                 i = end
             elif kind == "struct":
-                sm = re.compile(r"\s*struct\s+\w+\s*\{").match(src, i)
-                i = match_brace(src, sm.end() - 1)
+                sm = re.compile(r"\s*struct\s+(\w+)\s*\{").match(src, i)
+                end = match_brace(src, sm.end() - 1)
+                fields = []
+                for fdecl in split_top(src[sm.end():end - 1]):
+                    fname, fty = fdecl.split(":", 1)
+                    fields.append((re.sub(r"@\w+(\([^)]*\))?", "", fname).strip(), fty.strip()))
+                structs.append((sm.group(1), fields))
+                i = end
+            elif kind == "@":
+                bm = re.compile(r"\s*@group\(\d+\)\s*@binding\(\d+\)\s*var(<[^>]*>)?\s+(\w+)\s*:\s*([^;]+);",
+                                re.S).match(src, i)
+                if bm:
+                    bindings.append((bm.group(1) or "", bm.group(2), bm.group(3).strip()))
+                    i = bm.end()
+                    continue
+                end = src.find(";", m.end())
+                brace = src.find("{", m.end())
+                i = (end + 1) if end >= 0 and (brace < 0 or end < brace) else (match_brace(src, brace) if brace >= 0 else len(src))
             else:
                 end = src.find(";", m.end())
                 brace = src.find("{", m.end())
                 i = (end + 1) if end >= 0 and (brace < 0 or end < brace) else (match_brace(src, brace) if brace >= 0 else len(src))
-    return consts, fns
+    return consts, fns, structs, bindings
 
 
 def closure(fns, roots):
@@ -158,21 +289,31 @@ def closure(fns, roots):
 
 def params_of(ptext: str):
     ps = []
-    for p in [p.strip() for p in ptext.split(",") if p.strip()]:
+    for p in split_top(ptext):
         name, ty = p.split(":", 1)
         ps.append((name.strip(), conv_type(ty)))
     return ps
 
 
 def main(shader_dir: Path, out: Path) -> None:
-    consts, fns = parse(shader_dir)
+    consts, fns, structs, bindings = parse(shader_dir)
     names = closure(fns, EXPORTS)
+    snames = [n for n, _ in structs]
     lines = ["// Generated by oracle/wgsl_to_cpp.py from the reference's WGSL; not committed.",
-             '#include "wgsl_shim.h"', "#include <cstring>", "namespace wgsl {",
-             "struct CamShim { vec4f cam_pos; vec4f voxel_params; };", "static CamShim cam;"]
+             '#include "wgsl_shim.h"', "#include <cstring>", "namespace wgsl {"]
     for name, ty, expr in consts:
         ty_c = conv_type(ty) if ty else "auto"
-        lines.append(f"static const {ty_c} {name} = {conv_expr(expr.strip())};")
+        lines.append(f"static const {ty_c} {name} = {brace_ctors(conv_expr(expr.strip()), snames)};")
+    for sname, fields in structs:  # the shader's structs, member for member
+        if any("atomic" in t or "texture" in t for _, t in fields):
+            continue
+        lines.append(f"struct {sname} {{ " + " ".join(f"{conv_type(t)} {f};" for f, t in fields) + " };")
+    for space, bname, bty in bindings:  # storage buffers and the uniform
+        m = re.match(r"array<\s*(\w+)\s*>$", bty)
+        if "storage" in space and m:
+            lines.append(f"static Buf<{conv_type(m.group(1))}> {bname};")
+        elif "uniform" in space:
+            lines.append(f"static {conv_type(bty)} {bname}{{}};")
     sigs = {}
     for f in names:
         ptext, ret, body, rel = fns[f]
@@ -184,7 +325,7 @@ def main(shader_dir: Path, out: Path) -> None:
         ptext, ret, body, rel = fns[f]
         ps, rt = sigs[f]
         lines.append(f"// {rel}")
-        lines.append(f"{rt} {f}({', '.join(f'{t} {n}' for n, t in ps)}) {{{conv_expr(body)}}}")
+        lines.append(f"{rt} {f}({', '.join(f'{t} {n}' for n, t in ps)}) {{{brace_ctors(conv_expr(body), snames)}}}")
     lines.append("}  // namespace wgsl")
     # the flat-slot dispatcher
     lines += ["using namespace wgsl;",
@@ -228,6 +369,8 @@ def main(shader_dir: Path, out: Path) -> None:
         call = f"{f}({', '.join(f'a{i}' for i in range(len(args)))})"
         lines.append(f'    if (!std::strcmp(name, "{f}")) {{ {decl}{";" if decl else ""} put(o, {call}); continue; }}')
     lines += ["  }", "  return 0;", "}"]
+    if "trace_chunk_interval_stream_macro" in sigs:
+        lines += CHUNK_WALK_EXPORT.splitlines()
     out.parent.mkdir(parents=True, exist_ok=True)
     out.write_text("\n".join(lines) + "\n")
 

@@ -1,12 +1,16 @@
-"""Pins the oracle's shading restatements to the reference's own WGSL.
+"""Pins the oracle to the reference's own WGSL.
 
-The reference's pure shading helpers (sky, sun, clouds, fog, phase, tonemap,
-wind, hashes, value noise) are translated mechanically from its WGSL into C++
-at build time (oracle/wgsl_to_cpp.py -> oracle/_ref/libref_wgsl.so, over
-oracle/wgsl_shim.h).  The oracle restates the same functions by hand
-(oracle/vxe_oracle.cpp, oracle_shading_eval).  With the same elementary
-functions on both sides, every output must be identical bit for bit on
-seeded inputs: a difference is a mis-reading in the restatement.
+The reference's shader functions are translated mechanically from its WGSL
+into C++ at build time (oracle/wgsl_to_cpp.py -> oracle/_ref/libref_wgsl.so,
+over oracle/wgsl_shim.h): the pure shading helpers (sky, sun, clouds, fog,
+phase, tonemap, materials, wind, hashes, value noise, godray and light
+helpers) and the chunk walk of chunk_trace.wgsl with everything it calls
+(macro DDA, rope walk, leaf descent, anchors, grass column probes, blade
+marches, leaves), reading the world from the same host arrays as the
+oracle.  The oracle restates the same functions by hand
+(oracle/vxe_oracle.cpp: oracle_shading_eval, ora_trace_chunk).  With the
+same elementary functions on both sides, every output must be identical bit
+for bit on seeded inputs: a difference is a mis-reading in the restatement.
 
 The translated library is built only where the reference's sources are
 present; elsewhere these tests are skipped.
@@ -181,3 +185,99 @@ def test_oracle_shading_equals_translated_reference_wgsl(name):
     diff = np.flatnonzero((want.view(np.uint32) != got.view(np.uint32)).any(axis=1))
     assert diff.size == 0, (f"{name}: {diff.size} of {len(x)} inputs differ, first input {x[diff[0]]}: "
                             f"reference {want[diff[0]]}, oracle {got[diff[0]]}")
+
+
+def _walk_setup(scene_fn):
+    """A world of `scene_fn`, the oracle scene over it, and the translated
+    reference library bound to the same host arrays."""
+    from oracle import oracle as O
+    from vxe.scenes import FrameDriver
+
+    ref, _ = load_libs()
+    sc = scene_fn()
+    drv = FrameDriver(sc)
+    drv.initial_uploads()
+    w = drv.world
+    _, _, clip, cam = drv.step()
+    clip_params = clip[0] if clip is not None else drv.empty_clip()  # config 1 has no clipmap
+    runner = O.OracleFrameRunner(w, sc.internal, sc.present, drv.clip.tex if drv.clip is not None else None,
+                                 sc.clip_res)
+    ora_scene = runner.scene(cam, clip_params)
+    fp, u64 = C.POINTER(C.c_float), C.c_uint64
+    keep = dict(cp=np.array(cam.cam_pos[:], np.float32), vp=np.array(cam.voxel_params[:], np.float32),
+                go=np.array(cam.grid_origin_chunk[:], np.int32), gd=np.array(cam.grid_dims[:], np.uint32))
+    ref.ref_wgsl_set_scene(C.c_void_p(w.metas.ctypes.data), u64(w.metas.shape[0]), C.c_void_p(w.nodes.ctypes.data),
+                           u64(len(w.nodes)), C.c_void_p(w.grid.ctypes.data), u64(len(w.grid)),
+                           C.c_void_p(w.macro.ctypes.data), u64(len(w.macro)), C.c_void_p(w.ropes.ctypes.data),
+                           u64(len(w.ropes)), C.c_void_p(w.colinfo.ctypes.data), u64(len(w.colinfo)),
+                           keep["cp"].ctypes.data_as(fp), keep["vp"].ctypes.data_as(fp), C.c_uint32(cam.chunk_size),
+                           C.c_uint32(cam.chunk_count), keep["go"].ctypes.data_as(C.POINTER(C.c_int32)),
+                           keep["gd"].ctypes.data_as(C.POINTER(C.c_uint32)))
+    lo = O.lib()
+    lo.ora_trace_chunk.argtypes = [C.POINTER(O.OraScene), C.c_void_p, C.c_void_p, C.c_uint32]
+    return ref, lo, ora_scene, w, cam, (runner, keep, clip_params)
+
+
+def _walk_rays(w, cam, n, rng):
+    """Rays through random chunks: origins in and around the chunk, targets
+    inside it, [t0, t1] the chunk box interval from t >= 0."""
+    vs = float(cam.voxel_params[0])
+    cs = cam.chunk_size * vs
+    metas = w.metas.view(np.int32).reshape(-1, 12)
+    slots = rng.integers(0, cam.chunk_count, n)
+    org = metas[slots, :3].astype(np.float64) * vs
+    ro = org + rng.uniform(-0.5, 1.5, (n, 3)) * cs
+    rd = org + rng.uniform(0, 1, (n, 3)) * cs - ro
+    rd /= np.linalg.norm(rd, axis=1, keepdims=True)
+    ro, rd = ro.astype(np.float32), rd.astype(np.float32)
+    inv = 1.0 / np.where(np.abs(rd) < 1e-8, 1e-8, rd.astype(np.float64))
+    ta, tb = (org - ro) * inv, (org + cs - ro) * inv
+    te = np.maximum(np.minimum(ta, tb).max(1), 0.0)
+    tx = np.maximum(np.maximum(ta, tb).min(1), te)
+    rays = np.zeros((n, 12), np.float32)
+    rays[:, 0:3], rays[:, 3:6], rays[:, 6], rays[:, 7] = ro, rd, te, tx
+    rays[:, 8] = slots.astype(np.uint32).view(np.float32)
+    rays[:, 10] = np.full(n, 0xFFFFFFFF, np.uint32).view(np.float32)
+    return rays
+
+
+def _walk_both(ref, lo, ora_scene, rays):
+    fp = C.POINTER(C.c_float)
+    want = np.full((len(rays), 16), np.nan, np.float32)
+    got = np.full((len(rays), 16), np.nan, np.float32)
+    ref.ref_wgsl_trace_chunk(rays.ctypes.data_as(fp), want.ctypes.data_as(fp), len(rays))
+    assert lo.ora_trace_chunk(C.byref(ora_scene), rays.ctypes.data, got.ctypes.data, len(rays)) == 0
+    return want, got
+
+
+@pytest.mark.parametrize("scene", ["features", "config1"])
+def test_oracle_chunk_walk_equals_translated_reference_wgsl(scene):
+    """The chunk walk (chunk_trace.wgsl trace_chunk_interval_stream_macro:
+    macro DDA, rope walk, leaf descent, anchors, grass column probes and blade
+    marches) of the oracle against the reference's own WGSL translated to
+    C++, on random rays through every kind of chunk: hit, material, t,
+    normal, chunk root, anchor, bit for bit."""
+    from vxe import scenes
+
+    fn = {"features": lambda: scenes.features(present=(64, 40)), "config1": scenes.config1}[scene]
+    ref, lo, ora_scene, w, cam, _keep = _walk_setup(fn)
+    rng = np.random.default_rng(11)
+    rays = _walk_rays(w, cam, 20000, rng)
+    want, got = _walk_both(ref, lo, ora_scene, rays)
+    hits = want[:, 0].view(np.uint32) != 0
+    assert 0.2 < hits.mean() < 0.98
+    mats = set(want[hits, 1].view(np.uint32).tolist())
+    assert {1, 2, 3} <= mats  # grass, dirt and stone hits at least
+    diff = np.flatnonzero((want.view(np.uint32) != got.view(np.uint32)).any(axis=1))
+    assert diff.size == 0, f"{diff.size} of {len(rays)} walks differ, first ray {rays[diff[0], :8]}"
+    # the anchor path: the same rays again from half way along, seeded with
+    # the anchor the first walk returned
+    valid = want[:, 12].view(np.uint32) != 0
+    assert valid.mean() > 0.2
+    rays2 = rays.copy()
+    rays2[:, 6] = 0.5 * (rays[:, 6] + rays[:, 7])
+    rays2[:, 9] = valid.astype(np.uint32).view(np.float32)
+    rays2[:, 10] = want[:, 13]
+    want2, got2 = _walk_both(ref, lo, ora_scene, rays2)
+    diff = np.flatnonzero((want2.view(np.uint32) != got2.view(np.uint32)).any(axis=1))
+    assert diff.size == 0, f"{diff.size} anchored walks differ, first ray {rays2[diff[0], :11]}"
