@@ -21,7 +21,8 @@
 // Rust toolchain, no graphics stack), so this restatement is pinned only in
 // part against the reference itself: its pure shading helpers and its chunk
 // walk are compared bit for bit with the reference's own WGSL translated to
-// C++ (oracle/wgsl_to_cpp.py; oracle_shading_eval and ora_trace_chunk below;
+// C++ (oracle/wgsl_to_cpp.py; oracle_shading_eval, ora_scene_eval and
+// ora_trace_chunk below;
 // tests/test_oracle_wgsl_pin.py), and the scene traversal is checked against
 // an independent FP64 voxel DDA (tests/test_oracle_kat.py).
 #include <algorithm>
@@ -495,7 +496,7 @@ LeafQuery query_leaf_at(const Scene& s, v3 p, v3 root_bmin, float root_size, uin
   return LeafQuery{bmin, size, MAT_AIR};
 }
 
-LeafQuery query_leaf_world(const Scene& s, v3 p) {  // svo_query.wgsl:270-291
+LeafQuery query_leaf_world(const Scene& s, v3 p) {  // svo_query.wgsl:115-136
   const float vs = vs_(s);
   const float cs = (float)s.cam->chunk_size * vs;
   const i3 c = chunk_coord_from_pos(p, cs);
@@ -3023,6 +3024,41 @@ void ora_debug_grass(int which, uint32_t n, const float* in, float* out) {
   }
 }
 
+
+// Pin interface (test infrastructure): the oracle's restatements of the
+// reference's scene-reading helpers (sun shadow march, godray integral,
+// local-light gather, leaf query) over the world of `sc`, in the flat-slot
+// layout of oracle_shading_eval.  Returns -1 for a name it does not know.
+int ora_scene_eval(const ora_scene* sc, const char* name, const float* in, float* out, uint32_t n) {
+  if (!sc) return 1;
+  Counters ctr;
+  const Scene s = make_scene(sc, &ctr, false);
+  const std::string nm(name);
+  unsigned iw = 0;
+  if (nm == "sun_transmittance_geom_only") iw = 6;
+  else if (nm == "godray_integrate_1") iw = 9;
+  else if (nm == "gather_voxel_lights") iw = 12;
+  else if (nm == "query_leaf_world") iw = 3;
+  else return -1;
+  for (uint32_t k = 0; k < n; ++k) {
+    const float* a = in + (size_t)k * iw;
+    if (nm == "sun_transmittance_geom_only") {
+      out[k] = sun_transmittance_geom_only(s, V3(a[0], a[1], a[2]), V3(a[3], a[4], a[5]));
+    } else if (nm == "godray_integrate_1") {
+      const v3 r = godray_integrate_1(s, V3(a[0], a[1], a[2]), V3(a[3], a[4], a[5]), a[6], a[7], a[8]);
+      out[3 * k] = r.x, out[3 * k + 1] = r.y, out[3 * k + 2] = r.z;
+    } else if (nm == "gather_voxel_lights") {  // root_size, node_base and macro_base are not read
+      const v3 r = gather_voxel_lights(s, V3(a[0], a[1], a[2]), V3(a[3], a[4], a[5]), V3(a[6], a[7], a[8]));
+      out[3 * k] = r.x, out[3 * k + 1] = r.y, out[3 * k + 2] = r.z;
+    } else {
+      const LeafQuery q = query_leaf_world(s, V3(a[0], a[1], a[2]));
+      float* o = out + (size_t)k * 5;
+      o[0] = q.bmin.x, o[1] = q.bmin.y, o[2] = q.bmin.z, o[3] = q.size;
+      std::memcpy(o + 4, &q.mat, 4);
+    }
+  }
+  return ctr.oob != 0 ? 2 : 0;
+}
 
 // Pin interface (test infrastructure): one chunk walk,
 // trace_chunk_interval_stream_macro (chunk_trace.wgsl:592-667) with the

@@ -38,7 +38,8 @@ from pathlib import Path
 
 FILES = ["common.wgsl", "ray/wind.wgsl", "ray/phase.wgsl", "ray/fog.wgsl", "ray/clouds.wgsl", "ray/sky.wgsl",
          "ray/composite.wgsl", "ray/grass.wgsl", "ray/shading.wgsl", "ray/godrays.wgsl", "ray/light.wgsl",
-         "ray/aabb.wgsl", "ray/svo_query.wgsl", "ray/leaves.wgsl", "clipmap.wgsl", "ray/chunk_trace.wgsl"]
+         "ray/aabb.wgsl", "ray/svo_query.wgsl", "ray/leaves.wgsl", "clipmap.wgsl", "ray/chunk_trace.wgsl",
+         "ray/shadows.wgsl"]
 
 # The functions the pin compares (each with its whole call closure).
 EXPORTS = ["hash_u32", "hash12", "hash31", "value_noise", "fbm", "hash1", "wind_field", "clamp_len",
@@ -52,7 +53,8 @@ EXPORTS = ["hash_u32", "hash12", "hash31", "value_noise", "fbm", "hash1", "wind_
            "apply_material_variation", "grass_wind_dir_xz", "grass_blade_slivers", "grass_blade_field",
            "grass_top_albedo", "base_albedo", "material_roughness", "material_f0", "material_emission",
            "approx_pow_0p75", "approx_pow_0p55", "exp_neg_fast", "godray_steps_for_tend", "godray_decompress",
-           "godray_compress", "rot_about_axis", "sphere_dir_local", "trace_chunk_interval_stream_macro"]
+           "godray_compress", "rot_about_axis", "sphere_dir_local", "trace_chunk_interval_stream_macro",
+           "sun_transmittance_geom_only", "godray_integrate_1", "gather_voxel_lights", "query_leaf_world"]
 
 # The chunk walk (chunk_trace.wgsl, trace_chunk_interval_stream_macro) over a
 # world the caller holds in host memory, in the layouts of include/vxe/vxe.h
@@ -69,7 +71,7 @@ extern "C" void ref_wgsl_set_scene(const void* chunk_metas, uint64_t chunks_n, c
                                    uint64_t macro_n, const void* rope_recs, uint64_t ropes_n,
                                    const uint32_t* colinfo_words, uint64_t colinfo_n, const float* cam_pos4,
                                    const float* voxel_params4, uint32_t chunk_size, uint32_t chunk_count,
-                                   const int32_t* grid_origin4, const uint32_t* grid_dims4) {
+                                   const int32_t* grid_origin4, const uint32_t* grid_dims4, uint32_t frame_index) {
   wgsl::chunks = Buf<ChunkMeta>{(const ChunkMeta*)chunk_metas, chunks_n};
   wgsl::nodes = Buf<Node>{(const Node*)node_recs, nodes_n};
   wgsl::chunk_grid = Buf<uint32_t>{grid, grid_n};
@@ -84,6 +86,7 @@ extern "C" void ref_wgsl_set_scene(const void* chunk_metas, uint64_t chunks_n, c
   }
   cam.chunk_size = chunk_size;
   cam.chunk_count = chunk_count;
+  cam.frame_index = frame_index;
 }
 extern "C" int ref_wgsl_trace_chunk(const float* rays, float* out, unsigned n) {
   for (unsigned k = 0; k < n; ++k) {
@@ -111,6 +114,8 @@ extern "C" int ref_wgsl_trace_chunk(const float* rays, float* out, unsigned n) {
   return 0;
 }
 """
+
+STRUCT_PUTS = []  # (struct name, field names) of flat structs, filled by main()
 
 TYPE_MAP = {"f32": "float", "u32": "uint32_t", "i32": "int32_t", "bool": "bool"}
 WIDTH = {"float": 1, "uint32_t": 1, "int32_t": 1, "bool": 1, "vec2f": 2, "vec3f": 3, "vec4f": 4}
@@ -314,6 +319,11 @@ def main(shader_dir: Path, out: Path) -> None:
             lines.append(f"static Buf<{conv_type(m.group(1))}> {bname};")
         elif "uniform" in space:
             lines.append(f"static {conv_type(bty)} {bname}{{}};")
+    for sname, fields in structs:  # structs of flat fields can be results
+        ftys = [conv_type(t) for _, t in fields]
+        if fields and all(t in WIDTH for t in ftys) and not sname.startswith("_"):
+            WIDTH[sname] = sum(WIDTH[t] for t in ftys)
+            STRUCT_PUTS.append((sname, [f for f, _ in fields]))
     sigs = {}
     for f in names:
         ptext, ret, body, rel = fns[f]
@@ -336,6 +346,8 @@ def main(shader_dir: Path, out: Path) -> None:
               "static void put(float*& o, uint32_t v) { std::memcpy(o++, &v, 4); }",
               "static void put(float*& o, int32_t v) { std::memcpy(o++, &v, 4); }",
               "template <int N> static void put(float*& o, const vec<float, N>& v) { for (int i = 0; i < N; ++i) *o++ = v[i]; }",
+              *[f"static void put_struct(float*& o, const {n}& v) {{ " + " ".join(f"put(o, v.{f});" for f in fs) + " }"
+                for n, fs in STRUCT_PUTS],
               'extern "C" void ref_wgsl_set_cam(const float* p, const float* vp) { for (int i = 0; i < 4; ++i) { cam.cam_pos[i] = p[i]; cam.voxel_params[i] = vp[i]; } }',
               'extern "C" int ref_wgsl_widths(const char* name, unsigned* in_w, unsigned* out_w) {']
     table = []
@@ -367,7 +379,8 @@ def main(shader_dir: Path, out: Path) -> None:
         # arguments are read in order into locals first (evaluation order)
         decl = "; ".join(f"const auto a{i} = {a}" for i, a in enumerate(args))
         call = f"{f}({', '.join(f'a{i}' for i in range(len(args)))})"
-        lines.append(f'    if (!std::strcmp(name, "{f}")) {{ {decl}{";" if decl else ""} put(o, {call}); continue; }}')
+        putter = "put_struct" if rt in dict(STRUCT_PUTS) else "put"
+        lines.append(f'    if (!std::strcmp(name, "{f}")) {{ {decl}{";" if decl else ""} {putter}(o, {call}); continue; }}')
     lines += ["  }", "  return 0;", "}"]
     if "trace_chunk_interval_stream_macro" in sigs:
         lines += CHUNK_WALK_EXPORT.splitlines()

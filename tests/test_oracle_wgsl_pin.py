@@ -6,9 +6,11 @@ over oracle/wgsl_shim.h): the pure shading helpers (sky, sun, clouds, fog,
 phase, tonemap, materials, wind, hashes, value noise, godray and light
 helpers) and the chunk walk of chunk_trace.wgsl with everything it calls
 (macro DDA, rope walk, leaf descent, anchors, grass column probes, blade
-marches, leaves), reading the world from the same host arrays as the
-oracle.  The oracle restates the same functions by hand
-(oracle/vxe_oracle.cpp: oracle_shading_eval, ora_trace_chunk).  With the
+marches, leaves) and the helpers that read the world (sun shadow march,
+godray integral, local-light gather, leaf query), reading the world from the
+same host arrays as the oracle.  The oracle restates the same functions by
+hand (oracle/vxe_oracle.cpp: oracle_shading_eval, ora_scene_eval,
+ora_trace_chunk).  With the
 same elementary functions on both sides, every output must be identical bit
 for bit on seeded inputs: a difference is a mis-reading in the restatement.
 
@@ -212,7 +214,7 @@ def _walk_setup(scene_fn):
                            u64(len(w.ropes)), C.c_void_p(w.colinfo.ctypes.data), u64(len(w.colinfo)),
                            keep["cp"].ctypes.data_as(fp), keep["vp"].ctypes.data_as(fp), C.c_uint32(cam.chunk_size),
                            C.c_uint32(cam.chunk_count), keep["go"].ctypes.data_as(C.POINTER(C.c_int32)),
-                           keep["gd"].ctypes.data_as(C.POINTER(C.c_uint32)))
+                           keep["gd"].ctypes.data_as(C.POINTER(C.c_uint32)), C.c_uint32(cam.frame_index))
     lo = O.lib()
     lo.ora_trace_chunk.argtypes = [C.POINTER(O.OraScene), C.c_void_p, C.c_void_p, C.c_uint32]
     return ref, lo, ora_scene, w, cam, (runner, keep, clip_params)
@@ -281,3 +283,60 @@ def test_oracle_chunk_walk_equals_translated_reference_wgsl(scene):
     want2, got2 = _walk_both(ref, lo, ora_scene, rays2)
     diff = np.flatnonzero((want2.view(np.uint32) != got2.view(np.uint32)).any(axis=1))
     assert diff.size == 0, f"{diff.size} anchored walks differ, first ray {rays2[diff[0], :11]}"
+
+
+def test_oracle_scene_helpers_equal_translated_reference_wgsl():
+    """The helpers that read the world, on the features world (caves, trees,
+    light voxels, grass): the sun shadow march (shadows.wgsl
+    sun_transmittance_geom_only), the godray in-scatter integral (godrays.wgsl
+    godray_integrate_1, with its cloud and shadow samples), the local-light
+    gather (light.wgsl gather_voxel_lights, its DDA to light voxels) and the
+    leaf query (svo_query.wgsl query_leaf_world), bit for bit."""
+    from vxe import scenes
+
+    ref, lo, ora_scene, w, cam, _keep = _walk_setup(lambda: scenes.features(present=(64, 40)))
+    lo.ora_scene_eval.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_uint32]
+    rng = np.random.default_rng(5)
+    rays = _walk_rays(w, cam, 20000, rng)
+    walk, _ = _walk_both(ref, lo, ora_scene, rays)
+    hit = walk[:, 0].view(np.uint32) != 0
+    hp = (rays[hit, :3] + rays[hit, 3:6] * walk[hit, 2:3]).astype(np.float32)
+    nrm, rb = walk[hit, 3:6], walk[hit, 6:9]
+    mats = walk[hit, 1].view(np.uint32)
+    lights = hp[mats == 6]
+    assert len(lights) > 0
+    # half of the gather points are the surface points nearest a light voxel
+    d = np.min(np.linalg.norm(hp[:, None, :] - lights[None, :64, :], axis=2), axis=1)
+    near = np.argsort(d)[:3000]
+    pick = np.concatenate([near, rng.choice(len(hp), 3000, replace=False)])
+    vs = float(cam.voxel_params[0])
+    cs = cam.chunk_size * vs
+    metas = w.metas.view(np.int32).reshape(-1, 12)[: cam.chunk_count]
+    lo3, hi3 = metas[:, :3].min(0) * vs, metas[:, :3].max(0) * vs + cs
+    sun = np.array([0.61237244, 0.5, 0.61237244], np.float32)
+    n = 6000
+    cases = {
+        "sun_transmittance_geom_only": np.hstack([np.vstack([hp[pick[:3000]] + nrm[pick[:3000]] * 0.01,
+                                                              rng.uniform(lo3, hi3, (3000, 3))]), np.tile(sun, (n, 1))]),
+        "godray_integrate_1": np.hstack([np.tile(np.array(cam.cam_pos[:3]), (n, 1)), _dirs(rng, n, 0.2),
+                                         rng.uniform(0, 100, (n, 1)), rng.uniform(0, 1, (n, 2))]),
+        "gather_voxel_lights": np.hstack([hp[pick], nrm[pick], rb[pick], np.zeros((n, 3))]),
+        "query_leaf_world": rng.uniform(lo3, hi3, (n, 3)),
+    }
+    fp = C.POINTER(C.c_float)
+    lit = 0
+    for name, x in cases.items():
+        x = np.ascontiguousarray(x, np.float32)
+        iw, ow = C.c_uint(), C.c_uint()
+        assert ref.ref_wgsl_widths(name.encode(), C.byref(iw), C.byref(ow)) == 0, name
+        assert x.shape[1] == iw.value
+        want = np.full((n, ow.value), np.nan, np.float32)
+        got = np.full((n, ow.value), np.nan, np.float32)
+        ref.ref_wgsl_eval(name.encode(), x.ctypes.data_as(fp), want.ctypes.data_as(fp), n)
+        assert lo.ora_scene_eval(C.addressof(ora_scene), name.encode(), x.ctypes.data, got.ctypes.data, n) == 0
+        diff = np.flatnonzero((want.view(np.uint32) != got.view(np.uint32)).any(axis=1))
+        assert diff.size == 0, f"{name}: {diff.size} of {n} differ, first input {x[diff[0]]}"
+        assert len(np.unique(want.view(np.uint32))) > 10, name
+        if name == "gather_voxel_lights":
+            lit = int((want != 0).any(axis=1).sum())
+    assert lit > 50  # the gather found light voxels for enough of its points
