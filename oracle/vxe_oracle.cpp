@@ -3027,7 +3027,8 @@ void ora_debug_grass(int which, uint32_t n, const float* in, float* out) {
 
 // Pin interface (test infrastructure): the oracle's restatements of the
 // reference's scene-reading helpers (sun shadow march, godray integral,
-// local-light gather, leaf query) over the world of `sc`, in the flat-slot
+// local-light gather, leaf query, clipmap heightfield march and samples) over
+// the world and clipmap of `sc`, in the flat-slot
 // layout of oracle_shading_eval.  Returns -1 for a name it does not know.
 int ora_scene_eval(const ora_scene* sc, const char* name, const float* in, float* out, uint32_t n) {
   if (!sc) return 1;
@@ -3039,6 +3040,8 @@ int ora_scene_eval(const ora_scene* sc, const char* name, const float* in, float
   else if (nm == "godray_integrate_1") iw = 9;
   else if (nm == "gather_voxel_lights") iw = 12;
   else if (nm == "query_leaf_world") iw = 3;
+  else if (nm == "clip_trace_heightfield") iw = 8;
+  else if (nm == "clip_height_at_level" || nm == "clip_height_at_level_nearest") iw = 3;
   else return -1;
   for (uint32_t k = 0; k < n; ++k) {
     const float* a = in + (size_t)k * iw;
@@ -3050,6 +3053,18 @@ int ora_scene_eval(const ora_scene* sc, const char* name, const float* in, float
     } else if (nm == "gather_voxel_lights") {  // root_size, node_base and macro_base are not read
       const v3 r = gather_voxel_lights(s, V3(a[0], a[1], a[2]), V3(a[3], a[4], a[5]), V3(a[6], a[7], a[8]));
       out[3 * k] = r.x, out[3 * k + 1] = r.y, out[3 * k + 2] = r.z;
+    } else if (nm == "clip_trace_heightfield") {
+      const ClipHit h = clip_trace_heightfield(s, V3(a[0], a[1], a[2]), V3(a[3], a[4], a[5]), a[6], a[7]);
+      float* o = out + (size_t)k * 6;
+      const uint32_t hit = h.hit ? 1u : 0u;
+      std::memcpy(o, &hit, 4);
+      o[1] = h.t, o[2] = h.n.x, o[3] = h.n.y, o[4] = h.n.z;
+      std::memcpy(o + 5, &h.mat, 4);
+    } else if (nm == "clip_height_at_level" || nm == "clip_height_at_level_nearest") {
+      uint32_t level;
+      std::memcpy(&level, a + 2, 4);
+      out[k] = nm == "clip_height_at_level" ? clip_height_at_level(s, V2(a[0], a[1]), level)
+                                            : clip_height_at_level_nearest(s, V2(a[0], a[1]), level);
     } else {
       const LeafQuery q = query_leaf_world(s, V3(a[0], a[1], a[2]));
       float* o = out + (size_t)k * 5;

@@ -216,6 +216,18 @@ inline vec4f operator*(const mat4x4f& m, const vec4f& v) {
   return m.c[0] * v.x + m.c[1] * v.y + m.c[2] * v.z + m.c[3] * v.w;
 }
 
+// texture_2d_array<f32> read with textureLoad (R32F layers of res x res
+// texels, row-major): a texel outside the texture reads zero.
+struct Tex2DArrayF {
+  const float* p = nullptr;
+  int32_t res = 0, layers = 0;
+};
+inline vec4f textureLoad(const Tex2DArrayF& t, vec<i32, 2> c, i32 layer, i32 /*mip*/) {
+  if (!t.p || c.x < 0 || c.y < 0 || c.x >= t.res || c.y >= t.res || layer < 0 || layer >= t.layers)
+    return vec4f(0.0f, 0.0f, 0.0f, 0.0f);
+  return vec4f(t.p[((size_t)layer * t.res + (size_t)c.y) * t.res + (size_t)c.x], 0.0f, 0.0f, 1.0f);
+}
+
 // A read-only storage buffer (array<T>): an index past the end reads a zero
 // record, as the oracle's checked reads do.
 template <class T>

@@ -54,7 +54,8 @@ EXPORTS = ["hash_u32", "hash12", "hash31", "value_noise", "fbm", "hash1", "wind_
            "grass_top_albedo", "base_albedo", "material_roughness", "material_f0", "material_emission",
            "approx_pow_0p75", "approx_pow_0p55", "exp_neg_fast", "godray_steps_for_tend", "godray_decompress",
            "godray_compress", "rot_about_axis", "sphere_dir_local", "trace_chunk_interval_stream_macro",
-           "sun_transmittance_geom_only", "godray_integrate_1", "gather_voxel_lights", "query_leaf_world"]
+           "sun_transmittance_geom_only", "godray_integrate_1", "gather_voxel_lights", "query_leaf_world",
+           "clip_trace_heightfield", "clip_height_at_level", "clip_height_at_level_nearest"]
 
 # The chunk walk (chunk_trace.wgsl, trace_chunk_interval_stream_macro) over a
 # world the caller holds in host memory, in the layouts of include/vxe/vxe.h
@@ -87,6 +88,11 @@ extern "C" void ref_wgsl_set_scene(const void* chunk_metas, uint64_t chunks_n, c
   cam.chunk_size = chunk_size;
   cam.chunk_count = chunk_count;
   cam.frame_index = frame_index;
+}
+static_assert(sizeof(ClipmapParams) == 528, "clipmap uniform layout");
+extern "C" void ref_wgsl_set_clip(const void* params528, const float* texels, int32_t res, int32_t layers) {
+  std::memcpy(&clip, params528, sizeof clip);
+  clip_height = Tex2DArrayF{texels, res, layers};
 }
 extern "C" int ref_wgsl_trace_chunk(const float* rays, float* out, unsigned n) {
   for (unsigned k = 0; k < n; ++k) {
@@ -319,6 +325,8 @@ def main(shader_dir: Path, out: Path) -> None:
             lines.append(f"static Buf<{conv_type(m.group(1))}> {bname};")
         elif "uniform" in space:
             lines.append(f"static {conv_type(bty)} {bname}{{}};")
+        elif bty.startswith("texture_2d_array<f32>"):
+            lines.append(f"static Tex2DArrayF {bname};")
     for sname, fields in structs:  # structs of flat fields can be results
         ftys = [conv_type(t) for _, t in fields]
         if fields and all(t in WIDTH for t in ftys) and not sname.startswith("_"):
@@ -345,6 +353,7 @@ def main(shader_dir: Path, out: Path) -> None:
               "static void put(float*& o, float v) { *o++ = v; }",
               "static void put(float*& o, uint32_t v) { std::memcpy(o++, &v, 4); }",
               "static void put(float*& o, int32_t v) { std::memcpy(o++, &v, 4); }",
+              "static void put(float*& o, bool v) { const uint32_t u = v ? 1u : 0u; std::memcpy(o++, &u, 4); }",
               "template <int N> static void put(float*& o, const vec<float, N>& v) { for (int i = 0; i < N; ++i) *o++ = v[i]; }",
               *[f"static void put_struct(float*& o, const {n}& v) {{ " + " ".join(f"put(o, v.{f});" for f in fs) + " }"
                 for n, fs in STRUCT_PUTS],

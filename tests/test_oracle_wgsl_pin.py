@@ -340,3 +340,39 @@ def test_oracle_scene_helpers_equal_translated_reference_wgsl():
         if name == "gather_voxel_lights":
             lit = int((want != 0).any(axis=1).sum())
     assert lit > 50  # the gather found light voxels for enough of its points
+
+
+def test_oracle_clipmap_march_equals_translated_reference_wgsl():
+    """The clipmap heightfield (clipmap.wgsl: clip_trace_heightfield, its
+    level samples, the toroidal texel offsets) on config 2's 5-level 256^2
+    clipmap, bit for bit."""
+    from vxe import scenes
+
+    ref, lo, ora_scene, w, cam, keep = _walk_setup(lambda: scenes.config2(present=(64, 36)))
+    runner, _, clip_params = keep
+    tex = np.ascontiguousarray(runner.clip_tex, np.float32)
+    ref.ref_wgsl_set_clip(C.c_void_p(C.addressof(clip_params)), tex.ctypes.data_as(C.POINTER(C.c_float)),
+                          C.c_int32(tex.shape[1]), C.c_int32(tex.shape[0]))
+    lo.ora_scene_eval.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p, C.c_void_p, C.c_uint32]
+    rng = np.random.default_rng(3)
+    n = 6000
+    cp = np.array(cam.cam_pos[:3], np.float32)
+    march = np.hstack([np.tile(cp, (n, 1)) + rng.uniform(-20, 20, (n, 3)) * [1, 0.2, 1], _dirs(rng, n, -0.4),
+                       np.zeros((n, 1)), rng.uniform(20, 400, (n, 1))])
+    levels = rng.integers(0, clip_params.levels, n).astype(np.uint32).view(np.float32)
+    samples = np.hstack([cp[[0, 2]] + rng.uniform(-600, 600, (n, 2)), levels[:, None]])
+    fp = C.POINTER(C.c_float)
+    for name, x in (("clip_trace_heightfield", march), ("clip_height_at_level", samples),
+                    ("clip_height_at_level_nearest", samples)):
+        x = np.ascontiguousarray(x, np.float32)
+        if name != "clip_trace_heightfield":
+            x[:, 2] = levels
+        iw, ow = C.c_uint(), C.c_uint()
+        assert ref.ref_wgsl_widths(name.encode(), C.byref(iw), C.byref(ow)) == 0, name
+        want = np.full((n, ow.value), np.nan, np.float32)
+        got = np.full((n, ow.value), np.nan, np.float32)
+        ref.ref_wgsl_eval(name.encode(), x.ctypes.data_as(fp), want.ctypes.data_as(fp), n)
+        assert lo.ora_scene_eval(C.addressof(ora_scene), name.encode(), x.ctypes.data, got.ctypes.data, n) == 0
+        diff = np.flatnonzero((want.view(np.uint32) != got.view(np.uint32)).any(axis=1))
+        assert diff.size == 0, f"{name}: {diff.size} of {n} differ, first input {x[diff[0]]}"
+        assert len(np.unique(want.view(np.uint32))) > 10, name  # nearest samples are whole voxel heights
