@@ -21,8 +21,8 @@
 // Rust toolchain, no graphics stack), so this restatement is pinned only in
 // part against the reference itself: its pure shading helpers and its chunk
 // walk are compared bit for bit with the reference's own WGSL translated to
-// C++ (oracle/wgsl_to_cpp.py; oracle_shading_eval, ora_scene_eval and
-// ora_trace_chunk below;
+// C++ (oracle/wgsl_to_cpp.py; oracle_shading_eval, ora_scene_eval,
+// ora_trace_chunk and ora_primary_tile below;
 // tests/test_oracle_wgsl_pin.py), and the scene traversal is checked against
 // an independent FP64 voxel DDA (tests/test_oracle_kat.py).
 #include <algorithm>
@@ -3073,6 +3073,44 @@ int ora_scene_eval(const ora_scene* sc, const char* name, const float* in, float
     }
   }
   return ctr.oob != 0 ? 2 : 0;
+}
+
+// Pin interface (test infrastructure): the cold primary voxel trace of the 64
+// pixels of tile (tx, ty) -- build_tile (main_primary's lane-0 candidate
+// list, ray_main.wgsl:179-197), then each pixel's
+// trace_scene_voxels_candidates from t = 0 without an anchor
+// (ray_main.wgsl:148-158) -- in the slot layout of the library
+// oracle/wgsl_to_cpp.py builds from the reference's own WGSL: 64 x 16 slots,
+// row-major pixels: in_grid (u32), hit (u32), mat (u32), t, n (3),
+// root_bmin (3), root_size, t_exit, anchor_valid (u32), anchor_key (u32),
+// anchor_chunk.xy (i32).  Returns the tile's candidate count.
+int ora_primary_tile(const ora_scene* sc, uint32_t tx, uint32_t ty, float* out) {
+  if (!sc) return -1;
+  Counters ctr;
+  const Scene s = make_scene(sc, &ctr, false);
+  TileList tl;
+  const uint32_t count = build_tile(s, tx, ty, tl);
+  auto putu = [](float*& o, uint32_t x) { std::memcpy(o++, &x, 4); };
+  for (uint32_t k = 0; k < 64u; ++k) {
+    const uint32_t gx = tx * 8u + (k & 7u), gy = ty * 8u + (k >> 3);
+    const v3 rd = ray_dir_from_pixel(s, V2((float)gx + 0.5f, (float)gy + 0.5f));
+    const VoxTraceResult r =
+        trace_scene_voxels_candidates(s, tl, cam_pos(s), rd, 0.0f, FOG_MAX_DIST, false, i3{0, 0, 0}, INVALID, count);
+    float* o = out + (size_t)k * 16;
+    putu(o, r.in_grid ? 1u : 0u);
+    putu(o, r.best.hit);
+    putu(o, r.best.mat);
+    *o++ = r.best.t;
+    *o++ = r.best.n.x, *o++ = r.best.n.y, *o++ = r.best.n.z;
+    *o++ = r.best.root_bmin.x, *o++ = r.best.root_bmin.y, *o++ = r.best.root_bmin.z;
+    *o++ = r.best.root_size;
+    *o++ = r.t_exit;
+    putu(o, r.anchor_valid ? 1u : 0u);
+    putu(o, r.anchor_key);
+    putu(o, (uint32_t)r.anchor_chunk.x);
+    putu(o, (uint32_t)r.anchor_chunk.y);
+  }
+  return (int)count;
 }
 
 // Pin interface (test infrastructure): one chunk walk,

@@ -228,6 +228,20 @@ inline vec4f textureLoad(const Tex2DArrayF& t, vec<i32, 2> c, i32 layer, i32 /*m
   return vec4f(t.p[((size_t)layer * t.res + (size_t)c.y) * t.res + (size_t)c.x], 0.0f, 0.0f, 1.0f);
 }
 
+// Workgroup atomics for a one-lane emulation of a workgroup (the tile's
+// lane-0 work runs alone, so the barriers have nothing to wait for).
+struct atomic_u32 {
+  u32 v;
+};
+inline u32 atomicLoad(atomic_u32* a) { return a->v; }
+inline void atomicStore(atomic_u32* a, u32 x) { a->v = x; }
+inline u32 atomicAdd(atomic_u32* a, u32 x) {
+  const u32 o = a->v;
+  a->v = o + x;
+  return o;
+}
+inline void workgroupBarrier() {}
+
 // A read-only storage buffer (array<T>): an index past the end reads a zero
 // record, as the oracle's checked reads do.
 template <class T>

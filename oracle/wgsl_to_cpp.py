@@ -55,7 +55,9 @@ EXPORTS = ["hash_u32", "hash12", "hash31", "value_noise", "fbm", "hash1", "wind_
            "approx_pow_0p75", "approx_pow_0p55", "exp_neg_fast", "godray_steps_for_tend", "godray_decompress",
            "godray_compress", "rot_about_axis", "sphere_dir_local", "trace_chunk_interval_stream_macro",
            "sun_transmittance_geom_only", "godray_integrate_1", "gather_voxel_lights", "query_leaf_world",
-           "clip_trace_heightfield", "clip_height_at_level", "clip_height_at_level_nearest"]
+           "clip_trace_heightfield", "clip_height_at_level", "clip_height_at_level_nearest",
+           "tile_append_candidates_for_ray", "tile_sort_candidates_by_enter", "trace_scene_voxels_candidates",
+           "ray_dir_from_pixel"]
 
 # The chunk walk (chunk_trace.wgsl, trace_chunk_interval_stream_macro) over a
 # world the caller holds in host memory, in the layouts of include/vxe/vxe.h
@@ -70,9 +72,7 @@ static_assert(sizeof(Node) == 16 && sizeof(NodeRopes) == 32 && sizeof(ChunkMeta)
 extern "C" void ref_wgsl_set_scene(const void* chunk_metas, uint64_t chunks_n, const void* node_recs, uint64_t nodes_n,
                                    const uint32_t* grid, uint64_t grid_n, const uint32_t* macro_words,
                                    uint64_t macro_n, const void* rope_recs, uint64_t ropes_n,
-                                   const uint32_t* colinfo_words, uint64_t colinfo_n, const float* cam_pos4,
-                                   const float* voxel_params4, uint32_t chunk_size, uint32_t chunk_count,
-                                   const int32_t* grid_origin4, const uint32_t* grid_dims4, uint32_t frame_index) {
+                                   const uint32_t* colinfo_words, uint64_t colinfo_n, const vxe_camera_gpu* c) {
   wgsl::chunks = Buf<ChunkMeta>{(const ChunkMeta*)chunk_metas, chunks_n};
   wgsl::nodes = Buf<Node>{(const Node*)node_recs, nodes_n};
   wgsl::chunk_grid = Buf<uint32_t>{grid, grid_n};
@@ -80,14 +80,26 @@ extern "C" void ref_wgsl_set_scene(const void* chunk_metas, uint64_t chunks_n, c
   wgsl::node_ropes = Buf<NodeRopes>{(const NodeRopes*)rope_recs, ropes_n};
   wgsl::chunk_colinfo = Buf<uint32_t>{colinfo_words, colinfo_n};
   for (int i = 0; i < 4; ++i) {
-    cam.cam_pos[i] = cam_pos4[i];
-    cam.voxel_params[i] = voxel_params4[i];
-    cam.grid_origin_chunk[i] = grid_origin4[i];
-    cam.grid_dims[i] = grid_dims4[i];
+    for (int j = 0; j < 4; ++j) {
+      cam.view_inv.c[i][j] = c->view_inv[i][j];
+      cam.proj_inv.c[i][j] = c->proj_inv[i][j];
+      cam.view_proj.c[i][j] = c->view_proj[i][j];
+      cam.prev_view_proj.c[i][j] = c->prev_view_proj[i][j];
+    }
+    cam.cam_pos[i] = c->cam_pos[i];
+    cam.ray00[i] = c->ray00[i];
+    cam.ray_dx[i] = c->ray_dx[i];
+    cam.ray_dy[i] = c->ray_dy[i];
+    cam.voxel_params[i] = c->voxel_params[i];
+    cam.grid_origin_chunk[i] = c->grid_origin_chunk[i];
+    cam.grid_dims[i] = c->grid_dims[i];
+    cam.render_present_px[i] = c->render_present_px[i];
   }
-  cam.chunk_size = chunk_size;
-  cam.chunk_count = chunk_count;
-  cam.frame_index = frame_index;
+  cam.chunk_size = c->chunk_size;
+  cam.chunk_count = c->chunk_count;
+  cam.max_steps = c->max_steps;
+  cam.frame_index = c->frame_index;
+  cam.profile_flags = c->profile_flags;
 }
 static_assert(sizeof(ClipmapParams) == 528, "clipmap uniform layout");
 extern "C" void ref_wgsl_set_clip(const void* params528, const float* texels, int32_t res, int32_t layers) {
@@ -118,6 +130,49 @@ extern "C" int ref_wgsl_trace_chunk(const float* rays, float* out, unsigned n) {
     put(o, 0.0f);
   }
   return 0;
+}
+// The cold primary voxel trace of the 64 pixels of tile (tx, ty): the tile's
+// candidate list built as main_primary's lane 0 builds it
+// (ray_main.wgsl:179-197), then each pixel's
+// trace_scene_voxels_candidates(ro, rd, 0, FOG_MAX_DIST, no anchor)
+// (ray_main.wgsl:148-158).  out: 64 x 16 slots per tile, row-major pixels:
+// in_grid (u32), hit (u32), mat (u32), t, n (3), root_bmin (3), root_size,
+// t_exit, anchor_valid (u32), anchor_key (u32), anchor_chunk.xy (i32);
+// returns the tile's candidate count.
+extern "C" int ref_wgsl_primary_tile(uint32_t tx, uint32_t ty, float* out) {
+  atomicStore(&WG_TILE_COUNT, 0u);
+  if (cam.chunk_count != 0u) {
+    const vec2f tile_base = vec2f(wgsl_f32(tx * TILE_SIZE), wgsl_f32(ty * TILE_SIZE));
+    const vec3f ro_tile = cam.cam_pos.xyz();
+    vec2f px = tile_base + vec2f(4.5f, 4.5f);
+    tile_append_candidates_for_ray(ro_tile, ray_dir_from_pixel(px), 0.0f, FOG_MAX_DIST);
+    px = tile_base + vec2f(1.5f, 1.5f);
+    tile_append_candidates_for_ray(ro_tile, ray_dir_from_pixel(px), 0.0f, FOG_MAX_DIST);
+  }
+  const uint32_t raw_count = min(atomicLoad(&WG_TILE_COUNT), MAX_TILE_CHUNKS);
+  tile_sort_candidates_by_enter(raw_count);
+  const uint32_t count = min(raw_count, PRIMARY_MAX_TILE_CHUNKS);
+  for (uint32_t k = 0; k < 64u; ++k) {
+    const uint32_t gx = tx * 8u + (k & 7u), gy = ty * 8u + (k >> 3);
+    const vec2f px = vec2f(wgsl_f32(gx) + 0.5f, wgsl_f32(gy) + 0.5f);
+    const uint32_t seed = (gx * 1973u) ^ (gy * 9277u) ^ (cam.frame_index * 26699u);
+    const VoxTraceResult r = trace_scene_voxels_candidates(cam.cam_pos.xyz(), ray_dir_from_pixel(px), 0.0f,
+                                                           FOG_MAX_DIST, false, vec3i(0), INVALID_U32, count, seed);
+    float* o = out + (size_t)k * 16;
+    put(o, (uint32_t)(r.in_grid ? 1u : 0u));
+    put(o, r.best.hit);
+    put(o, r.best.mat);
+    put(o, r.best.t);
+    put(o, r.best.n);
+    put(o, r.best.root_bmin);
+    put(o, r.best.root_size);
+    put(o, r.t_exit);
+    put(o, (uint32_t)(r.anchor_valid ? 1u : 0u));
+    put(o, r.anchor_key);
+    put(o, r.anchor_chunk.x);
+    put(o, r.anchor_chunk.y);
+  }
+  return (int)count;
 }
 """
 
@@ -153,6 +208,7 @@ def conv_type(t: str) -> str:
     t = re.sub(r"\bmat2x2<f32>", "mat2x2f", t)
     t = re.sub(r"\bmat4x4<f32>", "mat4x4f", t)
     t = re.sub(r"\bmat3x3<f32>", "mat3x3f", t)
+    t = re.sub(r"\batomic<u32>", "atomic_u32", t)
     pm = re.match(r"ptr<\s*function\s*,\s*(.+)>$", t)
     if pm:
         return conv_type(pm.group(1)) + "*"
@@ -238,7 +294,7 @@ def brace_ctors(s: str, names) -> str:
 
 
 def parse(shader_dir: Path):
-    consts, fns, structs, bindings = [], {}, [], []
+    consts, fns, structs, bindings, wg_vars = [], {}, [], [], []
     for rel in FILES:
         src = strip_comments((shader_dir / rel).read_text())
         i = 0
@@ -268,6 +324,10 @@ def parse(shader_dir: Path):
                     fields.append((re.sub(r"@\w+(\([^)]*\))?", "", fname).strip(), fty.strip()))
                 structs.append((sm.group(1), fields))
                 i = end
+            elif kind == "var" and re.compile(r"\s*var<(workgroup|private)>").match(src, i):
+                vm = re.compile(r"\s*var<(?:workgroup|private)>\s+(\w+)\s*:\s*([^;]+);").match(src, i)
+                wg_vars.append((vm.group(1), vm.group(2).strip()))
+                i = vm.end()
             elif kind == "@":
                 bm = re.compile(r"\s*@group\(\d+\)\s*@binding\(\d+\)\s*var(<[^>]*>)?\s+(\w+)\s*:\s*([^;]+);",
                                 re.S).match(src, i)
@@ -282,7 +342,7 @@ def parse(shader_dir: Path):
                 end = src.find(";", m.end())
                 brace = src.find("{", m.end())
                 i = (end + 1) if end >= 0 and (brace < 0 or end < brace) else (match_brace(src, brace) if brace >= 0 else len(src))
-    return consts, fns, structs, bindings
+    return consts, fns, structs, bindings, wg_vars
 
 
 def closure(fns, roots):
@@ -307,11 +367,11 @@ def params_of(ptext: str):
 
 
 def main(shader_dir: Path, out: Path) -> None:
-    consts, fns, structs, bindings = parse(shader_dir)
+    consts, fns, structs, bindings, wg_vars = parse(shader_dir)
     names = closure(fns, EXPORTS)
     snames = [n for n, _ in structs]
     lines = ["// Generated by oracle/wgsl_to_cpp.py from the reference's WGSL; not committed.",
-             '#include "wgsl_shim.h"', "#include <cstring>", "namespace wgsl {"]
+             '#include "wgsl_shim.h"', '#include "vxe/vxe.h"', "#include <cstring>", "namespace wgsl {"]
     for name, ty, expr in consts:
         ty_c = conv_type(ty) if ty else "auto"
         lines.append(f"static const {ty_c} {name} = {brace_ctors(conv_expr(expr.strip()), snames)};")
@@ -327,6 +387,8 @@ def main(shader_dir: Path, out: Path) -> None:
             lines.append(f"static {conv_type(bty)} {bname}{{}};")
         elif bty.startswith("texture_2d_array<f32>"):
             lines.append(f"static Tex2DArrayF {bname};")
+    for vname, vty in wg_vars:  # workgroup memory of a one-lane workgroup
+        lines.append(f"static {conv_type(vty)} {vname}{{}};")
     for sname, fields in structs:  # structs of flat fields can be results
         ftys = [conv_type(t) for _, t in fields]
         if fields and all(t in WIDTH for t in ftys) and not sname.startswith("_"):

@@ -6,11 +6,13 @@ over oracle/wgsl_shim.h): the pure shading helpers (sky, sun, clouds, fog,
 phase, tonemap, materials, wind, hashes, value noise, godray and light
 helpers) and the chunk walk of chunk_trace.wgsl with everything it calls
 (macro DDA, rope walk, leaf descent, anchors, grass column probes, blade
-marches, leaves) and the helpers that read the world (sun shadow march,
-godray integral, local-light gather, leaf query), reading the world from the
-same host arrays as the oracle.  The oracle restates the same functions by
-hand (oracle/vxe_oracle.cpp: oracle_shading_eval, ora_scene_eval,
-ora_trace_chunk).  With the
+marches, leaves), the whole cold primary voxel trace of a frame (tile
+candidate lists in a one-lane emulation of the workgroup, the candidate
+loop), the clipmap heightfield march and the helpers that read the world
+(sun shadow march, godray integral, local-light gather, leaf query), reading
+the world from the same host arrays as the oracle.  The oracle restates the
+same functions by hand (oracle/vxe_oracle.cpp: oracle_shading_eval,
+ora_scene_eval, ora_trace_chunk, ora_primary_tile).  With the
 same elementary functions on both sides, every output must be identical bit
 for bit on seeded inputs: a difference is a mis-reading in the restatement.
 
@@ -205,16 +207,13 @@ def _walk_setup(scene_fn):
     runner = O.OracleFrameRunner(w, sc.internal, sc.present, drv.clip.tex if drv.clip is not None else None,
                                  sc.clip_res)
     ora_scene = runner.scene(cam, clip_params)
-    fp, u64 = C.POINTER(C.c_float), C.c_uint64
-    keep = dict(cp=np.array(cam.cam_pos[:], np.float32), vp=np.array(cam.voxel_params[:], np.float32),
-                go=np.array(cam.grid_origin_chunk[:], np.int32), gd=np.array(cam.grid_dims[:], np.uint32))
+    u64 = C.c_uint64
+    keep = {}
     ref.ref_wgsl_set_scene(C.c_void_p(w.metas.ctypes.data), u64(w.metas.shape[0]), C.c_void_p(w.nodes.ctypes.data),
                            u64(len(w.nodes)), C.c_void_p(w.grid.ctypes.data), u64(len(w.grid)),
                            C.c_void_p(w.macro.ctypes.data), u64(len(w.macro)), C.c_void_p(w.ropes.ctypes.data),
                            u64(len(w.ropes)), C.c_void_p(w.colinfo.ctypes.data), u64(len(w.colinfo)),
-                           keep["cp"].ctypes.data_as(fp), keep["vp"].ctypes.data_as(fp), C.c_uint32(cam.chunk_size),
-                           C.c_uint32(cam.chunk_count), keep["go"].ctypes.data_as(C.POINTER(C.c_int32)),
-                           keep["gd"].ctypes.data_as(C.POINTER(C.c_uint32)), C.c_uint32(cam.frame_index))
+                           C.c_void_p(C.addressof(cam)))
     lo = O.lib()
     lo.ora_trace_chunk.argtypes = [C.POINTER(O.OraScene), C.c_void_p, C.c_void_p, C.c_uint32]
     return ref, lo, ora_scene, w, cam, (runner, keep, clip_params)
@@ -376,3 +375,36 @@ def test_oracle_clipmap_march_equals_translated_reference_wgsl():
         diff = np.flatnonzero((want.view(np.uint32) != got.view(np.uint32)).any(axis=1))
         assert diff.size == 0, f"{name}: {diff.size} of {n} differ, first input {x[diff[0]]}"
         assert len(np.unique(want.view(np.uint32))) > 10, name  # nearest samples are whole voxel heights
+
+
+@pytest.mark.parametrize("scene", ["features", "config2"])
+def test_oracle_primary_trace_equals_translated_reference_wgsl(scene):
+    """The cold primary voxel trace of every pixel of a frame: each 8x8
+    tile's candidate list as main_primary's lane 0 builds it (chunk grid DDA
+    of two tile rays, atomic appends, the sort by entry t) in a one-lane
+    emulation of the workgroup, then each pixel's candidate loop
+    (chunk_trace.wgsl trace_scene_voxels_candidates) with its chunk walks.
+    In-grid flag, hit, material, t, normal, chunk root, exit t and anchor,
+    bit for bit, and the same candidate count per tile."""
+    from vxe import scenes
+
+    fn = {"features": lambda: scenes.features(present=(128, 80)),
+          "config2": lambda: scenes.config2(present=(640, 360))}[scene]
+    ref, lo, ora_scene, w, cam, _keep = _walk_setup(fn)
+    lo.ora_primary_tile.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
+    ref.ref_wgsl_primary_tile.argtypes = [C.c_uint32, C.c_uint32, C.c_void_p]
+    iw, ih = cam.render_present_px[0], cam.render_present_px[1]
+    want = np.full((64, 16), np.nan, np.float32)
+    got = np.full((64, 16), np.nan, np.float32)
+    pixels = hits = 0
+    for ty in range((ih + 7) // 8):
+        for tx in range((iw + 7) // 8):
+            cw = ref.ref_wgsl_primary_tile(tx, ty, want.ctypes.data)
+            cg = lo.ora_primary_tile(C.addressof(ora_scene), tx, ty, got.ctypes.data)
+            assert cw == cg, f"tile ({tx}, {ty}): {cw} candidates in the reference, {cg} in the oracle"
+            bad = np.flatnonzero((want.view(np.uint32) != got.view(np.uint32)).any(axis=1))
+            assert bad.size == 0, (f"tile ({tx}, {ty}) pixel {bad[0]}: reference {want[bad[0]]}, "
+                                   f"oracle {got[bad[0]]}")
+            pixels += 64
+            hits += int((want[:, 1].view(np.uint32) != 0).sum())
+    assert hits > 0.3 * pixels
