@@ -17,14 +17,14 @@
 // Compile with -ffp-contract=off (no FMA contraction) so every float op is a
 // single IEEE binary32 operation, exactly as the device code evaluates it.
 //
-// Parity status: the reference is Rust + WGSL and cannot run whole here (no
-// Rust toolchain, no graphics stack), so this restatement is pinned only in
-// part against the reference itself: its pure shading helpers and its chunk
-// walk are compared bit for bit with the reference's own WGSL translated to
-// C++ (oracle/wgsl_to_cpp.py; oracle_shading_eval, ora_scene_eval,
-// ora_trace_chunk and ora_primary_tile below;
-// tests/test_oracle_wgsl_pin.py), and the scene traversal is checked against
-// an independent FP64 voxel DDA (tests/test_oracle_kat.py).
+// Parity status: the reference is Rust + WGSL and cannot run here as it is
+// (no Rust toolchain, no graphics stack).  Its shaders are translated to C++
+// instead (oracle/wgsl_to_cpp.py) and run beside this restatement: whole
+// frames of the five compute passes, every image, and the traces and helpers
+// function by function (oracle_shading_eval, ora_scene_eval, ora_trace_chunk
+// and ora_primary_tile below; tests/test_oracle_wgsl_pin.py), bit for bit.
+// The scene traversal is also checked against an independent FP64 voxel DDA
+// (tests/test_oracle_kat.py).
 #include <algorithm>
 #include <atomic>
 #include <cmath>

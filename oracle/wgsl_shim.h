@@ -191,6 +191,36 @@ WGSL_VEC_OP(*)
 WGSL_VEC_OP(/)
 #undef WGSL_VEC_OP
 
+// Component-wise comparisons -> vec<bool, N>, reduced by all / any.
+#define WGSL_VEC_CMP(op)                                                          \
+  template <class T, int N>                                                       \
+  inline vec<bool, N> operator op(const vec<T, N>& a, const vec<T, N>& b) {        \
+    vec<bool, N> r;                                                               \
+    for (int i = 0; i < N; ++i) r[i] = a[i] op b[i];                              \
+    return r;                                                                     \
+  }
+WGSL_VEC_CMP(<)
+WGSL_VEC_CMP(<=)
+WGSL_VEC_CMP(>)
+WGSL_VEC_CMP(>=)
+WGSL_VEC_CMP(==)
+WGSL_VEC_CMP(!=)
+#undef WGSL_VEC_CMP
+template <int N>
+inline bool all(const vec<bool, N>& v) {
+  for (int i = 0; i < N; ++i)
+    if (!v[i]) return false;
+  return true;
+}
+template <int N>
+inline bool any(const vec<bool, N>& v) {
+  for (int i = 0; i < N; ++i)
+    if (v[i]) return true;
+  return false;
+}
+inline bool all(bool b) { return b; }
+inline bool any(bool b) { return b; }
+
 // mat2x2<f32>: two columns; m * v sums column by column (c0 * v.x + c1 * v.y).
 struct mat2x2f {
   vec2f c0, c1;
@@ -227,6 +257,49 @@ inline vec4f textureLoad(const Tex2DArrayF& t, vec<i32, 2> c, i32 layer, i32 /*m
     return vec4f(0.0f, 0.0f, 0.0f, 0.0f);
   return vec4f(t.p[((size_t)layer * t.res + (size_t)c.y) * t.res + (size_t)c.x], 0.0f, 0.0f, 1.0f);
 }
+
+// texture_2d<f32> and texture_storage_2d<rgba32float | r32float> over host
+// images (w x h texels of `ch` floats, row-major).  Loads outside the image
+// read zero, stores outside it are dropped.  textureSampleLevel samples the
+// nearest texel with clamp-to-edge addressing, the reference's one sampler
+// (nearest, clamp).
+struct Tex2D {
+  float* p = nullptr;
+  int32_t w = 0, h = 0, ch = 4;
+};
+struct Sampler {};
+inline vec4f tex_fetch(const Tex2D& t, i32 x, i32 y) {
+  if (!t.p || x < 0 || y < 0 || x >= t.w || y >= t.h) return vec4f(0.0f, 0.0f, 0.0f, 0.0f);
+  const float* q = t.p + ((size_t)y * t.w + (size_t)x) * t.ch;
+  return t.ch == 4 ? vec4f(q[0], q[1], q[2], q[3]) : vec4f(q[0], 0.0f, 0.0f, 1.0f);
+}
+inline vec4f textureLoad(const Tex2D& t, vec<i32, 2> c, i32 /*mip*/) { return tex_fetch(t, c.x, c.y); }
+inline vec4f textureLoad(const Tex2D& t, vec<u32, 2> c, i32 mip) { return textureLoad(t, vec<i32, 2>((i32)c.x, (i32)c.y), mip); }
+inline void textureStore(Tex2D& t, vec<i32, 2> c, vec4f v) {
+  if (!t.p || c.x < 0 || c.y < 0 || c.x >= t.w || c.y >= t.h) return;
+  float* q = t.p + ((size_t)c.y * t.w + (size_t)c.x) * t.ch;
+  q[0] = v.x;
+  if (t.ch == 4) q[1] = v.y, q[2] = v.z, q[3] = v.w;
+}
+inline void textureStore(Tex2D& t, vec<u32, 2> c, vec4f v) { textureStore(t, vec<i32, 2>((i32)c.x, (i32)c.y), v); }
+inline vec<u32, 2> textureDimensions(const Tex2D& t) { return vec<u32, 2>((u32)t.w, (u32)t.h); }
+inline vec<u32, 2> textureDimensions(const Tex2D& t, i32 /*mip*/) { return textureDimensions(t); }
+inline vec4f textureSampleLevel(const Tex2D& t, const Sampler&, vec2f uv, float /*lod*/) {
+  const i32 x = wmin(wmax(wgsl_i32(std::floor(uv.x * (float)t.w)), (i32)0), (i32)(t.w - 1));
+  const i32 y = wmin(wmax(wgsl_i32(std::floor(uv.y * (float)t.h)), (i32)0), (i32)(t.h - 1));
+  return tex_fetch(t, x, y);
+}
+
+// A read-write storage buffer (array<T>): writes past the end are dropped.
+template <class T>
+struct RWBuf {
+  T* p = nullptr;
+  uint64_t n = 0;
+  T sink{};
+  T& operator[](uint64_t i) { return i < n ? p[i] : (sink = T{}); }
+  T& operator[](uint32_t i) { return (*this)[(uint64_t)i]; }
+  T& operator[](int32_t i) { return i >= 0 ? (*this)[(uint64_t)i] : (sink = T{}); }
+};
 
 // Workgroup atomics for a one-lane emulation of a workgroup (the tile's
 // lane-0 work runs alone, so the barriers have nothing to wait for).

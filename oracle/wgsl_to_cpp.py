@@ -24,9 +24,13 @@ and results are flattened into float slots (vecN = N slots; u32 / i32 / bool
 pass their bit patterns), n calls in a row; and, for the chunk walk,
     void ref_wgsl_set_scene(...)   (the world's host arrays and camera fields)
     int ref_wgsl_trace_chunk(const float* rays, float* out, unsigned n)
+and for whole frames of the five compute passes,
+    void ref_wgsl_set_clip(...)    (the clipmap uniform and layers)
+    int ref_wgsl_primary_tile(uint32_t tx, uint32_t ty, float* out)
+    int ref_wgsl_frame(uint32_t iw, uint32_t ih, uint32_t pw, uint32_t ph, float* const* images)
 The oracle exports the same interfaces over its own restatements
-(oracle_shading_eval, ora_trace_chunk), so a test compares the two function
-by function.
+(oracle_shading_eval, ora_scene_eval, ora_trace_chunk, ora_primary_tile;
+its frames through ora_render_frame), so a test compares the two.
 
 Usage: python oracle/wgsl_to_cpp.py <reference shader dir> <out .cpp>
 """
@@ -39,7 +43,7 @@ from pathlib import Path
 FILES = ["common.wgsl", "ray/wind.wgsl", "ray/phase.wgsl", "ray/fog.wgsl", "ray/clouds.wgsl", "ray/sky.wgsl",
          "ray/composite.wgsl", "ray/grass.wgsl", "ray/shading.wgsl", "ray/godrays.wgsl", "ray/light.wgsl",
          "ray/aabb.wgsl", "ray/svo_query.wgsl", "ray/leaves.wgsl", "clipmap.wgsl", "ray/chunk_trace.wgsl",
-         "ray/shadows.wgsl"]
+         "ray/shadows.wgsl", "ray_main.wgsl", "taa.wgsl"]
 
 # The functions the pin compares (each with its whole call closure).
 EXPORTS = ["hash_u32", "hash12", "hash31", "value_noise", "fbm", "hash1", "wind_field", "clamp_len",
@@ -57,7 +61,8 @@ EXPORTS = ["hash_u32", "hash12", "hash31", "value_noise", "fbm", "hash1", "wind_
            "sun_transmittance_geom_only", "godray_integrate_1", "gather_voxel_lights", "query_leaf_world",
            "clip_trace_heightfield", "clip_height_at_level", "clip_height_at_level_nearest",
            "tile_append_candidates_for_ray", "tile_sort_candidates_by_enter", "trace_scene_voxels_candidates",
-           "ray_dir_from_pixel"]
+           "ray_dir_from_pixel", "main_primary", "main_local_taa", "main_godray", "main_composite",
+           "main_composite_taa"]
 
 # The chunk walk (chunk_trace.wgsl, trace_chunk_interval_stream_macro) over a
 # world the caller holds in host memory, in the layouts of include/vxe/vxe.h
@@ -176,6 +181,77 @@ extern "C" int ref_wgsl_primary_tile(uint32_t tx, uint32_t ty, float* out) {
 }
 """
 
+# One cold frame of the reference's compute passes in the order
+# Renderer::encode_compute runs them (render/state/mod.rs:329-446):
+# main_primary, main_local_taa, main_godray, main_composite,
+# main_composite_taa, each over every pixel of its image; a workgroup of
+# main_primary runs its 64 lanes one after another, lane 0 first, so the tile
+# list lane 0 builds is there for the others (the barriers have nothing to
+# wait for).  The images are the caller's host arrays, wired as the frame's
+# bind groups wire them (render/state/bindgroups.rs): the godray and local
+# TAA passes write their "out" images, which the composite reads.  The
+# history inputs are the caller's (zero on a cold frame).
+#   img[0..15]: color, depth, local, primary_hist_in, primary_hist_out,
+#   shadow_hist_in, shadow_hist_out (buffer, rows padded to 256 B),
+#   local_hist_in, local_hist_out, godray_hist_in, godray_out, pre_taa,
+#   output_hist_in, output, output_hist_out (internal iw x ih, present
+#   pw x ph)
+FRAME_EXPORT = r"""
+extern "C" int ref_wgsl_frame(uint32_t iw, uint32_t ih, uint32_t pw, uint32_t ph, float* const* img) {
+  auto t4 = [](float* p, uint32_t w, uint32_t h) { return Tex2D{p, (int32_t)w, (int32_t)h, 4}; };
+  auto t1 = [](float* p, uint32_t w, uint32_t h) { return Tex2D{p, (int32_t)w, (int32_t)h, 1}; };
+  color_img = t4(img[0], iw, ih);
+  depth_img = t1(img[1], iw, ih);
+  local_img = t4(img[2], iw, ih);
+  primary_hist_tex = t4(img[3], iw, ih);
+  primary_hist_out = t4(img[4], iw, ih);
+  shadow_hist_in = t1(img[5], iw, ih);
+  const uint64_t stride = (((uint64_t)iw * 4u + 255u) & ~(uint64_t)255u) / 4u;
+  shadow_hist_out = RWBuf<float>{img[6], stride * ih};
+  local_in_tex = t4(img[2], iw, ih);
+  local_hist_in_tex = t4(img[7], iw, ih);
+  local_hist_out = t4(img[8], iw, ih);
+  depth_tex = t1(img[1], iw, ih);
+  godray_hist_tex = t4(img[9], iw, ih);
+  godray_out = t4(img[10], iw, ih);
+  color_tex = t4(img[0], iw, ih);
+  godray_tex = t4(img[10], iw, ih);
+  out_img = t4(img[11], pw, ph);
+  depth_full = t1(img[1], iw, ih);
+  local_hist_tex = t4(img[8], iw, ih);
+  composite_in_tex = t4(img[11], pw, ph);
+  depth_full_tex = t1(img[1], iw, ih);
+  hist_in_tex = t4(img[12], pw, ph);
+  output_tex = t4(img[13], pw, ph);
+  hist_out_tex = t4(img[14], pw, ph);
+  for (uint32_t wy = 0; wy < (ih + 7u) / 8u; ++wy)
+    for (uint32_t wx = 0; wx < (iw + 7u) / 8u; ++wx)
+      for (uint32_t lid = 0; lid < 64u; ++lid)
+        main_primary(vec3u(wx * 8u + (lid & 7u), wy * 8u + (lid >> 3), 0u), lid, vec3u(wx, wy, 0u));
+  for (uint32_t y = 0; y < ih; ++y)
+    for (uint32_t x = 0; x < iw; ++x) main_local_taa(vec3u(x, y, 0u));
+  // The godray pass binds scene_bg (render/state/bindgroups.rs:120-156):
+  // macro_occ at binding 8, node_ropes at 9, colinfo at 10, while the shader
+  // declares macro_occ at 9, node_ropes at 10 and chunk_colinfo at 11.
+  const Buf<uint32_t> macro_keep = wgsl::macro_occ;
+  const Buf<NodeRopes> ropes_keep = wgsl::node_ropes;
+  const Buf<uint32_t> colinfo_keep = wgsl::chunk_colinfo;
+  wgsl::macro_occ = Buf<uint32_t>{(const uint32_t*)ropes_keep.p, ropes_keep.n * 8u};
+  wgsl::node_ropes = Buf<NodeRopes>{(const NodeRopes*)colinfo_keep.p, colinfo_keep.n / 8u};
+  wgsl::chunk_colinfo = Buf<uint32_t>{};
+  for (uint32_t y = 0; y < ih; ++y)
+    for (uint32_t x = 0; x < iw; ++x) main_godray(vec3u(x, y, 0u));
+  wgsl::macro_occ = macro_keep;
+  wgsl::node_ropes = ropes_keep;
+  wgsl::chunk_colinfo = colinfo_keep;
+  for (uint32_t y = 0; y < ph; ++y)
+    for (uint32_t x = 0; x < pw; ++x) main_composite(vec3u(x, y, 0u));
+  for (uint32_t y = 0; y < ph; ++y)
+    for (uint32_t x = 0; x < pw; ++x) main_composite_taa(vec3u(x, y, 0u));
+  return 0;
+}
+"""
+
 STRUCT_PUTS = []  # (struct name, field names) of flat structs, filled by main()
 
 TYPE_MAP = {"f32": "float", "u32": "uint32_t", "i32": "int32_t", "bool": "bool"}
@@ -209,6 +285,12 @@ def conv_type(t: str) -> str:
     t = re.sub(r"\bmat4x4<f32>", "mat4x4f", t)
     t = re.sub(r"\bmat3x3<f32>", "mat3x3f", t)
     t = re.sub(r"\batomic<u32>", "atomic_u32", t)
+    if t.startswith("texture_2d<"):
+        return "const Tex2D&"
+    if t.startswith("texture_storage_2d<"):
+        return "Tex2D&"
+    if t == "sampler":
+        return "const Sampler&"
     pm = re.match(r"ptr<\s*function\s*,\s*(.+)>$", t)
     if pm:
         return conv_type(pm.group(1)) + "*"
@@ -328,6 +410,8 @@ def parse(shader_dir: Path):
                 vm = re.compile(r"\s*var<(?:workgroup|private)>\s+(\w+)\s*:\s*([^;]+);").match(src, i)
                 wg_vars.append((vm.group(1), vm.group(2).strip()))
                 i = vm.end()
+            elif kind == "@" and re.compile(r"\s*@compute").match(src, i):
+                i = re.compile(r"\s*@compute\s*@workgroup_size\([^)]*\)").match(src, i).end()
             elif kind == "@":
                 bm = re.compile(r"\s*@group\(\d+\)\s*@binding\(\d+\)\s*var(<[^>]*>)?\s+(\w+)\s*:\s*([^;]+);",
                                 re.S).match(src, i)
@@ -360,7 +444,7 @@ def closure(fns, roots):
 
 def params_of(ptext: str):
     ps = []
-    for p in split_top(ptext):
+    for p in split_top(re.sub(r"@\w+\([^)]*\)", "", ptext)):
         name, ty = p.split(":", 1)
         ps.append((name.strip(), conv_type(ty)))
     return ps
@@ -376,13 +460,21 @@ def main(shader_dir: Path, out: Path) -> None:
         ty_c = conv_type(ty) if ty else "auto"
         lines.append(f"static const {ty_c} {name} = {brace_ctors(conv_expr(expr.strip()), snames)};")
     for sname, fields in structs:  # the shader's structs, member for member
-        if any("atomic" in t or "texture" in t for _, t in fields):
+        if any("texture" in t for _, t in fields):
             continue
         lines.append(f"struct {sname} {{ " + " ".join(f"{conv_type(t)} {f};" for f, t in fields) + " };")
-    for space, bname, bty in bindings:  # storage buffers and the uniform
+    for space, bname, bty in bindings:  # storage buffers, the uniforms, images
         m = re.match(r"array<\s*(\w+)\s*>$", bty)
-        if "storage" in space and m:
+        if "read_write" in space and m:
+            lines.append(f"static RWBuf<{conv_type(m.group(1))}> {bname};")
+        elif "read_write" in space:
+            lines.append(f"static {conv_type(bty)} {bname}{{}};")
+        elif "storage" in space and m:
             lines.append(f"static Buf<{conv_type(m.group(1))}> {bname};")
+        elif bty.startswith("texture_2d<") or bty.startswith("texture_storage_2d<"):
+            lines.append(f"static Tex2D {bname};")
+        elif bty == "sampler":
+            lines.append(f"static Sampler {bname};")
         elif "uniform" in space:
             lines.append(f"static {conv_type(bty)} {bname}{{}};")
         elif bty.startswith("texture_2d_array<f32>"):
@@ -455,6 +547,8 @@ def main(shader_dir: Path, out: Path) -> None:
     lines += ["  }", "  return 0;", "}"]
     if "trace_chunk_interval_stream_macro" in sigs:
         lines += CHUNK_WALK_EXPORT.splitlines()
+    if "main_primary" in sigs:
+        lines += FRAME_EXPORT.splitlines()
     out.parent.mkdir(parents=True, exist_ok=True)
     out.write_text("\n".join(lines) + "\n")
 

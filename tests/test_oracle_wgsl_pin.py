@@ -1,20 +1,24 @@
 """Pins the oracle to the reference's own WGSL.
 
-The reference's shader functions are translated mechanically from its WGSL
-into C++ at build time (oracle/wgsl_to_cpp.py -> oracle/_ref/libref_wgsl.so,
-over oracle/wgsl_shim.h): the pure shading helpers (sky, sun, clouds, fog,
-phase, tonemap, materials, wind, hashes, value noise, godray and light
-helpers) and the chunk walk of chunk_trace.wgsl with everything it calls
-(macro DDA, rope walk, leaf descent, anchors, grass column probes, blade
-marches, leaves), the whole cold primary voxel trace of a frame (tile
-candidate lists in a one-lane emulation of the workgroup, the candidate
-loop), the clipmap heightfield march and the helpers that read the world
-(sun shadow march, godray integral, local-light gather, leaf query), reading
-the world from the same host arrays as the oracle.  The oracle restates the
-same functions by hand (oracle/vxe_oracle.cpp: oracle_shading_eval,
-ora_scene_eval, ora_trace_chunk, ora_primary_tile).  With the
-same elementary functions on both sides, every output must be identical bit
-for bit on seeded inputs: a difference is a mis-reading in the restatement.
+The reference's shaders are translated mechanically from its WGSL into C++ at
+build time (oracle/wgsl_to_cpp.py -> oracle/_ref/libref_wgsl.so, over
+oracle/wgsl_shim.h) and run beside the oracle, which restates them by hand
+(oracle/vxe_oracle.cpp):
+  * whole frames of the five compute passes (main_primary, main_local_taa,
+    main_godray, main_composite, main_composite_taa) with the images and bind
+    groups wired as the reference wires them, histories carried across
+    frames: every image;
+  * the cold primary voxel trace of every pixel (tile candidate lists in a
+    one-lane emulation of the workgroup, the candidate loop);
+  * the chunk walk of chunk_trace.wgsl with everything it calls (macro DDA,
+    rope walk, leaf descent, anchors, grass probes, blade marches, leaves);
+  * the clipmap heightfield march and the helpers that read the world (sun
+    shadow march, godray integral, local-light gather, leaf query);
+  * 54 pure shading helpers (sky, sun, clouds, fog, phase, tonemap,
+    materials, wind, hashes, value noise, godray and light helpers).
+With the same elementary functions on both sides (include/vxe/detmath.h),
+every output must be identical bit for bit: a difference is a mis-reading in
+the restatement.
 
 The translated library is built only where the reference's sources are
 present; elsewhere these tests are skipped.
@@ -207,16 +211,35 @@ def _walk_setup(scene_fn):
     runner = O.OracleFrameRunner(w, sc.internal, sc.present, drv.clip.tex if drv.clip is not None else None,
                                  sc.clip_res)
     ora_scene = runner.scene(cam, clip_params)
-    u64 = C.c_uint64
+    runner._driver = drv  # the path's next frames (whole-frame test)
     keep = {}
+    _set_ref_camera(ref, w, cam)
+    lo = O.lib()
+    lo.ora_trace_chunk.argtypes = [C.POINTER(O.OraScene), C.c_void_p, C.c_void_p, C.c_uint32]
+    return ref, lo, ora_scene, w, cam, (runner, keep, clip_params)
+
+
+def _set_ref_camera(ref, w, cam):
+    """Binds the world's host arrays and copies `cam` into the translated
+    reference's scene bindings."""
+    u64 = C.c_uint64
     ref.ref_wgsl_set_scene(C.c_void_p(w.metas.ctypes.data), u64(w.metas.shape[0]), C.c_void_p(w.nodes.ctypes.data),
                            u64(len(w.nodes)), C.c_void_p(w.grid.ctypes.data), u64(len(w.grid)),
                            C.c_void_p(w.macro.ctypes.data), u64(len(w.macro)), C.c_void_p(w.ropes.ctypes.data),
                            u64(len(w.ropes)), C.c_void_p(w.colinfo.ctypes.data), u64(len(w.colinfo)),
                            C.c_void_p(C.addressof(cam)))
-    lo = O.lib()
-    lo.ora_trace_chunk.argtypes = [C.POINTER(O.OraScene), C.c_void_p, C.c_void_p, C.c_uint32]
-    return ref, lo, ora_scene, w, cam, (runner, keep, clip_params)
+
+
+def _set_ref_clip(ref, runner, clip_params):
+    """The clipmap uniform and texture layers of the oracle runner, for the
+    translated reference (no layers: a clipmap with no texture)."""
+    if runner.clip_tex is not None:
+        runner._ref_tex = np.ascontiguousarray(runner.clip_tex, np.float32)
+        t = runner._ref_tex
+        ref.ref_wgsl_set_clip(C.c_void_p(C.addressof(clip_params)), t.ctypes.data_as(C.POINTER(C.c_float)),
+                              C.c_int32(t.shape[1]), C.c_int32(t.shape[0]))
+    else:
+        ref.ref_wgsl_set_clip(C.c_void_p(C.addressof(clip_params)), None, C.c_int32(0), C.c_int32(0))
 
 
 def _walk_rays(w, cam, n, rng):
@@ -408,3 +431,61 @@ def test_oracle_primary_trace_equals_translated_reference_wgsl(scene):
             pixels += 64
             hits += int((want[:, 1].view(np.uint32) != 0).sum())
     assert hits > 0.3 * pixels
+
+
+def _frame_io(iw, ih, pw, ph):
+    z = lambda *s: np.zeros(s, np.float32)
+    stride = ((iw * 4 + 255) & ~255) // 4
+    return [z(ih, iw, 4), z(ih, iw), z(ih, iw, 4), z(ih, iw, 4), z(ih, iw, 4), z(ih, iw), z(ih, stride),
+            z(ih, iw, 4), z(ih, iw, 4), z(ih, iw, 4), z(ih, iw, 4), z(ph, pw, 4), z(ph, pw, 4), z(ph, pw, 4),
+            z(ph, pw, 4)]
+
+
+@pytest.mark.parametrize("scene,frames", [("features", 3), ("config1", 1), ("config2", 2)])
+def test_oracle_frames_equal_translated_reference_wgsl(scene, frames):
+    """Whole frames of the reference's own compute passes -- main_primary,
+    main_local_taa, main_godray, main_composite, main_composite_taa, run per
+    pixel in the order Renderer::encode_compute runs them, with the
+    images and the godray pass's scene bind group wired as the reference
+    wires them -- against the oracle's frames: every image bit for bit (color,
+    depth, local, primary-hit history, shadow history, local TAA history,
+    godray, pre-TAA composite, output, output history).  After each frame the
+    histories feed the next one, as the reference's ping-pong and its shadow
+    buffer -> texture copy do."""
+    from vxe import scenes
+
+    fn = {"features": lambda: scenes.features(present=(128, 80)), "config1": scenes.config1,
+          "config2": lambda: scenes.config2(present=(320, 180))}[scene]
+    ref, lo, ora_scene, w, cam, keep = _walk_setup(fn)
+    runner, _, clip_params = keep
+    drv_cam, drv_clip = cam, clip_params
+    iw, ih, pw, ph = (cam.render_present_px[i] for i in range(4))
+    io = _frame_io(iw, ih, pw, ph)
+    ref.ref_wgsl_frame.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p]
+    names = {0: "color", 1: "depth", 2: "local", 4: "primary_hist", 8: "local_hist", 10: "godray",
+             11: "output_pre_taa", 13: "output", 14: "output_hist"}
+    for f in range(frames):
+        if f > 0:  # the next path frame on both sides
+            _, _, clip, drv_cam = runner._driver.step()
+            drv_clip = clip[0] if clip is not None else runner._driver.empty_clip()
+            ora_scene = runner.scene(drv_cam, drv_clip)
+            _set_ref_camera(ref, w, drv_cam)
+        _set_ref_clip(ref, runner, drv_clip)
+        ptrs = (C.c_void_p * 15)(*[a.ctypes.data for a in io])
+        assert ref.ref_wgsl_frame(iw, ih, pw, ph, ptrs) == 0
+        runner.render(drv_cam, drv_clip)
+        o = runner.outputs()
+        for k, nm in names.items():
+            got = np.ascontiguousarray(o[nm]).reshape(-1).view(np.uint32)
+            want = io[k].reshape(-1).view(np.uint32)
+            bad = np.flatnonzero(want != got)
+            assert bad.size == 0, f"frame {f} {nm}: {bad.size} of {want.size} values differ, first at {bad[0]}"
+        bad = np.flatnonzero(io[6][:, :iw].reshape(-1).view(np.uint32) != o["shadow"].reshape(-1).view(np.uint32))
+        assert bad.size == 0, f"frame {f} shadow: {bad.size} values differ"
+        assert len(np.unique(io[13].view(np.uint32))) > 1000
+        # histories for the next frame (the reference's ping-pong)
+        io[3][:] = io[4]
+        io[5][:] = io[6][:, :iw]
+        io[7][:] = io[8]
+        io[9][:] = io[10]
+        io[12][:] = io[14]
