@@ -27,7 +27,8 @@ pass their bit patterns), n calls in a row; and, for the chunk walk,
 and for whole frames of the five compute passes,
     void ref_wgsl_set_clip(...)    (the clipmap uniform and layers)
     int ref_wgsl_primary_tile(uint32_t tx, uint32_t ty, float* out)
-    int ref_wgsl_frame(uint32_t iw, uint32_t ih, uint32_t pw, uint32_t ph, float* const* images)
+    int ref_wgsl_frame(uint32_t iw, uint32_t ih, uint32_t pw, uint32_t ph, float* const* images,
+                       uint32_t threads)
 The oracle exports the same interfaces over its own restatements
 (oracle_shading_eval, ora_scene_eval, ora_trace_chunk, ora_primary_tile;
 its frames through ora_render_frame), so a test compares the two.
@@ -197,7 +198,22 @@ extern "C" int ref_wgsl_primary_tile(uint32_t tx, uint32_t ty, float* out) {
 #   output_hist_in, output, output_hist_out (internal iw x ih, present
 #   pw x ph)
 FRAME_EXPORT = r"""
-extern "C" int ref_wgsl_frame(uint32_t iw, uint32_t ih, uint32_t pw, uint32_t ph, float* const* img) {
+// Runs body(row) for rows [0, rows) on `threads` host threads (interleaved).
+template <class F>
+static void parallel_rows(uint32_t rows, uint32_t threads, F body) {
+  if (threads <= 1u) {
+    for (uint32_t r = 0; r < rows; ++r) body(r);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (uint32_t t = 0; t < threads; ++t)
+    pool.emplace_back([=] {
+      for (uint32_t r = t; r < rows; r += threads) body(r);
+    });
+  for (auto& th : pool) th.join();
+}
+extern "C" int ref_wgsl_frame(uint32_t iw, uint32_t ih, uint32_t pw, uint32_t ph, float* const* img,
+                              uint32_t threads) {
   auto t4 = [](float* p, uint32_t w, uint32_t h) { return Tex2D{p, (int32_t)w, (int32_t)h, 4}; };
   auto t1 = [](float* p, uint32_t w, uint32_t h) { return Tex2D{p, (int32_t)w, (int32_t)h, 1}; };
   color_img = t4(img[0], iw, ih);
@@ -224,12 +240,14 @@ extern "C" int ref_wgsl_frame(uint32_t iw, uint32_t ih, uint32_t pw, uint32_t ph
   hist_in_tex = t4(img[12], pw, ph);
   output_tex = t4(img[13], pw, ph);
   hist_out_tex = t4(img[14], pw, ph);
-  for (uint32_t wy = 0; wy < (ih + 7u) / 8u; ++wy)
+  parallel_rows((ih + 7u) / 8u, threads, [&](uint32_t wy) {
     for (uint32_t wx = 0; wx < (iw + 7u) / 8u; ++wx)
       for (uint32_t lid = 0; lid < 64u; ++lid)
         main_primary(vec3u(wx * 8u + (lid & 7u), wy * 8u + (lid >> 3), 0u), lid, vec3u(wx, wy, 0u));
-  for (uint32_t y = 0; y < ih; ++y)
+  });
+  parallel_rows(ih, threads, [&](uint32_t y) {
     for (uint32_t x = 0; x < iw; ++x) main_local_taa(vec3u(x, y, 0u));
+  });
   // The godray pass binds scene_bg (render/state/bindgroups.rs:120-156):
   // macro_occ at binding 8, node_ropes at 9, colinfo at 10, while the shader
   // declares macro_occ at 9, node_ropes at 10 and chunk_colinfo at 11.
@@ -239,15 +257,18 @@ extern "C" int ref_wgsl_frame(uint32_t iw, uint32_t ih, uint32_t pw, uint32_t ph
   wgsl::macro_occ = Buf<uint32_t>{(const uint32_t*)ropes_keep.p, ropes_keep.n * 8u};
   wgsl::node_ropes = Buf<NodeRopes>{(const NodeRopes*)colinfo_keep.p, colinfo_keep.n / 8u};
   wgsl::chunk_colinfo = Buf<uint32_t>{};
-  for (uint32_t y = 0; y < ih; ++y)
+  parallel_rows(ih, threads, [&](uint32_t y) {
     for (uint32_t x = 0; x < iw; ++x) main_godray(vec3u(x, y, 0u));
+  });
   wgsl::macro_occ = macro_keep;
   wgsl::node_ropes = ropes_keep;
   wgsl::chunk_colinfo = colinfo_keep;
-  for (uint32_t y = 0; y < ph; ++y)
+  parallel_rows(ph, threads, [&](uint32_t y) {
     for (uint32_t x = 0; x < pw; ++x) main_composite(vec3u(x, y, 0u));
-  for (uint32_t y = 0; y < ph; ++y)
+  });
+  parallel_rows(ph, threads, [&](uint32_t y) {
     for (uint32_t x = 0; x < pw; ++x) main_composite_taa(vec3u(x, y, 0u));
+  });
   return 0;
 }
 """
@@ -455,7 +476,8 @@ def main(shader_dir: Path, out: Path) -> None:
     names = closure(fns, EXPORTS)
     snames = [n for n, _ in structs]
     lines = ["// Generated by oracle/wgsl_to_cpp.py from the reference's WGSL; not committed.",
-             '#include "wgsl_shim.h"', '#include "vxe/vxe.h"', "#include <cstring>", "namespace wgsl {"]
+             '#include "wgsl_shim.h"', '#include "vxe/vxe.h"', "#include <cstring>", "#include <thread>",
+             "#include <vector>", "namespace wgsl {"]
     for name, ty, expr in consts:
         ty_c = conv_type(ty) if ty else "auto"
         lines.append(f"static const {ty_c} {name} = {brace_ctors(conv_expr(expr.strip()), snames)};")
@@ -479,8 +501,8 @@ def main(shader_dir: Path, out: Path) -> None:
             lines.append(f"static {conv_type(bty)} {bname}{{}};")
         elif bty.startswith("texture_2d_array<f32>"):
             lines.append(f"static Tex2DArrayF {bname};")
-    for vname, vty in wg_vars:  # workgroup memory of a one-lane workgroup
-        lines.append(f"static {conv_type(vty)} {vname}{{}};")
+    for vname, vty in wg_vars:  # workgroup memory: each host thread runs whole workgroups
+        lines.append(f"static thread_local {conv_type(vty)} {vname}{{}};")
     for sname, fields in structs:  # structs of flat fields can be results
         ftys = [conv_type(t) for _, t in fields]
         if fields and all(t in WIDTH for t in ftys) and not sname.startswith("_"):

@@ -461,7 +461,7 @@ def test_oracle_frames_equal_translated_reference_wgsl(scene, frames):
     drv_cam, drv_clip = cam, clip_params
     iw, ih, pw, ph = (cam.render_present_px[i] for i in range(4))
     io = _frame_io(iw, ih, pw, ph)
-    ref.ref_wgsl_frame.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p]
+    ref.ref_wgsl_frame.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32]
     names = {0: "color", 1: "depth", 2: "local", 4: "primary_hist", 8: "local_hist", 10: "godray",
              11: "output_pre_taa", 13: "output", 14: "output_hist"}
     for f in range(frames):
@@ -472,7 +472,7 @@ def test_oracle_frames_equal_translated_reference_wgsl(scene, frames):
             _set_ref_camera(ref, w, drv_cam)
         _set_ref_clip(ref, runner, drv_clip)
         ptrs = (C.c_void_p * 15)(*[a.ctypes.data for a in io])
-        assert ref.ref_wgsl_frame(iw, ih, pw, ph, ptrs) == 0
+        assert ref.ref_wgsl_frame(iw, ih, pw, ph, ptrs, 1 + f) == 0  # 1, 2, 3 host threads: the same images
         runner.render(drv_cam, drv_clip)
         o = runner.outputs()
         for k, nm in names.items():

@@ -140,7 +140,7 @@ def build_ref_wgsl(verbose: bool = False, force: bool = False):
     cpp = REF_WGSL_DIR / "ref_wgsl.cpp"
     _run([sys.executable, translator, REF_SHADERS, cpp], verbose)
     tmp = REF_WGSL_LIB.with_suffix(".so.tmp")
-    _run(["g++", *CXX_FLAGS, f"-I{REPO / 'oracle'}", "-shared", "-o", tmp, cpp], verbose)
+    _run(["g++", *CXX_FLAGS, f"-I{REPO / 'oracle'}", "-shared", "-o", tmp, cpp, "-lpthread"], verbose)
     os.replace(tmp, REF_WGSL_LIB)
     return REF_WGSL_LIB
 
