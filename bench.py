@@ -21,6 +21,7 @@ internal over a streamed world of 16x4x16 chunks with 3D caves, a 5-level
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import contextlib
 import gc
 import json
@@ -1078,10 +1079,61 @@ def main():
     print(json.dumps(line))
 
 
+def _ref_wgsl_frames(drv, sc, threads):
+    """The reference's own five compute passes, translated mechanically from
+    its WGSL to C++ (oracle/_ref/libref_wgsl.so, built by vxe_build where the
+    reference's sources are), as a per-step frame function; None where that
+    library is absent.  The world is bound once, the camera and clipmap per
+    frame (not timed); the histories ping-pong as the reference's do."""
+    import vxe_build
+
+    if not vxe_build.REF_WGSL_LIB.exists():
+        return None
+    ref = C.CDLL(str(vxe_build.REF_WGSL_LIB))
+    ref.ref_wgsl_frame.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32]
+    w = drv.world
+    iw, ih = sc.internal
+    pw, ph = sc.present
+    z = lambda *shape: np.zeros(shape, np.float32)
+    stride = ((iw * 4 + 255) & ~255) // 4
+    io = [z(ih, iw, 4), z(ih, iw), z(ih, iw, 4), z(ih, iw, 4), z(ih, iw, 4), z(ih, iw), z(ih, stride),
+          z(ih, iw, 4), z(ih, iw, 4), z(ih, iw, 4), z(ih, iw, 4), z(ph, pw, 4), z(ph, pw, 4), z(ph, pw, 4),
+          z(ph, pw, 4)]
+    u64 = C.c_uint64
+    keep = {}
+
+    def frame(cam, clip_params):
+        keep["cam"], keep["clip"] = cam, clip_params
+        keep["tex"] = np.ascontiguousarray(drv.clip.tex, np.float32)
+        ref.ref_wgsl_set_scene(C.c_void_p(w.metas.ctypes.data), u64(w.metas.shape[0]),
+                               C.c_void_p(w.nodes.ctypes.data), u64(len(w.nodes)), C.c_void_p(w.grid.ctypes.data),
+                               u64(len(w.grid)), C.c_void_p(w.macro.ctypes.data), u64(len(w.macro)),
+                               C.c_void_p(w.ropes.ctypes.data), u64(len(w.ropes)),
+                               C.c_void_p(w.colinfo.ctypes.data), u64(len(w.colinfo)), C.c_void_p(C.addressof(cam)))
+        t = keep["tex"]
+        ref.ref_wgsl_set_clip(C.c_void_p(C.addressof(clip_params)), t.ctypes.data_as(C.POINTER(C.c_float)),
+                              C.c_int32(t.shape[1]), C.c_int32(t.shape[0]))
+        ptrs = (C.c_void_p * 15)(*[a.ctypes.data for a in io])
+        t0 = time.perf_counter()
+        ref.ref_wgsl_frame(iw, ih, pw, ph, ptrs, threads)
+        dt = time.perf_counter() - t0
+        io[3], io[4] = io[4], io[3]  # this frame's histories are the next one's inputs
+        io[5][:] = io[6][:, :iw]  # the shadow buffer -> texture copy
+        io[7], io[8] = io[8], io[7]
+        io[9], io[10] = io[10], io[9]
+        io[12], io[14] = io[14], io[12]
+        return dt
+
+    return frame
+
+
 def main_reference(args, rank, world_size):
-    """The reference arm: the reference's passes as the CPU restatement of its
-    WGSL (oracle/) on all host cores, one full frame of the same workload per
-    step.  Its frame inputs come from a host-only build of the producers
+    """The reference arm, on all host cores, one full frame of the same
+    workload per step.  Where the reference's sources were present at build
+    time it runs the reference's own compute passes -- its WGSL translated
+    mechanically to C++ (oracle/wgsl_to_cpp.py), shown bit-identical to the
+    oracle's frames -- else the oracle's C++ restatement of them (oracle/).
+    Its frame inputs come from a host-only build of the producers
     (oracle/libref_producer.so), so this process maps no CUDA library of this
     repository; the producer work between frames is not timed."""
     if rank != 0:
@@ -1099,12 +1151,16 @@ def main_reference(args, rank, world_size):
     sc = config2(present=present)
     drv = FrameDriver(sc)
     drv.initial_uploads()
-    runner = O.OracleFrameRunner(drv.world, sc.internal, sc.present, drv.clip.tex, sc.clip_res)
+    ref_frame = _ref_wgsl_frames(drv, sc, threads)
+    runner = None if ref_frame is not None else O.OracleFrameRunner(drv.world, sc.internal, sc.present,
+                                                                    drv.clip.tex, sc.clip_res)
 
     def step():
         if drv.frame >= 64:
             drv.frame = 0
         _, _, clip, cam = drv.step()
+        if ref_frame is not None:
+            return ref_frame(cam, clip[0])
         t0 = time.perf_counter()
         runner.render(cam, clip[0], threads=threads)
         return time.perf_counter() - t0
@@ -1114,18 +1170,23 @@ def main_reference(args, rank, world_size):
     dt = sum(step() for _ in range(args.steps))
     rays = sc.internal[0] * sc.internal[1] * args.steps
     v = rays / dt / 1e6
+    kind = "reference" if ref_frame is not None else "port"
+    note = ("the reference's own WGSL compute passes (main_primary, main_local_taa, main_godray, main_composite, "
+            "main_composite_taa) translated mechanically to C++ and run on the host cores; no Rust toolchain or "
+            "graphics stack here to run them as they are" if ref_frame is not None else
+            "reference is Rust+WGSL; no Rust toolchain or graphics stack here, so this arm runs the C++ scalar "
+            "restatement of its WGSL (oracle/) on the host cores")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": max(1, world_size),
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 2),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded value-noise world)",
         "config": bench_config(present, sc.internal, max(1, world_size)),
-        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": threads, "kind": kind,
                          "sample": "full frames of the same workload, one per step (path frames "
                                    f"{args.warmup}..{args.warmup + args.steps - 1}); passes timed, producers not"},
         "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "reference is Rust+WGSL; no Rust toolchain or graphics stack here, so this arm runs the C++ "
-                "scalar restatement of its WGSL (oracle/) on the host cores",
+        "note": note,
     }))
 
 
