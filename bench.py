@@ -1089,7 +1089,11 @@ def _ref_wgsl_frames(drv, sc, threads):
 
     if not vxe_build.REF_WGSL_LIB.exists():
         return None
-    ref = C.CDLL(str(vxe_build.REF_WGSL_LIB))
+    try:
+        ref = C.CDLL(str(vxe_build.REF_WGSL_LIB))
+    except OSError as e:  # built on another machine and unusable here: the port runs instead
+        print(f"reference arm: {vxe_build.REF_WGSL_LIB.name} does not load ({e}); timing the port", file=sys.stderr)
+        return None
     ref.ref_wgsl_frame.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32]
     w = drv.world
     iw, ih = sc.internal
