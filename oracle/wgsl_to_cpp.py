@@ -191,7 +191,10 @@ extern "C" int ref_wgsl_primary_tile(uint32_t tx, uint32_t ty, float* out) {
 # wait for).  The images are the caller's host arrays, wired as the frame's
 # bind groups wire them (render/state/bindgroups.rs): the godray and local
 # TAA passes write their "out" images, which the composite reads.  The
-# history inputs are the caller's (zero on a cold frame).
+# history inputs are the caller's (zero on a cold frame).  With more than one
+# host thread each thread runs whole workgroups (workgroup memory is
+# thread-local); the work counters of profile_flags are plain increments there,
+# so they are exact only on one thread (the bench and the pin keep them off).
 #   img[0..15]: color, depth, local, primary_hist_in, primary_hist_out,
 #   shadow_hist_in, shadow_hist_out (buffer, rows padded to 256 B),
 #   local_hist_in, local_hist_out, godray_hist_in, godray_out, pre_taa,
