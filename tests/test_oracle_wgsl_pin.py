@@ -441,7 +441,7 @@ def _frame_io(iw, ih, pw, ph):
             z(ph, pw, 4)]
 
 
-@pytest.mark.parametrize("scene,frames", [("features", 3), ("config1", 1), ("config2", 2)])
+@pytest.mark.parametrize("scene,frames", [("features", 3), ("config1", 1), ("config2", 2), ("config5", 1)])
 def test_oracle_frames_equal_translated_reference_wgsl(scene, frames):
     """Whole frames of the reference's own compute passes -- main_primary,
     main_local_taa, main_godray, main_composite, main_composite_taa, run per
@@ -455,7 +455,8 @@ def test_oracle_frames_equal_translated_reference_wgsl(scene, frames):
     from vxe import scenes
 
     fn = {"features": lambda: scenes.features(present=(128, 80)), "config1": scenes.config1,
-          "config2": lambda: scenes.config2(present=(320, 180))}[scene]
+          "config2": lambda: scenes.config2(present=(320, 180)),
+          "config5": lambda: scenes.config5(present=(320, 180))}[scene]
     ref, lo, ora_scene, w, cam, keep = _walk_setup(fn)
     runner, _, clip_params = keep
     drv_cam, drv_clip = cam, clip_params
