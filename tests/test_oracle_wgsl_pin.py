@@ -441,7 +441,7 @@ def _frame_io(iw, ih, pw, ph):
             z(ph, pw, 4)]
 
 
-@pytest.mark.parametrize("scene,frames", [("features", 3), ("config1", 1), ("config2", 2), ("config5", 1)])
+@pytest.mark.parametrize("scene,frames", [("features", 3), ("config1", 1), ("config2", 18), ("config5", 1)])
 def test_oracle_frames_equal_translated_reference_wgsl(scene, frames):
     """Whole frames of the reference's own compute passes -- main_primary,
     main_local_taa, main_godray, main_composite, main_composite_taa, run per
