@@ -215,6 +215,15 @@ static void parallel_rows(uint32_t rows, uint32_t threads, F body) {
     });
   for (auto& th : pool) th.join();
 }
+// The work counters of main_primary (profile_counts: VOXEL, GRASS, HDR, FOG,
+// SHADOW), accumulated while cam.profile_flags & 1; read into out5 and
+// cleared.
+extern "C" void ref_wgsl_take_profile(uint32_t* out5) {
+  for (int i = 0; i < 5; ++i) {
+    out5[i] = profile_counts.counts[i].v;
+    profile_counts.counts[i].v = 0u;
+  }
+}
 extern "C" int ref_wgsl_frame(uint32_t iw, uint32_t ih, uint32_t pw, uint32_t ph, float* const* img,
                               uint32_t threads) {
   auto t4 = [](float* p, uint32_t w, uint32_t h) { return Tex2D{p, (int32_t)w, (int32_t)h, 4}; };

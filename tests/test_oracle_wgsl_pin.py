@@ -490,3 +490,43 @@ def test_oracle_frames_equal_translated_reference_wgsl(scene, frames):
         io[7][:] = io[8]
         io[9][:] = io[10]
         io[12][:] = io[14]
+
+
+@pytest.mark.parametrize("scene", ["features", "config2"])
+def test_oracle_work_counters_equal_translated_reference_wgsl(scene):
+    """The work counters the reference's main_primary keeps while
+    cam.profile_flags & 1 (profile_counts: VOXEL, GRASS, HDR, FOG, SHADOW,
+    ray_main.wgsl:32-74), over two frames on one host thread, against the
+    oracle's counters of the same frames."""
+    from vxe import scenes
+
+    fn = {"features": lambda: scenes.features(present=(128, 80)),
+          "config2": lambda: scenes.config2(present=(320, 180))}[scene]
+    ref, lo, ora_scene, w, cam, keep = _walk_setup(fn)
+    runner, _, clip_params = keep
+    iw, ih, pw, ph = (cam.render_present_px[i] for i in range(4))
+    io = _frame_io(iw, ih, pw, ph)
+    ref.ref_wgsl_frame.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32]
+    ref.ref_wgsl_take_profile.argtypes = [C.c_void_p]
+    want = np.zeros(5, np.uint32)
+    ref.ref_wgsl_take_profile(want.ctypes.data)  # cleared
+    runner.profile[:] = 0
+    drv_cam, drv_clip = cam, clip_params
+    for f in range(2):
+        if f > 0:
+            _, _, clip, drv_cam = runner._driver.step()
+            drv_clip = clip[0] if clip is not None else runner._driver.empty_clip()
+        drv_cam.profile_flags = 1
+        _set_ref_camera(ref, w, drv_cam)
+        _set_ref_clip(ref, runner, drv_clip)
+        ptrs = (C.c_void_p * 15)(*[a.ctypes.data for a in io])
+        assert ref.ref_wgsl_frame(iw, ih, pw, ph, ptrs, 1) == 0
+        runner.render(drv_cam, drv_clip)
+        io[3][:] = io[4]
+        io[5][:] = io[6][:, :iw]
+        io[7][:] = io[8]
+        io[9][:] = io[10]
+        io[12][:] = io[14]
+    ref.ref_wgsl_take_profile(want.ctypes.data)
+    assert want[0] > 0 and want[4] > 0
+    assert want.tolist() == runner.profile.tolist()
