@@ -1,6 +1,8 @@
 """Known-answer checks of the oracle (CPU only).
 
-The reference ships no tests or golden vectors, so the oracle is pinned by:
+The reference ships no tests or golden vectors.  Its shaders themselves are
+run beside the oracle, translated to C++ (tests/test_oracle_wgsl_pin.py); the
+checks here pin the oracle independently of them:
   * an independent FP64 Amanatides-Woo voxel DDA over the dense material grid
     (first solid voxel identical, t within 1e-5 relative),
   * determinism across thread counts,
